@@ -1,0 +1,403 @@
+"""B200-native BK/BP Hex3D hot path: Python binding of libbp_b200.so.
+
+The library (include/bp_b200.h) replaces benchParanumal's OCCA platform layer
+and OKL kernels for the Hex3D BK/BP path.  This module mirrors the reference's
+host objects for that path:
+
+    Mesh      mesh_t for the Hex3D box + its masked ogs numbering
+              (libs/mesh/meshSetup.cpp, meshMaskedGatherScatterSetup.cpp)
+    BP        bpN_t : solver_t with Operator / forcing / cg::Solve
+              (BP/BP5/src/bp5{Setup,Operator,Run}.cpp, libs/core/linearSolverCG.cpp)
+    ax_hex3d  the bp5AxHex3D / bp5AxAffineHex3D / bp6AxHex3D kernels
+    ogs_gather / ogs_scatter   the ogs Gather(Add, Trans) / Scatter(NoTrans)
+
+Errors raise BPError carrying the library's message, the way the reference
+throws libp::exception.  There is no CPU fallback: without the built library
+or without a CUDA device every call fails loudly.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libbp_b200.so")
+
+BP_SUCCESS = 0
+BP_PRECON_NONE = 0
+BP_PRECON_JACOBI = 1
+BP_RHS_ANALYTIC = 0
+BP_RHS_RANDOM = 1
+
+EXPORTS = [
+    "bp_last_error", "bp_version", "bp_platform_init", "bp_device_count", "bp_device_info",
+    "bp_malloc", "bp_free", "bp_host_malloc", "bp_host_free", "bp_memcpy_htod", "bp_memcpy_dtoh",
+    "bp_memcpy_dtod", "bp_memset", "bp_stream_create", "bp_stream_destroy", "bp_finish",
+    "bp_event_create", "bp_event_destroy", "bp_event_record", "bp_event_elapsed_ms",
+    "bp_ax_hex3d", "bp_ogs_gather", "bp_ogs_scatter", "bp_linalg_set", "bp_linalg_axpy",
+    "bp_linalg_inner_prod", "bp_linalg_norm2", "bp_update_cg",
+    "bp_mesh_create", "bp_mesh_view", "bp_mesh_destroy",
+    "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
+    "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
+    "bp_box_numbering", "bp_basis_gll", "bp_box_vertices",
+]
+
+
+class BPError(RuntimeError):
+    """A C-ABI call returned an error status (libp::exception equivalent)."""
+
+    def __init__(self, code, msg):
+        super().__init__("bp error %d: %s" % (code, msg))
+        self.code = code
+
+
+class AxDesc(ctypes.Structure):
+    _fields_ = [("bp", ctypes.c_int32), ("N", ctypes.c_int32), ("affine", ctypes.c_int32),
+                ("Nfields", ctypes.c_int32)]
+
+
+class BoxDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("N", ctypes.c_int32),
+                ("affine", ctypes.c_int32), ("Nfields", ctypes.c_int32), ("pert", ctypes.c_double),
+                ("pert_seed", ctypes.c_uint64)]
+
+
+class MeshView(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int32), ("Nq", ctypes.c_int32), ("Np", ctypes.c_int32),
+                ("Nelements", ctypes.c_int32), ("Nfields", ctypes.c_int32), ("affine", ctypes.c_int32),
+                ("Ngather", ctypes.c_int32), ("nnz", ctypes.c_int32), ("Nlocal", ctypes.c_int64)] + [
+        (n, ctypes.c_void_p) for n in ("elementList", "GlobalToLocal", "rowStarts", "colIds", "wJ", "ggeo", "D",
+                                       "gllz", "gllw", "EX", "EY", "EZ")]
+
+
+class SolverDesc(ctypes.Structure):
+    _fields_ = [("bp", ctypes.c_int32), ("lambda_", ctypes.c_double), ("precon", ctypes.c_int32)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("rdotr0", ctypes.c_double), ("rdotr", ctypes.c_double),
+                ("elapsed_ms", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libbp_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BPError(-1, "libbp_b200.so is not built; run python -m benchparanumal_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64, dbl, u64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_uint64
+        sz = ctypes.c_size_t
+        L.bp_last_error.restype = ctypes.c_char_p
+        L.bp_version.restype = ctypes.c_char_p
+        sigs = {
+            "bp_platform_init": [ctypes.c_int],
+            "bp_device_count": [ctypes.POINTER(ctypes.c_int)],
+            "bp_device_info": [ctypes.c_char_p, sz, ctypes.POINTER(ctypes.c_int)],
+            "bp_malloc": [ctypes.POINTER(vp), sz],
+            "bp_free": [vp],
+            "bp_host_malloc": [ctypes.POINTER(vp), sz],
+            "bp_host_free": [vp],
+            "bp_memcpy_htod": [vp, vp, sz, vp],
+            "bp_memcpy_dtoh": [vp, vp, sz, vp],
+            "bp_memcpy_dtod": [vp, vp, sz, vp],
+            "bp_memset": [vp, ctypes.c_int, sz, vp],
+            "bp_stream_create": [ctypes.POINTER(vp)],
+            "bp_stream_destroy": [vp],
+            "bp_finish": [vp],
+            "bp_event_create": [ctypes.POINTER(vp)],
+            "bp_event_destroy": [vp],
+            "bp_event_record": [vp, vp],
+            "bp_event_elapsed_ms": [vp, vp, ctypes.POINTER(ctypes.c_float)],
+            "bp_ax_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
+            "bp_ogs_gather": [i32, vp, vp, vp, vp, vp],
+            "bp_ogs_scatter": [i32, vp, vp, vp, vp, vp],
+            "bp_linalg_set": [i32, dbl, vp, vp],
+            "bp_linalg_axpy": [i32, dbl, vp, dbl, vp, vp],
+            "bp_linalg_inner_prod": [i32, vp, vp, vp, vp],
+            "bp_linalg_norm2": [i32, vp, vp, vp],
+            "bp_update_cg": [i32, vp, dbl, vp, vp, vp],
+            "bp_mesh_create": [ctypes.POINTER(BoxDesc), ctypes.POINTER(vp)],
+            "bp_mesh_view": [vp, ctypes.POINTER(MeshView)],
+            "bp_mesh_destroy": [vp],
+            "bp_solver_create": [vp, ctypes.POINTER(SolverDesc), ctypes.POINTER(vp)],
+            "bp_solver_destroy": [vp],
+            "bp_solver_size": [vp, ctypes.POINTER(i32)],
+            "bp_solver_operator": [vp, vp, vp, vp],
+            "bp_solver_rhs": [vp, i32, u64, vp, vp],
+            "bp_solver_diagonal": [vp, vp],
+            "bp_solver_solve": [vp, vp, vp, dbl, i32, vp, vp, ctypes.POINTER(SolveStats)],
+            "bp_solver_solve_host": [vp, vp, vp, dbl, i32, ctypes.POINTER(SolveStats)],
+            "bp_driver_main": [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)],
+            "bp_box_numbering": [ctypes.POINTER(BoxDesc), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, vp, vp],
+            "bp_basis_gll": [i32, vp, vp, vp],
+            "bp_box_vertices": [ctypes.POINTER(BoxDesc), vp, vp, vp],
+        }
+        for name, args in sigs.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != BP_SUCCESS:
+        raise BPError(rc, lib().bp_last_error().decode(errors="replace"))
+
+
+_initialised = None
+
+
+def platform_init(device=0):
+    """-m CUDA -d <device>: select the device (sm_100a required)."""
+    global _initialised
+    if _initialised != device:
+        _check(lib().bp_platform_init(device))
+        _initialised = device
+
+
+def finish():
+    """platform.finish(): wait for the library's stream."""
+    _check(lib().bp_finish(None))
+
+
+class DeviceBuffer:
+    """A device allocation from bp_malloc holding `n` items of `dtype`."""
+
+    def __init__(self, n, dtype=np.float64):
+        self.dtype = np.dtype(dtype)
+        self.n = int(n)
+        self.nbytes = self.n * self.dtype.itemsize
+        p = ctypes.c_void_p()
+        _check(lib().bp_malloc(ctypes.byref(p), self.nbytes))
+        self.ptr = p.value or 0
+
+    @classmethod
+    def from_host(cls, a):
+        a = np.ascontiguousarray(a)
+        b = cls(a.size, a.dtype)
+        b.upload(a)
+        return b
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        assert a.size == self.n
+        _check(lib().bp_memcpy_htod(self.ptr, a.ctypes.data, self.nbytes, None))
+        finish()
+
+    def download(self):
+        out = np.empty(self.n, dtype=self.dtype)
+        _check(lib().bp_memcpy_dtoh(out.ctypes.data, self.ptr, self.nbytes, None))
+        finish()
+        return out
+
+    def zero(self):
+        _check(lib().bp_memset(self.ptr, 0, self.nbytes, None))
+
+    def free(self):
+        if getattr(self, "ptr", 0):
+            lib().bp_free(self.ptr)
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class PinnedBuffer:
+    """Page-locked host memory from bp_host_malloc, viewed as a numpy array."""
+
+    def __init__(self, n, dtype=np.float64):
+        self.dtype = np.dtype(dtype)
+        self.n = int(n)
+        p = ctypes.c_void_p()
+        _check(lib().bp_host_malloc(ctypes.byref(p), self.n * self.dtype.itemsize))
+        self.ptr = p.value or 0
+        ct = np.ctypeslib.as_ctypes_type(self.dtype)
+        self.array = np.frombuffer((ct * self.n).from_address(self.ptr), dtype=self.dtype) if self.n else \
+            np.empty(0, self.dtype)
+
+    def free(self):
+        if getattr(self, "ptr", 0):
+            self.array = None
+            lib().bp_host_free(self.ptr)
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _dl(ptr, n, dtype):
+    out = np.empty(n, dtype=dtype)
+    if n:
+        _check(lib().bp_memcpy_dtoh(out.ctypes.data, ptr, out.nbytes, None))
+        finish()
+    return out
+
+
+class Mesh:
+    """Hex3D box mesh on the device (mesh_t + masked ogs), built by bp_mesh_create."""
+
+    def __init__(self, nx, ny=None, nz=None, N=4, affine=False, Nfields=1, pert=0.0, pert_seed=1, device=0):
+        platform_init(device)
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        d = BoxDesc(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), int(pert_seed))
+        h = ctypes.c_void_p()
+        _check(lib().bp_mesh_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h.value
+        self.view = MeshView()
+        _check(lib().bp_mesh_view(self._h, ctypes.byref(self.view)))
+        v = self.view
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.N, self.Nq, self.Np, self.E = v.N, v.Nq, v.Np, v.Nelements
+        self.Nfields, self.affine = v.Nfields, bool(v.affine)
+        self.Ngather, self.nnz, self.NL = v.Ngather, v.nnz, int(v.Nlocal)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().bp_mesh_destroy(self._h)
+            self._h = None
+
+    def array(self, name):
+        """Copy a device mesh array to the host (names as in bp_mesh_view_t)."""
+        v = self.view
+        ng = self.E if self.affine else self.E * self.Np
+        spec = {
+            "elementList": (self.E, np.int32), "GlobalToLocal": (self.NL, np.int32),
+            "rowStarts": (self.Ngather + 1, np.int32), "colIds": (self.nnz, np.int32),
+            "wJ": (ng, np.float64), "ggeo": (6 * ng, np.float64), "D": (self.Nq * self.Nq, np.float64),
+            "gllz": (self.Nq, np.float64), "gllw": (self.Nq, np.float64), "EX": (8 * self.E, np.float64),
+            "EY": (8 * self.E, np.float64), "EZ": (8 * self.E, np.float64),
+        }
+        n, dt = spec[name]
+        return _dl(getattr(v, name), n, dt)
+
+
+def ax_hex3d(mesh, q, Aq, lam=1.0, elementList=None, Nelements=None, stream=None):
+    """bp_ax_hex3d on device buffers: Aq (E-vector) = A_e q[GlobalToLocal]."""
+    v = mesh.view
+    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    el = v.elementList if elementList is None else elementList
+    ne = mesh.E if Nelements is None else Nelements
+    _check(lib().bp_ax_hex3d(ctypes.byref(d), ne, el, v.GlobalToLocal, v.wJ, v.ggeo, v.gllw, v.D, float(lam),
+                             _ptr(q), _ptr(Aq), stream))
+
+
+def ogs_gather(mesh, v, gv, stream=None):
+    _check(lib().bp_ogs_gather(mesh.Ngather, mesh.view.rowStarts, mesh.view.colIds, _ptr(v), _ptr(gv), stream))
+
+
+def ogs_scatter(mesh, gv, v, stream=None):
+    _check(lib().bp_ogs_scatter(mesh.Ngather, mesh.view.rowStarts, mesh.view.colIds, _ptr(gv), _ptr(v), stream))
+
+
+def _ptr(b):
+    if isinstance(b, DeviceBuffer):
+        return b.ptr
+    if isinstance(b, int):
+        return b
+    raise TypeError("expected a DeviceBuffer or a device address")
+
+
+class BP:
+    """Benchmark problem on a Mesh: bp 5 (scalar) or 6 (three fields)."""
+
+    def __init__(self, mesh, bp=None, lam=1.0, precon="NONE"):
+        self.mesh = mesh
+        bp = bp or (6 if mesh.Nfields == 3 else 5)
+        pc = {"NONE": BP_PRECON_NONE, "JACOBI": BP_PRECON_JACOBI}[precon.upper()]
+        d = SolverDesc(bp, float(lam), pc)
+        h = ctypes.c_void_p()
+        _check(lib().bp_solver_create(mesh._h, ctypes.byref(d), ctypes.byref(h)))
+        self._h = h.value
+        self.N = mesh.Ngather
+        self.precon = precon.upper()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().bp_solver_destroy(self._h)
+            self._h = None
+
+    def operator(self, q, Aq, stream=None):
+        """solver_t::Operator: Aq = Gather(A_e q[G2L]) on device buffers."""
+        _check(lib().bp_solver_operator(self._h, _ptr(q), _ptr(Aq), stream))
+
+    def rhs(self, mode="ANALYTIC", seed=0, b=None, f=None):
+        """Gathered forcing into a device buffer (returned)."""
+        b = b or DeviceBuffer(self.N)
+        m = {"ANALYTIC": BP_RHS_ANALYTIC, "RANDOM": BP_RHS_RANDOM}[mode.upper()]
+        _check(lib().bp_solver_rhs(self._h, m, int(seed), b.ptr, f.ptr if f is not None else None))
+        return b
+
+    def diagonal(self):
+        d = DeviceBuffer(self.N)
+        _check(lib().bp_solver_diagonal(self._h, d.ptr))
+        return d
+
+    def solve(self, x, r, tol=0.0, maxit=100, history=True):
+        """cg::Solve on device buffers (x in/out, r = b in / residual out).
+        Returns (stats, rnorm_history, alpha_history)."""
+        st = SolveStats()
+        hr = np.zeros(max(maxit, 1))
+        ha = np.zeros(max(maxit, 1))
+        _check(lib().bp_solver_solve(self._h, x.ptr, r.ptr, float(tol), int(maxit),
+                                     hr.ctypes.data if history else None, ha.ctypes.data if history else None,
+                                     ctypes.byref(st)))
+        it = st.iterations
+        return st, hr[:it], ha[:it]
+
+    def solve_host(self, b_host, x_host, tol=0.0, maxit=100):
+        """The same solve from host arrays (copies inside the call)."""
+        st = SolveStats()
+        b_host = np.ascontiguousarray(b_host, dtype=np.float64)
+        assert x_host.dtype == np.float64 and x_host.flags.c_contiguous
+        _check(lib().bp_solver_solve_host(self._h, b_host.ctypes.data, x_host.ctypes.data, float(tol), int(maxit),
+                                          ctypes.byref(st)))
+        return st
+
+
+def box_numbering(nx, ny, nz, N, Nfields=1):
+    """Host-only masked numbering of the box: (GlobalToLocal, rowStarts, colIds)."""
+    d = BoxDesc(nx, ny, nz, N, 0, Nfields, 0.0, 1)
+    ng, nnz = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().bp_box_numbering(ctypes.byref(d), ctypes.byref(ng), ctypes.byref(nnz), None, None, None))
+    E = nx * ny * nz
+    Np = (N + 1) ** 3
+    g2l = np.empty(E * Np * Nfields, np.int32)
+    rs = np.empty(ng.value + 1, np.int32)
+    ci = np.empty(nnz.value, np.int32)
+    _check(lib().bp_box_numbering(ctypes.byref(d), None, None, g2l.ctypes.data, rs.ctypes.data, ci.ctypes.data))
+    return g2l, rs, ci
+
+
+def basis_gll(N):
+    """Host-only GLL nodes, weights and differentiation matrix of degree N."""
+    z = np.empty(N + 1); w = np.empty(N + 1); D = np.empty((N + 1) * (N + 1))
+    _check(lib().bp_basis_gll(N, z.ctypes.data, w.ctypes.data, D.ctypes.data))
+    return z, w, D.reshape(N + 1, N + 1)
+
+
+def box_vertices(nx, ny, nz, pert=0.0, pert_seed=1):
+    """Host-only vertex coordinates (EX, EY, EZ), each [E*8]."""
+    d = BoxDesc(nx, ny, nz, 1, 0, 1, float(pert), int(pert_seed))
+    E = nx * ny * nz
+    ex, ey, ez = (np.empty(8 * E) for _ in range(3))
+    _check(lib().bp_box_vertices(ctypes.byref(d), ex.ctypes.data, ey.ctypes.data, ez.ctypes.data))
+    return ex, ey, ez
+
+
+def driver_main(name, args):
+    """Run a BK/BP executable's main() in-process (e.g. driver_main("BP5", ["-nx","8"]))."""
+    argv = [name.encode()] + [a.encode() for a in args]
+    arr = (ctypes.c_char_p * len(argv))(*argv)
+    return lib().bp_driver_main(name.encode(), len(argv), arr)

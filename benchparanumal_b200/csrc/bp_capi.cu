@@ -1,0 +1,351 @@
+// C ABI: platform (device, memory, streams, events), kernel entry points and
+// mesh setup.  See include/bp_b200.h for the contract of each function.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "bp_internal.hpp"
+
+namespace bp {
+
+static thread_local std::string g_last_error;
+static cudaStream_t g_stream = nullptr;
+static int g_sm_count = 0;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t err, const char* what, const char* file, int line) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%s failed at %s:%d: %s", what, file, line, cudaGetErrorString(err));
+  g_last_error = buf;
+  return err == cudaErrorMemoryAllocation ? BP_ERROR_ALLOC : BP_ERROR_CUDA;
+}
+
+cudaStream_t default_stream() {
+  if (!g_stream) cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking);
+  return g_stream;
+}
+
+int sm_count() {
+  if (!g_sm_count) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+}  // namespace bp
+
+using namespace bp;
+
+extern "C" {
+
+const char* bp_last_error(void) { return g_last_error.c_str(); }
+
+const char* bp_version(void) { return "benchparanumal_b200 0.1 (sm_100a)"; }
+
+int bp_platform_init(int device_id) {
+  int n = 0;
+  BP_CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device_id < 0 || device_id >= n)
+    return fail(BP_ERROR_ARG, "bp_platform_init: device " + std::to_string(device_id) + " not present (" +
+                                  std::to_string(n) + " devices)");
+  BP_CUDA_TRY(cudaSetDevice(device_id));
+  BP_CUDA_TRY(cudaFree(0));
+  int major = 0, minor = 0;
+  BP_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device_id));
+  BP_CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device_id));
+  if (major != 10)
+    return fail(BP_ERROR_ARG, "bp_platform_init: this build targets sm_100a (B200); device has sm_" +
+                                  std::to_string(major) + std::to_string(minor));
+  (void)default_stream();
+  clear_error();
+  return BP_SUCCESS;
+}
+
+int bp_device_count(int* count) {
+  if (!count) return fail(BP_ERROR_ARG, "bp_device_count: null pointer");
+  BP_CUDA_TRY(cudaGetDeviceCount(count));
+  return BP_SUCCESS;
+}
+
+int bp_device_info(char* name, size_t name_len, int* sms) {
+  int dev = 0;
+  BP_CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceProp p;
+  BP_CUDA_TRY(cudaGetDeviceProperties(&p, dev));
+  if (name && name_len) {
+    std::strncpy(name, p.name, name_len - 1);
+    name[name_len - 1] = 0;
+  }
+  if (sms) *sms = p.multiProcessorCount;
+  return BP_SUCCESS;
+}
+
+int bp_malloc(void** ptr, size_t bytes) {
+  if (!ptr) return fail(BP_ERROR_ARG, "bp_malloc: null pointer");
+  *ptr = nullptr;
+  if (bytes == 0) return BP_SUCCESS;
+  BP_CUDA_TRY(cudaMalloc(ptr, bytes));
+  return BP_SUCCESS;
+}
+
+int bp_free(void* ptr) {
+  if (ptr) BP_CUDA_TRY(cudaFree(ptr));
+  return BP_SUCCESS;
+}
+
+int bp_host_malloc(void** ptr, size_t bytes) {
+  if (!ptr) return fail(BP_ERROR_ARG, "bp_host_malloc: null pointer");
+  *ptr = nullptr;
+  if (bytes == 0) return BP_SUCCESS;
+  BP_CUDA_TRY(cudaMallocHost(ptr, bytes));
+  return BP_SUCCESS;
+}
+
+int bp_host_free(void* ptr) {
+  if (ptr) BP_CUDA_TRY(cudaFreeHost(ptr));
+  return BP_SUCCESS;
+}
+
+int bp_memcpy_htod(void* dst, const void* src, size_t bytes, bp_stream_t s) {
+  if (bytes == 0) return BP_SUCCESS;
+  BP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, to_stream(s)));
+  return BP_SUCCESS;
+}
+
+int bp_memcpy_dtoh(void* dst, const void* src, size_t bytes, bp_stream_t s) {
+  if (bytes == 0) return BP_SUCCESS;
+  BP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, to_stream(s)));
+  return BP_SUCCESS;
+}
+
+int bp_memcpy_dtod(void* dst, const void* src, size_t bytes, bp_stream_t s) {
+  if (bytes == 0) return BP_SUCCESS;
+  BP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, to_stream(s)));
+  return BP_SUCCESS;
+}
+
+int bp_memset(void* dst, int value, size_t bytes, bp_stream_t s) {
+  if (bytes == 0) return BP_SUCCESS;
+  BP_CUDA_TRY(cudaMemsetAsync(dst, value, bytes, to_stream(s)));
+  return BP_SUCCESS;
+}
+
+int bp_stream_create(bp_stream_t* s) {
+  if (!s) return fail(BP_ERROR_ARG, "bp_stream_create: null pointer");
+  cudaStream_t cs;
+  BP_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  *s = reinterpret_cast<bp_stream_t>(cs);
+  return BP_SUCCESS;
+}
+
+int bp_stream_destroy(bp_stream_t s) {
+  if (s) BP_CUDA_TRY(cudaStreamDestroy(reinterpret_cast<cudaStream_t>(s)));
+  return BP_SUCCESS;
+}
+
+int bp_finish(bp_stream_t s) {
+  BP_CUDA_TRY(cudaStreamSynchronize(to_stream(s)));
+  return BP_SUCCESS;
+}
+
+int bp_event_create(bp_event_t* ev) {
+  if (!ev) return fail(BP_ERROR_ARG, "bp_event_create: null pointer");
+  cudaEvent_t e;
+  BP_CUDA_TRY(cudaEventCreate(&e));
+  *ev = reinterpret_cast<bp_event_t>(e);
+  return BP_SUCCESS;
+}
+
+int bp_event_destroy(bp_event_t ev) {
+  if (ev) BP_CUDA_TRY(cudaEventDestroy(reinterpret_cast<cudaEvent_t>(ev)));
+  return BP_SUCCESS;
+}
+
+int bp_event_record(bp_event_t ev, bp_stream_t s) {
+  BP_CUDA_TRY(cudaEventRecord(reinterpret_cast<cudaEvent_t>(ev), to_stream(s)));
+  return BP_SUCCESS;
+}
+
+int bp_event_elapsed_ms(bp_event_t a, bp_event_t b, float* ms) {
+  if (!ms) return fail(BP_ERROR_ARG, "bp_event_elapsed_ms: null pointer");
+  BP_CUDA_TRY(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(b)));
+  BP_CUDA_TRY(cudaEventElapsedTime(ms, reinterpret_cast<cudaEvent_t>(a), reinterpret_cast<cudaEvent_t>(b)));
+  return BP_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// kernel entry points
+// ---------------------------------------------------------------------------
+static int check_ax_desc(const bp_ax_desc_t* d) {
+  if (!d) return fail(BP_ERROR_ARG, "bp_ax_hex3d: null descriptor");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_hex3d: degree N must be in 1..15");
+  if (d->Nfields != 1 && d->Nfields != 3) return fail(BP_ERROR_ARG, "bp_ax_hex3d: Nfields must be 1 or 3");
+  if (d->bp != 5 && d->bp != 6) return fail(BP_ERROR_ARG, "bp_ax_hex3d: bp must be 5 or 6");
+  if ((d->bp == 6) != (d->Nfields == 3)) return fail(BP_ERROR_ARG, "bp_ax_hex3d: BP6 has 3 fields, BP5 one");
+  return BP_SUCCESS;
+}
+
+int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                const int32_t* GlobalToLocal, const double* wJ, const double* ggeo, const double* gllw,
+                const double* D, double lambda, const double* q, double* Aq, bp_stream_t stream) {
+  BP_TRY(check_ax_desc(desc));
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_hex3d: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  if (!elementList || !GlobalToLocal || !wJ || !ggeo || !D || !q || !Aq || (desc->affine && !gllw))
+    return fail(BP_ERROR_ARG, "bp_ax_hex3d: null array");
+  return launch_ax(*desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq,
+                   to_stream(stream));
+}
+
+int bp_ogs_gather(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* v, double* gv,
+                  bp_stream_t stream) {
+  if (Nrows < 0) return fail(BP_ERROR_ARG, "bp_ogs_gather: negative row count");
+  if (Nrows == 0) return BP_SUCCESS;
+  if (!rowStarts || !colIds || !v || !gv) return fail(BP_ERROR_ARG, "bp_ogs_gather: null array");
+  return launch_gather(Nrows, rowStarts, colIds, v, gv, to_stream(stream));
+}
+
+int bp_ogs_scatter(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* gv, double* v,
+                   bp_stream_t stream) {
+  if (Nrows < 0) return fail(BP_ERROR_ARG, "bp_ogs_scatter: negative row count");
+  if (Nrows == 0) return BP_SUCCESS;
+  if (!rowStarts || !colIds || !v || !gv) return fail(BP_ERROR_ARG, "bp_ogs_scatter: null array");
+  return launch_scatter(Nrows, rowStarts, colIds, gv, v, to_stream(stream));
+}
+
+int bp_linalg_set(int32_t N, double alpha, double* x, bp_stream_t s) {
+  if (N < 0 || (N > 0 && !x)) return fail(BP_ERROR_ARG, "bp_linalg_set: bad arguments");
+  return launch_set(N, alpha, x, to_stream(s));
+}
+
+int bp_linalg_axpy(int32_t N, double alpha, const double* x, double beta, double* y, bp_stream_t s) {
+  if (N < 0 || (N > 0 && (!x || !y))) return fail(BP_ERROR_ARG, "bp_linalg_axpy: bad arguments");
+  return launch_axpy(N, alpha, x, beta, y, to_stream(s));
+}
+
+// scratch for the standalone reductions: partial sums and the arrival counter
+static double* g_red_partials = nullptr;
+static unsigned int* g_red_counter = nullptr;
+static int red_scratch() {
+  if (!g_red_partials) {
+    BP_CUDA_TRY(cudaMalloc(&g_red_partials, sizeof(double) * 4 * reduction_blocks()));
+    BP_CUDA_TRY(cudaMalloc(&g_red_counter, sizeof(unsigned int) * 4));
+    BP_CUDA_TRY(cudaMemset(g_red_counter, 0, sizeof(unsigned int) * 4));
+  }
+  return BP_SUCCESS;
+}
+
+int bp_linalg_inner_prod(int32_t N, const double* x, const double* y, double* result, bp_stream_t s) {
+  if (N < 0 || !result || (N > 0 && (!x || !y))) return fail(BP_ERROR_ARG, "bp_linalg_inner_prod: bad arguments");
+  BP_TRY(red_scratch());
+  return launch_dot(N, x, y, result, g_red_partials, g_red_counter, to_stream(s));
+}
+
+int bp_linalg_norm2(int32_t N, const double* x, double* result, bp_stream_t s) {
+  if (N < 0 || !result || (N > 0 && !x)) return fail(BP_ERROR_ARG, "bp_linalg_norm2: bad arguments");
+  BP_TRY(red_scratch());
+  BP_TRY(launch_dot(N, x, x, result, g_red_partials, g_red_counter, to_stream(s)));
+  return launch_sqrt1(result, to_stream(s));
+}
+
+int bp_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* rdotr, bp_stream_t s) {
+  if (N < 0 || !rdotr || (N > 0 && (!Ap || !r))) return fail(BP_ERROR_ARG, "bp_update_cg: bad arguments");
+  BP_TRY(red_scratch());
+  return launch_update_cg(N, Ap, alpha, r, rdotr, g_red_partials, g_red_counter, to_stream(s));
+}
+
+// ---------------------------------------------------------------------------
+// mesh
+// ---------------------------------------------------------------------------
+int bp_mesh_create(const bp_box_desc_t* d, bp_mesh_t* out) {
+  if (!d || !out) return fail(BP_ERROR_ARG, "bp_mesh_create: null pointer");
+  *out = nullptr;
+  if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
+  if (d->Nfields != 1 && d->Nfields != 3) return fail(BP_ERROR_ARG, "bp_mesh_create: Nfields must be 1 or 3");
+  if (!(d->pert >= 0.0 && d->pert < 0.5)) return fail(BP_ERROR_ARG, "bp_mesh_create: perturbation must be in [0, 0.5)");
+  const int64_t E64 = (int64_t)d->nx * d->ny * d->nz;
+  const int Nq = d->N + 1, Np = Nq * Nq * Nq;
+  if (E64 * Np * d->Nfields >= (int64_t)INT32_MAX)
+    return fail(BP_ERROR_ARG, "bp_mesh_create: local node count exceeds int32 (dlong) range");
+  cudaStream_t s = default_stream();
+
+  HostMesh hm;
+  hm.N = d->N; hm.Nq = Nq; hm.Np = Np;
+  hm.nx = d->nx; hm.ny = d->ny; hm.nz = d->nz;
+  hm.E = (int)E64; hm.affine = d->affine ? 1 : 0; hm.Nfields = d->Nfields;
+  gll_nodes_weights(hm.N, hm.gllz, hm.gllw);
+  diff_matrix(hm.gllz, hm.D);
+  box_vertices(hm, d->pert, d->pert_seed);
+  box_numbering(hm);
+
+  bp_mesh_s* m = new bp_mesh_s();
+  m->N = hm.N; m->Nq = Nq; m->Np = Np; m->E = hm.E; m->Nfields = hm.Nfields; m->affine = hm.affine;
+  m->Ngather = hm.Ngather; m->nnz = hm.nnz;
+  std::vector<int32_t> elist(hm.E);
+  for (int e = 0; e < hm.E; ++e) elist[e] = e;
+  int rc = BP_SUCCESS;
+  int* d_bad = nullptr;
+  do {
+    if ((rc = m->elementList.upload(elist, s))) break;
+    if ((rc = m->G2L.upload(hm.G2L, s))) break;
+    if ((rc = m->rowStarts.upload(hm.rowStarts, s))) break;
+    if ((rc = m->colIds.upload(hm.colIds, s))) break;
+    if ((rc = m->D.upload(hm.D, s))) break;
+    if ((rc = m->gllz.upload(hm.gllz, s))) break;
+    if ((rc = m->gllw.upload(hm.gllw, s))) break;
+    if ((rc = m->EX.upload(hm.EX, s))) break;
+    if ((rc = m->EY.upload(hm.EY, s))) break;
+    if ((rc = m->EZ.upload(hm.EZ, s))) break;
+    const size_t ng = hm.affine ? (size_t)hm.E : (size_t)hm.E * Np;
+    if ((rc = m->wJ.alloc(ng))) break;
+    if ((rc = m->ggeo.alloc(6 * ng))) break;
+    cudaError_t ce = cudaMalloc(&d_bad, sizeof(int));
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "cudaMalloc", __FILE__, __LINE__); break; }
+    cudaMemsetAsync(d_bad, 0, sizeof(int), s);
+    if ((rc = launch_geometry(hm.N, hm.affine, hm.E, m->EX.ptr, m->EY.ptr, m->EZ.ptr, m->gllz.ptr, m->gllw.ptr,
+                              m->wJ.ptr, m->ggeo.ptr, d_bad, s)))
+      break;
+    int bad = 0;
+    ce = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "geometry setup", __FILE__, __LINE__); break; }
+    if (bad) { rc = fail(BP_ERROR_NUMERIC, "bp_mesh_create: non-positive Jacobian found (perturbation too large?)"); break; }
+  } while (0);
+  if (d_bad) cudaFree(d_bad);
+  if (rc != BP_SUCCESS) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return BP_SUCCESS;
+}
+
+int bp_mesh_view(bp_mesh_t m, bp_mesh_view_t* v) {
+  if (!m || !v) return fail(BP_ERROR_ARG, "bp_mesh_view: null pointer");
+  v->N = m->N; v->Nq = m->Nq; v->Np = m->Np; v->Nelements = m->E; v->Nfields = m->Nfields;
+  v->affine = m->affine; v->Ngather = m->Ngather; v->nnz = m->nnz;
+  v->Nlocal = (int64_t)m->E * m->Np * m->Nfields;
+  v->elementList = m->elementList.ptr; v->GlobalToLocal = m->G2L.ptr;
+  v->rowStarts = m->rowStarts.ptr; v->colIds = m->colIds.ptr;
+  v->wJ = m->wJ.ptr; v->ggeo = m->ggeo.ptr; v->D = m->D.ptr; v->gllz = m->gllz.ptr; v->gllw = m->gllw.ptr;
+  v->EX = m->EX.ptr; v->EY = m->EY.ptr; v->EZ = m->EZ.ptr;
+  return BP_SUCCESS;
+}
+
+int bp_mesh_destroy(bp_mesh_t m) {
+  delete m;
+  return BP_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,345 @@
+// BK5 / BP5 drivers behind bp_driver_main(): the reference executables'
+// command-line keys, settings semantics and result lines, running on the C ABI.
+//
+// Settings semantics follow libs/core/settings.cpp:
+//   * every setting has a short key, long key, name, default, description and
+//     an optional list of allowed values (updateVal rejects anything else);
+//   * "-v"/"--verbose" and "-a"/"--affine" take no value;
+//   * a setting given twice on the command line is an error;
+//   * compareSetting is a substring test; "-h"/"--help" prints the usage.
+// Keys come from libs/core/platformSettings.cpp:31-50,
+// libs/mesh/meshSettings.cpp:31-62 and BP/BP5/src/bp5Settings.cpp:30-46.
+// Keys marked "extension" select the modes the reference does not have.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/bp_b200.h"
+
+namespace {
+
+struct Setting {
+  std::string shortkey, longkey, name, val, description;
+  std::vector<std::string> options;
+  bool set_on_cmdline = false;
+};
+
+class Settings {
+ public:
+  void add(const std::string& sk, const std::string& lk, const std::string& name, const std::string& val,
+           const std::string& desc, const std::vector<std::string>& options = {}) {
+    for (auto& it : map_)
+      if (it.second.shortkey == sk || it.second.longkey == lk)
+        throw std::runtime_error("Setting with key: [" + sk + "] already exists.");
+    if (map_.count(name)) throw std::runtime_error("Setting with name: [" + name + "] already exists.");
+    map_[name] = Setting{sk, lk, name, val, desc, options, false};
+    order_.push_back(name);
+  }
+  void change(const std::string& name, const std::string& v) {
+    auto it = map_.find(name);
+    if (it == map_.end()) throw std::runtime_error("Setting with name: [" + name + "] does not exist.");
+    Setting& s = it->second;
+    if (!s.options.empty()) {
+      bool ok = false;
+      for (auto& o : s.options) ok = ok || (o == v);
+      if (!ok) {
+        std::ostringstream ss;
+        ss << "Value: \"" << v << "\" not valid for setting " << name << "\nPossible values are: { ";
+        for (size_t i = 0; i < s.options.size(); ++i) ss << s.options[i] << (i + 1 < s.options.size() ? ", " : " }");
+        throw std::runtime_error(ss.str());
+      }
+    }
+    s.val = v;
+  }
+  // returns false when -h was given (usage printed)
+  bool parse(int argc, char** argv) {
+    for (int i = 1; i < argc;) {
+      if (!std::strcmp(argv[i], "-h") || !std::strcmp(argv[i], "--help")) {
+        usage();
+        return false;
+      }
+      bool matched = false;
+      for (auto& it : map_) {
+        Setting& s = it.second;
+        if (s.shortkey != argv[i] && s.longkey != argv[i]) continue;
+        matched = true;
+        if (s.set_on_cmdline)
+          throw std::runtime_error("Cannot set setting [" + s.name + "] twice in run command.");
+        if (!std::strcmp(argv[i], "-v") || !std::strcmp(argv[i], "--verbose")) {
+          change("VERBOSE", "TRUE");
+          i += 1;
+        } else if (!std::strcmp(argv[i], "-a") || !std::strcmp(argv[i], "--affine")) {
+          change("AFFINE MESH", "TRUE");
+          i += 1;
+        } else {
+          if (i + 1 >= argc) throw std::runtime_error(std::string("Missing value for option ") + argv[i]);
+          change(s.name, argv[i + 1]);
+          i += 2;
+        }
+        s.set_on_cmdline = true;
+        break;
+      }
+      if (!matched) throw std::runtime_error(std::string("Unknown option ") + argv[i] + " (see -h)");
+    }
+    return true;
+  }
+  std::string get(const std::string& name) const {
+    auto it = map_.find(name);
+    if (it == map_.end()) throw std::runtime_error("Unable to find setting: [" + name + "]");
+    return it->second.val;
+  }
+  bool compare(const std::string& name, const std::string& token) const {
+    return get(name).find(token) != std::string::npos;
+  }
+  void usage() const {
+    std::cout << "Usage:\n\n";
+    for (auto& n : order_) {
+      const Setting& s = map_.at(n);
+      std::cout << "Name:     [" << s.name << "]\n";
+      std::cout << "CL keys:  [" << s.shortkey << ", " << s.longkey << "]\n";
+      if (!s.description.empty()) std::cout << "Description: " << s.description << "\n";
+      if (!s.options.empty()) {
+        std::cout << "Possible values: { ";
+        for (size_t i = 0; i < s.options.size(); ++i) std::cout << s.options[i] << (i + 1 < s.options.size() ? ", " : " }");
+        std::cout << "\n";
+      }
+      std::cout << "\n";
+    }
+    std::cout << "Name:     [HELP]\nCL keys:  [-h, --help]\nDescription: Print this help message\n";
+  }
+  void report() const {
+    std::cout << "Settings:\n\n";
+    for (auto& n : order_) {
+      const Setting& s = map_.at(n);
+      std::cout << "Name:     [" << s.name << "]\nCL keys:  [" << s.shortkey << ", " << s.longkey << "]\nValue:    "
+                << s.val << "\n\n";
+    }
+  }
+
+ private:
+  std::map<std::string, Setting> map_;
+  std::vector<std::string> order_;
+};
+
+void add_common(Settings& S, bool bp) {
+  // platform (libs/core/platformSettings.cpp:31-50)
+  S.add("-m", "--mode", "THREAD MODEL", "CUDA", "OCCA's Parallel execution platform",
+        {"Serial", "OpenMP", "CUDA", "HIP", "OpenCL"});
+  S.add("-pl", "--platform", "PLATFORM NUMBER", "0", "Parallel platform number (used in OpenCL mode)");
+  S.add("-d", "--device", "DEVICE NUMBER", "0", "Parallel device number");
+  // mesh (libs/mesh/meshSettings.cpp:31-62)
+  S.add("-e", "--elements", "ELEMENT TYPE", "Hex", "Type of mesh elements", {"Tri", "Quad", "Tet", "Hex"});
+  S.add("-nx", "--dimx", "BOX NX", "10", "Number of elements in X-dimension per rank");
+  S.add("-ny", "--dimy", "BOX NY", "10", "Number of elements in Y-dimension per rank");
+  S.add("-nz", "--dimz", "BOX NZ", "10", "Number of elements in Z-dimension per rank");
+  S.add("-p", "--degree", "POLYNOMIAL DEGREE", "4", "Degree of polynomial finite element space",
+        {"1", "2", "3", "4", "5", "6", "7", "8", "9", "10", "11", "12", "13", "14", "15"});
+  S.add("-a", "--affine", "AFFINE MESH", "FALSE", "Assume elements are affine images of reference element",
+        {"TRUE", "FALSE"});
+  if (bp) S.add("-o", "--output", "OUTPUT FILE NAME", "", "");
+  S.add("-v", "--verbose", "VERBOSE", "FALSE", "Enable verbose output", {"TRUE", "FALSE"});
+  // extensions
+  S.add("-pc", "--precon", "PRECONDITIONER", "NONE", "CG preconditioner (extension)", {"NONE", "JACOBI"});
+  S.add("-f", "--forcing", "FORCING", "ANALYTIC",
+        "Right-hand side: analytic sin forcing, or f=2u-1 per gathered node from the seeded LCG (extension)",
+        {"ANALYTIC", "RANDOM"});
+  S.add("-s", "--seed", "FORCING SEED", "0", "LCG seed of the RANDOM forcing (extension)");
+  S.add("-pt", "--perturb", "VERTEX PERTURBATION", "0", "Interior vertex perturbation, fraction of h (extension)");
+  S.add("-ps", "--perturb-seed", "PERTURBATION SEED", "1", "LCG seed of the vertex perturbation (extension)");
+  if (bp) {
+    S.add("-it", "--iterations", "CG ITERATIONS", "100", "Maximum CG iterations of the timed solve (extension)");
+    S.add("-wi", "--warmup-iterations", "WARMUP ITERATIONS", "1000", "CG iterations of the warmup solve (extension)");
+    S.add("-tol", "--tolerance", "CG TOLERANCE", "0", "CG stop tolerance of the timed solve (extension)");
+  }
+}
+
+void check(int rc) {
+  if (rc != BP_SUCCESS) throw std::runtime_error(bp_last_error());
+}
+
+double now_after_finish() {
+  check(bp_finish(nullptr));
+  return std::chrono::duration<double>(std::chrono::high_resolution_clock::now().time_since_epoch()).count();
+}
+
+struct Problem {
+  bp_mesh_t mesh = nullptr;
+  bp_solver_t solver = nullptr;
+  bp_mesh_view_t view{};
+  ~Problem() {
+    if (solver) bp_solver_destroy(solver);
+    if (mesh) bp_mesh_destroy(mesh);
+  }
+};
+
+void setup(const Settings& S, Problem& P, int Nfields, int bp) {
+  if (!S.compare("THREAD MODEL", "CUDA"))
+    throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
+                             " is not available: this build runs the CUDA (sm_100a) path only");
+  if (!S.compare("ELEMENT TYPE", "Hex"))
+    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex only");
+  check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
+  bp_box_desc_t d{};
+  d.nx = std::atoi(S.get("BOX NX").c_str());
+  d.ny = std::atoi(S.get("BOX NY").c_str());
+  d.nz = std::atoi(S.get("BOX NZ").c_str());
+  d.N = std::atoi(S.get("POLYNOMIAL DEGREE").c_str());
+  d.affine = S.compare("AFFINE MESH", "TRUE") ? 1 : 0;
+  d.Nfields = Nfields;
+  d.pert = std::atof(S.get("VERTEX PERTURBATION").c_str());
+  d.pert_seed = std::strtoull(S.get("PERTURBATION SEED").c_str(), nullptr, 10);
+  check(bp_mesh_create(&d, &P.mesh));
+  check(bp_mesh_view(P.mesh, &P.view));
+  bp_solver_desc_t sd{};
+  sd.bp = bp;
+  sd.lambda = 1.0;   // BP/BP5/bp5Main.cpp:47
+  sd.precon = S.compare("PRECONDITIONER", "JACOBI") ? BP_PRECON_JACOBI : BP_PRECON_NONE;
+  check(bp_solver_create(P.mesh, &sd, &P.solver));
+}
+
+struct DevVec {
+  double* p = nullptr;
+  explicit DevVec(size_t n) { check(bp_malloc(reinterpret_cast<void**>(&p), n * sizeof(double))); }
+  ~DevVec() { bp_free(p); }
+};
+
+// reference byte model for one Ax application (bp5Run.cpp:106-142, bk5Run.cpp:97-125)
+double ax_bytes(const bp_mesh_view_t& v, long long Ndofs) {
+  const double E = v.Nelements, Np = v.Np, Nf = v.Nfields;
+  if (v.affine) return Ndofs * 8.0 + (7 * 8.0 + 4.0 + Np * Nf * 4.0 + Np * Nf * 8.0) * E;
+  return Ndofs * 8.0 + (Np * 7 * 8.0 + 4.0 + Np * Nf * 4.0 + Np * Nf * 8.0) * E;
+}
+double ax_flops(const bp_mesh_view_t& v) {
+  const double Nq = v.Nq, E = v.Nelements, Nf = v.Nfields;
+  if (v.affine) return (12 * Nq * Nq * Nq * Nq + 21 * Nq * Nq * Nq) * Nf * E;
+  return (12 * Nq * Nq * Nq * Nq + 18 * Nq * Nq * Nq) * Nf * E;
+}
+
+int run_bp(const char* name, int bp, Settings& S) {
+  const int Nfields = (bp == 6 || bp == 4 || bp == 2) ? 3 : 1;
+  Problem P;
+  setup(S, P, Nfields, bp);
+  if (S.compare("VERBOSE", "TRUE")) S.report();
+  const int32_t N = P.view.Ngather;
+  DevVec x(N), r(N), b(N);
+  const bool random = S.compare("FORCING", "RANDOM");
+  const uint64_t seed = std::strtoull(S.get("FORCING SEED").c_str(), nullptr, 10);
+  check(bp_solver_rhs(P.solver, random ? BP_RHS_RANDOM : BP_RHS_ANALYTIC, seed, b.p, nullptr));
+  const int maxIter = std::atoi(S.get("CG ITERATIONS").c_str());
+  const int warmIter = std::atoi(S.get("WARMUP ITERATIONS").c_str());
+  const double tol = std::atof(S.get("CG TOLERANCE").c_str());
+  const int verbose = S.compare("VERBOSE", "TRUE") ? 1 : 0;
+  bp_solve_stats_t st{};
+  // warmup solve (bp5Run.cpp:66-69)
+  check(bp_linalg_set(N, 0.0, x.p, nullptr));
+  check(bp_memcpy_dtod(r.p, b.p, sizeof(double) * N, nullptr));
+  check(bp_solver_solve(P.solver, x.p, r.p, 0.0, warmIter, nullptr, nullptr, &st));
+  // timed solve (bp5Run.cpp:71-95)
+  check(bp_linalg_set(N, 0.0, x.p, nullptr));
+  check(bp_memcpy_dtod(r.p, b.p, sizeof(double) * N, nullptr));
+  std::vector<double> hr(maxIter > 0 ? maxIter : 1), ha(maxIter > 0 ? maxIter : 1);
+  const double t0 = now_after_finish();
+  check(bp_solver_solve(P.solver, x.p, r.p, tol, maxIter, hr.data(), ha.data(), &st));
+  const double t1 = now_after_finish();
+  const double elapsed = t1 - t0;
+  const int Niter = st.iterations;
+  if (verbose) {
+    std::printf("CG: initial res norm %12.12f \n", std::sqrt(st.rdotr0));
+    for (int k = 0; k < Niter; ++k) std::printf("CG: it %d, r norm %12.12le, alpha = %le \n", k + 1, hr[k], ha[k]);
+  }
+  const long long Ndofs = N;
+  const double NGlobal = (double)P.view.Nlocal;
+  const double NbytesAx = ax_bytes(P.view, Ndofs);
+  const double NbytesGather = (Ndofs + 1) * 4.0 + NGlobal * 4.0 + NGlobal * 8.0 + Ndofs * 8.0;
+  const double Nbytes = (4 * Ndofs * 8.0 + NbytesAx + NbytesGather) + (11 * Ndofs * 8.0 + NbytesAx + NbytesGather) * Niter;
+  const double NflopsAx = ax_flops(P.view);
+  const double Nflops = (5.0 * Ndofs + NflopsAx + NGlobal) + (11.0 * Ndofs + NflopsAx + NGlobal) * Niter;
+  std::string suffix = "Element=Hex";
+  if (P.view.affine) suffix += ", Affine";
+  std::printf(
+      "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, iterations=%d, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
+      "DOFs*iterations/ranks*time=%1.2e, %s \n",
+      name, P.view.N, Ndofs, elapsed, Niter, elapsed / Ndofs, Nbytes / (1.0e9 * elapsed), Nflops / (1.0e9 * elapsed),
+      Ndofs * ((double)Niter / (1 * elapsed)), suffix.c_str());
+  const double rel = std::sqrt(st.rdotr / (st.rdotr0 > 0 ? st.rdotr0 : 1.0));
+  std::printf("%s extra: precon=%s, forcing=%s, final r norm=%.6e, relative residual=%.6e, device ms=%.4f\n", name,
+              S.get("PRECONDITIONER").c_str(), S.get("FORCING").c_str(), std::sqrt(st.rdotr), rel, st.elapsed_ms);
+  std::fflush(stdout);
+  return BP_SUCCESS;
+}
+
+int run_bk(const char* name, int bk, Settings& S) {
+  const int Nfields = (bk == 6 || bk == 4 || bk == 2) ? 3 : 1;
+  Problem P;
+  setup(S, P, Nfields, bk);
+  if (S.compare("VERBOSE", "TRUE")) S.report();
+  const int32_t Ngather = P.view.Ngather;
+  DevVec q(Ngather), Aq((size_t)P.view.Nlocal);
+  const bool random = S.compare("FORCING", "RANDOM");
+  const uint64_t seed = std::strtoull(S.get("FORCING SEED").c_str(), nullptr, 10);
+  if (random) {
+    // BK input q = 2u-1 per gathered node (the forcing's f)
+    DevVec b(Ngather);
+    check(bp_solver_rhs(P.solver, BP_RHS_RANDOM, seed, b.p, q.p));
+  } else {
+    // gathered analytic forcing (bk5Run.cpp:38-50)
+    check(bp_solver_rhs(P.solver, BP_RHS_ANALYTIC, 0, q.p, nullptr));
+  }
+  bp_ax_desc_t d{};
+  d.bp = (Nfields == 3) ? 6 : 5;
+  d.N = P.view.N;
+  d.affine = P.view.affine;
+  d.Nfields = Nfields;
+  auto apply = [&]() {
+    check(bp_ax_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
+                      P.view.gllw, P.view.D, 1.0, q.p, Aq.p, nullptr));
+  };
+  for (int n = 0; n < 5; ++n) apply();
+  const int Ntests = 50;
+  const double t0 = now_after_finish();
+  for (int n = 0; n < Ntests; ++n) apply();
+  const double t1 = now_after_finish();
+  const double elapsed = (t1 - t0) / Ntests;
+  const long long Ndofs = Ngather;
+  const double Nbytes = ax_bytes(P.view, Ndofs);
+  const double Nflops = ax_flops(P.view);
+  std::string suffix = "Element=Hex";
+  if (P.view.affine) suffix += ", Affine";
+  std::printf(
+      "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
+      "DOFs/ranks*time=%1.2e, %s \n",
+      name, P.view.N, Ndofs, elapsed, elapsed / Ndofs, Nbytes / (1.0e9 * elapsed), Nflops / (1.0e9 * elapsed),
+      Ndofs / (1 * elapsed), suffix.c_str());
+  std::fflush(stdout);
+  return BP_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int bp_driver_main(const char* name, int argc, char** argv) {
+  try {
+    std::string n = name ? name : "";
+    const bool bp = n.size() == 3 && n[0] == 'B' && n[1] == 'P';
+    const bool bk = n.size() == 3 && n[0] == 'B' && n[1] == 'K';
+    const int which = (bp || bk) ? n[2] - '0' : 0;
+    if (!(bp || bk) || (which != 5 && which != 6))
+      throw std::runtime_error("bp_driver_main: available drivers are BP5, BP6, BK5, BK6");
+    Settings S;
+    add_common(S, bp);
+    if (!S.parse(argc, argv)) return BP_SUCCESS;
+    return bp ? run_bp(n.c_str(), which, S) : run_bk(n.c_str(), which, S);
+  } catch (const std::exception& e) {
+    std::string banner = "---[ Error ]";
+    std::fprintf(stderr, "\n%s%s\n    Message  : %s\n%s\n", banner.c_str(), std::string(80 - banner.size(), '-').c_str(),
+                 e.what(), std::string(80, '=').c_str());
+    return BP_ERROR;
+  }
+}

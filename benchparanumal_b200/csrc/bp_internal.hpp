@@ -1,0 +1,138 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/bp_b200.h"
+
+namespace bp {
+
+// ---- error state (libp::exception / LIBP_ABORT replacement) ----
+void set_error(const std::string& msg);
+void clear_error();
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t err, const char* what, const char* file, int line);
+
+#define BP_CUDA_TRY(call)                                                   \
+  do {                                                                      \
+    cudaError_t bp_err_ = (call);                                           \
+    if (bp_err_ != cudaSuccess) return bp::cuda_fail(bp_err_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define BP_TRY(call)                    \
+  do {                                  \
+    int bp_rc_ = (call);                \
+    if (bp_rc_ != BP_SUCCESS) return bp_rc_; \
+  } while (0)
+
+// the library's default stream (created on first use)
+cudaStream_t default_stream();
+inline cudaStream_t to_stream(bp_stream_t s) {
+  return s ? reinterpret_cast<cudaStream_t>(s) : default_stream();
+}
+int sm_count();
+
+// ---- device buffer owned by the library ----
+template <class T>
+struct DeviceArray {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  ~DeviceArray() { release(); }
+  int alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return BP_SUCCESS;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr), count * sizeof(T));
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      n = 0;
+      return fail(BP_ERROR_ALLOC, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+                                      " bytes failed: " + cudaGetErrorString(e));
+    }
+    return BP_SUCCESS;
+  }
+  int upload(const std::vector<T>& h, cudaStream_t s) {
+    BP_TRY(alloc(h.size()));
+    if (!h.empty()) BP_CUDA_TRY(cudaMemcpyAsync(ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return BP_SUCCESS;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+};
+
+// ---- host-side mesh description produced by the setup code ----
+struct HostMesh {
+  int N = 0, Nq = 0, Np = 0, nx = 0, ny = 0, nz = 0, E = 0, affine = 0, Nfields = 1;
+  std::vector<double> gllz, gllw, D;
+  std::vector<double> EX, EY, EZ;        // E*8 (perturbed vertices)
+  int32_t Ngather = 0, nnz = 0;
+  std::vector<int32_t> G2L;              // E*Np*Nf
+  std::vector<int32_t> rowStarts;        // Ngather+1
+  std::vector<int32_t> colIds;           // nnz
+};
+
+// basis (GLL nodes by Newton iteration, lumped weights, differentiation matrix)
+void gll_nodes_weights(int N, std::vector<double>& z, std::vector<double>& w);
+void diff_matrix(const std::vector<double>& z, std::vector<double>& D);
+// box vertices with optional seeded interior perturbation
+void box_vertices(HostMesh& m, double pert, uint64_t seed);
+// masked gathered numbering, CSR and GlobalToLocal for the box
+void box_numbering(HostMesh& m);
+
+}  // namespace bp
+
+// ---- the opaque objects of the C ABI ----
+struct bp_mesh_s {
+  int N, Nq, Np, E, Nfields, affine;
+  int32_t Ngather, nnz;
+  bp::DeviceArray<int32_t> elementList, G2L, rowStarts, colIds;
+  bp::DeviceArray<double> wJ, ggeo, D, gllz, gllw, EX, EY, EZ;
+};
+
+struct bp_solver_s;
+
+// ---- kernel launchers (bp_kernels.cu) ----
+namespace bp {
+int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
+                   const double* q, double* Aq, const int* skip, cudaStream_t s);
+int launch_ax(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+              const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
+              const double* q, double* Aq, cudaStream_t s);
+int launch_gather(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* v, double* gv,
+                  cudaStream_t s);
+int launch_scatter(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* gv, double* v,
+                   cudaStream_t s);
+int launch_geometry(int N, int affine, int E, const double* EX, const double* EY, const double* EZ,
+                    const double* gllz, const double* gllw, double* wJ, double* ggeo, int* bad, cudaStream_t s);
+int launch_rhs_analytic(int N, int affine, int Nfields, int E, const double* EX, const double* EY,
+                        const double* EZ, const double* gllz, const double* gllw, const double* wJ, double lambda,
+                        double* rL, cudaStream_t s);
+int launch_rhs_random(int32_t Ngather, uint64_t seed, double* f, cudaStream_t s);
+int launch_mass_local(int N, int affine, int Nfields, int E, const int32_t* G2L, const double* gllw,
+                      const double* wJ, const double* f, double* rL, cudaStream_t s);
+int launch_diag_local(int N, int affine, int Nfields, int E, const double* ggeo, const double* wJ,
+                      const double* gllw, const double* D, double lambda, double* dL, cudaStream_t s);
+int launch_set(int32_t N, double alpha, double* x, cudaStream_t s);
+int launch_axpy(int32_t N, double alpha, const double* x, double beta, double* y, cudaStream_t s);
+int launch_reciprocal(int32_t N, double* x, cudaStream_t s);
+int launch_sqrt1(double* v, cudaStream_t s);   // v[0] = sqrt(v[0]) on the device
+
+// deterministic fused reductions: result[0] = sum over i of term(i)
+int launch_dot(int32_t N, const double* x, const double* y, double* result, double* partials,
+               unsigned int* counter, cudaStream_t s);
+int launch_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* result, double* partials,
+                     unsigned int* counter, cudaStream_t s);
+
+int reduction_blocks();
+}  // namespace bp

@@ -1,0 +1,277 @@
+// Host-side setup of the Hex3D box: 1D basis, vertices, and the masked
+// gathered numbering (GlobalToLocal + CSR) computed in closed form from the
+// box structure.
+//
+// The numbering reproduces, integer for integer, what the reference computes
+// with generic connectivity (libs/mesh/meshConnectNodes.cpp:32-82,
+// libs/mesh/meshMaskedGatherScatterSetup.cpp:31-77, libs/ogs/ogsSetup.cpp:
+// 492-579 and 833-849):
+//   * a node's class is the set of local nodes at the same lattice point; its
+//     representative is the local node of the lowest-numbered element of the
+//     class (the reference's globalId = 1 + smallest local index);
+//   * nodes on the box boundary are masked (GlobalToLocal = -1);
+//   * gathered rows are the unmasked classes in order of first appearance
+//     over the local index e*Np*Nf + f*Np + n;
+//   * each CSR row lists its local nodes in ascending local index.
+// Here those orders follow from the lattice coordinates, so every element is
+// handled independently (OpenMP over elements) with no sort.
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+
+#include "bp_internal.hpp"
+
+namespace bp {
+
+// GLL nodes: Newton iteration on (1-x^2) P_N'(x) with the Legendre
+// recurrence, started from the Chebyshev-Gauss-Lobatto points; weights
+// 2 / (N (N+1) P_N(x)^2).
+void gll_nodes_weights(int N, std::vector<double>& z, std::vector<double>& w) {
+  const int n1 = N + 1;
+  z.assign(n1, 0.0);
+  w.assign(n1, 0.0);
+  const double pi = 3.14159265358979323846;
+  std::vector<double> x(n1), xold(n1, 2.0), PN(n1), PN1(n1);
+  for (int i = 0; i < n1; ++i) x[i] = -std::cos(pi * i / N);
+  for (int it = 0; it < 100; ++it) {
+    double delta = 0.0;
+    for (int i = 0; i < n1; ++i) delta = std::max(delta, std::fabs(x[i] - xold[i]));
+    if (delta <= 1e-16) break;
+    for (int i = 0; i < n1; ++i) {
+      xold[i] = x[i];
+      double p0 = 1.0, p1 = x[i];
+      for (int k = 2; k <= N; ++k) {
+        const double p2 = ((2 * k - 1) * x[i] * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      PN[i] = p1;     // P_N
+      PN1[i] = p0;    // P_{N-1}
+      if (N == 1) { PN[i] = x[i]; PN1[i] = 1.0; }
+      x[i] = xold[i] - (x[i] * PN[i] - PN1[i]) / (n1 * PN[i]);
+    }
+  }
+  x[0] = -1.0;
+  x[N] = 1.0;
+  for (int i = 0; i < n1; ++i) {
+    double p0 = 1.0, p1 = x[i];
+    for (int k = 2; k <= N; ++k) {
+      const double p2 = ((2 * k - 1) * x[i] * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    z[i] = x[i];
+    w[i] = 2.0 / (N * (N + 1.0) * p1 * p1);
+  }
+  // symmetrise
+  for (int i = 0; i < n1 / 2; ++i) {
+    const double a = 0.5 * (z[N - i] - z[i]);
+    z[i] = -a;
+    z[N - i] = a;
+    const double b = 0.5 * (w[i] + w[N - i]);
+    w[i] = w[N - i] = b;
+  }
+  if (n1 % 2) z[N / 2] = 0.0;
+}
+
+// Lagrange differentiation matrix by barycentric weights:
+// D[i*Nq+m] = l_m'(z_i) = (b_m / b_i) / (z_i - z_m), diagonal = -(row sum).
+void diff_matrix(const std::vector<double>& z, std::vector<double>& D) {
+  const int n = (int)z.size();
+  std::vector<double> b(n, 1.0);
+  for (int j = 0; j < n; ++j)
+    for (int k = 0; k < n; ++k)
+      if (k != j) b[j] *= (z[j] - z[k]);
+  for (int j = 0; j < n; ++j) b[j] = 1.0 / b[j];
+  D.assign(n * n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int m = 0; m < n; ++m) {
+      if (m == i) continue;
+      const double v = (b[m] / b[i]) / (z[i] - z[m]);
+      D[i * n + m] = v;
+      s += v;
+    }
+    D[i * n + i] = -s;
+  }
+}
+
+// Box vertices as in libs/mesh/meshSetupBoxHex3D.cpp:31-131 (one rank), with
+// interior vertices moved by pert*h*(2u-1) per coordinate; u is the reference
+// LCG stream (libs/primitives/random.cpp) seeded with `seed`, three values per
+// global vertex id, x/y/z interleaved.
+void box_vertices(HostMesh& m, double pert, uint64_t seed) {
+  const int nx = m.nx, ny = m.ny, nz = m.nz;
+  const int64_t NnX = nx + 1, NnY = ny + 1, NnZ = nz + 1;
+  const double dx = 2.0 / nx, dy = 2.0 / ny, dz = 2.0 / nz;
+  m.EX.resize((size_t)m.E * 8);
+  m.EY.resize((size_t)m.E * 8);
+  m.EZ.resize((size_t)m.E * 8);
+  std::vector<double> u;
+  if (pert != 0.0) {
+    u.resize((size_t)3 * NnX * NnY * NnZ);
+    uint64_t x = 6364136223846793005ULL * (~seed) + 1ULL;
+    const double scale = 1.0 / (double)std::numeric_limits<uint64_t>::max();
+    for (size_t r = 0; r < u.size(); ++r) {
+      u[r] = (double)x * scale;
+      x = 6364136223846793005ULL * x + 1ULL;
+    }
+  }
+  static const int ci[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+  static const int cj[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+  static const int ck[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+#pragma omp parallel for
+  for (int e = 0; e < m.E; ++e) {
+    const int i = e % nx, j = (e / nx) % ny, k = e / (nx * ny);
+    const double x0 = -1.0 + dx * i, y0 = -1.0 + dy * j, z0 = -1.0 + dz * k;
+    for (int c = 0; c < 8; ++c) {
+      double X = ci[c] ? x0 + dx : x0;
+      double Y = cj[c] ? y0 + dy : y0;
+      double Z = ck[c] ? z0 + dz : z0;
+      const int64_t I = i + ci[c], J = j + cj[c], K = k + ck[c];
+      if (pert != 0.0 && I > 0 && I < nx && J > 0 && J < ny && K > 0 && K < nz) {
+        const int64_t g = I + J * NnX + K * NnX * NnY;
+        X += pert * dx * (2 * u[3 * g + 0] - 1);
+        Y += pert * dy * (2 * u[3 * g + 1] - 1);
+        Z += pert * dz * (2 * u[3 * g + 2] - 1);
+      }
+      m.EX[(size_t)e * 8 + c] = X;
+      m.EY[(size_t)e * 8 + c] = Y;
+      m.EZ[(size_t)e * 8 + c] = Z;
+    }
+  }
+}
+
+namespace {
+// Per-direction lattice helpers for lattice index L in [0, n*N]:
+//  first(L) : element index of the first (lowest) element containing L
+//  count(L) : number of elements containing L (1 or 2)
+struct Axis {
+  int n, N;
+  int first(int L) const { return (L > 0 && L % N == 0) ? L / N - 1 : std::min(L / N, n - 1); }
+  int count(int L) const { return (L > 0 && L < n * N && L % N == 0) ? 2 : 1; }
+  bool boundary(int L) const { return L == 0 || L == n * N; }
+  // representatives of element index a: local indices 1..N-1, plus N if a < n-1
+  int reps(int a) const { return N - 1 + (a < n - 1 ? 1 : 0); }
+};
+}  // namespace
+
+void box_numbering(HostMesh& m) {
+  const int N = m.N, Nq = m.Nq, Np = m.Np, Nf = m.Nfields;
+  const Axis ax{m.nx, N}, ay{m.ny, N}, az{m.nz, N};
+  const int E = m.E;
+  // rows contributed by each element, in element order
+  std::vector<int64_t> rowBase((size_t)E + 1, 0);
+  for (int e = 0; e < E; ++e) {
+    const int ex = e % m.nx, ey = (e / m.nx) % m.ny, ez = e / (m.nx * m.ny);
+    rowBase[e + 1] = rowBase[e] + (int64_t)Nf * ax.reps(ex) * ay.reps(ey) * az.reps(ez);
+  }
+  m.Ngather = (int32_t)rowBase[E];
+  auto row_of = [&](int ex, int ey, int ez, int i, int j, int k, int f) -> int32_t {
+    // (ex,ey,ez) is the representative element, (i,j,k) >= 1 its local indices
+    const int e = ex + m.nx * (ey + m.ny * ez);
+    const int ci = ax.reps(ex), cj = ay.reps(ey), ck = az.reps(ez);
+    return (int32_t)(rowBase[e] + (int64_t)f * ci * cj * ck + ((int64_t)(k - 1) * cj + (j - 1)) * ci + (i - 1));
+  };
+  // multiplicities -> rowStarts
+  m.rowStarts.assign((size_t)m.Ngather + 1, 0);
+#pragma omp parallel for
+  for (int e = 0; e < E; ++e) {
+    const int ex = e % m.nx, ey = (e / m.nx) % m.ny, ez = e / (m.nx * m.ny);
+    for (int k = 1; k <= az.reps(ez); ++k)
+      for (int j = 1; j <= ay.reps(ey); ++j)
+        for (int i = 1; i <= ax.reps(ex); ++i) {
+          const int mult = ax.count(ex * N + i) * ay.count(ey * N + j) * az.count(ez * N + k);
+          for (int f = 0; f < Nf; ++f) m.rowStarts[(size_t)row_of(ex, ey, ez, i, j, k, f) + 1] = mult;
+        }
+  }
+  for (int32_t r = 0; r < m.Ngather; ++r) m.rowStarts[r + 1] += m.rowStarts[r];
+  m.nnz = m.rowStarts[m.Ngather];
+  m.colIds.assign((size_t)m.nnz, 0);
+  m.G2L.assign((size_t)E * Np * Nf, -1);
+#pragma omp parallel for
+  for (int e = 0; e < E; ++e) {
+    const int ex = e % m.nx, ey = (e / m.nx) % m.ny, ez = e / (m.nx * m.ny);
+    for (int k = 0; k < Nq; ++k) {
+      const int LK = ez * N + k;
+      if (az.boundary(LK)) continue;
+      const int rz = az.first(LK);
+      for (int j = 0; j < Nq; ++j) {
+        const int LJ = ey * N + j;
+        if (ay.boundary(LJ)) continue;
+        const int ry = ay.first(LJ);
+        for (int i = 0; i < Nq; ++i) {
+          const int LI = ex * N + i;
+          if (ax.boundary(LI)) continue;
+          const int rx = ax.first(LI);
+          const int n = i + Nq * (j + Nq * k);
+          // position among the class members (ascending element index)
+          const int cx = ax.count(LI), cy = ay.count(LJ);
+          const int pos = ((ez - rz) * cy + (ey - ry)) * cx + (ex - rx);
+          for (int f = 0; f < Nf; ++f) {
+            const int32_t row = row_of(rx, ry, rz, LI - rx * N, LJ - ry * N, LK - rz * N, f);
+            const int64_t l = ((int64_t)e * Nf + f) * Np + n;
+            m.G2L[(size_t)l] = row;
+            m.colIds[(size_t)m.rowStarts[row] + pos] = (int32_t)l;
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace bp
+
+// ---------------------------------------------------------------------------
+// host-only C entry points
+// ---------------------------------------------------------------------------
+namespace {
+int host_mesh_from_desc(const bp_box_desc_t* d, bp::HostMesh& m) {
+  if (!d) return bp::fail(BP_ERROR_ARG, "null descriptor");
+  if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->N < 1 || d->N > 15 || (d->Nfields != 1 && d->Nfields != 3))
+    return bp::fail(BP_ERROR_ARG, "bad box descriptor");
+  m.N = d->N; m.Nq = d->N + 1; m.Np = m.Nq * m.Nq * m.Nq;
+  m.nx = d->nx; m.ny = d->ny; m.nz = d->nz;
+  const int64_t E = (int64_t)d->nx * d->ny * d->nz;
+  if (E * m.Np * d->Nfields >= (int64_t)INT32_MAX) return bp::fail(BP_ERROR_ARG, "local node count exceeds int32");
+  m.E = (int)E; m.affine = d->affine ? 1 : 0; m.Nfields = d->Nfields;
+  return BP_SUCCESS;
+}
+}  // namespace
+
+extern "C" int bp_box_numbering(const bp_box_desc_t* d, int32_t* Ngather, int32_t* nnz, int32_t* G2L,
+                                int32_t* rowStarts, int32_t* colIds) {
+  bp::HostMesh m;
+  int rc = host_mesh_from_desc(d, m);
+  if (rc) return rc;
+  bp::box_numbering(m);
+  if (Ngather) *Ngather = m.Ngather;
+  if (nnz) *nnz = m.nnz;
+  if (G2L) std::copy(m.G2L.begin(), m.G2L.end(), G2L);
+  if (rowStarts) std::copy(m.rowStarts.begin(), m.rowStarts.end(), rowStarts);
+  if (colIds) std::copy(m.colIds.begin(), m.colIds.end(), colIds);
+  return BP_SUCCESS;
+}
+
+extern "C" int bp_basis_gll(int32_t N, double* z, double* w, double* D) {
+  if (N < 1 || N > 15) return bp::fail(BP_ERROR_ARG, "degree must be in 1..15");
+  std::vector<double> zz, ww, DD;
+  bp::gll_nodes_weights(N, zz, ww);
+  bp::diff_matrix(zz, DD);
+  if (z) std::copy(zz.begin(), zz.end(), z);
+  if (w) std::copy(ww.begin(), ww.end(), w);
+  if (D) std::copy(DD.begin(), DD.end(), D);
+  return BP_SUCCESS;
+}
+
+extern "C" int bp_box_vertices(const bp_box_desc_t* d, double* EX, double* EY, double* EZ) {
+  bp::HostMesh m;
+  int rc = host_mesh_from_desc(d, m);
+  if (rc) return rc;
+  bp::box_vertices(m, d->pert, d->pert_seed);
+  if (EX) std::copy(m.EX.begin(), m.EX.end(), EX);
+  if (EY) std::copy(m.EY.begin(), m.EY.end(), EY);
+  if (EZ) std::copy(m.EZ.begin(), m.EZ.end(), EZ);
+  return BP_SUCCESS;
+}

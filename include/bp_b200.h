@@ -1,0 +1,251 @@
+/*
+ * bp_b200.h -- C ABI of the B200-native BK/BP Hex3D hot path.
+ *
+ * The library replaces the OCCA platform layer and the OKL kernels of
+ * benchParanumal for the Hex3D BK/BP path (one rank, one GPU, CUDA only).
+ * Every entry point returns BP_SUCCESS (0) or a negative error code; the text
+ * of the last error is available from bp_last_error().  Pointers named
+ * "device" must come from bp_malloc (or any CUDA device allocation); all other
+ * arrays are host memory.  The library is not thread-safe: drive it from one
+ * host thread, like the reference drives OCCA.
+ *
+ * Reference interfaces replaced are cited as path:line relative to the
+ * reference project root.
+ */
+#ifndef BP_B200_H
+#define BP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: LIBP_SUCCESS / LIBP_ERROR (include/utils.hpp:47-48) plus detail. */
+#define BP_SUCCESS 0
+#define BP_ERROR -1            /* generic failure (LIBP_ABORT)                      */
+#define BP_ERROR_ARG -2        /* invalid argument or unsupported configuration    */
+#define BP_ERROR_CUDA -3       /* a CUDA runtime call failed                        */
+#define BP_ERROR_ALLOC -4      /* device or pinned-host allocation failed           */
+#define BP_ERROR_NUMERIC -5    /* non-positive Jacobian, CG breakdown, NaN          */
+#define BP_ERROR_TIMEOUT -6    /* a bounded device-side wait gave up                */
+
+typedef void* bp_stream_t;     /* cudaStream_t; NULL = the library's default stream */
+typedef void* bp_event_t;      /* cudaEvent_t                                       */
+
+/* Text of the most recent error (empty string when none).
+   Replaces the message carried by libp::exception (libs/core/exception.cpp:78-90). */
+const char* bp_last_error(void);
+
+/* Library version string. */
+const char* bp_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Platform: device, memory, streams, timing.
+ * Replaces platform_t (include/platform.hpp:61-185), platform_t::malloc /
+ * hostMalloc (platform.hpp:99-144), deviceMemory<T>::copyFrom/copyTo
+ * (include/memory.hpp:288-464), platform.finish() (platform.hpp:161-163).
+ * ------------------------------------------------------------------------- */
+
+/* "-m CUDA -d id" device selection (libs/core/platformDeviceConfig.cpp:63-101). */
+int bp_platform_init(int device_id);
+int bp_device_count(int* count);
+/* Name and SM count of the current device. */
+int bp_device_info(char* name, size_t name_len, int* sm_count);
+
+int bp_malloc(void** device_ptr, size_t bytes);
+int bp_free(void* device_ptr);
+int bp_host_malloc(void** host_ptr, size_t bytes);       /* pinned host memory */
+int bp_host_free(void* host_ptr);
+int bp_memcpy_htod(void* device_dst, const void* host_src, size_t bytes, bp_stream_t stream);
+int bp_memcpy_dtoh(void* host_dst, const void* device_src, size_t bytes, bp_stream_t stream);
+int bp_memcpy_dtod(void* device_dst, const void* device_src, size_t bytes, bp_stream_t stream);
+int bp_memset(void* device_ptr, int value, size_t bytes, bp_stream_t stream);
+
+int bp_stream_create(bp_stream_t* stream);
+int bp_stream_destroy(bp_stream_t stream);
+/* platform.finish(): wait for all work on the stream. */
+int bp_finish(bp_stream_t stream);
+int bp_event_create(bp_event_t* event);
+int bp_event_destroy(bp_event_t event);
+int bp_event_record(bp_event_t event, bp_stream_t stream);
+int bp_event_elapsed_ms(bp_event_t start, bp_event_t end, float* ms);
+
+/* ---------------------------------------------------------------------------
+ * Device kernels.  Each replaces one OKL kernel with the same argument
+ * meaning; compile-time OKL defines (p_N, p_Nfields, affine) become fields of
+ * bp_ax_desc_t.  Index arrays are int32 (dlong, include/types.h:59-63).
+ * ------------------------------------------------------------------------- */
+
+typedef struct bp_ax_desc {
+  int32_t bp;        /* benchmark problem: 5 (Nfields 1) or 6 (Nfields 3)         */
+  int32_t N;         /* polynomial degree 1..15 (p_N)                             */
+  int32_t affine;    /* 1: per-element factors (bp5AxAffineHex3D)                 */
+  int32_t Nfields;   /* 1 or 3 (p_Nfields)                                        */
+} bp_ax_desc_t;
+
+/* Element-local stiffness + lambda*mass operator, Aq[e] = A_e q[GlobalToLocal].
+   Replaces bp5AxHex3D (okl/bp5AxHex3D.okl:415-569, :50-185),
+   bp5AxAffineHex3D (okl/bp5AxAffineHex3D.okl:419-579) and the BP6 variants
+   (okl/bp6AxHex3D.okl:50-255).  Argument order follows the OKL signature
+   (okl/bp5AxHex3D.okl:415-427) minus the unused vgeo, S and MM.
+   ggeo: non-affine [E*Np*6] node-major G00,G01,G02,G11,G12,G22 with the GLL
+   weights folded in, wJ [E*Np]; affine ggeo [E*6], wJ [E] (weights applied in
+   the kernel from gllw).  D: [Nq*Nq] row-major, D[i*Nq+m] = l_m'(r_i).
+   q: gathered vector; Aq: E-vector [E*Np*Nfields], layout e*Np*Nf + f*Np + n. */
+int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                const int32_t* GlobalToLocal, const double* wJ, const double* ggeo,
+                const double* gllw, const double* D, double lambda, const double* q,
+                double* Aq, bp_stream_t stream);
+
+/* ogs Gather(Add, Trans): gv[r] = sum over c in row r of v[colIds[c]] in column
+   order.  Replaces ogsOperator_t::Gather (libs/ogs/ogsOperator.cpp:160-188) and
+   the OKL gather kernel (libs/ogs/okl/ogsKernels.okl:86-122), K=1, T=double. */
+int bp_ogs_gather(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds,
+                  const double* v, double* gv, bp_stream_t stream);
+
+/* ogs Scatter(NoTrans): v[colIds[c]] = gv[r] for every c in row r.
+   Replaces the OKL scatter kernel (libs/ogs/okl/ogsKernels.okl:127-164). */
+int bp_ogs_scatter(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds,
+                   const double* gv, double* v, bp_stream_t stream);
+
+/* linAlg_t vector kernels (libs/core/linAlg.cpp:38-89, libs/core/okl/linAlg*.okl).
+   Reductions write their result to a device scalar instead of a pinned host
+   buffer, so no host synchronisation is implied. */
+int bp_linalg_set(int32_t N, double alpha, double* x, bp_stream_t stream);
+int bp_linalg_axpy(int32_t N, double alpha, const double* x, double beta, double* y,
+                   bp_stream_t stream);
+int bp_linalg_inner_prod(int32_t N, const double* x, const double* y, double* result,
+                         bp_stream_t stream);
+int bp_linalg_norm2(int32_t N, const double* x, double* result, bp_stream_t stream);
+
+/* cg::UpdateCG first half (libs/core/linearSolverCG.cpp:131-156,
+   libs/core/okl/linearSolverUpdateCG.okl:29-103): r <- r - alpha Ap and
+   rdotr <- r.r, written to a device scalar. */
+int bp_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* rdotr,
+                 bp_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Mesh and masked gather-scatter setup.  Replaces mesh_t::Setup for the Hex3D
+ * box (libs/mesh/meshSetup.cpp:31-85, meshSetupBoxHex3D.cpp:31-131,
+ * meshGeometricFactorsHex3D.cpp:31-153), mesh_t::MaskedGatherScatterSetup
+ * (libs/mesh/meshMaskedGatherScatterSetup.cpp:31-77), ogs_t::Setup
+ * (libs/ogs/ogsSetup.cpp:87-290) and ogs_t::SetupGlobalToLocalMapping
+ * (libs/ogs/ogsSetup.cpp:833-849).  All arrays live on the device.
+ * ------------------------------------------------------------------------- */
+
+typedef struct bp_mesh_s* bp_mesh_t;
+
+typedef struct bp_box_desc {
+  int32_t nx, ny, nz;   /* -nx -ny -nz: elements per direction                    */
+  int32_t N;            /* -p: degree 1..15                                        */
+  int32_t affine;       /* -a                                                      */
+  int32_t Nfields;      /* 1 (BP1/3/5) or 3 (BP2/4/6)                              */
+  double pert;          /* interior vertex perturbation, fraction of h (0 = none)  */
+  uint64_t pert_seed;   /* LCG seed of the perturbation                            */
+} bp_box_desc_t;
+
+typedef struct bp_mesh_view {
+  int32_t N, Nq, Np, Nelements, Nfields, affine;
+  int32_t Ngather;           /* CG unknowns (masked, gathered rows)              */
+  int32_t nnz;               /* unmasked local nodes (= colIds length)            */
+  int64_t Nlocal;            /* E * Np * Nfields                                  */
+  /* device arrays */
+  const int32_t* elementList;     /* [E]                                          */
+  const int32_t* GlobalToLocal;   /* [Nlocal], -1 = masked                        */
+  const int32_t* rowStarts;       /* [Ngather+1]                                  */
+  const int32_t* colIds;          /* [nnz]                                        */
+  const double* wJ;               /* [E*Np] (affine: [E])                         */
+  const double* ggeo;             /* [E*Np*6] (affine: [E*6])                     */
+  const double* D;                /* [Nq*Nq]                                      */
+  const double* gllz;             /* [Nq]                                         */
+  const double* gllw;             /* [Nq]                                         */
+  const double* EX;               /* [E*8] vertex coordinates                     */
+  const double* EY;
+  const double* EZ;
+} bp_mesh_view_t;
+
+int bp_mesh_create(const bp_box_desc_t* desc, bp_mesh_t* mesh);
+
+/* Host-only pieces of the same setup (no device needed).
+   bp_box_numbering: the masked gathered numbering of the box
+   (ogsSetup.cpp:492-579 EnumerateGatherGroups + :833-849
+   SetupGlobalToLocalMapping).  Call with NULL arrays to get Ngather and nnz,
+   then with GlobalToLocal [E*Np*Nfields], rowStarts [Ngather+1], colIds [nnz].
+   bp_basis_gll: GLL nodes z, weights w [N+1] and D [(N+1)^2]
+   (meshBasis1D.cpp:218-264 JacobiGLL, :114-136 Dmatrix1D).
+   bp_box_vertices: vertex coordinates EX/EY/EZ [E*8] with the seeded
+   perturbation (meshSetupBoxHex3D.cpp:31-131). */
+int bp_box_numbering(const bp_box_desc_t* desc, int32_t* Ngather, int32_t* nnz, int32_t* GlobalToLocal,
+                     int32_t* rowStarts, int32_t* colIds);
+int bp_basis_gll(int32_t N, double* z, double* w, double* D);
+int bp_box_vertices(const bp_box_desc_t* desc, double* EX, double* EY, double* EZ);
+int bp_mesh_view(bp_mesh_t mesh, bp_mesh_view_t* view);
+int bp_mesh_destroy(bp_mesh_t mesh);
+
+/* ---------------------------------------------------------------------------
+ * Benchmark problem: operator, forcing and CG.  Replaces bp5_t::Setup /
+ * Operator / Run (BP/BP5/src/bp5Setup.cpp:29-95, bp5Operator.cpp:29-85,
+ * bp5Run.cpp:30-239) and cg::Solve (libs/core/linearSolverCG.cpp:62-129).
+ * ------------------------------------------------------------------------- */
+
+typedef struct bp_solver_s* bp_solver_t;
+
+#define BP_PRECON_NONE 0
+#define BP_PRECON_JACOBI 1
+
+typedef struct bp_solver_desc {
+  int32_t bp;          /* 5 (scalar) or 6 (vector, mesh Nfields must be 3)        */
+  double lambda;       /* 1.0 for BP3-BP6 (BP/BP5/bp5Main.cpp:47)                   */
+  int32_t precon;      /* BP_PRECON_NONE (reference) or BP_PRECON_JACOBI             */
+} bp_solver_desc_t;
+
+#define BP_RHS_ANALYTIC 0   /* rhsHex3D forcing (okl/rhsHex3D.okl:29-128)         */
+#define BP_RHS_RANDOM 1     /* f = 2u-1 per gathered row (seeded LCG), b = M f     */
+
+typedef struct bp_solve_stats {
+  int32_t iterations;      /* cg::Solve return value                              */
+  double rdotr0;           /* initial r.r                                          */
+  double rdotr;            /* final r.r                                            */
+  double elapsed_ms;       /* device time of the solve (CUDA events)               */
+} bp_solve_stats_t;
+
+int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* desc, bp_solver_t* solver);
+int bp_solver_destroy(bp_solver_t solver);
+/* Number of CG unknowns (ogs.Ngather). */
+int bp_solver_size(bp_solver_t solver, int32_t* Ngather);
+/* solver_t::Operator (include/solver.hpp:47-49): Aq = Gather(A_e q[G2L]). */
+int bp_solver_operator(bp_solver_t solver, const double* q, double* Aq, bp_stream_t stream);
+/* Forcing then Trans-gather into the device vector b [Ngather]
+   (bp5Run.cpp:53-64).  For BP_RHS_RANDOM, f_out (device, may be NULL) receives f. */
+int bp_solver_rhs(bp_solver_t solver, int32_t mode, uint64_t seed, double* b, double* f_out);
+/* Assembled operator diagonal (device [Ngather]), the Jacobi preconditioner's inverse. */
+int bp_solver_diagonal(bp_solver_t solver, double* diag);
+/* cg::Solve on device vectors: x (initial guess in, solution out) and r
+   (b in, final residual out).  tol and maxit as in the reference; with the
+   Jacobi preconditioner the stop rule is ||r|| <= tol ||b||.  hist_rnorm and
+   hist_alpha (host, length maxit, may be NULL) receive sqrt(r.r) and alpha of
+   every iteration (the "-v" output).  No host synchronisation happens inside
+   the iteration loop except one flag read every 20 iterations when tol > 0. */
+int bp_solver_solve(bp_solver_t solver, double* x, double* r, double tol, int32_t maxit,
+                    double* hist_rnorm, double* hist_alpha, bp_solve_stats_t* stats);
+/* The same solve from HOST buffers: copies b (host, pinned or pageable) to the
+   device, solves from x=0, copies x back to x_host.  The device time reported
+   in stats covers the copies and the solve. */
+int bp_solver_solve_host(bp_solver_t solver, const double* b_host, double* x_host, double tol,
+                         int32_t maxit, bp_solve_stats_t* stats);
+
+/* ---------------------------------------------------------------------------
+ * Drivers: the BK/BP executables' main() with the reference's command-line
+ * keys (libs/core/platformSettings.cpp:31-50, libs/mesh/meshSettings.cpp:31-62,
+ * BP/BP5/src/bp5Settings.cpp:30-46) and result line (bp5Run.cpp:208-217,
+ * BK/BK5/src/bk5Run.cpp:186-194).  name is "BP5" or "BK5".
+ * ------------------------------------------------------------------------- */
+int bp_driver_main(const char* name, int argc, char** argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BP_B200_H */

@@ -1,0 +1,182 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the CPU oracle.
+
+Tolerances (from the path's specification): integer indexing bit-exact; Ax
+and ogs within 1e-12 relative in FP64; CG residual history within 1e-10
+relative per iteration.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+AX_TOL = 1e-12
+HIST_TOL = 1e-10
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+AX_CASES = [(2, 2, 2, N, aff, pert, Nf) for N in range(1, 16) for (aff, pert) in [(False, 0.0), (True, 0.0)]
+            for Nf in (1,)] + [
+    (3, 2, 2, 7, False, 0.1, 1), (3, 2, 2, 4, False, 0.2, 1), (2, 3, 2, 3, False, 0.1, 3),
+    (2, 2, 2, 7, True, 0.0, 3), (2, 2, 1, 15, False, 0.1, 3), (1, 1, 1, 1, False, 0.0, 1), (4, 3, 2, 5, False, 0.1, 1)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,N,affine,pert,Nf", AX_CASES)
+def test_ax_and_gather_match_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, Nf):
+    om = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, Nfields=Nf, pert=pert)
+    assert (gm.Ngather, gm.nnz) == (om.Ngather, om.nnz)
+    # indexing bit-exact
+    np.testing.assert_array_equal(gm.array("GlobalToLocal"), om.array("G2L"))
+    np.testing.assert_array_equal(gm.array("rowStarts"), om.array("rowStarts"))
+    np.testing.assert_array_equal(gm.array("colIds"), om.array("colIds"))
+    # geometric factors computed on the device
+    assert _rel(gm.array("wJ"), om.array("wJ")) < 1e-13
+    assert _rel(gm.array("ggeo"), om.array("ggeo")) < 1e-13
+    if om.Ngather == 0:
+        return
+    q = 2 * oracle.random(11, om.Ngather) - 1
+    dq = gpu.DeviceBuffer.from_host(q)
+    dAq = gpu.DeviceBuffer(om.NL)
+    gpu.ax_hex3d(gm, dq, dAq)
+    AqL = dAq.download()
+    want = om.ax(q)
+    assert _rel(AqL, want) < AX_TOL
+    # masked local nodes contribute the operator applied to zero there
+    # gather: same input E-vector -> bit-identical sums (same order)
+    dg = gpu.DeviceBuffer(om.Ngather)
+    gpu.ogs_gather(gm, dAq, dg)
+    np.testing.assert_array_equal(dg.download(), om.gather(AqL))
+    # scatter (NoTrans)
+    dv = gpu.DeviceBuffer.from_host(np.zeros(om.NL))
+    gpu.ogs_scatter(gm, dq, dv)
+    np.testing.assert_array_equal(dv.download(), om.scatter(q))
+
+
+@pytest.mark.parametrize("affine,pert,Nf", [(False, 0.1, 1), (True, 0.0, 1), (False, 0.0, 3)])
+def test_operator_forcing_and_diagonal(gpu, oracle, affine, pert, Nf):
+    om = oracle.Mesh(3, 3, 2, 4, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(3, 3, 2, N=4, affine=affine, Nfields=Nf, pert=pert)
+    S = gpu.BP(gm)
+    q = 2 * oracle.random(3, om.Ngather) - 1
+    dq, dAq = gpu.DeviceBuffer.from_host(q), gpu.DeviceBuffer(om.Ngather)
+    S.operator(dq, dAq)
+    assert _rel(dAq.download(), om.operator(q)) < AX_TOL
+    # seeded forcing: f bit-exact, b = M f
+    f_o, b_o = om.rhs_random(0)
+    df = gpu.DeviceBuffer(om.Ngather)
+    b = S.rhs("RANDOM", 0, f=df)
+    np.testing.assert_array_equal(df.download(), f_o)
+    assert _rel(b.download(), b_o) < 1e-13
+    # analytic forcing
+    assert _rel(S.rhs("ANALYTIC").download(), om.rhs_analytic(1.0)) < 1e-12
+    # assembled diagonal
+    assert _rel(S.diagonal().download(), om.jacobi_diag(1.0)) < 1e-12
+
+
+CG_CASES = [(4, 4, 4, 4, True, 0.0, "NONE", "RANDOM"), (4, 4, 4, 4, False, 0.0, "JACOBI", "RANDOM"),
+            (3, 3, 3, 7, False, 0.1, "JACOBI", "RANDOM"), (3, 3, 3, 7, False, 0.1, "NONE", "ANALYTIC"),
+            (2, 2, 2, 10, False, 0.1, "NONE", "RANDOM"), (2, 2, 2, 3, False, 0.0, "JACOBI", "RANDOM")]
+
+
+@pytest.mark.parametrize("nx,ny,nz,N,affine,pert,precon,forcing", CG_CASES)
+def test_cg_history_matches_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, precon, forcing):
+    om = oracle.Mesh(nx, ny, nz, N, affine=affine, pert=pert)
+    gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, pert=pert)
+    S = gpu.BP(gm, precon=precon)
+    b_o = om.rhs_random(0)[1] if forcing == "RANDOM" else om.rhs_analytic(1.0)
+    maxit = 100
+    x_o, r_o, it_o, hr_o, ha_o = om.cg(b_o, 1.0, 0.0, maxit, precon=(precon == "JACOBI"))
+    db = S.rhs(forcing, 0)
+    x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
+    st, hr, ha = S.solve(x, db, tol=0.0, maxit=maxit)
+    assert st.iterations == it_o == maxit
+    np.testing.assert_array_less(np.abs(hr - hr_o) / hr_o, HIST_TOL)
+    np.testing.assert_array_less(np.abs(ha - ha_o) / np.abs(ha_o), HIST_TOL)
+    assert _rel(x.download(), x_o) < 1e-9
+
+
+def test_cg_tolerance_stop_and_host_entry(gpu, oracle):
+    om = oracle.Mesh(4, 4, 4, 3, pert=0.1)
+    gm = gpu.Mesh(4, 4, 4, N=3, pert=0.1)
+    S = gpu.BP(gm, precon="JACOBI")
+    f_o, b_o = om.rhs_random(0)
+    x_o, r_o, it_o, hr_o, _ = om.cg(b_o, 1.0, 1e-8, 5000, precon=True)
+    assert it_o < 5000
+    db = gpu.DeviceBuffer.from_host(b_o)
+    x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
+    st, hr, ha = S.solve(x, db, tol=1e-8, maxit=5000)
+    assert st.iterations == it_o
+    assert np.sqrt(st.rdotr / st.rdotr0) <= 1e-8
+    # the host-buffer entry point gives the same solution
+    xh = np.zeros(om.Ngather)
+    st2 = S.solve_host(b_o, xh, tol=1e-8, maxit=5000)
+    assert st2.iterations == it_o
+    np.testing.assert_array_equal(xh, x.download())
+    assert _rel(xh, x_o) < 1e-8
+
+
+def test_plain_cg_reference_stop_rule(gpu, oracle):
+    # the reference's rule TOL = max(tol^2 r0.r0, tol^2) (linearSolverCG.cpp:87)
+    om = oracle.Mesh(3, 3, 3, 4)
+    gm = gpu.Mesh(3, 3, 3, N=4)
+    S = gpu.BP(gm)
+    b_o = om.rhs_analytic(1.0)
+    for tol in (1e-3, 1e-6, 1e-9):
+        _, _, it_o, _, _ = om.cg(b_o, 1.0, tol, 1000)
+        st, _, _ = S.solve(gpu.DeviceBuffer.from_host(np.zeros(om.Ngather)), S.rhs("ANALYTIC"), tol=tol, maxit=1000)
+        assert st.iterations == it_o
+
+
+def test_empty_problem_and_zero_iterations(gpu):
+    gm = gpu.Mesh(1, 1, 1, N=1)       # every node is on the boundary: no unknowns
+    assert gm.Ngather == 0
+    S = gpu.BP(gm)
+    st, hr, ha = S.solve(gpu.DeviceBuffer(0), gpu.DeviceBuffer(0), maxit=10)
+    assert st.iterations == 0
+    gm2 = gpu.Mesh(2, 2, 2, N=2)
+    S2 = gpu.BP(gm2)
+    st, _, _ = S2.solve(gpu.DeviceBuffer.from_host(np.zeros(gm2.Ngather)), S2.rhs("RANDOM"), maxit=0)
+    assert st.iterations == 0
+
+
+def test_bad_arguments_fail_loudly(gpu):
+    with pytest.raises(gpu.BPError):
+        gpu.Mesh(2, 2, 2, N=4, pert=0.7)
+    gm = gpu.Mesh(2, 2, 2, N=2)
+    with pytest.raises(gpu.BPError):
+        gpu.BP(gm, bp=6)                  # BP6 needs three fields
+    with pytest.raises(gpu.BPError):
+        gpu.BP(gm).solve(gpu.DeviceBuffer(gm.Ngather), gpu.DeviceBuffer(gm.Ngather), maxit=-1)
+
+
+def test_driver_result_line(gpu, capfd):
+    assert gpu.driver_main("BP5", ["-nx", "4", "-ny", "4", "-nz", "4", "-p", "3", "-wi", "10", "-v"]) == 0
+    out = capfd.readouterr().out
+    line = [l for l in out.splitlines() if l.startswith("BP5: N=")][0]
+    assert line.startswith("BP5: N= 3, DOFs=1331, elapsed=")
+    assert "iterations=100, time per DOF=" in line and line.endswith("Element=Hex ")
+    assert "CG: it 100, r norm" in out
+    assert gpu.driver_main("BK5", ["-nx", "4", "-ny", "4", "-nz", "4", "-p", "3", "-a"]) == 0
+    out = capfd.readouterr().out
+    assert [l for l in out.splitlines() if l.startswith("BK5: N= 3, DOFs=1331,")][0].endswith("Element=Hex, Affine ")
+
+
+@pytest.mark.slow
+def test_full_size_properties(gpu, oracle):
+    # the benchmark mesh (40^3, p=7, perturbed): operator symmetric positive and
+    # the first CG iterations against the oracle on the same mesh
+    gm = gpu.Mesh(40, 40, 40, N=7, pert=0.1, pert_seed=1)
+    assert gm.Ngather == 279 ** 3
+    S = gpu.BP(gm, precon="JACOBI")
+    rng = np.random.default_rng(0)
+    u, v = rng.standard_normal(gm.Ngather), rng.standard_normal(gm.Ngather)
+    du, dv, dAu, dAv = (gpu.DeviceBuffer.from_host(u), gpu.DeviceBuffer.from_host(v), gpu.DeviceBuffer(gm.Ngather),
+                        gpu.DeviceBuffer(gm.Ngather))
+    S.operator(du, dAu)
+    S.operator(dv, dAv)
+    Au, Av = dAu.download(), dAv.download()
+    assert abs(u @ Av - v @ Au) <= 1e-11 * abs(u @ Av)
+    assert u @ Au > 0
