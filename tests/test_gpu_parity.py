@@ -76,9 +76,27 @@ def test_operator_forcing_and_diagonal(gpu, oracle, affine, pert, Nf):
     assert _rel(S.diagonal().download(), om.jacobi_diag(1.0)) < 1e-12
 
 
-CG_CASES = [(4, 4, 4, 4, True, 0.0, "NONE", "RANDOM"), (4, 4, 4, 4, False, 0.0, "JACOBI", "RANDOM"),
-            (3, 3, 3, 7, False, 0.1, "JACOBI", "RANDOM"), (3, 3, 3, 7, False, 0.1, "NONE", "ANALYTIC"),
-            (2, 2, 2, 10, False, 0.1, "NONE", "RANDOM"), (2, 2, 2, 3, False, 0.0, "JACOBI", "RANDOM")]
+# (16,16,16,4) affine with Jacobi-CG and the seeded forcing is the reference's
+# CPU-runnable configuration; the others cover non-affine, perturbed, high
+# degree and the analytic forcing.
+CG_CASES = [(16, 16, 16, 4, True, 0.0, "JACOBI", "RANDOM"), (16, 16, 16, 4, True, 0.0, "NONE", "RANDOM"),
+            (16, 16, 16, 4, False, 0.0, "NONE", "ANALYTIC"), (6, 6, 6, 7, False, 0.1, "JACOBI", "RANDOM"),
+            (6, 6, 6, 7, False, 0.1, "NONE", "RANDOM"), (4, 4, 4, 10, False, 0.1, "JACOBI", "RANDOM"),
+            (3, 3, 3, 3, False, 0.0, "JACOBI", "RANDOM")]
+
+
+def _check_history(h, h_o, tol=HIST_TOL, floor=1e-6, tail=True):
+    # Per-iteration bound while the residual is above floor*r0.  Once CG has
+    # reduced the residual further, rounding differences of 1e-16 (summation
+    # order, FMA) are amplified by roughly r0/r_k (measured: 5e-6 relative at
+    # r_k = 1e-9 r0 between two CPU summation orders), so deeper iterations are
+    # held to an absolute bound relative to r0 instead.
+    live = h_o >= floor * h_o[0]
+    rel = np.abs(h - h_o) / h_o
+    assert np.all(rel[live] < tol), (np.flatnonzero(~(rel < tol) & live), rel.max())
+    if tail:
+        assert np.all(np.abs(h - h_o) <= tol * h_o[0])
+    return live
 
 
 @pytest.mark.parametrize("nx,ny,nz,N,affine,pert,precon,forcing", CG_CASES)
@@ -93,8 +111,18 @@ def test_cg_history_matches_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, pre
     x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
     st, hr, ha = S.solve(x, db, tol=0.0, maxit=maxit)
     assert st.iterations == it_o == maxit
-    np.testing.assert_array_less(np.abs(hr - hr_o) / hr_o, HIST_TOL)
-    np.testing.assert_array_less(np.abs(ha - ha_o) / np.abs(ha_o), HIST_TOL)
+    if forcing == "ANALYTIC":
+        # The analytic forcing (okl/rhsHex3D.okl:31-33) is nearly an eigenvector
+        # of the operator: CG collapses the residual by eight orders within four
+        # iterations (17-21 here).  Inside that window the history is not
+        # reproducible between FP64 implementations -- the oracle's own affine
+        # and stored-factor operators, 1.6e-14 apart, differ by 65% at
+        # iteration 19 -- so it is compared up to the collapse, and the
+        # converged solution below.
+        live = _check_history(hr, hr_o, floor=1e-3, tail=False)
+    else:
+        live = _check_history(hr, hr_o)
+    assert np.all((np.abs(ha - ha_o) / np.abs(ha_o))[live] < HIST_TOL)
     assert _rel(x.download(), x_o) < 1e-9
 
 
