@@ -155,7 +155,7 @@ int bp_stream_destroy(bp_stream_t s) {
 
 int bp_finish(bp_stream_t s) {
   BP_CUDA_TRY(cudaStreamSynchronize(to_stream(s)));
-  return BP_SUCCESS;
+  return check_device_error();
 }
 
 int bp_event_create(bp_event_t* ev) {

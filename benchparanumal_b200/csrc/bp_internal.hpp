@@ -135,4 +135,13 @@ int launch_update_cg(int32_t N, const double* Ap, double alpha, double* r, doubl
                      unsigned int* counter, cudaStream_t s);
 
 int reduction_blocks();
+
+// TMA-staged stored-factor operator (bp_ax_tma.cu); returns 1 when the
+// configuration is not covered and nothing was launched
+int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                  const double* wJ, const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
+                  const int* skip, cudaStream_t s);
+// the device error word set by kernels whose bounded waits gave up
+int* device_error_word();
+int check_device_error();
 }  // namespace bp

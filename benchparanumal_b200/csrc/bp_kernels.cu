@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
+#include <string>
 
 #include "bp_internal.hpp"
 
@@ -173,12 +175,29 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
   }
 }
 
+// Kernel variant of the stored-factor operator: the TMA-staged kernel where it
+// applies, else the register-pencil kernel.  BP_AX_VARIANT=pencil in the
+// environment selects the pencil kernel everywhere (for comparisons).
+enum { AX_AUTO = 0, AX_PENCIL = 1 };
+static int ax_variant() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("BP_AX_VARIANT");
+    v = (e && std::string(e) == "pencil") ? AX_PENCIL : AX_AUTO;
+  }
+  return v;
+}
+
 template <int NQ>
 static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
                         const int32_t* G2L, const double* wJ, const double* ggeo, const double* gllw,
                         const double* D, double lambda, const double* q, double* Aq, const int* skip,
                         cudaStream_t s) {
   constexpr int EPB = AxShape<NQ>::EPB;
+  if (!d.affine && ax_variant() != AX_PENCIL) {
+    const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, s);
+    if (rc != 1) return rc;   // 1: configuration not covered by the TMA kernel
+  }
   const dim3 block(NQ, NQ, EPB);
   const dim3 grid((Nelements + EPB - 1) / EPB);
   const bool vec = ((reinterpret_cast<uintptr_t>(ggeo) & 15) == 0);

@@ -360,6 +360,7 @@ static int solve_device(bp_solver_s* S, double* x, double* r, double tol, int ma
       stats->elapsed_ms = ms;
     }
   }
+  BP_TRY(check_device_error());
   if (h.breakdown) return fail(BP_ERROR_NUMERIC, "bp_solver_solve: CG breakdown (p.Ap <= 0 or non-finite residual)");
   return BP_SUCCESS;
 }
