@@ -39,7 +39,7 @@ EXPORTS = [
     "bp_mesh_create", "bp_mesh_view", "bp_mesh_destroy",
     "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
-    "bp_box_numbering", "bp_basis_gll", "bp_box_vertices",
+    "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc",
 ]
 
 
@@ -135,6 +135,8 @@ def lib():
             "bp_box_numbering": [ctypes.POINTER(BoxDesc), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, vp, vp],
             "bp_basis_gll": [i32, vp, vp, vp],
             "bp_box_vertices": [ctypes.POINTER(BoxDesc), vp, vp, vp],
+            "bp_operator_hex3d_noalloc": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, i32, vp, vp,
+                                          vp, vp, vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -299,6 +301,21 @@ def ogs_gather(mesh, v, gv, stream=None):
 
 def ogs_scatter(mesh, gv, v, stream=None):
     _check(lib().bp_ogs_scatter(mesh.Ngather, mesh.view.rowStarts, mesh.view.colIds, _ptr(gv), _ptr(v), stream))
+
+
+NOALLOC_MAX_LOCAL = 1 << 20
+
+
+def operator_noalloc(mesh, q, Aq, lam=1.0, stream=None):
+    """bp_operator_hex3d_noalloc: Aq = Gather(A_e q[G2L]) with no device
+    allocation (element results in the library's fixed scratch array), for
+    callers that may not call cudaMalloc.  Meshes with E*Np*Nfields above
+    NOALLOC_MAX_LOCAL are rejected."""
+    v = mesh.view
+    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    _check(lib().bp_operator_hex3d_noalloc(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, v.wJ, v.ggeo,
+                                           v.gllw, v.D, float(lam), mesh.Ngather, v.rowStarts, v.colIds, _ptr(q),
+                                           _ptr(Aq), stream))
 
 
 def _ptr(b):

@@ -126,6 +126,29 @@ int bp_linalg_norm2(int32_t N, const double* x, double* result, bp_stream_t stre
 int bp_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* rdotr,
                  bp_stream_t stream);
 
+/* The BP5/BP6 operator, Aq = Gather(A_e q[GlobalToLocal]), without any device
+   allocation.  No counterpart in the reference: it exists for callers that
+   cannot call cudaMalloc -- an application whose own pool allocator owns the
+   device memory budget, or a pipeline that cannot accept the device-wide
+   synchronisation that cudaMalloc/cudaFree imply.  The element-local results
+   live in a fixed 8 MiB array inside the library image (every GPU that loads
+   the library holds it until the process exits), so Nelements*Np*Nfields may
+   not exceed BP_NOALLOC_MAX_LOCAL; larger meshes are rejected with
+   BP_ERROR_ARG (use bp_solver_operator for them).  The first call on a device
+   looks up the array's device address with that device current; make that
+   first call before any stream capture.  All calls share the array and it
+   keeps the last call's contents (nothing in it needs to start at zero), so
+   calls that overlap on the GPU -- on different streams, or from several host
+   threads -- race with each other.  Arguments are those of bp_ax_hex3d plus
+   the gather's CSR (Ngather, rowStarts, colIds); q [Ngather] in, Aq
+   [Ngather] out, both device memory. */
+#define BP_NOALLOC_MAX_LOCAL (1 << 20)
+int bp_operator_hex3d_noalloc(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                              const int32_t* GlobalToLocal, const double* wJ, const double* ggeo,
+                              const double* gllw, const double* D, double lambda, int32_t Ngather,
+                              const int32_t* rowStarts, const int32_t* colIds, const double* q, double* Aq,
+                              bp_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Mesh and masked gather-scatter setup.  Replaces mesh_t::Setup for the Hex3D
  * box (libs/mesh/meshSetup.cpp:31-85, meshSetupBoxHex3D.cpp:31-131,
