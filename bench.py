@@ -248,7 +248,7 @@ def main():
     bp._check(L.bp_event_elapsed_ms(e0, e1, bp.ctypes.byref(ms)))
     t_dev = max_over_ranks(ms.value / 1e3, world)
     value = world * Nd * ITERS * args.steps / t_dev / 1e9
-    launches_per_step = 3 + 4 * ITERS + 1
+    launches_per_step = 3 + 3 * ITERS + 1   # operator + init, 3 kernels per iteration, final x update
 
     # ---- dominant kernel: the element operator, timed alone with events (BK5 style) ----
     q = b

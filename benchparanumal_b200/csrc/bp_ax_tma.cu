@@ -20,7 +20,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
+#include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
 
 namespace bp {
@@ -95,27 +97,28 @@ struct TmaShape {
   static constexpr int NQ2 = NQ * NQ;
   static constexpr int SLICE_G = NQ2 * 6;          // doubles of ggeo per slice
   static constexpr int SLICE_BYTES = NQ2 * 56;     // ggeo + wJ bytes per slice
-  // ring depth: whole element up to p=7, a partial ring above
-  static constexpr int R = NQ <= 8 ? NQ : (NQ <= 12 ? 6 : 4);
+  // ring depth: whole element up to p=5, four slices above (measured faster at p=7)
+  static constexpr int R = NQ <= 6 ? NQ : (NQ <= 12 ? 4 : 4);
   static constexpr int EPB = NQ <= 4 ? 8 : (NQ <= 6 ? 2 : 1);   // elements per block
 };
 
 }  // namespace
 
-template <int NQ, int NF>
+template <int NQ, int NF, bool DOT, int R>
 __global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ>::EPB * NF)
 ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
               const double* __restrict__ wJ, const double* __restrict__ ggeo, const double* __restrict__ Dg,
-              double lambda, const double* __restrict__ q, double* __restrict__ Aq, const int* __restrict__ skip) {
+              double lambda, const double* __restrict__ q, double* __restrict__ Aq, const int* __restrict__ skip,
+              CgFuse fuse) {
   if (skip && *skip) return;
   using T = TmaShape<NQ>;
-  constexpr int NQ2 = T::NQ2, NP = NQ2 * NQ, R = T::R, EPB = T::EPB, S = EPB * NF;
+  constexpr int NQ2 = T::NQ2, NP = NQ2 * NQ, EPB = T::EPB, S = EPB * NF;
   constexpr int PAD = (NQ % 2 == 0) ? 1 : 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // layout: [EPB][R] slots of ggeo slices, [EPB][R] slots of wJ slices, D, q/v/w scratch, barriers
   double* s_g = reinterpret_cast<double*>(smem_raw);
   double* s_J = s_g + EPB * R * T::SLICE_G;
-  double* s_D = s_J + EPB * R * NQ2;                     // [NQ][NQ+1]
+  double* s_D = s_J + EPB * R * NQ2;                     // [NQ][NQ] row-major, rows 16-byte aligned
   double* s_q = s_D + NQ * (NQ + 1);                     // [S][NQ][NQ+PAD]
   double* s_v = s_q + S * NQ * (NQ + PAD);
   double* s_w = s_v + S * NQ * (NQ + PAD);
@@ -145,7 +148,7 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
       }
     }
   }
-  for (int n = t; n < NQ2; n += NQ2 * S) s_D[(n / NQ) * (NQ + 1) + n % NQ] = Dg[n];
+  for (int n = t; n < NQ2; n += NQ2 * S) s_D[n] = Dg[n];
 
   // the pencil of q and the D rows of this thread, while the copies fly
   const size_t lbase = ((size_t)e * NF + f) * NP + j * NQ + i;
@@ -161,11 +164,18 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     }
   }
   __syncthreads();   // s_D
-  double Di[NQ], Dj[NQ];
+  // rows i, j of D and (up to Nq=10) columns i, j in registers; row k per slice
+  // comes from shared memory as 16-byte broadcasts
+  constexpr bool DTREG = false;   // columns i, j from shared memory: registers buy more occupancy
+  double Di[NQ], Dj[NQ], DTi[DTREG ? NQ : 1], DTj[DTREG ? NQ : 1];
 #pragma unroll
   for (int m = 0; m < NQ; ++m) {
-    Di[m] = s_D[i * (NQ + 1) + m];
-    Dj[m] = s_D[j * (NQ + 1) + m];
+    Di[m] = s_D[i * NQ + m];
+    Dj[m] = s_D[j * NQ + m];
+    if (DTREG) {
+      DTi[m] = s_D[m * NQ + i];
+      DTj[m] = s_D[m * NQ + j];
+    }
   }
   double* sq = s_q + slot * NQ * (NQ + PAD);
   double* sv = s_v + slot * NQ * (NQ + PAD);
@@ -184,9 +194,16 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
 
     sq[j * (NQ + PAD) + i] = r_u[k];
     __syncthreads();
+    double Dk[NQ];
+#pragma unroll
+    for (int m = 0; m < NQ; m += 2) {
+      const double2 d2 = *reinterpret_cast<const double2*>(s_D + k * NQ + m);
+      Dk[m] = d2.x;
+      Dk[m + 1] = d2.y;
+    }
     double ur = 0.0, us = 0.0, ut = 0.0;
 #pragma unroll
-    for (int m = 0; m < NQ; ++m) ut += s_D[k * (NQ + 1) + m] * r_u[m];
+    for (int m = 0; m < NQ; ++m) ut += Dk[m] * r_u[m];
 #pragma unroll
     for (int m = 0; m < NQ; ++m) {
       ur += Di[m] * sq[j * (NQ + PAD) + m];
@@ -195,7 +212,7 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     sw[j * (NQ + PAD) + i] = G01 * ur + G11 * us + G12 * ut;
     sv[j * (NQ + PAD) + i] = G00 * ur + G01 * us + G02 * ut;
     const double GDut = G02 * ur + G12 * us + G22 * ut;
-    double Auk = GwJ * lambda * r_u[k];
+    double Auk = GwJ * lambda * r_u[k], Auk2 = 0.0;
     __syncthreads();
     // slot rs is free again: refill it with slice k+R
     if (R < NQ && k + R < NQ && t == 0) {
@@ -208,48 +225,93 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
       }
     }
 #pragma unroll
-    for (int m = 0; m < NQ; ++m) r_Au[m] += s_D[k * (NQ + 1) + m] * GDut;
+    for (int m = 0; m < NQ; ++m) r_Au[m] += Dk[m] * GDut;
 #pragma unroll
     for (int m = 0; m < NQ; ++m) {
-      Auk += s_D[m * (NQ + 1) + j] * sw[m * (NQ + PAD) + i];
-      Auk += s_D[m * (NQ + 1) + i] * sv[j * (NQ + PAD) + m];
+      Auk += (DTREG ? DTj[m] : s_D[m * NQ + j]) * sw[m * (NQ + PAD) + i];
+      Auk2 += (DTREG ? DTi[m] : s_D[m * NQ + i]) * sv[j * (NQ + PAD) + m];
     }
-    r_Au[k] += Auk;
+    r_Au[k] += Auk + Auk2;
   }
-  if (!ok) {
-    atomicExch(&g_device_error, 1);
+  if (!__syncthreads_and(ok)) {   // block-uniform: every thread leaves together
+    if (t == 0) atomicExch(&g_device_error, 1);
     return;
   }
   if (active) {
 #pragma unroll
     for (int k = 0; k < NQ; ++k) Aq[lbase + k * NQ2] = r_Au[k];
   }
+  if (DOT) {
+    double v = 0.0;
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) v += r_u[k] * r_Au[k];
+    }
+    fuse_pap(v, fuse, s_g);   // the factor ring is free now and holds >= one double per thread
+  }
 }
 
-template <int NQ, int NF>
+template <int NQ, int NF, int R>
 static size_t tma_smem_bytes() {
   using T = TmaShape<NQ>;
   constexpr int S = T::EPB * NF, PAD = (NQ % 2 == 0) ? 1 : 0;
-  return sizeof(double) * ((size_t)T::EPB * T::R * (T::SLICE_G + T::NQ2) + NQ * (NQ + 1) + 3 * S * NQ * (NQ + PAD)) +
-         sizeof(uint64_t) * T::R;
+  return sizeof(double) * ((size_t)T::EPB * R * (T::SLICE_G + T::NQ2) + NQ * (NQ + 1) + 3 * S * NQ * (NQ + PAD)) +
+         sizeof(uint64_t) * R;
+}
+
+template <int NQ, int NF, bool DOT, int R>
+static int launch_tma_r(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
+                        const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
+                        const int* skip, const CgFuse& fuse, cudaStream_t s, int* nblocks) {
+  using T = TmaShape<NQ>;
+  const size_t smem = tma_smem_bytes<NQ, NF, R>();
+  static bool configured = false;
+  if (!configured) {
+    BP_CUDA_TRY(
+        cudaFuncSetAttribute(ax_tma_kernel<NQ, NF, DOT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  const dim3 block(NQ, NQ, T::EPB * NF);
+  const dim3 grid((Nelements + T::EPB - 1) / T::EPB);
+  if (nblocks) *nblocks = (int)grid.x;
+  ax_tma_kernel<NQ, NF, DOT, R><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq,
+                                                          skip, fuse);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
+// ring depth: BP_TMA_RING=half in the environment halves the default ring
+// (for tuning runs)
+static bool tma_half_ring() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("BP_TMA_RING");
+    v = (e && e[0] == 'h') ? 1 : 0;
+  }
+  return v == 1;
+}
+
+template <int NQ, int NF, bool DOT>
+static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
+                          const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
+                          const int* skip, const CgFuse& fuse, cudaStream_t s, int* nblocks) {
+  constexpr int R = TmaShape<NQ>::R, RH = R / 2 > 0 ? R / 2 : 1;
+  if (tma_half_ring())
+    return launch_tma_r<NQ, NF, DOT, RH>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s,
+                                         nblocks);
+  return launch_tma_r<NQ, NF, DOT, R>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s,
+                                      nblocks);
 }
 
 template <int NQ, int NF>
 static int launch_tma(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
                       const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
-                      const int* skip, cudaStream_t s) {
-  using T = TmaShape<NQ>;
-  const size_t smem = tma_smem_bytes<NQ, NF>();
-  static bool configured = false;
-  if (!configured) {
-    BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
-  const dim3 block(NQ, NQ, T::EPB * NF);
-  const dim3 grid((Nelements + T::EPB - 1) / T::EPB);
-  ax_tma_kernel<NQ, NF><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip);
-  BP_CUDA_TRY(cudaGetLastError());
-  return BP_SUCCESS;
+                      const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
+  if (fuse)
+    return launch_tma_dot<NQ, NF, true>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, *fuse, s,
+                                        nblocks);
+  return launch_tma_dot<NQ, NF, false>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, CgFuse{}, s,
+                                       nblocks);
 }
 
 // Stored-factor operator through the TMA path.  Returns 1 (and launches
@@ -257,7 +319,7 @@ static int launch_tma(int32_t Nelements, const int32_t* elementList, const int32
 // multiple of 16 bytes), affine factors, or factor arrays not 16-byte aligned.
 int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const double* wJ, const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
-                  const int* skip, cudaStream_t s) {
+                  const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   const int NQ = d.N + 1;
   if (d.affine || (NQ % 2) != 0 || ((reinterpret_cast<uintptr_t>(ggeo) | reinterpret_cast<uintptr_t>(wJ)) & 15))
     return 1;
@@ -266,11 +328,11 @@ int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
   switch (NQ) {
 #define BP_TMA_CASE(nq)                                                                                         \
   case nq:                                                                                                      \
-    return three ? launch_tma<nq, 3>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, s)          \
-                 : launch_tma<nq, 1>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, s);
+    return three ? launch_tma<nq, 3>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks)          \
+                 : launch_tma<nq, 1>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
 #define BP_TMA_CASE1(nq) \
   case nq:               \
-    return launch_tma<nq, 1>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, s);
+    return launch_tma<nq, 1>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
     BP_TMA_CASE(2) BP_TMA_CASE(4) BP_TMA_CASE(6) BP_TMA_CASE(8) BP_TMA_CASE(10) BP_TMA_CASE1(12)
     BP_TMA_CASE1(14) BP_TMA_CASE1(16)
 #undef BP_TMA_CASE

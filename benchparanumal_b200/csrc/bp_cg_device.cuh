@@ -1,0 +1,61 @@
+// Device-side CG state and the p.Ap epilogue shared by the element-operator
+// kernels and the CG kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace bp {
+
+struct CgScalars {
+  double rdotr;       // r.r after the last update (plain CG: the reference's rdotr)
+  double rdotr_prev;  // r.r one update earlier
+  double rz, rz_prev; // r.z for Jacobi CG
+  double pAp, alpha;
+  double tol2;        // stop when rdotr <= tol2
+  double rdotr0;
+  int iter;           // completed iterations
+  int done;           // 1 once converged, at maxit, or broken down
+  int maxit;
+  int breakdown;
+  int precon;
+  int pad;
+};
+
+// Where an element-operator launch inside CG leaves p.Ap.  Because
+// A = sum_e Q_e^T A_e Q_e, p.Ap = sum_e (Q_e p).(A_e Q_e p): each block adds up
+// q*Aq over its own nodes and stores the sum in partials[blockIdx.x];
+// cg_alpha_kernel then adds the partials in index order and forms alpha.
+struct CgFuse {
+  double* partials;        // [number of blocks of the operator launch]
+};
+
+// Sum of v over the block in a fixed order, valid in thread 0.  `scratch`
+// holds at least one double per thread and is free for the caller to reuse
+// (any block shape, partial warps included).
+__device__ __forceinline__ double fuse_block_sum(double v, double* scratch) {
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  __syncthreads();   // the caller's last reads of scratch are done
+  scratch[t] = v;
+  __syncthreads();
+  if (t < 32) {
+    double r = 0.0;
+    for (int k = t; k < nt; k += 32) r += scratch[k];
+    scratch[t] = r;   // index t is read by this thread only
+  }
+  __syncthreads();
+  double r = 0.0;
+  if (t == 0)
+    for (int k = 0; k < (nt < 32 ? nt : 32); ++k) r += scratch[k];
+  return r;
+}
+
+// block partial of p.Ap (plain store; the next kernel reads it)
+__device__ __forceinline__ void fuse_pap(double v, const CgFuse& F, double* scratch) {
+  const double bs = fuse_block_sum(v, scratch);
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) F.partials[blockIdx.x] = bs;
+}
+
+}  // namespace bp

@@ -103,9 +103,12 @@ struct bp_solver_s;
 
 // ---- kernel launchers (bp_kernels.cu) ----
 namespace bp {
+struct CgFuse;
+// element operator; with `fuse` it also produces p.Ap and alpha for CG (bp_cg_device.cuh)
 int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                    const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
-                   const double* q, double* Aq, const int* skip, cudaStream_t s);
+                   const double* q, double* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse = nullptr,
+                   int* nblocks = nullptr);
 int launch_ax(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
               const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
               const double* q, double* Aq, cudaStream_t s);
@@ -140,7 +143,7 @@ int reduction_blocks();
 // configuration is not covered and nothing was launched
 int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const double* wJ, const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
-                  const int* skip, cudaStream_t s);
+                  const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

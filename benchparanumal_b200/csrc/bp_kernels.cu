@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <string>
 
+#include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
 
 namespace bp {
@@ -42,12 +43,13 @@ struct AxShape {
   static constexpr int MINB = NQ <= 8 ? 2 : 1; // resident blocks per SM the register budget must allow
 };
 
-template <int NQ, int NF, bool AFFINE, bool VEC>
+template <int NQ, int NF, bool AFFINE, bool VEC, bool DOT>
 __global__ void __launch_bounds__(NQ * NQ * AxShape<NQ>::EPB, AxShape<NQ>::MINB)
 ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
                  const double* __restrict__ wJ, const double* __restrict__ ggeo,
                  const double* __restrict__ gllw, const double* __restrict__ Dg, double lambda,
-                 const double* __restrict__ q, double* __restrict__ Aq, const int* __restrict__ skip) {
+                 const double* __restrict__ q, double* __restrict__ Aq, const int* __restrict__ skip,
+                 CgFuse fuse) {
   if (skip && *skip) return;
   constexpr int EPB = AxShape<NQ>::EPB;
   constexpr int NP = NQ * NQ * NQ;
@@ -88,6 +90,7 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
     wij = s_gw[i] * s_gw[j];
   }
 
+  double pdot = 0.0;   // sum of q*Aq over this thread's nodes (DOT)
 #pragma unroll 1
   for (int f = 0; f < NF; ++f) {
     const size_t lbase = ((size_t)e * NF + f) * NP + j * NQ + i;
@@ -171,8 +174,13 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
     if (active) {
 #pragma unroll
       for (int k = 0; k < NQ; ++k) Aq[lbase + k * NQ2] = r_Au[k];
+      if (DOT) {
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) pdot += r_u[k] * r_Au[k];
+      }
     }
   }
+  if (DOT) fuse_pap(pdot, fuse, &s_q[0][0][0]);   // s_q holds one double per thread
 }
 
 // Kernel variant of the stored-factor operator: the TMA-staged kernel where it
@@ -192,42 +200,51 @@ template <int NQ>
 static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
                         const int32_t* G2L, const double* wJ, const double* ggeo, const double* gllw,
                         const double* D, double lambda, const double* q, double* Aq, const int* skip,
-                        cudaStream_t s) {
+                        const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   constexpr int EPB = AxShape<NQ>::EPB;
   if (!d.affine && ax_variant() != AX_PENCIL) {
-    const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, s);
+    const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
     if (rc != 1) return rc;   // 1: configuration not covered by the TMA kernel
   }
   const dim3 block(NQ, NQ, EPB);
   const dim3 grid((Nelements + EPB - 1) / EPB);
+  if (nblocks) *nblocks = (int)grid.x;
   const bool vec = ((reinterpret_cast<uintptr_t>(ggeo) & 15) == 0);
-  if (d.Nfields == 1) {
-    if (d.affine)
-      ax_pencil_kernel<NQ, 1, true, true><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip);
-    else if (vec)
-      ax_pencil_kernel<NQ, 1, false, true><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip);
-    else
-      ax_pencil_kernel<NQ, 1, false, false><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip);
+  const CgFuse F = fuse ? *fuse : CgFuse{};
+#define BP_PENCIL(NF, AFF, VEC, DOT) \
+  ax_pencil_kernel<NQ, NF, AFF, VEC, DOT><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, \
+                                                                 lambda, q, Aq, skip, F)
+  if (fuse) {
+    if (!d.affine && !vec) return fail(BP_ERROR_ARG, "CG operator needs 16-byte aligned geometric factors");
+    if (d.Nfields == 1) {
+      if (d.affine) BP_PENCIL(1, true, true, true); else BP_PENCIL(1, false, true, true);
+    } else {
+      if (d.affine) BP_PENCIL(3, true, true, true); else BP_PENCIL(3, false, true, true);
+    }
+  } else if (d.Nfields == 1) {
+    if (d.affine) BP_PENCIL(1, true, true, false);
+    else if (vec) BP_PENCIL(1, false, true, false);
+    else BP_PENCIL(1, false, false, false);
   } else {
-    if (d.affine)
-      ax_pencil_kernel<NQ, 3, true, true><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip);
-    else if (vec)
-      ax_pencil_kernel<NQ, 3, false, true><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip);
-    else
-      ax_pencil_kernel<NQ, 3, false, false><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip);
+    if (d.affine) BP_PENCIL(3, true, true, false);
+    else if (vec) BP_PENCIL(3, false, true, false);
+    else BP_PENCIL(3, false, false, false);
   }
+#undef BP_PENCIL
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
 int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                    const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
-                   const double* q, double* Aq, const int* skip, cudaStream_t s) {
+                   const double* q, double* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse,
+                   int* nblocks) {
+  if (nblocks) *nblocks = 0;
   if (Nelements == 0) return BP_SUCCESS;
   switch (d.N + 1) {
 #define BP_AX_CASE(nq) \
   case nq:             \
-    return launch_ax_nq<nq>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s);
+    return launch_ax_nq<nq>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s, nblocks);
     BP_AX_CASE(2) BP_AX_CASE(3) BP_AX_CASE(4) BP_AX_CASE(5) BP_AX_CASE(6) BP_AX_CASE(7) BP_AX_CASE(8)
     BP_AX_CASE(9) BP_AX_CASE(10) BP_AX_CASE(11) BP_AX_CASE(12) BP_AX_CASE(13) BP_AX_CASE(14)
     BP_AX_CASE(15) BP_AX_CASE(16)

@@ -3,12 +3,12 @@
 // libs/core/linearSolverCG.cpp:62-156).
 //
 // CG runs with every scalar on the device.  One iteration is four kernels:
-//   cg_direction_kernel  x += alpha_{k-1} p_{k-1} (deferred),  p = z + beta p
-//   ax_pencil_kernel     AqL = A_e p                (element-local operator)
-//   cg_gather_dot_kernel Ap = Gather(AqL), pAp = p.Ap, alpha = rho / pAp
-//   cg_update_kernel     r -= alpha Ap, r.r (and r.z), stop test
-// The reductions finish in the last block to arrive, so there is no host
-// round trip per iteration.  Iterations are captured once into a CUDA graph
+//   cg_direction_kernel     x += alpha_{k-1} p_{k-1} (deferred),  p = z + beta p
+//   element operator        AqL = A_e p, and block partials of p.Ap = sum_e p_e.(A_e p_e)
+//   cg_alpha_kernel         p.Ap from the partials, alpha = rho / p.Ap
+//   cg_gather_update_kernel r -= alpha Gather(AqL), r.r (and r.z), stop test
+// so A p is never stored as a gathered vector.  The reductions finish in the
+// last block to arrive, so there is no host round trip per iteration.  Iterations are captured once into a CUDA graph
 // (kChunk iterations per graph) and replayed; a finished solve turns the
 // remaining kernels into immediate returns through a device flag.
 #include <cuda_runtime.h>
@@ -17,24 +17,10 @@
 #include <cstring>
 #include <vector>
 
+#include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
 
 namespace bp {
-
-struct CgScalars {
-  double rdotr;       // r.r after the last update (plain CG: the reference's rdotr)
-  double rdotr_prev;  // r.r one update earlier
-  double rz, rz_prev; // r.z for Jacobi CG
-  double pAp, alpha;
-  double tol2;        // stop when rdotr <= tol2
-  double rdotr0;
-  int iter;           // completed iterations
-  int done;           // 1 once converged, at maxit, or broken down
-  int maxit;
-  int breakdown;
-  int precon;
-  int pad;
-};
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 20;   // iterations per captured graph (divides the usual 100 and 1000)
@@ -149,23 +135,20 @@ cg_direction_kernel(int32_t N, double* __restrict__ x, double* __restrict__ p, c
   }
 }
 
-// Ap[row] = sum of AqL over the row (column order), pAp = p.Ap, alpha
-__global__ void __launch_bounds__(kThreads)
-cg_gather_dot_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const int32_t* __restrict__ colIds,
-                     const double* __restrict__ AqL, const double* __restrict__ p, double* __restrict__ Ap,
-                     CgScalars* sc, double* hist_alpha, double* partials, unsigned int* counter) {
+// p.Ap from the element operator's block partials (index order), then alpha
+constexpr int kAlphaThreads = 1024;
+__global__ void __launch_bounds__(kAlphaThreads)
+cg_alpha_kernel(int nparts, const double* __restrict__ parts, CgScalars* sc, double* hist_alpha) {
   if (sc->done) return;
-  double acc[1] = {0.0};
-  for (int32_t r = blockIdx.x * kThreads + threadIdx.x; r < Nrows; r += kThreads * gridDim.x) {
-    const int32_t start = rowStarts[r], end = rowStarts[r + 1];
-    double s = 0.0;
-    for (int32_t c = start; c < end; ++c) s += __ldg(AqL + __ldg(colIds + c));
-    Ap[r] = s;
-    acc[0] += p[r] * s;
-  }
-  double tot[1];
-  if (grid_sum_cg<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
-    const double pAp = tot[0];
+  __shared__ double s_w[kAlphaThreads / 32];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < nparts; k += kAlphaThreads) acc += parts[k];
+  acc = warp_sum_cg(acc);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double pAp = 0.0;
+    for (int w = 0; w < kAlphaThreads / 32; ++w) pAp += s_w[w];
     const double rho = sc->precon ? sc->rz : sc->rdotr;
     const double alpha = rho / pAp;
     sc->pAp = pAp;
@@ -179,19 +162,29 @@ cg_gather_dot_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const
   }
 }
 
-// r -= alpha Ap; r.r (and r.z); stop test
+// r -= alpha Gather(AqL); r.r (and r.z); stop test.  alpha comes from the
+// element operator's p.Ap epilogue.
+// One row per thread: r and invD of the row are requested first, then the
+// row's local values in column order (the reference's order, so the sums match
+// its gather bit for bit).
 __global__ void __launch_bounds__(kThreads)
-cg_update_kernel(int32_t N, const double* __restrict__ Ap, double* __restrict__ r, const double* __restrict__ invD,
-                 CgScalars* sc, double* hist_rnorm, double* partials, unsigned int* counter) {
+cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const int32_t* __restrict__ colIds,
+                        const double* __restrict__ AqL, double* __restrict__ r, const double* __restrict__ invD,
+                        CgScalars* sc, double* hist_rnorm, double* partials, unsigned int* counter) {
   if (sc->done) return;
   const double alpha = sc->alpha;
   const bool precon = sc->precon != 0;
   double acc[2] = {0.0, 0.0};
-  for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
-    const double rn = r[n] - alpha * Ap[n];
-    r[n] = rn;
+  for (int32_t row = blockIdx.x * kThreads + threadIdx.x; row < Nrows; row += kThreads * gridDim.x) {
+    const double rold = r[row];
+    const double dinv = precon ? __ldg(invD + row) : 0.0;
+    const int32_t start = __ldg(rowStarts + row), end = __ldg(rowStarts + row + 1);
+    double s = 0.0;
+    for (int32_t c = start; c < end; ++c) s += __ldg(AqL + __ldg(colIds + c));
+    const double rn = rold - alpha * s;
+    r[row] = rn;
     acc[0] += rn * rn;
-    if (precon) acc[1] += rn * invD[n] * rn;
+    if (precon) acc[1] += rn * dinv * rn;
   }
   double tot[2];
   if (grid_sum_cg<2>(acc, partials, counter, tot) && threadIdx.x == 0) {
@@ -239,7 +232,7 @@ struct bp_solver_s {
   int precon = 0;
   int32_t N = 0;               // Ngather
   bp_ax_desc_t ax{};
-  DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist;
+  DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist, fuse_partials;
   DeviceArray<unsigned int> counter;
   DeviceArray<CgScalars> sc;
   int hist_len = 0;
@@ -273,13 +266,14 @@ static int enqueue_iteration(bp_solver_s* S, double* x, double* r, cudaStream_t 
   double* hist_rnorm = S->hist.ptr ? S->hist.ptr + S->hist_len : nullptr;
   cg_direction_kernel<<<g, kThreads, 0, s>>>(N, x, S->p.ptr, r, S->invD.ptr, S->sc.ptr);
   BP_CUDA_TRY(cudaGetLastError());
+  const CgFuse fuse{S->fuse_partials.ptr};
+  int nparts = 0;
   BP_TRY(launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, m->wJ.ptr, m->ggeo.ptr, m->gllw.ptr, m->D.ptr,
-                        S->lambda, S->p.ptr, S->AqL.ptr, &S->sc.ptr->done, s));
-  cg_gather_dot_kernel<<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, S->p.ptr, S->Ap.ptr,
-                                              S->sc.ptr, hist_alpha, S->partials.ptr, S->counter.ptr);
+                        S->lambda, S->p.ptr, S->AqL.ptr, &S->sc.ptr->done, s, &fuse, &nparts));
+  cg_alpha_kernel<<<1, kAlphaThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->sc.ptr, hist_alpha);
   BP_CUDA_TRY(cudaGetLastError());
-  cg_update_kernel<<<g, kThreads, 0, s>>>(N, S->Ap.ptr, r, S->invD.ptr, S->sc.ptr, hist_rnorm, S->partials.ptr,
-                                          S->counter.ptr);
+  cg_gather_update_kernel<<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, r, S->invD.ptr,
+                                                 S->sc.ptr, hist_rnorm, S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
@@ -396,6 +390,9 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
     if ((rc = S->Ap.alloc(S->N))) break;
     if ((rc = S->partials.alloc((size_t)4 * reduction_blocks()))) break;
     if ((rc = S->counter.alloc(4))) break;
+    // p.Ap epilogue of the element operator: one partial per block, at most
+    // one block per element
+    if ((rc = S->fuse_partials.alloc((size_t)mesh->E + 1))) break;
     if ((rc = S->sc.alloc(1))) break;
     cudaError_t ce = cudaMemsetAsync(S->p.ptr, 0, sizeof(double) * S->N, s);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(S->counter.ptr, 0, sizeof(unsigned int) * 4, s);
