@@ -39,6 +39,7 @@ WORKLOAD = ("BP5 Hex3D p=7, 40^3 elements, interior vertices perturbed 0.1h (see
             "FP64 Jacobi-PCG, 100 iterations per step, forcing f=2u-1 (seed 0)")
 # CPU sample: the same problem family on a 20^3 sub-box (1/8 of the elements)
 CPU_NX, CPU_ITERS = 20, 100
+MIXED_TOL = 1e-8
 # DRAM traffic of one Ax launch of this workload, from the ncu capture summarised
 # in profiles/ax_bp5_p7_40cubed.md (None until captured)
 AX_DRAM_BYTES = None
@@ -198,6 +199,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ax-launches", type=int, default=20)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the time-to-tolerance comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -281,6 +283,40 @@ def main():
     t_e2e = max_over_ranks(t1 - t0, world)
     e2e = world * Nd * ITERS * args.steps / t_e2e / 1e9
 
+    # ---- time to 1e-8 relative residual: FP64 Jacobi-CG against the mixed solver ----
+    mixed = None
+    if not args.no_mixed:
+        Sm = bp.BP(mesh, precon="JACOBI", precision="MIXED")
+
+        def to_tol(solver):
+            bp._check(L.bp_memset(x.ptr, 0, x.nbytes, None))
+            bp._check(L.bp_memcpy_dtod(r.ptr, b.ptr, r.nbytes, None))
+            st = bp.SolveStats()
+            bp._check(L.bp_solver_solve(solver._h, x.ptr, r.ptr, MIXED_TOL, 50000, None, None, bp.ctypes.byref(st)))
+            return st
+
+        to_tol(S)
+        to_tol(Sm)                                  # warm: graphs captured, caches primed
+        barrier(world)
+        st64 = to_tol(S)
+        stmx = to_tol(Sm)
+        t64 = max_over_ranks(st64.elapsed_ms / 1e3, world)
+        tmx = max_over_ranks(stmx.elapsed_ms / 1e3, world)
+        # FP64 check of the mixed solution's residual
+        Ax = bp.DeviceBuffer(Nd)
+        S.operator(x, Ax)
+        resid = float(np.linalg.norm(b.download() - Ax.download()) / np.linalg.norm(b.download()))
+        mixed = {"tolerance": MIXED_TOL,
+                 "fp64": {"iterations": st64.iterations, "seconds": t64,
+                          "gdof_it_s": world * Nd * st64.iterations / t64 / 1e9,
+                          "relative_residual": float(np.sqrt(st64.rdotr / st64.rdotr0))},
+                 "mixed": {"iterations": stmx.iterations, "reliable_updates": stmx.updates, "seconds": tmx,
+                           "gdof_it_s": world * Nd * stmx.iterations / tmx / 1e9,
+                           "relative_residual_fp64_check": resid},
+                 "speedup_time_to_solution": t64 / tmx,
+                 "speedup_gdof_it_s": (stmx.iterations / tmx) / (st64.iterations / t64)}
+        del Sm, Ax
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample, _ = cpu_sample(steps=1, warmup=0)
@@ -305,6 +341,7 @@ def main():
                          "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes, "launch_ms": ax_s * 1e3},
             "model_bw_gbs": step_bytes * args.steps / (t_dev / world) / 1e9 if world == 1 else None,
             "cpu_baseline": cpu,
+            "mixed_vs_fp64_to_1e-8": mixed,
         }
         print(json.dumps(line))
     if world > 1:

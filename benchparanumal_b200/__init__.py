@@ -28,6 +28,8 @@ BP_PRECON_NONE = 0
 BP_PRECON_JACOBI = 1
 BP_RHS_ANALYTIC = 0
 BP_RHS_RANDOM = 1
+BP_PRECISION_FP64 = 0
+BP_PRECISION_MIXED = 1
 
 EXPORTS = [
     "bp_last_error", "bp_version", "bp_platform_init", "bp_device_count", "bp_device_info",
@@ -71,12 +73,13 @@ class MeshView(ctypes.Structure):
 
 
 class SolverDesc(ctypes.Structure):
-    _fields_ = [("bp", ctypes.c_int32), ("lambda_", ctypes.c_double), ("precon", ctypes.c_int32)]
+    _fields_ = [("bp", ctypes.c_int32), ("lambda_", ctypes.c_double), ("precon", ctypes.c_int32),
+                ("precision", ctypes.c_int32)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("rdotr0", ctypes.c_double), ("rdotr", ctypes.c_double),
-                ("elapsed_ms", ctypes.c_double)]
+                ("elapsed_ms", ctypes.c_double), ("updates", ctypes.c_int32)]
 
 
 _lib = None
@@ -329,16 +332,18 @@ def _ptr(b):
 class BP:
     """Benchmark problem on a Mesh: bp 5 (scalar) or 6 (three fields)."""
 
-    def __init__(self, mesh, bp=None, lam=1.0, precon="NONE"):
+    def __init__(self, mesh, bp=None, lam=1.0, precon="NONE", precision="FP64"):
         self.mesh = mesh
         bp = bp or (6 if mesh.Nfields == 3 else 5)
         pc = {"NONE": BP_PRECON_NONE, "JACOBI": BP_PRECON_JACOBI}[precon.upper()]
-        d = SolverDesc(bp, float(lam), pc)
+        pr = {"FP64": BP_PRECISION_FP64, "MIXED": BP_PRECISION_MIXED}[precision.upper()]
+        d = SolverDesc(bp, float(lam), pc, pr)
         h = ctypes.c_void_p()
         _check(lib().bp_solver_create(mesh._h, ctypes.byref(d), ctypes.byref(h)))
         self._h = h.value
         self.N = mesh.Ngather
         self.precon = precon.upper()
+        self.precision = precision.upper()
 
     def __del__(self):
         if getattr(self, "_h", None):

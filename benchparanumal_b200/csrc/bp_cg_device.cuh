@@ -13,14 +13,18 @@ struct CgScalars {
   double rdotr_prev;  // r.r one update earlier
   double rz, rz_prev; // r.z for Jacobi CG
   double pAp, alpha;
-  double tol2;        // stop when rdotr <= tol2
+  double tol2;        // stop when rdotr <= tol2 (mixed: when the FP64 residual r.r <= tol2)
   double rdotr0;
+  double rtrue2;      // mixed: r.r of the FP64 residual b - A x at the last replacement
+  double rmax2;       // mixed: the same, the reference level for the next replacement
   int iter;           // completed iterations
-  int done;           // 1 once converged, at maxit, or broken down
+  int done;           // 1 once converged, at maxit, broken down, or (mixed) a replacement is due
   int maxit;
   int breakdown;
   int precon;
-  int pad;
+  int mixed;          // 1 in a mixed-precision solve
+  int skip_x;         // 1: the last iteration's x update has been applied already
+  int update;         // mixed: 1 asks the host for a reliable update
 };
 
 // Where an element-operator launch inside CG leaves p.Ap.  Because

@@ -148,6 +148,8 @@ void add_common(Settings& S, bool bp) {
   S.add("-v", "--verbose", "VERBOSE", "FALSE", "Enable verbose output", {"TRUE", "FALSE"});
   // extensions
   S.add("-pc", "--precon", "PRECONDITIONER", "NONE", "CG preconditioner (extension)", {"NONE", "JACOBI"});
+  S.add("-fp", "--precision", "PRECISION", "FP64",
+        "FP64, or MIXED: FP32 CG with FP64 reliable updates, needs -tol (extension)", {"FP64", "MIXED"});
   S.add("-f", "--forcing", "FORCING", "ANALYTIC",
         "Right-hand side: analytic sin forcing, or f=2u-1 per gathered node from the seeded LCG (extension)",
         {"ANALYTIC", "RANDOM"});
@@ -202,6 +204,7 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
   sd.bp = bp;
   sd.lambda = 1.0;   // BP/BP5/bp5Main.cpp:47
   sd.precon = S.compare("PRECONDITIONER", "JACOBI") ? BP_PRECON_JACOBI : BP_PRECON_NONE;
+  sd.precision = S.compare("PRECISION", "MIXED") ? BP_PRECISION_MIXED : BP_PRECISION_FP64;
   check(bp_solver_create(P.mesh, &sd, &P.solver));
 }
 
@@ -241,7 +244,8 @@ int run_bp(const char* name, int bp, Settings& S) {
   // warmup solve (bp5Run.cpp:66-69)
   check(bp_linalg_set(N, 0.0, x.p, nullptr));
   check(bp_memcpy_dtod(r.p, b.p, sizeof(double) * N, nullptr));
-  check(bp_solver_solve(P.solver, x.p, r.p, 0.0, warmIter, nullptr, nullptr, &st));
+  const bool mixed = S.compare("PRECISION", "MIXED");
+  check(bp_solver_solve(P.solver, x.p, r.p, mixed ? 1e-30 : 0.0, warmIter, nullptr, nullptr, &st));
   // timed solve (bp5Run.cpp:71-95)
   check(bp_linalg_set(N, 0.0, x.p, nullptr));
   check(bp_memcpy_dtod(r.p, b.p, sizeof(double) * N, nullptr));
@@ -270,8 +274,10 @@ int run_bp(const char* name, int bp, Settings& S) {
       name, P.view.N, Ndofs, elapsed, Niter, elapsed / Ndofs, Nbytes / (1.0e9 * elapsed), Nflops / (1.0e9 * elapsed),
       Ndofs * ((double)Niter / (1 * elapsed)), suffix.c_str());
   const double rel = std::sqrt(st.rdotr / (st.rdotr0 > 0 ? st.rdotr0 : 1.0));
-  std::printf("%s extra: precon=%s, forcing=%s, final r norm=%.6e, relative residual=%.6e, device ms=%.4f\n", name,
-              S.get("PRECONDITIONER").c_str(), S.get("FORCING").c_str(), std::sqrt(st.rdotr), rel, st.elapsed_ms);
+  std::printf("%s extra: precision=%s, precon=%s, forcing=%s, final r norm=%.6e, relative residual=%.6e, "
+              "reliable updates=%d, device ms=%.4f\n",
+              name, S.get("PRECISION").c_str(), S.get("PRECONDITIONER").c_str(), S.get("FORCING").c_str(),
+              std::sqrt(st.rdotr), rel, st.updates, st.elapsed_ms);
   std::fflush(stdout);
   return BP_SUCCESS;
 }

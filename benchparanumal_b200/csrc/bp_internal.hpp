@@ -109,6 +109,10 @@ int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elem
                    const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
                    const double* q, double* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse = nullptr,
                    int* nblocks = nullptr);
+int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
+                   const float* q, float* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse = nullptr,
+                   int* nblocks = nullptr);
 int launch_ax(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
               const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
               const double* q, double* Aq, cudaStream_t s);
@@ -143,6 +147,9 @@ int reduction_blocks();
 // configuration is not covered and nothing was launched
 int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const double* wJ, const double* ggeo, const double* D, double lambda, const double* q, double* Aq,
+                  const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                  const float* wJ, const float* ggeo, const float* D, float lambda, const float* q, float* Aq,
                   const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();

@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <string>
+#include <type_traits>
 
 #include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
@@ -43,23 +44,25 @@ struct AxShape {
   static constexpr int MINB = NQ <= 8 ? 2 : 1; // resident blocks per SM the register budget must allow
 };
 
-template <int NQ, int NF, bool AFFINE, bool VEC, bool DOT>
+template <int NQ, int NF, bool AFFINE, bool VEC, bool DOT, class F>
 __global__ void __launch_bounds__(NQ * NQ * AxShape<NQ>::EPB, AxShape<NQ>::MINB)
 ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
-                 const double* __restrict__ wJ, const double* __restrict__ ggeo,
-                 const double* __restrict__ gllw, const double* __restrict__ Dg, double lambda,
-                 const double* __restrict__ q, double* __restrict__ Aq, const int* __restrict__ skip,
-                 CgFuse fuse) {
+                 const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ gllw,
+                 const F* __restrict__ Dg, F lambda, const F* __restrict__ q, F* __restrict__ Aq,
+                 const int* __restrict__ skip, CgFuse fuse) {
   if (skip && *skip) return;
+  using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
   constexpr int EPB = AxShape<NQ>::EPB;
   constexpr int NP = NQ * NQ * NQ;
   constexpr int NQ2 = NQ * NQ;
   constexpr int PAD = (NQ % 2 == 0) ? 1 : 0;
-  __shared__ double s_D[NQ][NQ + 1];
-  __shared__ double s_gw[NQ];
-  __shared__ double s_q[EPB][NQ][NQ + PAD];
-  __shared__ double s_v[EPB][NQ][NQ + PAD];
-  __shared__ double s_w[EPB][NQ][NQ + PAD];
+  __shared__ F s_D[NQ][NQ + 1];
+  __shared__ F s_gw[NQ];
+  __shared__ F s_q[EPB][NQ][NQ + PAD];
+  __shared__ F s_v[EPB][NQ][NQ + PAD];
+  __shared__ F s_w[EPB][NQ][NQ + PAD];
+  // one double per thread for the p.Ap block sum (DOT)
+  __shared__ double s_red[DOT ? NQ * NQ * EPB : 1];
 
   const int i = threadIdx.x, j = threadIdx.y, es = threadIdx.z;
   const int t = i + NQ * (j + NQ * es);
@@ -71,7 +74,7 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
   const int e = active ? elementList[eIdx] : 0;
   __syncthreads();
 
-  double Di[AxShape<NQ>::DREG ? NQ : 1], Dj[AxShape<NQ>::DREG ? NQ : 1];
+  F Di[AxShape<NQ>::DREG ? NQ : 1], Dj[AxShape<NQ>::DREG ? NQ : 1];
   if (AxShape<NQ>::DREG) {
 #pragma unroll
     for (int m = 0; m < NQ; ++m) {
@@ -80,7 +83,7 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
     }
   }
 
-  double aG[6] = {0, 0, 0, 0, 0, 0}, aJ = 0.0, wij = 0.0;
+  F aG[6] = {0, 0, 0, 0, 0, 0}, aJ = 0, wij = 0;
   if (AFFINE) {
     if (active) {
 #pragma unroll
@@ -95,71 +98,60 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
   for (int f = 0; f < NF; ++f) {
     const size_t lbase = ((size_t)e * NF + f) * NP + j * NQ + i;
     const size_t gbase = (size_t)e * NP + j * NQ + i;
-    double r_u[NQ], r_Au[NQ];
+    F r_u[NQ], r_Au[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
       const int id = active ? __ldg(G2L + lbase + k * NQ2) : -1;
-      r_u[k] = (id >= 0) ? __ldg(q + id) : 0.0;
-      r_Au[k] = 0.0;
+      r_u[k] = (id >= 0) ? __ldg(q + id) : F(0);
+      r_Au[k] = F(0);
     }
 
     // prefetch slice 0 of the geometric factors
-    double n00 = 0, n01 = 0, n02 = 0, n11 = 0, n12 = 0, n22 = 0, nJ = 0;
-    if (!AFFINE && active) {
+    F n00 = 0, n01 = 0, n02 = 0, n11 = 0, n12 = 0, n22 = 0, nJ = 0;
+    auto load_factors = [&](size_t gb) {
       if (VEC) {
-        const double2* g2 = reinterpret_cast<const double2*>(ggeo + 6 * gbase);
-        const double2 a = __ldg(g2), b = __ldg(g2 + 1), c = __ldg(g2 + 2);
+        const V2* g2 = reinterpret_cast<const V2*>(ggeo + 6 * gb);
+        const V2 a = g2[0], b = g2[1], c = g2[2];
         n00 = a.x; n01 = a.y; n02 = b.x; n11 = b.y; n12 = c.x; n22 = c.y;
       } else {
-        const double* g = ggeo + 6 * gbase;
+        const F* g = ggeo + 6 * gb;
         n00 = __ldg(g); n01 = __ldg(g + 1); n02 = __ldg(g + 2);
         n11 = __ldg(g + 3); n12 = __ldg(g + 4); n22 = __ldg(g + 5);
       }
-      nJ = __ldg(wJ + gbase);
-    }
+      nJ = __ldg(wJ + gb);
+    };
+    if (!AFFINE && active) load_factors(gbase);
 
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
-      double G00, G01, G02, G11, G12, G22, GwJ;
+      F G00, G01, G02, G11, G12, G22, GwJ;
       if (AFFINE) {
-        const double w = wij * s_gw[k];
+        const F w = wij * s_gw[k];
         G00 = aG[0] * w; G01 = aG[1] * w; G02 = aG[2] * w;
         G11 = aG[3] * w; G12 = aG[4] * w; G22 = aG[5] * w;
         GwJ = aJ * w;
       } else {
         G00 = n00; G01 = n01; G02 = n02; G11 = n11; G12 = n12; G22 = n22; GwJ = nJ;
-        if (k + 1 < NQ && active) {
-          const size_t gb = gbase + (size_t)(k + 1) * NQ2;
-          if (VEC) {
-            const double2* g2 = reinterpret_cast<const double2*>(ggeo + 6 * gb);
-            const double2 a = __ldg(g2), b = __ldg(g2 + 1), c = __ldg(g2 + 2);
-            n00 = a.x; n01 = a.y; n02 = b.x; n11 = b.y; n12 = c.x; n22 = c.y;
-          } else {
-            const double* g = ggeo + 6 * gb;
-            n00 = __ldg(g); n01 = __ldg(g + 1); n02 = __ldg(g + 2);
-            n11 = __ldg(g + 3); n12 = __ldg(g + 4); n22 = __ldg(g + 5);
-          }
-          nJ = __ldg(wJ + gb);
-        }
+        if (k + 1 < NQ && active) load_factors(gbase + (size_t)(k + 1) * NQ2);
       }
 
       s_q[es][j][i] = r_u[k];
       __syncthreads();
 
-      double ur = 0.0, us = 0.0, ut = 0.0;
+      F ur = 0, us = 0, ut = 0;
 #pragma unroll
       for (int m = 0; m < NQ; ++m) ut += s_D[k][m] * r_u[m];
 #pragma unroll
       for (int m = 0; m < NQ; ++m) {
-        const double dim = AxShape<NQ>::DREG ? Di[m] : s_D[i][m];
-        const double djm = AxShape<NQ>::DREG ? Dj[m] : s_D[j][m];
+        const F dim = AxShape<NQ>::DREG ? Di[m] : s_D[i][m];
+        const F djm = AxShape<NQ>::DREG ? Dj[m] : s_D[j][m];
         ur += dim * s_q[es][j][m];
         us += djm * s_q[es][m][i];
       }
       s_w[es][j][i] = G01 * ur + G11 * us + G12 * ut;
       s_v[es][j][i] = G00 * ur + G01 * us + G02 * ut;
-      const double GDut = G02 * ur + G12 * us + G22 * ut;
-      double Auk = GwJ * lambda * r_u[k];
+      const F GDut = G02 * ur + G12 * us + G22 * ut;
+      F Auk = GwJ * lambda * r_u[k];
       __syncthreads();
 
 #pragma unroll
@@ -176,11 +168,11 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
       for (int k = 0; k < NQ; ++k) Aq[lbase + k * NQ2] = r_Au[k];
       if (DOT) {
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) pdot += r_u[k] * r_Au[k];
+        for (int k = 0; k < NQ; ++k) pdot += (double)r_u[k] * (double)r_Au[k];
       }
     }
   }
-  if (DOT) fuse_pap(pdot, fuse, &s_q[0][0][0]);   // s_q holds one double per thread
+  if (DOT) fuse_pap(pdot, fuse, s_red);
 }
 
 // Kernel variant of the stored-factor operator: the TMA-staged kernel where it
@@ -196,11 +188,10 @@ static int ax_variant() {
   return v;
 }
 
-template <int NQ>
+template <int NQ, class F>
 static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
-                        const int32_t* G2L, const double* wJ, const double* ggeo, const double* gllw,
-                        const double* D, double lambda, const double* q, double* Aq, const int* skip,
-                        const CgFuse* fuse, cudaStream_t s, int* nblocks) {
+                        const int32_t* G2L, const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda,
+                        const F* q, F* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   constexpr int EPB = AxShape<NQ>::EPB;
   if (!d.affine && ax_variant() != AX_PENCIL) {
     const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
@@ -209,13 +200,13 @@ static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t*
   const dim3 block(NQ, NQ, EPB);
   const dim3 grid((Nelements + EPB - 1) / EPB);
   if (nblocks) *nblocks = (int)grid.x;
-  const bool vec = ((reinterpret_cast<uintptr_t>(ggeo) & 15) == 0);
-  const CgFuse F = fuse ? *fuse : CgFuse{};
-#define BP_PENCIL(NF, AFF, VEC, DOT) \
-  ax_pencil_kernel<NQ, NF, AFF, VEC, DOT><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, \
-                                                                 lambda, q, Aq, skip, F)
+  const bool vec = ((reinterpret_cast<uintptr_t>(ggeo) & (2 * sizeof(F) - 1)) == 0);
+  const CgFuse Fz = fuse ? *fuse : CgFuse{};
+#define BP_PENCIL(NF, AFF, VEC, DOT)                                                                          \
+  ax_pencil_kernel<NQ, NF, AFF, VEC, DOT, F><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, \
+                                                                    lambda, q, Aq, skip, Fz)
   if (fuse) {
-    if (!d.affine && !vec) return fail(BP_ERROR_ARG, "CG operator needs 16-byte aligned geometric factors");
+    if (!d.affine && !vec) return fail(BP_ERROR_ARG, "CG operator needs aligned geometric factors");
     if (d.Nfields == 1) {
       if (d.affine) BP_PENCIL(1, true, true, true); else BP_PENCIL(1, false, true, true);
     } else {
@@ -235,16 +226,16 @@ static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t*
   return BP_SUCCESS;
 }
 
-int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
-                   const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
-                   const double* q, double* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse,
-                   int* nblocks) {
+template <class F>
+static int launch_ax_t(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                       const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda, const F* q, F* Aq,
+                       const int* skip, cudaStream_t s, const CgFuse* fuse, int* nblocks) {
   if (nblocks) *nblocks = 0;
   if (Nelements == 0) return BP_SUCCESS;
   switch (d.N + 1) {
 #define BP_AX_CASE(nq) \
   case nq:             \
-    return launch_ax_nq<nq>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s, nblocks);
+    return launch_ax_nq<nq, F>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s, nblocks);
     BP_AX_CASE(2) BP_AX_CASE(3) BP_AX_CASE(4) BP_AX_CASE(5) BP_AX_CASE(6) BP_AX_CASE(7) BP_AX_CASE(8)
     BP_AX_CASE(9) BP_AX_CASE(10) BP_AX_CASE(11) BP_AX_CASE(12) BP_AX_CASE(13) BP_AX_CASE(14)
     BP_AX_CASE(15) BP_AX_CASE(16)
@@ -252,6 +243,22 @@ int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elem
     default:
       return fail(BP_ERROR_ARG, "bp_ax_hex3d: degree N must be in 1..15");
   }
+}
+
+int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
+                   const double* q, double* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse,
+                   int* nblocks) {
+  return launch_ax_t<double>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse,
+                             nblocks);
+}
+
+int launch_ax_skip(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
+                   const float* q, float* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse,
+                   int* nblocks) {
+  return launch_ax_t<float>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse,
+                            nblocks);
 }
 
 int launch_ax(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,

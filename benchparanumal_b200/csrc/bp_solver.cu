@@ -1,5 +1,5 @@
 // Benchmark problem object: operator, forcing, Jacobi diagonal and the CG
-// solve (reference: BP/BP5/src/bp5{Setup,Operator,Run}.cpp,
+// solves (reference: BP/BP5/src/bp5{Setup,Operator,Run}.cpp,
 // libs/core/linearSolverCG.cpp:62-156).
 //
 // CG runs with every scalar on the device.  One iteration is four kernels:
@@ -8,9 +8,19 @@
 //   cg_alpha_kernel         p.Ap from the partials, alpha = rho / p.Ap
 //   cg_gather_update_kernel r -= alpha Gather(AqL), r.r (and r.z), stop test
 // so A p is never stored as a gathered vector.  The reductions finish in the
-// last block to arrive, so there is no host round trip per iteration.  Iterations are captured once into a CUDA graph
-// (kChunk iterations per graph) and replayed; a finished solve turns the
-// remaining kernels into immediate returns through a device flag.
+// last block to arrive, so there is no host round trip per iteration.
+// Iterations are captured once into a CUDA graph (kChunk iterations per graph)
+// and replayed; a finished solve turns the remaining kernels into immediate
+// returns through a device flag.
+//
+// Mixed precision: the same kernels run on FP32 vectors, FP32 factors and an
+// FP32 operator (dot products accumulate in FP64).  The FP64 iterate is x_hi;
+// the FP32 recursion carries a correction x_lo and residual r_lo.  When the
+// FP32 residual has dropped by kReliableDrop since the last replacement (or
+// reaches the tolerance), the host folds x_lo into x_hi, recomputes the FP64
+// residual b - A x_hi with the FP64 operator and restarts r_lo from it while
+// keeping the search direction -- a reliable update -- so the FP32 CG keeps
+// its Krylov space and needs about as many iterations as FP64 CG.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -23,11 +33,8 @@
 namespace bp {
 
 constexpr int kThreads = 256;
-constexpr int kChunk = 20;   // iterations per captured graph (divides the usual 100 and 1000)
-
-template <int NS>
-__device__ __forceinline__ bool grid_sum_cg(const double (&v)[NS], double* partials, unsigned int* counter,
-                                            double (&tot)[NS]);
+constexpr int kChunk = 20;            // iterations per captured graph (divides the usual 100 and 1000)
+constexpr double kReliableDrop = 1e-2;
 
 __device__ __forceinline__ double warp_sum_cg(double v) {
 #pragma unroll
@@ -113,24 +120,30 @@ cg_init_kernel(int32_t N, const double* __restrict__ Ap, double* __restrict__ r,
     sc->maxit = maxit;
     sc->breakdown = 0;
     sc->precon = precon;
+    sc->mixed = 0;
+    sc->skip_x = 0;
+    sc->update = 0;
     sc->done = (rdotr <= sc->tol2 || maxit <= 0) ? 1 : 0;
   }
 }
 
-// x += alpha p (the previous iteration's update, deferred), p = z + beta p
+// x += alpha p (the previous iteration's update, deferred unless a reliable
+// update has applied it already), p = z + beta p
+template <class V>
 __global__ void __launch_bounds__(kThreads)
-cg_direction_kernel(int32_t N, double* __restrict__ x, double* __restrict__ p, const double* __restrict__ r,
-                    const double* __restrict__ invD, const CgScalars* __restrict__ sc) {
+cg_direction_kernel(int32_t N, V* __restrict__ x, V* __restrict__ p, const V* __restrict__ r,
+                    const V* __restrict__ invD, const CgScalars* __restrict__ sc) {
   if (sc->done) return;
   const int iter = sc->iter;
-  const double alpha = sc->alpha;
-  double beta = 0.0;
-  if (iter > 0) beta = sc->precon ? sc->rz / sc->rz_prev : sc->rdotr / sc->rdotr_prev;
+  const bool addx = iter > 0 && !sc->skip_x;
+  const V alpha = (V)sc->alpha;
+  V beta = 0;
+  if (iter > 0) beta = (V)(sc->precon ? sc->rz / sc->rz_prev : sc->rdotr / sc->rdotr_prev);
   const bool precon = sc->precon != 0;
   for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
-    const double pn = p[n];
-    if (iter > 0) x[n] = alpha * pn + 1.0 * x[n];
-    const double z = precon ? invD[n] * r[n] : 1.0 * r[n];
+    const V pn = p[n];
+    if (addx) x[n] = alpha * pn + V(1) * x[n];
+    const V z = precon ? invD[n] * r[n] : V(1) * r[n];
     p[n] = (iter > 0) ? z + beta * pn : z;   // p is not read at iteration 0
   }
 }
@@ -162,29 +175,29 @@ cg_alpha_kernel(int nparts, const double* __restrict__ parts, CgScalars* sc, dou
   }
 }
 
-// r -= alpha Gather(AqL); r.r (and r.z); stop test.  alpha comes from the
-// element operator's p.Ap epilogue.
 // One row per thread: r and invD of the row are requested first, then the
 // row's local values in column order (the reference's order, so the sums match
-// its gather bit for bit).
+// its gather bit for bit).  r -= alpha Gather(AqL); r.r (and r.z); stop test.
+// In a mixed solve the test also asks the host for a reliable update.
+template <class V>
 __global__ void __launch_bounds__(kThreads)
 cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const int32_t* __restrict__ colIds,
-                        const double* __restrict__ AqL, double* __restrict__ r, const double* __restrict__ invD,
-                        CgScalars* sc, double* hist_rnorm, double* partials, unsigned int* counter) {
+                        const V* __restrict__ AqL, V* __restrict__ r, const V* __restrict__ invD, CgScalars* sc,
+                        double* hist_rnorm, double* partials, unsigned int* counter) {
   if (sc->done) return;
-  const double alpha = sc->alpha;
+  const V alpha = (V)sc->alpha;
   const bool precon = sc->precon != 0;
   double acc[2] = {0.0, 0.0};
   for (int32_t row = blockIdx.x * kThreads + threadIdx.x; row < Nrows; row += kThreads * gridDim.x) {
-    const double rold = r[row];
-    const double dinv = precon ? __ldg(invD + row) : 0.0;
+    const V rold = r[row];
+    const V dinv = precon ? __ldg(invD + row) : V(0);
     const int32_t start = __ldg(rowStarts + row), end = __ldg(rowStarts + row + 1);
-    double s = 0.0;
+    V s = 0;
     for (int32_t c = start; c < end; ++c) s += __ldg(AqL + __ldg(colIds + c));
-    const double rn = rold - alpha * s;
+    const V rn = rold - alpha * s;
     r[row] = rn;
-    acc[0] += rn * rn;
-    if (precon) acc[1] += rn * dinv * rn;
+    acc[0] += (double)rn * (double)rn;
+    if (precon) acc[1] += (double)rn * (double)dinv * (double)rn;
   }
   double tot[2];
   if (grid_sum_cg<2>(acc, partials, counter, tot) && threadIdx.x == 0) {
@@ -196,9 +209,15 @@ cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, co
     }
     if (hist_rnorm) hist_rnorm[sc->iter] = sqrt(tot[0]);
     sc->iter += 1;
+    sc->skip_x = 0;
     if (!isfinite(tot[0])) {
       sc->breakdown = 1;
       sc->done = 1;
+    } else if (sc->mixed) {
+      if (tot[0] <= sc->tol2 || tot[0] < kReliableDrop * kReliableDrop * sc->rmax2 || sc->iter >= sc->maxit) {
+        sc->update = 1;
+        sc->done = 1;
+      }
     } else if (tot[0] <= sc->tol2 || sc->iter >= sc->maxit) {
       sc->done = 1;
     }
@@ -206,12 +225,70 @@ cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, co
 }
 
 // apply the last completed iteration's x update
+template <class V>
 __global__ void __launch_bounds__(kThreads)
-cg_final_kernel(int32_t N, double* __restrict__ x, const double* __restrict__ p, const CgScalars* __restrict__ sc) {
-  if (sc->iter == 0 || sc->breakdown) return;
-  const double alpha = sc->alpha;
+cg_final_kernel(int32_t N, V* __restrict__ x, const V* __restrict__ p, const CgScalars* __restrict__ sc) {
+  if (sc->iter == 0 || sc->breakdown || sc->skip_x) return;
+  const V alpha = (V)sc->alpha;
   for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x)
-    x[n] = alpha * p[n] + 1.0 * x[n];
+    x[n] = alpha * p[n] + V(1) * x[n];
+}
+
+// mixed: x_hi += x_lo, x_lo = 0
+__global__ void __launch_bounds__(kThreads)
+mixed_fold_kernel(int32_t N, double* __restrict__ x_hi, float* __restrict__ x_lo) {
+  for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
+    x_hi[n] += (double)x_lo[n];
+    x_lo[n] = 0.0f;
+  }
+}
+
+// mixed: r_hi = b - Ax_hi (FP64), r_lo = (float) r_hi, and the norms that
+// restart the FP32 recursion.  init != 0: first call of a solve.
+__global__ void __launch_bounds__(kThreads)
+mixed_replace_kernel(int32_t N, const double* __restrict__ b, const double* __restrict__ Ax, double* __restrict__ r_hi,
+                     float* __restrict__ r_lo, const float* __restrict__ invD, CgScalars* sc, int init, double tol,
+                     int maxit, int precon, double* partials, unsigned int* counter) {
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
+    const double rn = b[n] - Ax[n];
+    r_hi[n] = rn;
+    const float rl = (float)rn;
+    r_lo[n] = rl;
+    acc[0] += rn * rn;
+    acc[1] += (double)rl * (double)rl;
+    if (precon) acc[2] += (double)rl * (double)invD[n] * (double)rl;
+  }
+  double tot[3];
+  if (grid_sum_cg<3>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    sc->rtrue2 = tot[0];
+    sc->rmax2 = tot[0];
+    sc->rdotr = tot[1];
+    sc->rz = precon ? tot[2] : tot[1];
+    if (init) {
+      sc->rdotr0 = tot[0];
+      sc->tol2 = tol * tol * tot[0];
+      sc->rdotr_prev = tot[1];
+      sc->rz_prev = sc->rz;
+      sc->pAp = 0.0;
+      sc->alpha = 0.0;
+      sc->iter = 0;
+      sc->maxit = maxit;
+      sc->breakdown = 0;
+      sc->precon = precon;
+      sc->mixed = 1;
+      sc->skip_x = 0;
+    } else {
+      sc->skip_x = 1;   // x_lo += alpha p of the last iteration is already folded in
+    }
+    sc->update = 0;
+    sc->done = (tot[0] <= sc->tol2 || sc->iter >= sc->maxit) ? 1 : 0;
+  }
+}
+
+__global__ void d2f_kernel(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
 }
 
 static int vec_grid(int32_t N) {
@@ -219,6 +296,15 @@ static int vec_grid(int32_t N) {
   const int cap = reduction_blocks();
   if (g > cap) g = cap;
   return g < 1 ? 1 : g;
+}
+
+static int to_float(const double* a, float* b, size_t n, cudaStream_t s) {
+  if (n == 0) return BP_SUCCESS;
+  size_t g = (n + 255) / 256;
+  if (g > 8192) g = 8192;
+  d2f_kernel<<<(unsigned)g, 256, 0, s>>>(n, a, b);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
 }
 
 }  // namespace bp
@@ -230,9 +316,12 @@ struct bp_solver_s {
   int bp = 5;
   double lambda = 1.0;
   int precon = 0;
+  int mixed = 0;
   int32_t N = 0;               // Ngather
   bp_ax_desc_t ax{};
-  DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist, fuse_partials;
+  DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist, fuse_partials, bcopy;
+  // FP32 data of the mixed-precision solve
+  DeviceArray<float> wJ32, ggeo32, D32, gllw32, invD32, AqL32, p32, x32, r32;
   DeviceArray<unsigned int> counter;
   DeviceArray<CgScalars> sc;
   int hist_len = 0;
@@ -240,9 +329,11 @@ struct bp_solver_s {
   cudaGraphExec_t graph = nullptr;
   const double* g_x = nullptr;
   const double* g_r = nullptr;
+  cudaGraphExec_t graph32 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~bp_solver_s() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph32) cudaGraphExecDestroy(graph32);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
@@ -257,43 +348,62 @@ static int operator_apply(bp_solver_s* S, const double* q, double* Aq, const int
   return launch_gather(m->Ngather, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, Aq, s);
 }
 
-// enqueue one CG iteration
-static int enqueue_iteration(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
+// enqueue one CG iteration on vectors of type V (FP64, or FP32 in a mixed solve)
+template <class V>
+static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* invD, const V* wJ, const V* ggeo,
+                             const V* gllw, const V* D, cudaStream_t s) {
   bp_mesh_s* m = S->mesh;
   const int32_t N = S->N;
   const int g = vec_grid(N);
   double* hist_alpha = S->hist.ptr;
   double* hist_rnorm = S->hist.ptr ? S->hist.ptr + S->hist_len : nullptr;
-  cg_direction_kernel<<<g, kThreads, 0, s>>>(N, x, S->p.ptr, r, S->invD.ptr, S->sc.ptr);
+  cg_direction_kernel<V><<<g, kThreads, 0, s>>>(N, x, p, r, invD, S->sc.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   const CgFuse fuse{S->fuse_partials.ptr};
   int nparts = 0;
-  BP_TRY(launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, m->wJ.ptr, m->ggeo.ptr, m->gllw.ptr, m->D.ptr,
-                        S->lambda, S->p.ptr, S->AqL.ptr, &S->sc.ptr->done, s, &fuse, &nparts));
+  BP_TRY(launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, wJ, ggeo, gllw, D, (V)S->lambda, p, AqL,
+                        &S->sc.ptr->done, s, &fuse, &nparts));
   cg_alpha_kernel<<<1, kAlphaThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->sc.ptr, hist_alpha);
   BP_CUDA_TRY(cudaGetLastError());
-  cg_gather_update_kernel<<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, r, S->invD.ptr,
-                                                 S->sc.ptr, hist_rnorm, S->partials.ptr, S->counter.ptr);
+  cg_gather_update_kernel<V><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, AqL, r, invD, S->sc.ptr,
+                                                    hist_rnorm, S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
-static int ensure_graph(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
-  if (S->graph && S->g_x == x && S->g_r == r) return BP_SUCCESS;
-  if (S->graph) {
-    cudaGraphExecDestroy(S->graph);
-    S->graph = nullptr;
+static int capture(cudaGraphExec_t* out, cudaStream_t s, int (*body)(bp_solver_s*, void*, void*, cudaStream_t),
+                   bp_solver_s* S, void* a, void* b) {
+  if (*out) {
+    cudaGraphExecDestroy(*out);
+    *out = nullptr;
   }
   cudaGraph_t g;
   BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int rc = BP_SUCCESS;
-  for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k) rc = enqueue_iteration(S, x, r, s);
+  for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k) rc = body(S, a, b, s);
   cudaError_t ce = cudaStreamEndCapture(s, &g);
   if (rc != BP_SUCCESS) return rc;
   BP_CUDA_TRY(ce);
-  ce = cudaGraphInstantiate(&S->graph, g, 0);
+  ce = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   BP_CUDA_TRY(ce);
+  return BP_SUCCESS;
+}
+
+static int body64(bp_solver_s* S, void* x, void* r, cudaStream_t s) {
+  bp_mesh_s* m = S->mesh;
+  return enqueue_iteration<double>(S, (double*)x, (double*)r, S->p.ptr, S->AqL.ptr, S->invD.ptr, m->wJ.ptr,
+                                   m->ggeo.ptr, m->gllw.ptr, m->D.ptr, s);
+}
+
+static int body32(bp_solver_s* S, void*, void*, cudaStream_t s) {
+  return enqueue_iteration<float>(S, S->x32.ptr, S->r32.ptr, S->p32.ptr, S->AqL32.ptr, S->invD32.ptr, S->wJ32.ptr,
+                                  S->ggeo32.ptr, S->gllw32.ptr, S->D32.ptr, s);
+}
+
+static int ensure_graph(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
+  if (S->graph && S->g_x == x && S->g_r == r) return BP_SUCCESS;
+  BP_TRY(capture(&S->graph, s, body64, S, x, r));
   S->g_x = x;
   S->g_r = r;
   return BP_SUCCESS;
@@ -301,10 +411,14 @@ static int ensure_graph(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
 
 static int ensure_hist(bp_solver_s* S, int maxit) {
   if (maxit <= S->hist_len) return BP_SUCCESS;
-  // history buffers move: the captured graph refers to them
+  // history buffers move: the captured graphs refer to them
   if (S->graph) {
     cudaGraphExecDestroy(S->graph);
     S->graph = nullptr;
+  }
+  if (S->graph32) {
+    cudaGraphExecDestroy(S->graph32);
+    S->graph32 = nullptr;
   }
   const int len = std::max(maxit, 128);
   BP_TRY(S->hist.alloc((size_t)2 * len));
@@ -312,8 +426,38 @@ static int ensure_hist(bp_solver_s* S, int maxit) {
   return BP_SUCCESS;
 }
 
-static int solve_device(bp_solver_s* S, double* x, double* r, double tol, int maxit, double* hist_rnorm,
-                        double* hist_alpha, bp_solve_stats_t* stats, cudaStream_t s, bool record_events) {
+static int read_scalars(bp_solver_s* S, CgScalars& h, cudaStream_t s) {
+  BP_CUDA_TRY(cudaMemcpyAsync(&h, S->sc.ptr, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  return BP_SUCCESS;
+}
+
+static int finish_solve(bp_solver_s* S, const CgScalars& h, double* hist_rnorm, double* hist_alpha,
+                        bp_solve_stats_t* stats, bool record_events, int updates) {
+  const int it = h.iter;
+  if (hist_alpha && it > 0)
+    BP_CUDA_TRY(cudaMemcpy(hist_alpha, S->hist.ptr, sizeof(double) * it, cudaMemcpyDeviceToHost));
+  if (hist_rnorm && it > 0)
+    BP_CUDA_TRY(cudaMemcpy(hist_rnorm, S->hist.ptr + S->hist_len, sizeof(double) * it, cudaMemcpyDeviceToHost));
+  if (stats) {
+    stats->iterations = it;
+    stats->rdotr0 = h.rdotr0;
+    stats->rdotr = S->mixed ? h.rtrue2 : h.rdotr;
+    stats->updates = updates;
+    stats->elapsed_ms = 0.0;
+    if (record_events) {
+      float ms = 0.f;
+      BP_CUDA_TRY(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+      stats->elapsed_ms = ms;
+    }
+  }
+  BP_TRY(check_device_error());
+  if (h.breakdown) return fail(BP_ERROR_NUMERIC, "bp_solver_solve: CG breakdown (p.Ap <= 0 or non-finite residual)");
+  return BP_SUCCESS;
+}
+
+static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxit, double* hist_rnorm,
+                      double* hist_alpha, bp_solve_stats_t* stats, cudaStream_t s, bool record_events) {
   const int32_t N = S->N;
   BP_TRY(ensure_hist(S, maxit));
   BP_TRY(ensure_graph(S, x, r, s));
@@ -328,35 +472,65 @@ static int solve_device(bp_solver_s* S, double* x, double* r, double tol, int ma
   for (int c = 0; c < nchunks; ++c) {
     BP_CUDA_TRY(cudaGraphLaunch(S->graph, s));
     if (tol > 0.0 && c + 1 < nchunks) {
-      BP_CUDA_TRY(cudaMemcpyAsync(&h, S->sc.ptr, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
-      BP_CUDA_TRY(cudaStreamSynchronize(s));
+      BP_TRY(read_scalars(S, h, s));
       if (h.done) break;
     }
   }
-  cg_final_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->sc.ptr);
+  cg_final_kernel<double><<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->sc.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev1, s));
-  BP_CUDA_TRY(cudaMemcpyAsync(&h, S->sc.ptr, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
-  BP_CUDA_TRY(cudaStreamSynchronize(s));
-  const int it = h.iter;
-  if (hist_alpha && it > 0)
-    BP_CUDA_TRY(cudaMemcpy(hist_alpha, S->hist.ptr, sizeof(double) * it, cudaMemcpyDeviceToHost));
-  if (hist_rnorm && it > 0)
-    BP_CUDA_TRY(cudaMemcpy(hist_rnorm, S->hist.ptr + S->hist_len, sizeof(double) * it, cudaMemcpyDeviceToHost));
-  if (stats) {
-    stats->iterations = it;
-    stats->rdotr0 = h.rdotr0;
-    stats->rdotr = h.rdotr;
-    stats->elapsed_ms = 0.0;
-    if (record_events) {
-      float ms = 0.f;
-      BP_CUDA_TRY(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
-      stats->elapsed_ms = ms;
-    }
-  }
-  BP_TRY(check_device_error());
-  if (h.breakdown) return fail(BP_ERROR_NUMERIC, "bp_solver_solve: CG breakdown (p.Ap <= 0 or non-finite residual)");
+  BP_TRY(read_scalars(S, h, s));
+  return finish_solve(S, h, hist_rnorm, hist_alpha, stats, record_events, 0);
+}
+
+// FP64 residual r_hi = b - A x_hi and the FP32 restart (init: start of a solve)
+static int mixed_replace(bp_solver_s* S, double* x, double* r, bool init, double tol, int maxit, cudaStream_t s) {
+  const int32_t N = S->N;
+  BP_TRY(operator_apply(S, x, S->Ap.ptr, nullptr, s));
+  mixed_replace_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, S->bcopy.ptr, S->Ap.ptr, r, S->r32.ptr, S->invD32.ptr,
+                                                        S->sc.ptr, init ? 1 : 0, tol, maxit, S->precon,
+                                                        S->partials.ptr, S->counter.ptr);
+  BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
+}
+
+static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int maxit, double* hist_rnorm,
+                       double* hist_alpha, bp_solve_stats_t* stats, cudaStream_t s, bool record_events) {
+  const int32_t N = S->N;
+  if (!(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_solver_solve: a mixed-precision solve needs tol > 0");
+  BP_TRY(ensure_hist(S, maxit));
+  if (!S->graph32) BP_TRY(capture(&S->graph32, s, body32, S, nullptr, nullptr));
+  if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
+  BP_CUDA_TRY(cudaMemcpyAsync(S->bcopy.ptr, r, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  BP_CUDA_TRY(cudaMemsetAsync(S->x32.ptr, 0, sizeof(float) * N, s));
+  BP_TRY(mixed_replace(S, x, r, true, tol, maxit, s));
+  CgScalars h{};
+  BP_TRY(read_scalars(S, h, s));
+  int updates = 0;
+  while (!h.done || h.update) {
+    if (h.update) {
+      // reliable update: fold the pending x_lo step, x_hi += x_lo, FP64 residual
+      cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, S->x32.ptr, S->p32.ptr, S->sc.ptr);
+      BP_CUDA_TRY(cudaGetLastError());
+      mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, x, S->x32.ptr);
+      BP_CUDA_TRY(cudaGetLastError());
+      BP_TRY(mixed_replace(S, x, r, false, tol, maxit, s));
+      ++updates;
+    } else {
+      BP_CUDA_TRY(cudaGraphLaunch(S->graph32, s));
+    }
+    BP_TRY(read_scalars(S, h, s));
+    if (h.breakdown) break;
+  }
+  if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev1, s));
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  return finish_solve(S, h, hist_rnorm, hist_alpha, stats, record_events, updates);
+}
+
+static int solve_device(bp_solver_s* S, double* x, double* r, double tol, int maxit, double* hist_rnorm,
+                        double* hist_alpha, bp_solve_stats_t* stats, cudaStream_t s, bool record_events) {
+  if (S->mixed) return solve_mixed(S, x, r, tol, maxit, hist_rnorm, hist_alpha, stats, s, record_events);
+  return solve_fp64(S, x, r, tol, maxit, hist_rnorm, hist_alpha, stats, s, record_events);
 }
 
 }  // namespace bp
@@ -371,12 +545,15 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
     return fail(BP_ERROR_ARG, "bp_solver_create: BP6 needs a 3-field mesh, BP5 a 1-field mesh");
   if (d->precon != BP_PRECON_NONE && d->precon != BP_PRECON_JACOBI)
     return fail(BP_ERROR_ARG, "bp_solver_create: unknown preconditioner");
+  if (d->precision != BP_PRECISION_FP64 && d->precision != BP_PRECISION_MIXED)
+    return fail(BP_ERROR_ARG, "bp_solver_create: unknown precision");
   cudaStream_t s = default_stream();
   bp_solver_s* S = new bp_solver_s();
   S->mesh = mesh;
   S->bp = d->bp;
   S->lambda = d->lambda;
   S->precon = d->precon;
+  S->mixed = d->precision == BP_PRECISION_MIXED;
   S->N = mesh->Ngather;
   S->ax.bp = d->bp;
   S->ax.N = mesh->N;
@@ -404,6 +581,29 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
       if ((rc = S->invD.alloc(S->N))) break;
       if ((rc = bp_solver_diagonal(S, S->invD.ptr))) break;
       if ((rc = launch_reciprocal(S->N, S->invD.ptr, s))) break;
+    }
+    if (S->mixed) {
+      // FP32 copies of the stored factors and the 1D operators, FP32 CG vectors
+      const size_t ng = mesh->wJ.n;
+      if ((rc = S->wJ32.alloc(ng))) break;
+      if ((rc = S->ggeo32.alloc(6 * ng))) break;
+      if ((rc = S->D32.alloc(mesh->D.n))) break;
+      if ((rc = S->gllw32.alloc(mesh->gllw.n))) break;
+      if ((rc = S->AqL32.alloc(NL))) break;
+      if ((rc = S->p32.alloc(S->N))) break;
+      if ((rc = S->x32.alloc(S->N))) break;
+      if ((rc = S->r32.alloc(S->N))) break;
+      if ((rc = S->bcopy.alloc(S->N))) break;
+      if ((rc = to_float(mesh->wJ.ptr, S->wJ32.ptr, ng, s))) break;
+      if ((rc = to_float(mesh->ggeo.ptr, S->ggeo32.ptr, 6 * ng, s))) break;
+      if ((rc = to_float(mesh->D.ptr, S->D32.ptr, mesh->D.n, s))) break;
+      if ((rc = to_float(mesh->gllw.ptr, S->gllw32.ptr, mesh->gllw.n, s))) break;
+      if (S->precon == BP_PRECON_JACOBI) {
+        if ((rc = S->invD32.alloc(S->N))) break;
+        if ((rc = to_float(S->invD.ptr, S->invD32.ptr, S->N, s))) break;
+      }
+      ce = cudaMemsetAsync(S->p32.ptr, 0, sizeof(float) * S->N, s);
+      if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_solver_create", __FILE__, __LINE__); break; }
     }
     ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_solver_create", __FILE__, __LINE__); break; }
@@ -488,21 +688,28 @@ int bp_solver_solve_host(bp_solver_t S, const double* b_host, double* x_host, do
     BP_TRY(S->rw.alloc(S->N));
   }
   const size_t bytes = sizeof(double) * S->N;
-  BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
-  BP_CUDA_TRY(cudaMemcpyAsync(S->rw.ptr, b_host, bytes, cudaMemcpyHostToDevice, s));
-  BP_CUDA_TRY(cudaMemsetAsync(S->xw.ptr, 0, bytes, s));
-  cudaEvent_t e0 = S->ev0;
-  // inner solve without its own events, then the copy back
-  BP_TRY(solve_device(S, S->xw.ptr, S->rw.ptr, tol, maxit, nullptr, nullptr, stats, s, false));
-  BP_CUDA_TRY(cudaMemcpyAsync(x_host, S->xw.ptr, bytes, cudaMemcpyDeviceToHost, s));
-  BP_CUDA_TRY(cudaEventRecord(S->ev1, s));
-  BP_CUDA_TRY(cudaEventSynchronize(S->ev1));
-  if (stats) {
+  cudaEvent_t e0, e1;
+  BP_CUDA_TRY(cudaEventCreate(&e0));
+  BP_CUDA_TRY(cudaEventCreate(&e1));
+  int rc = BP_SUCCESS;
+  do {
+    cudaError_t ce = cudaEventRecord(e0, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(S->rw.ptr, b_host, bytes, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(S->xw.ptr, 0, bytes, s);
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_solver_solve_host", __FILE__, __LINE__); break; }
+    // inner solve without its own events, then the copy back
+    if ((rc = solve_device(S, S->xw.ptr, S->rw.ptr, tol, maxit, nullptr, nullptr, stats, s, false))) break;
+    ce = cudaMemcpyAsync(x_host, S->xw.ptr, bytes, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
     float ms = 0.f;
-    BP_CUDA_TRY(cudaEventElapsedTime(&ms, e0, S->ev1));
-    stats->elapsed_ms = ms;
-  }
-  return BP_SUCCESS;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_solver_solve_host", __FILE__, __LINE__); break; }
+    if (stats) stats->elapsed_ms = ms;
+  } while (0);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }
 
 }  // extern "C"

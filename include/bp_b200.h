@@ -218,20 +218,25 @@ typedef struct bp_solver_s* bp_solver_t;
 #define BP_PRECON_NONE 0
 #define BP_PRECON_JACOBI 1
 
+#define BP_PRECISION_FP64 0    /* every operation in FP64 (the reference's dfloat)       */
+#define BP_PRECISION_MIXED 1   /* FP32 CG with FP64 reliable updates (extension)          */
+
 typedef struct bp_solver_desc {
   int32_t bp;          /* 5 (scalar) or 6 (vector, mesh Nfields must be 3)        */
   double lambda;       /* 1.0 for BP3-BP6 (BP/BP5/bp5Main.cpp:47)                   */
   int32_t precon;      /* BP_PRECON_NONE (reference) or BP_PRECON_JACOBI             */
+  int32_t precision;   /* BP_PRECISION_FP64 or BP_PRECISION_MIXED                    */
 } bp_solver_desc_t;
 
 #define BP_RHS_ANALYTIC 0   /* rhsHex3D forcing (okl/rhsHex3D.okl:29-128)         */
 #define BP_RHS_RANDOM 1     /* f = 2u-1 per gathered row (seeded LCG), b = M f     */
 
 typedef struct bp_solve_stats {
-  int32_t iterations;      /* cg::Solve return value                              */
+  int32_t iterations;      /* cg::Solve return value (mixed: FP32 iterations)      */
   double rdotr0;           /* initial r.r                                          */
-  double rdotr;            /* final r.r                                            */
+  double rdotr;            /* final r.r (mixed: of the FP64 residual b - A x)      */
   double elapsed_ms;       /* device time of the solve (CUDA events)               */
+  int32_t updates;         /* mixed: FP64 residual replacements; FP64: 0           */
 } bp_solve_stats_t;
 
 int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* desc, bp_solver_t* solver);
@@ -247,7 +252,12 @@ int bp_solver_rhs(bp_solver_t solver, int32_t mode, uint64_t seed, double* b, do
 int bp_solver_diagonal(bp_solver_t solver, double* diag);
 /* cg::Solve on device vectors: x (initial guess in, solution out) and r
    (b in, final residual out).  tol and maxit as in the reference; with the
-   Jacobi preconditioner the stop rule is ||r|| <= tol ||b||.  hist_rnorm and
+   Jacobi preconditioner the stop rule is ||r|| <= tol ||b||.  A solver made
+   with BP_PRECISION_MIXED runs the CG recursion, the operator and the stored
+   factors in FP32 and replaces the FP32 residual by the FP64 residual b - A x
+   (x accumulated in FP64) whenever the FP32 residual has dropped by 1e-2 since
+   the last replacement; it stops on the FP64 residual, ||b - A x|| <= tol ||b||
+   (tol > 0 required), and r returns that FP64 residual.  hist_rnorm and
    hist_alpha (host, length maxit, may be NULL) receive sqrt(r.r) and alpha of
    every iteration (the "-v" output).  No host synchronisation happens inside
    the iteration loop except one flag read every 20 iterations when tol > 0. */

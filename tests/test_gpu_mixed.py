@@ -1,0 +1,65 @@
+"""Mixed-precision CG (FP32 recursion and operator, FP64 reliable updates).
+
+The stop rule is on the FP64 residual, ||b - A x|| <= tol ||b||, so the
+solution must satisfy it when re-checked with the FP64 operator, and agree
+with the oracle's FP64 CG solution to the accuracy the tolerance implies.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(6, 6, 6, 7, False, 0.1, "JACOBI", 1), (8, 8, 8, 4, True, 0.0, "JACOBI", 1),
+         (5, 5, 5, 5, False, 0.1, "NONE", 1), (4, 4, 4, 6, False, 0.1, "JACOBI", 3),
+         (3, 3, 3, 9, False, 0.1, "JACOBI", 1)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,N,affine,pert,precon,Nf", CASES)
+def test_mixed_reaches_fp64_tolerance(gpu, oracle, nx, ny, nz, N, affine, pert, precon, Nf):
+    tol = 1e-8
+    om = oracle.Mesh(nx, ny, nz, N, affine=affine, pert=pert, Nfields=Nf)
+    gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, pert=pert, Nfields=Nf)
+    Sm = gpu.BP(gm, precon=precon, precision="MIXED")
+    S64 = gpu.BP(gm, precon=precon)
+    _, b_o = om.rhs_random(0)
+    x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
+    r = gpu.DeviceBuffer.from_host(b_o)
+    st, hr, ha = Sm.solve(x, r, tol=tol, maxit=20000)
+    assert st.updates >= 1
+    xh = x.download()
+    # independent FP64 check of the residual
+    Ax = gpu.DeviceBuffer(om.Ngather)
+    S64.operator(x, Ax)
+    res = np.linalg.norm(b_o - Ax.download()) / np.linalg.norm(b_o)
+    assert res <= tol * 1.0001, res
+    assert abs(np.sqrt(st.rdotr / st.rdotr0) - res) <= 1e-3 * res + 1e-16
+    # the FP64 oracle's CG to the same tolerance
+    x_o, _, it_o, _, _ = om.cg(b_o, 1.0, tol, 20000, precon=(precon == "JACOBI"))
+    err = np.linalg.norm(xh - x_o) / np.linalg.norm(x_o)
+    assert err < 1e-5, err
+    # the reliable updates keep the Krylov space: about FP64 CG's iteration count
+    assert st.iterations <= 1.25 * it_o + 20, (st.iterations, it_o)
+
+
+def test_mixed_needs_tolerance_and_reports_maxit(gpu):
+    gm = gpu.Mesh(3, 3, 3, N=4)
+    S = gpu.BP(gm, precon="JACOBI", precision="MIXED")
+    b = S.rhs("RANDOM", 0)
+    with pytest.raises(gpu.BPError, match="tol"):
+        S.solve(gpu.DeviceBuffer.from_host(np.zeros(gm.Ngather)), b, tol=0.0, maxit=10)
+    b = S.rhs("RANDOM", 0)
+    st, _, _ = S.solve(gpu.DeviceBuffer.from_host(np.zeros(gm.Ngather)), b, tol=1e-14, maxit=7)
+    assert st.iterations == 7
+
+
+def test_mixed_host_entry_matches_device_entry(gpu):
+    gm = gpu.Mesh(4, 4, 4, N=5, pert=0.1)
+    S = gpu.BP(gm, precon="JACOBI", precision="MIXED")
+    b = S.rhs("RANDOM", 0)
+    bh = b.download()
+    x = gpu.DeviceBuffer.from_host(np.zeros(gm.Ngather))
+    st, _, _ = S.solve(x, gpu.DeviceBuffer.from_host(bh), tol=1e-8, maxit=5000)
+    xh = np.zeros(gm.Ngather)
+    st2 = S.solve_host(bh, xh, tol=1e-8, maxit=5000)
+    assert st2.iterations == st.iterations and st2.updates == st.updates
+    np.testing.assert_array_equal(xh, x.download())
