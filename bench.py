@@ -250,7 +250,9 @@ def main():
     bp._check(L.bp_event_elapsed_ms(e0, e1, bp.ctypes.byref(ms)))
     t_dev = max_over_ranks(ms.value / 1e3, world)
     value = world * Nd * ITERS * args.steps / t_dev / 1e9
-    launches_per_step = 3 + 3 * ITERS + 1   # operator + init, 3 kernels per iteration, final x update
+    # r = b - A x (operator + gather), CG init, 4 kernels per iteration (direction, operator with p.Ap
+    # partials, alpha, gather + r update), final x update
+    launches_per_step = 3 + 4 * ITERS + 1
 
     # ---- dominant kernel: the element operator, timed alone with events (BK5 style) ----
     q = b
@@ -336,7 +338,7 @@ def main():
             "clocks": clk,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * Nd, "d2h_bytes_per_step": 8 * Nd},
             "gpu_launches": launches_per_step * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "ax_pencil_kernel<Nq=8>", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,double> (bp_ax_hex3d)", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes, "launch_ms": ax_s * 1e3},
             "model_bw_gbs": step_bytes * args.steps / (t_dev / world) / 1e9 if world == 1 else None,

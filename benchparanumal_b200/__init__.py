@@ -9,6 +9,7 @@ host objects for that path:
     BP        bpN_t : solver_t with Operator / forcing / cg::Solve
               (BP/BP5/src/bp5{Setup,Operator,Run}.cpp, libs/core/linearSolverCG.cpp)
     ax_hex3d  the bp5AxHex3D / bp5AxAffineHex3D / bp6AxHex3D kernels
+    ax_cub_hex3d  the over-integrated bp1-bp4 (Affine) Hex3D kernels
     ogs_gather / ogs_scatter   the ogs Gather(Add, Trans) / Scatter(NoTrans)
 
 Errors raise BPError carrying the library's message, the way the reference
@@ -42,6 +43,7 @@ EXPORTS = [
     "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc",
+    "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
 ]
 
 
@@ -70,6 +72,11 @@ class MeshView(ctypes.Structure):
                 ("Ngather", ctypes.c_int32), ("nnz", ctypes.c_int32), ("Nlocal", ctypes.c_int64)] + [
         (n, ctypes.c_void_p) for n in ("elementList", "GlobalToLocal", "rowStarts", "colIds", "wJ", "ggeo", "D",
                                        "gllz", "gllw", "EX", "EY", "EZ")]
+
+
+class CubatureView(ctypes.Structure):
+    _fields_ = [("cubNq", ctypes.c_int32), ("cubNp", ctypes.c_int32)] + [
+        (n, ctypes.c_void_p) for n in ("cubr", "cubw", "cubInterp", "cubD", "invV", "MM", "cubwJ", "cubggeo")]
 
 
 class SolverDesc(ctypes.Structure):
@@ -140,6 +147,10 @@ def lib():
             "bp_box_vertices": [ctypes.POINTER(BoxDesc), vp, vp, vp],
             "bp_operator_hex3d_noalloc": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, i32, vp, vp,
                                           vp, vp, vp],
+            "bp_ax_cub_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
+            "bp_mesh_cubature": [vp],
+            "bp_mesh_cubature_view": [vp, ctypes.POINTER(CubatureView)],
+            "bp_basis_cubature": [i32, vp, vp, vp, vp, vp, vp, vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -284,8 +295,26 @@ class Mesh:
             "gllz": (self.Nq, np.float64), "gllw": (self.Nq, np.float64), "EX": (8 * self.E, np.float64),
             "EY": (8 * self.E, np.float64), "EZ": (8 * self.E, np.float64),
         }
-        n, dt = spec[name]
-        return _dl(getattr(v, name), n, dt)
+        if name in spec:
+            n, dt = spec[name]
+            return _dl(getattr(v, name), n, dt)
+        c = self.cubature()
+        G, Nq = c.cubNq, self.Nq
+        ncub = self.E if self.affine else self.E * c.cubNp
+        cspec = {
+            "cubr": G, "cubw": G, "cubInterp": G * Nq, "cubD": (Nq * Nq if self.affine else G * G),
+            "invV": Nq * Nq, "MM": Nq * Nq, "cubwJ": ncub, "cubggeo": 6 * ncub,
+        }
+        return _dl(getattr(c, name), cspec[name], np.float64)
+
+    def cubature(self):
+        """Set up (once) and return the cubature view of the BP1-BP4 operators."""
+        if getattr(self, "_cub", None) is None:
+            _check(lib().bp_mesh_cubature(self._h))
+            c = CubatureView()
+            _check(lib().bp_mesh_cubature_view(self._h, ctypes.byref(c)))
+            self._cub = c
+        return self._cub
 
 
 def ax_hex3d(mesh, q, Aq, lam=1.0, elementList=None, Nelements=None, stream=None):
@@ -296,6 +325,15 @@ def ax_hex3d(mesh, q, Aq, lam=1.0, elementList=None, Nelements=None, stream=None
     ne = mesh.E if Nelements is None else Nelements
     _check(lib().bp_ax_hex3d(ctypes.byref(d), ne, el, v.GlobalToLocal, v.wJ, v.ggeo, v.gllw, v.D, float(lam),
                              _ptr(q), _ptr(Aq), stream))
+
+
+def ax_cub_hex3d(mesh, bp, q, Aq, lam=1.0, stream=None):
+    """bp_ax_cub_hex3d on device buffers: the over-integrated BP1-BP4 element
+    operator, Aq (E-vector) = A_e q[GlobalToLocal]."""
+    v, c = mesh.view, mesh.cubature()
+    d = AxDesc(bp, mesh.N, int(mesh.affine), mesh.Nfields)
+    _check(lib().bp_ax_cub_hex3d(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, c.cubwJ, c.cubggeo,
+                                 c.cubD, c.cubInterp, c.invV, c.MM, float(lam), _ptr(q), _ptr(Aq), stream))
 
 
 def ogs_gather(mesh, v, gv, stream=None):
@@ -330,7 +368,8 @@ def _ptr(b):
 
 
 class BP:
-    """Benchmark problem on a Mesh: bp 5 (scalar) or 6 (three fields)."""
+    """Benchmark problem on a Mesh: bp 1..6 (odd: one field, even: three
+    fields; default 5 or 6 by the mesh's field count)."""
 
     def __init__(self, mesh, bp=None, lam=1.0, precon="NONE", precision="FP64"):
         self.mesh = mesh
@@ -407,6 +446,20 @@ def basis_gll(N):
     z = np.empty(N + 1); w = np.empty(N + 1); D = np.empty((N + 1) * (N + 1))
     _check(lib().bp_basis_gll(N, z.ctypes.data, w.ctypes.data, D.ctypes.data))
     return z, w, D.reshape(N + 1, N + 1)
+
+
+def basis_cubature(N):
+    """Host-only cubature data of degree N: dict of r, w (N+2), I [(N+2) x (N+1)],
+    D [(N+2) x (N+2)], invV, Dmodal, MM [(N+1) x (N+1)]."""
+    G, Nq = N + 2, N + 1
+    out = {"r": np.empty(G), "w": np.empty(G), "I": np.empty(G * Nq), "D": np.empty(G * G),
+           "invV": np.empty(Nq * Nq), "Dmodal": np.empty(Nq * Nq), "MM": np.empty(Nq * Nq)}
+    _check(lib().bp_basis_cubature(N, *(out[k].ctypes.data for k in ("r", "w", "I", "D", "invV", "Dmodal", "MM"))))
+    out["I"] = out["I"].reshape(G, Nq)
+    out["D"] = out["D"].reshape(G, G)
+    for k in ("invV", "Dmodal", "MM"):
+        out[k] = out[k].reshape(Nq, Nq)
+    return out
 
 
 def box_vertices(nx, ny, nz, pert=0.0, pert_seed=1):

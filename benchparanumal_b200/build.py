@@ -17,7 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libbp_b200.so")
-APPS = ["BP5", "BP6", "BK5", "BK6"]
+APPS = ["BP%d" % k for k in range(1, 7)] + ["BK%d" % k for k in range(1, 7)]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOSTCXX = "/usr/bin/g++"   # the system g++ carries libgomp
@@ -26,7 +26,8 @@ CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOSTCXX, "-Xcompil
                   "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-march=x86-64-v3", "-Wall", "-Wno-unknown-pragmas",
             "-I/usr/local/cuda/include"]
-HEADERS = [os.path.join(CSRC, "bp_internal.hpp"), os.path.join(ROOT, "include", "bp_b200.h")]
+HEADERS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh"))) + [
+    os.path.join(ROOT, "include", "bp_b200.h")]
 
 
 def _newer(src, dst, extra=()):

@@ -207,6 +207,24 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                    to_stream(stream));
 }
 
+int bp_ax_cub_hex3d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* elementList,
+                    const int32_t* GlobalToLocal, const double* cubwJ, const double* cubggeo, const double* cubD,
+                    const double* cubInterp, const double* invV, const double* MM, double lambda, const double* q,
+                    double* Aq, bp_stream_t stream) {
+  if (!d) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: null descriptor");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: degree N must be in 1..15");
+  if (d->bp < 1 || d->bp > 4) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: bp must be 1..4");
+  if (d->Nfields != ((d->bp % 2) ? 1 : 3)) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: BP1/BP3 have 1 field, BP2/BP4 3");
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  const bool stiff = d->bp >= 3;
+  const double* T = !d->affine ? cubInterp : (stiff ? invV : MM);
+  if (!elementList || !GlobalToLocal || !cubwJ || !T || !q || !Aq || (stiff && (!cubggeo || !cubD)))
+    return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: null array");
+  const CubOperands<double> ops{cubwJ, cubggeo, cubD, T};
+  return launch_ax_cub(*d, Nelements, elementList, GlobalToLocal, ops, lambda, q, Aq, nullptr, to_stream(stream));
+}
+
 int bp_ogs_gather(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* v, double* gv,
                   bp_stream_t stream) {
   if (Nrows < 0) return fail(BP_ERROR_ARG, "bp_ogs_gather: negative row count");
@@ -340,6 +358,86 @@ int bp_mesh_view(bp_mesh_t m, bp_mesh_view_t* v) {
   v->rowStarts = m->rowStarts.ptr; v->colIds = m->colIds.ptr;
   v->wJ = m->wJ.ptr; v->ggeo = m->ggeo.ptr; v->D = m->D.ptr; v->gllz = m->gllz.ptr; v->gllw = m->gllw.ptr;
   v->EX = m->EX.ptr; v->EY = m->EY.ptr; v->EZ = m->EZ.ptr;
+  return BP_SUCCESS;
+}
+
+int bp_mesh_cubature(bp_mesh_t m) {
+  if (!m) return fail(BP_ERROR_ARG, "bp_mesh_cubature: null mesh");
+  if (m->cubNq) return BP_SUCCESS;
+  cudaStream_t s = default_stream();
+  std::vector<double> z(m->Nq);
+  BP_CUDA_TRY(cudaMemcpy(z.data(), m->gllz.ptr, sizeof(double) * m->Nq, cudaMemcpyDeviceToHost));
+  CubBasis cb;
+  cubature_basis(m->N, z, cb);
+  const int Nq = m->Nq, G = cb.cNq;
+  std::vector<double> DV;
+  if (m->affine) {
+    DV.assign((size_t)Nq * Nq, 0.0);
+    for (int i = 0; i < Nq; ++i)
+      for (int a = 0; a < Nq; ++a) {
+        double acc = 0;
+        for (int l = 0; l < Nq; ++l) acc += cb.Dmodal[(size_t)i * Nq + l] * cb.invV[(size_t)l * Nq + a];
+        DV[(size_t)i * Nq + a] = acc;
+      }
+  } else {
+    DV.assign((size_t)G * Nq, 0.0);
+    for (int i = 0; i < G; ++i)
+      for (int a = 0; a < Nq; ++a) {
+        double acc = 0;
+        for (int l = 0; l < G; ++l) acc += cb.D[(size_t)i * G + l] * cb.I[(size_t)l * Nq + a];
+        DV[(size_t)i * Nq + a] = acc;
+      }
+  }
+  int rc = BP_SUCCESS;
+  int* d_bad = nullptr;
+  do {
+    if ((rc = m->cubr.upload(cb.r, s))) break;
+    if ((rc = m->cubw.upload(cb.w, s))) break;
+    if ((rc = m->cubInterp.upload(cb.I, s))) break;
+    if ((rc = m->cubD.upload(cb.D, s))) break;
+    if ((rc = m->invV.upload(cb.invV, s))) break;
+    if ((rc = m->cubDmodal.upload(cb.Dmodal, s))) break;
+    if ((rc = m->MM.upload(cb.MM, s))) break;
+    if ((rc = m->cubDV.upload(DV, s))) break;
+    if (!m->affine) {
+      const size_t n = (size_t)m->E * G * G * G;
+      if ((rc = m->cubwJ_c.alloc(n))) break;
+      if ((rc = m->cubggeo_c.alloc(6 * n))) break;
+      cudaError_t ce = cudaMalloc(&d_bad, sizeof(int));
+      if (ce == cudaSuccess) ce = cudaMemsetAsync(d_bad, 0, sizeof(int), s);
+      if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_mesh_cubature", __FILE__, __LINE__); break; }
+      if ((rc = launch_geometry_at(G, m->E, m->EX.ptr, m->EY.ptr, m->EZ.ptr, m->cubr.ptr, m->cubw.ptr,
+                                   m->cubwJ_c.ptr, m->cubggeo_c.ptr, d_bad, s)))
+        break;
+      int bad = 0;
+      ce = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+      if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_mesh_cubature", __FILE__, __LINE__); break; }
+      if (bad) { rc = fail(BP_ERROR_NUMERIC, "bp_mesh_cubature: non-positive Jacobian at a Gauss point"); break; }
+    } else {
+      cudaError_t ce = cudaStreamSynchronize(s);
+      if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_mesh_cubature", __FILE__, __LINE__); break; }
+    }
+  } while (0);
+  if (d_bad) cudaFree(d_bad);
+  if (rc != BP_SUCCESS) {
+    m->cubwJ_c.release();
+    m->cubggeo_c.release();
+    return rc;
+  }
+  m->cubNq = G;
+  return BP_SUCCESS;
+}
+
+int bp_mesh_cubature_view(bp_mesh_t m, bp_cubature_view_t* v) {
+  if (!m || !v) return fail(BP_ERROR_ARG, "bp_mesh_cubature_view: null pointer");
+  if (!m->cubNq) return fail(BP_ERROR_ARG, "bp_mesh_cubature_view: call bp_mesh_cubature first");
+  v->cubNq = m->cubNq;
+  v->cubNp = m->cubNq * m->cubNq * m->cubNq;
+  v->cubr = m->cubr.ptr; v->cubw = m->cubw.ptr; v->cubInterp = m->cubInterp.ptr;
+  v->cubD = m->affine ? m->cubDmodal.ptr : m->cubD.ptr;
+  v->invV = m->invV.ptr; v->MM = m->MM.ptr;
+  v->cubwJ = m->cubwJ(); v->cubggeo = m->cubggeo();
   return BP_SUCCESS;
 }
 

@@ -1,5 +1,6 @@
-// BK5 / BP5 drivers behind bp_driver_main(): the reference executables'
-// command-line keys, settings semantics and result lines, running on the C ABI.
+// BK1-BK6 / BP1-BP6 drivers behind bp_driver_main(): the reference
+// executables' command-line keys, settings semantics and result lines, running
+// on the C ABI.
 //
 // Settings semantics follow libs/core/settings.cpp:
 //   * every setting has a short key, long key, name, default, description and
@@ -176,6 +177,7 @@ struct Problem {
   bp_mesh_t mesh = nullptr;
   bp_solver_t solver = nullptr;
   bp_mesh_view_t view{};
+  bp_cubature_view_t cub{};   // BP1-BP4
   ~Problem() {
     if (solver) bp_solver_destroy(solver);
     if (mesh) bp_mesh_destroy(mesh);
@@ -206,6 +208,7 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
   sd.precon = S.compare("PRECONDITIONER", "JACOBI") ? BP_PRECON_JACOBI : BP_PRECON_NONE;
   sd.precision = S.compare("PRECISION", "MIXED") ? BP_PRECISION_MIXED : BP_PRECISION_FP64;
   check(bp_solver_create(P.mesh, &sd, &P.solver));
+  if (bp <= 4) check(bp_mesh_cubature_view(P.mesh, &P.cub));
 }
 
 struct DevVec {
@@ -214,16 +217,26 @@ struct DevVec {
   ~DevVec() { bp_free(p); }
 };
 
-// reference byte model for one Ax application (bp5Run.cpp:106-142, bk5Run.cpp:97-125)
-double ax_bytes(const bp_mesh_view_t& v, long long Ndofs) {
+// reference byte model for one Ax application: BP5/BP6 bp5Run.cpp:106-142,
+// bk5Run.cpp:97-125; BP3/BP4 bp3Run.cpp:107-122; BP1/BP2 bp1Run.cpp and
+// bk1Run.cpp (one factor per point, J or JW)
+double ax_bytes(int bp, const bp_mesh_view_t& v, long long Ndofs) {
   const double E = v.Nelements, Np = v.Np, Nf = v.Nfields;
-  if (v.affine) return Ndofs * 8.0 + (7 * 8.0 + 4.0 + Np * Nf * 4.0 + Np * Nf * 8.0) * E;
-  return Ndofs * 8.0 + (Np * 7 * 8.0 + 4.0 + Np * Nf * 4.0 + Np * Nf * 8.0) * E;
+  const double cNq = v.N + 2, cNp = cNq * cNq * cNq;
+  const double per_point = bp <= 2 ? 1.0 : 7.0;          // J, or ggeo + wJ
+  const double points = v.affine ? 1.0 : (bp <= 4 ? cNp : Np);
+  return Ndofs * 8.0 + (points * per_point * 8.0 + 4.0 + Np * Nf * 4.0 + Np * Nf * 8.0) * E;
 }
-double ax_flops(const bp_mesh_view_t& v) {
+// reference flop model for one Ax application (the same files, Hex branches)
+double ax_flops(int bp, const bp_mesh_view_t& v) {
   const double Nq = v.Nq, E = v.Nelements, Nf = v.Nfields;
-  if (v.affine) return (12 * Nq * Nq * Nq * Nq + 21 * Nq * Nq * Nq) * Nf * E;
-  return (12 * Nq * Nq * Nq * Nq + 18 * Nq * Nq * Nq) * Nf * E;
+  const double cNq = v.N + 2, Nq3 = Nq * Nq * Nq, cNq3 = cNq * cNq * cNq;
+  const double interp = 4 * cNq * Nq3 + 4 * cNq * cNq * Nq * Nq + 4 * cNq3 * Nq;
+  double f;
+  if (bp <= 2) f = v.affine ? 6 * Nq * Nq3 + Nq3 : interp + cNq3;
+  else if (bp <= 4) f = v.affine ? 24 * Nq * Nq3 + 17 * Nq3 : interp + 12 * cNq * cNq3 + 17 * cNq3;
+  else f = v.affine ? 12 * Nq * Nq3 + 21 * Nq3 : 12 * Nq * Nq3 + 18 * Nq3;
+  return f * Nf * E;
 }
 
 int run_bp(const char* name, int bp, Settings& S) {
@@ -261,10 +274,10 @@ int run_bp(const char* name, int bp, Settings& S) {
   }
   const long long Ndofs = N;
   const double NGlobal = (double)P.view.Nlocal;
-  const double NbytesAx = ax_bytes(P.view, Ndofs);
+  const double NbytesAx = ax_bytes(bp, P.view, Ndofs);
   const double NbytesGather = (Ndofs + 1) * 4.0 + NGlobal * 4.0 + NGlobal * 8.0 + Ndofs * 8.0;
   const double Nbytes = (4 * Ndofs * 8.0 + NbytesAx + NbytesGather) + (11 * Ndofs * 8.0 + NbytesAx + NbytesGather) * Niter;
-  const double NflopsAx = ax_flops(P.view);
+  const double NflopsAx = ax_flops(bp, P.view);
   const double Nflops = (5.0 * Ndofs + NflopsAx + NGlobal) + (11.0 * Ndofs + NflopsAx + NGlobal) * Niter;
   std::string suffix = "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
@@ -300,13 +313,18 @@ int run_bk(const char* name, int bk, Settings& S) {
     check(bp_solver_rhs(P.solver, BP_RHS_ANALYTIC, 0, q.p, nullptr));
   }
   bp_ax_desc_t d{};
-  d.bp = (Nfields == 3) ? 6 : 5;
+  d.bp = bk;
   d.N = P.view.N;
   d.affine = P.view.affine;
   d.Nfields = Nfields;
   auto apply = [&]() {
-    check(bp_ax_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
-                      P.view.gllw, P.view.D, 1.0, q.p, Aq.p, nullptr));
+    if (bk >= 5)
+      check(bp_ax_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
+                        P.view.gllw, P.view.D, 1.0, q.p, Aq.p, nullptr));
+    else
+      check(bp_ax_cub_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.cub.cubwJ,
+                            P.cub.cubggeo, P.cub.cubD, P.cub.cubInterp, P.cub.invV, P.cub.MM, 1.0, q.p, Aq.p,
+                            nullptr));
   };
   for (int n = 0; n < 5; ++n) apply();
   const int Ntests = 50;
@@ -315,8 +333,8 @@ int run_bk(const char* name, int bk, Settings& S) {
   const double t1 = now_after_finish();
   const double elapsed = (t1 - t0) / Ntests;
   const long long Ndofs = Ngather;
-  const double Nbytes = ax_bytes(P.view, Ndofs);
-  const double Nflops = ax_flops(P.view);
+  const double Nbytes = ax_bytes(bk, P.view, Ndofs);
+  const double Nflops = ax_flops(bk, P.view);
   std::string suffix = "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
@@ -336,8 +354,8 @@ extern "C" int bp_driver_main(const char* name, int argc, char** argv) {
     const bool bp = n.size() == 3 && n[0] == 'B' && n[1] == 'P';
     const bool bk = n.size() == 3 && n[0] == 'B' && n[1] == 'K';
     const int which = (bp || bk) ? n[2] - '0' : 0;
-    if (!(bp || bk) || (which != 5 && which != 6))
-      throw std::runtime_error("bp_driver_main: available drivers are BP5, BP6, BK5, BK6");
+    if (!(bp || bk) || which < 1 || which > 6)
+      throw std::runtime_error("bp_driver_main: available drivers are BP1-BP6 and BK1-BK6");
     Settings S;
     add_common(S, bp);
     if (!S.parse(argc, argv)) return BP_SUCCESS;

@@ -84,6 +84,19 @@ struct HostMesh {
 // basis (GLL nodes by Newton iteration, lumped weights, differentiation matrix)
 void gll_nodes_weights(int N, std::vector<double>& z, std::vector<double>& w);
 void diff_matrix(const std::vector<double>& z, std::vector<double>& D);
+// Gauss-Legendre points and weights (n points)
+void gauss_nodes_weights(int n, std::vector<double>& r, std::vector<double>& w);
+// 1D data of the over-integrated (BP1-BP4) operators
+struct CubBasis {
+  int cNq = 0;                        // N+2 Gauss points
+  std::vector<double> r, w;           // Gauss points and weights [cNq]
+  std::vector<double> I;              // GLL -> Gauss interpolation [cNq*Nq]
+  std::vector<double> D;              // differentiation on the Gauss points [cNq*cNq]
+  std::vector<double> invV;           // inverse orthonormal Legendre Vandermonde on GLL [Nq*Nq]
+  std::vector<double> Dmodal;         // invV * Vr [Nq*Nq]
+  std::vector<double> MM;             // exact GLL mass matrix [Nq*Nq]
+};
+void cubature_basis(int N, const std::vector<double>& gllz, CubBasis& cb);
 // box vertices with optional seeded interior perturbation
 void box_vertices(HostMesh& m, double pert, uint64_t seed);
 // masked gathered numbering, CSR and GlobalToLocal for the box
@@ -97,6 +110,16 @@ struct bp_mesh_s {
   int32_t Ngather, nnz;
   bp::DeviceArray<int32_t> elementList, G2L, rowStarts, colIds;
   bp::DeviceArray<double> wJ, ggeo, D, gllz, gllw, EX, EY, EZ;
+  // cubature of the BP1-BP4 operators (bp_mesh_cubature); cubNq = 0 until set up
+  int cubNq = 0;
+  bp::DeviceArray<double> cubr, cubw, cubInterp, cubD, invV, cubDmodal, MM;
+  bp::DeviceArray<double> cubDV;                // derivative columns for the diagonal: cubD*cubInterp
+                                                // (curved) or cubDmodal*invV (affine)
+  bp::DeviceArray<double> cubwJ_c, cubggeo_c;   // curved mesh only
+  // factors at the quadrature points: curved [E*cubNp], [6*E*cubNp]; affine the
+  // per-element wJ and ggeo
+  const double* cubwJ() const { return affine ? wJ.ptr : cubwJ_c.ptr; }
+  const double* cubggeo() const { return affine ? ggeo.ptr : cubggeo_c.ptr; }
 };
 
 struct bp_solver_s;
@@ -151,6 +174,29 @@ int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
 int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const float* wJ, const float* ggeo, const float* D, float lambda, const float* q, float* Aq,
                   const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+// over-integrated BP1-BP4 operator (bp_ax_cub*.cu).  T is the 1D transform:
+// curved cubInterp [cubNq*Nq]; affine BP3/BP4 invV [Nq*Nq]; affine BP1/BP2 MM
+// [Nq*Nq].  D is cubD (curved) or the modal cubD (affine BP3/BP4); unused for
+// BP1/BP2.  With fuse, the block partials of q.Aq go to fuse->partials.
+template <class F>
+struct CubOperands {
+  const F* wJ;
+  const F* ggeo;
+  const F* D;
+  const F* T;
+};
+int launch_ax_cub(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                  const CubOperands<double>& ops, double lambda, const double* q, double* Aq, const int* skip,
+                  cudaStream_t s, const CgFuse* fuse = nullptr, int* nblocks = nullptr);
+int launch_ax_cub(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                  const CubOperands<float>& ops, float lambda, const float* q, float* Aq, const int* skip,
+                  cudaStream_t s, const CgFuse* fuse = nullptr, int* nblocks = nullptr);
+// element-local diagonal of the BP1-BP4 operators (DV = D*T, the derivative columns)
+int launch_diag_cub(const bp_ax_desc_t& d, int32_t Nelements, const double* wJ, const double* ggeo,
+                    const double* T, const double* DV, double lambda, double* dL, cudaStream_t s);
+// cubature geometric factors of a curved mesh at the Gauss points
+int launch_geometry_at(int Nq, int E, const double* EX, const double* EY, const double* EZ, const double* r,
+                       const double* w, double* wJ, double* ggeo, int* bad, cudaStream_t s);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

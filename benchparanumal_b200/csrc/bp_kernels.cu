@@ -460,6 +460,21 @@ int launch_geometry(int N, int affine, int E, const double* EX, const double* EY
   return BP_SUCCESS;
 }
 
+// Factors of a curved mesh at any tensor grid of points r (weights w), e.g.
+// the N+2 Gauss points of the over-integrated operators.  The reference
+// interpolates the GLL-node derivatives of x, y, z to the Gauss points
+// (meshCubatureSetupHex3D.cpp:104-225); for the trilinear element map those
+// derivatives are exactly representable, so the analytic Jacobian at the
+// points is the same quantity.
+int launch_geometry_at(int Nq, int E, const double* EX, const double* EY, const double* EZ, const double* r,
+                       const double* w, double* wJ, double* ggeo, int* bad, cudaStream_t s) {
+  if (E == 0) return BP_SUCCESS;
+  const long long tot = (long long)E * Nq * Nq * Nq;
+  geometry_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(Nq, E, EX, EY, EZ, r, w, wJ, ggeo, bad);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
 // ---------------------------------------------------------------------------
 // Forcing (okl/rhsHex3D.okl:29-128) on the fly from the vertex map
 // ---------------------------------------------------------------------------

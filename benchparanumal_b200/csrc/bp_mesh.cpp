@@ -97,6 +97,124 @@ void diff_matrix(const std::vector<double>& z, std::vector<double>& D) {
   }
 }
 
+// Legendre P_n(x) and P_n'(x) by the three-term recurrence and
+// P'_{k+1} = P'_{k-1} + (2k+1) P_k.
+static void legendre(int n, double x, double& p, double& dp) {
+  double p0 = 1.0, p1 = x, d0 = 0.0, d1 = 1.0;
+  if (n == 0) { p = 1.0; dp = 0.0; return; }
+  for (int k = 1; k < n; ++k) {
+    const double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
+    const double d2 = d0 + (2 * k + 1) * p1;
+    p0 = p1; p1 = p2; d0 = d1; d1 = d2;
+  }
+  p = p1;
+  dp = d1;
+}
+
+// Gauss-Legendre points and weights, n points: Newton on P_n from the
+// Chebyshev guesses cos(pi (i+3/4)/(n+1/2)); w = 2 / ((1-x^2) P_n'(x)^2).
+void gauss_nodes_weights(int n, std::vector<double>& r, std::vector<double>& w) {
+  const double pi = 3.14159265358979323846;
+  r.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double x = -std::cos(pi * (i + 0.75) / (n + 0.5)), p, dp;
+    for (int it = 0; it < 100; ++it) {
+      legendre(n, x, p, dp);
+      const double dx = p / dp;
+      x -= dx;
+      if (std::fabs(dx) <= 1e-16) break;
+    }
+    legendre(n, x, p, dp);
+    r[i] = x;
+    w[i] = 2.0 / ((1.0 - x * x) * dp * dp);
+  }
+  for (int i = 0; i < n / 2; ++i) {   // symmetrise
+    const double a = 0.5 * (r[n - 1 - i] - r[i]), b = 0.5 * (w[i] + w[n - 1 - i]);
+    r[i] = -a; r[n - 1 - i] = a;
+    w[i] = w[n - 1 - i] = b;
+  }
+  if (n % 2) r[n / 2] = 0.0;
+}
+
+// Lagrange interpolation from nodes z to points x: I[i*nz + m] = l_m(x_i).
+static void interp_matrix(const std::vector<double>& z, const std::vector<double>& x, std::vector<double>& I) {
+  const int nz = (int)z.size(), nx = (int)x.size();
+  I.assign((size_t)nx * nz, 0.0);
+  for (int i = 0; i < nx; ++i)
+    for (int m = 0; m < nz; ++m) {
+      double l = 1.0;
+      for (int k = 0; k < nz; ++k)
+        if (k != m) l *= (x[i] - z[k]) / (z[m] - z[k]);
+      I[(size_t)i * nz + m] = l;
+    }
+}
+
+// In-place inverse of a small dense matrix (Gauss-Jordan, partial pivoting).
+static bool invert(int n, std::vector<double>& A) {
+  std::vector<double> X((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) X[(size_t)i * n + i] = 1.0;
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
+    if (A[(size_t)piv * n + c] == 0.0) return false;
+    for (int k = 0; k < n; ++k) {
+      std::swap(A[(size_t)c * n + k], A[(size_t)piv * n + k]);
+      std::swap(X[(size_t)c * n + k], X[(size_t)piv * n + k]);
+    }
+    const double d = A[(size_t)c * n + c];
+    for (int k = 0; k < n; ++k) { A[(size_t)c * n + k] /= d; X[(size_t)c * n + k] /= d; }
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      const double f = A[(size_t)r * n + c];
+      if (f == 0.0) continue;
+      for (int k = 0; k < n; ++k) {
+        A[(size_t)r * n + k] -= f * A[(size_t)c * n + k];
+        X[(size_t)r * n + k] -= f * X[(size_t)c * n + k];
+      }
+    }
+  }
+  A = X;
+  return true;
+}
+
+// 1D data of the over-integrated operators (libs/mesh/meshCubatureSetupHex3D.cpp:
+// 31-80): N+2 Gauss points, GLL->Gauss interpolation, differentiation on the
+// Gauss points; the inverse orthonormal-Legendre Vandermonde on the GLL nodes,
+// the modal differentiation matrix invV*Vr and the exact GLL mass matrix
+// MM = invV^T invV (= (V V^T)^-1).
+void cubature_basis(int N, const std::vector<double>& gllz, CubBasis& cb) {
+  const int Nq = N + 1, cNq = N + 2;
+  cb.cNq = cNq;
+  gauss_nodes_weights(cNq, cb.r, cb.w);
+  interp_matrix(gllz, cb.r, cb.I);
+  diff_matrix(cb.r, cb.D);
+  std::vector<double> V((size_t)Nq * Nq), Vr((size_t)Nq * Nq);
+  for (int i = 0; i < Nq; ++i)
+    for (int n = 0; n < Nq; ++n) {
+      double p, dp;
+      legendre(n, gllz[i], p, dp);
+      const double s = std::sqrt((2.0 * n + 1.0) / 2.0);
+      V[(size_t)i * Nq + n] = s * p;
+      Vr[(size_t)i * Nq + n] = s * dp;
+    }
+  cb.invV = V;
+  invert(Nq, cb.invV);
+  cb.Dmodal.assign((size_t)Nq * Nq, 0.0);
+  cb.MM.assign((size_t)Nq * Nq, 0.0);
+  for (int a = 0; a < Nq; ++a)
+    for (int b = 0; b < Nq; ++b) {
+      double d = 0.0, mm = 0.0;
+      for (int k = 0; k < Nq; ++k) {
+        d += cb.invV[(size_t)a * Nq + k] * Vr[(size_t)k * Nq + b];
+        mm += cb.invV[(size_t)k * Nq + a] * cb.invV[(size_t)k * Nq + b];
+      }
+      cb.Dmodal[(size_t)a * Nq + b] = d;
+      cb.MM[(size_t)a * Nq + b] = mm;
+    }
+}
+
 // Box vertices as in libs/mesh/meshSetupBoxHex3D.cpp:31-131 (one rank), with
 // interior vertices moved by pert*h*(2u-1) per coordinate; u is the reference
 // LCG stream (libs/primitives/random.cpp) seeded with `seed`, three values per
@@ -262,6 +380,24 @@ extern "C" int bp_basis_gll(int32_t N, double* z, double* w, double* D) {
   if (z) std::copy(zz.begin(), zz.end(), z);
   if (w) std::copy(ww.begin(), ww.end(), w);
   if (D) std::copy(DD.begin(), DD.end(), D);
+  return BP_SUCCESS;
+}
+
+extern "C" int bp_basis_cubature(int32_t N, double* r, double* w, double* I, double* D, double* invV,
+                                 double* Dmodal, double* MM) {
+  if (N < 1 || N > 15) return bp::fail(BP_ERROR_ARG, "bp_basis_cubature: degree must be in 1..15");
+  if (!r || !w || !I || !D || !invV || !Dmodal || !MM) return bp::fail(BP_ERROR_ARG, "bp_basis_cubature: null array");
+  std::vector<double> z, zw;
+  bp::gll_nodes_weights(N, z, zw);
+  bp::CubBasis cb;
+  bp::cubature_basis(N, z, cb);
+  std::copy(cb.r.begin(), cb.r.end(), r);
+  std::copy(cb.w.begin(), cb.w.end(), w);
+  std::copy(cb.I.begin(), cb.I.end(), I);
+  std::copy(cb.D.begin(), cb.D.end(), D);
+  std::copy(cb.invV.begin(), cb.invV.end(), invV);
+  std::copy(cb.Dmodal.begin(), cb.Dmodal.end(), Dmodal);
+  std::copy(cb.MM.begin(), cb.MM.end(), MM);
   return BP_SUCCESS;
 }
 

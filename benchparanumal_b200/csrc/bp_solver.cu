@@ -321,7 +321,7 @@ struct bp_solver_s {
   bp_ax_desc_t ax{};
   DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist, fuse_partials, bcopy;
   // FP32 data of the mixed-precision solve
-  DeviceArray<float> wJ32, ggeo32, D32, gllw32, invD32, AqL32, p32, x32, r32;
+  DeviceArray<float> wJ32, ggeo32, D32, gllw32, T32, invD32, AqL32, p32, x32, r32;
   DeviceArray<unsigned int> counter;
   DeviceArray<CgScalars> sc;
   int hist_len = 0;
@@ -341,17 +341,51 @@ struct bp_solver_s {
 
 namespace bp {
 
+// Operands of the element operator in one arithmetic type: BP5/BP6 use wJ,
+// ggeo, gllw, D (GLL collocation); BP1-BP4 use wJ, ggeo, D and the 1D
+// transform T at the quadrature points (CubOperands).
+template <class V>
+struct ElemOperands {
+  const V* wJ;
+  const V* ggeo;
+  const V* gllw;
+  const V* D;
+  const V* T;
+};
+
+static ElemOperands<double> operands64(const bp_solver_s* S) {
+  const bp_mesh_s* m = S->mesh;
+  if (S->bp >= 5) return {m->wJ.ptr, m->ggeo.ptr, m->gllw.ptr, m->D.ptr, nullptr};
+  const double* D = m->affine ? m->cubDmodal.ptr : m->cubD.ptr;
+  const double* T = !m->affine ? m->cubInterp.ptr : (S->bp >= 3 ? m->invV.ptr : m->MM.ptr);
+  return {m->cubwJ(), m->cubggeo(), nullptr, D, T};
+}
+
+static ElemOperands<float> operands32(const bp_solver_s* S) {
+  return {S->wJ32.ptr, S->ggeo32.ptr, S->gllw32.ptr, S->D32.ptr, S->T32.ptr};
+}
+
+template <class V>
+static int elem_apply(bp_solver_s* S, const ElemOperands<V>& o, const V* q, V* AqL, const int* skip, cudaStream_t s,
+                      const CgFuse* fuse = nullptr, int* nblocks = nullptr) {
+  bp_mesh_s* m = S->mesh;
+  if (S->bp >= 5)
+    return launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D, (V)S->lambda, q,
+                          AqL, skip, s, fuse, nblocks);
+  const CubOperands<V> c{o.wJ, o.ggeo, o.D, o.T};
+  return launch_ax_cub(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, c, (V)S->lambda, q, AqL, skip, s, fuse, nblocks);
+}
+
 static int operator_apply(bp_solver_s* S, const double* q, double* Aq, const int* skip, cudaStream_t s) {
   bp_mesh_s* m = S->mesh;
-  BP_TRY(launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, m->wJ.ptr, m->ggeo.ptr, m->gllw.ptr,
-                        m->D.ptr, S->lambda, q, S->AqL.ptr, skip, s));
+  BP_TRY(elem_apply<double>(S, operands64(S), q, S->AqL.ptr, skip, s));
   return launch_gather(m->Ngather, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, Aq, s);
 }
 
 // enqueue one CG iteration on vectors of type V (FP64, or FP32 in a mixed solve)
 template <class V>
-static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* invD, const V* wJ, const V* ggeo,
-                             const V* gllw, const V* D, cudaStream_t s) {
+static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* invD, const ElemOperands<V>& o,
+                             cudaStream_t s) {
   bp_mesh_s* m = S->mesh;
   const int32_t N = S->N;
   const int g = vec_grid(N);
@@ -361,8 +395,7 @@ static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* 
   BP_CUDA_TRY(cudaGetLastError());
   const CgFuse fuse{S->fuse_partials.ptr};
   int nparts = 0;
-  BP_TRY(launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, wJ, ggeo, gllw, D, (V)S->lambda, p, AqL,
-                        &S->sc.ptr->done, s, &fuse, &nparts));
+  BP_TRY(elem_apply<V>(S, o, p, AqL, &S->sc.ptr->done, s, &fuse, &nparts));
   cg_alpha_kernel<<<1, kAlphaThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->sc.ptr, hist_alpha);
   BP_CUDA_TRY(cudaGetLastError());
   cg_gather_update_kernel<V><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, AqL, r, invD, S->sc.ptr,
@@ -391,14 +424,12 @@ static int capture(cudaGraphExec_t* out, cudaStream_t s, int (*body)(bp_solver_s
 }
 
 static int body64(bp_solver_s* S, void* x, void* r, cudaStream_t s) {
-  bp_mesh_s* m = S->mesh;
-  return enqueue_iteration<double>(S, (double*)x, (double*)r, S->p.ptr, S->AqL.ptr, S->invD.ptr, m->wJ.ptr,
-                                   m->ggeo.ptr, m->gllw.ptr, m->D.ptr, s);
+  return enqueue_iteration<double>(S, (double*)x, (double*)r, S->p.ptr, S->AqL.ptr, S->invD.ptr, operands64(S), s);
 }
 
 static int body32(bp_solver_s* S, void*, void*, cudaStream_t s) {
-  return enqueue_iteration<float>(S, S->x32.ptr, S->r32.ptr, S->p32.ptr, S->AqL32.ptr, S->invD32.ptr, S->wJ32.ptr,
-                                  S->ggeo32.ptr, S->gllw32.ptr, S->D32.ptr, s);
+  return enqueue_iteration<float>(S, S->x32.ptr, S->r32.ptr, S->p32.ptr, S->AqL32.ptr, S->invD32.ptr, operands32(S),
+                                  s);
 }
 
 static int ensure_graph(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
@@ -540,13 +571,14 @@ extern "C" {
 int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out) {
   if (!mesh || !d || !out) return fail(BP_ERROR_ARG, "bp_solver_create: null pointer");
   *out = nullptr;
-  if (d->bp != 5 && d->bp != 6) return fail(BP_ERROR_ARG, "bp_solver_create: only BP5 and BP6 are available");
-  if ((d->bp == 6) != (mesh->Nfields == 3))
-    return fail(BP_ERROR_ARG, "bp_solver_create: BP6 needs a 3-field mesh, BP5 a 1-field mesh");
+  if (d->bp < 1 || d->bp > 6) return fail(BP_ERROR_ARG, "bp_solver_create: bp must be 1..6");
+  if ((d->bp % 2 == 0) != (mesh->Nfields == 3))
+    return fail(BP_ERROR_ARG, "bp_solver_create: BP2/BP4/BP6 need a 3-field mesh, BP1/BP3/BP5 a 1-field mesh");
   if (d->precon != BP_PRECON_NONE && d->precon != BP_PRECON_JACOBI)
     return fail(BP_ERROR_ARG, "bp_solver_create: unknown preconditioner");
   if (d->precision != BP_PRECISION_FP64 && d->precision != BP_PRECISION_MIXED)
     return fail(BP_ERROR_ARG, "bp_solver_create: unknown precision");
+  if (d->bp <= 4) BP_TRY(bp_mesh_cubature(mesh));
   cudaStream_t s = default_stream();
   bp_solver_s* S = new bp_solver_s();
   S->mesh = mesh;
@@ -584,20 +616,26 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
     }
     if (S->mixed) {
       // FP32 copies of the stored factors and the 1D operators, FP32 CG vectors
-      const size_t ng = mesh->wJ.n;
+      const ElemOperands<double> o = operands64(S);
+      const bool cub = S->bp <= 4;
+      const size_t ng = cub ? (mesh->affine ? (size_t)mesh->E : mesh->cubwJ_c.n) : mesh->wJ.n;
+      const size_t nD = cub ? (mesh->affine ? mesh->cubDmodal.n : mesh->cubD.n) : mesh->D.n;
+      const size_t nT = cub ? (mesh->affine ? mesh->MM.n : mesh->cubInterp.n) : 0;
       if ((rc = S->wJ32.alloc(ng))) break;
       if ((rc = S->ggeo32.alloc(6 * ng))) break;
-      if ((rc = S->D32.alloc(mesh->D.n))) break;
+      if ((rc = S->D32.alloc(nD))) break;
       if ((rc = S->gllw32.alloc(mesh->gllw.n))) break;
+      if ((rc = S->T32.alloc(nT))) break;
       if ((rc = S->AqL32.alloc(NL))) break;
       if ((rc = S->p32.alloc(S->N))) break;
       if ((rc = S->x32.alloc(S->N))) break;
       if ((rc = S->r32.alloc(S->N))) break;
       if ((rc = S->bcopy.alloc(S->N))) break;
-      if ((rc = to_float(mesh->wJ.ptr, S->wJ32.ptr, ng, s))) break;
-      if ((rc = to_float(mesh->ggeo.ptr, S->ggeo32.ptr, 6 * ng, s))) break;
-      if ((rc = to_float(mesh->D.ptr, S->D32.ptr, mesh->D.n, s))) break;
+      if ((rc = to_float(o.wJ, S->wJ32.ptr, ng, s))) break;
+      if ((rc = to_float(o.ggeo, S->ggeo32.ptr, 6 * ng, s))) break;
+      if ((rc = to_float(o.D, S->D32.ptr, nD, s))) break;
       if ((rc = to_float(mesh->gllw.ptr, S->gllw32.ptr, mesh->gllw.n, s))) break;
+      if (nT && (rc = to_float(o.T, S->T32.ptr, nT, s))) break;
       if (S->precon == BP_PRECON_JACOBI) {
         if ((rc = S->invD32.alloc(S->N))) break;
         if ((rc = to_float(S->invD.ptr, S->invD32.ptr, S->N, s))) break;
@@ -637,8 +675,10 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
   bp_mesh_s* m = S->mesh;
   cudaStream_t s = default_stream();
   if (mode == BP_RHS_ANALYTIC) {
+    // BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
+    const double lam = S->bp <= 2 ? 0.0 : S->lambda;
     BP_TRY(launch_rhs_analytic(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->EZ.ptr, m->gllz.ptr,
-                               m->gllw.ptr, m->wJ.ptr, S->lambda, S->AqL.ptr, s));
+                               m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
   } else if (mode == BP_RHS_RANDOM) {
     DeviceArray<double> ftmp;
     double* f = f_out;
@@ -664,8 +704,13 @@ int bp_solver_diagonal(bp_solver_t S, double* diag) {
   if (!S || !diag) return fail(BP_ERROR_ARG, "bp_solver_diagonal: null pointer");
   bp_mesh_s* m = S->mesh;
   cudaStream_t s = default_stream();
-  BP_TRY(launch_diag_local(m->N, m->affine, m->Nfields, m->E, m->ggeo.ptr, m->wJ.ptr, m->gllw.ptr, m->D.ptr,
-                           S->lambda, S->AqL.ptr, s));
+  if (S->bp >= 5) {
+    BP_TRY(launch_diag_local(m->N, m->affine, m->Nfields, m->E, m->ggeo.ptr, m->wJ.ptr, m->gllw.ptr, m->D.ptr,
+                             S->lambda, S->AqL.ptr, s));
+  } else {
+    const ElemOperands<double> o = operands64(S);
+    BP_TRY(launch_diag_cub(S->ax, m->E, o.wJ, o.ggeo, o.T, m->cubDV.ptr, S->lambda, S->AqL.ptr, s));
+  }
   BP_TRY(launch_gather(m->Ngather, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, diag, s));
   BP_CUDA_TRY(cudaStreamSynchronize(s));
   return BP_SUCCESS;

@@ -79,7 +79,8 @@ int bp_event_elapsed_ms(bp_event_t start, bp_event_t end, float* ms);
  * ------------------------------------------------------------------------- */
 
 typedef struct bp_ax_desc {
-  int32_t bp;        /* benchmark problem: 5 (Nfields 1) or 6 (Nfields 3)         */
+  int32_t bp;        /* benchmark problem 1..6; odd: Nfields 1, even: Nfields 3;
+                        bp_ax_hex3d takes 5/6, bp_ax_cub_hex3d 1..4               */
   int32_t N;         /* polynomial degree 1..15 (p_N)                             */
   int32_t affine;    /* 1: per-element factors (bp5AxAffineHex3D)                 */
   int32_t Nfields;   /* 1 or 3 (p_Nfields)                                        */
@@ -98,6 +99,23 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                 const int32_t* GlobalToLocal, const double* wJ, const double* ggeo,
                 const double* gllw, const double* D, double lambda, const double* q,
                 double* Aq, bp_stream_t stream);
+
+/* Element-local over-integrated operators of BP1-BP4 on N+2 Gauss points per
+   direction, Aq[e] = A_e q[GlobalToLocal].  Replaces bp1AxHex3D / bp2AxHex3D
+   (mass, okl/bp1AxHex3D.okl, okl/bp2AxHex3D.okl), bp3AxHex3D / bp4AxHex3D
+   (stiffness + lambda mass, okl/bp3AxHex3D.okl:29-340, okl/bp4AxHex3D.okl) and
+   their Affine variants (okl/bp1AxAffineHex3D.okl:29-135,
+   okl/bp3AxAffineHex3D.okl:29-258).  Argument order follows the OKL signature
+   (okl/bp3AxHex3D.okl:29-41) minus the unused S; the arrays are those of
+   bp_cubature_view_t.  Curved mesh: cubwJ [E*cubNp], cubggeo [E*cubNp*6],
+   cubD [cubNq^2], cubInterp [cubNq*Nq]; affine mesh: cubwJ [E], cubggeo [E*6]
+   (the GLL wJ/ggeo), cubD the modal [Nq^2], invV [Nq^2] (BP3/BP4) or MM
+   [Nq^2] (BP1/BP2).  Arrays a form does not use may be NULL; BP1/BP2 ignore
+   lambda. */
+int bp_ax_cub_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                    const int32_t* GlobalToLocal, const double* cubwJ, const double* cubggeo, const double* cubD,
+                    const double* cubInterp, const double* invV, const double* MM, double lambda, const double* q,
+                    double* Aq, bp_stream_t stream);
 
 /* ogs Gather(Add, Trans): gv[r] = sum over c in row r of v[colIds[c]] in column
    order.  Replaces ogsOperator_t::Gather (libs/ogs/ogsOperator.cpp:160-188) and
@@ -200,6 +218,34 @@ int bp_mesh_create(const bp_box_desc_t* desc, bp_mesh_t* mesh);
    (meshBasis1D.cpp:218-264 JacobiGLL, :114-136 Dmatrix1D).
    bp_box_vertices: vertex coordinates EX/EY/EZ [E*8] with the seeded
    perturbation (meshSetupBoxHex3D.cpp:31-131). */
+/* Cubature data of the BP1-BP4 operators (device arrays), filled by
+   bp_mesh_cubature.  Replaces mesh_t::CubatureSetupHex3D
+   (libs/mesh/meshCubatureSetupHex3D.cpp:31-258). */
+typedef struct bp_cubature_view {
+  int32_t cubNq, cubNp;     /* N+2 Gauss points per direction, cubNq^3          */
+  const double* cubr;       /* [cubNq] Gauss points                              */
+  const double* cubw;       /* [cubNq] Gauss weights                             */
+  const double* cubInterp;  /* [cubNq*Nq] GLL -> Gauss interpolation             */
+  const double* cubD;       /* curved [cubNq^2] on the Gauss points; affine the
+                               modal invV*Vr [Nq^2]                              */
+  const double* invV;       /* [Nq^2] inverse orthonormal-Legendre Vandermonde   */
+  const double* MM;         /* [Nq^2] exact GLL mass matrix                      */
+  const double* cubwJ;      /* curved [E*cubNp] J*w_i*w_j*w_k; affine = wJ [E]   */
+  const double* cubggeo;    /* curved [E*cubNp*6]; affine = ggeo [E*6]           */
+} bp_cubature_view_t;
+
+/* Set up (once; later calls return at once) the cubature of a mesh: the 1D
+   data and, for a curved mesh, the factors at the Gauss points
+   (7*8*E*cubNp bytes of device memory). */
+int bp_mesh_cubature(bp_mesh_t mesh);
+int bp_mesh_cubature_view(bp_mesh_t mesh, bp_cubature_view_t* view);
+
+/* Host-only 1D cubature data for degree N (meshCubatureSetupHex3D.cpp:31-51,
+   meshBasis1D.cpp JacobiGQ / InterpolationMatrix1D / Dmatrix1D / MassMatrix1D):
+   r, w [N+2], I [(N+2)*(N+1)], D [(N+2)^2], invV, Dmodal, MM [(N+1)^2]. */
+int bp_basis_cubature(int32_t N, double* r, double* w, double* I, double* D, double* invV, double* Dmodal,
+                      double* MM);
+
 int bp_box_numbering(const bp_box_desc_t* desc, int32_t* Ngather, int32_t* nnz, int32_t* GlobalToLocal,
                      int32_t* rowStarts, int32_t* colIds);
 int bp_basis_gll(int32_t N, double* z, double* w, double* D);
@@ -222,7 +268,7 @@ typedef struct bp_solver_s* bp_solver_t;
 #define BP_PRECISION_MIXED 1   /* FP32 CG with FP64 reliable updates (extension)          */
 
 typedef struct bp_solver_desc {
-  int32_t bp;          /* 5 (scalar) or 6 (vector, mesh Nfields must be 3)        */
+  int32_t bp;          /* 1..6; BP2/BP4/BP6 need a 3-field mesh, BP1/3/5 one field  */
   double lambda;       /* 1.0 for BP3-BP6 (BP/BP5/bp5Main.cpp:47)                   */
   int32_t precon;      /* BP_PRECON_NONE (reference) or BP_PRECON_JACOBI             */
   int32_t precision;   /* BP_PRECISION_FP64 or BP_PRECISION_MIXED                    */

@@ -334,6 +334,12 @@ struct bpo_mesh {
   dlong Ngather, nnz;
   std::vector<dlong> rowStarts, colIds, G2L, blockRowStarts;
   std::vector<dlong> elementList;
+  // cubature for BP1-BP4 (cubNq = N+2 Gauss points), set up on first use
+  int cubNq = 0, cubNp = 0;
+  std::vector<double> cubr, cubw, cubInterp;   // cubInterp [cubNq*Nq]
+  std::vector<double> cubD;                    // curved: [cubNq^2]; affine: modal [Nq^2]
+  std::vector<double> invV;                    // affine: inverse Legendre Vandermonde [Nq^2]
+  std::vector<double> cubwJ, cubggeo;          // curved: [E*cubNp], [6*E*cubNp]; affine: wJ, ggeo
 };
 
 static const int kFaceVertices[6][4] = {{0, 1, 2, 3}, {0, 4, 5, 1}, {1, 5, 6, 2},
@@ -743,9 +749,13 @@ extern "C" int64_t bpo_mesh_int(const bpo_mesh* m, const char* name) {
   return -1;
 }
 
-/* Returns a pointer to a named array and its length (elements). */
+static void ensure_cubature(bpo_mesh& m);
+
+/* Returns a pointer to a named array and its length (elements).  Asking for a
+   cubature array sets the cubature up. */
 extern "C" const void* bpo_mesh_array(const bpo_mesh* m, const char* name, int64_t* len) {
   std::string s(name);
+  if (s.rfind("cub", 0) == 0 || s == "invV") ensure_cubature(*const_cast<bpo_mesh*>(m));
 #define RET(vec) do { *len = (int64_t)(vec).size(); return (const void*)(vec).data(); } while (0)
   if (s == "gllz") RET(m->gllz);
   if (s == "gllw") RET(m->gllw);
@@ -768,6 +778,13 @@ extern "C" const void* bpo_mesh_array(const bpo_mesh* m, const char* name, int64
   if (s == "G2L") RET(m->G2L);
   if (s == "blockRowStarts") RET(m->blockRowStarts);
   if (s == "elementList") RET(m->elementList);
+  if (s == "cubr") RET(m->cubr);
+  if (s == "cubw") RET(m->cubw);
+  if (s == "cubInterp") RET(m->cubInterp);
+  if (s == "cubD") RET(m->cubD);
+  if (s == "invV") RET(m->invV);
+  if (s == "cubwJ") RET(m->cubwJ);
+  if (s == "cubggeo") RET(m->cubggeo);
 #undef RET
   *len = -1;   // unknown name
   return nullptr;
@@ -1004,6 +1021,316 @@ extern "C" void bpo_jacobi_diag_bp5(const bpo_mesh* m, double lambda, double* di
 }
 
 /* ------------------------------------------------------------------------ */
+/* cubature and the over-integrated operators (BP1-BP4)                       */
+/* ------------------------------------------------------------------------ */
+
+/* CubatureSetupHex3D, libs/mesh/meshCubatureSetupHex3D.cpp:31-258.
+   cubNq = N+2 Gauss points (JacobiGQ(0,0,N+1)) and the GLL->Gauss
+   interpolation cubInterp [cubNq x Nq].
+   Affine mesh: the reference's affine kernels work in the orthonormal
+   Legendre (modal) basis instead: invV = V^-1 [Nq x Nq] and the modal
+   differentiation matrix cubD = invV * Vr [Nq x Nq]; cubwJ and cubggeo are the
+   per-element wJ and ggeo (no weights: the modal mass matrix is I).
+   Curved mesh: cubD differentiates on the Gauss points [cubNq x cubNq]; the
+   nine GLL-node derivatives of x, y, z are interpolated to the Gauss points
+   (i, then j, then k) and cubwJ, cubggeo formed there with the Gauss weights. */
+static void ensure_cubature(bpo_mesh& m) {
+  if (m.cubNq) return;
+  const int Nq = m.Nq, Np = m.Np, cNq = m.N + 2, cNp = cNq * cNq * cNq;
+  m.cubr.resize(cNq); m.cubw.resize(cNq);
+  bpo_jacobi_gq(0, 0, m.N + 1, m.cubr.data(), m.cubw.data());
+  m.cubInterp.resize(cNq * Nq);
+  bpo_interp_matrix1d(m.N, m.gllz.data(), cNq, m.cubr.data(), m.cubInterp.data());
+  if (m.affine) {
+    std::vector<double> Vr;
+    grad_vandermonde1d(m.N, m.gllz, Vr);
+    vandermonde1d(m.N, m.gllz, m.invV);
+    dense_inverse(Nq, m.invV);
+    m.cubD.assign(Nq * Nq, 0.0);
+    for (int n = 0; n < Nq; ++n)
+      for (int mm = 0; mm < Nq; ++mm) {
+        double acc = 0;
+        for (int k = 0; k < Nq; ++k) acc += m.invV[n * Nq + k] * Vr[k * Nq + mm];
+        m.cubD[n * Nq + mm] = acc;
+      }
+    m.cubwJ = m.wJ;
+    m.cubggeo = m.ggeo;
+    m.cubNp = cNp; m.cubNq = cNq;
+    return;
+  }
+  m.cubD.resize(cNq * cNq);
+  bpo_dmatrix1d(m.N + 1, m.cubr.data(), cNq, m.cubr.data(), m.cubD.data());
+  m.cubwJ.assign((size_t)m.E * cNp, 0.0);
+  m.cubggeo.assign((size_t)6 * m.E * cNp, 0.0);
+  const double* I = m.cubInterp.data();
+  const int n1 = Nq * Nq * cNq, n2 = Nq * cNq * cNq;
+#pragma omp parallel
+  {
+    std::vector<double> d(9 * (size_t)Np), d1(9 * (size_t)n1), d2(9 * (size_t)n2);
+    const std::vector<double>* X[3] = {&m.x, &m.y, &m.z};
+#pragma omp for
+    for (dlong e = 0; e < m.E; ++e) {
+      // d[comp][n], comp = 3*coordinate + direction: xr xs xt yr ys yt zr zs zt
+      for (int k = 0; k < Nq; ++k)
+        for (int j = 0; j < Nq; ++j)
+          for (int i = 0; i < Nq; ++i) {
+            const int n = i + j * Nq + k * Nq * Nq;
+            for (int c = 0; c < 3; ++c) {
+              const double* xe = X[c]->data() + (size_t)e * Np;
+              double r = 0, sd = 0, t = 0;
+              for (int mm = 0; mm < Nq; ++mm) {
+                r += m.D[i * Nq + mm] * xe[k * Nq * Nq + j * Nq + mm];
+                sd += m.D[j * Nq + mm] * xe[k * Nq * Nq + mm * Nq + i];
+                t += m.D[k * Nq + mm] * xe[mm * Nq * Nq + j * Nq + i];
+              }
+              d[(3 * c + 0) * Np + n] = r;
+              d[(3 * c + 1) * Np + n] = sd;
+              d[(3 * c + 2) * Np + n] = t;
+            }
+          }
+      for (int comp = 0; comp < 9; ++comp) {
+        const double* f = &d[(size_t)comp * Np];
+        double* f1 = &d1[(size_t)comp * n1];
+        double* f2 = &d2[(size_t)comp * n2];
+        for (int k = 0; k < Nq; ++k)
+          for (int j = 0; j < Nq; ++j)
+            for (int i = 0; i < cNq; ++i) {
+              double acc = 0;
+              for (int n = 0; n < Nq; ++n) acc += I[i * Nq + n] * f[k * Nq * Nq + j * Nq + n];
+              f1[k * Nq * cNq + j * cNq + i] = acc;
+            }
+        for (int k = 0; k < Nq; ++k)
+          for (int j = 0; j < cNq; ++j)
+            for (int i = 0; i < cNq; ++i) {
+              double acc = 0;
+              for (int n = 0; n < Nq; ++n) acc += I[j * Nq + n] * f1[k * Nq * cNq + n * cNq + i];
+              f2[k * cNq * cNq + j * cNq + i] = acc;
+            }
+      }
+      for (int k = 0; k < cNq; ++k)
+        for (int j = 0; j < cNq; ++j)
+          for (int i = 0; i < cNq; ++i) {
+            double v[9];
+            for (int comp = 0; comp < 9; ++comp) {
+              double acc = 0;
+              for (int n = 0; n < Nq; ++n) acc += I[k * Nq + n] * d2[(size_t)comp * n2 + n * cNq * cNq + j * cNq + i];
+              v[comp] = acc;
+            }
+            const double xr = v[0], xs = v[1], xt = v[2], yr = v[3], ys = v[4], yt = v[5];
+            const double zr = v[6], zs = v[7], zt = v[8];
+            const double J = xr * (ys * zt - zs * yt) - yr * (xs * zt - zs * xt) + zr * (xs * yt - ys * xt);
+            const double rx = (ys * zt - zs * yt) / J, ry = -(xs * zt - zs * xt) / J, rz = (xs * yt - ys * xt) / J;
+            const double sx = -(yr * zt - zr * yt) / J, sy = (xr * zt - zr * xt) / J, sz = -(xr * yt - yr * xt) / J;
+            const double tx = (yr * zs - zr * ys) / J, ty = -(xr * zs - zr * xs) / J, tz = (xr * ys - yr * xs) / J;
+            const double JW = J * m.cubw[i] * m.cubw[j] * m.cubw[k];
+            const size_t id = (size_t)e * cNp + i + j * cNq + k * cNq * cNq;
+            m.cubwJ[id] = JW;
+            double* g = &m.cubggeo[6 * id];
+            g[0] = JW * (rx * rx + ry * ry + rz * rz);
+            g[1] = JW * (rx * sx + ry * sy + rz * sz);
+            g[2] = JW * (rx * tx + ry * ty + rz * tz);
+            g[3] = JW * (sx * sx + sy * sy + sz * sz);
+            g[4] = JW * (sx * tx + sy * ty + sz * tz);
+            g[5] = JW * (tx * tx + ty * ty + tz * tz);
+          }
+    }
+  }
+  m.cubNp = cNp; m.cubNq = cNq;
+}
+
+/* Apply a 1D matrix A [no x ni] along one direction of a 3D field
+   in[n2][n1][n0] (n0 fastest): dir 0 maps n0 -> no, 1 maps n1, 2 maps n2.
+   out(...,o,...) = sum_i A[o*ni + i] * in(...,i,...) (AT: A[i*no + o]). */
+static void apply1d(const double* A, bool AT, int no, int ni, int dir, const int dims[3], const double* in,
+                    double* out) {
+  int od[3] = {dims[0], dims[1], dims[2]};
+  od[dir] = no;
+  for (int c = 0; c < od[2]; ++c)
+    for (int b = 0; b < od[1]; ++b)
+      for (int a = 0; a < od[0]; ++a) {
+        const int o = dir == 0 ? a : dir == 1 ? b : c;
+        double acc = 0;
+        for (int i = 0; i < ni; ++i) {
+          const int ia = dir == 0 ? i : a, ib = dir == 1 ? i : b, ic = dir == 2 ? i : c;
+          acc += (AT ? A[i * no + o] : A[o * ni + i]) * in[(ic * dims[1] + ib) * dims[0] + ia];
+        }
+        out[(c * od[1] + b) * od[0] + a] = acc;
+      }
+}
+
+/* Three 1D applications in the order b (dir 1), a (dir 0), c (dir 2), the
+   order of the reference's interpolation and projection stages
+   (okl/bp3AxHex3D.okl:77-161 and :258-338). */
+static void apply3d(const double* A, bool AT, int no, int ni, const double* in, double* out) {
+  std::vector<double> t1((size_t)ni * no * ni), t2((size_t)ni * no * no);
+  const int d0[3] = {ni, ni, ni};
+  apply1d(A, AT, no, ni, 1, d0, in, t1.data());
+  const int d1[3] = {ni, no, ni};
+  apply1d(A, AT, no, ni, 0, d1, t1.data(), t2.data());
+  const int d2[3] = {no, no, ni};
+  apply1d(A, AT, no, ni, 2, d2, t2.data(), out);
+}
+
+/* Stiffness (plus lambda*mass) on a tensor grid of n^3 points with the 1D
+   differentiation matrix Dm: gradient, the symmetric factor G (6 per point
+   or per element), lambda*wJ*q, weak divergence with Dm^T; the loop
+   structure of okl/bp3AxHex3D.okl:164-245. */
+static void stiffness_grid(int n, const double* Dm, const double* G, const double* wJ, bool per_point,
+                           double lambda, const double* q, double* r) {
+  std::vector<double> qr(n * n * n), qs(n * n * n), qt(n * n * n);
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        const int id = i + j * n + k * n * n;
+        const double* g = per_point ? &G[6 * id] : G;
+        const double w = per_point ? wJ[id] : wJ[0];
+        double dr = 0, ds = 0, dt = 0;
+        for (int l = 0; l < n; ++l) {
+          dr += Dm[i * n + l] * q[k * n * n + j * n + l];
+          ds += Dm[j * n + l] * q[k * n * n + l * n + i];
+          dt += Dm[k * n + l] * q[l * n * n + j * n + i];
+        }
+        qr[id] = g[0] * dr + g[1] * ds + g[2] * dt;
+        qs[id] = g[1] * dr + g[3] * ds + g[4] * dt;
+        qt[id] = g[2] * dr + g[4] * ds + g[5] * dt;
+        r[id] = lambda * w * q[id];
+      }
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        double acc = 0;
+        for (int l = 0; l < n; ++l) {
+          acc += Dm[l * n + i] * qr[k * n * n + j * n + l];
+          acc += Dm[l * n + j] * qs[k * n * n + l * n + i];
+          acc += Dm[l * n + k] * qt[l * n * n + j * n + i];
+        }
+        r[i + j * n + k * n * n] += acc;
+      }
+}
+
+/* Element operators of BP1/BP2 (mass) and BP3/BP4 (stiffness + lambda mass)
+   with over-integration, one field:
+   - curved, BP3 (okl/bp3AxHex3D.okl:29-340): q -> Gauss points (I in b, a, c),
+     stiffness_grid on cubNq^3 with cubD, cubggeo, cubwJ, project with I^T;
+   - curved, BP1 (okl/bp1AxHex3D.okl): the same with cubwJ*q only;
+   - affine, BP3 (okl/bp3AxAffineHex3D.okl:29-258): q -> modal (invV in b, a, c),
+     stiffness_grid on Nq^3 with the modal cubD and the per-element ggeo,
+     wJ, back with invV^T;
+   - affine, BP1 (okl/bp1AxAffineHex3D.okl:29-135): wJ * (MM x MM x MM) q,
+     applied in r, s, t order. */
+static void ax_cub_e(const bpo_mesh& m, dlong e, bool stiff, double lambda, const double* q, double* AqL, int f) {
+  const int Nq = m.Nq, Np = m.Np, Nf = m.Nfields, cNq = m.cubNq, cNp = m.cubNp;
+  const size_t lbase = (size_t)e * Np * Nf + (size_t)f * Np;
+  std::vector<double> qn(Np), rn(Np);
+  for (int n = 0; n < Np; ++n) {
+    const dlong id = m.G2L[lbase + n];
+    qn[n] = (id != -1) ? q[id] : 0.0;
+  }
+  if (m.affine && !stiff) {
+    std::vector<double> t1(Np), t2(Np);
+    const int dims[3] = {Nq, Nq, Nq};
+    apply1d(m.MM.data(), true, Nq, Nq, 0, dims, qn.data(), t1.data());
+    apply1d(m.MM.data(), true, Nq, Nq, 1, dims, t1.data(), t2.data());
+    apply1d(m.MM.data(), true, Nq, Nq, 2, dims, t2.data(), rn.data());
+    for (int n = 0; n < Np; ++n) AqL[lbase + n] = m.cubwJ[e] * rn[n];
+    return;
+  }
+  if (m.affine) {
+    std::vector<double> qh(Np), rh(Np);
+    apply3d(m.invV.data(), false, Nq, Nq, qn.data(), qh.data());
+    stiffness_grid(Nq, m.cubD.data(), &m.cubggeo[6 * (size_t)e], &m.cubwJ[e], false, lambda, qh.data(), rh.data());
+    apply3d(m.invV.data(), true, Nq, Nq, rh.data(), rn.data());
+    for (int n = 0; n < Np; ++n) AqL[lbase + n] = rn[n];
+    return;
+  }
+  std::vector<double> qc(cNp), rc(cNp);
+  apply3d(m.cubInterp.data(), false, cNq, Nq, qn.data(), qc.data());
+  if (stiff) {
+    stiffness_grid(cNq, m.cubD.data(), &m.cubggeo[6 * (size_t)e * cNp], &m.cubwJ[(size_t)e * cNp], true, lambda,
+                   qc.data(), rc.data());
+  } else {
+    for (int n = 0; n < cNp; ++n) rc[n] = m.cubwJ[(size_t)e * cNp + n] * qc[n];
+  }
+  apply3d(m.cubInterp.data(), true, Nq, cNq, rc.data(), rn.data());
+  for (int n = 0; n < Np; ++n) AqL[lbase + n] = rn[n];
+}
+
+/* Element-local operator of benchmark problem bp (1..6) on every field of the
+   mesh: BP1/BP2 mass, BP3/BP4 over-integrated stiffness, BP5/BP6 collocated
+   stiffness (bpo_ax_bp5).  BP1/BP2 ignore lambda, as bp1AxHex3D has none. */
+extern "C" void bpo_ax(bpo_mesh* m, int bp, double lambda, const double* q, double* AqL) {
+  if (bp >= 5) { bpo_ax_bp5(m, lambda, q, AqL); return; }
+  ensure_cubature(*m);
+  const bool stiff = bp >= 3;
+#pragma omp parallel for schedule(static)
+  for (dlong e = 0; e < m->E; ++e)
+    for (int f = 0; f < m->Nfields; ++f) ax_cub_e(*m, e, stiff, lambda, q, AqL, f);
+}
+
+/* bpN_t::Operator (BP/BP3/src/bp3Operator.cpp:29-85 and its siblings) at one
+   rank: the element operator, then the Trans gather. */
+extern "C" void bpo_operator(bpo_mesh* m, int bp, double lambda, const double* q, double* Aq) {
+  std::vector<double> AqL((size_t)m->E * m->Np * m->Nfields);
+  bpo_ax(m, bp, lambda, q, AqL.data());
+  bpo_gather(m, AqL.data(), Aq);
+}
+
+/* Assembled diagonal of the BP1-BP4 operators (extension for Jacobi CG).  The
+   element matrix is B^T W B with B a tensor product of 1D matrices, so the
+   diagonal entry at node (a,b,c) is a sum over the quadrature grid of W times
+   products of one 1D column per direction:
+   curved:  columns of I (value) and DI = cubD I (derivative) over cubNq points;
+   affine:  BP1 exact, wJ MM[a][a] MM[b][b] MM[c][c]; BP3 over the modal grid
+            with columns of invV and cubD invV. */
+static void jacobi_diag_cub(bpo_mesh& m, int bp, double lambda, double* diag) {
+  ensure_cubature(m);
+  const int Nq = m.Nq, Np = m.Np, Nf = m.Nfields;
+  const bool stiff = bp >= 3;
+  const bool aff = m.affine != 0;
+  const int n = aff ? Nq : m.cubNq;   // quadrature grid points per direction
+  const double* V = aff ? m.invV.data() : m.cubInterp.data();   // [n x Nq]
+  std::vector<double> DV(n * Nq, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int a = 0; a < Nq; ++a) {
+      double acc = 0;
+      for (int l = 0; l < n; ++l) acc += m.cubD[i * n + l] * V[l * Nq + a];
+      DV[i * Nq + a] = acc;
+    }
+  std::vector<double> dL((size_t)m.E * Np * Nf);
+#pragma omp parallel for
+  for (dlong e = 0; e < m.E; ++e)
+    for (int c = 0; c < Nq; ++c)
+      for (int b = 0; b < Nq; ++b)
+        for (int a = 0; a < Nq; ++a) {
+          double d = 0.0;
+          if (aff && !stiff) {
+            d = m.cubwJ[e] * m.MM[a * Nq + a] * m.MM[b * Nq + b] * m.MM[c * Nq + c];
+          } else {
+            for (int k = 0; k < n; ++k)
+              for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                  const size_t id = aff ? (size_t)e : (size_t)e * m.cubNp + i + j * n + k * n * n;
+                  const double Vi = V[i * Nq + a], Vj = V[j * Nq + b], Vk = V[k * Nq + c];
+                  const double mass = m.cubwJ[id] * Vi * Vi * Vj * Vj * Vk * Vk;
+                  if (!stiff) { d += mass; continue; }
+                  const double gr = DV[i * Nq + a] * Vj * Vk, gs = Vi * DV[j * Nq + b] * Vk;
+                  const double gt = Vi * Vj * DV[k * Nq + c];
+                  const double* g = &m.cubggeo[6 * id];
+                  d += g[0] * gr * gr + g[3] * gs * gs + g[5] * gt * gt + 2 * g[1] * gr * gs + 2 * g[2] * gr * gt +
+                       2 * g[4] * gs * gt + lambda * mass;
+                }
+          }
+          for (int f = 0; f < Nf; ++f) dL[(size_t)e * Np * Nf + (size_t)f * Np + a + b * Nq + c * Nq * Nq] = d;
+        }
+  bpo_gather(&m, dL.data(), diag);
+}
+
+extern "C" void bpo_jacobi_diag(bpo_mesh* m, int bp, double lambda, double* diag) {
+  if (bp >= 5) bpo_jacobi_diag_bp5(m, lambda, diag);
+  else jacobi_diag_cub(*m, bp, lambda, diag);
+}
+
+/* ------------------------------------------------------------------------ */
 /* reductions in the reference's device order                                 */
 /* ------------------------------------------------------------------------ */
 /* Two-stage block tree: stage 1 as innerProd_1/norm2_1/updateCG_1
@@ -1044,12 +1371,13 @@ static double tree_reduce(dlong N, int bs, F term) {
    its stop rule rdotr <= max(tol^2 rdotr0, tol^2).  r holds b on entry and the
    final residual on exit.  hist_rnorm/hist_alpha (length >= maxit) receive
    sqrt(rdotr) and alpha of every iteration; returns the iteration count. */
-extern "C" int bpo_cg(const bpo_mesh* m, double lambda, double* x, double* r, double tol, int maxit,
-                      int precon, const double* invDiag, double* hist_rnorm, double* hist_alpha) {
+extern "C" int bpo_cg_bp(bpo_mesh* m, int bp, double lambda, double* x, double* r, double tol, int maxit,
+                         int precon, const double* invDiag, double* hist_rnorm, double* hist_alpha) {
   const dlong N = m->Ngather;
+  auto op = [m, bp, lambda](const double* q, double* Aq) { bpo_operator(m, bp, lambda, q, Aq); };
   std::vector<double> p(N, 0.0), Ap(N, 0.0), z;
   if (precon) z.assign(N, 0.0);
-  bpo_operator_bp5(m, lambda, x, Ap.data());
+  op(x, Ap.data());
 #pragma omp parallel for
   for (dlong n = 0; n < N; ++n) r[n] = -1.0 * Ap[n] + 1.0 * r[n];
   if (!precon) {
@@ -1065,7 +1393,7 @@ extern "C" int bpo_cg(const bpo_mesh* m, double lambda, double* x, double* r, do
       const double beta = (iter == 0) ? 0.0 : rdotr1 / rdotr2;
 #pragma omp parallel for
       for (dlong n = 0; n < N; ++n) p[n] = 1.0 * r[n] + beta * p[n];
-      bpo_operator_bp5(m, lambda, p.data(), Ap.data());
+      op(p.data(), Ap.data());
       const double pAp = tree_reduce(N, 256, [&](dlong i) { return p[i] * Ap[i]; });
       const double alpha = rdotr1 / pAp;
       rdotr = tree_reduce(N, 512, [&](dlong i) {
@@ -1091,7 +1419,7 @@ extern "C" int bpo_cg(const bpo_mesh* m, double lambda, double* x, double* r, do
     const double beta = (iter == 0) ? 0.0 : rz / rz_old;
 #pragma omp parallel for
     for (dlong n = 0; n < N; ++n) p[n] = z[n] + beta * p[n];
-    bpo_operator_bp5(m, lambda, p.data(), Ap.data());
+    op(p.data(), Ap.data());
     const double pAp = tree_reduce(N, 256, [&](dlong i) { return p[i] * Ap[i]; });
     const double alpha = rz / pAp;
 #pragma omp parallel for
@@ -1103,6 +1431,12 @@ extern "C" int bpo_cg(const bpo_mesh* m, double lambda, double* x, double* r, do
     if (hist_alpha) hist_alpha[iter] = alpha;
   }
   return iter;
+}
+
+/* BP5/BP6 CG (the operator by the mesh's field count) */
+extern "C" int bpo_cg(bpo_mesh* m, double lambda, double* x, double* r, double tol, int maxit, int precon,
+                      const double* invDiag, double* hist_rnorm, double* hist_alpha) {
+  return bpo_cg_bp(m, 5, lambda, x, r, tol, maxit, precon, invDiag, hist_rnorm, hist_alpha);
 }
 
 extern "C" int bpo_num_threads(void) {

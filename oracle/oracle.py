@@ -54,6 +54,12 @@ def lib():
         L.bpo_cg.restype = ctypes.c_int
         L.bpo_cg.argtypes = [ctypes.c_void_p, ctypes.c_double, _c_dp, _c_dp, ctypes.c_double,
                              ctypes.c_int, ctypes.c_int, _c_dp, _c_dp, _c_dp]
+        L.bpo_ax.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _c_dp, _c_dp]
+        L.bpo_operator.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _c_dp, _c_dp]
+        L.bpo_jacobi_diag.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _c_dp]
+        L.bpo_cg_bp.restype = ctypes.c_int
+        L.bpo_cg_bp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _c_dp, _c_dp, ctypes.c_double,
+                                ctypes.c_int, ctypes.c_int, _c_dp, _c_dp, _c_dp]
         L.bpo_num_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -108,6 +114,8 @@ _DTYPES = {
     "z": np.float64, "wJ": np.float64, "ggeo": np.float64, "maskedIds": np.int64,
     "rowStarts": np.int32, "colIds": np.int32, "G2L": np.int32,
     "blockRowStarts": np.int32, "elementList": np.int32,
+    "cubr": np.float64, "cubw": np.float64, "cubInterp": np.float64, "cubD": np.float64,
+    "invV": np.float64, "cubwJ": np.float64, "cubggeo": np.float64,
 }
 
 
@@ -153,11 +161,16 @@ class Mesh:
     def NL(self):
         return self.E * self.Np * self.Nfields
 
-    def ax(self, q, lam=1.0):
-        """Element-local BP5/BP6 operator AqL = A_e q[G2L]."""
+    def ax(self, q, lam=1.0, bp=5):
+        """Element-local operator AqL = A_e q[G2L] of benchmark problem bp:
+        1/2 mass, 3/4 over-integrated stiffness, 5/6 collocated stiffness
+        (the field count comes from the mesh)."""
         q = np.ascontiguousarray(q, dtype=np.float64)
         out = np.empty(self.NL)
-        lib().bpo_ax_bp5(self._h, lam, _dp(q), _dp(out))
+        if bp >= 5:
+            lib().bpo_ax_bp5(self._h, lam, _dp(q), _dp(out))
+        else:
+            lib().bpo_ax(self._h, bp, lam, _dp(q), _dp(out))
         return out
 
     def gather(self, v):
@@ -172,10 +185,10 @@ class Mesh:
         lib().bpo_scatter(self._h, _dp(gv), _dp(out))
         return out
 
-    def operator(self, q, lam=1.0):
+    def operator(self, q, lam=1.0, bp=5):
         q = np.ascontiguousarray(q, dtype=np.float64)
         out = np.empty(self.Ngather)
-        lib().bpo_operator_bp5(self._h, lam, _dp(q), _dp(out))
+        lib().bpo_operator(self._h, bp, lam, _dp(q), _dp(out))
         return out
 
     def rhs_analytic(self, lam=1.0):
@@ -190,20 +203,21 @@ class Mesh:
         lib().bpo_rhs_random(self._h, seed, _dp(f), _dp(b))
         return f, b
 
-    def jacobi_diag(self, lam=1.0):
+    def jacobi_diag(self, lam=1.0, bp=5):
         d = np.empty(self.Ngather)
-        lib().bpo_jacobi_diag_bp5(self._h, lam, _dp(d))
+        lib().bpo_jacobi_diag(self._h, bp, lam, _dp(d))
         return d
 
-    def cg(self, b, lam=1.0, tol=0.0, maxit=100, precon=False, x0=None):
+    def cg(self, b, lam=1.0, tol=0.0, maxit=100, precon=False, x0=None, bp=5):
         """cg::Solve.  Returns (x, r_final, iterations, rnorm_history, alpha_history)."""
         x = np.zeros(self.Ngather) if x0 is None else np.array(x0, dtype=np.float64)
         r = np.array(b, dtype=np.float64)
         hr = np.zeros(maxit); ha = np.zeros(maxit)
         inv = None
         if precon:
-            inv = 1.0 / self.jacobi_diag(lam)
-        it = lib().bpo_cg(self._h, lam, _dp(x), _dp(r), tol, maxit, int(bool(precon)), _dp(inv), _dp(hr), _dp(ha))
+            inv = 1.0 / self.jacobi_diag(lam, bp)
+        it = lib().bpo_cg_bp(self._h, bp, lam, _dp(x), _dp(r), tol, maxit, int(bool(precon)), _dp(inv),
+                             _dp(hr), _dp(ha))
         return x, r, it, hr[:it], ha[:it]
 
 

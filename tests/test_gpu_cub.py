@@ -1,0 +1,119 @@
+"""GPU parity of the over-integrated operators (BP1-BP4) against the oracle.
+
+Same bars as the BP5/BP6 path: element operator, assembled operator and
+diagonal within 1e-12 relative in FP64, cubature factors within 1e-13, CG
+residual history within 1e-10 relative per iteration while the residual is
+above 1e-6 of its start.
+"""
+import numpy as np
+import pytest
+
+from test_gpu_parity import HIST_TOL, _check_history, _rel
+
+pytestmark = pytest.mark.gpu
+
+AX_TOL = 1e-12
+
+CUB_AX_CASES = ([(2, 2, 2, N, aff, 0.0 if aff else 0.1, bp) for N in (1, 2, 3, 4, 5, 6, 7, 8, 9, 11, 13, 15)
+                 for aff in (False, True) for bp in (1, 3)] +
+                [(2, 3, 2, N, aff, 0.0 if aff else 0.1, bp) for N in (1, 4, 7, 10, 15) for aff in (False, True)
+                 for bp in (2, 4)] + [(3, 2, 2, 7, False, 0.2, 3), (4, 3, 2, 5, False, 0.1, 1)])
+
+
+@pytest.mark.parametrize("nx,ny,nz,N,affine,pert,bp", CUB_AX_CASES)
+def test_cub_ax_matches_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, bp):
+    Nf = 1 if bp % 2 else 3
+    om = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, Nfields=Nf, pert=pert)
+    # cubature data set up on the device against the oracle's restatement
+    for name, tol in (("cubr", 1e-15), ("cubw", 1e-14), ("cubInterp", 1e-13), ("cubD", 1e-13)):
+        assert _rel(gm.array(name), om.array(name)) < tol, name
+    if affine:
+        assert _rel(gm.array("invV"), om.array("invV")) < 1e-13
+    else:
+        assert _rel(gm.array("cubwJ"), om.array("cubwJ")) < 1e-13
+        assert _rel(gm.array("cubggeo"), om.array("cubggeo")) < 1e-13
+    if om.Ngather == 0:
+        return
+    q = 2 * oracle.random(5, om.Ngather) - 1
+    dq, dAq = gpu.DeviceBuffer.from_host(q), gpu.DeviceBuffer(om.NL)
+    gpu.ax_cub_hex3d(gm, bp, dq, dAq, lam=1.0)
+    assert _rel(dAq.download(), om.ax(q, 1.0, bp)) < AX_TOL
+
+
+@pytest.mark.parametrize("bp,affine,pert", [(1, False, 0.1), (1, True, 0.0), (2, False, 0.1), (3, False, 0.1),
+                                            (3, True, 0.0), (4, False, 0.0), (4, True, 0.0)])
+def test_cub_operator_forcing_and_diagonal(gpu, oracle, bp, affine, pert):
+    Nf = 1 if bp % 2 else 3
+    om = oracle.Mesh(3, 3, 2, 4, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(3, 3, 2, N=4, affine=affine, Nfields=Nf, pert=pert)
+    S = gpu.BP(gm, bp=bp)
+    q = 2 * oracle.random(3, om.Ngather) - 1
+    dq, dAq = gpu.DeviceBuffer.from_host(q), gpu.DeviceBuffer(om.Ngather)
+    S.operator(dq, dAq)
+    assert _rel(dAq.download(), om.operator(q, 1.0, bp)) < AX_TOL
+    # BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
+    lam_rhs = 0.0 if bp <= 2 else 1.0
+    assert _rel(S.rhs("ANALYTIC").download(), om.rhs_analytic(lam_rhs)) < 1e-12
+    assert _rel(S.diagonal().download(), om.jacobi_diag(1.0, bp)) < 1e-12
+
+
+CUB_CG_CASES = [(3, 6, 6, 6, 5, False, 0.1, "NONE"), (3, 6, 6, 6, 5, False, 0.1, "JACOBI"),
+                (3, 8, 8, 8, 3, True, 0.0, "NONE"), (3, 3, 3, 3, 9, False, 0.1, "JACOBI"),
+                (1, 6, 6, 6, 5, False, 0.1, "NONE"), (1, 5, 5, 5, 4, True, 0.0, "JACOBI"),
+                (4, 4, 4, 4, 4, False, 0.1, "JACOBI"), (2, 4, 4, 4, 3, False, 0.1, "NONE")]
+
+
+@pytest.mark.parametrize("bp,nx,ny,nz,N,affine,pert,precon", CUB_CG_CASES)
+def test_cub_cg_history_matches_oracle(gpu, oracle, bp, nx, ny, nz, N, affine, pert, precon):
+    Nf = 1 if bp % 2 else 3
+    om = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, Nfields=Nf, pert=pert)
+    S = gpu.BP(gm, bp=bp, precon=precon)
+    b_o = om.rhs_random(0)[1]
+    maxit = 60
+    x_o, r_o, it_o, hr_o, ha_o = om.cg(b_o, 1.0, 0.0, maxit, precon=(precon == "JACOBI"), bp=bp)
+    x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
+    st, hr, ha = S.solve(x, S.rhs("RANDOM", 0), tol=0.0, maxit=maxit)
+    assert st.iterations == it_o == maxit
+    live = _check_history(hr, hr_o)
+    assert np.all((np.abs(ha - ha_o) / np.abs(ha_o))[live] < HIST_TOL)
+    assert _rel(x.download(), x_o) < 1e-9
+
+
+@pytest.mark.parametrize("bp,affine,pert", [(3, False, 0.1), (1, False, 0.1), (4, True, 0.0)])
+def test_cub_mixed_precision_reaches_tolerance(gpu, oracle, bp, affine, pert):
+    Nf = 1 if bp % 2 else 3
+    om = oracle.Mesh(5, 5, 5, 5, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(5, 5, 5, N=5, affine=affine, Nfields=Nf, pert=pert)
+    S = gpu.BP(gm, bp=bp, precon="JACOBI", precision="MIXED")
+    b_o = om.rhs_random(0)[1]
+    x_o, _, it_o, _, _ = om.cg(b_o, 1.0, 1e-8, 5000, precon=True, bp=bp)
+    x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
+    st, _, _ = S.solve(x, gpu.DeviceBuffer.from_host(b_o), tol=1e-8, maxit=5000)
+    assert st.iterations <= 1.25 * it_o + 20
+    xs = x.download()
+    # FP64 residual of the returned solution, by the oracle operator
+    r = b_o - om.operator(xs, 1.0, bp)
+    assert np.linalg.norm(r) <= 1.0001e-8 * np.linalg.norm(b_o)
+    assert _rel(xs, x_o) < 1e-5
+
+
+def test_cub_bad_arguments_fail_loudly(gpu):
+    gm = gpu.Mesh(2, 2, 2, N=3)
+    with pytest.raises(gpu.BPError):
+        gpu.BP(gm, bp=4)                  # BP4 needs three fields
+    dq, dAq = gpu.DeviceBuffer(gm.Ngather), gpu.DeviceBuffer(gm.NL)
+    with pytest.raises(gpu.BPError):
+        gpu.ax_cub_hex3d(gm, 5, dq, dAq)  # the cubature kernel covers BP1-BP4 only
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_cub_driver_result_lines(gpu, capfd, k):
+    assert gpu.driver_main("BP%d" % k, ["-nx", "3", "-ny", "3", "-nz", "3", "-p", "4", "-wi", "5", "-it", "20"]) == 0
+    out = capfd.readouterr().out
+    line = [l for l in out.splitlines() if l.startswith("BP%d: N=" % k)][0]
+    assert "iterations=20, time per DOF=" in line and line.endswith("Element=Hex ")
+    assert gpu.driver_main("BK%d" % k, ["-nx", "3", "-ny", "3", "-nz", "3", "-p", "4", "-a"]) == 0
+    out = capfd.readouterr().out
+    assert [l for l in out.splitlines() if l.startswith("BK%d: N= 4," % k)][0].endswith("Element=Hex, Affine ")
