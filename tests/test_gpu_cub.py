@@ -20,9 +20,9 @@ CUB_AX_CASES = ([(2, 2, 2, N, aff, 0.0 if aff else 0.1, bp) for N in (1, 2, 3, 4
                  for bp in (2, 4)] + [(3, 2, 2, 7, False, 0.2, 3), (4, 3, 2, 5, False, 0.1, 1)])
 
 
-@pytest.mark.parametrize("nx,ny,nz,N,affine,pert,bp", CUB_AX_CASES)
-def test_cub_ax_matches_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, bp):
-    Nf = 1 if bp % 2 else 3
+@pytest.mark.parametrize("nx,ny,nz,N,affine,pert,bpn", CUB_AX_CASES)
+def test_cub_ax_matches_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, bpn):
+    Nf = 1 if bpn % 2 else 3
     om = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=Nf, pert=pert)
     gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, Nfields=Nf, pert=pert)
     # cubature data set up on the device against the oracle's restatement
@@ -37,25 +37,25 @@ def test_cub_ax_matches_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, bp):
         return
     q = 2 * oracle.random(5, om.Ngather) - 1
     dq, dAq = gpu.DeviceBuffer.from_host(q), gpu.DeviceBuffer(om.NL)
-    gpu.ax_cub_hex3d(gm, bp, dq, dAq, lam=1.0)
-    assert _rel(dAq.download(), om.ax(q, 1.0, bp)) < AX_TOL
+    gpu.ax_cub_hex3d(gm, bpn, dq, dAq, lam=1.0)
+    assert _rel(dAq.download(), om.ax(q, 1.0, bpn)) < AX_TOL
 
 
-@pytest.mark.parametrize("bp,affine,pert", [(1, False, 0.1), (1, True, 0.0), (2, False, 0.1), (3, False, 0.1),
+@pytest.mark.parametrize("bpn,affine,pert", [(1, False, 0.1), (1, True, 0.0), (2, False, 0.1), (3, False, 0.1),
                                             (3, True, 0.0), (4, False, 0.0), (4, True, 0.0)])
-def test_cub_operator_forcing_and_diagonal(gpu, oracle, bp, affine, pert):
-    Nf = 1 if bp % 2 else 3
+def test_cub_operator_forcing_and_diagonal(gpu, oracle, bpn, affine, pert):
+    Nf = 1 if bpn % 2 else 3
     om = oracle.Mesh(3, 3, 2, 4, affine=affine, Nfields=Nf, pert=pert)
     gm = gpu.Mesh(3, 3, 2, N=4, affine=affine, Nfields=Nf, pert=pert)
-    S = gpu.BP(gm, bp=bp)
+    S = gpu.BP(gm, bp=bpn)
     q = 2 * oracle.random(3, om.Ngather) - 1
     dq, dAq = gpu.DeviceBuffer.from_host(q), gpu.DeviceBuffer(om.Ngather)
     S.operator(dq, dAq)
-    assert _rel(dAq.download(), om.operator(q, 1.0, bp)) < AX_TOL
+    assert _rel(dAq.download(), om.operator(q, 1.0, bpn)) < AX_TOL
     # BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
-    lam_rhs = 0.0 if bp <= 2 else 1.0
+    lam_rhs = 0.0 if bpn <= 2 else 1.0
     assert _rel(S.rhs("ANALYTIC").download(), om.rhs_analytic(lam_rhs)) < 1e-12
-    assert _rel(S.diagonal().download(), om.jacobi_diag(1.0, bp)) < 1e-12
+    assert _rel(S.diagonal().download(), om.jacobi_diag(1.0, bpn)) < 1e-12
 
 
 CUB_CG_CASES = [(3, 6, 6, 6, 5, False, 0.1, "NONE"), (3, 6, 6, 6, 5, False, 0.1, "JACOBI"),
@@ -64,37 +64,51 @@ CUB_CG_CASES = [(3, 6, 6, 6, 5, False, 0.1, "NONE"), (3, 6, 6, 6, 5, False, 0.1,
                 (4, 4, 4, 4, 4, False, 0.1, "JACOBI"), (2, 4, 4, 4, 3, False, 0.1, "NONE")]
 
 
-@pytest.mark.parametrize("bp,nx,ny,nz,N,affine,pert,precon", CUB_CG_CASES)
-def test_cub_cg_history_matches_oracle(gpu, oracle, bp, nx, ny, nz, N, affine, pert, precon):
-    Nf = 1 if bp % 2 else 3
+@pytest.mark.parametrize("bpn,nx,ny,nz,N,affine,pert,precon", CUB_CG_CASES)
+def test_cub_cg_history_matches_oracle(gpu, oracle, bpn, nx, ny, nz, N, affine, pert, precon):
+    Nf = 1 if bpn % 2 else 3
     om = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=Nf, pert=pert)
     gm = gpu.Mesh(nx, ny, nz, N=N, affine=affine, Nfields=Nf, pert=pert)
-    S = gpu.BP(gm, bp=bp, precon=precon)
+    S = gpu.BP(gm, bp=bpn, precon=precon)
     b_o = om.rhs_random(0)[1]
     maxit = 60
-    x_o, r_o, it_o, hr_o, ha_o = om.cg(b_o, 1.0, 0.0, maxit, precon=(precon == "JACOBI"), bp=bp)
+    x_o, r_o, it_o, hr_o, ha_o = om.cg(b_o, 1.0, 0.0, maxit, precon=(precon == "JACOBI"), bp=bpn)
     x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
     st, hr, ha = S.solve(x, S.rhs("RANDOM", 0), tol=0.0, maxit=maxit)
     assert st.iterations == it_o == maxit
-    live = _check_history(hr, hr_o)
-    assert np.all((np.abs(ha - ha_o) / np.abs(ha_o))[live] < HIST_TOL)
+    # How far this problem's history is reproducible at all: the oracle run
+    # again on b perturbed by 1e-15 relative (a rounding-sized change).  The
+    # mass matrices cluster their spectrum and amplify such a change fast
+    # (measured: 1.7e-10 by iteration 11 of BP1 with Jacobi at r/r0 = 4e-5,
+    # the oracle's own affine and curved operators 1e-15 apart give the
+    # same).  The 1e-10 bar holds up to the first iteration where the oracle
+    # disagrees with itself by more than 1e-11.
+    noise = 1.0 + 1e-15 * (2 * oracle.random(99, om.Ngather) - 1)
+    _, _, _, hr_p, _ = om.cg(b_o * noise, 1.0, 0.0, maxit, precon=(precon == "JACOBI"), bp=bpn)
+    self_rel = np.abs(hr_p - hr_o) / hr_o
+    bad = np.flatnonzero(self_rel > HIST_TOL / 10)
+    reproducible = np.arange(maxit) < (bad[0] if bad.size else maxit)
+    live = _check_history(hr[reproducible], hr_o[reproducible])
+    assert np.all((np.abs(ha - ha_o) / np.abs(ha_o))[reproducible][live] < HIST_TOL)
+    # past that range: as converged as the oracle, and the same solution
+    assert hr[-1] <= max(100 * hr_o[-1], 1e-12 * hr_o[0])
     assert _rel(x.download(), x_o) < 1e-9
 
 
-@pytest.mark.parametrize("bp,affine,pert", [(3, False, 0.1), (1, False, 0.1), (4, True, 0.0)])
-def test_cub_mixed_precision_reaches_tolerance(gpu, oracle, bp, affine, pert):
-    Nf = 1 if bp % 2 else 3
+@pytest.mark.parametrize("bpn,affine,pert", [(3, False, 0.1), (1, False, 0.1), (4, True, 0.0)])
+def test_cub_mixed_precision_reaches_tolerance(gpu, oracle, bpn, affine, pert):
+    Nf = 1 if bpn % 2 else 3
     om = oracle.Mesh(5, 5, 5, 5, affine=affine, Nfields=Nf, pert=pert)
     gm = gpu.Mesh(5, 5, 5, N=5, affine=affine, Nfields=Nf, pert=pert)
-    S = gpu.BP(gm, bp=bp, precon="JACOBI", precision="MIXED")
+    S = gpu.BP(gm, bp=bpn, precon="JACOBI", precision="MIXED")
     b_o = om.rhs_random(0)[1]
-    x_o, _, it_o, _, _ = om.cg(b_o, 1.0, 1e-8, 5000, precon=True, bp=bp)
+    x_o, _, it_o, _, _ = om.cg(b_o, 1.0, 1e-8, 5000, precon=True, bp=bpn)
     x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
     st, _, _ = S.solve(x, gpu.DeviceBuffer.from_host(b_o), tol=1e-8, maxit=5000)
     assert st.iterations <= 1.25 * it_o + 20
     xs = x.download()
     # FP64 residual of the returned solution, by the oracle operator
-    r = b_o - om.operator(xs, 1.0, bp)
+    r = b_o - om.operator(xs, 1.0, bpn)
     assert np.linalg.norm(r) <= 1.0001e-8 * np.linalg.norm(b_o)
     assert _rel(xs, x_o) < 1e-5
 
