@@ -1,7 +1,8 @@
 // Over-integrated element operators of BP1-BP4 (mass, and stiffness + lambda
-// mass, evaluated at N+2 Gauss points per direction), templated on the degree,
-// the operator form and the arithmetic type.  Instantiated by bp_ax_cub64.cu
-// (FP64) and bp_ax_cub32.cu (FP32, the mixed-precision CG).
+// mass, evaluated at N+2 Gauss points per direction).  Included once by
+// bp_ax_cub64.cu (BP_CUB_REAL = double) and once by bp_ax_cub32.cu
+// (BP_CUB_REAL = float, the mixed-precision CG); each inclusion is its own
+// CUDA module with its own constant bank.
 //
 // Forms (reference kernels):
 //   CUB_MASS_AFFINE   wJ_e (MM x MM x MM) q                  okl/bp1AxAffineHex3D.okl:29-135
@@ -11,16 +12,26 @@
 // with S = Dr^T(G00 Dr + G01 Ds + G02 Dt) + Ds^T(...) + Dt^T(...) on the
 // quadrature grid.  BP2/BP4 apply the same operator to each of the 3 fields.
 //
-// Layout of one element slot es (threads (i, j) of a G x G plane, G the grid
-// points per direction): the field lives in shared memory s_q[G][G][G] while
-// it is transformed one direction at a time (b, then a, then c, in place);
-// after the c transform thread (i, j) also holds its column q(i, j, 0:G-1) in
-// registers, so the t-derivative and the t-part of the weak divergence stay in
-// registers and only the r/s fluxes of the current k-slice go through shared
-// memory.  The projection back runs b, a, c again, the c step from registers
-// of the node thread (i, j), which also holds its q column for the q.Aq sum of
-// the fused CG.
+// Work mapping.  Every 1D step (interpolation, derivative, projection, weak
+// derivative) is a small matrix applied along lines of the element's grid.
+// A thread owns whole lines: it reads one line into registers and writes all
+// of that line's outputs, so the matrix index of every multiply-add is the
+// same in all threads of the warp.  The matrices therefore live in the
+// constant bank (c_cub below), read uniformly through the constant cache;
+// shared memory only carries the field between steps whose line direction
+// changes.
+// The G x G threads of an element slot take the roles
+//   (b-line of node a, c) -> (a-line of point j, c) -> (c-line of point i, j)
+// through the interpolation, keep the c-line (the t-direction) in registers
+// for the t-derivative and the t-part of the weak divergence, and run the
+// r- and s-parts as row/column roles over shared memory.  The projection runs
+// the same roles backwards and ends on b-lines of node (a, c), the lines the
+// thread loaded q along; its q.Aq sum for the fused CG re-reads q there.
 #pragma once
+
+#ifndef BP_CUB_REAL
+#error "define BP_CUB_REAL (double or float) before including bp_ax_cub.cuh"
+#endif
 
 #include <cuda_runtime.h>
 
@@ -31,8 +42,39 @@
 #include "bp_internal.hpp"
 
 namespace bp {
+namespace {
+
+using CubReal = BP_CUB_REAL;
+
+// Outer (output) loops of the line steps.  Fully unrolled, every matrix index
+// is a compile-time constant, but the unrolled FP64 steps need more registers
+// than two resident blocks allow; measured at p=7 (BK3 40^3 curved): FP64
+// 1.4 ms rolled against 2.1-2.2 ms unrolled, FP32 (mixed BP3 CG to 1e-8)
+// 1.57 s unrolled against 1.81 s rolled.  So FP64 keeps them rolled and FP32
+// unrolls them.
+#ifndef BP_CUB_OUTER
+#define BP_CUB_OUTER _Pragma("unroll 1")
+#endif
 
 enum CubForm { CUB_MASS_AFFINE = 0, CUB_MASS = 1, CUB_STIFF_AFFINE = 2, CUB_STIFF = 3 };
+
+// Constant-bank table: one slot per degree for the curved forms (T = cubInterp
+// [G x NQ], then cubD [G x G]) and one per degree for the affine forms (T =
+// invV, or MM for BP1/BP2, [NQ x NQ], then the modal cubD [NQ x NQ]).  Each
+// launch first copies its operands into its slot on the launch stream.
+__host__ __device__ constexpr int cub_curved_size(int nq) { return (nq + 1) * nq + (nq + 1) * (nq + 1); }
+__host__ __device__ constexpr int cub_affine_size(int nq) { return 2 * nq * nq; }
+__host__ __device__ constexpr int cub_slot(int nq, bool affine) {
+  int off = 0;
+  for (int n = 2; n < (affine ? 17 : nq); ++n) off += cub_curved_size(n);
+  if (affine)
+    for (int n = 2; n < nq; ++n) off += cub_affine_size(n);
+  return off;
+}
+constexpr int kCubTable = cub_slot(17, true);
+static_assert(kCubTable * sizeof(double) <= 64 * 1024, "constant table exceeds the 64 KB bank");
+
+static __constant__ CubReal c_cub[kCubTable];
 
 template <int NQ, int FORM>
 struct CubShape {
@@ -40,48 +82,52 @@ struct CubShape {
   static constexpr bool STIFF = (FORM == CUB_STIFF_AFFINE || FORM == CUB_STIFF);
   static constexpr int G = CURVED ? NQ + 1 : NQ;   // quadrature points per direction
   static constexpr int G2 = G * G;
-  static constexpr int GP = G * G * G;
+  static constexpr int RS = (G % 2) ? G : G + 1;   // row stride: odd, so rows of a warp spread over banks
+  static constexpr int PLANE = G * RS;
+  static constexpr int FIELD = G * PLANE;           // one G^3 field in shared memory
+  static constexpr int NBUF = STIFF ? 3 : 1;        // u, and the r/s buffers of the stiffness
   static constexpr int EPB0 = 256 / G2 < 1 ? 1 : 256 / G2;
-  static constexpr int EPB = EPB0 > 16 ? 16 : EPB0;   // element slots per block
+  static constexpr int EPB = EPB0 > 8 ? 8 : EPB0;   // element slots per block
   static constexpr int THREADS = G2 * EPB;
+  // resident blocks per SM the register budget must allow (caps registers per thread)
+  static constexpr int MINB = G <= 12 ? 2 : 1;
+  static constexpr int SLOT = cub_slot(NQ, !CURVED);
+  static constexpr int TSIZE = G * NQ;              // T rows = output points
+  static constexpr int DSIZE = STIFF ? G * G : 0;
+  static constexpr size_t SMEM = sizeof(CubReal) * (size_t)NBUF * FIELD * EPB;
 };
 
-template <int NQ, int FORM, class F>
-__global__ void __launch_bounds__(CubShape<NQ, FORM>::THREADS)
+template <int NQ, int FORM>
+__global__ void __launch_bounds__(CubShape<NQ, FORM>::THREADS, CubShape<NQ, FORM>::MINB)
 ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
-              const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg,
-              const F* __restrict__ Tg, F lambda, const F* __restrict__ q, F* __restrict__ Aq,
-              const int* __restrict__ skip, double* __restrict__ partials, int vec) {
+              const CubReal* __restrict__ wJ, const CubReal* __restrict__ ggeo, CubReal lambda,
+              const CubReal* __restrict__ q, CubReal* __restrict__ Aq, const int* __restrict__ skip,
+              double* __restrict__ partials) {
   if (skip && *skip) return;
+  using F = CubReal;
   using Sh = CubShape<NQ, FORM>;
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
-  constexpr int G = Sh::G, G2 = Sh::G2, GP = Sh::GP, EPB = Sh::EPB;
+  constexpr int G = Sh::G, GP = G * G * G, RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB;
   constexpr int NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
-  constexpr int GS = Sh::STIFF ? G : 1;
-  __shared__ F s_T[G][NQ];                 // 1D transform, row = output point
-  __shared__ F s_D[GS][GS + 1];            // differentiation on the grid
-  __shared__ __align__(16) F s_q[EPB][G][G][G];   // the field of each element slot (also the
-                                                  // double scratch of the q.Aq block sum)
-  __shared__ F s_qr[EPB][GS][GS + 1];      // r-flux of the current k-slice
-  __shared__ F s_qs[EPB][GS][GS + 1];      // s-flux of the current k-slice
+  constexpr int SLOT = Sh::SLOT, DOFF = Sh::SLOT + Sh::TSIZE;
+  // T(o, i): 1D transform from NQ nodes to G points; MASS_AFFINE applies MM^T
+#define T_(o, i) (FORM == CUB_MASS_AFFINE ? c_cub[SLOT + (i) * NQ + (o)] : c_cub[SLOT + (o) * NQ + (i)])
+#define D_(a, b) c_cub[DOFF + (a) * G + (b)]
 
-  const int i = threadIdx.x, j = threadIdx.y, es = threadIdx.z;
-  const int tid = i + G * (j + G * es);
-  for (int t = tid; t < G * NQ; t += Sh::THREADS) {
-    // BP1 affine multiplies by MM^T (okl/bp1AxAffineHex3D.okl: s_MM[m][i])
-    if (FORM == CUB_MASS_AFFINE) s_T[t / NQ][t % NQ] = Tg[(t % NQ) * NQ + t / NQ];
-    else s_T[t / NQ][t % NQ] = Tg[t];
-  }
-  if (Sh::STIFF)
-    for (int t = tid; t < G * G; t += Sh::THREADS) s_D[t / G][t % G] = Dg[t];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  F* const sbase = reinterpret_cast<F*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
+  const int tid = tx + G * (ty + G * es);
+  F* const U = sbase + (size_t)es * Sh::NBUF * Sh::FIELD;   // the field
+  F* const R = U + Sh::FIELD;                                // r-derivative / r-flux
+  F* const S = R + Sh::FIELD;                                // s-derivative / s-flux
+#define AT(B, z, y, x) B[(z) * PLANE + (y) * RS + (x)]
 
   const int eidx = blockIdx.x * EPB + es;
   const bool valid = eidx < Nelements;
   const int element = valid ? elementList[eidx] : 0;
-  const bool node = (i < NQ) && (j < NQ);   // owns the GLL column (i, j, :)
   double pdot = 0.0;
 
-  // affine factors are per element
   F wa = 0, ga[6] = {0, 0, 0, 0, 0, 0};
   if (!Sh::CURVED) {
     wa = wJ[element];
@@ -92,205 +138,267 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
 
   for (int f = 0; f < Nfields; ++f) {
     const size_t lbase = ((size_t)element * Nfields + f) * NP;
-    F qcol[NQ];
-    __syncthreads();   // s_T/s_D loaded; the previous field's reads of s_q are done
-    if (node) {
+    if (f > 0) __syncthreads();   // the previous field's last reads of U are done
+    // load q[c][b][a] along b and interpolate along b in registers
+    if (tx < NQ && ty < NQ) {
+      F qb[NQ];   // q along b of node (a, c) = (tx, ty)
 #pragma unroll
-      for (int c = 0; c < NQ; ++c) {
+      for (int b = 0; b < NQ; ++b) {
         F v = 0;
         if (valid) {
-          const int32_t id = G2L[lbase + c * NQ2 + j * NQ + i];
+          const int32_t id = G2L[lbase + ty * NQ2 + b * NQ + tx];
           v = (id >= 0) ? q[id] : F(0);
         }
-        qcol[c] = v;
-        s_q[es][c][j][i] = v;
+        qb[b] = v;
       }
-    }
-    __syncthreads();
-    // transform in b: thread (a = i, c = j), column s_q[c][:][a]
-    if (node) {
-      F r[NQ];
-#pragma unroll
-      for (int b = 0; b < NQ; ++b) r[b] = s_q[es][j][b][i];
-#pragma unroll
+BP_CUB_OUTER
       for (int jj = 0; jj < G; ++jj) {
         F t = 0;
 #pragma unroll
-        for (int b = 0; b < NQ; ++b) t += s_T[jj][b] * r[b];
-        s_q[es][j][jj][i] = t;
+        for (int b = 0; b < NQ; ++b) t += T_(jj, b) * qb[b];
+        AT(U, ty, jj, tx) = t;
       }
     }
     __syncthreads();
-    // transform in a: thread (jj = i, c = j), row s_q[c][jj][:]
-    if (j < NQ) {
+    // along a: thread (jj, c) = (tx, ty)
+    if (ty < NQ) {
       F r[NQ];
 #pragma unroll
-      for (int a = 0; a < NQ; ++a) r[a] = s_q[es][j][i][a];
-#pragma unroll
+      for (int a = 0; a < NQ; ++a) r[a] = AT(U, ty, tx, a);
+BP_CUB_OUTER
       for (int ii = 0; ii < G; ++ii) {
         F t = 0;
 #pragma unroll
-        for (int a = 0; a < NQ; ++a) t += s_T[ii][a] * r[a];
-        s_q[es][j][i][ii] = t;
+        for (int a = 0; a < NQ; ++a) t += T_(ii, a) * r[a];
+        AT(U, ty, tx, ii) = t;
       }
     }
     __syncthreads();
-    // transform in c: thread (ii = i, jj = j), column kept in registers
+    // along c: thread (ii, jj) = (tx, ty); the grid column stays in registers
     F qk[G];
     {
       F r[NQ];
 #pragma unroll
-      for (int c = 0; c < NQ; ++c) r[c] = s_q[es][c][j][i];
+      for (int c = 0; c < NQ; ++c) r[c] = AT(U, c, ty, tx);
 #pragma unroll
       for (int k = 0; k < G; ++k) {
         F t = 0;
 #pragma unroll
-        for (int c = 0; c < NQ; ++c) t += s_T[k][c] * r[c];
+        for (int c = 0; c < NQ; ++c) t += T_(k, c) * r[c];
         qk[k] = t;
       }
     }
     if (FORM == CUB_MASS_AFFINE) {
-      // G == NQ: thread (i, j) is the node thread and holds the result column
+      // G == NQ: the result column of node (tx, ty) is wJ_e * qk
       if (valid) {
 #pragma unroll
         for (int k = 0; k < NQ; ++k) {
           const F out = wa * qk[k];
-          Aq[lbase + k * NQ2 + j * NQ + i] = out;
-          pdot += (double)qcol[k] * (double)out;
+          const size_t l = lbase + k * NQ2 + ty * NQ + tx;
+          Aq[l] = out;
+          if (partials) {
+            const int32_t id = G2L[l];
+            pdot += (double)(id >= 0 ? q[id] : F(0)) * (double)out;
+          }
         }
       }
       continue;
     }
     F acc[G];
     if (FORM == CUB_MASS) {
-      const size_t gb = (size_t)element * GP + j * G + i;
+      const size_t gb = (size_t)element * GP + ty * G + tx;
 #pragma unroll
-      for (int k = 0; k < G; ++k) acc[k] = wJ[gb + k * G2] * qk[k];
+      for (int k = 0; k < G; ++k) acc[k] = wJ[gb + k * G * G] * qk[k];
     } else {
+      // own column: every earlier read of it was this thread's
+#pragma unroll
+      for (int k = 0; k < G; ++k) AT(U, k, ty, tx) = qk[k];
+      __syncthreads();
+      // r-derivative on the row (y, z) = (tx, ty); s-derivative on the column (x, z) = (tx, ty)
+      {
+        F r[G];
+#pragma unroll
+        for (int n = 0; n < G; ++n) r[n] = AT(U, ty, tx, n);
+BP_CUB_OUTER
+        for (int i = 0; i < G; ++i) {
+          F t = 0;
+#pragma unroll
+          for (int n = 0; n < G; ++n) t += D_(i, n) * r[n];
+          AT(R, ty, tx, i) = t;
+        }
+#pragma unroll
+        for (int n = 0; n < G; ++n) r[n] = AT(U, ty, n, tx);
+BP_CUB_OUTER
+        for (int j = 0; j < G; ++j) {
+          F t = 0;
+#pragma unroll
+          for (int n = 0; n < G; ++n) t += D_(j, n) * r[n];
+          AT(S, ty, j, tx) = t;
+        }
+      }
+      // t-derivative on the column (x, y) = (tx, ty) in registers
+      F gt[G];
 #pragma unroll
       for (int k = 0; k < G; ++k) {
-        acc[k] = 0;
-        s_q[es][k][j][i] = qk[k];   // own column: every read of it above is this thread's
+        F t = 0;
+#pragma unroll
+        for (int n = 0; n < G; ++n) t += D_(k, n) * qk[n];
+        gt[k] = t;
       }
       __syncthreads();
+      // fluxes at the points of column (tx, ty)
 #pragma unroll
       for (int k = 0; k < G; ++k) {
-        F dr = 0, ds = 0, dt = 0;
-#pragma unroll
-        for (int n = 0; n < G; ++n) {
-          dr += s_D[i][n] * s_q[es][k][j][n];
-          ds += s_D[j][n] * s_q[es][k][n][i];
-          dt += s_D[k][n] * qk[n];
-        }
         F g0, g1, g2, g3, g4, g5, w;
         if (Sh::CURVED) {
-          const size_t gb = (size_t)element * GP + k * G2 + j * G + i;
-          if (vec) {
-            const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * gb);
-            const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
-            g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
-          } else {
-            const F* gp = ggeo + 6 * gb;
-            g0 = gp[0]; g1 = gp[1]; g2 = gp[2]; g3 = gp[3]; g4 = gp[4]; g5 = gp[5];
-          }
+          const size_t gb = (size_t)element * GP + k * G * G + ty * G + tx;
+          const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * gb);
+          const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
+          g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
           w = wJ[gb];
         } else {
           g0 = ga[0]; g1 = ga[1]; g2 = ga[2]; g3 = ga[3]; g4 = ga[4]; g5 = ga[5];
           w = wa;
         }
-        s_qr[es][j][i] = g0 * dr + g1 * ds + g2 * dt;
-        s_qs[es][j][i] = g1 * dr + g3 * ds + g4 * dt;
-        const F qt = g2 * dr + g4 * ds + g5 * dt;
-        acc[k] += lambda * w * qk[k];
-        __syncthreads();
-        F a = 0;
-#pragma unroll
-        for (int n = 0; n < G; ++n) {
-          a += s_D[n][i] * s_qr[es][j][n];
-          a += s_D[n][j] * s_qs[es][n][i];
-          acc[n] += s_D[k][n] * qt;
-        }
-        acc[k] += a;
-        __syncthreads();
+        const F dr = AT(R, k, ty, tx), ds = AT(S, k, ty, tx), dt = gt[k];
+        AT(R, k, ty, tx) = g0 * dr + g1 * ds + g2 * dt;
+        AT(S, k, ty, tx) = g1 * dr + g3 * ds + g4 * dt;
+        gt[k] = g2 * dr + g4 * ds + g5 * dt;
+        acc[k] = lambda * w * qk[k];
       }
-    }
-    // project: the grid field back to s_q, then b, a (shared) and c (registers)
+      // t-part of the weak divergence, in registers
 #pragma unroll
-    for (int k = 0; k < G; ++k) s_q[es][k][j][i] = acc[k];
+      for (int n = 0; n < G; ++n) {
+        F t = acc[n];
+#pragma unroll
+        for (int k = 0; k < G; ++k) t += D_(k, n) * gt[k];
+        acc[n] = t;
+      }
+      __syncthreads();
+      // r-part on rows, s-part on columns, in place
+      {
+        F r[G];
+#pragma unroll
+        for (int n = 0; n < G; ++n) r[n] = AT(R, ty, tx, n);
+BP_CUB_OUTER
+        for (int i = 0; i < G; ++i) {
+          F t = 0;
+#pragma unroll
+          for (int n = 0; n < G; ++n) t += D_(n, i) * r[n];
+          AT(R, ty, tx, i) = t;
+        }
+#pragma unroll
+        for (int n = 0; n < G; ++n) r[n] = AT(S, ty, n, tx);
+BP_CUB_OUTER
+        for (int j = 0; j < G; ++j) {
+          F t = 0;
+#pragma unroll
+          for (int n = 0; n < G; ++n) t += D_(n, j) * r[n];
+          AT(S, ty, j, tx) = t;
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < G; ++k) acc[k] += AT(R, k, ty, tx) + AT(S, k, ty, tx);
+    }
+    // projection along c in registers: column (ii, jj) = (tx, ty); own column of U
+BP_CUB_OUTER
+    for (int c = 0; c < NQ; ++c) {
+      F t = 0;
+#pragma unroll
+      for (int k = 0; k < G; ++k) t += T_(k, c) * acc[k];
+      AT(U, c, ty, tx) = t;
+    }
     __syncthreads();
-    // back in b: thread (ii = i, k = j), column s_q[k][:][ii]
-    {
+    // along a: row (jj, c) = (tx, ty)
+    if (ty < NQ) {
       F r[G];
 #pragma unroll
-      for (int jj = 0; jj < G; ++jj) r[jj] = s_q[es][j][jj][i];
+      for (int ii = 0; ii < G; ++ii) r[ii] = AT(U, ty, tx, ii);
+BP_CUB_OUTER
+      for (int a = 0; a < NQ; ++a) {
+        F t = 0;
+#pragma unroll
+        for (int ii = 0; ii < G; ++ii) t += T_(ii, a) * r[ii];
+        AT(U, ty, tx, a) = t;
+      }
+    }
+    __syncthreads();
+    // along b: node (a, c) = (tx, ty), the line q was loaded along
+    if (tx < NQ && ty < NQ && valid) {
+      F r[G];
+#pragma unroll
+      for (int jj = 0; jj < G; ++jj) r[jj] = AT(U, ty, jj, tx);
 #pragma unroll
       for (int b = 0; b < NQ; ++b) {
         F t = 0;
 #pragma unroll
-        for (int jj = 0; jj < G; ++jj) t += s_T[jj][b] * r[jj];
-        s_q[es][j][b][i] = t;
-      }
-    }
-    __syncthreads();
-    // back in a: thread (b = i, k = j), row s_q[k][b][:]
-    if (i < NQ) {
-      F r[G];
-#pragma unroll
-      for (int ii = 0; ii < G; ++ii) r[ii] = s_q[es][j][i][ii];
-#pragma unroll
-      for (int a = 0; a < NQ; ++a) {
-        F t = 0;
-#pragma unroll
-        for (int ii = 0; ii < G; ++ii) t += s_T[ii][a] * r[ii];
-        s_q[es][j][i][a] = t;
-      }
-    }
-    __syncthreads();
-    // back in c: node thread (a = i, b = j), column s_q[:][b][a]
-    if (node && valid) {
-      F r[G];
-#pragma unroll
-      for (int k = 0; k < G; ++k) r[k] = s_q[es][k][j][i];
-#pragma unroll
-      for (int c = 0; c < NQ; ++c) {
-        F t = 0;
-#pragma unroll
-        for (int k = 0; k < G; ++k) t += s_T[k][c] * r[k];
-        Aq[lbase + c * NQ2 + j * NQ + i] = t;
-        pdot += (double)qcol[c] * (double)t;
+        for (int jj = 0; jj < G; ++jj) t += T_(jj, b) * r[jj];
+        const size_t l = lbase + ty * NQ2 + b * NQ + tx;
+        Aq[l] = t;
+        if (partials) {   // q again (a cache hit) rather than a line held in registers throughout
+          const int32_t id = G2L[l];
+          pdot += (double)(id >= 0 ? q[id] : F(0)) * (double)t;
+        }
       }
     }
   }
   if (partials) {
-    // s_q as the block-sum scratch: at least one double per thread
-    static_assert(sizeof(F) * EPB * GP >= sizeof(double) * Sh::THREADS, "scratch too small");
-    const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(&s_q[0][0][0][0]));
+    static_assert(sizeof(F) * Sh::NBUF * Sh::FIELD * EPB >= sizeof(double) * Sh::THREADS, "scratch too small");
+    const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(sbase));
     if (tid == 0) partials[blockIdx.x] = bs;
   }
+#undef AT
+#undef D_
+#undef T_
 }
 
-template <int NQ, int FORM, class F>
+// device address of the constant table (per device, looked up on first use)
+static CubReal* cub_table_address() {
+  static CubReal* addr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, c_cub) != cudaSuccess) return nullptr;
+    addr[dev] = static_cast<CubReal*>(p);
+  }
+  return addr[dev];
+}
+
+template <int NQ, int FORM>
 static int launch_cub_form(int32_t Nelements, int Nfields, const int32_t* elementList, const int32_t* G2L,
-                           const CubOperands<F>& o, F lambda, const F* q, F* Aq, const int* skip,
-                           cudaStream_t s, double* partials, int* nblocks) {
+                           const CubOperands<CubReal>& o, CubReal lambda, const CubReal* q, CubReal* Aq,
+                           const int* skip, cudaStream_t s, double* partials, int* nblocks) {
   using Sh = CubShape<NQ, FORM>;
+  if (Sh::CURVED && Sh::STIFF && (reinterpret_cast<uintptr_t>(o.ggeo) % (2 * sizeof(CubReal))))
+    return fail(BP_ERROR_ARG, "over-integrated operator: cubggeo must be aligned to two elements");
+  CubReal* tab = cub_table_address();
+  if (!tab) return fail(BP_ERROR_CUDA, "over-integrated operator: constant table address lookup failed");
+  // this launch's 1D operands into its slot of the constant bank, in stream order
+  BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT, o.T, sizeof(CubReal) * Sh::TSIZE, cudaMemcpyDeviceToDevice, s));
+  if (Sh::STIFF)
+    BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT + Sh::TSIZE, o.D, sizeof(CubReal) * Sh::DSIZE,
+                                cudaMemcpyDeviceToDevice, s));
+  if (Sh::SMEM > 48 * 1024)
+    BP_CUDA_TRY(cudaFuncSetAttribute(ax_cub_kernel<NQ, FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)Sh::SMEM));
   const dim3 block(Sh::G, Sh::G, Sh::EPB);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
-  const int vec = (reinterpret_cast<uintptr_t>(o.ggeo) % (2 * sizeof(F))) == 0;
-  ax_cub_kernel<NQ, FORM, F><<<grid, block, 0, s>>>(Nelements, Nfields, elementList, G2L, o.wJ, o.ggeo, o.D, o.T,
-                                                    lambda, q, Aq, skip, partials, vec);
+  ax_cub_kernel<NQ, FORM><<<grid, block, Sh::SMEM, s>>>(Nelements, Nfields, elementList, G2L, o.wJ, o.ggeo, lambda,
+                                                         q, Aq, skip, partials);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
-template <int NQ, class F>
+template <int NQ>
 static int launch_cub_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
-                         const CubOperands<F>& o, F lambda, const F* q, F* Aq, const int* skip, cudaStream_t s,
-                         double* partials, int* nblocks) {
+                         const CubOperands<CubReal>& o, CubReal lambda, const CubReal* q, CubReal* Aq,
+                         const int* skip, cudaStream_t s, double* partials, int* nblocks) {
   const bool stiff = d.bp >= 3;
 #define BP_CUB(FORM) \
-  return launch_cub_form<NQ, FORM, F>(Nelements, d.Nfields, elementList, G2L, o, lambda, q, Aq, skip, s, partials, nblocks)
+  return launch_cub_form<NQ, FORM>(Nelements, d.Nfields, elementList, G2L, o, lambda, q, Aq, skip, s, partials, nblocks)
   if (d.affine) {
     if (stiff) BP_CUB(CUB_STIFF_AFFINE);
     BP_CUB(CUB_MASS_AFFINE);
@@ -300,19 +408,19 @@ static int launch_cub_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t
 #undef BP_CUB
 }
 
-template <class F>
-int launch_ax_cub_t(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
-                    const CubOperands<F>& o, F lambda, const F* q, F* Aq, const int* skip, cudaStream_t s,
-                    const CgFuse* fuse, int* nblocks) {
+int launch_ax_cub_impl(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                       const CubOperands<CubReal>& o, CubReal lambda, const CubReal* q, CubReal* Aq,
+                       const int* skip, cudaStream_t s, const CgFuse* fuse, int* nblocks) {
   if (nblocks) *nblocks = 0;
   if (d.bp < 1 || d.bp > 4) return fail(BP_ERROR_ARG, "over-integrated operator: bp must be 1..4");
-  if (d.Nfields != ((d.bp % 2) ? 1 : 3)) return fail(BP_ERROR_ARG, "over-integrated operator: BP1/BP3 take 1 field, BP2/BP4 3");
+  if (d.Nfields != ((d.bp % 2) ? 1 : 3))
+    return fail(BP_ERROR_ARG, "over-integrated operator: BP1/BP3 take 1 field, BP2/BP4 3");
   if (Nelements == 0) return BP_SUCCESS;
   double* partials = fuse ? fuse->partials : nullptr;
   switch (d.N + 1) {
 #define BP_CUB_CASE(nq) \
   case nq:              \
-    return launch_cub_nq<nq, F>(d, Nelements, elementList, G2L, o, lambda, q, Aq, skip, s, partials, nblocks);
+    return launch_cub_nq<nq>(d, Nelements, elementList, G2L, o, lambda, q, Aq, skip, s, partials, nblocks);
     BP_CUB_CASE(2) BP_CUB_CASE(3) BP_CUB_CASE(4) BP_CUB_CASE(5) BP_CUB_CASE(6) BP_CUB_CASE(7) BP_CUB_CASE(8)
     BP_CUB_CASE(9) BP_CUB_CASE(10) BP_CUB_CASE(11) BP_CUB_CASE(12) BP_CUB_CASE(13) BP_CUB_CASE(14)
     BP_CUB_CASE(15) BP_CUB_CASE(16)
@@ -322,4 +430,5 @@ int launch_ax_cub_t(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* ele
   }
 }
 
+}  // namespace
 }  // namespace bp

@@ -1,5 +1,6 @@
 // FP64 instantiation of the over-integrated BP1-BP4 operators, and the
 // element-local diagonal of those operators (the Jacobi preconditioner).
+#define BP_CUB_REAL double
 #include "bp_ax_cub.cuh"
 
 namespace bp {
@@ -7,7 +8,7 @@ namespace bp {
 int launch_ax_cub(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const CubOperands<double>& ops, double lambda, const double* q, double* Aq, const int* skip,
                   cudaStream_t s, const CgFuse* fuse, int* nblocks) {
-  return launch_ax_cub_t<double>(d, Nelements, elementList, G2L, ops, lambda, q, Aq, skip, s, fuse, nblocks);
+  return launch_ax_cub_impl(d, Nelements, elementList, G2L, ops, lambda, q, Aq, skip, s, fuse, nblocks);
 }
 
 // ---------------------------------------------------------------------------
