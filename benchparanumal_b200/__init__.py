@@ -44,6 +44,8 @@ EXPORTS = [
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc",
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
+    "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
+    "bp_batch_vectors", "bp_batch_solver",
 ]
 
 
@@ -77,6 +79,12 @@ class MeshView(ctypes.Structure):
 class CubatureView(ctypes.Structure):
     _fields_ = [("cubNq", ctypes.c_int32), ("cubNp", ctypes.c_int32)] + [
         (n, ctypes.c_void_p) for n in ("cubr", "cubw", "cubInterp", "cubD", "invV", "MM", "cubwJ", "cubggeo")]
+
+
+class BatchProblem(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("N", ctypes.c_int32),
+                ("pert", ctypes.c_double), ("pert_seed", ctypes.c_uint64), ("nrhs", ctypes.c_int32),
+                ("rhs_seed", ctypes.c_uint64)]
 
 
 class SolverDesc(ctypes.Structure):
@@ -151,6 +159,13 @@ def lib():
             "bp_mesh_cubature": [vp],
             "bp_mesh_cubature_view": [vp, ctypes.POINTER(CubatureView)],
             "bp_basis_cubature": [i32, vp, vp, vp, vp, vp, vp, vp],
+            "bp_batch_create": [ctypes.POINTER(BatchProblem), i32, ctypes.POINTER(SolverDesc), ctypes.POINTER(vp)],
+            "bp_batch_destroy": [vp],
+            "bp_batch_systems": [vp, ctypes.POINTER(i32)],
+            "bp_batch_system_info": [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)],
+            "bp_batch_solve": [vp, dbl, i32, ctypes.POINTER(SolveStats), ctypes.POINTER(dbl)],
+            "bp_batch_vectors": [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(vp)],
+            "bp_batch_solver": [vp, i32, ctypes.POINTER(vp)],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -425,6 +440,87 @@ class BP:
         _check(lib().bp_solver_solve_host(self._h, b_host.ctypes.data, x_host.ctypes.data, float(tol), int(maxit),
                                           ctypes.byref(st)))
         return st
+
+
+class Batch:
+    """Many independent problems with several right-hand sides each, solved
+    together (bp_batch_*).  problems: iterable of dicts with nx, ny, nz, N,
+    pert, pert_seed, nrhs, rhs_seed."""
+
+    def __init__(self, problems, bp=5, lam=1.0, precon="JACOBI", precision="MIXED"):
+        platform_init(0)
+        probs = list(problems)
+        arr = (BatchProblem * len(probs))(*[
+            BatchProblem(p["nx"], p.get("ny", p["nx"]), p.get("nz", p["nx"]), p["N"], float(p.get("pert", 0.0)),
+                         int(p.get("pert_seed", 1)), int(p.get("nrhs", 1)), int(p.get("rhs_seed", 0)))
+            for p in probs])
+        pc = {"NONE": BP_PRECON_NONE, "JACOBI": BP_PRECON_JACOBI}[precon.upper()]
+        pr = {"FP64": BP_PRECISION_FP64, "MIXED": BP_PRECISION_MIXED}[precision.upper()]
+        d = SolverDesc(bp, float(lam), pc, pr)
+        h = ctypes.c_void_p()
+        _check(lib().bp_batch_create(arr, len(probs), ctypes.byref(d), ctypes.byref(h)))
+        self._h = h.value
+        n = ctypes.c_int32()
+        _check(lib().bp_batch_systems(self._h, ctypes.byref(n)))
+        self.nsystems = n.value
+        self.problem, self.Ngather = [], []
+        for s in range(self.nsystems):
+            pj, ng = ctypes.c_int32(), ctypes.c_int32()
+            _check(lib().bp_batch_system_info(self._h, s, ctypes.byref(pj), ctypes.byref(ng)))
+            self.problem.append(pj.value)
+            self.Ngather.append(ng.value)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().bp_batch_destroy(self._h)
+            self._h = None
+
+    def solve(self, tol=1e-8, maxit=5000):
+        """Solve every system; returns (list of SolveStats, device ms)."""
+        st = (SolveStats * self.nsystems)()
+        ms = ctypes.c_double()
+        _check(lib().bp_batch_solve(self._h, float(tol), int(maxit), st, ctypes.byref(ms)))
+        return list(st), ms.value
+
+    def vectors(self, system):
+        """(x, b) of a system copied to the host."""
+        xp, bp_ = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().bp_batch_vectors(self._h, system, ctypes.byref(xp), ctypes.byref(bp_)))
+        n = self.Ngather[system]
+        return _dl(xp.value, n, np.float64), _dl(bp_.value, n, np.float64)
+
+    def operator(self, system, q, Aq):
+        """The system's operator (bp_solver_operator) on device buffers."""
+        sv = ctypes.c_void_p()
+        _check(lib().bp_batch_solver(self._h, system, ctypes.byref(sv)))
+        _check(lib().bp_solver_operator(sv.value, _ptr(q), _ptr(Aq), None))
+
+
+def lcg_uniform(seed, n):
+    """n draws of the reference's seeded LCG (libs/primitives/random.cpp): the
+    state starts at a*(~seed)+1 and each value is state/(2^64-1) before the
+    step.  Host-side, for generating problem sets."""
+    a, mask = 6364136223846793005, (1 << 64) - 1
+    x = (a * (mask ^ (seed & mask)) + 1) & mask
+    out = []
+    for _ in range(n):
+        out.append(float(x) / float(mask))
+        x = (a * x + 1) & mask
+    return out
+
+
+def uneven_problems(count=64, seed=2, nrhs=4, pmin=3, pmax=10, nmin=8, nmax=24, pert=0.1):
+    """The batched problem set: problem i has degree p_i = pmin + floor(u_{2i}
+    (pmax-pmin+1)) and n_i = nmin + floor(u_{2i+1} (nmax-nmin+1)) elements per
+    side (draws u of the LCG with `seed`), interior vertices perturbed by
+    pert*h (seed 100+i), and nrhs right-hand sides with seeds 1000+nrhs*i+k."""
+    u = lcg_uniform(seed, 2 * count)
+    probs = []
+    for i in range(count):
+        p = pmin + min(int(u[2 * i] * (pmax - pmin + 1)), pmax - pmin)
+        n = nmin + min(int(u[2 * i + 1] * (nmax - nmin + 1)), nmax - nmin)
+        probs.append({"nx": n, "N": p, "pert": pert, "pert_seed": 100 + i, "nrhs": nrhs, "rhs_seed": 1000 + nrhs * i})
+    return probs
 
 
 def box_numbering(nx, ny, nz, N, Nfields=1):

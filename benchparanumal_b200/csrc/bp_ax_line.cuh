@@ -1,0 +1,280 @@
+// BP5/BP6 element operator (GLL collocation) in the line-per-thread form of
+// bp_ax_cub.cuh: every 1D derivative is a constant-bank matrix applied along
+// whole lines owned by single threads.  Included once by bp_ax_line64.cu
+// (BP_LINE_REAL = double) and once by bp_ax_line32.cu (float).
+//
+//   Aq_e = Dr^T(G00 ur + G01 us + G02 ut) + Ds^T(G01 ur + G11 us + G12 ut)
+//        + Dt^T(G02 ur + G12 us + G22 ut) + lambda wJ q,  (ur,us,ut) = (Dr,Ds,Dt) q
+// (okl/bp5AxHex3D.okl:415-569, okl/bp5AxAffineHex3D.okl:419-579,
+// okl/bp6AxHex3D.okl:50-255).  Stored factors carry the GLL weights; affine
+// factors are per element and the weights w_i w_j w_k are applied here.
+//
+// Thread (x, y) of an element slot owns the t-line of point (x, y): it loads
+// q along t, keeps it and the t-derivative in registers, and writes its
+// result line along t (coalesced over x).  The r-derivative runs on rows
+// (y, z) and the s-derivative on columns (x, z) of shared memory, and their
+// weak forms the same way after the fluxes.
+#pragma once
+
+#ifndef BP_LINE_REAL
+#error "define BP_LINE_REAL (double or float) before including bp_ax_line.cuh"
+#endif
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "bp_cg_device.cuh"
+#include "bp_internal.hpp"
+
+#ifndef BP_LINE_OUTER
+#define BP_LINE_OUTER _Pragma("unroll 1")
+#endif
+
+namespace bp {
+namespace {
+
+using LineReal = BP_LINE_REAL;
+
+// constant table: per degree D [NQ x NQ] then gllw [NQ]
+__host__ __device__ constexpr int line_slot(int nq) {
+  int off = 0;
+  for (int n = 2; n < nq; ++n) off += n * n + n;
+  return off;
+}
+constexpr int kLineTable = line_slot(17);
+static __constant__ LineReal c_line[kLineTable];
+
+template <int NQ>
+struct LineShape {
+  static constexpr int G2 = NQ * NQ;
+  static constexpr int RS = (NQ % 2) ? NQ : NQ + 1;
+  static constexpr int PLANE = NQ * RS;
+  static constexpr int FIELD = NQ * PLANE;
+  static constexpr int EPB0 = 256 / G2 < 1 ? 1 : 256 / G2;
+  static constexpr int EPB = EPB0 > 8 ? 8 : EPB0;
+  static constexpr int THREADS = G2 * EPB;
+  static constexpr int MINB = NQ <= 11 ? 2 : 1;
+  static constexpr int SLOT = line_slot(NQ);
+  static constexpr size_t SMEM = sizeof(LineReal) * (size_t)3 * FIELD * EPB;
+};
+
+template <int NQ, bool AFFINE>
+__global__ void __launch_bounds__(LineShape<NQ>::THREADS, LineShape<NQ>::MINB)
+ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+               const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
+               const LineReal* __restrict__ gllw, LineReal lambda, const LineReal* __restrict__ q,
+               LineReal* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
+  if (skip && *skip) return;
+  using F = LineReal;
+  using Sh = LineShape<NQ>;
+  using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
+  constexpr int RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB, NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
+  constexpr int SLOT = Sh::SLOT;
+#define D_(a, b) c_line[SLOT + (a) * NQ + (b)]
+#define W_(a) c_line[SLOT + NQ * NQ + (a)]
+#define AT(B, z, y, x) B[(z) * PLANE + (y) * RS + (x)]
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  F* const sbase = reinterpret_cast<F*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
+  const int tid = tx + NQ * (ty + NQ * es);
+  F* const U = sbase + (size_t)es * 3 * Sh::FIELD;
+  F* const R = U + Sh::FIELD;
+  F* const S = R + Sh::FIELD;
+
+  const int eidx = blockIdx.x * EPB + es;
+  const bool valid = eidx < Nelements;
+  const int element = valid ? elementList[eidx] : 0;
+  double pdot = 0.0;
+
+  F wa = 0, ga[6] = {0, 0, 0, 0, 0, 0}, wxy = 0;
+  if (AFFINE) {
+    wxy = gllw[tx] * gllw[ty];
+    wa = wJ[element];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) ga[c] = ggeo[6 * (size_t)element + c];
+  }
+
+  for (int f = 0; f < Nfields; ++f) {
+    const size_t lbase = ((size_t)element * Nfields + f) * NP;
+    if (f > 0) __syncthreads();   // the previous field's last reads of U, R, S are done
+    F qk[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      F v = 0;
+      if (valid) {
+        const int32_t id = G2L[lbase + k * NQ2 + ty * NQ + tx];
+        v = (id >= 0) ? q[id] : F(0);
+      }
+      qk[k] = v;
+      AT(U, k, ty, tx) = v;
+    }
+    F gt[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      F t = 0;
+#pragma unroll
+      for (int n = 0; n < NQ; ++n) t += D_(k, n) * qk[n];
+      gt[k] = t;
+    }
+    __syncthreads();
+    {
+      F r[NQ];
+#pragma unroll
+      for (int n = 0; n < NQ; ++n) r[n] = AT(U, ty, tx, n);
+      BP_LINE_OUTER
+      for (int i = 0; i < NQ; ++i) {
+        F t = 0;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) t += D_(i, n) * r[n];
+        AT(R, ty, tx, i) = t;
+      }
+#pragma unroll
+      for (int n = 0; n < NQ; ++n) r[n] = AT(U, ty, n, tx);
+      BP_LINE_OUTER
+      for (int j = 0; j < NQ; ++j) {
+        F t = 0;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) t += D_(j, n) * r[n];
+        AT(S, ty, j, tx) = t;
+      }
+    }
+    __syncthreads();
+    F acc[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      F g0, g1, g2, g3, g4, g5, w;
+      if (AFFINE) {
+        const F wk = wxy * W_(k);
+        g0 = ga[0] * wk; g1 = ga[1] * wk; g2 = ga[2] * wk; g3 = ga[3] * wk; g4 = ga[4] * wk; g5 = ga[5] * wk;
+        w = wa * wk;
+      } else {
+        const size_t gb = (size_t)element * NP + k * NQ2 + ty * NQ + tx;
+        const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * gb);
+        const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
+        g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
+        w = wJ[gb];
+      }
+      const F dr = AT(R, k, ty, tx), ds = AT(S, k, ty, tx), dt = gt[k];
+      AT(R, k, ty, tx) = g0 * dr + g1 * ds + g2 * dt;
+      AT(S, k, ty, tx) = g1 * dr + g3 * ds + g4 * dt;
+      gt[k] = g2 * dr + g4 * ds + g5 * dt;
+      acc[k] = lambda * w * qk[k];
+    }
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+      F t = acc[n];
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) t += D_(k, n) * gt[k];
+      acc[n] = t;
+    }
+    __syncthreads();
+    {
+      F r[NQ];
+#pragma unroll
+      for (int n = 0; n < NQ; ++n) r[n] = AT(R, ty, tx, n);
+      BP_LINE_OUTER
+      for (int i = 0; i < NQ; ++i) {
+        F t = 0;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) t += D_(n, i) * r[n];
+        AT(R, ty, tx, i) = t;
+      }
+#pragma unroll
+      for (int n = 0; n < NQ; ++n) r[n] = AT(S, ty, n, tx);
+      BP_LINE_OUTER
+      for (int j = 0; j < NQ; ++j) {
+        F t = 0;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) t += D_(n, j) * r[n];
+        AT(S, ty, j, tx) = t;
+      }
+    }
+    __syncthreads();
+    if (valid) {
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        const F out = acc[k] + AT(R, k, ty, tx) + AT(S, k, ty, tx);
+        Aq[lbase + k * NQ2 + ty * NQ + tx] = out;
+        pdot += (double)AT(U, k, ty, tx) * (double)out;
+      }
+    }
+  }
+  if (partials) {
+    const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(sbase));
+    if (tid == 0) partials[blockIdx.x] = bs;
+  }
+#undef AT
+#undef W_
+#undef D_
+}
+
+static LineReal* line_table_address() {
+  static LineReal* addr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, c_line) != cudaSuccess) return nullptr;
+    addr[dev] = static_cast<LineReal*>(p);
+  }
+  return addr[dev];
+}
+
+template <int NQ>
+static int launch_line_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                          const LineReal* wJ, const LineReal* ggeo, const LineReal* gllw, const LineReal* D,
+                          LineReal lambda, const LineReal* q, LineReal* Aq, const int* skip, cudaStream_t s,
+                          double* partials, int* nblocks) {
+  using Sh = LineShape<NQ>;
+  if (!d.affine && (reinterpret_cast<uintptr_t>(ggeo) % (2 * sizeof(LineReal))))
+    return fail(BP_ERROR_ARG, "element operator: ggeo must be aligned to two elements");
+  LineReal* tab = line_table_address();
+  if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
+  BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT, D, sizeof(LineReal) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  if (d.affine)
+    BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT + NQ * NQ, gllw, sizeof(LineReal) * NQ, cudaMemcpyDeviceToDevice, s));
+  const dim3 block(NQ, NQ, Sh::EPB);
+  const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
+  if (nblocks) *nblocks = (int)grid.x;
+  if (d.affine) {
+    if (Sh::SMEM > 48 * 1024)
+      BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Sh::SMEM));
+    ax_line_kernel<NQ, true><<<grid, block, Sh::SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
+                                                           lambda, q, Aq, skip, partials);
+  } else {
+    if (Sh::SMEM > 48 * 1024)
+      BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Sh::SMEM));
+    ax_line_kernel<NQ, false><<<grid, block, Sh::SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
+                                                            lambda, q, Aq, skip, partials);
+  }
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
+int launch_ax_line_impl(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                        const LineReal* wJ, const LineReal* ggeo, const LineReal* gllw, const LineReal* D,
+                        LineReal lambda, const LineReal* q, LineReal* Aq, const int* skip, cudaStream_t s,
+                        const CgFuse* fuse, int* nblocks) {
+  if (nblocks) *nblocks = 0;
+  if (Nelements == 0) return BP_SUCCESS;
+  double* partials = fuse ? fuse->partials : nullptr;
+  switch (d.N + 1) {
+#define BP_LINE_CASE(nq) \
+  case nq:               \
+    return launch_line_nq<nq>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, partials, nblocks);
+    BP_LINE_CASE(2) BP_LINE_CASE(3) BP_LINE_CASE(4) BP_LINE_CASE(5) BP_LINE_CASE(6) BP_LINE_CASE(7)
+    BP_LINE_CASE(8) BP_LINE_CASE(9) BP_LINE_CASE(10) BP_LINE_CASE(11) BP_LINE_CASE(12) BP_LINE_CASE(13)
+    BP_LINE_CASE(14) BP_LINE_CASE(15) BP_LINE_CASE(16)
+#undef BP_LINE_CASE
+    default:
+      return fail(BP_ERROR_ARG, "element operator: degree N must be in 1..15");
+  }
+}
+
+}  // namespace
+}  // namespace bp

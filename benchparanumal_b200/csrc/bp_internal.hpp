@@ -120,6 +120,13 @@ struct bp_mesh_s {
   // per-element wJ and ggeo
   const double* cubwJ() const { return affine ? wJ.ptr : cubwJ_c.ptr; }
   const double* cubggeo() const { return affine ? ggeo.ptr : cubggeo_c.ptr; }
+  // FP32 copies of the operator data for mixed-precision solvers, one set per
+  // operator family (0: GLL collocation, 1: BP3/BP4 cubature, 2: BP1/BP2
+  // cubature), built on first use and shared by the solvers on this mesh
+  struct Fp32Ops {
+    bp::DeviceArray<float> wJ, ggeo, gllw, D, T;
+    bool ready = false;
+  } f32[3];
 };
 
 struct bp_solver_s;
@@ -174,6 +181,14 @@ int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
 int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const float* wJ, const float* ggeo, const float* D, float lambda, const float* q, float* Aq,
                   const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+// line-per-thread BP5/BP6 element operator (bp_ax_line*.cu), same arguments
+// as launch_ax_skip
+int launch_ax_line(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
+                   const double* q, double* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse, int* nblocks);
+int launch_ax_line(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
+                   const float* q, float* Aq, const int* skip, cudaStream_t s, const CgFuse* fuse, int* nblocks);
 // over-integrated BP1-BP4 operator (bp_ax_cub*.cu).  T is the 1D transform:
 // curved cubInterp [cubNq*Nq]; affine BP3/BP4 invV [Nq*Nq]; affine BP1/BP2 MM
 // [Nq*Nq].  D is cubD (curved) or the modal cubD (affine BP3/BP4); unused for

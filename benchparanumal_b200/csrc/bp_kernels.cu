@@ -175,15 +175,17 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
   if (DOT) fuse_pap(pdot, fuse, s_red);
 }
 
-// Kernel variant of the stored-factor operator: the TMA-staged kernel where it
-// applies, else the register-pencil kernel.  BP_AX_VARIANT=pencil in the
-// environment selects the pencil kernel everywhere (for comparisons).
-enum { AX_AUTO = 0, AX_PENCIL = 1 };
+// Kernel variant of the element operator: stored factors use the TMA-staged
+// kernel where it applies and the line-per-thread kernel (bp_ax_line.cuh)
+// elsewhere; affine factors the line kernel in FP32 and the register-pencil
+// kernel in FP64.  BP_AX_VARIANT=pencil
+// or =line in the environment selects that kernel everywhere (for comparisons).
+enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2 };
 static int ax_variant() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("BP_AX_VARIANT");
-    v = (e && std::string(e) == "pencil") ? AX_PENCIL : AX_AUTO;
+    v = !e ? AX_AUTO : std::string(e) == "pencil" ? AX_PENCIL : std::string(e) == "line" ? AX_LINE : AX_AUTO;
   }
   return v;
 }
@@ -193,9 +195,19 @@ static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t*
                         const int32_t* G2L, const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda,
                         const F* q, F* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   constexpr int EPB = AxShape<NQ>::EPB;
+  // Measured choices (40^3 or 24^3 boxes): stored factors take the TMA kernel
+  // where it applies (even Nq), else the line kernel (FP32 mixed BP5 to 1e-8:
+  // p=10 0.61 vs 1.15 s pencil, p=6 0.68 vs 0.84 s; FP64 BK5 p=6 0.6 vs 0.7 ms).
+  // Affine factors: the line kernel in FP32 (p=15: 4.28 vs 4.99 s), the pencil
+  // kernel in FP64 (BK5 p=7 0.6 vs 0.8 ms, BK6 p=15 7.4 vs 8.8 ms).
+  if (ax_variant() == AX_LINE || (d.affine && sizeof(F) == 4 && ax_variant() == AX_AUTO))
+    return launch_ax_line(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse, nblocks);
   if (!d.affine && ax_variant() != AX_PENCIL) {
     const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
     if (rc != 1) return rc;   // 1: configuration not covered by the TMA kernel
+    if (ax_variant() == AX_AUTO)
+      return launch_ax_line(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse,
+                            nblocks);
   }
   const dim3 block(NQ, NQ, EPB);
   const dim3 grid((Nelements + EPB - 1) / EPB);

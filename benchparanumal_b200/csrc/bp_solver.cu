@@ -321,9 +321,11 @@ struct bp_solver_s {
   bp_ax_desc_t ax{};
   DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist, fuse_partials, bcopy;
   // FP32 data of the mixed-precision solve
-  DeviceArray<float> wJ32, ggeo32, D32, gllw32, T32, invD32, AqL32, p32, x32, r32;
+  DeviceArray<float> invD32, AqL32, p32, x32, r32;
+  int family = 0;              // operator family of the FP32 data on the mesh (mesh_fp32)
   DeviceArray<unsigned int> counter;
   DeviceArray<CgScalars> sc;
+  CgScalars* scal = nullptr;   // the CG scalars: sc.ptr, or a slot of a batch's array
   int hist_len = 0;
   // graph of kChunk iterations, keyed by the vectors it was captured for
   cudaGraphExec_t graph = nullptr;
@@ -362,7 +364,34 @@ static ElemOperands<double> operands64(const bp_solver_s* S) {
 }
 
 static ElemOperands<float> operands32(const bp_solver_s* S) {
-  return {S->wJ32.ptr, S->ggeo32.ptr, S->gllw32.ptr, S->D32.ptr, S->T32.ptr};
+  const bp_mesh_s::Fp32Ops& f = S->mesh->f32[S->family];
+  return {f.wJ.ptr, f.ggeo.ptr, f.gllw.ptr, f.D.ptr, f.T.ptr};
+}
+
+// FP32 copies of a mesh's operator data for mixed-precision solvers, built once
+// per operator family and shared by every solver on the mesh
+static int mesh_fp32(bp_solver_s* S, cudaStream_t s) {
+  bp_mesh_s* mesh = S->mesh;
+  bp_mesh_s::Fp32Ops& f = mesh->f32[S->family];
+  if (f.ready) return BP_SUCCESS;
+  const ElemOperands<double> o = operands64(S);
+  const bool cub = S->bp <= 4;
+  const size_t ng = cub ? (mesh->affine ? (size_t)mesh->E : mesh->cubwJ_c.n) : mesh->wJ.n;
+  const size_t nD = cub ? (mesh->affine ? mesh->cubDmodal.n : mesh->cubD.n) : mesh->D.n;
+  const size_t nT = cub ? (mesh->affine ? mesh->MM.n : mesh->cubInterp.n) : 0;
+  BP_TRY(f.wJ.alloc(ng));
+  BP_TRY(f.ggeo.alloc(6 * ng));
+  BP_TRY(f.D.alloc(nD));
+  BP_TRY(f.gllw.alloc(mesh->gllw.n));
+  BP_TRY(f.T.alloc(nT));
+  BP_TRY(to_float(o.wJ, f.wJ.ptr, ng, s));
+  BP_TRY(to_float(o.ggeo, f.ggeo.ptr, 6 * ng, s));
+  BP_TRY(to_float(o.D, f.D.ptr, nD, s));
+  BP_TRY(to_float(mesh->gllw.ptr, f.gllw.ptr, mesh->gllw.n, s));
+  if (nT) BP_TRY(to_float(o.T, f.T.ptr, nT, s));
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  f.ready = true;
+  return BP_SUCCESS;
 }
 
 template <class V>
@@ -391,14 +420,14 @@ static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* 
   const int g = vec_grid(N);
   double* hist_alpha = S->hist.ptr;
   double* hist_rnorm = S->hist.ptr ? S->hist.ptr + S->hist_len : nullptr;
-  cg_direction_kernel<V><<<g, kThreads, 0, s>>>(N, x, p, r, invD, S->sc.ptr);
+  cg_direction_kernel<V><<<g, kThreads, 0, s>>>(N, x, p, r, invD, S->scal);
   BP_CUDA_TRY(cudaGetLastError());
   const CgFuse fuse{S->fuse_partials.ptr};
   int nparts = 0;
-  BP_TRY(elem_apply<V>(S, o, p, AqL, &S->sc.ptr->done, s, &fuse, &nparts));
-  cg_alpha_kernel<<<1, kAlphaThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->sc.ptr, hist_alpha);
+  BP_TRY(elem_apply<V>(S, o, p, AqL, &S->scal->done, s, &fuse, &nparts));
+  cg_alpha_kernel<<<1, kAlphaThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->scal, hist_alpha);
   BP_CUDA_TRY(cudaGetLastError());
-  cg_gather_update_kernel<V><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, AqL, r, invD, S->sc.ptr,
+  cg_gather_update_kernel<V><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, AqL, r, invD, S->scal,
                                                     hist_rnorm, S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
@@ -458,7 +487,7 @@ static int ensure_hist(bp_solver_s* S, int maxit) {
 }
 
 static int read_scalars(bp_solver_s* S, CgScalars& h, cudaStream_t s) {
-  BP_CUDA_TRY(cudaMemcpyAsync(&h, S->sc.ptr, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  BP_CUDA_TRY(cudaMemcpyAsync(&h, S->scal, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
   BP_CUDA_TRY(cudaStreamSynchronize(s));
   return BP_SUCCESS;
 }
@@ -495,7 +524,7 @@ static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxi
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
   // r = b - A x
   BP_TRY(operator_apply(S, x, S->Ap.ptr, nullptr, s));
-  cg_init_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, S->Ap.ptr, r, S->invD.ptr, S->sc.ptr, tol, maxit, S->precon,
+  cg_init_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, S->Ap.ptr, r, S->invD.ptr, S->scal, tol, maxit, S->precon,
                                                   S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   const int nchunks = (maxit + kChunk - 1) / kChunk;
@@ -507,7 +536,7 @@ static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxi
       if (h.done) break;
     }
   }
-  cg_final_kernel<double><<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->sc.ptr);
+  cg_final_kernel<double><<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->scal);
   BP_CUDA_TRY(cudaGetLastError());
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev1, s));
   BP_TRY(read_scalars(S, h, s));
@@ -519,33 +548,43 @@ static int mixed_replace(bp_solver_s* S, double* x, double* r, bool init, double
   const int32_t N = S->N;
   BP_TRY(operator_apply(S, x, S->Ap.ptr, nullptr, s));
   mixed_replace_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, S->bcopy.ptr, S->Ap.ptr, r, S->r32.ptr, S->invD32.ptr,
-                                                        S->sc.ptr, init ? 1 : 0, tol, maxit, S->precon,
+                                                        S->scal, init ? 1 : 0, tol, maxit, S->precon,
                                                         S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
+// start of a mixed solve: keep b, x_lo = 0, FP64 residual and the FP32 restart
+static int mixed_begin(bp_solver_s* S, double* x, double* r, double tol, int maxit, cudaStream_t s) {
+  const int32_t N = S->N;
+  BP_CUDA_TRY(cudaMemcpyAsync(S->bcopy.ptr, r, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  BP_CUDA_TRY(cudaMemsetAsync(S->x32.ptr, 0, sizeof(float) * N, s));
+  return mixed_replace(S, x, r, true, tol, maxit, s);
+}
+
+// reliable update: fold the pending x_lo step, x_hi += x_lo, FP64 residual
+static int mixed_reliable(bp_solver_s* S, double* x, double* r, double tol, int maxit, cudaStream_t s) {
+  const int32_t N = S->N;
+  cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, S->x32.ptr, S->p32.ptr, S->scal);
+  BP_CUDA_TRY(cudaGetLastError());
+  mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, x, S->x32.ptr);
+  BP_CUDA_TRY(cudaGetLastError());
+  return mixed_replace(S, x, r, false, tol, maxit, s);
+}
+
 static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int maxit, double* hist_rnorm,
                        double* hist_alpha, bp_solve_stats_t* stats, cudaStream_t s, bool record_events) {
-  const int32_t N = S->N;
   if (!(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_solver_solve: a mixed-precision solve needs tol > 0");
   BP_TRY(ensure_hist(S, maxit));
   if (!S->graph32) BP_TRY(capture(&S->graph32, s, body32, S, nullptr, nullptr));
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
-  BP_CUDA_TRY(cudaMemcpyAsync(S->bcopy.ptr, r, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-  BP_CUDA_TRY(cudaMemsetAsync(S->x32.ptr, 0, sizeof(float) * N, s));
-  BP_TRY(mixed_replace(S, x, r, true, tol, maxit, s));
+  BP_TRY(mixed_begin(S, x, r, tol, maxit, s));
   CgScalars h{};
   BP_TRY(read_scalars(S, h, s));
   int updates = 0;
   while (!h.done || h.update) {
     if (h.update) {
-      // reliable update: fold the pending x_lo step, x_hi += x_lo, FP64 residual
-      cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, S->x32.ptr, S->p32.ptr, S->sc.ptr);
-      BP_CUDA_TRY(cudaGetLastError());
-      mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, x, S->x32.ptr);
-      BP_CUDA_TRY(cudaGetLastError());
-      BP_TRY(mixed_replace(S, x, r, false, tol, maxit, s));
+      BP_TRY(mixed_reliable(S, x, r, tol, maxit, s));
       ++updates;
     } else {
       BP_CUDA_TRY(cudaGraphLaunch(S->graph32, s));
@@ -603,9 +642,10 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
     // one block per element
     if ((rc = S->fuse_partials.alloc((size_t)mesh->E + 1))) break;
     if ((rc = S->sc.alloc(1))) break;
+    S->scal = S->sc.ptr;
     cudaError_t ce = cudaMemsetAsync(S->p.ptr, 0, sizeof(double) * S->N, s);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(S->counter.ptr, 0, sizeof(unsigned int) * 4, s);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(S->sc.ptr, 0, sizeof(CgScalars), s);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(S->scal, 0, sizeof(CgScalars), s);
     if (ce == cudaSuccess) ce = cudaEventCreate(&S->ev0);
     if (ce == cudaSuccess) ce = cudaEventCreate(&S->ev1);
     if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_solver_create", __FILE__, __LINE__); break; }
@@ -615,27 +655,14 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
       if ((rc = launch_reciprocal(S->N, S->invD.ptr, s))) break;
     }
     if (S->mixed) {
-      // FP32 copies of the stored factors and the 1D operators, FP32 CG vectors
-      const ElemOperands<double> o = operands64(S);
-      const bool cub = S->bp <= 4;
-      const size_t ng = cub ? (mesh->affine ? (size_t)mesh->E : mesh->cubwJ_c.n) : mesh->wJ.n;
-      const size_t nD = cub ? (mesh->affine ? mesh->cubDmodal.n : mesh->cubD.n) : mesh->D.n;
-      const size_t nT = cub ? (mesh->affine ? mesh->MM.n : mesh->cubInterp.n) : 0;
-      if ((rc = S->wJ32.alloc(ng))) break;
-      if ((rc = S->ggeo32.alloc(6 * ng))) break;
-      if ((rc = S->D32.alloc(nD))) break;
-      if ((rc = S->gllw32.alloc(mesh->gllw.n))) break;
-      if ((rc = S->T32.alloc(nT))) break;
+      // FP32 copies of the stored factors and the 1D operators (on the mesh), FP32 CG vectors
+      S->family = S->bp >= 5 ? 0 : (S->bp >= 3 ? 1 : 2);
+      if ((rc = mesh_fp32(S, s))) break;
       if ((rc = S->AqL32.alloc(NL))) break;
       if ((rc = S->p32.alloc(S->N))) break;
       if ((rc = S->x32.alloc(S->N))) break;
       if ((rc = S->r32.alloc(S->N))) break;
       if ((rc = S->bcopy.alloc(S->N))) break;
-      if ((rc = to_float(o.wJ, S->wJ32.ptr, ng, s))) break;
-      if ((rc = to_float(o.ggeo, S->ggeo32.ptr, 6 * ng, s))) break;
-      if ((rc = to_float(o.D, S->D32.ptr, nD, s))) break;
-      if ((rc = to_float(mesh->gllw.ptr, S->gllw32.ptr, mesh->gllw.n, s))) break;
-      if (nT && (rc = to_float(o.T, S->T32.ptr, nT, s))) break;
       if (S->precon == BP_PRECON_JACOBI) {
         if ((rc = S->invD32.alloc(S->N))) break;
         if ((rc = to_float(S->invD.ptr, S->invD32.ptr, S->N, s))) break;
@@ -755,6 +782,267 @@ int bp_solver_solve_host(bp_solver_t S, const double* b_host, double* x_host, do
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched solves: many independent problems (each its own box, degree and
+// element count) with several right-hand sides each.  Every (problem, rhs)
+// pair is a CG system with its own solver state on a shared mesh; one CUDA
+// graph holds kChunk iterations of every system, the systems spread over
+// kBranches parallel branches (fork/join events), so small and large
+// problems of different degrees run side by side on the GPU and one graph
+// launch advances all of them.  Finished systems skip their kernels through
+// their device flag.  In a mixed-precision batch the host visits the systems
+// between graph launches and applies the reliable updates they ask for.
+// ---------------------------------------------------------------------------
+struct bp_batch_s {
+  std::vector<bp_mesh_s*> meshes;             // owned
+  std::vector<bp_solver_s*> solvers;          // owned, one per system
+  std::vector<int> sys_prob;                  // problem of each system
+  std::vector<DeviceArray<double>*> x, r, b;  // per system (owned)
+  DeviceArray<CgScalars> sc;                  // the systems' CG scalars, one array
+  int mixed = 0;
+  std::vector<cudaStream_t> branches;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  ~bp_batch_s() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto* S : solvers) delete S;
+    for (auto* m : meshes) bp_mesh_destroy(m);
+    for (auto* v : x) delete v;
+    for (auto* v : r) delete v;
+    for (auto* v : b) delete v;
+    for (auto st : branches) cudaStreamDestroy(st);
+    for (auto e : joins) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+namespace bp {
+
+constexpr int kBranches = 16;
+
+static int batch_capture(bp_batch_s* B, cudaStream_t s) {
+  if (B->graph) return BP_SUCCESS;
+  cudaGraph_t g;
+  BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int rc = BP_SUCCESS;
+  cudaError_t ce = cudaEventRecord(B->fork, s);
+  const int nb = (int)B->branches.size();
+  for (int k = 0; k < nb && ce == cudaSuccess; ++k) ce = cudaStreamWaitEvent(B->branches[k], B->fork, 0);
+  for (size_t i = 0; i < B->solvers.size() && ce == cudaSuccess && rc == BP_SUCCESS; ++i) {
+    cudaStream_t bs = B->branches[i % nb];
+    for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k)
+      rc = B->mixed ? body32(B->solvers[i], nullptr, nullptr, bs) : body64(B->solvers[i], B->x[i]->ptr, B->r[i]->ptr, bs);
+  }
+  for (int k = 0; k < nb && ce == cudaSuccess; ++k) {
+    ce = cudaEventRecord(B->joins[k], B->branches[k]);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s, B->joins[k], 0);
+  }
+  cudaError_t ce2 = cudaStreamEndCapture(s, &g);
+  if (rc != BP_SUCCESS) return rc;
+  BP_CUDA_TRY(ce);
+  BP_CUDA_TRY(ce2);
+  ce = cudaGraphInstantiate(&B->graph, g, 0);
+  cudaGraphDestroy(g);
+  BP_CUDA_TRY(ce);
+  return BP_SUCCESS;
+}
+
+static int batch_read(bp_batch_s* B, std::vector<CgScalars>& h, cudaStream_t s) {
+  h.resize(B->solvers.size());
+  BP_CUDA_TRY(cudaMemcpyAsync(h.data(), B->sc.ptr, sizeof(CgScalars) * h.size(), cudaMemcpyDeviceToHost, s));
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  return BP_SUCCESS;
+}
+
+static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* stats, double* elapsed_ms) {
+  cudaStream_t s = default_stream();
+  const size_t ns = B->solvers.size();
+  if (B->mixed && !(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_batch_solve: a mixed-precision batch needs tol > 0");
+  BP_TRY(batch_capture(B, s));
+  std::vector<int> updates(ns, 0);
+  BP_CUDA_TRY(cudaEventRecord(B->ev0, s));
+  // x = 0, r = b, and each system's start
+  for (size_t i = 0; i < ns; ++i) {
+    bp_solver_s* S = B->solvers[i];
+    const size_t bytes = sizeof(double) * S->N;
+    BP_CUDA_TRY(cudaMemsetAsync(B->x[i]->ptr, 0, bytes, s));
+    BP_CUDA_TRY(cudaMemcpyAsync(B->r[i]->ptr, B->b[i]->ptr, bytes, cudaMemcpyDeviceToDevice, s));
+    if (B->mixed) {
+      BP_TRY(mixed_begin(S, B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
+    } else {
+      BP_TRY(operator_apply(S, B->x[i]->ptr, S->Ap.ptr, nullptr, s));
+      cg_init_kernel<<<vec_grid(S->N), kThreads, 0, s>>>(S->N, S->Ap.ptr, B->r[i]->ptr, S->invD.ptr, S->scal, tol,
+                                                          maxit, S->precon, S->partials.ptr, S->counter.ptr);
+      BP_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  std::vector<CgScalars> h;
+  BP_TRY(batch_read(B, h, s));
+  for (;;) {
+    bool running = false, updated = false;
+    for (size_t i = 0; i < ns; ++i) {
+      if (h[i].breakdown) continue;
+      if (B->mixed && h[i].update) {
+        BP_TRY(mixed_reliable(B->solvers[i], B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
+        ++updates[i];
+        updated = true;
+      } else if (!h[i].done) {
+        running = true;
+      }
+    }
+    if (updated) {   // the updated systems may have converged or resumed
+      BP_TRY(batch_read(B, h, s));
+      continue;
+    }
+    if (!running) break;
+    BP_CUDA_TRY(cudaGraphLaunch(B->graph, s));
+    BP_TRY(batch_read(B, h, s));
+  }
+  if (!B->mixed)
+    for (size_t i = 0; i < ns; ++i) {
+      bp_solver_s* S = B->solvers[i];
+      cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, s>>>(S->N, B->x[i]->ptr, S->p.ptr, S->scal);
+      BP_CUDA_TRY(cudaGetLastError());
+    }
+  BP_CUDA_TRY(cudaEventRecord(B->ev1, s));
+  BP_TRY(batch_read(B, h, s));
+  float ms = 0.f;
+  BP_CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+  if (elapsed_ms) *elapsed_ms = ms;
+  BP_TRY(check_device_error());
+  bool breakdown = false;
+  for (size_t i = 0; i < ns; ++i) {
+    if (stats) {
+      stats[i].iterations = h[i].iter;
+      stats[i].rdotr0 = h[i].rdotr0;
+      stats[i].rdotr = B->mixed ? h[i].rtrue2 : h[i].rdotr;
+      stats[i].elapsed_ms = ms;
+      stats[i].updates = updates[i];
+    }
+    breakdown = breakdown || h[i].breakdown;
+  }
+  if (breakdown) return fail(BP_ERROR_NUMERIC, "bp_batch_solve: CG breakdown in a system (p.Ap <= 0 or non-finite)");
+  return BP_SUCCESS;
+}
+
+}  // namespace bp
+
+extern "C" {
+
+int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const bp_solver_desc_t* d,
+                    bp_batch_t* out) {
+  if (!problems || !d || !out || nproblems < 1) return fail(BP_ERROR_ARG, "bp_batch_create: bad arguments");
+  *out = nullptr;
+  if (d->bp != 1 && d->bp != 3 && d->bp != 5) return fail(BP_ERROR_ARG, "bp_batch_create: bp must be 1, 3 or 5");
+  for (int j = 0; j < nproblems; ++j)
+    if (problems[j].nrhs < 1 || problems[j].nrhs > 64) return fail(BP_ERROR_ARG, "bp_batch_create: nrhs must be 1..64");
+  cudaStream_t s = default_stream();
+  bp_batch_s* B = new bp_batch_s();
+  B->mixed = d->precision == BP_PRECISION_MIXED;
+  int rc = BP_SUCCESS;
+  do {
+    cudaError_t ce = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&B->ev0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&B->ev1);
+    for (int k = 0; k < kBranches && ce == cudaSuccess; ++k) {
+      cudaStream_t st;
+      cudaEvent_t e;
+      ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+      if (ce != cudaSuccess) break;
+      B->branches.push_back(st);
+      ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+      if (ce != cudaSuccess) break;
+      B->joins.push_back(e);
+    }
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_batch_create", __FILE__, __LINE__); break; }
+    int nsys = 0;
+    for (int j = 0; j < nproblems; ++j) nsys += problems[j].nrhs;
+    if ((rc = B->sc.alloc(nsys))) break;
+    for (int j = 0; j < nproblems && rc == BP_SUCCESS; ++j) {
+      const bp_batch_problem_t& P = problems[j];
+      bp_box_desc_t bd{};
+      bd.nx = P.nx; bd.ny = P.ny; bd.nz = P.nz; bd.N = P.N; bd.affine = 0; bd.Nfields = 1;
+      bd.pert = P.pert; bd.pert_seed = P.pert_seed;
+      bp_mesh_t m = nullptr;
+      if ((rc = bp_mesh_create(&bd, &m))) break;
+      B->meshes.push_back(m);
+      for (int k = 0; k < P.nrhs && rc == BP_SUCCESS; ++k) {
+        bp_solver_t S = nullptr;
+        if ((rc = bp_solver_create(m, d, &S))) break;
+        B->solvers.push_back(S);
+        B->sys_prob.push_back(j);
+        S->scal = B->sc.ptr + (B->solvers.size() - 1);
+        auto* xv = new DeviceArray<double>();
+        auto* rv = new DeviceArray<double>();
+        auto* bv = new DeviceArray<double>();
+        B->x.push_back(xv);
+        B->r.push_back(rv);
+        B->b.push_back(bv);
+        if ((rc = xv->alloc(S->N))) break;
+        if ((rc = rv->alloc(S->N))) break;
+        if ((rc = bv->alloc(S->N))) break;
+        rc = bp_solver_rhs(S, BP_RHS_RANDOM, P.rhs_seed + (uint64_t)k, bv->ptr, nullptr);
+      }
+    }
+    if (rc == BP_SUCCESS) {
+      cudaError_t ce2 = cudaMemsetAsync(B->sc.ptr, 0, sizeof(CgScalars) * B->sc.n, s);
+      if (ce2 == cudaSuccess) ce2 = cudaStreamSynchronize(s);
+      if (ce2 != cudaSuccess) rc = cuda_fail(ce2, "bp_batch_create", __FILE__, __LINE__);
+    }
+  } while (0);
+  if (rc != BP_SUCCESS) {
+    delete B;
+    return rc;
+  }
+  *out = B;
+  return BP_SUCCESS;
+}
+
+int bp_batch_destroy(bp_batch_t B) {
+  delete B;
+  return BP_SUCCESS;
+}
+
+int bp_batch_systems(bp_batch_t B, int32_t* nsystems) {
+  if (!B || !nsystems) return fail(BP_ERROR_ARG, "bp_batch_systems: null pointer");
+  *nsystems = (int32_t)B->solvers.size();
+  return BP_SUCCESS;
+}
+
+int bp_batch_system_info(bp_batch_t B, int32_t system, int32_t* problem, int32_t* Ngather) {
+  if (!B || system < 0 || system >= (int32_t)B->solvers.size())
+    return fail(BP_ERROR_ARG, "bp_batch_system_info: bad system index");
+  if (problem) *problem = B->sys_prob[system];
+  if (Ngather) *Ngather = B->solvers[system]->N;
+  return BP_SUCCESS;
+}
+
+int bp_batch_solve(bp_batch_t B, double tol, int32_t maxit, bp_solve_stats_t* stats, double* elapsed_ms) {
+  if (!B) return fail(BP_ERROR_ARG, "bp_batch_solve: null batch");
+  if (maxit < 0 || !(tol >= 0.0)) return fail(BP_ERROR_ARG, "bp_batch_solve: bad tol or maxit");
+  return batch_solve(B, tol, maxit, stats, elapsed_ms);
+}
+
+int bp_batch_vectors(bp_batch_t B, int32_t system, double** x, double** b) {
+  if (!B || system < 0 || system >= (int32_t)B->solvers.size())
+    return fail(BP_ERROR_ARG, "bp_batch_vectors: bad system index");
+  if (x) *x = B->x[system]->ptr;
+  if (b) *b = B->b[system]->ptr;
+  return BP_SUCCESS;
+}
+
+int bp_batch_solver(bp_batch_t B, int32_t system, bp_solver_t* solver) {
+  if (!B || !solver || system < 0 || system >= (int32_t)B->solvers.size())
+    return fail(BP_ERROR_ARG, "bp_batch_solver: bad system index");
+  *solver = B->solvers[system];
+  return BP_SUCCESS;
 }
 
 }  // extern "C"

@@ -316,6 +316,45 @@ int bp_solver_solve_host(bp_solver_t solver, const double* b_host, double* x_hos
                          int32_t maxit, bp_solve_stats_t* stats);
 
 /* ---------------------------------------------------------------------------
+ * Batched solves (extension; the reference solves one problem per run).
+ * Many independent problems -- each its own perturbed box, degree and element
+ * count -- with several right-hand sides each, solved together: every
+ * (problem, rhs) pair is one CG system, and one CUDA graph launch advances
+ * all systems by 20 iterations, small and large problems side by side on the
+ * GPU.  Each system behaves exactly as bp_solver_solve on its own problem
+ * (same kernels, same stop rules, same mixed-precision reliable updates).
+ * ------------------------------------------------------------------------- */
+
+typedef struct bp_batch_s* bp_batch_t;
+
+typedef struct bp_batch_problem {
+  int32_t nx, ny, nz;   /* elements per direction                                  */
+  int32_t N;            /* degree 1..15                                             */
+  double pert;          /* interior vertex perturbation, fraction of h              */
+  uint64_t pert_seed;   /* LCG seed of the perturbation                             */
+  int32_t nrhs;         /* right-hand sides: BP_RHS_RANDOM forcing ...              */
+  uint64_t rhs_seed;    /* ... with seeds rhs_seed, rhs_seed+1, ..., +nrhs-1        */
+} bp_batch_problem_t;
+
+/* Meshes, solvers (desc: bp 1, 3 or 5; preconditioner; precision) and
+   right-hand sides for every system, in problem order, rhs order within a
+   problem.  The meshes are curved (stored factors). */
+int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const bp_solver_desc_t* desc,
+                    bp_batch_t* batch);
+int bp_batch_destroy(bp_batch_t batch);
+int bp_batch_systems(bp_batch_t batch, int32_t* nsystems);
+/* problem index and number of unknowns of a system (either may be NULL) */
+int bp_batch_system_info(bp_batch_t batch, int32_t system, int32_t* problem, int32_t* Ngather);
+/* Solve every system from x = 0 to its own stop rule (see bp_solver_solve).
+   stats (host, one entry per system, may be NULL) and elapsed_ms (device
+   time of the whole batch, may be NULL). */
+int bp_batch_solve(bp_batch_t batch, double tol, int32_t maxit, bp_solve_stats_t* stats, double* elapsed_ms);
+/* Device pointers of a system's solution x and right-hand side b [Ngather]. */
+int bp_batch_vectors(bp_batch_t batch, int32_t system, double** x, double** b);
+/* The solver object of a system (owned by the batch), e.g. for bp_solver_operator. */
+int bp_batch_solver(bp_batch_t batch, int32_t system, bp_solver_t* solver);
+
+/* ---------------------------------------------------------------------------
  * Drivers: the BK/BP executables' main() with the reference's command-line
  * keys (libs/core/platformSettings.cpp:31-50, libs/mesh/meshSettings.cpp:31-62,
  * BP/BP5/src/bp5Settings.cpp:30-46) and result line (bp5Run.cpp:208-217,

@@ -1,0 +1,70 @@
+"""Batched solves (bp_batch_*): many problems of uneven degree and size with
+several right-hand sides each, solved together, against the single-problem
+solver and the oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PROBLEMS = [
+    {"nx": 3, "N": 3, "pert": 0.1, "pert_seed": 100, "nrhs": 2, "rhs_seed": 1000},
+    {"nx": 4, "N": 5, "pert": 0.1, "pert_seed": 101, "nrhs": 2, "rhs_seed": 1002},
+    {"nx": 2, "N": 7, "pert": 0.1, "pert_seed": 102, "nrhs": 1, "rhs_seed": 1004},
+    {"nx": 3, "N": 10, "pert": 0.1, "pert_seed": 103, "nrhs": 3, "rhs_seed": 1005},
+]
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def test_batch_fp64_matches_single_solver(gpu):
+    B = gpu.Batch(PROBLEMS, precon="JACOBI", precision="FP64")
+    assert B.nsystems == sum(p["nrhs"] for p in PROBLEMS)
+    stats, ms = B.solve(tol=1e-8, maxit=3000)
+    assert ms > 0
+    sysno = 0
+    for j, p in enumerate(PROBLEMS):
+        gm = gpu.Mesh(p["nx"], N=p["N"], pert=p["pert"], pert_seed=p["pert_seed"])
+        S = gpu.BP(gm, precon="JACOBI")
+        for k in range(p["nrhs"]):
+            assert B.problem[sysno] == j and B.Ngather[sysno] == gm.Ngather
+            b = S.rhs("RANDOM", p["rhs_seed"] + k)
+            x = gpu.DeviceBuffer.from_host(np.zeros(gm.Ngather))
+            st, _, _ = S.solve(x, b, tol=1e-8, maxit=3000)
+            xb, bb = B.vectors(sysno)
+            # the same kernels in the same order: the same iterations and solution
+            np.testing.assert_array_equal(bb, S.rhs("RANDOM", p["rhs_seed"] + k).download())
+            assert stats[sysno].iterations == st.iterations
+            assert _rel(xb, x.download()) < 1e-13
+            assert np.sqrt(stats[sysno].rdotr / stats[sysno].rdotr0) <= 1e-8
+            sysno += 1
+
+
+def test_batch_mixed_reaches_tolerance_against_oracle(gpu, oracle):
+    B = gpu.Batch(PROBLEMS, precon="JACOBI", precision="MIXED")
+    stats, _ = B.solve(tol=1e-8, maxit=5000)
+    for s in range(B.nsystems):
+        p = PROBLEMS[B.problem[s]]
+        k = s - sum(PROBLEMS[i]["nrhs"] for i in range(B.problem[s]))
+        om = oracle.Mesh(p["nx"], p["nx"], p["nx"], p["N"], pert=p["pert"], pert_seed=p["pert_seed"])
+        f_o, b_o = om.rhs_random(p["rhs_seed"] + k)
+        xb, bb = B.vectors(s)
+        assert _rel(bb, b_o) < 1e-13
+        # FP64 residual of the returned solution by the oracle's operator
+        r = b_o - om.operator(xb)
+        assert np.linalg.norm(r) <= 1.0001e-8 * np.linalg.norm(b_o)
+        assert np.sqrt(stats[s].rdotr / stats[s].rdotr0) <= 1e-8
+        x_o, _, it_o, _, _ = om.cg(b_o, 1.0, 1e-10, 5000, precon=True)
+        assert _rel(xb, x_o) < 1e-5
+        assert stats[s].iterations <= 1.25 * it_o + 20
+
+
+def test_batch_bad_arguments(gpu):
+    with pytest.raises(gpu.BPError):
+        gpu.Batch([{"nx": 2, "N": 3, "nrhs": 0}])
+    with pytest.raises(gpu.BPError):
+        gpu.Batch([{"nx": 2, "N": 3, "nrhs": 1}], bp=6)
+    B = gpu.Batch([{"nx": 2, "N": 3, "nrhs": 1}], precision="MIXED")
+    with pytest.raises(gpu.BPError):
+        B.solve(tol=0.0)   # a mixed batch needs a tolerance

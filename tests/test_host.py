@@ -51,3 +51,14 @@ def test_numbering_rejects_bad_sizes(bp):
     # E*Np*Nfields beyond int32 (dlong) is refused, not wrapped
     with pytest.raises(bp.BPError):
         bp.box_numbering(100, 100, 100, 15)
+
+
+def test_uneven_problem_set(bp, oracle):
+    # the LCG matches the reference's (the oracle's restatement)
+    np.testing.assert_array_equal(np.array(bp.lcg_uniform(7, 50)), oracle.random(7, 50))
+    P = bp.uneven_problems()
+    assert len(P) == 64 and all(p["nrhs"] == 4 for p in P)
+    assert {p["N"] for p in P} == set(range(3, 11))
+    assert min(p["nx"] for p in P) >= 8 and max(p["nx"] for p in P) <= 24
+    assert [p["pert_seed"] for p in P] == list(range(100, 164))
+    assert [p["rhs_seed"] for p in P] == [1000 + 4 * i for i in range(64)]
