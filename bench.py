@@ -1,14 +1,19 @@
-"""Benchmark: BP5 p=7 CG throughput (GDOF*iterations/s) on B200.
+"""Benchmark: BP5 p=7 mixed-precision batched CG against plain FP64 CG, to 1e-8.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Workload (one "step"): the BP5 Hex3D problem on a 40x40x40 box with interior
 vertices perturbed by 0.1h (seed 1), degree p=7, stored per-node geometric
-factors, FP64 Jacobi-preconditioned CG for exactly 100 iterations from x=0
-with the seeded nodal forcing b = M f, f = 2u-1 (seed 0).  21,717,639
-unknowns.  `value` is device-timed with every input resident in HBM (the
-step resets x and r, then runs the solve); `e2e` is the same solve through
-the host-buffer entry point (b copied in from pinned memory, x copied back).
+factors (21,717,639 unknowns), with four right-hand sides b = M f, f = 2u-1
+(LCG seeds 0..3), all four solved together by the batched mixed-precision
+Jacobi-PCG (FP32 recursion and operator, FP64 reliable updates) from x = 0 to
+||b - A x|| <= 1e-8 ||b|| in FP64.  `value` is GDOF*iterations/s of that step
+(sum over the four systems of unknowns x iterations, divided by the
+device-timed step); inputs are resident in HBM.  `e2e` is the same step with
+the four b copied in from pinned host memory and the four x copied back, inside
+the timed region.  The comparison the metric names, plain FP64 Jacobi-PCG on
+the same problem to the same tolerance, is measured in the same run and
+reported under "plain_fp64".
 
 With --gpus N > 1 (launched by torch.distributed.run) every rank solves its
 own replica of the problem: the path has no exchange at one rank per problem,
@@ -35,26 +40,23 @@ sys.path.insert(0, ROOT)
 METRIC = "BP5 p=7 GDOF·it/s: mixed+batched vs plain FP64 CG at 1e-8 rel residual"
 UNIT = "GDOF·it/s"
 NX, P, PERT, PERT_SEED, RHS_SEED, ITERS = 40, 7, 0.1, 1, 0, 100
-WORKLOAD = ("BP5 Hex3D p=7, 40^3 elements, interior vertices perturbed 0.1h (seed 1), stored per-node factors, "
-            "FP64 Jacobi-PCG, 100 iterations per step, forcing f=2u-1 (seed 0)")
+NRHS, TOL, MAXIT = 4, 1e-8, 20000
+WORKLOAD = ("BP5 Hex3D p=7, 40^3 elements, interior vertices perturbed 0.1h (seed 1), stored per-node factors; "
+            "4 right-hand sides f=2u-1 (seeds 0..3) solved together by the mixed-precision batched Jacobi-PCG "
+            "(FP32 recursion and operator, FP64 reliable updates) to ||b-Ax|| <= 1e-8 ||b||")
 # CPU sample: the same problem family on a 20^3 sub-box (1/8 of the elements)
 CPU_NX, CPU_ITERS = 20, 100
 MIXED_TOL = 1e-8
-# DRAM traffic of one Ax launch of this workload, from the ncu capture summarised
-# in profiles/ax_bp5_p7_40cubed.md (None until captured)
-AX_DRAM_BYTES = None
+# DRAM traffic of one launch of the FP32 element operator on this workload: the
+# ncu capture of BK5 -fp MIXED on the 20^3 box (profiles/ax_tma_f32_bk5_p7_20cubed.md,
+# 150.4 MB for 8000 elements) scaled by the element count to 64,000 elements
+AX_DRAM_BYTES = 150.36e6 * 8
 
 
-def ax_model_bytes(Ndofs, E, Np, Nf=1):
+def ax_model_bytes(Ndofs, E, Np, Nf=1, s=8):
     # reference byte model of one non-affine Ax (BP/BP5/src/bp5Run.cpp:106-142)
-    return Ndofs * 8 + (Np * 7 * 8 + 4 + Np * Nf * 4 + Np * Nf * 8) * E
-
-
-def cg_model_bytes(Ndofs, E, Np, iters):
-    NL = E * Np
-    bax = ax_model_bytes(Ndofs, E, Np)
-    bg = (Ndofs + 1) * 4 + NL * 4 + NL * 8 + Ndofs * 8
-    return (4 * Ndofs * 8 + bax + bg) + (11 * Ndofs * 8 + bax + bg) * iters
+    # with s-byte values (8: FP64 as the reference; 4: the FP32 inner operator)
+    return Ndofs * s + (Np * 7 * s + 4 + Np * Nf * 4 + Np * Nf * s) * E
 
 
 def read_peaks():
@@ -194,12 +196,11 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ax-launches", type=int, default=20)
-    ap.add_argument("--no-mixed", action="store_true", help="skip the time-to-tolerance comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -209,29 +210,23 @@ def main():
 
     bp.platform_init(local)
     L = bp.lib()
-    mesh = bp.Mesh(NX, NX, NX, N=P, pert=PERT, pert_seed=PERT_SEED)
-    S = bp.BP(mesh, precon="JACOBI")
-    Nd, E, Np = mesh.Ngather, mesh.E, mesh.Np
-    b = S.rhs("RANDOM", RHS_SEED)
-    x = bp.DeviceBuffer(Nd)
-    r = bp.DeviceBuffer(Nd)
-
-    def step():
-        bp._check(L.bp_memset(x.ptr, 0, x.nbytes, None))
-        bp._check(L.bp_memcpy_dtod(r.ptr, b.ptr, r.nbytes, None))
-        st = bp.SolveStats()
-        bp._check(L.bp_solver_solve(S._h, x.ptr, r.ptr, 0.0, ITERS, None, None, bp.ctypes.byref(st)))
-        return st
+    prob = {"nx": NX, "N": P, "pert": PERT, "pert_seed": PERT_SEED, "nrhs": NRHS, "rhs_seed": RHS_SEED}
+    B = bp.Batch([prob], precon="JACOBI", precision="MIXED")
+    Nd = B.Ngather[0]
 
     def ev():
         e = bp.ctypes.c_void_p()
         bp._check(L.bp_event_create(bp.ctypes.byref(e)))
         return e.value
 
+    def step():
+        return B.solve(tol=TOL, maxit=MAXIT)[0]
+
     for _ in range(args.warmup):
         st = step()
-    assert st.iterations == ITERS
-    rel_res = float(np.sqrt(st.rdotr / st.rdotr0))
+    dofit = sum(Nd * s.iterations for s in st)
+    rel_res = max(float(np.sqrt(s.rdotr / s.rdotr0)) for s in st)
+    launches_per_step = sum(s.kernel_launches for s in st)
 
     # ---- device-timed region: K steps, inputs resident in HBM ----
     e0, e1 = ev(), ev()
@@ -241,7 +236,7 @@ def main():
     clocks.start()
     bp._check(L.bp_event_record(e0, None))
     for _ in range(args.steps):
-        step()
+        st = step()
     bp._check(L.bp_event_record(e1, None))
     bp.finish()
     barrier(world)
@@ -249,103 +244,128 @@ def main():
     ms = bp.ctypes.c_float()
     bp._check(L.bp_event_elapsed_ms(e0, e1, bp.ctypes.byref(ms)))
     t_dev = max_over_ranks(ms.value / 1e3, world)
-    value = world * Nd * ITERS * args.steps / t_dev / 1e9
-    # r = b - A x (operator + gather), CG init, 4 kernels per iteration (direction, operator with p.Ap
-    # partials, alpha, gather + r update), final x update
-    launches_per_step = 3 + 4 * ITERS + 1
+    assert sum(Nd * s.iterations for s in st) == dofit
+    value = world * dofit * args.steps / t_dev / 1e9
 
-    # ---- dominant kernel: the element operator, timed alone with events (BK5 style) ----
-    q = b
-    AqL = bp.DeviceBuffer(mesh.NL)
-    for _ in range(3):
-        bp.ax_hex3d(mesh, q, AqL)
-    a0, a1 = ev(), ev()
-    bp._check(L.bp_event_record(a0, None))
-    for _ in range(args.ax_launches):
-        bp.ax_hex3d(mesh, q, AqL)
-    bp._check(L.bp_event_record(a1, None))
-    bp._check(L.bp_event_elapsed_ms(a0, a1, bp.ctypes.byref(ms)))
-    ax_s = ms.value / 1e3 / args.ax_launches
-    ax_bytes = ax_model_bytes(Nd, E, Np)
-    peak, peak_kind = read_peaks()
-    achieved = ax_bytes / ax_s / 1e9
-    del AqL
+    # ---- end to end: the four b from pinned host memory in, the four x out ----
+    bh = [bp.PinnedBuffer(Nd) for _ in range(NRHS)]
+    xh = [bp.PinnedBuffer(Nd) for _ in range(NRHS)]
+    dev = []
+    for k in range(NRHS):
+        xp, bptr = bp.ctypes.c_void_p(), bp.ctypes.c_void_p()
+        bp._check(L.bp_batch_vectors(B._h, k, bp.ctypes.byref(xp), bp.ctypes.byref(bptr)))
+        dev.append((xp.value, bptr.value))
+        bh[k].array[:] = B.vectors(k)[1]
+    nbytes = 8 * Nd
 
-    # ---- end to end through the host-buffer entry point ----
-    bh = bp.PinnedBuffer(Nd)
-    xh = bp.PinnedBuffer(Nd)
-    bh.array[:] = b.download()
-    S.solve_host(bh.array, xh.array, 0.0, ITERS)   # warm
+    def e2e_step():
+        for k in range(NRHS):
+            bp._check(L.bp_memcpy_htod(dev[k][1], bh[k].array.ctypes.data, nbytes, None))
+        B.solve(tol=TOL, maxit=MAXIT)
+        for k in range(NRHS):
+            bp._check(L.bp_memcpy_dtoh(xh[k].array.ctypes.data, dev[k][0], nbytes, None))
+        bp.finish()
+
+    e2e_step()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        S.solve_host(bh.array, xh.array, 0.0, ITERS)
+        e2e_step()
     t1 = time.perf_counter()
     barrier(world)
     t_e2e = max_over_ranks(t1 - t0, world)
-    e2e = world * Nd * ITERS * args.steps / t_e2e / 1e9
+    e2e = world * dofit * args.steps / t_e2e / 1e9
+    # FP64 check of the returned solutions
+    Ax = bp.DeviceBuffer(Nd)
+    xd = bp.DeviceBuffer(Nd)
+    resid = []
+    for k in range(NRHS):
+        xd.upload(xh[k].array)
+        B.operator(k, xd, Ax)
+        resid.append(float(np.linalg.norm(bh[k].array - Ax.download()) / np.linalg.norm(bh[k].array)))
 
-    # ---- time to 1e-8 relative residual: FP64 Jacobi-CG against the mixed solver ----
-    mixed = None
-    if not args.no_mixed:
-        Sm = bp.BP(mesh, precon="JACOBI", precision="MIXED")
+    # ---- the comparison: plain FP64 Jacobi-PCG on the same problem and tolerance ----
+    mesh = bp.Mesh(NX, NX, NX, N=P, pert=PERT, pert_seed=PERT_SEED)
+    S = bp.BP(mesh, precon="JACOBI")
+    b0 = S.rhs("RANDOM", RHS_SEED)
+    x = bp.DeviceBuffer(Nd)
+    r = bp.DeviceBuffer(Nd)
 
-        def to_tol(solver):
-            bp._check(L.bp_memset(x.ptr, 0, x.nbytes, None))
-            bp._check(L.bp_memcpy_dtod(r.ptr, b.ptr, r.nbytes, None))
-            st = bp.SolveStats()
-            bp._check(L.bp_solver_solve(solver._h, x.ptr, r.ptr, MIXED_TOL, 50000, None, None, bp.ctypes.byref(st)))
-            return st
+    def fp64_solve(tol, maxit):
+        bp._check(L.bp_memset(x.ptr, 0, x.nbytes, None))
+        bp._check(L.bp_memcpy_dtod(r.ptr, b0.ptr, r.nbytes, None))
+        st = bp.SolveStats()
+        bp._check(L.bp_solver_solve(S._h, x.ptr, r.ptr, tol, maxit, None, None, bp.ctypes.byref(st)))
+        return st
 
-        to_tol(S)
-        to_tol(Sm)                                  # warm: graphs captured, caches primed
-        barrier(world)
-        st64 = to_tol(S)
-        stmx = to_tol(Sm)
-        t64 = max_over_ranks(st64.elapsed_ms / 1e3, world)
-        tmx = max_over_ranks(stmx.elapsed_ms / 1e3, world)
-        # FP64 check of the mixed solution's residual
-        Ax = bp.DeviceBuffer(Nd)
-        S.operator(x, Ax)
-        resid = float(np.linalg.norm(b.download() - Ax.download()) / np.linalg.norm(b.download()))
-        mixed = {"tolerance": MIXED_TOL,
-                 "fp64": {"iterations": st64.iterations, "seconds": t64,
-                          "gdof_it_s": world * Nd * st64.iterations / t64 / 1e9,
-                          "relative_residual": float(np.sqrt(st64.rdotr / st64.rdotr0))},
-                 "mixed": {"iterations": stmx.iterations, "reliable_updates": stmx.updates, "seconds": tmx,
-                           "gdof_it_s": world * Nd * stmx.iterations / tmx / 1e9,
-                           "relative_residual_fp64_check": resid},
-                 "speedup_time_to_solution": t64 / tmx,
-                 "speedup_gdof_it_s": (stmx.iterations / tmx) / (st64.iterations / t64)}
-        del Sm, Ax
+    fp64_solve(TOL, MAXIT)
+    st64 = fp64_solve(TOL, MAXIT)
+    t64 = max_over_ranks(st64.elapsed_ms / 1e3, world)
+    plain = {"iterations": st64.iterations, "seconds": t64, "gdof_it_s": world * Nd * st64.iterations / t64 / 1e9,
+             "relative_residual": float(np.sqrt(st64.rdotr / st64.rdotr0))}
+    # and the reference's own step, exactly 100 FP64 iterations (bp5Run.cpp:71-95)
+    fp64_solve(0.0, ITERS)
+    st100 = fp64_solve(0.0, ITERS)
+    plain["fixed_100_iterations_gdof_it_s"] = world * Nd * ITERS / (st100.elapsed_ms / 1e3) / 1e9
+
+    # ---- dominant kernel of the step: the FP32 element operator, timed alone ----
+    v = mesh.view
+    ng = mesh.E * mesh.Np
+    ops = {"wJ": bp.DeviceBuffer(ng, np.float32), "ggeo": bp.DeviceBuffer(6 * ng, np.float32),
+           "gllw": bp.DeviceBuffer(mesh.Nq, np.float32), "D": bp.DeviceBuffer(mesh.Nq * mesh.Nq, np.float32)}
+    for name, n in (("wJ", ng), ("ggeo", 6 * ng), ("gllw", mesh.Nq), ("D", mesh.Nq * mesh.Nq)):
+        bp.convert_f64_f32(getattr(v, name), n, ops[name])
+    q32 = bp.DeviceBuffer(Nd, np.float32)
+    bp.convert_f64_f32(b0, Nd, q32)
+    AqL = bp.DeviceBuffer(mesh.NL, np.float32)
+    for _ in range(3):
+        bp.ax_hex3d_f32(mesh, q32, AqL, ops)
+    a0, a1 = ev(), ev()
+    bp._check(L.bp_event_record(a0, None))
+    for _ in range(args.ax_launches):
+        bp.ax_hex3d_f32(mesh, q32, AqL, ops)
+    bp._check(L.bp_event_record(a1, None))
+    bp._check(L.bp_event_elapsed_ms(a0, a1, bp.ctypes.byref(ms)))
+    ax_s = ms.value / 1e3 / args.ax_launches
+    E, Np = mesh.E, mesh.Np
+    ax_bytes = ax_model_bytes(Nd, E, Np, s=4)
+    peak, peak_kind = read_peaks()
+    achieved = ax_bytes / ax_s / 1e9
+    del AqL, ops, q32
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample, _ = cpu_sample(steps=1, warmup=0)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        cv, cores, sample, _ = cpu_sample(steps=1, warmup=0)
+        cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
-        step_bytes = cg_model_bytes(Nd, E, Np, ITERS)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded LCG forcing f=2u-1 (seed 0) on a seeded perturbed box (seed 1)",
-            "config": {"workload": WORKLOAD, "nx": NX, "ny": NX, "nz": NX, "p": P, "Ndofs": Nd,
-                       "iterations_per_step": ITERS, "precon": "JACOBI", "parallelism": "replicas" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (geometric factors 1.84 GB per step pass)",
-                       "final_relative_residual": rel_res},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
+            "data": "synthetic: seeded LCG forcing f=2u-1 (seeds 0..3) on a seeded perturbed box (seed 1)",
+            "config": {"workload": WORKLOAD, "nx": NX, "ny": NX, "nz": NX, "p": P, "Ndofs": Nd, "rhs": NRHS,
+                       "tolerance": TOL, "precon": "JACOBI",
+                       "iterations_per_system": [s.iterations for s in st],
+                       "reliable_updates_per_system": [s.updates for s in st],
+                       "final_relative_residual_max": rel_res,
+                       "fp64_check_relative_residual": resid,
+                       "parallelism": "replicas" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (FP32 factors 0.92 GB read per operator apply)"},
             "clocks": clk,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * Nd, "d2h_bytes_per_step": 8 * Nd},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": NRHS * 8 * Nd,
+                    "d2h_bytes_per_step": NRHS * 8 * Nd},
             "gpu_launches": launches_per_step * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,double> (bp_ax_hex3d)", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes, "launch_ms": ax_s * 1e3},
-            "model_bw_gbs": step_bytes * args.steps / (t_dev / world) / 1e9 if world == 1 else None,
+            "plain_fp64": plain,
+            "speedup_vs_plain_fp64": value / plain["gdof_it_s"],
+            "roofline": {"bound": "hbm", "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,float> (bp_ax_hex3d_f32)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes,
+                         "launch_ms": ax_s * 1e3},
             "cpu_baseline": cpu,
-            "mixed_vs_fp64_to_1e-8": mixed,
         }
         print(json.dumps(line))
+    del B
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

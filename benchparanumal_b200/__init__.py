@@ -45,7 +45,7 @@ EXPORTS = [
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc",
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
-    "bp_batch_vectors", "bp_batch_solver",
+    "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32",
 ]
 
 
@@ -94,7 +94,7 @@ class SolverDesc(ctypes.Structure):
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("rdotr0", ctypes.c_double), ("rdotr", ctypes.c_double),
-                ("elapsed_ms", ctypes.c_double), ("updates", ctypes.c_int32)]
+                ("elapsed_ms", ctypes.c_double), ("updates", ctypes.c_int32), ("kernel_launches", ctypes.c_int64)]
 
 
 _lib = None
@@ -166,6 +166,8 @@ def lib():
             "bp_batch_solve": [vp, dbl, i32, ctypes.POINTER(SolveStats), ctypes.POINTER(dbl)],
             "bp_batch_vectors": [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(vp)],
             "bp_batch_solver": [vp, i32, ctypes.POINTER(vp)],
+            "bp_ax_hex3d_f32": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp, vp],
+            "bp_convert_f64_f32": [sz, vp, vp, vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -349,6 +351,20 @@ def ax_cub_hex3d(mesh, bp, q, Aq, lam=1.0, stream=None):
     d = AxDesc(bp, mesh.N, int(mesh.affine), mesh.Nfields)
     _check(lib().bp_ax_cub_hex3d(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, c.cubwJ, c.cubggeo,
                                  c.cubD, c.cubInterp, c.invV, c.MM, float(lam), _ptr(q), _ptr(Aq), stream))
+
+
+def convert_f64_f32(src, n, dst, stream=None):
+    """dst (FP32 device) = src (FP64 device address or buffer), n elements."""
+    _check(lib().bp_convert_f64_f32(n, src if isinstance(src, int) else _ptr(src), _ptr(dst), stream))
+
+
+def ax_hex3d_f32(mesh, q, Aq, ops, lam=1.0, stream=None):
+    """bp_ax_hex3d_f32 on FP32 device buffers; ops = dict of FP32 buffers wJ, ggeo, gllw, D."""
+    v = mesh.view
+    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    _check(lib().bp_ax_hex3d_f32(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, _ptr(ops["wJ"]),
+                                 _ptr(ops["ggeo"]), _ptr(ops["gllw"]), _ptr(ops["D"]), float(lam), _ptr(q),
+                                 _ptr(Aq), stream))
 
 
 def ogs_gather(mesh, v, gv, stream=None):

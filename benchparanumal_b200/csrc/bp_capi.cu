@@ -207,6 +207,23 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                    to_stream(stream));
 }
 
+int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                    const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
+                    const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream) {
+  BP_TRY(check_ax_desc(desc));
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  if (!elementList || !GlobalToLocal || !wJ || !ggeo || !D || !q || !Aq || (desc->affine && !gllw))
+    return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32: null array");
+  return launch_ax_skip(*desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq, nullptr,
+                        to_stream(stream));
+}
+
+int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream) {
+  if (n > 0 && (!src || !dst)) return fail(BP_ERROR_ARG, "bp_convert_f64_f32: null array");
+  return launch_d2f(n, src, dst, to_stream(stream));
+}
+
 int bp_ax_cub_hex3d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* elementList,
                     const int32_t* GlobalToLocal, const double* cubwJ, const double* cubggeo, const double* cubD,
                     const double* cubInterp, const double* invV, const double* MM, double lambda, const double* q,

@@ -216,16 +216,26 @@ struct DevVec {
   explicit DevVec(size_t n) { check(bp_malloc(reinterpret_cast<void**>(&p), n * sizeof(double))); }
   ~DevVec() { bp_free(p); }
 };
+struct DevVec32 {
+  float* p = nullptr;
+  explicit DevVec32(size_t n) {
+    if (n) check(bp_malloc(reinterpret_cast<void**>(&p), n * sizeof(float)));
+  }
+  ~DevVec32() {
+    if (p) bp_free(p);
+  }
+};
 
 // reference byte model for one Ax application: BP5/BP6 bp5Run.cpp:106-142,
 // bk5Run.cpp:97-125; BP3/BP4 bp3Run.cpp:107-122; BP1/BP2 bp1Run.cpp and
-// bk1Run.cpp (one factor per point, J or JW)
-double ax_bytes(int bp, const bp_mesh_view_t& v, long long Ndofs) {
+// bk1Run.cpp (one factor per point, J or JW).  sv: bytes per value (8 as the
+// reference; 4 for the FP32 operator of the mixed-precision solver).
+double ax_bytes(int bp, const bp_mesh_view_t& v, long long Ndofs, double sv = 8.0) {
   const double E = v.Nelements, Np = v.Np, Nf = v.Nfields;
   const double cNq = v.N + 2, cNp = cNq * cNq * cNq;
   const double per_point = bp <= 2 ? 1.0 : 7.0;          // J, or ggeo + wJ
   const double points = v.affine ? 1.0 : (bp <= 4 ? cNp : Np);
-  return Ndofs * 8.0 + (points * per_point * 8.0 + 4.0 + Np * Nf * 4.0 + Np * Nf * 8.0) * E;
+  return Ndofs * sv + (points * per_point * sv + 4.0 + Np * Nf * 4.0 + Np * Nf * sv) * E;
 }
 // reference flop model for one Ax application (the same files, Hex branches)
 double ax_flops(int bp, const bp_mesh_view_t& v) {
@@ -317,8 +327,25 @@ int run_bk(const char* name, int bk, Settings& S) {
   d.N = P.view.N;
   d.affine = P.view.affine;
   d.Nfields = Nfields;
+  // -fp MIXED times the FP32 operator of the mixed-precision solver (BK5/BK6)
+  const bool fp32 = S.compare("PRECISION", "MIXED");
+  if (fp32 && bk < 5) throw std::runtime_error("-fp MIXED is available for BK5 and BK6");
+  const size_t ng = P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.view.Np;
+  DevVec32 wJ32(fp32 ? ng : 0), ggeo32(fp32 ? 6 * ng : 0), gllw32(fp32 ? P.view.Nq : 0),
+      D32(fp32 ? (size_t)P.view.Nq * P.view.Nq : 0), q32(fp32 ? (size_t)Ngather : 0),
+      Aq32(fp32 ? (size_t)P.view.Nlocal : 0);
+  if (fp32) {
+    check(bp_convert_f64_f32(ng, P.view.wJ, wJ32.p, nullptr));
+    check(bp_convert_f64_f32(6 * ng, P.view.ggeo, ggeo32.p, nullptr));
+    check(bp_convert_f64_f32(P.view.Nq, P.view.gllw, gllw32.p, nullptr));
+    check(bp_convert_f64_f32((size_t)P.view.Nq * P.view.Nq, P.view.D, D32.p, nullptr));
+    check(bp_convert_f64_f32(Ngather, q.p, q32.p, nullptr));
+  }
   auto apply = [&]() {
-    if (bk >= 5)
+    if (fp32)
+      check(bp_ax_hex3d_f32(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, wJ32.p, ggeo32.p,
+                            gllw32.p, D32.p, 1.0f, q32.p, Aq32.p, nullptr));
+    else if (bk >= 5)
       check(bp_ax_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
                         P.view.gllw, P.view.D, 1.0, q.p, Aq.p, nullptr));
     else
@@ -333,7 +360,7 @@ int run_bk(const char* name, int bk, Settings& S) {
   const double t1 = now_after_finish();
   const double elapsed = (t1 - t0) / Ntests;
   const long long Ndofs = Ngather;
-  const double Nbytes = ax_bytes(bk, P.view, Ndofs);
+  const double Nbytes = ax_bytes(bk, P.view, Ndofs, fp32 ? 4.0 : 8.0);
   const double Nflops = ax_flops(bk, P.view);
   std::string suffix = "Element=Hex";
   if (P.view.affine) suffix += ", Affine";

@@ -161,6 +161,7 @@ int launch_mass_local(int N, int affine, int Nfields, int E, const int32_t* G2L,
 int launch_diag_local(int N, int affine, int Nfields, int E, const double* ggeo, const double* wJ,
                       const double* gllw, const double* D, double lambda, double* dL, cudaStream_t s);
 int launch_set(int32_t N, double alpha, double* x, cudaStream_t s);
+int launch_d2f(size_t n, const double* a, float* b, cudaStream_t s);   // b = (float) a
 int launch_axpy(int32_t N, double alpha, const double* x, double beta, double* y, cudaStream_t s);
 int launch_reciprocal(int32_t N, double* x, cudaStream_t s);
 int launch_sqrt1(double* v, cudaStream_t s);   // v[0] = sqrt(v[0]) on the device

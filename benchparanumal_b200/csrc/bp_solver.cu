@@ -298,6 +298,15 @@ static int vec_grid(int32_t N) {
   return g < 1 ? 1 : g;
 }
 
+int launch_d2f(size_t n, const double* a, float* b, cudaStream_t s) {
+  if (n == 0) return BP_SUCCESS;
+  size_t g = (n + 255) / 256;
+  if (g > 8192) g = 8192;
+  d2f_kernel<<<(unsigned)g, 256, 0, s>>>(n, a, b);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
 static int to_float(const double* a, float* b, size_t n, cudaStream_t s) {
   if (n == 0) return BP_SUCCESS;
   size_t g = (n + 255) / 256;
@@ -326,6 +335,7 @@ struct bp_solver_s {
   DeviceArray<unsigned int> counter;
   DeviceArray<CgScalars> sc;
   CgScalars* scal = nullptr;   // the CG scalars: sc.ptr, or a slot of a batch's array
+  int64_t launches = 0;        // kernels launched (graph nodes included) since the solve began
   int hist_len = 0;
   // graph of kChunk iterations, keyed by the vectors it was captured for
   cudaGraphExec_t graph = nullptr;
@@ -407,6 +417,7 @@ static int elem_apply(bp_solver_s* S, const ElemOperands<V>& o, const V* q, V* A
 
 static int operator_apply(bp_solver_s* S, const double* q, double* Aq, const int* skip, cudaStream_t s) {
   bp_mesh_s* m = S->mesh;
+  S->launches += 2;
   BP_TRY(elem_apply<double>(S, operands64(S), q, S->AqL.ptr, skip, s));
   return launch_gather(m->Ngather, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, Aq, s);
 }
@@ -504,6 +515,7 @@ static int finish_solve(bp_solver_s* S, const CgScalars& h, double* hist_rnorm, 
     stats->rdotr0 = h.rdotr0;
     stats->rdotr = S->mixed ? h.rtrue2 : h.rdotr;
     stats->updates = updates;
+    stats->kernel_launches = S->launches;
     stats->elapsed_ms = 0.0;
     if (record_events) {
       float ms = 0.f;
@@ -521,9 +533,11 @@ static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxi
   const int32_t N = S->N;
   BP_TRY(ensure_hist(S, maxit));
   BP_TRY(ensure_graph(S, x, r, s));
+  S->launches = 0;
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
   // r = b - A x
   BP_TRY(operator_apply(S, x, S->Ap.ptr, nullptr, s));
+  S->launches += 1;
   cg_init_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, S->Ap.ptr, r, S->invD.ptr, S->scal, tol, maxit, S->precon,
                                                   S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
@@ -531,11 +545,13 @@ static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxi
   CgScalars h{};
   for (int c = 0; c < nchunks; ++c) {
     BP_CUDA_TRY(cudaGraphLaunch(S->graph, s));
+    S->launches += 4 * kChunk;
     if (tol > 0.0 && c + 1 < nchunks) {
       BP_TRY(read_scalars(S, h, s));
       if (h.done) break;
     }
   }
+  S->launches += 1;
   cg_final_kernel<double><<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->scal);
   BP_CUDA_TRY(cudaGetLastError());
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev1, s));
@@ -547,6 +563,7 @@ static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxi
 static int mixed_replace(bp_solver_s* S, double* x, double* r, bool init, double tol, int maxit, cudaStream_t s) {
   const int32_t N = S->N;
   BP_TRY(operator_apply(S, x, S->Ap.ptr, nullptr, s));
+  S->launches += 1;
   mixed_replace_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, S->bcopy.ptr, S->Ap.ptr, r, S->r32.ptr, S->invD32.ptr,
                                                         S->scal, init ? 1 : 0, tol, maxit, S->precon,
                                                         S->partials.ptr, S->counter.ptr);
@@ -565,6 +582,7 @@ static int mixed_begin(bp_solver_s* S, double* x, double* r, double tol, int max
 // reliable update: fold the pending x_lo step, x_hi += x_lo, FP64 residual
 static int mixed_reliable(bp_solver_s* S, double* x, double* r, double tol, int maxit, cudaStream_t s) {
   const int32_t N = S->N;
+  S->launches += 2;
   cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, S->x32.ptr, S->p32.ptr, S->scal);
   BP_CUDA_TRY(cudaGetLastError());
   mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, x, S->x32.ptr);
@@ -577,6 +595,7 @@ static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int max
   if (!(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_solver_solve: a mixed-precision solve needs tol > 0");
   BP_TRY(ensure_hist(S, maxit));
   if (!S->graph32) BP_TRY(capture(&S->graph32, s, body32, S, nullptr, nullptr));
+  S->launches = 0;
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
   BP_TRY(mixed_begin(S, x, r, tol, maxit, s));
   CgScalars h{};
@@ -588,6 +607,7 @@ static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int max
       ++updates;
     } else {
       BP_CUDA_TRY(cudaGraphLaunch(S->graph32, s));
+      S->launches += 4 * kChunk;
     }
     BP_TRY(read_scalars(S, h, s));
     if (h.breakdown) break;
@@ -867,6 +887,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
   if (B->mixed && !(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_batch_solve: a mixed-precision batch needs tol > 0");
   BP_TRY(batch_capture(B, s));
   std::vector<int> updates(ns, 0);
+  for (auto* S : B->solvers) S->launches = 0;
   BP_CUDA_TRY(cudaEventRecord(B->ev0, s));
   // x = 0, r = b, and each system's start
   for (size_t i = 0; i < ns; ++i) {
@@ -878,6 +899,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       BP_TRY(mixed_begin(S, B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
     } else {
       BP_TRY(operator_apply(S, B->x[i]->ptr, S->Ap.ptr, nullptr, s));
+      S->launches += 1;
       cg_init_kernel<<<vec_grid(S->N), kThreads, 0, s>>>(S->N, S->Ap.ptr, B->r[i]->ptr, S->invD.ptr, S->scal, tol,
                                                           maxit, S->precon, S->partials.ptr, S->counter.ptr);
       BP_CUDA_TRY(cudaGetLastError());
@@ -903,11 +925,13 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
     }
     if (!running) break;
     BP_CUDA_TRY(cudaGraphLaunch(B->graph, s));
+    for (auto* S : B->solvers) S->launches += 4 * kChunk;
     BP_TRY(batch_read(B, h, s));
   }
   if (!B->mixed)
     for (size_t i = 0; i < ns; ++i) {
       bp_solver_s* S = B->solvers[i];
+      S->launches += 1;
       cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, s>>>(S->N, B->x[i]->ptr, S->p.ptr, S->scal);
       BP_CUDA_TRY(cudaGetLastError());
     }
@@ -925,6 +949,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       stats[i].rdotr = B->mixed ? h[i].rtrue2 : h[i].rdotr;
       stats[i].elapsed_ms = ms;
       stats[i].updates = updates[i];
+      stats[i].kernel_launches = B->solvers[i]->launches;
     }
     breakdown = breakdown || h[i].breakdown;
   }

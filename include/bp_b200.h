@@ -100,6 +100,15 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                 const double* gllw, const double* D, double lambda, const double* q,
                 double* Aq, bp_stream_t stream);
 
+/* The same operator in FP32 (the inner operator of the mixed-precision CG):
+   all arrays FP32, dot products of the CG stay FP64.  No counterpart in the
+   reference (dfloat is FP64 there, include/types.h:31-39). */
+int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                    const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
+                    const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream);
+/* dst[i] = (float) src[i], i < n, device arrays (to build FP32 operands). */
+int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream);
+
 /* Element-local over-integrated operators of BP1-BP4 on N+2 Gauss points per
    direction, Aq[e] = A_e q[GlobalToLocal].  Replaces bp1AxHex3D / bp2AxHex3D
    (mass, okl/bp1AxHex3D.okl, okl/bp2AxHex3D.okl), bp3AxHex3D / bp4AxHex3D
@@ -283,6 +292,7 @@ typedef struct bp_solve_stats {
   double rdotr;            /* final r.r (mixed: of the FP64 residual b - A x)      */
   double elapsed_ms;       /* device time of the solve (CUDA events)               */
   int32_t updates;         /* mixed: FP64 residual replacements; FP64: 0           */
+  int64_t kernel_launches; /* kernels launched by the solve, CUDA-graph nodes included */
 } bp_solve_stats_t;
 
 int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* desc, bp_solver_t* solver);
