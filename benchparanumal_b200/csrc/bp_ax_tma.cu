@@ -23,6 +23,7 @@
 
 #include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
+#include "bp_pack.cuh"
 
 namespace bp {
 
@@ -110,29 +111,45 @@ struct TmaShape {
 
 }  // namespace
 
-// F is the arithmetic and storage type of factors, q, Aq (double, or float for
-// the inner solve of the mixed-precision CG); p.Ap partials are summed in double.
-template <int NQ, int NF, bool DOT, int R, class F>
+// Shared-memory layout of ax_tma_kernel: [EPB][R] slots of ggeo slices, [EPB][R]
+// slots of wJ slices, D, then the q/v/w scratch of the S slots (values of type
+// T, 16-byte aligned), then R mbarriers.
+template <int NQ, int NF, int R, class F, class T>
+struct TmaSmem {
+  using Sh = TmaShape<NQ, F>;
+  static constexpr int S = Sh::EPB * NF;
+  static constexpr int PAD = 1;   // rows of NQ+1: conflict-free row and column walks
+  static constexpr size_t FACT = sizeof(F) * ((size_t)Sh::EPB * R * (Sh::SLICE_G + Sh::NQ2) + NQ * (NQ + 2));
+  static constexpr size_t QOFF = (FACT + 15) & ~(size_t)15;
+  static constexpr size_t QVALS = (size_t)S * NQ * (NQ + PAD);
+  static constexpr size_t BAR = (QOFF + 3 * QVALS * sizeof(T) + 7) & ~(size_t)7;
+  static constexpr size_t BYTES = BAR + sizeof(uint64_t) * R;
+};
+
+// F is the arithmetic and storage type of the factors (double, or float for the
+// inner solve of the mixed-precision CG); T the type of the q and Aq values: F,
+// or Pack<F, PK> for PK right-hand sides of one mesh in lockstep (then NF = 1
+// and the q/Aq arrays hold one pack per node).  p.Ap partials are summed in
+// double, one per lane: fuse.partials[lane * gridDim.x + blockIdx.x].
+template <int NQ, int NF, bool DOT, int R, class F, class T>
 __global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF)
 ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
               const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
-              const F* __restrict__ q, F* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
+              const T* __restrict__ q, T* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
   if (skip && *skip) return;
   using Sh = TmaShape<NQ, F>;
+  using Lay = TmaSmem<NQ, NF, R, F, T>;
   using V2 = typename Vec2<F>::type;
-  constexpr int NQ2 = Sh::NQ2, NP = NQ2 * NQ, EPB = Sh::EPB, S = EPB * NF;
-  constexpr int PAD = 1;   // rows of NQ+1: conflict-free row and column walks
+  constexpr int NQ2 = Sh::NQ2, NP = NQ2 * NQ, EPB = Sh::EPB, S = EPB * NF, LANES = PackTraits<T>::R;
+  constexpr int PAD = Lay::PAD;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  // layout: [EPB][R] slots of ggeo slices, [EPB][R] slots of wJ slices, D, q/v/w scratch, barriers
   F* s_g = reinterpret_cast<F*>(smem_raw);
   F* s_J = s_g + EPB * R * Sh::SLICE_G;
   F* s_D = s_J + EPB * R * NQ2;                     // [NQ][NQ] row-major, rows 8-byte aligned
-  F* s_q = s_D + NQ * (NQ + 2);                     // [S][NQ][NQ+PAD]
-  F* s_v = s_q + S * NQ * (NQ + PAD);
-  F* s_w = s_v + S * NQ * (NQ + PAD);
-  uint64_t* s_bar = reinterpret_cast<uint64_t*>(
-      smem_raw + ((sizeof(F) * (size_t)(EPB * R * (Sh::SLICE_G + NQ2) + NQ * (NQ + 2) + 3 * S * NQ * (NQ + PAD)) + 7) &
-                  ~(size_t)7));   // [R]
+  T* s_q = reinterpret_cast<T*>(smem_raw + Lay::QOFF);   // [S][NQ][NQ+PAD]
+  T* s_v = s_q + Lay::QVALS;
+  T* s_w = s_v + Lay::QVALS;
+  uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem_raw + Lay::BAR);   // [R]
 
   const int i = threadIdx.x, j = threadIdx.y, slot = threadIdx.z;
   const int t = i + NQ * (j + NQ * slot);
@@ -162,15 +179,15 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
 
   // the pencil of q and the D rows of this thread, while the copies fly
   const size_t lbase = ((size_t)e * NF + f) * NP + j * NQ + i;
-  F r_u[NQ], r_Au[NQ];
+  T r_u[NQ], r_Au[NQ];
   {
     int id[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) id[k] = active ? __ldg(G2L + lbase + k * NQ2) : -1;
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
-      r_u[k] = (id[k] >= 0) ? __ldg(q + id[k]) : F(0);
-      r_Au[k] = F(0);
+      r_u[k] = (id[k] >= 0) ? q[id[k]] : pack_zero<T>();
+      r_Au[k] = pack_zero<T>();
     }
   }
   __syncthreads();   // s_D
@@ -183,9 +200,9 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     Di[m] = s_D[i * NQ + m];
     Dj[m] = s_D[j * NQ + m];
   }
-  F* sq = s_q + slot * NQ * (NQ + PAD);
-  F* sv = s_v + slot * NQ * (NQ + PAD);
-  F* sw = s_w + slot * NQ * (NQ + PAD);
+  T* sq = s_q + slot * NQ * (NQ + PAD);
+  T* sv = s_v + slot * NQ * (NQ + PAD);
+  T* sw = s_w + slot * NQ * (NQ + PAD);
   bool ok = true;
 
 #pragma unroll
@@ -206,7 +223,7 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
       Dk[m] = d2.x;
       Dk[m + 1] = d2.y;
     }
-    F ur = 0, us = 0, ut = 0;
+    T ur = pack_zero<T>(), us = pack_zero<T>(), ut = pack_zero<T>();
 #pragma unroll
     for (int m = 0; m < NQ; ++m) ut += Dk[m] * r_u[m];
 #pragma unroll
@@ -216,8 +233,8 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     }
     sw[j * (NQ + PAD) + i] = G01 * ur + G11 * us + G12 * ut;
     sv[j * (NQ + PAD) + i] = G00 * ur + G01 * us + G02 * ut;
-    const F GDut = G02 * ur + G12 * us + G22 * ut;
-    F Auk = GwJ * lambda * r_u[k], Auk2 = 0;
+    const T GDut = G02 * ur + G12 * us + G22 * ut;
+    T Auk = (GwJ * lambda) * r_u[k], Auk2 = pack_zero<T>();
     __syncthreads();
     // slot rs is free again: refill it with slice k+R
     if (R < NQ && k + R < NQ && t == 0) {
@@ -247,55 +264,53 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     for (int k = 0; k < NQ; ++k) Aq[lbase + k * NQ2] = r_Au[k];
   }
   if (DOT) {
-    double v = 0.0;
+    double v[LANES];
+#pragma unroll
+    for (int l = 0; l < LANES; ++l) v[l] = 0.0;
     if (active) {
 #pragma unroll
-      for (int k = 0; k < NQ; ++k) v += (double)r_u[k] * (double)r_Au[k];
+      for (int k = 0; k < NQ; ++k) lane_dot(v, r_u[k], r_Au[k]);
     }
     // the factor ring is free now and holds at least one double per thread
-    fuse_pap(v, fuse, reinterpret_cast<double*>(s_g));
+#pragma unroll
+    for (int l = 0; l < LANES; ++l) {
+      const double bs = fuse_block_sum(v[l], reinterpret_cast<double*>(s_g));
+      if (t == 0) fuse.partials[(size_t)l * gridDim.x + blockIdx.x] = bs;
+    }
   }
 }
 
-template <int NQ, int NF, int R, class F>
-static size_t tma_smem_bytes() {
-  using Sh = TmaShape<NQ, F>;
-  constexpr int S = Sh::EPB * NF;
-  const size_t vals = (size_t)Sh::EPB * R * (Sh::SLICE_G + Sh::NQ2) + NQ * (NQ + 2) + 3 * S * NQ * (NQ + 1);
-  return ((sizeof(F) * vals + 7) & ~(size_t)7) + sizeof(uint64_t) * R;
-}
-
-template <int NQ, int NF, bool DOT, class F>
+template <int NQ, int NF, bool DOT, class F, class T>
 static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ,
-                          const F* ggeo, const F* D, F lambda, const F* q, F* Aq, const int* skip,
+                          const F* ggeo, const F* D, F lambda, const T* q, T* Aq, const int* skip,
                           const CgFuse& fuse, cudaStream_t s, int* nblocks) {
   using Sh = TmaShape<NQ, F>;
   constexpr int R = Sh::R;
-  const size_t smem = tma_smem_bytes<NQ, NF, R, F>();
+  const size_t smem = TmaSmem<NQ, NF, R, F, T>::BYTES;
   static bool configured = false;
   if (!configured) {
-    BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, NF, DOT, R, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+    BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, NF, DOT, R, F, T>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = true;
   }
   const dim3 block(NQ, NQ, Sh::EPB * NF);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
-  ax_tma_kernel<NQ, NF, DOT, R, F><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q,
-                                                             Aq, skip, fuse);
+  ax_tma_kernel<NQ, NF, DOT, R, F, T><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda,
+                                                                q, Aq, skip, fuse);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
-template <int NQ, int NF, class F>
+template <int NQ, int NF, class F, class T>
 static int launch_tma(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ, const F* ggeo,
-                      const F* D, F lambda, const F* q, F* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                      const F* D, F lambda, const T* q, T* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                       int* nblocks) {
   if (fuse)
-    return launch_tma_dot<NQ, NF, true, F>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, *fuse, s,
-                                           nblocks);
-  return launch_tma_dot<NQ, NF, false, F>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, CgFuse{},
-                                          s, nblocks);
+    return launch_tma_dot<NQ, NF, true, F, T>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, *fuse,
+                                              s, nblocks);
+  return launch_tma_dot<NQ, NF, false, F, T>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip,
+                                             CgFuse{}, s, nblocks);
 }
 
 // Stored-factor operator through the TMA path.  Returns 1 (and launches
@@ -314,10 +329,10 @@ static int launch_ax_tma_t(const bp_ax_desc_t& d, int32_t Nelements, const int32
 #define BP_TMA_ARGS Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks
 #define BP_TMA_CASE(nq) \
   case nq:              \
-    return three ? launch_tma<nq, 3, F>(BP_TMA_ARGS) : launch_tma<nq, 1, F>(BP_TMA_ARGS);
+    return three ? launch_tma<nq, 3, F, F>(BP_TMA_ARGS) : launch_tma<nq, 1, F, F>(BP_TMA_ARGS);
 #define BP_TMA_CASE1(nq) \
   case nq:               \
-    return launch_tma<nq, 1, F>(BP_TMA_ARGS);
+    return launch_tma<nq, 1, F, F>(BP_TMA_ARGS);
     BP_TMA_CASE(2) BP_TMA_CASE(4) BP_TMA_CASE(6) BP_TMA_CASE(8) BP_TMA_CASE(10) BP_TMA_CASE1(12)
     BP_TMA_CASE1(14) BP_TMA_CASE1(16)
 #undef BP_TMA_CASE
@@ -338,6 +353,45 @@ int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
                   const float* wJ, const float* ggeo, const float* D, float lambda, const float* q, float* Aq,
                   const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   return launch_ax_tma_t<float>(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
+}
+
+// FP32 operator on PK right-hand sides packed per node (q, Aq hold PK floats per
+// node; one field).  Returns 1 when the configuration is not covered.
+template <int PK>
+static int launch_ax_tma_pk(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                            const float* wJ, const float* ggeo, const float* D, float lambda, const float* q,
+                            float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
+  using T = Pack<float, PK>;
+  const int NQ = d.N + 1;
+  if (d.affine || d.Nfields != 1 || (NQ % 2) != 0 ||
+      ((reinterpret_cast<uintptr_t>(ggeo) | reinterpret_cast<uintptr_t>(wJ)) & 15) ||
+      (reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(Aq)) % alignof(T))
+    return 1;
+  const T* qp = reinterpret_cast<const T*>(q);
+  T* ap = reinterpret_cast<T*>(Aq);
+  switch (NQ) {
+#define BP_TMA_PK_CASE(nq) \
+  case nq:                 \
+    return launch_tma<nq, 1, float, T>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, qp, ap, skip, fuse, s, nblocks);
+    BP_TMA_PK_CASE(2) BP_TMA_PK_CASE(4) BP_TMA_PK_CASE(6) BP_TMA_PK_CASE(8) BP_TMA_PK_CASE(10) BP_TMA_PK_CASE(12)
+#undef BP_TMA_PK_CASE
+    default:
+      return 1;
+  }
+}
+
+int launch_ax_tma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                         const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
+                         const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                         int* nblocks) {
+  switch (pk) {
+    case 2:
+      return launch_ax_tma_pk<2>(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
+    case 4:
+      return launch_ax_tma_pk<4>(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
+    default:
+      return 1;
+  }
 }
 
 }  // namespace bp

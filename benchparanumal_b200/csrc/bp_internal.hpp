@@ -213,6 +213,11 @@ int launch_diag_cub(const bp_ax_desc_t& d, int32_t Nelements, const double* wJ, 
 // cubature geometric factors of a curved mesh at the Gauss points
 int launch_geometry_at(int Nq, int E, const double* EX, const double* EY, const double* EZ, const double* r,
                        const double* w, double* wJ, double* ggeo, int* bad, cudaStream_t s);
+// the same FP32 operator on pk (2 or 4) right-hand sides packed per node; 1 when not covered
+int launch_ax_tma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                         const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
+                         const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                         int* nblocks);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

@@ -23,12 +23,14 @@
 // its Krylov space and needs about as many iterations as FP64 CG.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
+#include "bp_pack.cuh"
 
 namespace bp {
 
@@ -224,22 +226,24 @@ cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, co
   }
 }
 
-// apply the last completed iteration's x update
+// apply the last completed iteration's x update (x and p with element stride
+// `stride`: 1, or the lane count of a packed group)
 template <class V>
 __global__ void __launch_bounds__(kThreads)
-cg_final_kernel(int32_t N, V* __restrict__ x, const V* __restrict__ p, const CgScalars* __restrict__ sc) {
+cg_final_kernel(int32_t N, V* __restrict__ x, const V* __restrict__ p, const CgScalars* __restrict__ sc,
+                int stride = 1) {
   if (sc->iter == 0 || sc->breakdown || sc->skip_x) return;
   const V alpha = (V)sc->alpha;
   for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x)
-    x[n] = alpha * p[n] + V(1) * x[n];
+    x[(size_t)n * stride] = alpha * p[(size_t)n * stride] + V(1) * x[(size_t)n * stride];
 }
 
-// mixed: x_hi += x_lo, x_lo = 0
+// mixed: x_hi += x_lo, x_lo = 0 (x_lo with element stride `stride`)
 __global__ void __launch_bounds__(kThreads)
-mixed_fold_kernel(int32_t N, double* __restrict__ x_hi, float* __restrict__ x_lo) {
+mixed_fold_kernel(int32_t N, double* __restrict__ x_hi, float* __restrict__ x_lo, int stride = 1) {
   for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
-    x_hi[n] += (double)x_lo[n];
-    x_lo[n] = 0.0f;
+    x_hi[n] += (double)x_lo[(size_t)n * stride];
+    x_lo[(size_t)n * stride] = 0.0f;
   }
 }
 
@@ -248,13 +252,13 @@ mixed_fold_kernel(int32_t N, double* __restrict__ x_hi, float* __restrict__ x_lo
 __global__ void __launch_bounds__(kThreads)
 mixed_replace_kernel(int32_t N, const double* __restrict__ b, const double* __restrict__ Ax, double* __restrict__ r_hi,
                      float* __restrict__ r_lo, const float* __restrict__ invD, CgScalars* sc, int init, double tol,
-                     int maxit, int precon, double* partials, unsigned int* counter) {
+                     int maxit, int precon, double* partials, unsigned int* counter, int stride = 1) {
   double acc[3] = {0.0, 0.0, 0.0};
   for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
     const double rn = b[n] - Ax[n];
     r_hi[n] = rn;
     const float rl = (float)rn;
-    r_lo[n] = rl;
+    r_lo[(size_t)n * stride] = rl;
     acc[0] += rn * rn;
     acc[1] += (double)rl * (double)rl;
     if (precon) acc[2] += (double)rl * (double)invD[n] * (double)rl;
@@ -283,6 +287,141 @@ mixed_replace_kernel(int32_t N, const double* __restrict__ b, const double* __re
     }
     sc->update = 0;
     sc->done = (tot[0] <= sc->tol2 || sc->iter >= sc->maxit) ? 1 : 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Packed groups: PK systems on one mesh advanced in lockstep.  Their FP32
+// vectors hold one Pack<float, PK> per node (lane l = system l), so the
+// direction update, the gather and the element operator read every index and
+// factor once for all lanes.  Each lane keeps its own scalars (alpha, beta,
+// norms, stop flags) in its own CgScalars slot; a finished lane stops changing
+// while the others continue.
+// ---------------------------------------------------------------------------
+template <int PK>
+__global__ void __launch_bounds__(kThreads)
+grp_direction_kernel(int32_t N, Pack<float, PK>* __restrict__ x, Pack<float, PK>* __restrict__ p,
+                     const Pack<float, PK>* __restrict__ r, const float* __restrict__ invD,
+                     const CgScalars* __restrict__ sc) {
+  bool act[PK], addx[PK], first[PK];
+  float alpha[PK], beta[PK];
+  bool any = false;
+#pragma unroll
+  for (int l = 0; l < PK; ++l) {
+    const CgScalars& c = sc[l];
+    act[l] = !c.done;
+    any = any || act[l];
+    first[l] = c.iter == 0;
+    addx[l] = c.iter > 0 && !c.skip_x;
+    alpha[l] = (float)c.alpha;
+    beta[l] = first[l] ? 0.0f : (float)(c.precon ? c.rz / c.rz_prev : c.rdotr / c.rdotr_prev);
+  }
+  if (!any) return;
+  const bool precon = sc[0].precon != 0;
+  for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x) {
+    Pack<float, PK> pn = p[n], xn = x[n];
+    const Pack<float, PK> rn = r[n];
+    const float d = precon ? invD[n] : 1.0f;
+#pragma unroll
+    for (int l = 0; l < PK; ++l) {
+      if (!act[l]) continue;
+      if (addx[l]) xn.v[l] = alpha[l] * pn.v[l] + 1.0f * xn.v[l];
+      const float z = d * rn.v[l];
+      pn.v[l] = first[l] ? z : z + beta[l] * pn.v[l];
+    }
+    x[n] = xn;
+    p[n] = pn;
+  }
+}
+
+// p.Ap of every active lane from the operator's per-lane block partials, then alpha
+template <int PK>
+__global__ void __launch_bounds__(kAlphaThreads)
+grp_alpha_kernel(int nparts, const double* __restrict__ parts, CgScalars* sc) {
+  __shared__ double s_w[kAlphaThreads / 32];
+  __shared__ int s_act[PK];
+  if (threadIdx.x < PK) s_act[threadIdx.x] = !sc[threadIdx.x].done;
+  __syncthreads();
+  for (int l = 0; l < PK; ++l) {
+    if (!s_act[l]) continue;   // block-uniform
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nparts; k += kAlphaThreads) acc += parts[(size_t)l * nparts + k];
+    acc = warp_sum_cg(acc);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double pAp = 0.0;
+      for (int w = 0; w < kAlphaThreads / 32; ++w) pAp += s_w[w];
+      CgScalars& c = sc[l];
+      const double rho = c.precon ? c.rz : c.rdotr;
+      const double alpha = rho / pAp;
+      c.pAp = pAp;
+      if (!(pAp > 0.0) || !isfinite(alpha)) {
+        c.breakdown = 1;
+        c.done = 1;
+      } else {
+        c.alpha = alpha;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// r -= alpha Gather(AqL) per lane, r.r and r.z per lane, each lane's stop test
+template <int PK>
+__global__ void __launch_bounds__(kThreads)
+grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const int32_t* __restrict__ colIds,
+                         const Pack<float, PK>* __restrict__ AqL, Pack<float, PK>* __restrict__ r,
+                         const float* __restrict__ invD, CgScalars* sc, double* partials, unsigned int* counter) {
+  bool act[PK];
+  float alpha[PK];
+  bool any = false;
+#pragma unroll
+  for (int l = 0; l < PK; ++l) {
+    act[l] = !sc[l].done;
+    any = any || act[l];
+    alpha[l] = (float)sc[l].alpha;
+  }
+  if (!any) return;
+  const bool precon = sc[0].precon != 0;
+  double acc[2 * PK];
+#pragma unroll
+  for (int c = 0; c < 2 * PK; ++c) acc[c] = 0.0;
+  for (int32_t row = blockIdx.x * kThreads + threadIdx.x; row < Nrows; row += kThreads * gridDim.x) {
+    Pack<float, PK> rn = r[row];
+    const float dinv = precon ? __ldg(invD + row) : 0.0f;
+    const int32_t start = __ldg(rowStarts + row), end = __ldg(rowStarts + row + 1);
+    Pack<float, PK> sum(0.0f);
+    for (int32_t c = start; c < end; ++c) sum += AqL[__ldg(colIds + c)];
+#pragma unroll
+    for (int l = 0; l < PK; ++l) {
+      if (act[l]) rn.v[l] = rn.v[l] - alpha[l] * sum.v[l];
+      acc[l] += (double)rn.v[l] * (double)rn.v[l];
+      if (precon) acc[PK + l] += (double)rn.v[l] * (double)dinv * (double)rn.v[l];
+    }
+    r[row] = rn;
+  }
+  double tot[2 * PK];
+  if (grid_sum_cg<2 * PK>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    for (int l = 0; l < PK; ++l) {
+      if (!act[l]) continue;
+      CgScalars& c = sc[l];
+      c.rdotr_prev = c.rdotr;
+      c.rdotr = tot[l];
+      if (precon) {
+        c.rz_prev = c.rz;
+        c.rz = tot[PK + l];
+      }
+      c.iter += 1;
+      c.skip_x = 0;
+      if (!isfinite(tot[l])) {
+        c.breakdown = 1;
+        c.done = 1;
+      } else if (tot[l] <= c.tol2 || tot[l] < kReliableDrop * kReliableDrop * c.rmax2 || c.iter >= c.maxit) {
+        c.update = 1;   // a packed group always runs the mixed-precision recursion
+        c.done = 1;
+      }
+    }
   }
 }
 
@@ -809,20 +948,36 @@ int bp_solver_solve_host(bp_solver_t S, const double* b_host, double* x_host, do
 // ---------------------------------------------------------------------------
 // Batched solves: many independent problems (each its own box, degree and
 // element count) with several right-hand sides each.  Every (problem, rhs)
-// pair is a CG system with its own solver state on a shared mesh; one CUDA
-// graph holds kChunk iterations of every system, the systems spread over
-// kBranches parallel branches (fork/join events), so small and large
-// problems of different degrees run side by side on the GPU and one graph
-// launch advances all of them.  Finished systems skip their kernels through
-// their device flag.  In a mixed-precision batch the host visits the systems
-// between graph launches and applies the reliable updates they ask for.
+// pair is a CG system on its problem's mesh.  In a mixed-precision batch the
+// right-hand sides of a problem whose FP32 operator has a packed form (even
+// Nq, stored factors) are solved in lockstep as one packed group of 2 or 4
+// lanes (padding lanes carry b = 0 and finish at once); the others are
+// standalone systems.  One CUDA graph holds 20 iterations of every group and
+// standalone system, spread over kBranches parallel branches (fork/join
+// events), so problems of different degree and size run side by side; finished
+// systems skip their kernels through their device flags.  Between graph
+// launches the host applies the reliable updates the systems ask for.
 // ---------------------------------------------------------------------------
+struct CgGroup {
+  int pk = 0;                                   // lanes
+  bp_solver_s* base = nullptr;                  // mixed solver on the mesh: FP64 operator, invD, FP32 data
+  DeviceArray<float> x32, r32, p32, AqL32;      // packed [N][pk], AqL [NL][pk]
+  DeviceArray<double> parts;                    // operator p.Ap partials [pk][blocks]
+  DeviceArray<double> gparts;                   // gather-update grid sums [2 pk][reduction blocks]
+  DeviceArray<unsigned int> gcount;             // their arrival counter (zero between launches)
+  CgScalars* sc = nullptr;                      // pk consecutive slots
+  std::vector<double*> x, r, b;                 // per lane FP64 vectors
+};
+
 struct bp_batch_s {
   std::vector<bp_mesh_s*> meshes;             // owned
-  std::vector<bp_solver_s*> solvers;          // owned, one per system
-  std::vector<int> sys_prob;                  // problem of each system
+  std::vector<bp_solver_s*> owned;            // owned solvers (standalone systems and group bases)
+  std::vector<CgGroup*> groups;               // owned
+  std::vector<bp_solver_s*> sys_solver;       // per system: its solver (a group's base for grouped systems)
+  std::vector<int> sys_prob, sys_group, sys_lane, sys_slot;
   std::vector<DeviceArray<double>*> x, r, b;  // per system (owned)
-  DeviceArray<CgScalars> sc;                  // the systems' CG scalars, one array
+  std::vector<DeviceArray<double>*> pad;      // padding lanes' x, r, b (owned)
+  DeviceArray<CgScalars> sc;                  // every slot's CG scalars, one array
   int mixed = 0;
   std::vector<cudaStream_t> branches;
   std::vector<cudaEvent_t> joins;
@@ -830,11 +985,13 @@ struct bp_batch_s {
   cudaGraphExec_t graph = nullptr;
   ~bp_batch_s() {
     if (graph) cudaGraphExecDestroy(graph);
-    for (auto* S : solvers) delete S;
+    for (auto* G : groups) delete G;
+    for (auto* S : owned) delete S;
     for (auto* m : meshes) bp_mesh_destroy(m);
     for (auto* v : x) delete v;
     for (auto* v : r) delete v;
     for (auto* v : b) delete v;
+    for (auto* v : pad) delete v;
     for (auto st : branches) cudaStreamDestroy(st);
     for (auto e : joins) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -847,6 +1004,64 @@ namespace bp {
 
 constexpr int kBranches = 16;
 
+// one packed iteration of a group: direction, operator with per-lane p.Ap
+// partials, alpha, gather + update
+template <int PK>
+static int grp_iteration(CgGroup* G, cudaStream_t s) {
+  bp_solver_s* S = G->base;
+  bp_mesh_s* m = S->mesh;
+  const int32_t N = S->N;
+  const int g = vec_grid(N);
+  using T = Pack<float, PK>;
+  grp_direction_kernel<PK><<<g, kThreads, 0, s>>>(N, reinterpret_cast<T*>(G->x32.ptr), reinterpret_cast<T*>(G->p32.ptr),
+                                                  reinterpret_cast<const T*>(G->r32.ptr), S->invD32.ptr, G->sc);
+  BP_CUDA_TRY(cudaGetLastError());
+  const ElemOperands<float> o = operands32(S);
+  const CgFuse fuse{G->parts.ptr};
+  int nparts = 0;
+  const int rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D,
+                                      (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
+  if (rc == 1) return fail(BP_ERROR_ARG, "packed group: operator form not available");
+  BP_TRY(rc);
+  grp_alpha_kernel<PK><<<1, kAlphaThreads, 0, s>>>(nparts, G->parts.ptr, G->sc);
+  BP_CUDA_TRY(cudaGetLastError());
+  grp_gather_update_kernel<PK><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr,
+                                                      reinterpret_cast<const T*>(G->AqL32.ptr),
+                                                      reinterpret_cast<T*>(G->r32.ptr), S->invD32.ptr, G->sc,
+                                                      G->gparts.ptr, G->gcount.ptr);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
+static int grp_body(CgGroup* G, cudaStream_t s) {
+  return G->pk == 4 ? grp_iteration<4>(G, s) : grp_iteration<2>(G, s);
+}
+
+// FP64 residual of lane l and the restart of its FP32 recursion (init: start of a solve)
+static int grp_replace(CgGroup* G, int l, bool init, double tol, int maxit, cudaStream_t s) {
+  bp_solver_s* S = G->base;
+  const int32_t N = S->N;
+  BP_TRY(operator_apply(S, G->x[l], S->Ap.ptr, nullptr, s));
+  S->launches += 1;
+  mixed_replace_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, G->b[l], S->Ap.ptr, G->r[l], G->r32.ptr + l,
+                                                        S->invD32.ptr, G->sc + l, init ? 1 : 0, tol, maxit,
+                                                        S->precon, S->partials.ptr, S->counter.ptr, G->pk);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
+// reliable update of lane l: the pending step, x_hi += x_lo, FP64 residual
+static int grp_reliable(CgGroup* G, int l, double tol, int maxit, cudaStream_t s) {
+  bp_solver_s* S = G->base;
+  const int32_t N = S->N;
+  S->launches += 2;
+  cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, G->x32.ptr + l, G->p32.ptr + l, G->sc + l, G->pk);
+  BP_CUDA_TRY(cudaGetLastError());
+  mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, G->x[l], G->x32.ptr + l, G->pk);
+  BP_CUDA_TRY(cudaGetLastError());
+  return grp_replace(G, l, false, tol, maxit, s);
+}
+
 static int batch_capture(bp_batch_s* B, cudaStream_t s) {
   if (B->graph) return BP_SUCCESS;
   cudaGraph_t g;
@@ -855,10 +1070,15 @@ static int batch_capture(bp_batch_s* B, cudaStream_t s) {
   cudaError_t ce = cudaEventRecord(B->fork, s);
   const int nb = (int)B->branches.size();
   for (int k = 0; k < nb && ce == cudaSuccess; ++k) ce = cudaStreamWaitEvent(B->branches[k], B->fork, 0);
-  for (size_t i = 0; i < B->solvers.size() && ce == cudaSuccess && rc == BP_SUCCESS; ++i) {
-    cudaStream_t bs = B->branches[i % nb];
+  int unit = 0;   // groups and standalone systems, round robin over the branches
+  for (size_t gi = 0; gi < B->groups.size() && ce == cudaSuccess && rc == BP_SUCCESS; ++gi, ++unit)
+    for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k) rc = grp_body(B->groups[gi], B->branches[unit % nb]);
+  for (size_t i = 0; i < B->sys_solver.size() && ce == cudaSuccess && rc == BP_SUCCESS; ++i) {
+    if (B->sys_group[i] >= 0) continue;
+    cudaStream_t bs = B->branches[unit++ % nb];
+    bp_solver_s* S = B->sys_solver[i];
     for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k)
-      rc = B->mixed ? body32(B->solvers[i], nullptr, nullptr, bs) : body64(B->solvers[i], B->x[i]->ptr, B->r[i]->ptr, bs);
+      rc = B->mixed ? body32(S, nullptr, nullptr, bs) : body64(S, B->x[i]->ptr, B->r[i]->ptr, bs);
   }
   for (int k = 0; k < nb && ce == cudaSuccess; ++k) {
     ce = cudaEventRecord(B->joins[k], B->branches[k]);
@@ -875,7 +1095,7 @@ static int batch_capture(bp_batch_s* B, cudaStream_t s) {
 }
 
 static int batch_read(bp_batch_s* B, std::vector<CgScalars>& h, cudaStream_t s) {
-  h.resize(B->solvers.size());
+  h.resize(B->sc.n);
   BP_CUDA_TRY(cudaMemcpyAsync(h.data(), B->sc.ptr, sizeof(CgScalars) * h.size(), cudaMemcpyDeviceToHost, s));
   BP_CUDA_TRY(cudaStreamSynchronize(s));
   return BP_SUCCESS;
@@ -883,18 +1103,26 @@ static int batch_read(bp_batch_s* B, std::vector<CgScalars>& h, cudaStream_t s) 
 
 static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* stats, double* elapsed_ms) {
   cudaStream_t s = default_stream();
-  const size_t ns = B->solvers.size();
+  const size_t ns = B->sys_solver.size();
   if (B->mixed && !(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_batch_solve: a mixed-precision batch needs tol > 0");
   BP_TRY(batch_capture(B, s));
-  std::vector<int> updates(ns, 0);
-  for (auto* S : B->solvers) S->launches = 0;
+  std::vector<int> updates(B->sc.n, 0);
+  for (auto* S : B->owned) S->launches = 0;
   BP_CUDA_TRY(cudaEventRecord(B->ev0, s));
-  // x = 0, r = b, and each system's start
+  // x = 0, r = b, and every system's start
   for (size_t i = 0; i < ns; ++i) {
-    bp_solver_s* S = B->solvers[i];
-    const size_t bytes = sizeof(double) * S->N;
+    const size_t bytes = sizeof(double) * B->sys_solver[i]->N;
     BP_CUDA_TRY(cudaMemsetAsync(B->x[i]->ptr, 0, bytes, s));
     BP_CUDA_TRY(cudaMemcpyAsync(B->r[i]->ptr, B->b[i]->ptr, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+  for (auto* G : B->groups) {
+    BP_CUDA_TRY(cudaMemsetAsync(G->x32.ptr, 0, sizeof(float) * G->x32.n, s));
+    BP_CUDA_TRY(cudaMemsetAsync(G->p32.ptr, 0, sizeof(float) * G->p32.n, s));
+    for (int l = 0; l < G->pk; ++l) BP_TRY(grp_replace(G, l, true, tol, maxit, s));
+  }
+  for (size_t i = 0; i < ns; ++i) {
+    if (B->sys_group[i] >= 0) continue;
+    bp_solver_s* S = B->sys_solver[i];
     if (B->mixed) {
       BP_TRY(mixed_begin(S, B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
     } else {
@@ -909,13 +1137,30 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
   BP_TRY(batch_read(B, h, s));
   for (;;) {
     bool running = false, updated = false;
+    for (size_t gi = 0; gi < B->groups.size(); ++gi) {
+      CgGroup* G = B->groups[gi];
+      const int slot0 = (int)(G->sc - B->sc.ptr);
+      for (int l = 0; l < G->pk; ++l) {
+        const CgScalars& c = h[slot0 + l];
+        if (c.breakdown) continue;
+        if (c.update) {
+          BP_TRY(grp_reliable(G, l, tol, maxit, s));
+          ++updates[slot0 + l];
+          updated = true;
+        } else if (!c.done) {
+          running = true;
+        }
+      }
+    }
     for (size_t i = 0; i < ns; ++i) {
-      if (h[i].breakdown) continue;
-      if (B->mixed && h[i].update) {
-        BP_TRY(mixed_reliable(B->solvers[i], B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
-        ++updates[i];
+      if (B->sys_group[i] >= 0) continue;
+      const CgScalars& c = h[B->sys_slot[i]];
+      if (c.breakdown) continue;
+      if (B->mixed && c.update) {
+        BP_TRY(mixed_reliable(B->sys_solver[i], B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
+        ++updates[B->sys_slot[i]];
         updated = true;
-      } else if (!h[i].done) {
+      } else if (!c.done) {
         running = true;
       }
     }
@@ -925,12 +1170,14 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
     }
     if (!running) break;
     BP_CUDA_TRY(cudaGraphLaunch(B->graph, s));
-    for (auto* S : B->solvers) S->launches += 4 * kChunk;
+    for (auto* G : B->groups) G->base->launches += 4 * kChunk;
+    for (size_t i = 0; i < ns; ++i)
+      if (B->sys_group[i] < 0) B->sys_solver[i]->launches += 4 * kChunk;
     BP_TRY(batch_read(B, h, s));
   }
   if (!B->mixed)
     for (size_t i = 0; i < ns; ++i) {
-      bp_solver_s* S = B->solvers[i];
+      bp_solver_s* S = B->sys_solver[i];
       S->launches += 1;
       cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, s>>>(S->N, B->x[i]->ptr, S->p.ptr, S->scal);
       BP_CUDA_TRY(cudaGetLastError());
@@ -943,15 +1190,19 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
   BP_TRY(check_device_error());
   bool breakdown = false;
   for (size_t i = 0; i < ns; ++i) {
+    const CgScalars& c = h[B->sys_slot[i]];
     if (stats) {
-      stats[i].iterations = h[i].iter;
-      stats[i].rdotr0 = h[i].rdotr0;
-      stats[i].rdotr = B->mixed ? h[i].rtrue2 : h[i].rdotr;
+      stats[i].iterations = c.iter;
+      stats[i].rdotr0 = c.rdotr0;
+      stats[i].rdotr = B->mixed ? c.rtrue2 : c.rdotr;
       stats[i].elapsed_ms = ms;
-      stats[i].updates = updates[i];
-      stats[i].kernel_launches = B->solvers[i]->launches;
+      stats[i].updates = updates[B->sys_slot[i]];
+      // a group's launches serve all its lanes: each lane reports an equal share
+      const int g = B->sys_group[i];
+      stats[i].kernel_launches =
+          g >= 0 ? B->sys_solver[i]->launches / B->groups[g]->pk : B->sys_solver[i]->launches;
     }
-    breakdown = breakdown || h[i].breakdown;
+    breakdown = breakdown || c.breakdown;
   }
   if (breakdown) return fail(BP_ERROR_NUMERIC, "bp_batch_solve: CG breakdown in a system (p.Ap <= 0 or non-finite)");
   return BP_SUCCESS;
@@ -987,38 +1238,102 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
       B->joins.push_back(e);
     }
     if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_batch_create", __FILE__, __LINE__); break; }
-    int nsys = 0;
-    for (int j = 0; j < nproblems; ++j) nsys += problems[j].nrhs;
-    if ((rc = B->sc.alloc(nsys))) break;
-    for (int j = 0; j < nproblems && rc == BP_SUCCESS; ++j) {
+    // plan: which systems are packed into groups, and the scalar slots
+    struct Unit { int prob, first_rhs, nrhs, pk; };   // pk 0: standalone system
+    std::vector<Unit> units;
+    int nslots = 0;
+    for (int j = 0; j < nproblems; ++j) {
       const bp_batch_problem_t& P = problems[j];
-      bp_box_desc_t bd{};
-      bd.nx = P.nx; bd.ny = P.ny; bd.nz = P.nz; bd.N = P.N; bd.affine = 0; bd.Nfields = 1;
-      bd.pert = P.pert; bd.pert_seed = P.pert_seed;
-      bp_mesh_t m = nullptr;
-      if ((rc = bp_mesh_create(&bd, &m))) break;
-      B->meshes.push_back(m);
-      for (int k = 0; k < P.nrhs && rc == BP_SUCCESS; ++k) {
-        bp_solver_t S = nullptr;
-        if ((rc = bp_solver_create(m, d, &S))) break;
-        B->solvers.push_back(S);
-        B->sys_prob.push_back(j);
-        S->scal = B->sc.ptr + (B->solvers.size() - 1);
+      const bool packable = B->mixed && d->bp == 5 && (P.N + 1) % 2 == 0 && P.N + 1 <= 12;
+      for (int k = 0; k < P.nrhs;) {
+        const int left = P.nrhs - k;
+        const int pk = !packable || left == 1 ? 0 : (left == 2 ? 2 : 4);
+        const int n = pk ? std::min(pk, left) : 1;
+        units.push_back({j, k, n, pk});
+        nslots += pk ? pk : 1;
+        k += n;
+      }
+    }
+    if ((rc = B->sc.alloc(nslots))) break;
+    ce = cudaMemsetAsync(B->sc.ptr, 0, sizeof(CgScalars) * nslots, s);
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_batch_create", __FILE__, __LINE__); break; }
+    int slot = 0, cur = -1;
+    bp_mesh_t m = nullptr;
+    for (const Unit& u : units) {
+      const bp_batch_problem_t& P = problems[u.prob];
+      if (u.prob != cur) {
+        bp_box_desc_t bd{};
+        bd.nx = P.nx; bd.ny = P.ny; bd.nz = P.nz; bd.N = P.N; bd.affine = 0; bd.Nfields = 1;
+        bd.pert = P.pert; bd.pert_seed = P.pert_seed;
+        m = nullptr;
+        if ((rc = bp_mesh_create(&bd, &m))) break;
+        B->meshes.push_back(m);
+        cur = u.prob;
+      }
+      bp_solver_t S = nullptr;
+      if ((rc = bp_solver_create(m, d, &S))) break;
+      B->owned.push_back(S);
+      CgGroup* G = nullptr;
+      if (u.pk) {
+        G = new CgGroup();
+        B->groups.push_back(G);
+        G->pk = u.pk;
+        G->base = S;
+        G->sc = B->sc.ptr + slot;
+        const size_t NL = (size_t)m->E * m->Np;
+        if ((rc = G->x32.alloc((size_t)S->N * u.pk))) break;
+        if ((rc = G->r32.alloc((size_t)S->N * u.pk))) break;
+        if ((rc = G->p32.alloc((size_t)S->N * u.pk))) break;
+        if ((rc = G->AqL32.alloc(NL * u.pk))) break;
+        if ((rc = G->parts.alloc(((size_t)m->E + 1) * u.pk))) break;
+        if ((rc = G->gparts.alloc((size_t)2 * u.pk * reduction_blocks()))) break;
+        if ((rc = G->gcount.alloc(1))) break;
+        ce = cudaMemsetAsync(G->gcount.ptr, 0, sizeof(unsigned int), s);
+        if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_batch_create", __FILE__, __LINE__); break; }
+      } else {
+        S->scal = B->sc.ptr + slot;
+      }
+      for (int k = 0; k < (u.pk ? u.pk : 1) && rc == BP_SUCCESS; ++k) {
         auto* xv = new DeviceArray<double>();
         auto* rv = new DeviceArray<double>();
         auto* bv = new DeviceArray<double>();
-        B->x.push_back(xv);
-        B->r.push_back(rv);
-        B->b.push_back(bv);
+        const bool real = k < u.nrhs;
+        if (real) {
+          B->x.push_back(xv);
+          B->r.push_back(rv);
+          B->b.push_back(bv);
+          B->sys_solver.push_back(S);
+          B->sys_prob.push_back(u.prob);
+          B->sys_group.push_back(G ? (int)B->groups.size() - 1 : -1);
+          B->sys_lane.push_back(G ? k : 0);
+          B->sys_slot.push_back(slot + k);
+        } else {
+          B->pad.push_back(xv);
+          B->pad.push_back(rv);
+          B->pad.push_back(bv);
+        }
         if ((rc = xv->alloc(S->N))) break;
         if ((rc = rv->alloc(S->N))) break;
         if ((rc = bv->alloc(S->N))) break;
-        rc = bp_solver_rhs(S, BP_RHS_RANDOM, P.rhs_seed + (uint64_t)k, bv->ptr, nullptr);
+        if (G) {
+          G->x.push_back(xv->ptr);
+          G->r.push_back(rv->ptr);
+          G->b.push_back(bv->ptr);
+        }
+        if (real) {
+          rc = bp_solver_rhs(S, BP_RHS_RANDOM, P.rhs_seed + (uint64_t)(u.first_rhs + k), bv->ptr, nullptr);
+        } else {
+          // a padding lane: b = 0 converges at its first test and stays idle
+          ce = cudaMemsetAsync(bv->ptr, 0, sizeof(double) * S->N, s);
+          if (ce == cudaSuccess) ce = cudaMemsetAsync(xv->ptr, 0, sizeof(double) * S->N, s);
+          if (ce != cudaSuccess) rc = cuda_fail(ce, "bp_batch_create", __FILE__, __LINE__);
+        }
       }
+      if (rc != BP_SUCCESS) break;
+      slot += u.pk ? u.pk : 1;
     }
     if (rc == BP_SUCCESS) {
-      cudaError_t ce2 = cudaMemsetAsync(B->sc.ptr, 0, sizeof(CgScalars) * B->sc.n, s);
-      if (ce2 == cudaSuccess) ce2 = cudaStreamSynchronize(s);
+      cudaError_t ce2 = cudaStreamSynchronize(s);
       if (ce2 != cudaSuccess) rc = cuda_fail(ce2, "bp_batch_create", __FILE__, __LINE__);
     }
   } while (0);
@@ -1037,15 +1352,15 @@ int bp_batch_destroy(bp_batch_t B) {
 
 int bp_batch_systems(bp_batch_t B, int32_t* nsystems) {
   if (!B || !nsystems) return fail(BP_ERROR_ARG, "bp_batch_systems: null pointer");
-  *nsystems = (int32_t)B->solvers.size();
+  *nsystems = (int32_t)B->sys_solver.size();
   return BP_SUCCESS;
 }
 
 int bp_batch_system_info(bp_batch_t B, int32_t system, int32_t* problem, int32_t* Ngather) {
-  if (!B || system < 0 || system >= (int32_t)B->solvers.size())
+  if (!B || system < 0 || system >= (int32_t)B->sys_solver.size())
     return fail(BP_ERROR_ARG, "bp_batch_system_info: bad system index");
   if (problem) *problem = B->sys_prob[system];
-  if (Ngather) *Ngather = B->solvers[system]->N;
+  if (Ngather) *Ngather = B->sys_solver[system]->N;
   return BP_SUCCESS;
 }
 
@@ -1056,7 +1371,7 @@ int bp_batch_solve(bp_batch_t B, double tol, int32_t maxit, bp_solve_stats_t* st
 }
 
 int bp_batch_vectors(bp_batch_t B, int32_t system, double** x, double** b) {
-  if (!B || system < 0 || system >= (int32_t)B->solvers.size())
+  if (!B || system < 0 || system >= (int32_t)B->sys_solver.size())
     return fail(BP_ERROR_ARG, "bp_batch_vectors: bad system index");
   if (x) *x = B->x[system]->ptr;
   if (b) *b = B->b[system]->ptr;
@@ -1064,9 +1379,9 @@ int bp_batch_vectors(bp_batch_t B, int32_t system, double** x, double** b) {
 }
 
 int bp_batch_solver(bp_batch_t B, int32_t system, bp_solver_t* solver) {
-  if (!B || !solver || system < 0 || system >= (int32_t)B->solvers.size())
+  if (!B || !solver || system < 0 || system >= (int32_t)B->sys_solver.size())
     return fail(BP_ERROR_ARG, "bp_batch_solver: bad system index");
-  *solver = B->solvers[system];
+  *solver = B->sys_solver[system];
   return BP_SUCCESS;
 }
 

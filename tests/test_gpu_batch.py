@@ -8,10 +8,14 @@ pytestmark = pytest.mark.gpu
 
 PROBLEMS = [
     {"nx": 3, "N": 3, "pert": 0.1, "pert_seed": 100, "nrhs": 2, "rhs_seed": 1000},
-    {"nx": 4, "N": 5, "pert": 0.1, "pert_seed": 101, "nrhs": 2, "rhs_seed": 1002},
-    {"nx": 2, "N": 7, "pert": 0.1, "pert_seed": 102, "nrhs": 1, "rhs_seed": 1004},
-    {"nx": 3, "N": 10, "pert": 0.1, "pert_seed": 103, "nrhs": 3, "rhs_seed": 1005},
+    {"nx": 4, "N": 5, "pert": 0.1, "pert_seed": 101, "nrhs": 3, "rhs_seed": 1002},
+    {"nx": 2, "N": 7, "pert": 0.1, "pert_seed": 102, "nrhs": 1, "rhs_seed": 1005},
+    {"nx": 3, "N": 10, "pert": 0.1, "pert_seed": 103, "nrhs": 3, "rhs_seed": 1006},
+    {"nx": 2, "N": 7, "pert": 0.1, "pert_seed": 104, "nrhs": 4, "rhs_seed": 1009},
 ]
+# In a mixed batch the right-hand sides of even-Nq problems run as packed
+# groups: problem 0 as two lanes, problem 1 as four lanes with one idle, problem
+# 4 as four lanes; the others are standalone systems.
 
 
 def _rel(a, b):
