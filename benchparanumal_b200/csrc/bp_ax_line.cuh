@@ -27,6 +27,7 @@
 
 #include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
+#include "bp_pack.cuh"
 
 #ifndef BP_LINE_OUTER
 #define BP_LINE_OUTER _Pragma("unroll 1")
@@ -57,37 +58,43 @@ struct LineShape {
   static constexpr int THREADS = G2 * EPB;
   static constexpr int MINB = NQ <= 11 ? 2 : 1;
   static constexpr int SLOT = line_slot(NQ);
-  static constexpr size_t SMEM = sizeof(LineReal) * (size_t)3 * FIELD * EPB;
+  template <class T>
+  static constexpr size_t smem() { return sizeof(T) * (size_t)3 * FIELD * EPB; }
 };
 
-template <int NQ, bool AFFINE>
+// T: the value type of q and Aq, LineReal or Pack<LineReal, PK> (PK right-hand
+// sides of one mesh in lockstep, one pack per node); p.Ap partials per lane at
+// partials[lane * gridDim.x + blockIdx.x].
+template <int NQ, bool AFFINE, class T>
 __global__ void __launch_bounds__(LineShape<NQ>::THREADS, LineShape<NQ>::MINB)
 ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
                const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
-               const LineReal* __restrict__ gllw, LineReal lambda, const LineReal* __restrict__ q,
-               LineReal* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
+               const LineReal* __restrict__ gllw, LineReal lambda, const T* __restrict__ q,
+               T* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
   if (skip && *skip) return;
   using F = LineReal;
   using Sh = LineShape<NQ>;
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
   constexpr int RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB, NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
-  constexpr int SLOT = Sh::SLOT;
+  constexpr int SLOT = Sh::SLOT, LANES = PackTraits<T>::R;
 #define D_(a, b) c_line[SLOT + (a) * NQ + (b)]
 #define W_(a) c_line[SLOT + NQ * NQ + (a)]
 #define AT(B, z, y, x) B[(z) * PLANE + (y) * RS + (x)]
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  F* const sbase = reinterpret_cast<F*>(smem_raw);
+  T* const sbase = reinterpret_cast<T*>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
   const int tid = tx + NQ * (ty + NQ * es);
-  F* const U = sbase + (size_t)es * 3 * Sh::FIELD;
-  F* const R = U + Sh::FIELD;
-  F* const S = R + Sh::FIELD;
+  T* const U = sbase + (size_t)es * 3 * Sh::FIELD;
+  T* const R = U + Sh::FIELD;
+  T* const S = R + Sh::FIELD;
 
   const int eidx = blockIdx.x * EPB + es;
   const bool valid = eidx < Nelements;
   const int element = valid ? elementList[eidx] : 0;
-  double pdot = 0.0;
+  double pdot[LANES];
+#pragma unroll
+  for (int l = 0; l < LANES; ++l) pdot[l] = 0.0;
 
   F wa = 0, ga[6] = {0, 0, 0, 0, 0, 0}, wxy = 0;
   if (AFFINE) {
@@ -100,33 +107,33 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
   for (int f = 0; f < Nfields; ++f) {
     const size_t lbase = ((size_t)element * Nfields + f) * NP;
     if (f > 0) __syncthreads();   // the previous field's last reads of U, R, S are done
-    F qk[NQ];
+    T qk[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
-      F v = 0;
+      T v = pack_zero<T>();
       if (valid) {
         const int32_t id = G2L[lbase + k * NQ2 + ty * NQ + tx];
-        v = (id >= 0) ? q[id] : F(0);
+        if (id >= 0) v = q[id];
       }
       qk[k] = v;
       AT(U, k, ty, tx) = v;
     }
-    F gt[NQ];
+    T gt[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
-      F t = 0;
+      T t = pack_zero<T>();
 #pragma unroll
       for (int n = 0; n < NQ; ++n) t += D_(k, n) * qk[n];
       gt[k] = t;
     }
     __syncthreads();
     {
-      F r[NQ];
+      T r[NQ];
 #pragma unroll
       for (int n = 0; n < NQ; ++n) r[n] = AT(U, ty, tx, n);
       BP_LINE_OUTER
       for (int i = 0; i < NQ; ++i) {
-        F t = 0;
+        T t = pack_zero<T>();
 #pragma unroll
         for (int n = 0; n < NQ; ++n) t += D_(i, n) * r[n];
         AT(R, ty, tx, i) = t;
@@ -135,14 +142,14 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       for (int n = 0; n < NQ; ++n) r[n] = AT(U, ty, n, tx);
       BP_LINE_OUTER
       for (int j = 0; j < NQ; ++j) {
-        F t = 0;
+        T t = pack_zero<T>();
 #pragma unroll
         for (int n = 0; n < NQ; ++n) t += D_(j, n) * r[n];
         AT(S, ty, j, tx) = t;
       }
     }
     __syncthreads();
-    F acc[NQ];
+    T acc[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
       F g0, g1, g2, g3, g4, g5, w;
@@ -157,27 +164,27 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
         g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
         w = wJ[gb];
       }
-      const F dr = AT(R, k, ty, tx), ds = AT(S, k, ty, tx), dt = gt[k];
+      const T dr = AT(R, k, ty, tx), ds = AT(S, k, ty, tx), dt = gt[k];
       AT(R, k, ty, tx) = g0 * dr + g1 * ds + g2 * dt;
       AT(S, k, ty, tx) = g1 * dr + g3 * ds + g4 * dt;
       gt[k] = g2 * dr + g4 * ds + g5 * dt;
-      acc[k] = lambda * w * qk[k];
+      acc[k] = (lambda * w) * qk[k];
     }
 #pragma unroll
     for (int n = 0; n < NQ; ++n) {
-      F t = acc[n];
+      T t = acc[n];
 #pragma unroll
       for (int k = 0; k < NQ; ++k) t += D_(k, n) * gt[k];
       acc[n] = t;
     }
     __syncthreads();
     {
-      F r[NQ];
+      T r[NQ];
 #pragma unroll
       for (int n = 0; n < NQ; ++n) r[n] = AT(R, ty, tx, n);
       BP_LINE_OUTER
       for (int i = 0; i < NQ; ++i) {
-        F t = 0;
+        T t = pack_zero<T>();
 #pragma unroll
         for (int n = 0; n < NQ; ++n) t += D_(n, i) * r[n];
         AT(R, ty, tx, i) = t;
@@ -186,7 +193,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       for (int n = 0; n < NQ; ++n) r[n] = AT(S, ty, n, tx);
       BP_LINE_OUTER
       for (int j = 0; j < NQ; ++j) {
-        F t = 0;
+        T t = pack_zero<T>();
 #pragma unroll
         for (int n = 0; n < NQ; ++n) t += D_(n, j) * r[n];
         AT(S, ty, j, tx) = t;
@@ -196,15 +203,18 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
     if (valid) {
 #pragma unroll
       for (int k = 0; k < NQ; ++k) {
-        const F out = acc[k] + AT(R, k, ty, tx) + AT(S, k, ty, tx);
+        const T out = acc[k] + AT(R, k, ty, tx) + AT(S, k, ty, tx);
         Aq[lbase + k * NQ2 + ty * NQ + tx] = out;
-        pdot += (double)AT(U, k, ty, tx) * (double)out;
+        lane_dot(pdot, AT(U, k, ty, tx), out);
       }
     }
   }
   if (partials) {
-    const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(sbase));
-    if (tid == 0) partials[blockIdx.x] = bs;
+#pragma unroll
+    for (int l = 0; l < LANES; ++l) {
+      const double bs = fuse_block_sum(pdot[l], reinterpret_cast<double*>(sbase));
+      if (tid == 0) partials[(size_t)l * gridDim.x + blockIdx.x] = bs;
+    }
   }
 #undef AT
 #undef W_
@@ -223,12 +233,13 @@ static LineReal* line_table_address() {
   return addr[dev];
 }
 
-template <int NQ>
+template <int NQ, class T = LineReal>
 static int launch_line_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                           const LineReal* wJ, const LineReal* ggeo, const LineReal* gllw, const LineReal* D,
-                          LineReal lambda, const LineReal* q, LineReal* Aq, const int* skip, cudaStream_t s,
+                          LineReal lambda, const T* q, T* Aq, const int* skip, cudaStream_t s,
                           double* partials, int* nblocks) {
   using Sh = LineShape<NQ>;
+  constexpr size_t SMEM = Sh::template smem<T>();
   if (!d.affine && (reinterpret_cast<uintptr_t>(ggeo) % (2 * sizeof(LineReal))))
     return fail(BP_ERROR_ARG, "element operator: ggeo must be aligned to two elements");
   LineReal* tab = line_table_address();
@@ -240,17 +251,17 @@ static int launch_line_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
   if (d.affine) {
-    if (Sh::SMEM > 48 * 1024)
-      BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)Sh::SMEM));
-    ax_line_kernel<NQ, true><<<grid, block, Sh::SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
-                                                           lambda, q, Aq, skip, partials);
+    if (SMEM > 48 * 1024)
+      BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)SMEM));
+    ax_line_kernel<NQ, true, T><<<grid, block, SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
+                                                          lambda, q, Aq, skip, partials);
   } else {
-    if (Sh::SMEM > 48 * 1024)
-      BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)Sh::SMEM));
-    ax_line_kernel<NQ, false><<<grid, block, Sh::SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
-                                                            lambda, q, Aq, skip, partials);
+    if (SMEM > 48 * 1024)
+      BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)SMEM));
+    ax_line_kernel<NQ, false, T><<<grid, block, SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
+                                                           lambda, q, Aq, skip, partials);
   }
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
@@ -273,6 +284,32 @@ int launch_ax_line_impl(const bp_ax_desc_t& d, int32_t Nelements, const int32_t*
 #undef BP_LINE_CASE
     default:
       return fail(BP_ERROR_ARG, "element operator: degree N must be in 1..15");
+  }
+}
+
+// the same operator on PK right-hand sides packed per node (one field)
+template <int PK>
+int launch_ax_line_pk(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                      const LineReal* wJ, const LineReal* ggeo, const LineReal* gllw, const LineReal* D,
+                      LineReal lambda, const LineReal* q, LineReal* Aq, const int* skip, cudaStream_t s,
+                      const CgFuse* fuse, int* nblocks) {
+  using T = Pack<LineReal, PK>;
+  if (nblocks) *nblocks = 0;
+  if (d.Nfields != 1) return fail(BP_ERROR_ARG, "packed element operator: one field only");
+  if (Nelements == 0) return BP_SUCCESS;
+  double* partials = fuse ? fuse->partials : nullptr;
+  const T* qp = reinterpret_cast<const T*>(q);
+  T* ap = reinterpret_cast<T*>(Aq);
+  switch (d.N + 1) {
+#define BP_LINE_PK_CASE(nq) \
+  case nq:                  \
+    return launch_line_nq<nq, T>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, qp, ap, skip, s, partials, nblocks);
+    BP_LINE_PK_CASE(2) BP_LINE_PK_CASE(3) BP_LINE_PK_CASE(4) BP_LINE_PK_CASE(5) BP_LINE_PK_CASE(6)
+    BP_LINE_PK_CASE(7) BP_LINE_PK_CASE(8) BP_LINE_PK_CASE(9) BP_LINE_PK_CASE(10) BP_LINE_PK_CASE(11)
+    BP_LINE_PK_CASE(12)
+#undef BP_LINE_PK_CASE
+    default:
+      return fail(BP_ERROR_ARG, "packed element operator: degree N must be in 1..11");
   }
 }
 

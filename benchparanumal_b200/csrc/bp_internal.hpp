@@ -218,6 +218,11 @@ int launch_ax_tma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const
                          const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
                          const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                          int* nblocks);
+// the line-per-thread FP32 operator on pk (2 or 4) packed right-hand sides (any Nq up to 12)
+int launch_ax_line_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                          const int32_t* G2L, const float* wJ, const float* ggeo, const float* gllw, const float* D,
+                          float lambda, const float* q, float* Aq, const int* skip, const CgFuse* fuse,
+                          cudaStream_t s, int* nblocks);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

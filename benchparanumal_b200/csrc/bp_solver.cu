@@ -948,11 +948,10 @@ int bp_solver_solve_host(bp_solver_t S, const double* b_host, double* x_host, do
 // ---------------------------------------------------------------------------
 // Batched solves: many independent problems (each its own box, degree and
 // element count) with several right-hand sides each.  Every (problem, rhs)
-// pair is a CG system on its problem's mesh.  In a mixed-precision batch the
-// right-hand sides of a problem whose FP32 operator has a packed form (even
-// Nq, stored factors) are solved in lockstep as one packed group of 2 or 4
-// lanes (padding lanes carry b = 0 and finish at once); the others are
-// standalone systems.  One CUDA graph holds 20 iterations of every group and
+// pair is a CG system on its problem's mesh.  In a mixed-precision BP5 batch
+// the right-hand sides of a problem (degree up to 11) are solved in lockstep as
+// packed groups of 2 or 4 lanes (padding lanes carry b = 0 and finish at once);
+// a single right-hand side and the other cases are standalone systems.  One CUDA graph holds 20 iterations of every group and
 // standalone system, spread over kBranches parallel branches (fork/join
 // events), so problems of different degree and size run side by side; finished
 // systems skip their kernels through their device flags.  Between graph
@@ -975,6 +974,7 @@ struct bp_batch_s {
   std::vector<CgGroup*> groups;               // owned
   std::vector<bp_solver_s*> sys_solver;       // per system: its solver (a group's base for grouped systems)
   std::vector<int> sys_prob, sys_group, sys_lane, sys_slot;
+  std::vector<int> group_branch, sys_branch;  // branch of each group / standalone system
   std::vector<DeviceArray<double>*> x, r, b;  // per system (owned)
   std::vector<DeviceArray<double>*> pad;      // padding lanes' x, r, b (owned)
   DeviceArray<CgScalars> sc;                  // every slot's CG scalars, one array
@@ -1019,9 +1019,11 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   const ElemOperands<float> o = operands32(S);
   const CgFuse fuse{G->parts.ptr};
   int nparts = 0;
-  const int rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D,
-                                      (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
-  if (rc == 1) return fail(BP_ERROR_ARG, "packed group: operator form not available");
+  int rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D,
+                                (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
+  if (rc == 1)   // no TMA form (odd Nq): the line-per-thread kernel
+    rc = launch_ax_line_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
+                               (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
   BP_TRY(rc);
   grp_alpha_kernel<PK><<<1, kAlphaThreads, 0, s>>>(nparts, G->parts.ptr, G->sc);
   BP_CUDA_TRY(cudaGetLastError());
@@ -1062,28 +1064,59 @@ static int grp_reliable(CgGroup* G, int l, double tol, int maxit, cudaStream_t s
   return grp_replace(G, l, false, tol, maxit, s);
 }
 
+// Balance the branches: groups and standalone systems, largest first, each to
+// the branch with the least work so far (work ~ unknowns x lanes per iteration)
+static void batch_assign_branches(bp_batch_s* B) {
+  const int nb = (int)B->branches.size();
+  struct Item { double cost; int group, sys; };
+  std::vector<Item> items;
+  for (size_t gi = 0; gi < B->groups.size(); ++gi)
+    items.push_back({(double)B->groups[gi]->base->N * B->groups[gi]->pk, (int)gi, -1});
+  for (size_t i = 0; i < B->sys_solver.size(); ++i)
+    if (B->sys_group[i] < 0) items.push_back({(double)B->sys_solver[i]->N, -1, (int)i});
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+  std::vector<double> load(nb, 0.0);
+  B->group_branch.assign(B->groups.size(), 0);
+  B->sys_branch.assign(B->sys_solver.size(), 0);
+  for (const Item& it : items) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[k] += it.cost;
+    if (it.group >= 0) B->group_branch[it.group] = k;
+    else B->sys_branch[it.sys] = k;
+  }
+}
+
+// fork the branches off s (their work follows) and join them back
+static int batch_fork(bp_batch_s* B, cudaStream_t s) {
+  BP_CUDA_TRY(cudaEventRecord(B->fork, s));
+  for (auto st : B->branches) BP_CUDA_TRY(cudaStreamWaitEvent(st, B->fork, 0));
+  return BP_SUCCESS;
+}
+static int batch_join(bp_batch_s* B, cudaStream_t s) {
+  for (size_t k = 0; k < B->branches.size(); ++k) {
+    BP_CUDA_TRY(cudaEventRecord(B->joins[k], B->branches[k]));
+    BP_CUDA_TRY(cudaStreamWaitEvent(s, B->joins[k], 0));
+  }
+  return BP_SUCCESS;
+}
+
 static int batch_capture(bp_batch_s* B, cudaStream_t s) {
   if (B->graph) return BP_SUCCESS;
   cudaGraph_t g;
   BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  int rc = BP_SUCCESS;
-  cudaError_t ce = cudaEventRecord(B->fork, s);
-  const int nb = (int)B->branches.size();
-  for (int k = 0; k < nb && ce == cudaSuccess; ++k) ce = cudaStreamWaitEvent(B->branches[k], B->fork, 0);
-  int unit = 0;   // groups and standalone systems, round robin over the branches
-  for (size_t gi = 0; gi < B->groups.size() && ce == cudaSuccess && rc == BP_SUCCESS; ++gi, ++unit)
-    for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k) rc = grp_body(B->groups[gi], B->branches[unit % nb]);
-  for (size_t i = 0; i < B->sys_solver.size() && ce == cudaSuccess && rc == BP_SUCCESS; ++i) {
+  int rc = batch_fork(B, s);
+  cudaError_t ce = cudaSuccess;
+  for (size_t gi = 0; gi < B->groups.size() && rc == BP_SUCCESS; ++gi)
+    for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k)
+      rc = grp_body(B->groups[gi], B->branches[B->group_branch[gi]]);
+  for (size_t i = 0; i < B->sys_solver.size() && rc == BP_SUCCESS; ++i) {
     if (B->sys_group[i] >= 0) continue;
-    cudaStream_t bs = B->branches[unit++ % nb];
+    cudaStream_t bs = B->branches[B->sys_branch[i]];
     bp_solver_s* S = B->sys_solver[i];
     for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k)
       rc = B->mixed ? body32(S, nullptr, nullptr, bs) : body64(S, B->x[i]->ptr, B->r[i]->ptr, bs);
   }
-  for (int k = 0; k < nb && ce == cudaSuccess; ++k) {
-    ce = cudaEventRecord(B->joins[k], B->branches[k]);
-    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s, B->joins[k], 0);
-  }
+  if (rc == BP_SUCCESS) rc = batch_join(B, s);
   cudaError_t ce2 = cudaStreamEndCapture(s, &g);
   if (rc != BP_SUCCESS) return rc;
   BP_CUDA_TRY(ce);
@@ -1136,7 +1169,9 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
   std::vector<CgScalars> h;
   BP_TRY(batch_read(B, h, s));
   for (;;) {
+    // reliable updates, each on its unit's branch (the units are independent)
     bool running = false, updated = false;
+    BP_TRY(batch_fork(B, s));
     for (size_t gi = 0; gi < B->groups.size(); ++gi) {
       CgGroup* G = B->groups[gi];
       const int slot0 = (int)(G->sc - B->sc.ptr);
@@ -1144,7 +1179,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
         const CgScalars& c = h[slot0 + l];
         if (c.breakdown) continue;
         if (c.update) {
-          BP_TRY(grp_reliable(G, l, tol, maxit, s));
+          BP_TRY(grp_reliable(G, l, tol, maxit, B->branches[B->group_branch[gi]]));
           ++updates[slot0 + l];
           updated = true;
         } else if (!c.done) {
@@ -1157,13 +1192,15 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       const CgScalars& c = h[B->sys_slot[i]];
       if (c.breakdown) continue;
       if (B->mixed && c.update) {
-        BP_TRY(mixed_reliable(B->sys_solver[i], B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
+        BP_TRY(mixed_reliable(B->sys_solver[i], B->x[i]->ptr, B->r[i]->ptr, tol, maxit,
+                              B->branches[B->sys_branch[i]]));
         ++updates[B->sys_slot[i]];
         updated = true;
       } else if (!c.done) {
         running = true;
       }
     }
+    BP_TRY(batch_join(B, s));
     if (updated) {   // the updated systems may have converged or resumed
       BP_TRY(batch_read(B, h, s));
       continue;
@@ -1244,10 +1281,13 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
     int nslots = 0;
     for (int j = 0; j < nproblems; ++j) {
       const bp_batch_problem_t& P = problems[j];
-      const bool packable = B->mixed && d->bp == 5 && (P.N + 1) % 2 == 0 && P.N + 1 <= 12;
+      const bool packable = B->mixed && d->bp == 5 && P.N + 1 <= 12;
+      // four lanes where the packed operator keeps its registers (TMA form at even
+      // Nq; line form up to Nq = 8), two above
+      const int maxpk = ((P.N + 1) % 2 == 0 || P.N + 1 <= 8) ? 4 : 2;
       for (int k = 0; k < P.nrhs;) {
         const int left = P.nrhs - k;
-        const int pk = !packable || left == 1 ? 0 : (left == 2 ? 2 : 4);
+        const int pk = !packable || left == 1 ? 0 : (left == 2 ? 2 : maxpk);
         const int n = pk ? std::min(pk, left) : 1;
         units.push_back({j, k, n, pk});
         nslots += pk ? pk : 1;
@@ -1333,6 +1373,7 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
       slot += u.pk ? u.pk : 1;
     }
     if (rc == BP_SUCCESS) {
+      batch_assign_branches(B);
       cudaError_t ce2 = cudaStreamSynchronize(s);
       if (ce2 != cudaSuccess) rc = cuda_fail(ce2, "bp_batch_create", __FILE__, __LINE__);
     }
