@@ -47,10 +47,10 @@ WORKLOAD = ("BP5 Hex3D p=7, 40^3 elements, interior vertices perturbed 0.1h (see
 # CPU sample: the same problem family on a 20^3 sub-box (1/8 of the elements)
 CPU_NX, CPU_ITERS = 20, 100
 MIXED_TOL = 1e-8
-# DRAM traffic of one launch of the FP32 element operator on this workload: the
-# ncu capture of BK5 -fp MIXED on the 20^3 box (profiles/ax_tma_f32_bk5_p7_20cubed.md,
-# 150.4 MB for 8000 elements) scaled by the element count to 64,000 elements
-AX_DRAM_BYTES = 150.36e6 * 8
+# DRAM traffic of one launch of the packed FP32 element operator (4 rhs) on this
+# workload: the ncu capture of BK5 -fp MIXED -nr 4 on the 20^3 box (217.6 MB for
+# 8000 elements) scaled by the element count to 64,000 elements
+AX_DRAM_BYTES = 217.597e6 * 8
 
 
 def ax_model_bytes(Ndofs, E, Np, Nf=1, s=8):
@@ -308,30 +308,34 @@ def main():
     st100 = fp64_solve(0.0, ITERS)
     plain["fixed_100_iterations_gdof_it_s"] = world * Nd * ITERS / (st100.elapsed_ms / 1e3) / 1e9
 
-    # ---- dominant kernel of the step: the FP32 element operator, timed alone ----
+    # ---- dominant kernel of the step: the packed FP32 element operator on the four
+    # right-hand sides (what the batched solve launches), timed alone ----
     v = mesh.view
     ng = mesh.E * mesh.Np
     ops = {"wJ": bp.DeviceBuffer(ng, np.float32), "ggeo": bp.DeviceBuffer(6 * ng, np.float32),
            "gllw": bp.DeviceBuffer(mesh.Nq, np.float32), "D": bp.DeviceBuffer(mesh.Nq * mesh.Nq, np.float32)}
     for name, n in (("wJ", ng), ("ggeo", 6 * ng), ("gllw", mesh.Nq), ("D", mesh.Nq * mesh.Nq)):
         bp.convert_f64_f32(getattr(v, name), n, ops[name])
-    q32 = bp.DeviceBuffer(Nd, np.float32)
-    bp.convert_f64_f32(b0, Nd, q32)
-    AqL = bp.DeviceBuffer(mesh.NL, np.float32)
+    q32 = bp.DeviceBuffer(Nd * NRHS, np.float32)
+    b32 = bp.DeviceBuffer(Nd, np.float32)
+    bp.convert_f64_f32(b0, Nd, b32)
+    q32.upload(np.repeat(b32.download(), NRHS))   # interleaved: row r, system k at r*NRHS + k
+    AqL = bp.DeviceBuffer(mesh.NL * NRHS, np.float32)
     for _ in range(3):
-        bp.ax_hex3d_f32(mesh, q32, AqL, ops)
+        bp.ax_hex3d_f32_multi(mesh, NRHS, q32, AqL, ops)
     a0, a1 = ev(), ev()
     bp._check(L.bp_event_record(a0, None))
     for _ in range(args.ax_launches):
-        bp.ax_hex3d_f32(mesh, q32, AqL, ops)
+        bp.ax_hex3d_f32_multi(mesh, NRHS, q32, AqL, ops)
     bp._check(L.bp_event_record(a1, None))
     bp._check(L.bp_event_elapsed_ms(a0, a1, bp.ctypes.byref(ms)))
     ax_s = ms.value / 1e3 / args.ax_launches
     E, Np = mesh.E, mesh.Np
-    ax_bytes = ax_model_bytes(Nd, E, Np, s=4)
+    # reference model with 4-byte values, the q and Aq terms once per right-hand side
+    ax_bytes = ax_model_bytes(Nd, E, Np, s=4) + (NRHS - 1) * (Nd * 4 + E * Np * 4)
     peak, peak_kind = read_peaks()
     achieved = ax_bytes / ax_s / 1e9
-    del AqL, ops, q32
+    del AqL, ops, q32, b32
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -351,14 +355,15 @@ def main():
                        "final_relative_residual_max": rel_res,
                        "fp64_check_relative_residual": resid,
                        "parallelism": "replicas" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (FP32 factors 0.92 GB read per operator apply)"},
+                       "l2": "inputs larger than L2 (FP32 factors 0.92 GB read per packed operator apply)"},
             "clocks": clk,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": NRHS * 8 * Nd,
                     "d2h_bytes_per_step": NRHS * 8 * Nd},
             "gpu_launches": launches_per_step * args.steps,
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": value / plain["gdof_it_s"],
-            "roofline": {"bound": "hbm", "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,float> (bp_ax_hex3d_f32)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,float,Pack<float,4>> (bp_ax_hex3d_f32_multi, 4 rhs)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes,
                          "launch_ms": ax_s * 1e3},

@@ -45,7 +45,7 @@ EXPORTS = [
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc",
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
-    "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32",
+    "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
 ]
 
 
@@ -168,6 +168,8 @@ def lib():
             "bp_batch_solver": [vp, i32, ctypes.POINTER(vp)],
             "bp_ax_hex3d_f32": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp, vp],
             "bp_convert_f64_f32": [sz, vp, vp, vp],
+            "bp_ax_hex3d_f32_multi": [ctypes.POINTER(AxDesc), i32, i32, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp,
+                                      vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -365,6 +367,15 @@ def ax_hex3d_f32(mesh, q, Aq, ops, lam=1.0, stream=None):
     _check(lib().bp_ax_hex3d_f32(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, _ptr(ops["wJ"]),
                                  _ptr(ops["ggeo"]), _ptr(ops["gllw"]), _ptr(ops["D"]), float(lam), _ptr(q),
                                  _ptr(Aq), stream))
+
+
+def ax_hex3d_f32_multi(mesh, nrhs, q, Aq, ops, lam=1.0, stream=None):
+    """bp_ax_hex3d_f32_multi: the FP32 operator on nrhs interleaved right-hand sides."""
+    v = mesh.view
+    d = AxDesc(5, mesh.N, int(mesh.affine), 1)
+    _check(lib().bp_ax_hex3d_f32_multi(ctypes.byref(d), nrhs, mesh.E, v.elementList, v.GlobalToLocal,
+                                       _ptr(ops["wJ"]), _ptr(ops["ggeo"]), _ptr(ops["gllw"]), _ptr(ops["D"]),
+                                       float(lam), _ptr(q), _ptr(Aq), stream))
 
 
 def ogs_gather(mesh, v, gv, stream=None):

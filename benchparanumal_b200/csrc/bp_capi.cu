@@ -219,6 +219,30 @@ int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* 
                         to_stream(stream));
 }
 
+int bp_ax_hex3d_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Nelements, const int32_t* elementList,
+                          const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
+                          const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream) {
+  if (nrhs == 1)
+    return bp_ax_hex3d_f32(desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq, stream);
+  BP_TRY(check_ax_desc(desc));
+  if (nrhs != 2 && nrhs != 4) return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: nrhs must be 1, 2 or 4");
+  if (desc->Nfields != 1 || desc->affine)
+    return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: one field, stored factors only");
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  if (!elementList || !GlobalToLocal || !wJ || !ggeo || !D || !q || !Aq)
+    return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: null array");
+  if ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(Aq)) % (sizeof(float) * nrhs))
+    return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: q and Aq must be aligned to nrhs floats");
+  const cudaStream_t s = to_stream(stream);
+  int rc = launch_ax_tma_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, D, lambda, q, Aq,
+                                nullptr, nullptr, s, nullptr);
+  if (rc == 1)
+    rc = launch_ax_line_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq,
+                               nullptr, nullptr, s, nullptr);
+  return rc;
+}
+
 int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream) {
   if (n > 0 && (!src || !dst)) return fail(BP_ERROR_ARG, "bp_convert_f64_f32: null array");
   return launch_d2f(n, src, dst, to_stream(stream));

@@ -157,6 +157,10 @@ void add_common(Settings& S, bool bp) {
   S.add("-s", "--seed", "FORCING SEED", "0", "LCG seed of the RANDOM forcing (extension)");
   S.add("-pt", "--perturb", "VERTEX PERTURBATION", "0", "Interior vertex perturbation, fraction of h (extension)");
   S.add("-ps", "--perturb-seed", "PERTURBATION SEED", "1", "LCG seed of the vertex perturbation (extension)");
+  if (!bp)
+    S.add("-nr", "--rhs", "RIGHT-HAND SIDES", "1",
+          "With -fp MIXED: apply the FP32 operator to 1, 2 or 4 interleaved right-hand sides at once (extension)",
+          {"1", "2", "4"});
   if (bp) {
     S.add("-it", "--iterations", "CG ITERATIONS", "100", "Maximum CG iterations of the timed solve (extension)");
     S.add("-wi", "--warmup-iterations", "WARMUP ITERATIONS", "1000", "CG iterations of the warmup solve (extension)");
@@ -331,20 +335,35 @@ int run_bk(const char* name, int bk, Settings& S) {
   const bool fp32 = S.compare("PRECISION", "MIXED");
   if (fp32 && bk < 5) throw std::runtime_error("-fp MIXED is available for BK5 and BK6");
   const size_t ng = P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.view.Np;
+  const int nr = std::atoi(S.get("RIGHT-HAND SIDES").c_str());
+  if (nr > 1 && !fp32) throw std::runtime_error("-nr needs -fp MIXED");
   DevVec32 wJ32(fp32 ? ng : 0), ggeo32(fp32 ? 6 * ng : 0), gllw32(fp32 ? P.view.Nq : 0),
-      D32(fp32 ? (size_t)P.view.Nq * P.view.Nq : 0), q32(fp32 ? (size_t)Ngather : 0),
-      Aq32(fp32 ? (size_t)P.view.Nlocal : 0);
+      D32(fp32 ? (size_t)P.view.Nq * P.view.Nq : 0), q32(fp32 ? (size_t)Ngather * nr : 0),
+      Aq32(fp32 ? (size_t)P.view.Nlocal * nr : 0);
   if (fp32) {
     check(bp_convert_f64_f32(ng, P.view.wJ, wJ32.p, nullptr));
     check(bp_convert_f64_f32(6 * ng, P.view.ggeo, ggeo32.p, nullptr));
     check(bp_convert_f64_f32(P.view.Nq, P.view.gllw, gllw32.p, nullptr));
     check(bp_convert_f64_f32((size_t)P.view.Nq * P.view.Nq, P.view.D, D32.p, nullptr));
-    check(bp_convert_f64_f32(Ngather, q.p, q32.p, nullptr));
+    // every right-hand side gets the same input (the timing does not depend on the values)
+    DevVec32 q1(Ngather);
+    check(bp_convert_f64_f32(Ngather, q.p, q1.p, nullptr));
+    for (int k = 0; k < nr; ++k)
+      check(bp_memcpy_dtod(q32.p + (size_t)Ngather * k, q1.p, sizeof(float) * Ngather, nullptr));
+    if (nr > 1) {   // interleave: q32[row*nr + k]
+      std::vector<float> h((size_t)Ngather * nr), t((size_t)Ngather * nr);
+      check(bp_memcpy_dtoh(h.data(), q32.p, sizeof(float) * h.size(), nullptr));
+      check(bp_finish(nullptr));
+      for (int k = 0; k < nr; ++k)
+        for (int32_t r = 0; r < Ngather; ++r) t[(size_t)r * nr + k] = h[(size_t)k * Ngather + r];
+      check(bp_memcpy_htod(q32.p, t.data(), sizeof(float) * t.size(), nullptr));
+      check(bp_finish(nullptr));
+    }
   }
   auto apply = [&]() {
     if (fp32)
-      check(bp_ax_hex3d_f32(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, wJ32.p, ggeo32.p,
-                            gllw32.p, D32.p, 1.0f, q32.p, Aq32.p, nullptr));
+      check(bp_ax_hex3d_f32_multi(&d, nr, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, wJ32.p,
+                                  ggeo32.p, gllw32.p, D32.p, 1.0f, q32.p, Aq32.p, nullptr));
     else if (bk >= 5)
       check(bp_ax_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
                         P.view.gllw, P.view.D, 1.0, q.p, Aq.p, nullptr));
@@ -360,15 +379,17 @@ int run_bk(const char* name, int bk, Settings& S) {
   const double t1 = now_after_finish();
   const double elapsed = (t1 - t0) / Ntests;
   const long long Ndofs = Ngather;
-  const double Nbytes = ax_bytes(bk, P.view, Ndofs, fp32 ? 4.0 : 8.0);
-  const double Nflops = ax_flops(bk, P.view);
+  // per apply: the model's bytes with 4-byte values, the q/Aq terms once per right-hand side
+  double Nbytes = ax_bytes(bk, P.view, Ndofs, fp32 ? 4.0 : 8.0);
+  if (nr > 1) Nbytes += (nr - 1) * (Ndofs * 4.0 + (double)P.view.Nlocal * 4.0);
+  const double Nflops = ax_flops(bk, P.view) * nr;
   std::string suffix = "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
       "DOFs/ranks*time=%1.2e, %s \n",
       name, P.view.N, Ndofs, elapsed, elapsed / Ndofs, Nbytes / (1.0e9 * elapsed), Nflops / (1.0e9 * elapsed),
-      Ndofs / (1 * elapsed), suffix.c_str());
+      Ndofs * (double)nr / (1 * elapsed), suffix.c_str());
   std::fflush(stdout);
   return BP_SUCCESS;
 }

@@ -106,6 +106,13 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
 int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
                     const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
                     const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream);
+/* The FP32 operator on nrhs (1, 2 or 4) right-hand sides at once: q and Aq hold
+   nrhs consecutive floats per gathered row / local node (system k at offset k),
+   so the index and factor traffic is shared by the systems.  One field, stored
+   factors.  No counterpart in the reference (one vector per Operator call). */
+int bp_ax_hex3d_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Nelements, const int32_t* elementList,
+                          const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
+                          const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream);
 /* dst[i] = (float) src[i], i < n, device arrays (to build FP32 operands). */
 int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream);
 

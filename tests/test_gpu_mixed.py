@@ -63,3 +63,31 @@ def test_mixed_host_entry_matches_device_entry(gpu):
     st2 = S.solve_host(bh, xh, tol=1e-8, maxit=5000)
     assert st2.iterations == st.iterations and st2.updates == st.updates
     np.testing.assert_array_equal(xh, x.download())
+
+
+@pytest.mark.parametrize("N,nrhs", [(7, 4), (7, 2), (4, 4), (6, 2), (9, 2), (3, 4)])
+def test_fp32_multi_rhs_operator_matches_single(gpu, oracle, N, nrhs):
+    # the packed operator (TMA form at even Nq, line form at odd Nq) gives each
+    # right-hand side what the single-rhs FP32 operator gives it, and both are
+    # the FP64 oracle's operator to FP32 accuracy
+    om = oracle.Mesh(3, 2, 2, N, pert=0.1)
+    gm = gpu.Mesh(3, 2, 2, N=N, pert=0.1)
+    v = gm.view
+    ng = gm.E * gm.Np
+    ops = {"wJ": gpu.DeviceBuffer(ng, np.float32), "ggeo": gpu.DeviceBuffer(6 * ng, np.float32),
+           "gllw": gpu.DeviceBuffer(gm.Nq, np.float32), "D": gpu.DeviceBuffer(gm.Nq * gm.Nq, np.float32)}
+    for name, n in (("wJ", ng), ("ggeo", 6 * ng), ("gllw", gm.Nq), ("D", gm.Nq * gm.Nq)):
+        gpu.convert_f64_f32(getattr(v, name), n, ops[name])
+    Q = np.stack([2 * oracle.random(20 + k, gm.Ngather) - 1 for k in range(nrhs)], axis=1).astype(np.float32)
+    dq = gpu.DeviceBuffer.from_host(np.ascontiguousarray(Q).ravel())
+    dA = gpu.DeviceBuffer(gm.NL * nrhs, np.float32)
+    gpu.ax_hex3d_f32_multi(gm, nrhs, dq, dA, ops)
+    A = dA.download().reshape(gm.NL, nrhs)
+    for k in range(nrhs):
+        q1 = gpu.DeviceBuffer.from_host(np.ascontiguousarray(Q[:, k]))
+        a1 = gpu.DeviceBuffer(gm.NL, np.float32)
+        gpu.ax_hex3d_f32(gm, q1, a1, ops)
+        single = a1.download()
+        assert np.max(np.abs(A[:, k] - single)) <= 1e-6 * np.max(np.abs(single))
+        want = om.ax(Q[:, k].astype(np.float64))
+        assert np.max(np.abs(A[:, k] - want)) <= 2e-5 * np.max(np.abs(want))
