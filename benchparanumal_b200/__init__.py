@@ -46,6 +46,7 @@ EXPORTS = [
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
+    "bp_ax_cub_hex3d_f32",
 ]
 
 
@@ -170,6 +171,8 @@ def lib():
             "bp_convert_f64_f32": [sz, vp, vp, vp],
             "bp_ax_hex3d_f32_multi": [ctypes.POINTER(AxDesc), i32, i32, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp,
                                       vp],
+            "bp_ax_cub_hex3d_f32": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp,
+                                    vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)

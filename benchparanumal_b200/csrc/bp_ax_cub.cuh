@@ -94,8 +94,26 @@ struct CubShape {
   static constexpr int SLOT = cub_slot(NQ, !CURVED);
   static constexpr int TSIZE = G * NQ;              // T rows = output points
   static constexpr int DSIZE = STIFF ? G * G : 0;
-  static constexpr size_t SMEM = sizeof(CubReal) * (size_t)NBUF * FIELD * EPB;
+  // FP32 curved forms stage each element's Gauss-point factors in shared memory
+  // with cp.async at the element's start, so their latency overlaps the gather
+  // and the interpolation (the FP64 factors would halve the resident blocks)
+  static constexpr bool STAGE = CURVED && sizeof(CubReal) == 4;
+  static constexpr int GP = G * G * G;
+  static constexpr size_t FIELDS = sizeof(CubReal) * (size_t)NBUF * FIELD * EPB;
+  static constexpr size_t GOFF = (FIELDS + 15) & ~(size_t)15;                        // [EPB][GP*6] ggeo
+  static constexpr size_t WOFF = GOFF + (STAGE && STIFF ? sizeof(CubReal) * (size_t)EPB * GP * 6 : 0);   // [EPB][GP] wJ
+  static constexpr size_t SMEM = STAGE ? WOFF + sizeof(CubReal) * (size_t)EPB * GP : FIELDS;
 };
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <int NQ, int FORM>
 __global__ void __launch_bounds__(CubShape<NQ, FORM>::THREADS, CubShape<NQ, FORM>::MINB)
@@ -107,7 +125,7 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
   using F = CubReal;
   using Sh = CubShape<NQ, FORM>;
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
-  constexpr int G = Sh::G, GP = G * G * G, RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB;
+  constexpr int G = Sh::G, GP = Sh::GP, RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB;
   constexpr int NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
   constexpr int SLOT = Sh::SLOT, DOFF = Sh::SLOT + Sh::TSIZE;
   // T(o, i): 1D transform from NQ nodes to G points; MASS_AFFINE applies MM^T
@@ -127,6 +145,19 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
   const bool valid = eidx < Nelements;
   const int element = valid ? elementList[eidx] : 0;
   double pdot = 0.0;
+
+  // the element's factors into shared memory, in flight while q is gathered and interpolated
+  F* const sG = reinterpret_cast<F*>(smem_raw + Sh::GOFF) + (size_t)es * GP * 6;
+  F* const sW = reinterpret_cast<F*>(smem_raw + Sh::WOFF) + (size_t)es * GP;
+  if (Sh::STAGE && valid) {
+    const int tl = tx + G * ty;
+    if (Sh::STIFF) {
+      const F* src = ggeo + 6 * (size_t)element * GP;   // 8-byte aligned: 24 bytes per point
+      for (int c = tl; c < GP * 3; c += G * G) cp_async8(sG + 2 * c, src + 2 * c);
+    }
+    const F* srcw = wJ + (size_t)element * GP;
+    for (int c = tl; c < GP; c += G * G) cp_async4(sW + c, srcw + c);
+  }
 
   F wa = 0, ga[6] = {0, 0, 0, 0, 0, 0};
   if (!Sh::CURVED) {
@@ -206,9 +237,16 @@ BP_CUB_OUTER
     }
     F acc[G];
     if (FORM == CUB_MASS) {
-      const size_t gb = (size_t)element * GP + ty * G + tx;
+      if (Sh::STAGE) {
+        cp_async_wait_all();
+        __syncthreads();
 #pragma unroll
-      for (int k = 0; k < G; ++k) acc[k] = wJ[gb + k * G * G] * qk[k];
+        for (int k = 0; k < G; ++k) acc[k] = sW[k * G * G + ty * G + tx] * qk[k];
+      } else {
+        const size_t gb = (size_t)element * GP + ty * G + tx;
+#pragma unroll
+        for (int k = 0; k < G; ++k) acc[k] = wJ[gb + k * G * G] * qk[k];
+      }
     } else {
       // own column: every earlier read of it was this thread's
 #pragma unroll
@@ -245,12 +283,19 @@ BP_CUB_OUTER
         for (int n = 0; n < G; ++n) t += D_(k, n) * qk[n];
         gt[k] = t;
       }
+      if (Sh::STAGE) cp_async_wait_all();   // this thread's copies; the barrier below makes all visible
       __syncthreads();
       // fluxes at the points of column (tx, ty)
 #pragma unroll
       for (int k = 0; k < G; ++k) {
         F g0, g1, g2, g3, g4, g5, w;
-        if (Sh::CURVED) {
+        if (Sh::STAGE) {
+          const int pt = k * G * G + ty * G + tx;
+          const V2* gv = reinterpret_cast<const V2*>(sG + 6 * pt);
+          const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
+          g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
+          w = sW[pt];
+        } else if (Sh::CURVED) {
           const size_t gb = (size_t)element * GP + k * G * G + ty * G + tx;
           const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * gb);
           const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
@@ -344,7 +389,7 @@ BP_CUB_OUTER
     }
   }
   if (partials) {
-    static_assert(sizeof(F) * Sh::NBUF * Sh::FIELD * EPB >= sizeof(double) * Sh::THREADS, "scratch too small");
+    static_assert(Sh::FIELDS >= sizeof(double) * Sh::THREADS, "scratch too small");
     const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(sbase));
     if (tid == 0) partials[blockIdx.x] = bs;
   }

@@ -266,6 +266,25 @@ int bp_ax_cub_hex3d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* ele
   return launch_ax_cub(*d, Nelements, elementList, GlobalToLocal, ops, lambda, q, Aq, nullptr, to_stream(stream));
 }
 
+int bp_ax_cub_hex3d_f32(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* elementList,
+                        const int32_t* GlobalToLocal, const float* cubwJ, const float* cubggeo, const float* cubD,
+                        const float* cubInterp, const float* invV, const float* MM, float lambda, const float* q,
+                        float* Aq, bp_stream_t stream) {
+  if (!d) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: null descriptor");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: degree N must be in 1..15");
+  if (d->bp < 1 || d->bp > 4) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: bp must be 1..4");
+  if (d->Nfields != ((d->bp % 2) ? 1 : 3))
+    return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: BP1/BP3 have 1 field, BP2/BP4 3");
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  const bool stiff = d->bp >= 3;
+  const float* T = !d->affine ? cubInterp : (stiff ? invV : MM);
+  if (!elementList || !GlobalToLocal || !cubwJ || !T || !q || !Aq || (stiff && (!cubggeo || !cubD)))
+    return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: null array");
+  const CubOperands<float> ops{cubwJ, cubggeo, cubD, T};
+  return launch_ax_cub(*d, Nelements, elementList, GlobalToLocal, ops, lambda, q, Aq, nullptr, to_stream(stream));
+}
+
 int bp_ogs_gather(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* v, double* gv,
                   bp_stream_t stream) {
   if (Nrows < 0) return fail(BP_ERROR_ARG, "bp_ogs_gather: negative row count");

@@ -333,10 +333,9 @@ int run_bk(const char* name, int bk, Settings& S) {
   d.Nfields = Nfields;
   // -fp MIXED times the FP32 operator of the mixed-precision solver (BK5/BK6)
   const bool fp32 = S.compare("PRECISION", "MIXED");
-  if (fp32 && bk < 5) throw std::runtime_error("-fp MIXED is available for BK5 and BK6");
   const size_t ng = P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.view.Np;
   const int nr = std::atoi(S.get("RIGHT-HAND SIDES").c_str());
-  if (nr > 1 && !fp32) throw std::runtime_error("-nr needs -fp MIXED");
+  if (nr > 1 && (!fp32 || bk != 5)) throw std::runtime_error("-nr is available for BK5 with -fp MIXED");
   DevVec32 wJ32(fp32 ? ng : 0), ggeo32(fp32 ? 6 * ng : 0), gllw32(fp32 ? P.view.Nq : 0),
       D32(fp32 ? (size_t)P.view.Nq * P.view.Nq : 0), q32(fp32 ? (size_t)Ngather * nr : 0),
       Aq32(fp32 ? (size_t)P.view.Nlocal * nr : 0);
@@ -360,8 +359,25 @@ int run_bk(const char* name, int bk, Settings& S) {
       check(bp_finish(nullptr));
     }
   }
+  // BK1-BK4 in FP32: FP32 copies of the cubature operands
+  const bool cub32 = fp32 && bk <= 4;
+  const size_t nc = !cub32 ? 0 : P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.cub.cubNp;
+  const size_t Nq2 = (size_t)P.view.Nq * P.view.Nq, nD = P.view.affine ? Nq2 : (size_t)P.cub.cubNq * P.cub.cubNq;
+  const size_t nI = (size_t)P.cub.cubNq * P.view.Nq;
+  DevVec32 cwJ(nc), cgeo(6 * nc), cD(cub32 ? nD : 0), cI(cub32 ? nI : 0), cV(cub32 ? Nq2 : 0), cM(cub32 ? Nq2 : 0);
+  if (cub32) {
+    check(bp_convert_f64_f32(nc, P.cub.cubwJ, cwJ.p, nullptr));
+    check(bp_convert_f64_f32(6 * nc, P.cub.cubggeo, cgeo.p, nullptr));
+    check(bp_convert_f64_f32(nD, P.cub.cubD, cD.p, nullptr));
+    check(bp_convert_f64_f32(nI, P.cub.cubInterp, cI.p, nullptr));
+    check(bp_convert_f64_f32(Nq2, P.cub.invV, cV.p, nullptr));
+    check(bp_convert_f64_f32(Nq2, P.cub.MM, cM.p, nullptr));
+  }
   auto apply = [&]() {
-    if (fp32)
+    if (cub32)
+      check(bp_ax_cub_hex3d_f32(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, cwJ.p, cgeo.p, cD.p,
+                                cI.p, cV.p, cM.p, 1.0f, q32.p, Aq32.p, nullptr));
+    else if (fp32)
       check(bp_ax_hex3d_f32_multi(&d, nr, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, wJ32.p,
                                   ggeo32.p, gllw32.p, D32.p, 1.0f, q32.p, Aq32.p, nullptr));
     else if (bk >= 5)

@@ -133,6 +133,13 @@ int bp_ax_cub_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* 
                     const double* cubInterp, const double* invV, const double* MM, double lambda, const double* q,
                     double* Aq, bp_stream_t stream);
 
+/* The same over-integrated operators in FP32 (the inner operator of the
+   mixed-precision CG for BP1-BP4), every array FP32. */
+int bp_ax_cub_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                        const int32_t* GlobalToLocal, const float* cubwJ, const float* cubggeo, const float* cubD,
+                        const float* cubInterp, const float* invV, const float* MM, float lambda, const float* q,
+                        float* Aq, bp_stream_t stream);
+
 /* ogs Gather(Add, Trans): gv[r] = sum over c in row r of v[colIds[c]] in column
    order.  Replaces ogsOperator_t::Gather (libs/ogs/ogsOperator.cpp:160-188) and
    the OKL gather kernel (libs/ogs/okl/ogsKernels.okl:86-122), K=1, T=double. */

@@ -131,3 +131,34 @@ def test_cub_driver_result_lines(gpu, capfd, k):
     assert gpu.driver_main("BK%d" % k, ["-nx", "3", "-ny", "3", "-nz", "3", "-p", "4", "-a"]) == 0
     out = capfd.readouterr().out
     assert [l for l in out.splitlines() if l.startswith("BK%d: N= 4," % k)][0].endswith("Element=Hex, Affine ")
+
+
+@pytest.mark.parametrize("bpn,N,affine", [(3, 7, False), (3, 4, False), (1, 7, False), (4, 5, False), (3, 6, True),
+                                          (1, 5, True)])
+def test_cub_fp32_operator_matches_oracle(gpu, oracle, bpn, N, affine):
+    # the FP32 over-integrated operator (the mixed-precision solver's inner
+    # operator) is the FP64 oracle's to FP32 accuracy
+    Nf = 1 if bpn % 2 else 3
+    pert = 0.0 if affine else 0.1
+    om = oracle.Mesh(3, 2, 2, N, affine=affine, Nfields=Nf, pert=pert)
+    gm = gpu.Mesh(3, 2, 2, N=N, affine=affine, Nfields=Nf, pert=pert)
+    c = gm.cubature()
+    G, Nq = c.cubNq, gm.Nq
+    nc = gm.E if affine else gm.E * c.cubNp
+    sizes = {"cubwJ": nc, "cubggeo": 6 * nc, "cubD": Nq * Nq if affine else G * G, "cubInterp": G * Nq,
+             "invV": Nq * Nq, "MM": Nq * Nq}
+    f32 = {}
+    for name, n in sizes.items():
+        f32[name] = gpu.DeviceBuffer(n, np.float32)
+        gpu.convert_f64_f32(getattr(c, name), n, f32[name])
+    q = 2 * oracle.random(8, om.Ngather) - 1
+    dq = gpu.DeviceBuffer.from_host(q.astype(np.float32))
+    dA = gpu.DeviceBuffer(om.NL, np.float32)
+    d = gpu.AxDesc(bpn, N, int(affine), Nf)
+    v = gm.view
+    gpu._check(gpu.lib().bp_ax_cub_hex3d_f32(gpu.ctypes.byref(d), gm.E, v.elementList, v.GlobalToLocal,
+                                             f32["cubwJ"].ptr, f32["cubggeo"].ptr, f32["cubD"].ptr,
+                                             f32["cubInterp"].ptr, f32["invV"].ptr, f32["MM"].ptr, 1.0, dq.ptr,
+                                             dA.ptr, None))
+    want = om.ax(q.astype(np.float32).astype(np.float64), 1.0, bpn)
+    assert _rel(dA.download().astype(np.float64), want) < 2e-5
