@@ -72,3 +72,26 @@ def test_batch_bad_arguments(gpu):
     B = gpu.Batch([{"nx": 2, "N": 3, "nrhs": 1}], precision="MIXED")
     with pytest.raises(gpu.BPError):
         B.solve(tol=0.0)   # a mixed batch needs a tolerance
+
+
+def test_batch_splits_and_other_problems(gpu, oracle):
+    # six right-hand sides split into a four-lane and a two-lane group; a BP3
+    # batch runs standalone over-integrated systems
+    B = gpu.Batch([{"nx": 2, "N": 5, "pert": 0.1, "pert_seed": 7, "nrhs": 6, "rhs_seed": 50}], precision="MIXED")
+    stats, _ = B.solve(tol=1e-8, maxit=3000)
+    om = oracle.Mesh(2, 2, 2, 5, pert=0.1, pert_seed=7)
+    for s in range(6):
+        xb, bb = B.vectors(s)
+        _, b_o = om.rhs_random(50 + s)
+        np.testing.assert_allclose(bb, b_o, rtol=0, atol=1e-13 * np.max(np.abs(b_o)))
+        assert np.linalg.norm(b_o - om.operator(xb)) <= 1.0001e-8 * np.linalg.norm(b_o)
+    B3 = gpu.Batch([{"nx": 2, "N": 4, "pert": 0.1, "pert_seed": 8, "nrhs": 2, "rhs_seed": 60},
+                    {"nx": 3, "N": 3, "pert": 0.1, "pert_seed": 9, "nrhs": 1, "rhs_seed": 62}], bp=3,
+                   precision="MIXED")
+    stats3, _ = B3.solve(tol=1e-8, maxit=3000)
+    for s in range(3):
+        p = [(2, 4, 8, 60), (2, 4, 8, 61), (3, 3, 9, 62)][s]
+        om3 = oracle.Mesh(p[0], p[0], p[0], p[1], pert=0.1, pert_seed=p[2])
+        xb, _ = B3.vectors(s)
+        _, b_o = om3.rhs_random(p[3])
+        assert np.linalg.norm(b_o - om3.operator(xb, 1.0, 3)) <= 1.0001e-8 * np.linalg.norm(b_o)
