@@ -11,6 +11,7 @@
 // Keys come from libs/core/platformSettings.cpp:31-50,
 // libs/mesh/meshSettings.cpp:31-62 and BP/BP5/src/bp5Settings.cpp:30-46.
 // Keys marked "extension" select the modes the reference does not have.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -162,6 +163,8 @@ void add_common(Settings& S, bool bp) {
           "With -fp MIXED: apply the FP32 operator to 1, 2 or 4 interleaved right-hand sides at once (extension)",
           {"1", "2", "4"});
   if (bp) {
+    S.add("-nr", "--rhs", "RIGHT-HAND SIDES", "1",
+          "Solve this many RANDOM right-hand sides (seeds s, s+1, ...) together with the batched solver (extension)");
     S.add("-it", "--iterations", "CG ITERATIONS", "100", "Maximum CG iterations of the timed solve (extension)");
     S.add("-wi", "--warmup-iterations", "WARMUP ITERATIONS", "1000", "CG iterations of the warmup solve (extension)");
     S.add("-tol", "--tolerance", "CG TOLERANCE", "0", "CG stop tolerance of the timed solve (extension)");
@@ -253,7 +256,91 @@ double ax_flops(int bp, const bp_mesh_view_t& v) {
   return f * Nf * E;
 }
 
+// CG model bytes and flops of one system (bpNRun.cpp: first iteration + Niter iterations)
+void cg_model(int bp, const bp_mesh_view_t& v, long long Ndofs, int Niter, double& Nbytes, double& Nflops) {
+  const double NGlobal = (double)v.Nlocal;
+  const double NbytesAx = ax_bytes(bp, v, Ndofs);
+  const double NbytesGather = (Ndofs + 1) * 4.0 + NGlobal * 4.0 + NGlobal * 8.0 + Ndofs * 8.0;
+  Nbytes = (4 * Ndofs * 8.0 + NbytesAx + NbytesGather) + (11 * Ndofs * 8.0 + NbytesAx + NbytesGather) * Niter;
+  const double NflopsAx = ax_flops(bp, v);
+  Nflops = (5.0 * Ndofs + NflopsAx + NGlobal) + (11.0 * Ndofs + NflopsAx + NGlobal) * Niter;
+}
+
+// -nr K: K right-hand sides of the same problem solved together by the batched
+// solver (packed lanes in a mixed-precision BP5 solve); the result line counts
+// every system's unknowns x iterations
+int run_bp_batch(const char* name, int bp, Settings& S, int nr) {
+  if (bp % 2 == 0) throw std::runtime_error("-nr is available for BP1, BP3 and BP5");
+  if (!S.compare("FORCING", "RANDOM")) throw std::runtime_error("-nr needs -f RANDOM");
+  if (S.compare("AFFINE MESH", "TRUE")) throw std::runtime_error("-nr runs stored-factor meshes (no -a)");
+  if (!S.compare("THREAD MODEL", "CUDA"))
+    throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
+                             " is not available: this build runs the CUDA (sm_100a) path only");
+  check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
+  bp_batch_problem_t pr{};
+  pr.nx = std::atoi(S.get("BOX NX").c_str());
+  pr.ny = std::atoi(S.get("BOX NY").c_str());
+  pr.nz = std::atoi(S.get("BOX NZ").c_str());
+  pr.N = std::atoi(S.get("POLYNOMIAL DEGREE").c_str());
+  pr.pert = std::atof(S.get("VERTEX PERTURBATION").c_str());
+  pr.pert_seed = std::strtoull(S.get("PERTURBATION SEED").c_str(), nullptr, 10);
+  pr.nrhs = nr;
+  pr.rhs_seed = std::strtoull(S.get("FORCING SEED").c_str(), nullptr, 10);
+  bp_solver_desc_t sd{};
+  sd.bp = bp;
+  sd.lambda = 1.0;
+  sd.precon = S.compare("PRECONDITIONER", "JACOBI") ? BP_PRECON_JACOBI : BP_PRECON_NONE;
+  sd.precision = S.compare("PRECISION", "MIXED") ? BP_PRECISION_MIXED : BP_PRECISION_FP64;
+  bp_batch_t B = nullptr;
+  check(bp_batch_create(&pr, 1, &sd, &B));
+  struct Guard {
+    bp_batch_t b;
+    ~Guard() { bp_batch_destroy(b); }
+  } guard{B};
+  const int maxIter = std::atoi(S.get("CG ITERATIONS").c_str());
+  const double tol = std::atof(S.get("CG TOLERANCE").c_str());
+  std::vector<bp_solve_stats_t> st(nr);
+  double ms = 0.0;
+  check(bp_batch_solve(B, tol, maxIter, st.data(), &ms));   // warmup (graph capture)
+  const double t0 = now_after_finish();
+  check(bp_batch_solve(B, tol, maxIter, st.data(), &ms));
+  const double t1 = now_after_finish();
+  const double elapsed = t1 - t0;
+  int32_t Nd = 0;
+  check(bp_batch_system_info(B, 0, nullptr, &Nd));
+  // the sizes the byte/flop model needs
+  bp_mesh_view_t v{};
+  v.N = pr.N; v.Nq = pr.N + 1; v.Np = v.Nq * v.Nq * v.Nq; v.Nelements = pr.nx * pr.ny * pr.nz; v.Nfields = 1;
+  v.affine = 0; v.Ngather = Nd; v.Nlocal = (int64_t)v.Nelements * v.Np;
+  double Nbytes = 0, Nflops = 0, dofit = 0;
+  int itmax = 0;
+  for (int k = 0; k < nr; ++k) {
+    double nb, nf;
+    cg_model(bp, v, Nd, st[k].iterations, nb, nf);
+    Nbytes += nb;
+    Nflops += nf;
+    dofit += (double)Nd * st[k].iterations;
+    itmax = std::max(itmax, (int)st[k].iterations);
+  }
+  std::printf(
+      "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, iterations=%d, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
+      "DOFs*iterations/ranks*time=%1.2e, %s \n",
+      name, pr.N, (long long)Nd, elapsed, itmax, elapsed / ((double)Nd * nr), Nbytes / (1.0e9 * elapsed),
+      Nflops / (1.0e9 * elapsed), dofit / elapsed, "Element=Hex");
+  std::printf("%s extra: right-hand sides=%d solved together, precision=%s, precon=%s, iterations per system:", name,
+              nr, S.get("PRECISION").c_str(), S.get("PRECONDITIONER").c_str());
+  for (int k = 0; k < nr; ++k) std::printf(" %d", st[k].iterations);
+  std::printf(", relative residuals:");
+  for (int k = 0; k < nr; ++k) std::printf(" %.3e", std::sqrt(st[k].rdotr / (st[k].rdotr0 > 0 ? st[k].rdotr0 : 1.0)));
+  std::printf(", device ms=%.4f\n", ms);
+  std::fflush(stdout);
+  return BP_SUCCESS;
+}
+
 int run_bp(const char* name, int bp, Settings& S) {
+  const int nr = std::atoi(S.get("RIGHT-HAND SIDES").c_str());
+  if (nr < 1 || nr > 64) throw std::runtime_error("-nr must be 1..64");
+  if (nr > 1) return run_bp_batch(name, bp, S, nr);
   const int Nfields = (bp == 6 || bp == 4 || bp == 2) ? 3 : 1;
   Problem P;
   setup(S, P, Nfields, bp);

@@ -95,3 +95,14 @@ def test_batch_splits_and_other_problems(gpu, oracle):
         xb, _ = B3.vectors(s)
         _, b_o = om3.rhs_random(p[3])
         assert np.linalg.norm(b_o - om3.operator(xb, 1.0, 3)) <= 1.0001e-8 * np.linalg.norm(b_o)
+
+
+def test_driver_batched_rhs(gpu, capfd):
+    assert gpu.driver_main("BP5", ["-nx", "4", "-ny", "4", "-nz", "4", "-p", "5", "-pt", "0.1", "-f", "RANDOM",
+                                   "-pc", "JACOBI", "-fp", "MIXED", "-tol", "1e-8", "-it", "3000", "-nr", "4"]) == 0
+    out = capfd.readouterr().out
+    line = [l for l in out.splitlines() if l.startswith("BP5: N= 5")][0]
+    assert "DOFs=6859," in line and line.endswith("Element=Hex ")
+    extra = [l for l in out.splitlines() if l.startswith("BP5 extra: right-hand sides=4 solved together")][0]
+    res = [float(v) for v in extra.split("relative residuals:")[1].split(",")[0].split()]
+    assert len(res) == 4 and max(res) <= 1.0001e-8
