@@ -391,8 +391,18 @@ grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, c
     Pack<float, PK> rn = r[row];
     const float dinv = precon ? __ldg(invD + row) : 0.0f;
     const int32_t start = __ldg(rowStarts + row), end = __ldg(rowStarts + row + 1);
-    Pack<float, PK> sum(0.0f);
-    for (int32_t c = start; c < end; ++c) sum += AqL[__ldg(colIds + c)];
+    // every row has a column; the first two (most rows have one or two) are
+    // fetched side by side, the sum keeps column order (464 -> 367 us per
+    // four-rhs launch at 40^3 p=7; the scalar FP64 gather is faster without it,
+    // 208 vs 290 us, and keeps the plain loop)
+    const bool two = start + 1 < end;
+    const int32_t c0 = __ldg(colIds + start);
+    const int32_t c1 = two ? __ldg(colIds + start + 1) : c0;
+    const Pack<float, PK> a0 = AqL[c0];
+    const Pack<float, PK> a1 = AqL[c1];
+    Pack<float, PK> sum = a0;
+    if (two) sum += a1;
+    for (int32_t c = start + 2; c < end; ++c) sum += AqL[__ldg(colIds + c)];
 #pragma unroll
     for (int l = 0; l < PK; ++l) {
       if (act[l]) rn.v[l] = rn.v[l] - alpha[l] * sum.v[l];
