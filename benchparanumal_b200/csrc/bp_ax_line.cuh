@@ -210,11 +210,18 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
     }
   }
   if (partials) {
-#pragma unroll
-    for (int l = 0; l < LANES; ++l) {
-      const double bs = fuse_block_sum(pdot[l], reinterpret_cast<double*>(sbase));
-      if (tid == 0) partials[(size_t)l * gridDim.x + blockIdx.x] = bs;
+    double bs[LANES];
+    if (LANES == 1) {
+      bs[0] = fuse_block_sum(pdot[0], reinterpret_cast<double*>(sbase));
+    } else {
+      static_assert(sizeof(T) * 3 * Sh::FIELD >= sizeof(double) * LANES * NQ2 &&
+                        sizeof(T) * 3 * Sh::FIELD * EPB >= sizeof(double) * LANES * 32,
+                    "block-sum scratch too small");
+      fuse_block_sum_lanes<LANES>(pdot, reinterpret_cast<double*>(sbase), bs);
     }
+    if (tid == 0)
+#pragma unroll
+      for (int l = 0; l < LANES; ++l) partials[(size_t)l * gridDim.x + blockIdx.x] = bs[l];
   }
 #undef AT
 #undef W_

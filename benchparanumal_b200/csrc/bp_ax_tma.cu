@@ -271,12 +271,18 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
 #pragma unroll
       for (int k = 0; k < NQ; ++k) lane_dot(v, r_u[k], r_Au[k]);
     }
-    // the factor ring is free now and holds at least one double per thread
-#pragma unroll
-    for (int l = 0; l < LANES; ++l) {
-      const double bs = fuse_block_sum(v[l], reinterpret_cast<double*>(s_g));
-      if (t == 0) fuse.partials[(size_t)l * gridDim.x + blockIdx.x] = bs;
+    // the factor ring and the q/v/w scratch are free now: LANES doubles per thread
+    double bs[LANES];
+    if (LANES == 1) {
+      bs[0] = fuse_block_sum(v[0], reinterpret_cast<double*>(s_g));
+    } else {
+      static_assert(Lay::BAR >= sizeof(double) * LANES * NQ2 * S && Lay::BAR >= sizeof(double) * LANES * 32,
+                    "block-sum scratch too small");
+      fuse_block_sum_lanes<LANES>(v, reinterpret_cast<double*>(s_g), bs);
     }
+    if (t == 0)
+#pragma unroll
+      for (int l = 0; l < LANES; ++l) fuse.partials[(size_t)l * gridDim.x + blockIdx.x] = bs[l];
   }
 }
 

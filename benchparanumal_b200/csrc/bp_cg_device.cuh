@@ -56,6 +56,56 @@ __device__ __forceinline__ double fuse_block_sum(double v, double* scratch) {
   return r;
 }
 
+// L sums at once (one per lane of a packed group), valid in thread 0, in a
+// fixed order: four barriers for any L instead of three per sum.  `scratch`
+// holds at least L doubles per thread and max(L*32, ...) doubles.
+template <int L>
+__device__ __forceinline__ void fuse_block_sum_lanes(const double (&v)[L], double* scratch, double (&out)[L]) {
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  __syncthreads();   // the caller's last reads of scratch are done
+#pragma unroll
+  for (int l = 0; l < L; ++l) scratch[l * nt + t] = v[l];
+  __syncthreads();
+  if (nt < 32) {   // tiny blocks: thread 0 adds everything
+    if (t == 0)
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        double r = 0.0;
+        for (int k = 0; k < nt; ++k) r += scratch[l * nt + k];
+        out[l] = r;
+      }
+    return;
+  }
+  // stage 1: strided partial sums, (lane, w) = (idx / 32, idx % 32), idx < 32 L
+  double part[L];
+#pragma unroll
+  for (int it = 0; it < L; ++it) {
+    const int idx = t + it * nt;
+    double r = 0.0;
+    if (idx < L * 32) {
+      const int lane = idx >> 5, w = idx & 31;
+      for (int k = w; k < nt; k += 32) r += scratch[lane * nt + k];
+    }
+    part[it] = r;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < L; ++it) {
+    const int idx = t + it * nt;
+    if (idx < L * 32) scratch[idx] = part[it];
+  }
+  __syncthreads();
+  if (t == 0) {
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      double r = 0.0;
+      for (int w = 0; w < 32; ++w) r += scratch[l * 32 + w];
+      out[l] = r;
+    }
+  }
+}
+
 // block partial of p.Ap (plain store; the next kernel reads it)
 __device__ __forceinline__ void fuse_pap(double v, const CgFuse& F, double* scratch) {
   const double bs = fuse_block_sum(v, scratch);
