@@ -131,8 +131,17 @@ struct TmaSmem {
 // or Pack<F, PK> for PK right-hand sides of one mesh in lockstep (then NF = 1
 // and the q/Aq arrays hold one pack per node).  p.Ap partials are summed in
 // double, one per lane: fuse.partials[lane * gridDim.x + blockIdx.x].
+// Packed values need about 128 registers a thread; the second launch bound
+// caps them there, so 65536 / (threads * 128) blocks stay resident (NQ=8: 8
+// blocks of 64 threads instead of 6 at 133 registers, 4 bytes of spills).
+template <int NQ, int NF, class F, class T>
+struct TmaMinBlocks {
+  static constexpr int THREADS = NQ * NQ * TmaShape<NQ, F>::EPB * NF;
+  static constexpr int V = (PackTraits<T>::R > 1) ? (65536 / (THREADS * 128) > 0 ? 65536 / (THREADS * 128) : 1) : 1;
+};
+
 template <int NQ, int NF, bool DOT, int R, class F, class T>
-__global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF)
+__global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF, (TmaMinBlocks<NQ, NF, F, T>::V))
 ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
               const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
               const T* __restrict__ q, T* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
