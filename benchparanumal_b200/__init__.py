@@ -46,7 +46,7 @@ EXPORTS = [
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
-    "bp_ax_cub_hex3d_f32",
+    "bp_ax_cub_hex3d_f32", "bp_mesh_write_vtu",
 ]
 
 
@@ -173,6 +173,7 @@ def lib():
                                       vp],
             "bp_ax_cub_hex3d_f32": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp,
                                     vp],
+            "bp_mesh_write_vtu": [vp, vp, ctypes.c_char_p],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -328,6 +329,13 @@ class Mesh:
             "invV": Nq * Nq, "MM": Nq * Nq, "cubwJ": ncub, "cubggeo": 6 * ncub,
         }
         return _dl(getattr(c, name), cspec[name], np.float64)
+
+    def write_vtu(self, xL, filename):
+        """bp_mesh_write_vtu: write a host E-vector [E*Np*Nfields] as a VTK XML grid."""
+        a = np.ascontiguousarray(xL, dtype=np.float64)
+        if a.size != self.NL:
+            raise ValueError("xL must hold E*Np*Nfields values")
+        _check(lib().bp_mesh_write_vtu(self._h, a.ctypes.data, str(filename).encode()))
 
     def cubature(self):
         """Set up (once) and return the cubature view of the BP1-BP4 operators."""

@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "bp_internal.hpp"
 
@@ -498,6 +500,82 @@ int bp_mesh_cubature_view(bp_mesh_t m, bp_cubature_view_t* v) {
   v->cubD = m->affine ? m->cubDmodal.ptr : m->cubD.ptr;
   v->invV = m->invV.ptr; v->MM = m->MM.ptr;
   v->cubwJ = m->cubwJ(); v->cubggeo = m->cubggeo();
+  return BP_SUCCESS;
+}
+
+int bp_mesh_write_vtu(bp_mesh_t m, const double* xL, const char* filename) {
+  if (!m || !xL || !filename) return fail(BP_ERROR_ARG, "bp_mesh_write_vtu: null pointer");
+  const int Nq = m->Nq, Np = m->Np, E = m->E, Nf = m->Nfields, N = m->N;
+  std::vector<double> EX((size_t)8 * E), EY((size_t)8 * E), EZ((size_t)8 * E), z(Nq);
+  BP_CUDA_TRY(cudaMemcpy(EX.data(), m->EX.ptr, sizeof(double) * EX.size(), cudaMemcpyDeviceToHost));
+  BP_CUDA_TRY(cudaMemcpy(EY.data(), m->EY.ptr, sizeof(double) * EY.size(), cudaMemcpyDeviceToHost));
+  BP_CUDA_TRY(cudaMemcpy(EZ.data(), m->EZ.ptr, sizeof(double) * EZ.size(), cudaMemcpyDeviceToHost));
+  BP_CUDA_TRY(cudaMemcpy(z.data(), m->gllz.ptr, sizeof(double) * Nq, cudaMemcpyDeviceToHost));
+  FILE* fp = std::fopen(filename, "w");
+  if (!fp) return fail(BP_ERROR, std::string("bp_mesh_write_vtu: cannot open ") + filename);
+  // VTK XML unstructured grid (the reference's mesh_t::PlotFields3D,
+  // libs/mesh/meshPlotFields3D.cpp:31-113): every element's GLL nodes are
+  // points, each sub-cube of the node lattice is cut into six tetrahedra along
+  // its main diagonal
+  const int ncell = 6 * N * N * N;
+  std::fprintf(fp, "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"BigEndian\">\n");
+  std::fprintf(fp, "  <UnstructuredGrid>\n");
+  std::fprintf(fp, "    <Piece NumberOfPoints=\"%d\" NumberOfCells=\"%d\">\n", E * Np, E * ncell);
+  std::fprintf(fp, "      <Points>\n");
+  std::fprintf(fp, "        <DataArray type=\"Float32\" NumberOfComponents=\"3\" Format=\"ascii\">\n");
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < Nq; ++k)
+      for (int j = 0; j < Nq; ++j)
+        for (int i = 0; i < Nq; ++i)
+          std::fprintf(fp, "       %g %g %g\n", trilinear(&EX[8 * (size_t)e], z[i], z[j], z[k]),
+                       trilinear(&EY[8 * (size_t)e], z[i], z[j], z[k]), trilinear(&EZ[8 * (size_t)e], z[i], z[j], z[k]));
+  std::fprintf(fp, "        </DataArray>\n");
+  std::fprintf(fp, "      </Points>\n");
+  std::fprintf(fp, "      <PointData Scalars=\"scalars\">\n");
+  std::fprintf(fp, "        <DataArray type=\"Float32\" Name=\"Fields\" NumberOfComponents=\"%d\" Format=\"ascii\">\n",
+               Nf);
+  for (int e = 0; e < E; ++e)
+    for (int n = 0; n < Np; ++n) {
+      std::fprintf(fp, "       ");
+      for (int f = 0; f < Nf; ++f) std::fprintf(fp, "%g ", xL[((size_t)e * Nf + f) * Np + n]);
+      std::fprintf(fp, "\n");
+    }
+  std::fprintf(fp, "       </DataArray>\n");
+  std::fprintf(fp, "     </PointData>\n");
+  std::fprintf(fp, "    <Cells>\n");
+  std::fprintf(fp, "      <DataArray type=\"Int32\" Name=\"connectivity\" Format=\"ascii\">\n");
+  // the six tetrahedra of a sub-cube: the lattice paths from its low corner to
+  // its high corner, one per order of the three axes; for an odd order the
+  // second and third vertices are swapped so every tetrahedron has positive
+  // orientation in reference coordinates
+  static const int kAxisOrder[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {0, 2, 1}, {1, 0, 2}, {2, 1, 0}};
+  for (int e = 0; e < E; ++e)
+    for (int c = 0; c < N; ++c)
+      for (int b = 0; b < N; ++b)
+        for (int a = 0; a < N; ++a)
+          for (int o = 0; o < 6; ++o) {
+            int off[3] = {a, b, c}, id[4];
+            for (int v = 0; v < 4; ++v) {
+              if (v > 0) off[kAxisOrder[o][v - 1]] += 1;
+              id[v] = e * Np + off[0] + off[1] * Nq + off[2] * Nq * Nq;
+            }
+            if (o >= 3) std::swap(id[1], id[2]);
+            std::fprintf(fp, "       %d %d %d %d \n", id[0], id[1], id[2], id[3]);
+          }
+  std::fprintf(fp, "        </DataArray>\n");
+  std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"offsets\" Format=\"ascii\">\n");
+  for (int c = 1; c <= E * ncell; ++c) std::fprintf(fp, "       %d\n", 4 * c);
+  std::fprintf(fp, "       </DataArray>\n");
+  std::fprintf(fp, "       <DataArray type=\"Int32\" Name=\"types\" Format=\"ascii\">\n");
+  for (int c = 0; c < E * ncell; ++c) std::fprintf(fp, "10\n");
+  std::fprintf(fp, "        </DataArray>\n");
+  std::fprintf(fp, "      </Cells>\n");
+  std::fprintf(fp, "    </Piece>\n");
+  std::fprintf(fp, "  </UnstructuredGrid>\n");
+  std::fprintf(fp, "</VTKFile>\n");
+  const bool ok = std::ferror(fp) == 0;
+  std::fclose(fp);
+  if (!ok) return fail(BP_ERROR, std::string("bp_mesh_write_vtu: write error on ") + filename);
   return BP_SUCCESS;
 }
 

@@ -146,7 +146,7 @@ void add_common(Settings& S, bool bp) {
         {"1", "2", "3", "4", "5", "6", "7", "8", "9", "10", "11", "12", "13", "14", "15"});
   S.add("-a", "--affine", "AFFINE MESH", "FALSE", "Assume elements are affine images of reference element",
         {"TRUE", "FALSE"});
-  if (bp) S.add("-o", "--output", "OUTPUT FILE NAME", "", "");
+  if (bp) S.add("-o", "--output", "OUTPUT FILE NAME", "", "Write the solution to <name>_0000.vtu");
   S.add("-v", "--verbose", "VERBOSE", "FALSE", "Enable verbose output", {"TRUE", "FALSE"});
   // extensions
   S.add("-pc", "--precon", "PRECONDITIONER", "NONE", "CG preconditioner (extension)", {"NONE", "JACOBI"});
@@ -393,6 +393,20 @@ int run_bp(const char* name, int bp, Settings& S) {
               name, S.get("PRECISION").c_str(), S.get("PRECONDITIONER").c_str(), S.get("FORCING").c_str(),
               std::sqrt(st.rdotr), rel, st.updates, st.elapsed_ms);
   std::fflush(stdout);
+  // "-o name": the solution scattered to the local nodes, name_0000.vtu (bp5Run.cpp:220-238)
+  const std::string out = S.get("OUTPUT FILE NAME");
+  if (!out.empty()) {
+    const size_t NL = (size_t)P.view.Nlocal;
+    DevVec xL(NL);
+    check(bp_memset(xL.p, 0, sizeof(double) * NL, nullptr));
+    check(bp_ogs_scatter(N, P.view.rowStarts, P.view.colIds, x.p, xL.p, nullptr));
+    std::vector<double> h(NL);
+    check(bp_memcpy_dtoh(h.data(), xL.p, sizeof(double) * NL, nullptr));
+    check(bp_finish(nullptr));
+    char fname[4096];
+    std::snprintf(fname, sizeof(fname), "%s_%04d.vtu", out.c_str(), 0);
+    check(bp_mesh_write_vtu(P.mesh, h.data(), fname));
+  }
   return BP_SUCCESS;
 }
 

@@ -102,6 +102,14 @@ void box_vertices(HostMesh& m, double pert, uint64_t seed);
 // masked gathered numbering, CSR and GlobalToLocal for the box
 void box_numbering(HostMesh& m);
 
+// trilinear map of the eight hex vertices v (mesh_t vertex order) at (r,s,t)
+__host__ __device__ inline double trilinear(const double* v, double r, double s, double t) {
+  return 0.125 * ((1 - r) * (1 - s) * (1 - t) * v[0] + (1 + r) * (1 - s) * (1 - t) * v[1] +
+                  (1 + r) * (1 + s) * (1 - t) * v[2] + (1 - r) * (1 + s) * (1 - t) * v[3] +
+                  (1 - r) * (1 - s) * (1 + t) * v[4] + (1 + r) * (1 - s) * (1 + t) * v[5] +
+                  (1 + r) * (1 + s) * (1 + t) * v[6] + (1 - r) * (1 + s) * (1 + t) * v[7]);
+}
+
 }  // namespace bp
 
 // ---- the opaque objects of the C ABI ----

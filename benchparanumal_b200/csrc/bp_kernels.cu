@@ -490,13 +490,6 @@ int launch_geometry_at(int Nq, int E, const double* EX, const double* EY, const 
 // ---------------------------------------------------------------------------
 // Forcing (okl/rhsHex3D.okl:29-128) on the fly from the vertex map
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double trilinear(const double* v, double r, double s, double t) {
-  return 0.125 * ((1 - r) * (1 - s) * (1 - t) * v[0] + (1 + r) * (1 - s) * (1 - t) * v[1] +
-                  (1 + r) * (1 + s) * (1 - t) * v[2] + (1 - r) * (1 + s) * (1 - t) * v[3] +
-                  (1 - r) * (1 - s) * (1 + t) * v[4] + (1 + r) * (1 - s) * (1 + t) * v[5] +
-                  (1 + r) * (1 + s) * (1 + t) * v[6] + (1 - r) * (1 + s) * (1 + t) * v[7]);
-}
-
 __global__ void rhs_analytic_kernel(int Nq, int affine, int Nfields, int E, const double* __restrict__ EX,
                                     const double* __restrict__ EY, const double* __restrict__ EZ,
                                     const double* __restrict__ gllz, const double* __restrict__ gllw,

@@ -274,6 +274,12 @@ int bp_box_numbering(const bp_box_desc_t* desc, int32_t* Ngather, int32_t* nnz, 
 int bp_basis_gll(int32_t N, double* z, double* w, double* D);
 int bp_box_vertices(const bp_box_desc_t* desc, double* EX, double* EY, double* EZ);
 int bp_mesh_view(bp_mesh_t mesh, bp_mesh_view_t* view);
+/* Write a host E-vector xL [E*Np*Nfields] (e.g. the solution scattered to the
+   local nodes) as a VTK XML unstructured grid (ASCII) of the element nodes and
+   six tetrahedra per node sub-cube: mesh_t::PlotFields3D
+   (libs/mesh/meshPlotFields3D.cpp:31-113), used by the "-o" output of the BP
+   drivers (BP/BP5/src/bp5Run.cpp:220-238). */
+int bp_mesh_write_vtu(bp_mesh_t mesh, const double* xL, const char* filename);
 int bp_mesh_destroy(bp_mesh_t mesh);
 
 /* ---------------------------------------------------------------------------
