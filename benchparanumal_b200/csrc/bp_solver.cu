@@ -150,31 +150,54 @@ cg_direction_kernel(int32_t N, V* __restrict__ x, V* __restrict__ p, const V* __
   }
 }
 
-// p.Ap from the element operator's block partials (index order), then alpha
-constexpr int kAlphaThreads = 1024;
-__global__ void __launch_bounds__(kAlphaThreads)
-cg_alpha_kernel(int nparts, const double* __restrict__ parts, CgScalars* sc, double* hist_alpha) {
-  if (sc->done) return;
-  __shared__ double s_w[kAlphaThreads / 32];
-  double acc = 0.0;
-  for (int k = threadIdx.x; k < nparts; k += kAlphaThreads) acc += parts[k];
-  acc = warp_sum_cg(acc);
-  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double pAp = 0.0;
-    for (int w = 0; w < kAlphaThreads / 32; ++w) pAp += s_w[w];
-    const double rho = sc->precon ? sc->rz : sc->rdotr;
-    const double alpha = rho / pAp;
-    sc->pAp = pAp;
-    if (!(pAp > 0.0) || !isfinite(alpha)) {
-      sc->breakdown = 1;
-      sc->done = 1;
-    } else {
-      sc->alpha = alpha;
-      if (hist_alpha) hist_alpha[sc->iter] = alpha;
+// p.Ap of lanes sc[0..NL-1] from the element operator's per-lane block
+// partials (parts[l * nparts + k]), then alpha.  Each block sums a strided
+// share of the partials, the last block to arrive adds the block sums in slot
+// order (grid_sum_cg), so the sum is reproducible; one block over 64000
+// partials per lane took 36 us, most of a small problem's iteration.
+template <int NL>
+__global__ void __launch_bounds__(kThreads)
+cg_alpha_kernel(int nparts, const double* __restrict__ parts, CgScalars* sc, double* hist_alpha, double* partials,
+                unsigned int* counter) {
+  bool act[NL];
+  bool any = false;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    act[l] = !sc[l].done;   // every block reads sc before the last block changes it
+    any = any || act[l];
+  }
+  if (!any) return;   // grid-uniform
+  double acc[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) acc[l] = 0.0;
+  for (int k = blockIdx.x * kThreads + threadIdx.x; k < nparts; k += kThreads * gridDim.x)
+#pragma unroll
+    for (int l = 0; l < NL; ++l) acc[l] += parts[(size_t)l * nparts + k];
+  double tot[NL];
+  if (grid_sum_cg<NL>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    for (int l = 0; l < NL; ++l) {
+      if (!act[l]) continue;
+      CgScalars& c = sc[l];
+      const double pAp = tot[l];
+      const double rho = c.precon ? c.rz : c.rdotr;
+      const double alpha = rho / pAp;
+      c.pAp = pAp;
+      if (!(pAp > 0.0) || !isfinite(alpha)) {
+        c.breakdown = 1;
+        c.done = 1;
+      } else {
+        c.alpha = alpha;
+        if (hist_alpha) hist_alpha[c.iter] = alpha;
+      }
     }
   }
+}
+
+// blocks of cg_alpha_kernel: about four partials per thread
+static int alpha_grid(int nparts) {
+  int g = (nparts + 4 * kThreads - 1) / (4 * kThreads);
+  if (g > reduction_blocks()) g = reduction_blocks();
+  return g < 1 ? 1 : g;
 }
 
 // One row per thread: r and invD of the row are requested first, then the
@@ -331,39 +354,6 @@ grp_direction_kernel(int32_t N, Pack<float, PK>* __restrict__ x, Pack<float, PK>
     }
     x[n] = xn;
     p[n] = pn;
-  }
-}
-
-// p.Ap of every active lane from the operator's per-lane block partials, then alpha
-template <int PK>
-__global__ void __launch_bounds__(kAlphaThreads)
-grp_alpha_kernel(int nparts, const double* __restrict__ parts, CgScalars* sc) {
-  __shared__ double s_w[kAlphaThreads / 32];
-  __shared__ int s_act[PK];
-  if (threadIdx.x < PK) s_act[threadIdx.x] = !sc[threadIdx.x].done;
-  __syncthreads();
-  for (int l = 0; l < PK; ++l) {
-    if (!s_act[l]) continue;   // block-uniform
-    double acc = 0.0;
-    for (int k = threadIdx.x; k < nparts; k += kAlphaThreads) acc += parts[(size_t)l * nparts + k];
-    acc = warp_sum_cg(acc);
-    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double pAp = 0.0;
-      for (int w = 0; w < kAlphaThreads / 32; ++w) pAp += s_w[w];
-      CgScalars& c = sc[l];
-      const double rho = c.precon ? c.rz : c.rdotr;
-      const double alpha = rho / pAp;
-      c.pAp = pAp;
-      if (!(pAp > 0.0) || !isfinite(alpha)) {
-        c.breakdown = 1;
-        c.done = 1;
-      } else {
-        c.alpha = alpha;
-      }
-    }
-    __syncthreads();
   }
 }
 
@@ -585,7 +575,8 @@ static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* 
   const CgFuse fuse{S->fuse_partials.ptr};
   int nparts = 0;
   BP_TRY(elem_apply<V>(S, o, p, AqL, &S->scal->done, s, &fuse, &nparts));
-  cg_alpha_kernel<<<1, kAlphaThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->scal, hist_alpha);
+  cg_alpha_kernel<1><<<alpha_grid(nparts), kThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->scal, hist_alpha,
+                                                              S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   cg_gather_update_kernel<V><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr, AqL, r, invD, S->scal,
                                                     hist_rnorm, S->partials.ptr, S->counter.ptr);
@@ -1035,7 +1026,8 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
     rc = launch_ax_line_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
                                (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
   BP_TRY(rc);
-  grp_alpha_kernel<PK><<<1, kAlphaThreads, 0, s>>>(nparts, G->parts.ptr, G->sc);
+  cg_alpha_kernel<PK><<<alpha_grid(nparts), kThreads, 0, s>>>(nparts, G->parts.ptr, G->sc, nullptr, G->gparts.ptr,
+                                                               G->gcount.ptr);
   BP_CUDA_TRY(cudaGetLastError());
   grp_gather_update_kernel<PK><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr,
                                                       reinterpret_cast<const T*>(G->AqL32.ptr),
