@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "bp_cg_device.cuh"
@@ -952,11 +953,11 @@ int bp_solver_solve_host(bp_solver_t S, const double* b_host, double* x_host, do
 // pair is a CG system on its problem's mesh.  In a mixed-precision BP5 batch
 // the right-hand sides of a problem (degree up to 11) are solved in lockstep as
 // packed groups of 2 or 4 lanes (padding lanes carry b = 0 and finish at once);
-// a single right-hand side and the other cases are standalone systems.  One CUDA graph holds 20 iterations of every group and
-// standalone system, spread over kBranches parallel branches (fork/join
-// events), so problems of different degree and size run side by side; finished
-// systems skip their kernels through their device flags.  Between graph
-// launches the host applies the reliable updates the systems ask for.
+// a single right-hand side and the other cases are standalone systems.  Each
+// group or standalone system (a unit) has a CUDA graph of kChunk iterations
+// and runs on one stream of a pool; the host drives every unit on its own
+// (reliable updates, next chunk, retirement) as its scalars arrive, so no unit
+// waits for another.
 // ---------------------------------------------------------------------------
 struct CgGroup {
   int pk = 0;                                   // lanes
@@ -969,23 +970,39 @@ struct CgGroup {
   std::vector<double*> x, r, b;                 // per lane FP64 vectors
 };
 
+// A unit of a batch: one packed group, or one standalone system.  Each unit
+// has its own graph of kChunk iterations and is driven independently.
+struct BatchUnit {
+  CgGroup* G = nullptr;
+  int sys = -1;                  // the standalone system (G == nullptr)
+  int slot0 = 0, lanes = 1;      // its CG scalar slots
+  double weight = 0.0;           // lane-nodes of element data per iteration
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t posted = nullptr;  // the host copy of its scalars has landed
+  int stream = -1;               // stream of the pool while in flight
+};
+
 struct bp_batch_s {
   std::vector<bp_mesh_s*> meshes;             // owned
   std::vector<bp_solver_s*> owned;            // owned solvers (standalone systems and group bases)
   std::vector<CgGroup*> groups;               // owned
   std::vector<bp_solver_s*> sys_solver;       // per system: its solver (a group's base for grouped systems)
   std::vector<int> sys_prob, sys_group, sys_lane, sys_slot;
-  std::vector<int> group_branch, sys_branch;  // branch of each group / standalone system
+  std::vector<BatchUnit> units;
   std::vector<DeviceArray<double>*> x, r, b;  // per system (owned)
   std::vector<DeviceArray<double>*> pad;      // padding lanes' x, r, b (owned)
   DeviceArray<CgScalars> sc;                  // every slot's CG scalars, one array
+  CgScalars* host_sc = nullptr;               // pinned host copy of sc
   int mixed = 0;
-  std::vector<cudaStream_t> branches;
+  std::vector<cudaStream_t> branches;         // the stream pool
   std::vector<cudaEvent_t> joins;
   cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-  cudaGraphExec_t graph = nullptr;
   ~bp_batch_s() {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& u : units) {
+      if (u.graph) cudaGraphExecDestroy(u.graph);
+      if (u.posted) cudaEventDestroy(u.posted);
+    }
+    if (host_sc) cudaFreeHost(host_sc);
     for (auto* G : groups) delete G;
     for (auto* S : owned) delete S;
     for (auto* m : meshes) bp_mesh_destroy(m);
@@ -1003,6 +1020,10 @@ struct bp_batch_s {
 
 namespace bp {
 
+// Streams of a batch's pool: units in flight at once.  Sixteen units side by
+// side, each driven on its own, took 64 uneven problems from 9.1 s (one graph
+// of all units with a host barrier after every chunk) to 7.1 s; 8 or 32
+// streams, largest or smallest unit first, all gave 7.1 s.
 constexpr int kBranches = 16;
 
 // one packed iteration of a group: direction, operator with per-lane p.Ap
@@ -1066,29 +1087,30 @@ static int grp_reliable(CgGroup* G, int l, double tol, int maxit, cudaStream_t s
   return grp_replace(G, l, false, tol, maxit, s);
 }
 
-// Balance the branches: groups and standalone systems, largest first, each to
-// the branch with the least work so far (work ~ unknowns x lanes per iteration)
-static void batch_assign_branches(bp_batch_s* B) {
-  const int nb = (int)B->branches.size();
-  struct Item { double cost; int group, sys; };
-  std::vector<Item> items;
-  for (size_t gi = 0; gi < B->groups.size(); ++gi)
-    items.push_back({(double)B->groups[gi]->base->N * B->groups[gi]->pk, (int)gi, -1});
-  for (size_t i = 0; i < B->sys_solver.size(); ++i)
-    if (B->sys_group[i] < 0) items.push_back({(double)B->sys_solver[i]->N, -1, (int)i});
-  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
-  std::vector<double> load(nb, 0.0);
-  B->group_branch.assign(B->groups.size(), 0);
-  B->sys_branch.assign(B->sys_solver.size(), 0);
-  for (const Item& it : items) {
-    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-    load[k] += it.cost;
-    if (it.group >= 0) B->group_branch[it.group] = k;
-    else B->sys_branch[it.sys] = k;
+// Units of the batch with their scalar slots and weights
+static int batch_units(bp_batch_s* B) {
+  for (auto* G : B->groups) {
+    BatchUnit u;
+    u.G = G;
+    u.slot0 = (int)(G->sc - B->sc.ptr);
+    u.lanes = G->pk;
+    u.weight = (double)G->base->mesh->E * G->base->mesh->Np * G->pk;
+    B->units.push_back(u);
   }
+  for (size_t i = 0; i < B->sys_solver.size(); ++i) {
+    if (B->sys_group[i] >= 0) continue;
+    BatchUnit u;
+    u.sys = (int)i;
+    u.slot0 = B->sys_slot[i];
+    const bp_mesh_s* m = B->sys_solver[i]->mesh;
+    u.weight = (double)m->E * m->Np;
+    B->units.push_back(u);
+  }
+  for (auto& u : B->units) BP_CUDA_TRY(cudaEventCreateWithFlags(&u.posted, cudaEventDisableTiming));
+  return BP_SUCCESS;
 }
 
-// fork the branches off s (their work follows) and join them back
+// fork the stream pool off s (their work follows) and join it back
 static int batch_fork(bp_batch_s* B, cudaStream_t s) {
   BP_CUDA_TRY(cudaEventRecord(B->fork, s));
   for (auto st : B->branches) BP_CUDA_TRY(cudaStreamWaitEvent(st, B->fork, 0));
@@ -1102,127 +1124,158 @@ static int batch_join(bp_batch_s* B, cudaStream_t s) {
   return BP_SUCCESS;
 }
 
-static int batch_capture(bp_batch_s* B, cudaStream_t s) {
-  if (B->graph) return BP_SUCCESS;
+// kChunk iterations of one unit as a graph
+static int unit_capture(bp_batch_s* B, BatchUnit& u, cudaStream_t s) {
+  if (u.graph) return BP_SUCCESS;
   cudaGraph_t g;
   BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  int rc = batch_fork(B, s);
-  cudaError_t ce = cudaSuccess;
-  for (size_t gi = 0; gi < B->groups.size() && rc == BP_SUCCESS; ++gi)
-    for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k)
-      rc = grp_body(B->groups[gi], B->branches[B->group_branch[gi]]);
-  for (size_t i = 0; i < B->sys_solver.size() && rc == BP_SUCCESS; ++i) {
-    if (B->sys_group[i] >= 0) continue;
-    cudaStream_t bs = B->branches[B->sys_branch[i]];
-    bp_solver_s* S = B->sys_solver[i];
-    for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k)
-      rc = B->mixed ? body32(S, nullptr, nullptr, bs) : body64(S, B->x[i]->ptr, B->r[i]->ptr, bs);
+  int rc = BP_SUCCESS;
+  for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k) {
+    if (u.G) {
+      rc = grp_body(u.G, s);
+    } else {
+      bp_solver_s* S = B->sys_solver[u.sys];
+      rc = B->mixed ? body32(S, nullptr, nullptr, s) : body64(S, B->x[u.sys]->ptr, B->r[u.sys]->ptr, s);
+    }
   }
-  if (rc == BP_SUCCESS) rc = batch_join(B, s);
-  cudaError_t ce2 = cudaStreamEndCapture(s, &g);
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
   if (rc != BP_SUCCESS) return rc;
   BP_CUDA_TRY(ce);
-  BP_CUDA_TRY(ce2);
-  ce = cudaGraphInstantiate(&B->graph, g, 0);
+  ce = cudaGraphInstantiate(&u.graph, g, 0);
   cudaGraphDestroy(g);
   BP_CUDA_TRY(ce);
   return BP_SUCCESS;
 }
 
-static int batch_read(bp_batch_s* B, std::vector<CgScalars>& h, cudaStream_t s) {
-  h.resize(B->sc.n);
-  BP_CUDA_TRY(cudaMemcpyAsync(h.data(), B->sc.ptr, sizeof(CgScalars) * h.size(), cudaMemcpyDeviceToHost, s));
-  BP_CUDA_TRY(cudaStreamSynchronize(s));
+// start of a unit's solve: x = 0, r = b, the initial residuals
+static int unit_start(bp_batch_s* B, BatchUnit& u, double tol, int maxit, cudaStream_t s) {
+  if (u.G) {
+    CgGroup* G = u.G;
+    const size_t bytes = sizeof(double) * G->base->N;
+    for (int l = 0; l < G->pk; ++l) {
+      BP_CUDA_TRY(cudaMemsetAsync(G->x[l], 0, bytes, s));
+      BP_CUDA_TRY(cudaMemcpyAsync(G->r[l], G->b[l], bytes, cudaMemcpyDeviceToDevice, s));
+    }
+    BP_CUDA_TRY(cudaMemsetAsync(G->x32.ptr, 0, sizeof(float) * G->x32.n, s));
+    BP_CUDA_TRY(cudaMemsetAsync(G->p32.ptr, 0, sizeof(float) * G->p32.n, s));
+    for (int l = 0; l < G->pk; ++l) BP_TRY(grp_replace(G, l, true, tol, maxit, s));
+    return BP_SUCCESS;
+  }
+  const int i = u.sys;
+  bp_solver_s* S = B->sys_solver[i];
+  const size_t bytes = sizeof(double) * S->N;
+  BP_CUDA_TRY(cudaMemsetAsync(B->x[i]->ptr, 0, bytes, s));
+  BP_CUDA_TRY(cudaMemcpyAsync(B->r[i]->ptr, B->b[i]->ptr, bytes, cudaMemcpyDeviceToDevice, s));
+  if (B->mixed) return mixed_begin(S, B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s);
+  BP_TRY(operator_apply(S, B->x[i]->ptr, S->Ap.ptr, nullptr, s));
+  S->launches += 1;
+  cg_init_kernel<<<vec_grid(S->N), kThreads, 0, s>>>(S->N, S->Ap.ptr, B->r[i]->ptr, S->invD.ptr, S->scal, tol, maxit,
+                                                      S->precon, S->partials.ptr, S->counter.ptr);
+  BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
+// copy the unit's scalars to the pinned host array, then mark the copy
+static int unit_post(bp_batch_s* B, BatchUnit& u, cudaStream_t s) {
+  BP_CUDA_TRY(cudaMemcpyAsync(B->host_sc + u.slot0, B->sc.ptr + u.slot0, sizeof(CgScalars) * u.lanes,
+                              cudaMemcpyDeviceToHost, s));
+  BP_CUDA_TRY(cudaEventRecord(u.posted, s));
+  return BP_SUCCESS;
+}
+
+// Every unit runs on a stream of the pool, driven by the host without a
+// global barrier: when a unit's scalars land, the host applies the reliable
+// updates of its lanes, launches its next chunk, or retires it and admits the
+// next unit (largest first).
 static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* stats, double* elapsed_ms) {
   cudaStream_t s = default_stream();
   const size_t ns = B->sys_solver.size();
   if (B->mixed && !(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_batch_solve: a mixed-precision batch needs tol > 0");
-  BP_TRY(batch_capture(B, s));
+  for (auto& u : B->units) BP_TRY(unit_capture(B, u, s));
   std::vector<int> updates(B->sc.n, 0);
   for (auto* S : B->owned) S->launches = 0;
   BP_CUDA_TRY(cudaEventRecord(B->ev0, s));
-  // x = 0, r = b, and every system's start
-  for (size_t i = 0; i < ns; ++i) {
-    const size_t bytes = sizeof(double) * B->sys_solver[i]->N;
-    BP_CUDA_TRY(cudaMemsetAsync(B->x[i]->ptr, 0, bytes, s));
-    BP_CUDA_TRY(cudaMemcpyAsync(B->r[i]->ptr, B->b[i]->ptr, bytes, cudaMemcpyDeviceToDevice, s));
-  }
-  for (auto* G : B->groups) {
-    BP_CUDA_TRY(cudaMemsetAsync(G->x32.ptr, 0, sizeof(float) * G->x32.n, s));
-    BP_CUDA_TRY(cudaMemsetAsync(G->p32.ptr, 0, sizeof(float) * G->p32.n, s));
-    for (int l = 0; l < G->pk; ++l) BP_TRY(grp_replace(G, l, true, tol, maxit, s));
-  }
-  for (size_t i = 0; i < ns; ++i) {
-    if (B->sys_group[i] >= 0) continue;
-    bp_solver_s* S = B->sys_solver[i];
-    if (B->mixed) {
-      BP_TRY(mixed_begin(S, B->x[i]->ptr, B->r[i]->ptr, tol, maxit, s));
-    } else {
-      BP_TRY(operator_apply(S, B->x[i]->ptr, S->Ap.ptr, nullptr, s));
-      S->launches += 1;
-      cg_init_kernel<<<vec_grid(S->N), kThreads, 0, s>>>(S->N, S->Ap.ptr, B->r[i]->ptr, S->invD.ptr, S->scal, tol,
-                                                          maxit, S->precon, S->partials.ptr, S->counter.ptr);
-      BP_CUDA_TRY(cudaGetLastError());
-    }
-  }
-  std::vector<CgScalars> h;
-  BP_TRY(batch_read(B, h, s));
-  for (;;) {
-    // reliable updates, each on its unit's branch (the units are independent)
-    bool running = false, updated = false;
-    BP_TRY(batch_fork(B, s));
-    for (size_t gi = 0; gi < B->groups.size(); ++gi) {
-      CgGroup* G = B->groups[gi];
-      const int slot0 = (int)(G->sc - B->sc.ptr);
-      for (int l = 0; l < G->pk; ++l) {
-        const CgScalars& c = h[slot0 + l];
+  BP_TRY(batch_fork(B, s));
+  const int nu = (int)B->units.size();
+  std::vector<int> order(nu);
+  for (int k = 0; k < nu; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return B->units[a].weight > B->units[b].weight; });
+  std::vector<int> free_streams;
+  for (int k = (int)B->branches.size() - 1; k >= 0; --k) free_streams.push_back(k);
+  std::vector<int> inflight;
+  int next = 0;   // order[next..]: not started
+  auto admit = [&](int ui) -> int {
+    BatchUnit& u = B->units[ui];
+    u.stream = free_streams.back();
+    free_streams.pop_back();
+    const cudaStream_t st = B->branches[u.stream];
+    BP_TRY(unit_start(B, u, tol, maxit, st));
+    BP_TRY(unit_post(B, u, st));
+    inflight.push_back(ui);
+    return BP_SUCCESS;
+  };
+  auto fill = [&]() -> int {
+    while (next < nu && !free_streams.empty()) BP_TRY(admit(order[next++]));
+    return BP_SUCCESS;
+  };
+  BP_TRY(fill());
+  while (!inflight.empty()) {
+    bool progressed = false;
+    for (size_t a = 0; a < inflight.size();) {
+      BatchUnit& u = B->units[inflight[a]];
+      const cudaError_t q = cudaEventQuery(u.posted);
+      if (q == cudaErrorNotReady) {
+        ++a;
+        continue;
+      }
+      BP_CUDA_TRY(q);
+      progressed = true;
+      const cudaStream_t st = B->branches[u.stream];
+      bool running = false, updated = false;
+      for (int l = 0; l < u.lanes; ++l) {
+        const CgScalars& c = B->host_sc[u.slot0 + l];
         if (c.breakdown) continue;
-        if (c.update) {
-          BP_TRY(grp_reliable(G, l, tol, maxit, B->branches[B->group_branch[gi]]));
-          ++updates[slot0 + l];
+        if (B->mixed && c.update) {
+          if (u.G) BP_TRY(grp_reliable(u.G, l, tol, maxit, st));
+          else BP_TRY(mixed_reliable(B->sys_solver[u.sys], B->x[u.sys]->ptr, B->r[u.sys]->ptr, tol, maxit, st));
+          ++updates[u.slot0 + l];
           updated = true;
         } else if (!c.done) {
           running = true;
         }
       }
-    }
-    for (size_t i = 0; i < ns; ++i) {
-      if (B->sys_group[i] >= 0) continue;
-      const CgScalars& c = h[B->sys_slot[i]];
-      if (c.breakdown) continue;
-      if (B->mixed && c.update) {
-        BP_TRY(mixed_reliable(B->sys_solver[i], B->x[i]->ptr, B->r[i]->ptr, tol, maxit,
-                              B->branches[B->sys_branch[i]]));
-        ++updates[B->sys_slot[i]];
-        updated = true;
-      } else if (!c.done) {
-        running = true;
+      if (updated) {   // the updated lanes may have converged or resume
+        BP_TRY(unit_post(B, u, st));
+        ++a;
+        continue;
       }
+      if (running) {
+        BP_CUDA_TRY(cudaGraphLaunch(u.graph, st));
+        (u.G ? u.G->base : B->sys_solver[u.sys])->launches += 4 * kChunk;
+        BP_TRY(unit_post(B, u, st));
+        ++a;
+        continue;
+      }
+      // retired: its stream goes back to the pool (stream order keeps its tail first)
+      if (!B->mixed && !u.G) {
+        bp_solver_s* S = B->sys_solver[u.sys];
+        S->launches += 1;
+        cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, st>>>(S->N, B->x[u.sys]->ptr, S->p.ptr, S->scal);
+        BP_CUDA_TRY(cudaGetLastError());
+      }
+      free_streams.push_back(u.stream);
+      u.stream = -1;
+      inflight.erase(inflight.begin() + (long)a);
+      BP_TRY(fill());
     }
-    BP_TRY(batch_join(B, s));
-    if (updated) {   // the updated systems may have converged or resumed
-      BP_TRY(batch_read(B, h, s));
-      continue;
-    }
-    if (!running) break;
-    BP_CUDA_TRY(cudaGraphLaunch(B->graph, s));
-    for (auto* G : B->groups) G->base->launches += 4 * kChunk;
-    for (size_t i = 0; i < ns; ++i)
-      if (B->sys_group[i] < 0) B->sys_solver[i]->launches += 4 * kChunk;
-    BP_TRY(batch_read(B, h, s));
+    if (!progressed) std::this_thread::yield();
   }
-  if (!B->mixed)
-    for (size_t i = 0; i < ns; ++i) {
-      bp_solver_s* S = B->sys_solver[i];
-      S->launches += 1;
-      cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, s>>>(S->N, B->x[i]->ptr, S->p.ptr, S->scal);
-      BP_CUDA_TRY(cudaGetLastError());
-    }
+  BP_TRY(batch_join(B, s));
   BP_CUDA_TRY(cudaEventRecord(B->ev1, s));
-  BP_TRY(batch_read(B, h, s));
+  BP_CUDA_TRY(cudaMemcpyAsync(B->host_sc, B->sc.ptr, sizeof(CgScalars) * B->sc.n, cudaMemcpyDeviceToHost, s));
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  const CgScalars* h = B->host_sc;
   float ms = 0.f;
   BP_CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
   if (elapsed_ms) *elapsed_ms = ms;
@@ -1374,8 +1427,12 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
       if (rc != BP_SUCCESS) break;
       slot += u.pk ? u.pk : 1;
     }
+    if (rc == BP_SUCCESS) rc = batch_units(B);
     if (rc == BP_SUCCESS) {
-      batch_assign_branches(B);
+      ce = cudaMallocHost(reinterpret_cast<void**>(&B->host_sc), sizeof(CgScalars) * B->sc.n);
+      if (ce != cudaSuccess) rc = cuda_fail(ce, "bp_batch_create", __FILE__, __LINE__);
+    }
+    if (rc == BP_SUCCESS) {
       cudaError_t ce2 = cudaStreamSynchronize(s);
       if (ce2 != cudaSuccess) rc = cuda_fail(ce2, "bp_batch_create", __FILE__, __LINE__);
     }
