@@ -56,17 +56,25 @@ struct LineShape {
   static constexpr int EPB0 = 256 / G2 < 1 ? 1 : 256 / G2;
   static constexpr int EPB = EPB0 > 8 ? 8 : EPB0;
   static constexpr int THREADS = G2 * EPB;
-  static constexpr int MINB = NQ <= 11 ? 2 : 1;
   static constexpr int SLOT = line_slot(NQ);
   template <class T>
   static constexpr size_t smem() { return sizeof(T) * (size_t)3 * FIELD * EPB; }
+};
+
+// Blocks per SM the registers are sized for: two up to NQ = 11, except four
+// packed lanes at NQ >= 10, whose 3 x 16-byte fields of about 250 nodes per
+// block leave room for one block per SM anyway; there the kernel may take all
+// the registers it needs (NQ = 11: 936 bytes of spills at 128 registers).
+template <int NQ, class T>
+struct LineMinBlocks {
+  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 10) ? 1 : (NQ <= 11 ? 2 : 1);
 };
 
 // T: the value type of q and Aq, LineReal or Pack<LineReal, PK> (PK right-hand
 // sides of one mesh in lockstep, one pack per node); p.Ap partials per lane at
 // partials[lane * gridDim.x + blockIdx.x].
 template <int NQ, bool AFFINE, class T>
-__global__ void __launch_bounds__(LineShape<NQ>::THREADS, LineShape<NQ>::MINB)
+__global__ void __launch_bounds__(LineShape<NQ>::THREADS, (LineMinBlocks<NQ, T>::V))
 ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
                const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
                const LineReal* __restrict__ gllw, LineReal lambda, const T* __restrict__ q,

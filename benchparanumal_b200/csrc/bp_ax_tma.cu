@@ -131,13 +131,20 @@ struct TmaSmem {
 // or Pack<F, PK> for PK right-hand sides of one mesh in lockstep (then NF = 1
 // and the q/Aq arrays hold one pack per node).  p.Ap partials are summed in
 // double, one per lane: fuse.partials[lane * gridDim.x + blockIdx.x].
-// Packed values need about 128 registers a thread; the second launch bound
-// caps them there, so 65536 / (threads * 128) blocks stay resident (NQ=8: 8
-// blocks of 64 threads instead of 6 at 133 registers, 4 bytes of spills).
+// Packed values: a thread holds 2*NQ packs of R values (its pencil of q and
+// of A q) and two rows of D, about REGS = max(128, 2*NQ*R + 2*NQ + 40)
+// registers.  The second launch bound caps them there, so 65536 / (REGS *
+// threads rounded up to whole warps) blocks stay resident (NQ=8, R=4: 8 blocks
+// of 64 threads instead of 6 at 133 registers, 4 bytes of spills; NQ=10, R=4:
+// 3 blocks without spills instead of 5 at 96 registers with 1.5 KB).
 template <int NQ, int NF, class F, class T>
 struct TmaMinBlocks {
   static constexpr int THREADS = NQ * NQ * TmaShape<NQ, F>::EPB * NF;
-  static constexpr int V = (PackTraits<T>::R > 1) ? (65536 / (THREADS * 128) > 0 ? 65536 / (THREADS * 128) : 1) : 1;
+  static constexpr int ALLOC = (THREADS + 31) / 32 * 32;
+  static constexpr int R = PackTraits<T>::R;
+  static constexpr int WANT = 2 * NQ * R + 2 * NQ + 40;
+  static constexpr int REGS = WANT > 128 ? WANT : 128;
+  static constexpr int V = R > 1 ? (65536 / (ALLOC * REGS) > 0 ? 65536 / (ALLOC * REGS) : 1) : 1;
 };
 
 template <int NQ, int NF, bool DOT, int R, class F, class T>

@@ -1337,9 +1337,11 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
     for (int j = 0; j < nproblems; ++j) {
       const bp_batch_problem_t& P = problems[j];
       const bool packable = B->mixed && d->bp == 5 && P.N + 1 <= 12;
-      // four lanes where the packed operator keeps its registers (TMA form at even
-      // Nq; line form up to Nq = 8), two above
-      const int maxpk = ((P.N + 1) % 2 == 0 || P.N + 1 <= 8) ? 4 : 2;
+      // four lanes, except at Nq = 9, where the four-lane line kernel's two
+      // 105 KB blocks per SM share the GPU badly with the other problems of a
+      // batch (64 uneven problems: 6.64 s; four lanes everywhere 6.87 s; two at
+      // Nq 9 and 11 as well 6.72 s)
+      const int maxpk = P.N + 1 == 9 ? 2 : 4;
       for (int k = 0; k < P.nrhs;) {
         const int left = P.nrhs - k;
         const int pk = !packable || left == 1 ? 0 : (left == 2 ? 2 : maxpk);

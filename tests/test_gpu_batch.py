@@ -13,9 +13,10 @@ PROBLEMS = [
     {"nx": 3, "N": 10, "pert": 0.1, "pert_seed": 103, "nrhs": 3, "rhs_seed": 1006},
     {"nx": 2, "N": 7, "pert": 0.1, "pert_seed": 104, "nrhs": 4, "rhs_seed": 1009},
 ]
-# In a mixed batch the right-hand sides of even-Nq problems run as packed
-# groups: problem 0 as two lanes, problem 1 as four lanes with one idle, problem
-# 4 as four lanes; the others are standalone systems.
+# In a mixed batch the right-hand sides of a problem run as packed groups:
+# problem 0 as two lanes, problems 1 and 3 as four lanes with one idle,
+# problem 4 as four lanes; problem 2 (one right-hand side) is a standalone
+# system.
 
 
 def _rel(a, b):

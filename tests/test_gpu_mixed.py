@@ -65,7 +65,8 @@ def test_mixed_host_entry_matches_device_entry(gpu):
     np.testing.assert_array_equal(xh, x.download())
 
 
-@pytest.mark.parametrize("N,nrhs", [(7, 4), (7, 2), (4, 4), (6, 2), (9, 2), (3, 4)])
+@pytest.mark.parametrize("N,nrhs", [(7, 4), (7, 2), (4, 4), (6, 2), (9, 2), (3, 4), (8, 4), (9, 4), (10, 4),
+                                    (11, 4), (5, 4)])
 def test_fp32_multi_rhs_operator_matches_single(gpu, oracle, N, nrhs):
     # the packed operator (TMA form at even Nq, line form at odd Nq) gives each
     # right-hand side what the single-rhs FP32 operator gives it, and both are
