@@ -438,6 +438,29 @@ static int vec_grid(int32_t N) {
   return g < 1 ? 1 : g;
 }
 
+// Grid of a grid-stride kernel that needs more registers than eight resident
+// blocks of kThreads allow: the blocks resident at once (one wave; a fixed
+// count per kernel and device, so its reductions stay reproducible).  The
+// four-lane gather at 48 registers keeps 5 blocks per SM: 1184 blocks ran as
+// 1.6 waves.
+static int vec_grid_wave(const void* kernel, int32_t N) {
+  static std::vector<std::pair<const void*, int>> cache;
+  int wave = 0;
+  for (const auto& c : cache)
+    if (c.first == kernel) wave = c.second;
+  if (wave == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess)
+      per_sm = 0;
+    wave = per_sm > 0 && sms > 0 ? std::min(per_sm * sms, reduction_blocks()) : reduction_blocks();
+    cache.push_back({kernel, wave});
+  }
+  int g = (N + kThreads - 1) / kThreads;
+  if (g > wave) g = wave;
+  return g < 1 ? 1 : g;
+}
+
 int launch_d2f(size_t n, const double* a, float* b, cudaStream_t s) {
   if (n == 0) return BP_SUCCESS;
   size_t g = (n + 255) / 256;
@@ -1033,8 +1056,8 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   bp_solver_s* S = G->base;
   bp_mesh_s* m = S->mesh;
   const int32_t N = S->N;
-  const int g = vec_grid(N);
   using T = Pack<float, PK>;
+  const int g = vec_grid_wave(reinterpret_cast<const void*>(&grp_direction_kernel<PK>), N);
   grp_direction_kernel<PK><<<g, kThreads, 0, s>>>(N, reinterpret_cast<T*>(G->x32.ptr), reinterpret_cast<T*>(G->p32.ptr),
                                                   reinterpret_cast<const T*>(G->r32.ptr), S->invD32.ptr, G->sc);
   BP_CUDA_TRY(cudaGetLastError());
@@ -1050,7 +1073,8 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   cg_alpha_kernel<PK><<<alpha_grid(nparts), kThreads, 0, s>>>(nparts, G->parts.ptr, G->sc, nullptr, G->gparts.ptr,
                                                                G->gcount.ptr);
   BP_CUDA_TRY(cudaGetLastError());
-  grp_gather_update_kernel<PK><<<g, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr,
+  const int gg = vec_grid_wave(reinterpret_cast<const void*>(&grp_gather_update_kernel<PK>), N);
+  grp_gather_update_kernel<PK><<<gg, kThreads, 0, s>>>(N, m->rowStarts.ptr, m->colIds.ptr,
                                                       reinterpret_cast<const T*>(G->AqL32.ptr),
                                                       reinterpret_cast<T*>(G->r32.ptr), S->invD32.ptr, G->sc,
                                                       G->gparts.ptr, G->gcount.ptr);
