@@ -367,20 +367,26 @@ int bp_mesh_create(const bp_box_desc_t* d, bp_mesh_t* out) {
   gll_nodes_weights(hm.N, hm.gllz, hm.gllw);
   diff_matrix(hm.gllz, hm.D);
   box_vertices(hm, d->pert, d->pert_seed);
-  box_numbering(hm);
+  int64_t ngather = 0, nnz = 0;
+  box_numbering_counts(hm.nx, hm.ny, hm.nz, hm.N, hm.Nfields, &ngather, &nnz);
 
   bp_mesh_s* m = new bp_mesh_s();
   m->N = hm.N; m->Nq = Nq; m->Np = Np; m->E = hm.E; m->Nfields = hm.Nfields; m->affine = hm.affine;
-  m->Ngather = hm.Ngather; m->nnz = hm.nnz;
+  m->Ngather = (int32_t)ngather; m->nnz = (int32_t)nnz;
   std::vector<int32_t> elist(hm.E);
   for (int e = 0; e < hm.E; ++e) elist[e] = e;
   int rc = BP_SUCCESS;
   int* d_bad = nullptr;
   do {
     if ((rc = m->elementList.upload(elist, s))) break;
-    if ((rc = m->G2L.upload(hm.G2L, s))) break;
-    if ((rc = m->rowStarts.upload(hm.rowStarts, s))) break;
-    if ((rc = m->colIds.upload(hm.colIds, s))) break;
+    // the numbering is computed on the device (closed form, bit-identical to
+    // the host box_numbering): no O(E*Np) host pass, no 0.35 GB upload at 40^3 p=7
+    if ((rc = m->G2L.alloc((size_t)hm.E * Np * hm.Nfields))) break;
+    if ((rc = m->rowStarts.alloc((size_t)ngather + 1))) break;
+    if ((rc = m->colIds.alloc((size_t)nnz))) break;
+    if ((rc = launch_box_numbering(hm.nx, hm.ny, hm.nz, hm.N, hm.Nfields, m->G2L.ptr, m->rowStarts.ptr,
+                                   m->colIds.ptr, s)))
+      break;
     if ((rc = m->D.upload(hm.D, s))) break;
     if ((rc = m->gllz.upload(hm.gllz, s))) break;
     if ((rc = m->gllw.upload(hm.gllw, s))) break;

@@ -158,6 +158,11 @@ int launch_gather(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds
                   cudaStream_t s);
 int launch_scatter(int32_t Nrows, const int32_t* rowStarts, const int32_t* colIds, const double* gv, double* v,
                    cudaStream_t s);
+// masked gathered numbering of the box on the device: GlobalToLocal, CSR row
+// starts (Ngather + 1) and columns, as box_numbering computes them on the host
+void box_numbering_counts(int nx, int ny, int nz, int N, int Nf, int64_t* Ngather, int64_t* nnz);
+int launch_box_numbering(int nx, int ny, int nz, int N, int Nf, int32_t* G2L, int32_t* rowStarts, int32_t* colIds,
+                         cudaStream_t s);
 int launch_geometry(int N, int affine, int E, const double* EX, const double* EY, const double* EZ,
                     const double* gllz, const double* gllw, double* wJ, double* ggeo, int* bad, cudaStream_t s);
 int launch_rhs_analytic(int N, int affine, int Nfields, int E, const double* EX, const double* EY,

@@ -472,6 +472,90 @@ int launch_geometry(int N, int affine, int E, const double* EX, const double* EY
   return BP_SUCCESS;
 }
 
+// ---------------------------------------------------------------------------
+// Masked gathered numbering of the box on the device (the host form is
+// box_numbering in bp_mesh.cpp; reference: ogsSetup.cpp:87-290, 492-579,
+// 833-849, meshMaskedGatherScatterSetup.cpp:31-77).  Along each axis of n
+// elements of degree N a lattice point L = a*N + i lies on the Dirichlet
+// boundary (L = 0 or n*N) or is shared by count(L) elements (2 on an interior
+// element face, else 1), the first of which represents it.  Rows follow the
+// representative element, then the field, then (k, j, i) inside it, and every
+// prefix sum of that order -- row numbers and CSR row starts -- has a closed
+// form, so each local node finds its row, its row's first column and its
+// position in the row (members in ascending element order) by itself.
+// ---------------------------------------------------------------------------
+struct BoxAxis {
+  int n, N;
+  __device__ bool boundary(int L) const { return L == 0 || L == n * N; }
+  __device__ int first(int L) const { return (L > 0 && L % N == 0) ? L / N - 1 : min(L / N, n - 1); }
+  __device__ int count(int L) const { return (L > 0 && L < n * N && L % N == 0) ? 2 : 1; }
+  __device__ int reps(int a) const { return N - 1 + (a < n - 1 ? 1 : 0); }                 // rows of element a
+  __device__ long long reps_before(int a) const { return (long long)a * (N - 1) + min(a, n - 1); }
+  __device__ int mult(int a) const { return N - 1 + (a < n - 1 ? 2 : 0); }                 // columns of element a
+  __device__ long long mult_before(int a) const { return (long long)a * (N - 1) + 2LL * min(a, n - 1); }
+};
+
+__global__ void box_numbering_kernel(int nx, int ny, int nz, int N, int Nf, long long NL, int32_t* __restrict__ G2L,
+                                     int32_t* __restrict__ rowStarts, int32_t* __restrict__ colIds) {
+  const BoxAxis ax{nx, N}, ay{ny, N}, az{nz, N};
+  const int Nq = N + 1, Np = Nq * Nq * Nq;
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < NL;
+       l += (long long)gridDim.x * blockDim.x) {
+    const int n = (int)(l % Np);
+    const long long ef = l / Np;
+    const int f = (int)(ef % Nf);
+    const int e = (int)(ef / Nf);
+    const int ex = e % nx, ey = (e / nx) % ny, ez = e / (nx * ny);
+    const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
+    const int LI = ex * N + i, LJ = ey * N + j, LK = ez * N + k;
+    if (ax.boundary(LI) || ay.boundary(LJ) || az.boundary(LK)) {
+      G2L[l] = -1;
+      continue;
+    }
+    const int rx = ax.first(LI), ry = ay.first(LJ), rz = az.first(LK);
+    const int li = LI - rx * N, lj = LJ - ry * N, lk = LK - rz * N;   // 1..reps
+    const long long Tx = ax.reps_before(nx), Ty = ay.reps_before(ny);
+    const int ci = ax.reps(rx), cj = ay.reps(ry), ck = az.reps(rz);
+    const long long rowBase =
+        (long long)Nf * (Tx * Ty * az.reps_before(rz) + Tx * ay.reps_before(ry) * ck + ax.reps_before(rx) * cj * ck);
+    const long long row = rowBase + (long long)f * ci * cj * ck + ((long long)(lk - 1) * cj + (lj - 1)) * ci + (li - 1);
+    const long long TMx = ax.mult_before(nx), TMy = ay.mult_before(ny);
+    const int mi = ax.mult(rx), mj = ay.mult(ry), mk = az.mult(rz);
+    const int cx = ax.count(LI), cy = ay.count(LJ), cz = az.count(LK);
+    const long long nnzBase = (long long)Nf * (TMx * TMy * az.mult_before(rz) + TMx * ay.mult_before(ry) * mk +
+                                               ax.mult_before(rx) * mj * mk);
+    const long long start = nnzBase + (long long)f * mi * mj * mk + (long long)(lk - 1) * mj * mi +
+                            (long long)cz * (lj - 1) * mi + (long long)cz * cy * (li - 1);
+    const int pos = ((ez - rz) * cy + (ey - ry)) * cx + (ex - rx);
+    G2L[l] = (int32_t)row;
+    colIds[start + pos] = (int32_t)l;
+    if (pos == 0) rowStarts[row] = (int32_t)start;
+  }
+}
+
+// rows and columns of the box numbering (closed forms of the kernel's prefix sums)
+void box_numbering_counts(int nx, int ny, int nz, int N, int Nf, int64_t* Ngather, int64_t* nnz) {
+  auto T = [N](int n) { return (int64_t)n * N - 1; };                          // interior lattice points
+  auto TM = [N](int n) { return (int64_t)n * (N - 1) + 2 * (int64_t)(n - 1); };  // their element memberships
+  *Ngather = (int64_t)Nf * T(nx) * T(ny) * T(nz);
+  *nnz = (int64_t)Nf * TM(nx) * TM(ny) * TM(nz);
+}
+
+int launch_box_numbering(int nx, int ny, int nz, int N, int Nf, int32_t* G2L, int32_t* rowStarts, int32_t* colIds,
+                         cudaStream_t s) {
+  const long long NL = (long long)nx * ny * nz * (N + 1) * (N + 1) * (N + 1) * Nf;
+  int64_t ng = 0, nnz = 0;
+  box_numbering_counts(nx, ny, nz, N, Nf, &ng, &nnz);
+  const int32_t last = (int32_t)nnz;   // pageable source: staged before the call returns
+  BP_CUDA_TRY(cudaMemcpyAsync(rowStarts + ng, &last, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  if (NL == 0) return BP_SUCCESS;
+  long long g = (NL + 255) / 256;
+  if (g > 65536) g = 65536;
+  box_numbering_kernel<<<(unsigned)g, 256, 0, s>>>(nx, ny, nz, N, Nf, NL, G2L, rowStarts, colIds);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
 // Factors of a curved mesh at any tensor grid of points r (weights w), e.g.
 // the N+2 Gauss points of the over-integrated operators.  The reference
 // interpolates the GLL-node derivatives of x, y, z to the Gauss points

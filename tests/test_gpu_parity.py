@@ -23,6 +23,18 @@ AX_CASES = [(2, 2, 2, N, aff, pert, Nf) for N in range(1, 16) for (aff, pert) in
     (2, 2, 2, 7, True, 0.0, 3), (2, 2, 1, 15, False, 0.1, 3), (1, 1, 1, 1, False, 0.0, 1), (4, 3, 2, 5, False, 0.1, 1)]
 
 
+@pytest.mark.parametrize("nx,ny,nz,N,Nf", [(12, 10, 8, 7, 1), (6, 5, 4, 4, 3), (1, 9, 2, 10, 1), (16, 1, 1, 2, 3)])
+def test_device_numbering_matches_host(gpu, nx, ny, nz, N, Nf):
+    # bp_mesh_create numbers the box on the device; the host form (bp_box_numbering)
+    # gives the same arrays bit for bit at sizes beyond the oracle cases
+    gm = gpu.Mesh(nx, ny, nz, N=N, Nfields=Nf)
+    g2l, rs, ci = gpu.box_numbering(nx, ny, nz, N, Nf)
+    assert (gm.Ngather, gm.nnz) == (len(rs) - 1, len(ci))
+    np.testing.assert_array_equal(gm.array("GlobalToLocal"), g2l)
+    np.testing.assert_array_equal(gm.array("rowStarts"), rs)
+    np.testing.assert_array_equal(gm.array("colIds"), ci)
+
+
 @pytest.mark.parametrize("nx,ny,nz,N,affine,pert,Nf", AX_CASES)
 def test_ax_and_gather_match_oracle(gpu, oracle, nx, ny, nz, N, affine, pert, Nf):
     om = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=Nf, pert=pert)
