@@ -176,7 +176,10 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       AT(R, k, ty, tx) = g0 * dr + g1 * ds + g2 * dt;
       AT(S, k, ty, tx) = g1 * dr + g3 * ds + g4 * dt;
       gt[k] = g2 * dr + g4 * ds + g5 * dt;
-      acc[k] = (lambda * w) * qk[k];
+      // q again from the slice copy (the same value as qk[k]): the pencil qk
+      // then dies after the t-gradient, 8 packs of registers fewer through the
+      // r/s phases (NQ = 8, four lanes: 128 registers with spills before)
+      acc[k] = (lambda * w) * AT(U, k, ty, tx);
     }
 #pragma unroll
     for (int n = 0; n < NQ; ++n) {
