@@ -29,8 +29,12 @@
 #include "bp_internal.hpp"
 #include "bp_pack.cuh"
 
-#ifndef BP_LINE_OUTER
-#define BP_LINE_OUTER _Pragma("unroll 1")
+// Outer loops of the line products (one output per pass) are unrolled up to
+// Nq = BP_LINE_UNROLL_MAX and rolled above: unrolled FP64 needs more registers
+// than two blocks allow; FP32 unrolls them all (rolled at Nq = 16: BK6 p=15
+// 5.6 against 4.0 ms).
+#ifndef BP_LINE_UNROLL_MAX
+#define BP_LINE_UNROLL_MAX 0
 #endif
 
 namespace bp {
@@ -61,13 +65,16 @@ struct LineShape {
   static constexpr size_t smem() { return sizeof(T) * (size_t)3 * FIELD * EPB; }
 };
 
-// Blocks per SM the registers are sized for: two up to NQ = 11, except four
-// packed lanes at NQ >= 10, whose 3 x 16-byte fields of about 250 nodes per
-// block leave room for one block per SM anyway; there the kernel may take all
-// the registers it needs (NQ = 11: 936 bytes of spills at 128 registers).
+// Blocks per SM the registers are sized for: two up to NQ = 13 (one element
+// of NQ^2 <= 169 threads per block leaves two blocks 170 registers a thread:
+// FP32 affine BK6 p=11 1.3 ms against 2.4 ms with one block), one above
+// (NQ = 16 at two blocks spills: p=15 5.8 against 4.0 ms).  Four packed lanes
+// at NQ >= 10 take one block too: their 3 x 16-byte fields of about 250 nodes
+// per block leave room for one block per SM anyway (NQ = 11: 936 bytes of
+// spills at 128 registers).
 template <int NQ, class T>
 struct LineMinBlocks {
-  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 10) ? 1 : (NQ <= 11 ? 2 : 1);
+  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 10) ? 1 : (NQ <= 13 ? 2 : 1);
 };
 
 // T: the value type of q and Aq, LineReal or Pack<LineReal, PK> (PK right-hand
@@ -85,6 +92,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
   constexpr int RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB, NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
   constexpr int SLOT = Sh::SLOT, LANES = PackTraits<T>::R;
+  constexpr int OUTER = NQ <= BP_LINE_UNROLL_MAX ? NQ : 1;
 #define D_(a, b) c_line[SLOT + (a) * NQ + (b)]
 #define W_(a) c_line[SLOT + NQ * NQ + (a)]
 #define AT(B, z, y, x) B[(z) * PLANE + (y) * RS + (x)]
@@ -139,7 +147,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       T r[NQ];
 #pragma unroll
       for (int n = 0; n < NQ; ++n) r[n] = AT(U, ty, tx, n);
-      BP_LINE_OUTER
+#pragma unroll OUTER
       for (int i = 0; i < NQ; ++i) {
         T t = pack_zero<T>();
 #pragma unroll
@@ -148,7 +156,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       }
 #pragma unroll
       for (int n = 0; n < NQ; ++n) r[n] = AT(U, ty, n, tx);
-      BP_LINE_OUTER
+#pragma unroll OUTER
       for (int j = 0; j < NQ; ++j) {
         T t = pack_zero<T>();
 #pragma unroll
@@ -160,12 +168,21 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
     T acc[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) {
-      F g0, g1, g2, g3, g4, g5, w;
       if (AFFINE) {
+        // the element's G applied first, the node weight after: scaling G by
+        // the weight per k let the compiler form all 7*NQ scaled factors up
+        // front (Nq = 16: 380 bytes of spills at 255 registers; BK6 p=15 FP32
+        // 4.5 -> 4.0 ms)
         const F wk = wxy * W_(k);
-        g0 = ga[0] * wk; g1 = ga[1] * wk; g2 = ga[2] * wk; g3 = ga[3] * wk; g4 = ga[4] * wk; g5 = ga[5] * wk;
-        w = wa * wk;
-      } else {
+        const T dr = AT(R, k, ty, tx), ds = AT(S, k, ty, tx), dt = gt[k];
+        AT(R, k, ty, tx) = wk * (ga[0] * dr + ga[1] * ds + ga[2] * dt);
+        AT(S, k, ty, tx) = wk * (ga[1] * dr + ga[3] * ds + ga[4] * dt);
+        gt[k] = wk * (ga[2] * dr + ga[4] * ds + ga[5] * dt);
+        acc[k] = (lambda * (wa * wk)) * AT(U, k, ty, tx);
+        continue;
+      }
+      F g0, g1, g2, g3, g4, g5, w;
+      {
         const size_t gb = (size_t)element * NP + k * NQ2 + ty * NQ + tx;
         const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * gb);
         const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
@@ -193,7 +210,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       T r[NQ];
 #pragma unroll
       for (int n = 0; n < NQ; ++n) r[n] = AT(R, ty, tx, n);
-      BP_LINE_OUTER
+#pragma unroll OUTER
       for (int i = 0; i < NQ; ++i) {
         T t = pack_zero<T>();
 #pragma unroll
@@ -202,7 +219,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
       }
 #pragma unroll
       for (int n = 0; n < NQ; ++n) r[n] = AT(S, ty, n, tx);
-      BP_LINE_OUTER
+#pragma unroll OUTER
       for (int j = 0; j < NQ; ++j) {
         T t = pack_zero<T>();
 #pragma unroll

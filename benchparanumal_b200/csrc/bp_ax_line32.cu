@@ -1,6 +1,6 @@
 // FP32 instantiation of the line-per-thread BP5/BP6 element operator (mixed-precision CG).
 #define BP_LINE_REAL float
-#define BP_LINE_OUTER _Pragma("unroll")
+#define BP_LINE_UNROLL_MAX 16
 #include "bp_ax_line.cuh"
 
 namespace bp {
