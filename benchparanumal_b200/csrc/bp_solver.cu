@@ -375,9 +375,11 @@ grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, c
   }
   if (!any) return;
   const bool precon = sc[0].precon != 0;
-  double acc[2 * PK];
+  // the per-thread FP64 sums live in shared memory (one column per thread):
+  // in registers they held the kernel at 48 registers, five blocks per SM
+  __shared__ double s_acc[2 * PK][kThreads];
 #pragma unroll
-  for (int c = 0; c < 2 * PK; ++c) acc[c] = 0.0;
+  for (int c = 0; c < 2 * PK; ++c) s_acc[c][threadIdx.x] = 0.0;
   for (int32_t row = blockIdx.x * kThreads + threadIdx.x; row < Nrows; row += kThreads * gridDim.x) {
     Pack<float, PK> rn = r[row];
     const float dinv = precon ? __ldg(invD + row) : 0.0f;
@@ -397,11 +399,14 @@ grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, c
 #pragma unroll
     for (int l = 0; l < PK; ++l) {
       if (act[l]) rn.v[l] = rn.v[l] - alpha[l] * sum.v[l];
-      acc[l] += (double)rn.v[l] * (double)rn.v[l];
-      if (precon) acc[PK + l] += (double)rn.v[l] * (double)dinv * (double)rn.v[l];
+      s_acc[l][threadIdx.x] += (double)rn.v[l] * (double)rn.v[l];
+      if (precon) s_acc[PK + l][threadIdx.x] += (double)rn.v[l] * (double)dinv * (double)rn.v[l];
     }
     r[row] = rn;
   }
+  double acc[2 * PK];
+#pragma unroll
+  for (int c = 0; c < 2 * PK; ++c) acc[c] = s_acc[c][threadIdx.x];
   double tot[2 * PK];
   if (grid_sum_cg<2 * PK>(acc, partials, counter, tot) && threadIdx.x == 0) {
     for (int l = 0; l < PK; ++l) {
