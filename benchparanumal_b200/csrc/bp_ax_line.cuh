@@ -51,17 +51,19 @@ __host__ __device__ constexpr int line_slot(int nq) {
 constexpr int kLineTable = line_slot(17);
 static __constant__ LineReal c_line[kLineTable];
 
-template <int NQ>
+// Elements per block: about 256 threads, but one element for four packed lanes
+// at NQ >= 10, whose 3 x 16-byte fields take 48-83 KB per element: small
+// blocks let two or three of them share an SM.
+template <int NQ, class T = LineReal>
 struct LineShape {
   static constexpr int G2 = NQ * NQ;
   static constexpr int RS = (NQ % 2) ? NQ : NQ + 1;
   static constexpr int PLANE = NQ * RS;
   static constexpr int FIELD = NQ * PLANE;
   static constexpr int EPB0 = 256 / G2 < 1 ? 1 : 256 / G2;
-  static constexpr int EPB = EPB0 > 8 ? 8 : EPB0;
+  static constexpr int EPB = (sizeof(T) >= 16 && NQ >= 10) ? 1 : (EPB0 > 8 ? 8 : EPB0);
   static constexpr int THREADS = G2 * EPB;
   static constexpr int SLOT = line_slot(NQ);
-  template <class T>
   static constexpr size_t smem() { return sizeof(T) * (size_t)3 * FIELD * EPB; }
 };
 
@@ -69,26 +71,27 @@ struct LineShape {
 // of NQ^2 <= 169 threads per block leaves two blocks 170 registers a thread:
 // FP32 affine BK6 p=11 1.3 ms against 2.4 ms with one block), one above
 // (NQ = 16 at two blocks spills: p=15 5.8 against 4.0 ms).  Four packed lanes
-// at NQ >= 10 take one block too: their 3 x 16-byte fields of about 250 nodes
-// per block leave room for one block per SM anyway (NQ = 11: 936 bytes of
-// spills at 128 registers).
+// at NQ >= 10 (one element per block) get about 168 registers a thread (NQ =
+// 11: 936 bytes of spills at 128).
 template <int NQ, class T>
 struct LineMinBlocks {
-  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 10) ? 1 : (NQ <= 13 ? 2 : 1);
+  static constexpr int ALLOC = (NQ * NQ + 31) / 32 * 32;
+  static constexpr int WIDE = 65536 / (ALLOC * 168) > 0 ? 65536 / (ALLOC * 168) : 1;
+  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 10) ? WIDE : (NQ <= 13 ? 2 : 1);
 };
 
 // T: the value type of q and Aq, LineReal or Pack<LineReal, PK> (PK right-hand
 // sides of one mesh in lockstep, one pack per node); p.Ap partials per lane at
 // partials[lane * gridDim.x + blockIdx.x].
 template <int NQ, bool AFFINE, class T>
-__global__ void __launch_bounds__(LineShape<NQ>::THREADS, (LineMinBlocks<NQ, T>::V))
+__global__ void __launch_bounds__(LineShape<NQ, T>::THREADS, (LineMinBlocks<NQ, T>::V))
 ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
                const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
                const LineReal* __restrict__ gllw, LineReal lambda, const T* __restrict__ q,
                T* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
   if (skip && *skip) return;
   using F = LineReal;
-  using Sh = LineShape<NQ>;
+  using Sh = LineShape<NQ, T>;
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
   constexpr int RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB, NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
   constexpr int SLOT = Sh::SLOT, LANES = PackTraits<T>::R;
@@ -273,8 +276,8 @@ static int launch_line_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_
                           const LineReal* wJ, const LineReal* ggeo, const LineReal* gllw, const LineReal* D,
                           LineReal lambda, const T* q, T* Aq, const int* skip, cudaStream_t s,
                           double* partials, int* nblocks) {
-  using Sh = LineShape<NQ>;
-  constexpr size_t SMEM = Sh::template smem<T>();
+  using Sh = LineShape<NQ, T>;
+  constexpr size_t SMEM = Sh::smem();
   if (!d.affine && (reinterpret_cast<uintptr_t>(ggeo) % (2 * sizeof(LineReal))))
     return fail(BP_ERROR_ARG, "element operator: ggeo must be aligned to two elements");
   LineReal* tab = line_table_address();
