@@ -52,8 +52,8 @@ constexpr int kLineTable = line_slot(17);
 static __constant__ LineReal c_line[kLineTable];
 
 // Elements per block: about 256 threads, but one element for four packed lanes
-// at NQ >= 10, whose 3 x 16-byte fields take 48-83 KB per element: small
-// blocks let two or three of them share an SM.
+// at NQ >= 9, whose 3 x 16-byte fields take 35-83 KB per element: small blocks
+// let two to four of them share an SM.
 template <int NQ, class T = LineReal>
 struct LineShape {
   static constexpr int G2 = NQ * NQ;
@@ -61,7 +61,7 @@ struct LineShape {
   static constexpr int PLANE = NQ * RS;
   static constexpr int FIELD = NQ * PLANE;
   static constexpr int EPB0 = 256 / G2 < 1 ? 1 : 256 / G2;
-  static constexpr int EPB = (sizeof(T) >= 16 && NQ >= 10) ? 1 : (EPB0 > 8 ? 8 : EPB0);
+  static constexpr int EPB = (sizeof(T) >= 16 && NQ >= 9) ? 1 : (EPB0 > 8 ? 8 : EPB0);
   static constexpr int THREADS = G2 * EPB;
   static constexpr int SLOT = line_slot(NQ);
   static constexpr size_t smem() { return sizeof(T) * (size_t)3 * FIELD * EPB; }
@@ -71,13 +71,14 @@ struct LineShape {
 // of NQ^2 <= 169 threads per block leaves two blocks 170 registers a thread:
 // FP32 affine BK6 p=11 1.3 ms against 2.4 ms with one block), one above
 // (NQ = 16 at two blocks spills: p=15 5.8 against 4.0 ms).  Four packed lanes
-// at NQ >= 10 (one element per block) get about 168 registers a thread (NQ =
-// 11: 936 bytes of spills at 128).
+// at NQ >= 9 (one element per block) get about 168 registers a thread (NQ =
+// 11: 936 bytes of spills at 128; BK5 four rhs p=10 6.0 -> 9.3, p=8 8.3 -> 9.1
+// x 10^10 DOF/s).
 template <int NQ, class T>
 struct LineMinBlocks {
   static constexpr int ALLOC = (NQ * NQ + 31) / 32 * 32;
   static constexpr int WIDE = 65536 / (ALLOC * 168) > 0 ? 65536 / (ALLOC * 168) : 1;
-  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 10) ? WIDE : (NQ <= 13 ? 2 : 1);
+  static constexpr int V = (PackTraits<T>::R >= 4 && NQ >= 9) ? WIDE : (NQ <= 13 ? 2 : 1);
 };
 
 // T: the value type of q and Aq, LineReal or Pack<LineReal, PK> (PK right-hand

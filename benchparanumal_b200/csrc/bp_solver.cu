@@ -1366,11 +1366,11 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
     for (int j = 0; j < nproblems; ++j) {
       const bp_batch_problem_t& P = problems[j];
       const bool packable = B->mixed && d->bp == 5 && P.N + 1 <= 12;
-      // four lanes, except at Nq = 9, where the four-lane line kernel's two
-      // 105 KB blocks per SM share the GPU badly with the other problems of a
-      // batch (64 uneven problems: 6.64 s; four lanes everywhere 6.87 s; two at
-      // Nq 9 and 11 as well 6.72 s)
-      const int maxpk = P.N + 1 == 9 ? 2 : 4;
+      // four lanes at every degree: per right-hand side the four-lane operator
+      // beats the two-lane one (BK5 18^3, FP32: p=8 9.13 vs 5.63 x 10^10 DOF/s),
+      // and in the C5 batch (64 uneven problems: 5.71 s, two lanes at Nq = 9
+      // 6.00 s)
+      const int maxpk = 4;
       for (int k = 0; k < P.nrhs;) {
         const int left = P.nrhs - k;
         const int pk = !packable || left == 1 ? 0 : (left == 2 ? 2 : maxpk);
