@@ -68,7 +68,7 @@ def test_mixed_host_entry_matches_device_entry(gpu):
 @pytest.mark.parametrize("N,nrhs", [(7, 4), (7, 2), (4, 4), (6, 2), (9, 2), (3, 4), (8, 4), (9, 4), (10, 4),
                                     (11, 4), (5, 4)])
 def test_fp32_multi_rhs_operator_matches_single(gpu, oracle, N, nrhs):
-    # the packed operator (TMA form at even Nq, line form at odd Nq) gives each
+    # the packed operator (TMA form at even Nq >= 8, line form otherwise) gives each
     # right-hand side what the single-rhs FP32 operator gives it, and both are
     # the FP64 oracle's operator to FP32 accuracy
     om = oracle.Mesh(3, 2, 2, N, pert=0.1)
