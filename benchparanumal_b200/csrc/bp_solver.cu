@@ -360,7 +360,7 @@ grp_direction_kernel(int32_t N, Pack<float, PK>* __restrict__ x, Pack<float, PK>
 
 // r -= alpha Gather(AqL) per lane, r.r and r.z per lane, each lane's stop test
 template <int PK>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)
 grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const int32_t* __restrict__ colIds,
                          const Pack<float, PK>* __restrict__ AqL, Pack<float, PK>* __restrict__ r,
                          const float* __restrict__ invD, CgScalars* sc, double* partials, unsigned int* counter) {
