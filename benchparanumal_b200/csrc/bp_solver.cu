@@ -37,6 +37,10 @@ namespace bp {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 20;            // iterations per captured graph (divides the usual 100 and 1000)
+// Iterations per graph of a batch unit.  A lane that asks for a reliable
+// update idles until its chunk ends while the group's other lanes go on, so
+// shorter chunks waste fewer iterations (and cost more host round trips).
+constexpr int kBatchChunk = 10;
 constexpr double kReliableDrop = 1e-2;
 
 __device__ __forceinline__ double warp_sum_cg(double v) {
@@ -982,7 +986,7 @@ int bp_solver_solve_host(bp_solver_t S, const double* b_host, double* x_host, do
 // the right-hand sides of a problem (degree up to 11) are solved in lockstep as
 // packed groups of 2 or 4 lanes (padding lanes carry b = 0 and finish at once);
 // a single right-hand side and the other cases are standalone systems.  Each
-// group or standalone system (a unit) has a CUDA graph of kChunk iterations
+// group or standalone system (a unit) has a CUDA graph of kBatchChunk iterations
 // and runs on one stream of a pool; the host drives every unit on its own
 // (reliable updates, next chunk, retirement) as its scalars arrive, so no unit
 // waits for another.
@@ -999,7 +1003,7 @@ struct CgGroup {
 };
 
 // A unit of a batch: one packed group, or one standalone system.  Each unit
-// has its own graph of kChunk iterations and is driven independently.
+// has its own graph of kBatchChunk iterations and is driven independently.
 struct BatchUnit {
   CgGroup* G = nullptr;
   int sys = -1;                  // the standalone system (G == nullptr)
@@ -1153,13 +1157,13 @@ static int batch_join(bp_batch_s* B, cudaStream_t s) {
   return BP_SUCCESS;
 }
 
-// kChunk iterations of one unit as a graph
+// kBatchChunk iterations of one unit as a graph
 static int unit_capture(bp_batch_s* B, BatchUnit& u, cudaStream_t s) {
   if (u.graph) return BP_SUCCESS;
   cudaGraph_t g;
   BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int rc = BP_SUCCESS;
-  for (int k = 0; k < kChunk && rc == BP_SUCCESS; ++k) {
+  for (int k = 0; k < kBatchChunk && rc == BP_SUCCESS; ++k) {
     if (u.G) {
       rc = grp_body(u.G, s);
     } else {
@@ -1281,7 +1285,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       }
       if (running) {
         BP_CUDA_TRY(cudaGraphLaunch(u.graph, st));
-        (u.G ? u.G->base : B->sys_solver[u.sys])->launches += 4 * kChunk;
+        (u.G ? u.G->base : B->sys_solver[u.sys])->launches += 4 * kBatchChunk;
         BP_TRY(unit_post(B, u, st));
         ++a;
         continue;
