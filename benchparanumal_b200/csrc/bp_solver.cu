@@ -427,9 +427,14 @@ grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, c
       if (!isfinite(tot[l])) {
         c.breakdown = 1;
         c.done = 1;
-      } else if (tot[l] <= c.tol2 || tot[l] < kReliableDrop * kReliableDrop * c.rmax2 || c.iter >= c.maxit) {
+      } else if (tot[l] <= c.tol2 || c.iter >= c.maxit) {
         c.update = 1;   // a packed group always runs the mixed-precision recursion
         c.done = 1;
+      } else if (tot[l] < kReliableDrop * kReliableDrop * c.rmax2) {
+        // the lane asks for a reliable update but keeps iterating: the group
+        // runs on for its other lanes anyway, and the host replaces this lane's
+        // residual when the chunk ends (stopping it here left it idle until then)
+        c.update = 1;
       }
     }
   }
