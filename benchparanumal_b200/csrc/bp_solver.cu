@@ -1031,7 +1031,7 @@ struct bp_batch_s {
   DeviceArray<CgScalars> sc;                  // every slot's CG scalars, one array
   CgScalars* host_sc = nullptr;               // pinned host copy of sc
   int mixed = 0;
-  std::vector<cudaStream_t> branches;         // the stream pool
+  std::vector<cudaStream_t> pool;             // the stream pool
   std::vector<cudaEvent_t> joins;
   cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
   ~bp_batch_s() {
@@ -1047,7 +1047,7 @@ struct bp_batch_s {
     for (auto* v : r) delete v;
     for (auto* v : b) delete v;
     for (auto* v : pad) delete v;
-    for (auto st : branches) cudaStreamDestroy(st);
+    for (auto st : pool) cudaStreamDestroy(st);
     for (auto e : joins) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
     if (ev0) cudaEventDestroy(ev0);
@@ -1061,7 +1061,7 @@ namespace bp {
 // side, each driven on its own, took 64 uneven problems from 9.1 s (one graph
 // of all units with a host barrier after every chunk) to 7.1 s; 8 or 32
 // streams, largest or smallest unit first, all gave 7.1 s.
-constexpr int kBranches = 16;
+constexpr int kPoolStreams = 16;
 
 // one packed iteration of a group: direction, operator with per-lane p.Ap
 // partials, alpha, gather + update
@@ -1151,12 +1151,12 @@ static int batch_units(bp_batch_s* B) {
 // fork the stream pool off s (their work follows) and join it back
 static int batch_fork(bp_batch_s* B, cudaStream_t s) {
   BP_CUDA_TRY(cudaEventRecord(B->fork, s));
-  for (auto st : B->branches) BP_CUDA_TRY(cudaStreamWaitEvent(st, B->fork, 0));
+  for (auto st : B->pool) BP_CUDA_TRY(cudaStreamWaitEvent(st, B->fork, 0));
   return BP_SUCCESS;
 }
 static int batch_join(bp_batch_s* B, cudaStream_t s) {
-  for (size_t k = 0; k < B->branches.size(); ++k) {
-    BP_CUDA_TRY(cudaEventRecord(B->joins[k], B->branches[k]));
+  for (size_t k = 0; k < B->pool.size(); ++k) {
+    BP_CUDA_TRY(cudaEventRecord(B->joins[k], B->pool[k]));
     BP_CUDA_TRY(cudaStreamWaitEvent(s, B->joins[k], 0));
   }
   return BP_SUCCESS;
@@ -1240,14 +1240,14 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return B->units[a].weight > B->units[b].weight; });
   std::vector<int> free_streams;
-  for (int k = (int)B->branches.size() - 1; k >= 0; --k) free_streams.push_back(k);
+  for (int k = (int)B->pool.size() - 1; k >= 0; --k) free_streams.push_back(k);
   std::vector<int> inflight;
   int next = 0;   // order[next..]: not started
   auto admit = [&](int ui) -> int {
     BatchUnit& u = B->units[ui];
     u.stream = free_streams.back();
     free_streams.pop_back();
-    const cudaStream_t st = B->branches[u.stream];
+    const cudaStream_t st = B->pool[u.stream];
     BP_TRY(unit_start(B, u, tol, maxit, st));
     BP_TRY(unit_post(B, u, st));
     inflight.push_back(ui);
@@ -1269,7 +1269,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       }
       BP_CUDA_TRY(q);
       progressed = true;
-      const cudaStream_t st = B->branches[u.stream];
+      const cudaStream_t st = B->pool[u.stream];
       bool running = false, updated = false;
       for (int l = 0; l < u.lanes; ++l) {
         const CgScalars& c = B->host_sc[u.slot0 + l];
@@ -1357,12 +1357,12 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
     cudaError_t ce = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaEventCreate(&B->ev0);
     if (ce == cudaSuccess) ce = cudaEventCreate(&B->ev1);
-    for (int k = 0; k < kBranches && ce == cudaSuccess; ++k) {
+    for (int k = 0; k < kPoolStreams && ce == cudaSuccess; ++k) {
       cudaStream_t st;
       cudaEvent_t e;
       ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
       if (ce != cudaSuccess) break;
-      B->branches.push_back(st);
+      B->pool.push_back(st);
       ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
       if (ce != cudaSuccess) break;
       B->joins.push_back(e);
