@@ -107,3 +107,34 @@ def test_driver_batched_rhs(gpu, capfd):
     extra = [l for l in out.splitlines() if l.startswith("BP5 extra: right-hand sides=4 solved together")][0]
     res = [float(v) for v in extra.split("relative residuals:")[1].split(",")[0].split()]
     assert len(res) == 4 and max(res) <= 1.0001e-8
+
+
+def test_batch_more_units_than_streams(gpu):
+    # 40 problems of uneven degree and size (the C5 generator at small sizes) with
+    # 2-4 right-hand sides: more units than the 16 streams of the pool, so units
+    # are started as others retire.  Every system reaches the tolerance by its own
+    # FP64 residual, and the FP64 batch gives each system exactly what a single
+    # solve gives it.
+    probs = gpu.uneven_problems(count=40, seed=5, nrhs=3, pmin=2, pmax=8, nmin=2, nmax=5)
+    probs = [dict(p, nrhs=2 + i % 3) for i, p in enumerate(probs)]
+    B = gpu.Batch(probs, precon="JACOBI", precision="MIXED")
+    assert B.nsystems == sum(p["nrhs"] for p in probs)
+    stats, _ = B.solve(tol=1e-8, maxit=5000)
+    stats2, _ = B.solve(tol=1e-8, maxit=5000)   # a second solve on the same batch
+    for s in range(B.nsystems):
+        assert np.sqrt(stats[s].rdotr / stats[s].rdotr0) <= 1e-8
+        assert stats2[s].iterations == stats[s].iterations
+    B64 = gpu.Batch(probs[:20], precon="JACOBI", precision="FP64")
+    st64, _ = B64.solve(tol=1e-8, maxit=5000)
+    sysno = 0
+    for j, p in enumerate(probs[:20]):
+        gm = gpu.Mesh(p["nx"], N=p["N"], pert=p["pert"], pert_seed=p["pert_seed"])
+        S = gpu.BP(gm, precon="JACOBI")
+        for k in range(p["nrhs"]):
+            b = S.rhs("RANDOM", p["rhs_seed"] + k)
+            x = gpu.DeviceBuffer.from_host(np.zeros(gm.Ngather))
+            st, _, _ = S.solve(x, b, tol=1e-8, maxit=5000)
+            xb, _ = B64.vectors(sysno)
+            assert st64[sysno].iterations == st.iterations
+            assert _rel(xb, x.download()) < 1e-13
+            sysno += 1
