@@ -52,6 +52,37 @@ namespace {
 
 constexpr uint32_t kWaitLimit = 1u << 22;   // try_wait rounds before a wait gives up
 
+// D of every degree in the constant bank (slot of NQ: sum of n^2 for n < NQ):
+// row k of the slice being processed is the same for every thread, so its
+// entries enter the FMAs as constant operands instead of shared-memory loads.
+// D depends on the degree only, so launches on any mesh write the same values.
+__host__ __device__ constexpr int tma_d_slot(int nq) {
+  int off = 0;
+  for (int n = 2; n < nq; ++n) off += n * n;
+  return off;
+}
+constexpr int kTmaDTable = tma_d_slot(17);
+__constant__ double c_tma_d64[kTmaDTable];
+__constant__ float c_tma_d32[kTmaDTable];
+
+template <class F>
+__device__ __forceinline__ F tma_d(int idx);
+template <>
+__device__ __forceinline__ double tma_d<double>(int idx) { return c_tma_d64[idx]; }
+template <>
+__device__ __forceinline__ float tma_d<float>(int idx) { return c_tma_d32[idx]; }
+
+template <class F>
+F* tma_d_table() {
+  static F* addr = nullptr;
+  if (!addr) {
+    void* p = nullptr;
+    const cudaError_t e = sizeof(F) == 8 ? cudaGetSymbolAddress(&p, c_tma_d64) : cudaGetSymbolAddress(&p, c_tma_d32);
+    if (e == cudaSuccess) addr = static_cast<F*>(p);
+  }
+  return addr;
+}
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -232,16 +263,10 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
 
     sq[j * (NQ + PAD) + i] = r_u[k];
     __syncthreads();
-    F Dk[NQ];
-#pragma unroll
-    for (int m = 0; m < NQ; m += 2) {
-      const V2 d2 = *reinterpret_cast<const V2*>(s_D + k * NQ + m);
-      Dk[m] = d2.x;
-      Dk[m + 1] = d2.y;
-    }
+    constexpr int DSLOT = tma_d_slot(NQ);
     T ur = pack_zero<T>(), us = pack_zero<T>(), ut = pack_zero<T>();
 #pragma unroll
-    for (int m = 0; m < NQ; ++m) ut += Dk[m] * r_u[m];
+    for (int m = 0; m < NQ; ++m) ut += tma_d<F>(DSLOT + k * NQ + m) * r_u[m];
 #pragma unroll
     for (int m = 0; m < NQ; ++m) {
       ur += Di[m] * sq[j * (NQ + PAD) + m];
@@ -263,7 +288,7 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
       }
     }
 #pragma unroll
-    for (int m = 0; m < NQ; ++m) r_Au[m] += Dk[m] * GDut;
+    for (int m = 0; m < NQ; ++m) r_Au[m] += tma_d<F>(DSLOT + k * NQ + m) * GDut;
 #pragma unroll
     for (int m = 0; m < NQ; ++m) {
       Auk += s_D[m * NQ + j] * sw[m * (NQ + PAD) + i];
@@ -315,6 +340,9 @@ static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const i
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = true;
   }
+  F* tab = tma_d_table<F>();
+  if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
+  BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), D, sizeof(F) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
   const dim3 block(NQ, NQ, Sh::EPB * NF);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
