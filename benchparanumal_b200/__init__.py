@@ -85,7 +85,7 @@ class CubatureView(ctypes.Structure):
 class BatchProblem(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("N", ctypes.c_int32),
                 ("pert", ctypes.c_double), ("pert_seed", ctypes.c_uint64), ("nrhs", ctypes.c_int32),
-                ("rhs_seed", ctypes.c_uint64)]
+                ("rhs_seed", ctypes.c_uint64), ("affine", ctypes.c_int32)]
 
 
 class SolverDesc(ctypes.Structure):
@@ -490,7 +490,8 @@ class Batch:
         probs = list(problems)
         arr = (BatchProblem * len(probs))(*[
             BatchProblem(p["nx"], p.get("ny", p["nx"]), p.get("nz", p["nx"]), p["N"], float(p.get("pert", 0.0)),
-                         int(p.get("pert_seed", 1)), int(p.get("nrhs", 1)), int(p.get("rhs_seed", 0)))
+                         int(p.get("pert_seed", 1)), int(p.get("nrhs", 1)), int(p.get("rhs_seed", 0)),
+                         int(bool(p.get("affine", False))))
             for p in probs])
         pc = {"NONE": BP_PRECON_NONE, "JACOBI": BP_PRECON_JACOBI}[precon.upper()]
         pr = {"FP64": BP_PRECISION_FP64, "MIXED": BP_PRECISION_MIXED}[precision.upper()]

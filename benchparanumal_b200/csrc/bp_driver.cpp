@@ -272,7 +272,6 @@ void cg_model(int bp, const bp_mesh_view_t& v, long long Ndofs, int Niter, doubl
 int run_bp_batch(const char* name, int bp, Settings& S, int nr) {
   if (bp % 2 == 0) throw std::runtime_error("-nr is available for BP1, BP3 and BP5");
   if (!S.compare("FORCING", "RANDOM")) throw std::runtime_error("-nr needs -f RANDOM");
-  if (S.compare("AFFINE MESH", "TRUE")) throw std::runtime_error("-nr runs stored-factor meshes (no -a)");
   if (!S.compare("THREAD MODEL", "CUDA"))
     throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
                              " is not available: this build runs the CUDA (sm_100a) path only");
@@ -286,6 +285,7 @@ int run_bp_batch(const char* name, int bp, Settings& S, int nr) {
   pr.pert_seed = std::strtoull(S.get("PERTURBATION SEED").c_str(), nullptr, 10);
   pr.nrhs = nr;
   pr.rhs_seed = std::strtoull(S.get("FORCING SEED").c_str(), nullptr, 10);
+  pr.affine = S.compare("AFFINE MESH", "TRUE") ? 1 : 0;
   bp_solver_desc_t sd{};
   sd.bp = bp;
   sd.lambda = 1.0;
@@ -311,7 +311,7 @@ int run_bp_batch(const char* name, int bp, Settings& S, int nr) {
   // the sizes the byte/flop model needs
   bp_mesh_view_t v{};
   v.N = pr.N; v.Nq = pr.N + 1; v.Np = v.Nq * v.Nq * v.Nq; v.Nelements = pr.nx * pr.ny * pr.nz; v.Nfields = 1;
-  v.affine = 0; v.Ngather = Nd; v.Nlocal = (int64_t)v.Nelements * v.Np;
+  v.affine = pr.affine; v.Ngather = Nd; v.Nlocal = (int64_t)v.Nelements * v.Np;
   double Nbytes = 0, Nflops = 0, dofit = 0;
   int itmax = 0;
   for (int k = 0; k < nr; ++k) {
@@ -326,7 +326,7 @@ int run_bp_batch(const char* name, int bp, Settings& S, int nr) {
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, iterations=%d, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
       "DOFs*iterations/ranks*time=%1.2e, %s \n",
       name, pr.N, (long long)Nd, elapsed, itmax, elapsed / ((double)Nd * nr), Nbytes / (1.0e9 * elapsed),
-      Nflops / (1.0e9 * elapsed), dofit / elapsed, "Element=Hex");
+      Nflops / (1.0e9 * elapsed), dofit / elapsed, pr.affine ? "Element=Hex, Affine" : "Element=Hex");
   std::printf("%s extra: right-hand sides=%d solved together, precision=%s, precon=%s, iterations per system:", name,
               nr, S.get("PRECISION").c_str(), S.get("PRECONDITIONER").c_str());
   for (int k = 0; k < nr; ++k) std::printf(" %d", st[k].iterations);

@@ -1398,7 +1398,7 @@ int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const
       const bp_batch_problem_t& P = problems[u.prob];
       if (u.prob != cur) {
         bp_box_desc_t bd{};
-        bd.nx = P.nx; bd.ny = P.ny; bd.nz = P.nz; bd.N = P.N; bd.affine = 0; bd.Nfields = 1;
+        bd.nx = P.nx; bd.ny = P.ny; bd.nz = P.nz; bd.N = P.N; bd.affine = P.affine ? 1 : 0; bd.Nfields = 1;
         bd.pert = P.pert; bd.pert_seed = P.pert_seed;
         m = nullptr;
         if ((rc = bp_mesh_create(&bd, &m))) break;

@@ -364,11 +364,13 @@ typedef struct bp_batch_problem {
   uint64_t pert_seed;   /* LCG seed of the perturbation                             */
   int32_t nrhs;         /* right-hand sides: BP_RHS_RANDOM forcing ...              */
   uint64_t rhs_seed;    /* ... with seeds rhs_seed, rhs_seed+1, ..., +nrhs-1        */
+  int32_t affine;       /* nonzero: per-element (affine) factors, as bp_box_desc_t  */
 } bp_batch_problem_t;
 
 /* Meshes, solvers (desc: bp 1, 3 or 5; preconditioner; precision) and
    right-hand sides for every system, in problem order, rhs order within a
-   problem.  The meshes are curved (stored factors). */
+   problem.  Each problem's mesh has stored per-node factors unless its
+   affine flag is set. */
 int bp_batch_create(const bp_batch_problem_t* problems, int32_t nproblems, const bp_solver_desc_t* desc,
                     bp_batch_t* batch);
 int bp_batch_destroy(bp_batch_t batch);

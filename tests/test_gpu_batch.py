@@ -138,3 +138,28 @@ def test_batch_more_units_than_streams(gpu):
             assert st64[sysno].iterations == st.iterations
             assert _rel(xb, x.download()) < 1e-13
             sysno += 1
+
+
+def test_batch_affine_problems(gpu, oracle):
+    # affine meshes (per-element factors) in a mixed batch: four packed lanes on an
+    # even and an odd degree, each system to the tolerance by the oracle's operator
+    probs = [{"nx": 3, "N": 4, "nrhs": 4, "rhs_seed": 70, "affine": True},
+             {"nx": 2, "N": 7, "nrhs": 3, "rhs_seed": 80, "affine": True}]
+    B = gpu.Batch(probs, precon="JACOBI", precision="MIXED")
+    stats, _ = B.solve(tol=1e-8, maxit=3000)
+    s = 0
+    for p in probs:
+        om = oracle.Mesh(p["nx"], p["nx"], p["nx"], p["N"], affine=True)
+        for k in range(p["nrhs"]):
+            xb, bb = B.vectors(s)
+            _, b_o = om.rhs_random(p["rhs_seed"] + k)
+            assert _rel(bb, b_o) < 1e-13
+            assert np.linalg.norm(b_o - om.operator(xb)) <= 1.0001e-8 * np.linalg.norm(b_o)
+            s += 1
+
+def test_driver_batched_affine(gpu, capfd):
+    assert gpu.driver_main("BP5", ["-nx", "4", "-ny", "4", "-nz", "4", "-p", "4", "-a", "-f", "RANDOM", "-pc", "JACOBI",
+                                   "-fp", "MIXED", "-tol", "1e-8", "-it", "3000", "-nr", "4"]) == 0
+    out = capfd.readouterr().out
+    line = [l for l in out.splitlines() if l.startswith("BP5: N= 4")][0]
+    assert line.endswith("Element=Hex, Affine ")
