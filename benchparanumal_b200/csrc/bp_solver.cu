@@ -63,31 +63,52 @@ __device__ __forceinline__ double block_sum_cg(double v, double* s_tmp) {
   return r;
 }
 
+// NS block sums at once, each with block_sum_cg's tree (warp sums, then warp
+// 0 over the warps in order), so the results are the same bits; two barriers
+// for all NS values instead of two per value.  Thread 0 holds the sums.
+template <int NS>
+__device__ __forceinline__ void block_sum_multi_cg(double (&v)[NS], double* s_tmp) {
+  constexpr int W = kThreads / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < NS; ++c) v[c] = warp_sum_cg(v[c]);
+  if (lane == 0)
+#pragma unroll
+    for (int c = 0; c < NS; ++c) s_tmp[c * W + w] = v[c];
+  __syncthreads();
+  if (w == 0)
+#pragma unroll
+    for (int c = 0; c < NS; ++c) v[c] = warp_sum_cg(lane < W ? s_tmp[c * W + lane] : 0.0);
+  __syncthreads();
+}
+
 // Deterministic grid sum: block partials in a fixed slot, the last block to
 // arrive adds them in slot order.  Returns true in the last block (thread 0
 // holds tot).
 template <int NS>
 __device__ __forceinline__ bool grid_sum_cg(const double (&v)[NS], double* partials, unsigned int* counter,
                                             double (&tot)[NS]) {
-  __shared__ double s_tmp[kThreads / 32];
+  __shared__ double s_tmp[NS * (kThreads / 32)];
   __shared__ bool s_last;
-  for (int c = 0; c < NS; ++c) {
-    const double b = block_sum_cg(v[c], s_tmp);
-    if (threadIdx.x == 0) partials[c * gridDim.x + blockIdx.x] = b;
-  }
+  double b[NS];
+#pragma unroll
+  for (int c = 0; c < NS; ++c) b[c] = v[c];
+  block_sum_multi_cg<NS>(b, s_tmp);
   if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < NS; ++c) partials[c * gridDim.x + blockIdx.x] = b[c];
     __threadfence();
     s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
   }
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
-  for (int c = 0; c < NS; ++c) {
-    double acc = 0.0;
-    for (unsigned int b = threadIdx.x; b < gridDim.x; b += kThreads)
-      acc += *((volatile double*)&partials[c * gridDim.x + b]);
-    tot[c] = block_sum_cg(acc, s_tmp);
-  }
+#pragma unroll
+  for (int c = 0; c < NS; ++c) tot[c] = 0.0;
+  for (unsigned int k = threadIdx.x; k < gridDim.x; k += kThreads)
+#pragma unroll
+    for (int c = 0; c < NS; ++c) tot[c] += *((volatile double*)&partials[c * gridDim.x + k]);
+  block_sum_multi_cg<NS>(tot, s_tmp);
   if (threadIdx.x == 0) *counter = 0u;
   return true;
 }
