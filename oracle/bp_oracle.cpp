@@ -34,6 +34,17 @@
  * Extensions that the reference does not have (seeded nodal forcing, vertex
  * perturbation, Jacobi diagonal, preconditioned CG) are restated here from
  * their mathematical definition so the product can be checked against them.
+ * The BP1-BP4 over-integrated forms follow libs/mesh/meshCubatureSetupHex3D.cpp
+ * and okl/bp{1,3}Ax{,Affine}Hex3D.okl.
+ *
+ * PARITY UNPINNED against the reference's own outputs: the reference ships no
+ * tests, golden vectors or fixtures for this path, and it cannot be built in
+ * this environment (its OCCA submodule is empty; MPI and LAPACK are absent), so
+ * no reference run can produce them.  The restatement is pinned instead by
+ * known answers of the mathematics it restates (tests/test_oracle.py,
+ * tests/test_cub_host.py): quadrature and differentiation exactness, the
+ * numbering invariants, affine/curved agreement, symmetry and positivity, and
+ * spectral convergence of a manufactured solution.
  */
 #include <algorithm>
 #include <cmath>

@@ -6,6 +6,11 @@ this module.
 
 The oracle restates the reference's Hex3D BK/BP hot path on the CPU (see the
 header of bp_oracle.cpp for the reference file:line of every routine).
+
+Parity unpinned against the reference's own outputs: the reference has no
+golden vectors or tests for this path and cannot be built here, so the oracle is
+pinned by known answers of the mathematics (tests/test_oracle.py,
+tests/test_cub_host.py).
 """
 import ctypes
 import os
