@@ -163,3 +163,18 @@ def test_driver_batched_affine(gpu, capfd):
     out = capfd.readouterr().out
     line = [l for l in out.splitlines() if l.startswith("BP5: N= 4")][0]
     assert line.endswith("Element=Hex, Affine ")
+
+
+def test_batch_iteration_cap(gpu):
+    # a cap below convergence: every lane stops at exactly maxit (mid-chunk for the
+    # ten-iteration graphs), with its residual replaced by the FP64 one, and the
+    # batch returns; a second solve gives the same counts
+    probs = [{"nx": 4, "N": 6, "pert": 0.1, "pert_seed": 3, "nrhs": 4, "rhs_seed": 90},
+             {"nx": 3, "N": 5, "pert": 0.1, "pert_seed": 4, "nrhs": 1, "rhs_seed": 95}]
+    for prec in ("MIXED", "FP64"):
+        B = gpu.Batch(probs, precon="JACOBI", precision=prec)
+        stats, _ = B.solve(tol=1e-8, maxit=15)
+        assert all(s.iterations == 15 for s in stats)
+        assert all(np.sqrt(s.rdotr / s.rdotr0) > 1e-8 for s in stats)
+        stats2, _ = B.solve(tol=1e-8, maxit=15)
+        assert [s.iterations for s in stats2] == [s.iterations for s in stats]
