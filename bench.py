@@ -48,9 +48,15 @@ WORKLOAD = ("BP5 Hex3D p=7, 40^3 elements, interior vertices perturbed 0.1h (see
 CPU_NX, CPU_ITERS = 20, 100
 MIXED_TOL = 1e-8
 # DRAM traffic of one launch of the packed FP32 element operator (4 rhs) on this
-# workload: the ncu capture of BK5 -fp MIXED -nr 4 on the 20^3 box (217.6 MB for
-# 8000 elements) scaled by the element count to 64,000 elements
-AX_DRAM_BYTES = 217.597e6 * 8
+# workload: the ncu capture of BK5 -fp MIXED -nr 4 on the 20^3 box (174.1 MB read
+# + 41.0 MB written for 8000 elements) scaled by the element count to 64,000
+# elements
+AX_DRAM_BYTES = 215.103488e6 * 8
+# Shared-memory wavefronts of the same launch (loads and stores; the same capture
+# counts 17,637,741 for 8000 elements), scaled to 64,000 elements.  The kernel is
+# bound by this pipe: one wavefront per SM and clock.
+AX_SMEM_WAVEFRONTS = 17.637741e6 * 8
+B200_SMS = 148
 
 
 def ax_model_bytes(Ndofs, E, Np, Nf=1, s=8):
@@ -339,6 +345,8 @@ def main():
     ax_bytes = ax_model_bytes(Nd, E, Np, s=4) + (NRHS - 1) * (Nd * 4 + E * Np * 4)
     peak, peak_kind = read_peaks()
     achieved = ax_bytes / ax_s / 1e9
+    smem_mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    smem_bound_ms = AX_SMEM_WAVEFRONTS / (B200_SMS * smem_mhz * 1e6) * 1e3
     del AqL, ops, q32, b32
 
     cpu = None
@@ -370,7 +378,11 @@ def main():
                          "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,float,Pack<float,4>> (bp_ax_hex3d_f32_multi, 4 rhs)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes,
-                         "launch_ms": ax_s * 1e3},
+                         "launch_ms": ax_s * 1e3,
+                         # the roof that binds this kernel: shared-memory wavefronts at one per SM and clock
+                         # (clock: the median SM clock sampled during the timed step, else the maximum)
+                         "smem": {"wavefronts": AX_SMEM_WAVEFRONTS, "sm_mhz": smem_mhz,
+                                  "bound_ms": smem_bound_ms, "frac": smem_bound_ms / (ax_s * 1e3)}},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
