@@ -154,8 +154,8 @@ def lib():
             "bp_box_numbering": [ctypes.POINTER(BoxDesc), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, vp, vp],
             "bp_basis_gll": [i32, vp, vp, vp],
             "bp_box_vertices": [ctypes.POINTER(BoxDesc), vp, vp, vp],
-            "bp_operator_hex3d_noalloc": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, i32, vp, vp,
-                                          vp, vp, vp],
+            "bp_operator_hex3d_noalloc": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, i32, i32, vp,
+                                          vp, vp, vp, vp],
             "bp_ax_cub_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
             "bp_mesh_cubature": [vp],
             "bp_mesh_cubature_view": [vp, ctypes.POINTER(CubatureView)],
@@ -400,16 +400,23 @@ def ogs_scatter(mesh, gv, v, stream=None):
 NOALLOC_MAX_LOCAL = 1 << 20
 
 
-def operator_noalloc(mesh, q, Aq, lam=1.0, stream=None):
+def operator_noalloc(mesh, q, Aq, lam=1.0, stream=None, elements=None, nelements=None, nlocal=None):
     """bp_operator_hex3d_noalloc: Aq = Gather(A_e q[G2L]) with no device
     allocation (element results in the library's fixed scratch array), for
     callers that may not call cudaMalloc.  Meshes with E*Np*Nfields above
-    NOALLOC_MAX_LOCAL are rejected."""
+    NOALLOC_MAX_LOCAL are rejected.  `elements` (a device address of int32
+    element ids, `nelements` of them) restricts the operator to a subset of the
+    mesh's elements; the default is the whole mesh.  `nlocal` (default: the
+    mesh's E*Np*Nfields) is the element-local length the indices must stay
+    below."""
     v = mesh.view
     d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
-    _check(lib().bp_operator_hex3d_noalloc(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, v.wJ, v.ggeo,
-                                           v.gllw, v.D, float(lam), mesh.Ngather, v.rowStarts, v.colIds, _ptr(q),
-                                           _ptr(Aq), stream))
+    if elements is None:
+        elements, nelements = v.elementList, mesh.E
+    _check(lib().bp_operator_hex3d_noalloc(ctypes.byref(d), int(nelements), _ptr(elements), v.GlobalToLocal, v.wJ,
+                                           v.ggeo, v.gllw, v.D, float(lam), mesh.NL if nlocal is None else int(nlocal),
+                                           mesh.Ngather, v.rowStarts,
+                                           v.colIds, _ptr(q), _ptr(Aq), stream))
 
 
 def _ptr(b):

@@ -58,20 +58,29 @@ using CubReal = BP_CUB_REAL;
 
 enum CubForm { CUB_MASS_AFFINE = 0, CUB_MASS = 1, CUB_STIFF_AFFINE = 2, CUB_STIFF = 3 };
 
-// Constant-bank table: one slot per degree for the curved forms (T = cubInterp
-// [G x NQ], then cubD [G x G]) and one per degree for the affine forms (T =
-// invV, or MM for BP1/BP2, [NQ x NQ], then the modal cubD [NQ x NQ]).  Each
-// launch first copies its operands into its slot on the launch stream.
+// Constant-bank table, three groups of one slot per degree: the curved forms
+// (T = cubInterp [G x NQ], then cubD [G x G]; mass and stiffness share the
+// slot, both write the mesh's cubInterp), the affine stiffness forms of
+// BP3/BP4 (T = invV [NQ x NQ], then the modal cubD [NQ x NQ]) and the affine
+// mass forms of BP1/BP2 (T = MM [NQ x NQ]).  Each launch first copies its
+// operands into its slot on the launch stream, so two launches of the same
+// degree and group on different streams must pass the same matrices (every
+// caller that passes its mesh's own matrices does); operators of different
+// groups never share a slot.
 __host__ __device__ constexpr int cub_curved_size(int nq) { return (nq + 1) * nq + (nq + 1) * (nq + 1); }
 __host__ __device__ constexpr int cub_affine_size(int nq) { return 2 * nq * nq; }
-__host__ __device__ constexpr int cub_slot(int nq, bool affine) {
+__host__ __device__ constexpr int cub_mass_affine_size(int nq) { return nq * nq; }
+__host__ __device__ constexpr int cub_slot(int nq, int form) {
+  const int group = (form == CUB_MASS || form == CUB_STIFF) ? 0 : form == CUB_STIFF_AFFINE ? 1 : 2;
   int off = 0;
-  for (int n = 2; n < (affine ? 17 : nq); ++n) off += cub_curved_size(n);
-  if (affine)
-    for (int n = 2; n < nq; ++n) off += cub_affine_size(n);
+  for (int n = 2; n < (group == 0 ? nq : 17); ++n) off += cub_curved_size(n);
+  if (group >= 1)
+    for (int n = 2; n < (group == 1 ? nq : 17); ++n) off += cub_affine_size(n);
+  if (group == 2)
+    for (int n = 2; n < nq; ++n) off += cub_mass_affine_size(n);
   return off;
 }
-constexpr int kCubTable = cub_slot(17, true);
+constexpr int kCubTable = cub_slot(17, CUB_MASS_AFFINE);
 static_assert(kCubTable * sizeof(double) <= 64 * 1024, "constant table exceeds the 64 KB bank");
 
 static __constant__ CubReal c_cub[kCubTable];
@@ -91,7 +100,7 @@ struct CubShape {
   static constexpr int THREADS = G2 * EPB;
   // resident blocks per SM the register budget must allow (caps registers per thread)
   static constexpr int MINB = G <= 12 ? 2 : 1;
-  static constexpr int SLOT = cub_slot(NQ, !CURVED);
+  static constexpr int SLOT = cub_slot(NQ, FORM);
   static constexpr int TSIZE = G * NQ;              // T rows = output points
   static constexpr int DSIZE = STIFF ? G * G : 0;
   // FP32 curved forms stage each element's Gauss-point factors in shared memory
@@ -398,17 +407,10 @@ BP_CUB_OUTER
 #undef T_
 }
 
-// device address of the constant table (per device, looked up on first use)
+// device address of the constant table on the current device
 static CubReal* cub_table_address() {
-  static CubReal* addr[64] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  if (!addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, c_cub) != cudaSuccess) return nullptr;
-    addr[dev] = static_cast<CubReal*>(p);
-  }
-  return addr[dev];
+  static DeviceSymbol sym(c_cub);
+  return static_cast<CubReal*>(sym.address());
 }
 
 template <int NQ, int FORM>

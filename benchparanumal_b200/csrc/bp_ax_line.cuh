@@ -260,16 +260,10 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
 #undef D_
 }
 
+// device address of the constant table on the current device
 static LineReal* line_table_address() {
-  static LineReal* addr[64] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  if (!addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, c_line) != cudaSuccess) return nullptr;
-    addr[dev] = static_cast<LineReal*>(p);
-  }
-  return addr[dev];
+  static DeviceSymbol sym(c_line);
+  return static_cast<LineReal*>(sym.address());
 }
 
 template <int NQ, class T = LineReal>

@@ -30,11 +30,8 @@ namespace bp {
 __device__ int g_device_error = 0;
 
 int* device_error_word() {
-  static int* p = nullptr;
-  if (!p) {
-    if (cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_device_error) != cudaSuccess) p = nullptr;
-  }
-  return p;
+  static DeviceSymbol sym(&g_device_error);
+  return static_cast<int*>(sym.address());
 }
 
 int check_device_error() {
@@ -74,13 +71,8 @@ __device__ __forceinline__ float tma_d<float>(int idx) { return c_tma_d32[idx]; 
 
 template <class F>
 F* tma_d_table() {
-  static F* addr = nullptr;
-  if (!addr) {
-    void* p = nullptr;
-    const cudaError_t e = sizeof(F) == 8 ? cudaGetSymbolAddress(&p, c_tma_d64) : cudaGetSymbolAddress(&p, c_tma_d32);
-    if (e == cudaSuccess) addr = static_cast<F*>(p);
-  }
-  return addr;
+  static DeviceSymbol sym(sizeof(F) == 8 ? static_cast<const void*>(c_tma_d64) : static_cast<const void*>(c_tma_d32));
+  return static_cast<F*>(sym.address());
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -334,12 +326,12 @@ static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const i
   using Sh = TmaShape<NQ, F>;
   constexpr int R = Sh::R;
   const size_t smem = TmaSmem<NQ, NF, R, F, T>::BYTES;
-  static bool configured = false;
-  if (!configured) {
+  static DeviceOnce configured;   // the shared-memory attribute is set once per device
+  BP_TRY(once_per_device(configured, [smem]() -> int {
     BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, NF, DOT, R, F, T>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+    return BP_SUCCESS;
+  }));
   F* tab = tma_d_table<F>();
   if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
   BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), D, sizeof(F) * NQ * NQ, cudaMemcpyDeviceToDevice, s));

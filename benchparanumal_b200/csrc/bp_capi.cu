@@ -13,8 +13,9 @@
 namespace bp {
 
 static thread_local std::string g_last_error;
-static cudaStream_t g_stream = nullptr;
-static int g_sm_count = 0;
+static std::atomic<cudaStream_t> g_stream[kMaxDevices] = {};
+static std::atomic<int> g_sm_count[kMaxDevices] = {};
+static std::mutex g_device_state_lock;
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 void clear_error() { g_last_error.clear(); }
@@ -29,19 +30,49 @@ int cuda_fail(cudaError_t err, const char* what, const char* file, int line) {
   return err == cudaErrorMemoryAllocation ? BP_ERROR_ALLOC : BP_ERROR_CUDA;
 }
 
+int current_device(int* dev) {
+  BP_CUDA_TRY(cudaGetDevice(dev));
+  if (*dev < 0 || *dev >= kMaxDevices)
+    return fail(BP_ERROR_ARG, "device ordinal " + std::to_string(*dev) + " is beyond the library's " +
+                                  std::to_string(kMaxDevices) + " per-device slots");
+  return BP_SUCCESS;
+}
+
+void* DeviceSymbol::address() {
+  int dev = 0;
+  if (current_device(&dev) != BP_SUCCESS) return nullptr;
+  void* p = addr_[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  const cudaError_t e = cudaGetSymbolAddress(&p, symbol_);
+  if (e != cudaSuccess) {
+    cuda_fail(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
+    return nullptr;
+  }
+  addr_[dev].store(p, std::memory_order_release);   // concurrent first lookups store the same address
+  return p;
+}
+
 cudaStream_t default_stream() {
-  if (!g_stream) cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking);
-  return g_stream;
+  int dev = 0;
+  if (current_device(&dev) != BP_SUCCESS) return nullptr;
+  cudaStream_t s = g_stream[dev].load(std::memory_order_acquire);
+  if (s) return s;
+  std::lock_guard<std::mutex> lock(g_device_state_lock);
+  s = g_stream[dev].load(std::memory_order_relaxed);
+  if (!s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess)
+    g_stream[dev].store(s, std::memory_order_release);
+  return s;
 }
 
 int sm_count() {
-  if (!g_sm_count) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sm_count <= 0) g_sm_count = 148;
+  int dev = 0;
+  if (current_device(&dev) != BP_SUCCESS) return 148;
+  int n = g_sm_count[dev].load(std::memory_order_relaxed);
+  if (n <= 0) {
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    g_sm_count[dev].store(n, std::memory_order_relaxed);
   }
-  return g_sm_count;
+  return n;
 }
 
 }  // namespace bp
@@ -313,35 +344,48 @@ int bp_linalg_axpy(int32_t N, double alpha, const double* x, double beta, double
   return launch_axpy(N, alpha, x, beta, y, to_stream(s));
 }
 
-// scratch for the standalone reductions: partial sums and the arrival counter
-static double* g_red_partials = nullptr;
-static unsigned int* g_red_counter = nullptr;
-static int red_scratch() {
-  if (!g_red_partials) {
-    BP_CUDA_TRY(cudaMalloc(&g_red_partials, sizeof(double) * 4 * reduction_blocks()));
-    BP_CUDA_TRY(cudaMalloc(&g_red_counter, sizeof(unsigned int) * 4));
-    BP_CUDA_TRY(cudaMemset(g_red_counter, 0, sizeof(unsigned int) * 4));
-  }
+// scratch for the standalone reductions, per device: partial sums and the
+// arrival counter (allocated on the first reduction on each device)
+struct RedScratch {
+  double* partials = nullptr;
+  unsigned int* counter = nullptr;
+};
+static RedScratch g_red[kMaxDevices];
+static DeviceOnce g_red_once;
+static int red_scratch(RedScratch** out) {
+  int dev = 0;
+  BP_TRY(current_device(&dev));
+  BP_TRY(once_per_device(g_red_once, [dev]() -> int {
+    RedScratch& r = g_red[dev];
+    BP_CUDA_TRY(cudaMalloc(&r.partials, sizeof(double) * 4 * reduction_blocks()));
+    BP_CUDA_TRY(cudaMalloc(&r.counter, sizeof(unsigned int) * 4));
+    BP_CUDA_TRY(cudaMemset(r.counter, 0, sizeof(unsigned int) * 4));
+    return BP_SUCCESS;
+  }));
+  *out = &g_red[dev];
   return BP_SUCCESS;
 }
 
 int bp_linalg_inner_prod(int32_t N, const double* x, const double* y, double* result, bp_stream_t s) {
   if (N < 0 || !result || (N > 0 && (!x || !y))) return fail(BP_ERROR_ARG, "bp_linalg_inner_prod: bad arguments");
-  BP_TRY(red_scratch());
-  return launch_dot(N, x, y, result, g_red_partials, g_red_counter, to_stream(s));
+  RedScratch* r = nullptr;
+  BP_TRY(red_scratch(&r));
+  return launch_dot(N, x, y, result, r->partials, r->counter, to_stream(s));
 }
 
 int bp_linalg_norm2(int32_t N, const double* x, double* result, bp_stream_t s) {
   if (N < 0 || !result || (N > 0 && !x)) return fail(BP_ERROR_ARG, "bp_linalg_norm2: bad arguments");
-  BP_TRY(red_scratch());
-  BP_TRY(launch_dot(N, x, x, result, g_red_partials, g_red_counter, to_stream(s)));
+  RedScratch* r = nullptr;
+  BP_TRY(red_scratch(&r));
+  BP_TRY(launch_dot(N, x, x, result, r->partials, r->counter, to_stream(s)));
   return launch_sqrt1(result, to_stream(s));
 }
 
 int bp_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* rdotr, bp_stream_t s) {
   if (N < 0 || !rdotr || (N > 0 && (!Ap || !r))) return fail(BP_ERROR_ARG, "bp_update_cg: bad arguments");
-  BP_TRY(red_scratch());
-  return launch_update_cg(N, Ap, alpha, r, rdotr, g_red_partials, g_red_counter, to_stream(s));
+  RedScratch* rs = nullptr;
+  BP_TRY(red_scratch(&rs));
+  return launch_update_cg(N, Ap, alpha, r, rdotr, rs->partials, rs->counter, to_stream(s));
 }
 
 // ---------------------------------------------------------------------------

@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -29,12 +31,51 @@ int cuda_fail(cudaError_t err, const char* what, const char* file, int line);
     if (bp_rc_ != BP_SUCCESS) return bp_rc_; \
   } while (0)
 
-// the library's default stream (created on first use)
+// ---- per-device state ----
+// Every cache of device-side state (symbol addresses, function attributes,
+// scratch buffers, the default stream) is kept per device: a process may
+// switch devices with bp_platform_init, and each device has its own copy of
+// the library image.
+constexpr int kMaxDevices = 64;
+int current_device(int* dev);   // BP_SUCCESS, or an error for an ordinal >= kMaxDevices
+
+// Runs `init` once per device (the current one), serialised by a lock; a
+// failed `init` is not recorded, so the next call retries it.
+struct DeviceOnce {
+  std::atomic<uint64_t> done{0};
+  std::mutex m;
+};
+template <class Fn>
+int once_per_device(DeviceOnce& o, Fn&& init) {
+  int dev = 0;
+  BP_TRY(current_device(&dev));
+  const uint64_t bit = uint64_t(1) << dev;
+  if (o.done.load(std::memory_order_acquire) & bit) return BP_SUCCESS;
+  std::lock_guard<std::mutex> lock(o.m);
+  if (o.done.load(std::memory_order_relaxed) & bit) return BP_SUCCESS;
+  BP_TRY(init());
+  o.done.fetch_or(bit, std::memory_order_release);
+  return BP_SUCCESS;
+}
+
+// The device address of a __device__ or __constant__ symbol on the current
+// device, looked up on first use per device.  Host code may not use the
+// symbol itself as a device address: it names a host-side shadow.
+class DeviceSymbol {
+ public:
+  explicit DeviceSymbol(const void* symbol) : symbol_(symbol) {}
+  void* address();   // nullptr (error text set) when the lookup fails
+ private:
+  const void* symbol_;
+  std::atomic<void*> addr_[kMaxDevices] = {};
+};
+
+// the library's default stream on the current device (created on first use)
 cudaStream_t default_stream();
 inline cudaStream_t to_stream(bp_stream_t s) {
   return s ? reinterpret_cast<cudaStream_t>(s) : default_stream();
 }
-int sm_count();
+int sm_count();   // multiprocessors of the current device
 
 // ---- device buffer owned by the library ----
 template <class T>

@@ -479,17 +479,20 @@ static int vec_grid(int32_t N) {
 // four-lane gather at 48 registers keeps 5 blocks per SM: 1184 blocks ran as
 // 1.6 waves.
 static int vec_grid_wave(const void* kernel, int32_t N) {
-  static std::vector<std::pair<const void*, int>> cache;
-  int wave = 0;
+  static std::mutex lock;
+  static std::vector<std::pair<std::pair<const void*, int>, int>> cache;   // (kernel, device) -> wave
+  int dev = 0, wave = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  std::lock_guard<std::mutex> guard(lock);
   for (const auto& c : cache)
-    if (c.first == kernel) wave = c.second;
+    if (c.first.first == kernel && c.first.second == dev) wave = c.second;
   if (wave == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+    int sms = 0, per_sm = 0;
+    if (dev < 0 || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess)
       per_sm = 0;
     wave = per_sm > 0 && sms > 0 ? std::min(per_sm * sms, reduction_blocks()) : reduction_blocks();
-    cache.push_back({kernel, wave});
+    cache.push_back({{kernel, dev}, wave});
   }
   int g = (N + kThreads - 1) / kThreads;
   if (g > wave) g = wave;

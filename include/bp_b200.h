@@ -173,22 +173,31 @@ int bp_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* r
    device memory budget, or a pipeline that cannot accept the device-wide
    synchronisation that cudaMalloc/cudaFree imply.  The element-local results
    live in a fixed 8 MiB array inside the library image (every GPU that loads
-   the library holds it until the process exits), so Nelements*Np*Nfields may
-   not exceed BP_NOALLOC_MAX_LOCAL; larger meshes are rejected with
-   BP_ERROR_ARG (use bp_solver_operator for them).  The first call on a device
-   looks up the array's device address with that device current; make that
-   first call before any stream capture.  All calls share the array and it
-   keeps the last call's contents (nothing in it needs to start at zero), so
-   calls that overlap on the GPU -- on different streams, or from several host
-   threads -- race with each other.  Arguments are those of bp_ax_hex3d plus
-   the gather's CSR (Ngather, rowStarts, colIds); q [Ngather] in, Aq
-   [Ngather] out, both device memory. */
+   the library holds it until the process exits).
+   Nlocal is the length of the element-local vector that elementList and the
+   CSR index: the mesh's total element count times Np*Nfields.  It may not
+   exceed BP_NOALLOC_MAX_LOCAL; larger meshes are rejected with BP_ERROR_ARG
+   (use bp_solver_operator for them).  elementList may name any subset of the
+   mesh's elements (entries below Nlocal/(Np*Nfields)); every colIds entry must
+   be below Nlocal.  Before launching the operator the call checks every
+   element id, row start and column index on the device and waits for that
+   check (a synchronisation of `stream`, no allocation): an index out of range
+   returns BP_ERROR_ARG and touches nothing.  Elements left out of a partial
+   list contribute zero: the call clears the first Nlocal entries of the
+   array before the element operator writes.
+   The first call on a device looks up the array's device address with that
+   device current; make that first call before any stream capture.  All calls
+   share the one array, so calls that overlap on the GPU -- on different
+   streams, or from several host threads -- race with each other.  Arguments
+   are those of bp_ax_hex3d plus Nlocal and the gather's CSR (Ngather,
+   rowStarts [Ngather+1], colIds); q [Ngather] in, Aq [Ngather] out, both
+   device memory. */
 #define BP_NOALLOC_MAX_LOCAL (1 << 20)
 int bp_operator_hex3d_noalloc(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
                               const int32_t* GlobalToLocal, const double* wJ, const double* ggeo,
-                              const double* gllw, const double* D, double lambda, int32_t Ngather,
-                              const int32_t* rowStarts, const int32_t* colIds, const double* q, double* Aq,
-                              bp_stream_t stream);
+                              const double* gllw, const double* D, double lambda, int32_t Nlocal,
+                              int32_t Ngather, const int32_t* rowStarts, const int32_t* colIds,
+                              const double* q, double* Aq, bp_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Mesh and masked gather-scatter setup.  Replaces mesh_t::Setup for the Hex3D
