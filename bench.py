@@ -19,9 +19,18 @@ With --gpus N > 1 (launched by torch.distributed.run) every rank solves its
 own replica of the problem: the path has no exchange at one rank per problem,
 so scaling is weak and no collective is on the data path.
 
---impl reference times the reference's CPU algorithm (the oracle port; the
-reference itself cannot be built here) on the host cores, on a bounded sample
-of the same workload.
+--impl reference times the reference's own algorithm for this path on the
+host cores: plain (unpreconditioned) FP64 CG, cg::Solve of
+libs/core/linearSolverCG.cpp:62-129 around the bp5AxHex3D operator and the
+ogs gather, one right-hand side, restated in C++/OpenMP by the oracle (the
+reference's OKL kernels need OCCA, which is absent).  It runs on the same 40^3
+mesh and forcing; each step is a bounded sample of 20 CG iterations.
+
+After the headline, the line carries the other configurations of the metric,
+each solved once to 1e-8 in mixed precision and (BP3, BP6) in FP64 beside it:
+BP3 p=7 over-integrated on the same perturbed box, BP6 p=15 on 24^3 affine
+elements with three fields, and the batch of 64 uneven problems
+(--no-extras skips them).
 """
 import argparse
 import json
@@ -44,18 +53,13 @@ NRHS, TOL, MAXIT = 4, 1e-8, 20000
 WORKLOAD = ("BP5 Hex3D p=7, 40^3 elements, interior vertices perturbed 0.1h (seed 1), stored per-node factors; "
             "4 right-hand sides f=2u-1 (seeds 0..3) solved together by the mixed-precision batched Jacobi-PCG "
             "(FP32 recursion and operator, FP64 reliable updates) to ||b-Ax|| <= 1e-8 ||b||")
-# CPU sample: the same problem family on a 20^3 sub-box (1/8 of the elements)
-CPU_NX, CPU_ITERS = 20, 100
-MIXED_TOL = 1e-8
-# DRAM traffic of one launch of the packed FP32 element operator (4 rhs) on this
-# workload: the ncu capture of BK5 -fp MIXED -nr 4 on the 20^3 box (174.1 MB read
-# + 41.0 MB written for 8000 elements) scaled by the element count to 64,000
-# elements
-AX_DRAM_BYTES = 215.103488e6 * 8
-# Shared-memory wavefronts of the same launch (loads and stores; the same capture
-# counts 17,637,741 for 8000 elements), scaled to 64,000 elements.  The kernel is
-# bound by this pipe: one wavefront per SM and clock.
-AX_SMEM_WAVEFRONTS = 17.637741e6 * 8
+# CPU legs (reference arm and cpu_baseline): the reference's plain CG on this
+# same mesh and forcing, REF_ITERS iterations per step
+REF_ITERS = 20
+# The workload's description, identical in both arms' lines
+CONFIG = {"workload": WORKLOAD, "nx": NX, "ny": NX, "nz": NX, "p": P, "Ndofs": (NX * P - 1) ** 3, "rhs": NRHS,
+          "tolerance": TOL, "perturbation": PERT, "perturbation_seed": PERT_SEED, "forcing_seeds": list(range(NRHS)),
+          "l2": "inputs larger than L2 (FP32 factors 0.92 GB read per packed operator apply)"}
 B200_SMS = 148
 
 
@@ -161,28 +165,55 @@ def max_over_ranks(v, world):
     return float(t.item())
 
 
+def cpu_info():
+    """CPU model, physical cores and logical CPUs of this host."""
+    model, cores = "unknown", set()
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name":
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+    except OSError:
+        pass
+    return {"model": model, "physical_cores": len(cores) or os.cpu_count(), "logical_cpus": os.cpu_count()}
+
+
 def cpu_sample(steps=1, warmup=0):
-    """The oracle's Jacobi-PCG on the CPU sample; returns (GDOF*it/s, cores, sample text)."""
+    """The reference's plain CG (oracle restatement) on this workload's mesh and
+    first forcing: REF_ITERS iterations from x = 0 per step, all host threads.
+    Returns (GDOF*it/s, threads, sample text, seconds per step)."""
     from oracle import oracle as O
-    m = O.Mesh(CPU_NX, CPU_NX, CPU_NX, P, pert=PERT, pert_seed=PERT_SEED)
+    m = O.Mesh(NX, NX, NX, P, pert=PERT, pert_seed=PERT_SEED)
     _, b = m.rhs_random(RHS_SEED)
-    inv = 1.0 / m.jacobi_diag(1.0)
     lib = O.lib()
     times = []
     for s in range(warmup + steps):
         x = np.zeros(m.Ngather)
         r = b.copy()
         t0 = time.perf_counter()
-        it = lib.bpo_cg(m._h, 1.0, O._dp(x), O._dp(r), 0.0, CPU_ITERS, 1, O._dp(inv), None, None)
+        it = lib.bpo_cg(m._h, 1.0, O._dp(x), O._dp(r), 0.0, REF_ITERS, 0, None, None, None)
         t1 = time.perf_counter()
-        assert it == CPU_ITERS
+        assert it == REF_ITERS
         if s >= warmup:
             times.append(t1 - t0)
     tot = sum(times)
-    v = m.Ngather * CPU_ITERS * steps / tot / 1e9
-    sample = ("oracle Jacobi-PCG (the reference's CG and BP5 kernels restated in C++/OpenMP), BP5 p=7 on a %d^3 "
-              "perturbed sub-box (%d unknowns, 1/8 of the elements), %d iterations per step" %
-              (CPU_NX, m.Ngather, CPU_ITERS))
+    v = m.Ngather * REF_ITERS * steps / tot / 1e9
+    info = cpu_info()
+    sample = ("the reference's cg::Solve (plain FP64 CG, libs/core/linearSolverCG.cpp:62-129) with the bp5AxHex3D "
+              "operator and ogs gather, restated in C++/OpenMP by the oracle, on this workload's 40^3 p=7 perturbed "
+              "mesh (%d unknowns) and forcing seed %d: %d iterations from x=0 per step, %d threads on %s "
+              "(%d physical cores)" % (m.Ngather, RHS_SEED, REF_ITERS, O.num_threads(), info["model"],
+                                       info["physical_cores"]))
     return v, O.num_threads(), sample, tot / steps
 
 
@@ -193,14 +224,76 @@ def run_reference(args):
     v, cores, sample, sec = cpu_sample(steps=args.steps, warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": "20^3 sub-box, 100 iterations per step",
-                       "reference_algorithm": "plain FP64 Jacobi-PCG, one right-hand side (the reference has no "
-                                              "mixed precision or batching)"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+            "reference_algorithm": "plain FP64 CG (the reference's cg::Solve), one right-hand side, %d iterations "
+                                   "per step; the reference has no preconditioner, mixed precision or batching"
+                                   % REF_ITERS,
+            "cpu": cpu_info(),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def solve_pair(bp, mesh, bpn, seed, maxit=20000):
+    """One problem to 1e-8 in FP64 and in mixed precision (Jacobi-PCG), each
+    after a short warm-up solve that builds its graphs and FP32 data.  Returns
+    the result entry with the mixed solution's error against the FP64 one."""
+    out, xs = {}, {}
+    for prec in ("FP64", "MIXED"):
+        S = bp.BP(mesh, bp=bpn, precon="JACOBI", precision=prec)
+        b = S.rhs("RANDOM", seed)
+        x, r = bp.DeviceBuffer(S.N), bp.DeviceBuffer(S.N)
+        for warm in (True, False):
+            x.zero()
+            bp._check(bp.lib().bp_memcpy_dtod(r.ptr, b.ptr, r.nbytes, None))
+            st, _, _ = S.solve(x, r, tol=TOL, maxit=30 if warm else maxit, history=False)
+        # FP64 check of the returned solution: ||b - A x|| / ||b||
+        bh, Ax = b.download(), bp.DeviceBuffer(S.N)
+        S.operator(x, Ax)
+        res = float(np.linalg.norm(bh - Ax.download()) / np.linalg.norm(bh))
+        xs[prec] = x.download()
+        out[prec] = {"iterations": st.iterations, "seconds": st.elapsed_ms / 1e3,
+                     "gdof_it_s": S.N * st.iterations / (st.elapsed_ms / 1e3) / 1e9,
+                     "fp64_relative_residual": res, "reliable_updates": st.updates}
+        del S, b, x, r, Ax
+    out["Ndofs"] = int(xs["FP64"].size)
+    out["speedup_mixed_vs_fp64"] = out["MIXED"]["gdof_it_s"] / out["FP64"]["gdof_it_s"]
+    out["mixed_error_vs_fp64_solution"] = float(np.linalg.norm(xs["MIXED"] - xs["FP64"]) /
+                                                np.linalg.norm(xs["FP64"]))
+    return out
+
+
+def extra_configs(bp):
+    """The metric's other configurations, each solved once (see the module doc)."""
+    ex = {}
+    m3 = bp.Mesh(NX, NX, NX, N=P, pert=PERT, pert_seed=PERT_SEED)
+    ex["BP3_p7_40cubed_curved"] = dict(solve_pair(bp, m3, 3, RHS_SEED), config=(
+        "BP3 Hex3D p=7, 9 Gauss points per direction, 40^3 elements perturbed 0.1h (seed 1), factors at the "
+        "Gauss points; f=2u-1 (seed 0); Jacobi-PCG to 1e-8"))
+    del m3
+    m6 = bp.Mesh(24, 24, 24, N=15, affine=True, Nfields=3)
+    ex["BP6_p15_24cubed_affine"] = dict(solve_pair(bp, m6, 6, RHS_SEED), config=(
+        "BP6 Hex3D p=15, 24^3 affine elements, three fields; f=2u-1 over the gathered rows (seed 0); "
+        "Jacobi-PCG to 1e-8"))
+    del m6
+    probs = bp.uneven_problems()
+    B = bp.Batch(probs, precon="JACOBI", precision="MIXED")
+    B.solve(tol=TOL, maxit=30)
+    st, ms = B.solve(tol=TOL, maxit=20000)
+    dofit = sum(B.Ngather[k] * s.iterations for k, s in enumerate(st))
+    ex["batch_64_uneven"] = {
+        "config": "64 problems, p in 3..10 and n in 8..24 (LCG seed 2), perturbation 0.1h (seeds 100+i), 4 rhs "
+                  "each (seeds 1000+4i+k); mixed-precision batched Jacobi-PCG to 1e-8",
+        "systems": B.nsystems, "Ndofs_total": int(sum(B.Ngather)), "seconds": ms / 1e3,
+        "gdof_it_s": dofit / (ms / 1e3) / 1e9,
+        "problems": [{"N": p["N"], "n": p["nx"], "iterations": [int(s.iterations) for k, s in enumerate(st)
+                                                                 if B.problem[k] == i],
+                      "max_relative_residual": max(float(np.sqrt(s.rdotr / s.rdotr0)) for k, s in enumerate(st)
+                                                   if B.problem[k] == i)}
+                     for i, p in enumerate(probs)]}
+    del B
+    return ex
 
 
 def main():
@@ -210,6 +303,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--ax-launches", type=int, default=20)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -223,6 +317,7 @@ def main():
     prob = {"nx": NX, "N": P, "pert": PERT, "pert_seed": PERT_SEED, "nrhs": NRHS, "rhs_seed": RHS_SEED}
     B = bp.Batch([prob], precon="JACOBI", precision="MIXED")
     Nd = B.Ngather[0]
+    assert Nd == CONFIG["Ndofs"]
 
     def ev():
         e = bp.ctypes.c_void_p()
@@ -349,6 +444,12 @@ def main():
     smem_bound_ms = AX_SMEM_WAVEFRONTS / (B200_SMS * smem_mhz * 1e6) * 1e3
     del AqL, ops, q32, b32
 
+    # free the headline's buffers before the other configurations
+    del S, b0, x, r, Ax, xd, mesh, B
+    extras = None
+    if not args.no_extras:
+        extras = extra_configs(bp)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cv, cores, sample, _ = cpu_sample(steps=1, warmup=0)
@@ -360,14 +461,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
             "data": "synthetic: seeded LCG forcing f=2u-1 (seeds 0..3) on a seeded perturbed box (seed 1)",
-            "config": {"workload": WORKLOAD, "nx": NX, "ny": NX, "nz": NX, "p": P, "Ndofs": Nd, "rhs": NRHS,
-                       "tolerance": TOL, "precon": "JACOBI",
-                       "iterations_per_system": [s.iterations for s in st],
-                       "reliable_updates_per_system": [s.updates for s in st],
-                       "final_relative_residual_max": rel_res,
-                       "fp64_check_relative_residual": resid,
-                       "parallelism": "replicas" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (FP32 factors 0.92 GB read per packed operator apply)"},
+            "config": CONFIG,
+            "results": {"iterations_per_system": [s.iterations for s in st],
+                        "reliable_updates_per_system": [s.updates for s in st],
+                        "final_relative_residual_max": rel_res,
+                        "fp64_check_relative_residual": resid,
+                        "parallelism": "replicas" if world > 1 else "1 GPU"},
             "clocks": clk,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": NRHS * 8 * Nd,
                     "d2h_bytes_per_step": NRHS * 8 * Nd},
@@ -384,9 +483,10 @@ def main():
                          "smem": {"wavefronts": AX_SMEM_WAVEFRONTS, "sm_mhz": smem_mhz,
                                   "bound_ms": smem_bound_ms, "frac": smem_bound_ms / (ax_s * 1e3)}},
             "cpu_baseline": cpu,
+            "cpu": cpu_info(),
+            "configs": extras,
         }
         print(json.dumps(line))
-    del B
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -25,6 +25,12 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libbp_b200.so")
 
 BP_SUCCESS = 0
+BP_ERROR = -1
+BP_ERROR_ARG = -2
+BP_ERROR_CUDA = -3
+BP_ERROR_ALLOC = -4
+BP_ERROR_NUMERIC = -5
+BP_ERROR_TIMEOUT = -6
 BP_PRECON_NONE = 0
 BP_PRECON_JACOBI = 1
 BP_RHS_ANALYTIC = 0
@@ -42,7 +48,8 @@ EXPORTS = [
     "bp_mesh_create", "bp_mesh_view", "bp_mesh_destroy",
     "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
-    "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc",
+    "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc", "bp_ogs_check",
+    "bp_test_wait_timeout",
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
@@ -154,6 +161,8 @@ def lib():
             "bp_box_numbering": [ctypes.POINTER(BoxDesc), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, vp, vp],
             "bp_basis_gll": [i32, vp, vp, vp],
             "bp_box_vertices": [ctypes.POINTER(BoxDesc), vp, vp, vp],
+            "bp_ogs_check": [ctypes.c_int64, vp, i32, vp, vp],
+            "bp_test_wait_timeout": [ctypes.c_int],
             "bp_operator_hex3d_noalloc": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, i32, i32, vp,
                                           vp, vp, vp, vp],
             "bp_ax_cub_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
@@ -602,6 +611,14 @@ def basis_cubature(N):
     for k in ("invV", "Dmodal", "MM"):
         out[k] = out[k].reshape(Nq, Nq)
     return out
+
+
+def ogs_check(g2l, rowStarts, colIds, Ngather):
+    """bp_ogs_check on host arrays: raises BPError naming the first broken rule."""
+    g = np.ascontiguousarray(g2l, dtype=np.int32)
+    rs = np.ascontiguousarray(rowStarts, dtype=np.int32)
+    ci = np.ascontiguousarray(colIds, dtype=np.int32)
+    _check(lib().bp_ogs_check(g.size, g.ctypes.data, int(Ngather), rs.ctypes.data, ci.ctypes.data))
 
 
 def box_vertices(nx, ny, nz, pert=0.0, pert_seed=1):

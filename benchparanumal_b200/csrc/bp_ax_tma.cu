@@ -47,7 +47,10 @@ int check_device_error() {
 
 namespace {
 
-constexpr uint32_t kWaitLimit = 1u << 22;   // try_wait rounds before a wait gives up
+// A wait gives up after about one second of SM clocks (2^31 cycles at
+// 1.965 GHz); the test-only instantiation below uses a short limit.
+constexpr long long kWaitCycles = 1ll << 31;
+constexpr long long kTestWaitCycles = 1ll << 21;
 
 // D of every degree in the constant bank (slot of NQ: sum of n^2 for n < NQ):
 // row k of the slice being processed is the same for every thread, so its
@@ -88,20 +91,26 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// bounded wait for the phase with the given parity; false if it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// bounded wait for the phase with the given parity; false if it gave up after
+// `limit` SM cycles (the clock is read only once the first try has failed)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
   const uint32_t a = smem_addr(bar);
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
+  if (mbar_try(a, parity)) return true;
+  const long long t0 = clock64();
+  while (clock64() - t0 < limit)
+    if (mbar_try(a, parity)) return true;
   return false;
 }
 
@@ -170,7 +179,10 @@ struct TmaMinBlocks {
   static constexpr int V = R > 1 ? (65536 / (ALLOC * REGS) > 0 ? 65536 / (ALLOC * REGS) : 1) : 1;
 };
 
-template <int NQ, int NF, bool DOT, int R, class F, class T>
+// WITHHOLD >= 0 builds the test-only form: the producer arms the mbarrier of
+// that slice but issues none of its copies, so the wait on it runs out (after
+// the short test limit) with nothing in flight.
+template <int NQ, int NF, bool DOT, int R, class F, class T, int WITHHOLD = -1>
 __global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF, (TmaMinBlocks<NQ, NF, F, T>::V))
 ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
               const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
@@ -203,10 +215,13 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  constexpr long long LIMIT = WITHHOLD >= 0 ? kTestWaitCycles : kWaitCycles;
+  int armed = R;   // slices whose mbarrier phase the producer (t == 0) has armed: 0 .. armed-1
   // producer: first R slices of every active element
   if (t == 0) {
     for (int k = 0; k < R; ++k) {
       mbar_expect_tx(&s_bar[k], nact * Sh::SLICE_BYTES);
+      if (k == WITHHOLD) continue;
       for (int a = 0; a < nact; ++a) {
         const size_t eb = (size_t)elementList[e0 + a] * NP + (size_t)k * NQ2;
         bulk_g2s(s_g + (a * R + k) * Sh::SLICE_G, ggeo + 6 * eb, NQ2 * 6 * sizeof(F), &s_bar[k]);
@@ -247,7 +262,7 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
 #pragma unroll
   for (int k = 0; k < NQ; ++k) {
     const int rs = k % R;
-    ok = mbar_wait(&s_bar[rs], (uint32_t)((k / R) & 1)) && ok;
+    if (ok) ok = mbar_wait(&s_bar[rs], (uint32_t)((k / R) & 1), LIMIT);   // after a give-up, no more waits
     const V2* g2 = reinterpret_cast<const V2*>(s_g + (el * R + rs) * Sh::SLICE_G + 6 * (j * NQ + i));
     const V2 ga = g2[0], gb = g2[1], gc = g2[2];
     const F G00 = ga.x, G01 = ga.y, G02 = gb.x, G11 = gb.y, G12 = gc.x, G22 = gc.y;
@@ -269,11 +284,13 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     const T GDut = G02 * ur + G12 * us + G22 * ut;
     T Auk = (GwJ * lambda) * r_u[k], Auk2 = pack_zero<T>();
     __syncthreads();
-    // slot rs is free again: refill it with slice k+R
-    if (R < NQ && k + R < NQ && t == 0) {
+    // slot rs is free again: refill it with slice k+R (never after the
+    // producer's own wait gave up: the slot's phase may still be open)
+    if (R < NQ && k + R < NQ && t == 0 && ok) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&s_bar[rs], nact * Sh::SLICE_BYTES);
-      for (int a = 0; a < nact; ++a) {
+      armed = k + R + 1;
+      for (int a = 0; a < nact && k + R != WITHHOLD; ++a) {
         const size_t eb = (size_t)elementList[e0 + a] * NP + (size_t)(k + R) * NQ2;
         bulk_g2s(s_g + (a * R + rs) * Sh::SLICE_G, ggeo + 6 * eb, NQ2 * 6 * sizeof(F), &s_bar[rs]);
         bulk_g2s(s_J + (a * R + rs) * NQ2, wJ + eb, NQ2 * sizeof(F), &s_bar[rs]);
@@ -289,7 +306,18 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     r_Au[k] += Auk + Auk2;
   }
   if (!__syncthreads_and(ok)) {   // block-uniform: every thread leaves together
-    if (t == 0) atomicExch(&g_device_error, 1);
+    if (t == 0) {
+      atomicExch(&g_device_error, 1);
+      // The block must not leave while its own bulk copies may still write its
+      // shared memory.  Every phase armed on a slot before its last one was
+      // seen complete by the producer (a slot is re-armed only after that), so
+      // wait, again bounded, for the last armed phase of each slot.
+      for (int r = 0; r < R; ++r) {
+        const int last = armed - 1 - ((armed - 1 - r) % R + R) % R;   // largest armed slice on slot r
+        if (last >= 0) mbar_wait(&s_bar[r], (uint32_t)((last / R) & 1), LIMIT);
+      }
+    }
+    __syncthreads();
     return;
   }
   if (active) {
@@ -395,6 +423,53 @@ int launch_ax_tma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
                   const float* wJ, const float* ggeo, const float* D, float lambda, const float* q, float* Aq,
                   const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   return launch_ax_tma_t<float>(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
+}
+
+// Test hook behind bp_test_wait_timeout: one element of the FP64 stored-factor
+// operator at Nq = 8 (ring of R = 4 slots), through the instantiation that
+// withholds slice `withhold` (0..7), or through the product instantiation for
+// withhold = -1; then the library's device error word.  Allocates and frees
+// its own small buffers.
+template <int W>
+static int tma_wait_test_launch(const int32_t* el, const int32_t* g2l, const double* wJ, const double* ggeo,
+                                const double* D, const double* q, double* Aq, cudaStream_t s) {
+  constexpr int NQ = 8, R = TmaShape<NQ, double>::R;
+  const size_t smem = TmaSmem<NQ, 1, R, double, double>::BYTES;
+  BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, 1, false, R, double, double, W>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ax_tma_kernel<NQ, 1, false, R, double, double, W><<<1, dim3(NQ, NQ, 1), smem, s>>>(1, el, g2l, wJ, ggeo, D, 1.0, q,
+                                                                                    Aq, nullptr, CgFuse{});
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
+int tma_wait_test(int withhold) {
+  constexpr int NQ = 8, NP = NQ * NQ * NQ;
+  if (withhold < -1 || withhold >= NQ) return fail(BP_ERROR_ARG, "bp_test_wait_timeout: slice must be -1..7");
+  DeviceArray<int32_t> el, g2l;
+  DeviceArray<double> wJ, ggeo, D, q, Aq;
+  const cudaStream_t s = default_stream();
+  BP_TRY(el.upload(std::vector<int32_t>(1, 0), s));
+  BP_TRY(g2l.upload(std::vector<int32_t>(NP, 0), s));
+  BP_TRY(wJ.upload(std::vector<double>(NP, 1.0), s));
+  BP_TRY(ggeo.upload(std::vector<double>(6 * NP, 1.0), s));
+  BP_TRY(D.upload(std::vector<double>(NQ * NQ, 0.0), s));
+  BP_TRY(q.upload(std::vector<double>(1, 1.0), s));
+  BP_TRY(Aq.alloc(NP));
+  int rc = BP_SUCCESS;
+  switch (withhold) {
+#define BP_WAIT_CASE(w) \
+  case w:               \
+    rc = tma_wait_test_launch<w>(el.ptr, g2l.ptr, wJ.ptr, ggeo.ptr, D.ptr, q.ptr, Aq.ptr, s); \
+    break;
+    BP_WAIT_CASE(-1) BP_WAIT_CASE(0) BP_WAIT_CASE(3) BP_WAIT_CASE(5) BP_WAIT_CASE(7)
+#undef BP_WAIT_CASE
+    default:
+      return fail(BP_ERROR_ARG, "bp_test_wait_timeout: slice must be one of -1, 0, 3, 5, 7");
+  }
+  BP_TRY(rc);
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_device_error();
 }
 
 // FP32 operator on PK right-hand sides packed per node (q, Aq hold PK floats per

@@ -85,6 +85,8 @@ const char* bp_last_error(void) { return g_last_error.c_str(); }
 
 const char* bp_version(void) { return "benchparanumal_b200 0.1 (sm_100a)"; }
 
+int bp_test_wait_timeout(int withhold_slice) { return tma_wait_test(withhold_slice); }
+
 int bp_platform_init(int device_id) {
   int n = 0;
   BP_CUDA_TRY(cudaGetDeviceCount(&n));

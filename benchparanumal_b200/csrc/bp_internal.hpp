@@ -280,4 +280,6 @@ int launch_ax_line_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, cons
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();
+// test hook: a stored-factor launch whose slice `withhold` never arrives (bp_ax_tma.cu)
+int tma_wait_test(int withhold);
 }  // namespace bp

@@ -411,3 +411,38 @@ extern "C" int bp_box_vertices(const bp_box_desc_t* d, double* EX, double* EY, d
   if (EZ) std::copy(m.EZ.begin(), m.EZ.end(), EZ);
   return BP_SUCCESS;
 }
+
+// Host validation of an externally built masked numbering (rules in bp_b200.h).
+extern "C" int bp_ogs_check(int64_t Nlocal, const int32_t* G2L, int32_t Ngather, const int32_t* rowStarts,
+                            const int32_t* colIds) {
+  using bp::fail;
+  if (Nlocal < 0 || Ngather < 0) return fail(BP_ERROR_ARG, "bp_ogs_check: negative size");
+  if (!rowStarts || (Nlocal > 0 && !G2L)) return fail(BP_ERROR_ARG, "bp_ogs_check: null array");
+  int64_t unmasked = 0;
+  for (int64_t l = 0; l < Nlocal; ++l) {
+    const int32_t r = G2L[l];
+    if (r < -1 || r >= Ngather)
+      return fail(BP_ERROR_ARG, "bp_ogs_check: GlobalToLocal[" + std::to_string(l) + "] = " + std::to_string(r) +
+                                    " is outside [-1, Ngather = " + std::to_string(Ngather) + ")");
+    unmasked += r >= 0;
+  }
+  if (rowStarts[0] != 0) return fail(BP_ERROR_ARG, "bp_ogs_check: rowStarts[0] is not 0");
+  for (int32_t r = 0; r < Ngather; ++r)
+    if (rowStarts[r + 1] <= rowStarts[r])
+      return fail(BP_ERROR_ARG, "bp_ogs_check: row " + std::to_string(r) + " is empty or rowStarts decrease there");
+  if (rowStarts[Ngather] != unmasked)
+    return fail(BP_ERROR_ARG, "bp_ogs_check: rowStarts[Ngather] = " + std::to_string(rowStarts[Ngather]) +
+                                  " but GlobalToLocal has " + std::to_string(unmasked) + " unmasked entries");
+  if (unmasked > 0 && !colIds) return fail(BP_ERROR_ARG, "bp_ogs_check: null colIds");
+  for (int32_t r = 0; r < Ngather; ++r)
+    for (int32_t c = rowStarts[r]; c < rowStarts[r + 1]; ++c) {
+      const int32_t l = colIds[c];
+      if (l < 0 || l >= Nlocal || G2L[l] != r)
+        return fail(BP_ERROR_ARG, "bp_ogs_check: colIds[" + std::to_string(c) + "] = " + std::to_string(l) +
+                                      " is not a local node of row " + std::to_string(r));
+      if (c > rowStarts[r] && l <= colIds[c - 1])
+        return fail(BP_ERROR_ARG, "bp_ogs_check: the columns of row " + std::to_string(r) + " do not ascend at colIds[" +
+                                      std::to_string(c) + "]");
+    }
+  return BP_SUCCESS;
+}

@@ -152,6 +152,12 @@ cg_init_kernel(int32_t N, const double* __restrict__ Ap, double* __restrict__ r,
     sc->skip_x = 0;
     sc->update = 0;
     sc->done = (rdotr <= sc->tol2 || maxit <= 0) ? 1 : 0;
+    // a non-finite initial residual (Inf or NaN in b or x) is a breakdown, not
+    // convergence: with Inf, r.r <= tol^2 r0.r0 would hold at once
+    if (!isfinite(rdotr) || !isfinite(sc->rz)) {
+      sc->breakdown = 1;
+      sc->done = 1;
+    }
   }
 }
 
@@ -336,6 +342,10 @@ mixed_replace_kernel(int32_t N, const double* __restrict__ b, const double* __re
     }
     sc->update = 0;
     sc->done = (tot[0] <= sc->tol2 || sc->iter >= sc->maxit) ? 1 : 0;
+    if (!isfinite(tot[0]) || !isfinite(tot[1]) || !isfinite(sc->rz)) {   // Inf or NaN: breakdown
+      sc->breakdown = 1;
+      sc->done = 1;
+    }
   }
 }
 

@@ -403,6 +403,31 @@ int bp_batch_solver(bp_batch_t batch, int32_t system, bp_solver_t* solver);
  * ------------------------------------------------------------------------- */
 int bp_driver_main(const char* name, int argc, char** argv);
 
+/* ---------------------------------------------------------------------------
+ * Validation and failure detection.
+ * ------------------------------------------------------------------------- */
+
+/* Host-side check of a masked numbering handed in from outside (for example
+   the reference's own mesh_t / ogs_t set-up, libs/ogs/ogsSetup.cpp:492-579,
+   833-849): every GlobalToLocal entry in [-1, Ngather); rowStarts starting at
+   0, non-decreasing, ending at the number of unmasked local nodes; every row
+   non-empty; and row r's colIds exactly the local indices l with
+   GlobalToLocal[l] == r, ascending.  All arrays are HOST memory.  Returns
+   BP_ERROR_ARG naming the first index that breaks a rule, without touching a
+   device.  No counterpart in the reference, which trusts its own set-up. */
+int bp_ogs_check(int64_t Nlocal, const int32_t* GlobalToLocal, int32_t Ngather, const int32_t* rowStarts,
+                 const int32_t* colIds);
+
+/* Test hook for the bounded device-side waits: one element of the FP64
+   stored-factor operator at degree 7 through a kernel instantiation whose
+   producer arms the mbarrier of slice `withhold_slice` (0, 3, 5 or 7) but
+   issues none of its bulk copies, so the consumers' wait runs out after a
+   short limit (about a millisecond) with nothing in flight; -1 runs the
+   product kernel.  Returns the library's device error status: BP_ERROR_TIMEOUT
+   when a wait gave up (the status is then cleared and the context stays
+   usable), BP_SUCCESS otherwise.  Allocates its own small buffers. */
+int bp_test_wait_timeout(int withhold_slice);
+
 #ifdef __cplusplus
 }
 #endif
