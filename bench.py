@@ -61,6 +61,13 @@ CONFIG = {"workload": WORKLOAD, "nx": NX, "ny": NX, "nz": NX, "p": P, "Ndofs": (
           "tolerance": TOL, "perturbation": PERT, "perturbation_seed": PERT_SEED, "forcing_seeds": list(range(NRHS)),
           "l2": "inputs larger than L2 (FP32 factors 0.92 GB read per packed operator apply)"}
 B200_SMS = 148
+# One launch of the packed FP32 element operator (4 rhs) on this workload,
+# captured by ncu at full size (BK5 -nx 40 -ny 40 -nz 40 -p 7 -pt 0.1 -f RANDOM
+# -fp MIXED -nr 4, one kernel, one launch): DRAM bytes read + written, and
+# shared-memory wavefronts (loads + stores).  The kernel is bound by that
+# pipe: one wavefront per SM and clock.
+AX_DRAM_BYTES = 1396588800 + 498959616
+AX_SMEM_WAVEFRONTS = 141570589
 
 
 def ax_model_bytes(Ndofs, E, Np, Nf=1, s=8):
