@@ -277,6 +277,15 @@ int launch_ax_line_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, cons
                           const int32_t* G2L, const float* wJ, const float* ggeo, const float* gllw, const float* D,
                           float lambda, const float* q, float* Aq, const int* skip, const CgFuse* fuse,
                           cudaStream_t s, int* nblocks);
+// affine operator on the tensor cores (bp_ax_mma.cu: DMMA in FP64, split TF32
+// in FP32); returns 1 when the configuration is not covered (stored factors,
+// or Nq other than 16) and nothing was launched
+int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                  const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
+                  const double* q, double* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                  const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
+                  const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

@@ -177,15 +177,17 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
 
 // Kernel variant of the element operator: stored factors use the TMA-staged
 // kernel where it applies and the line-per-thread kernel (bp_ax_line.cuh)
-// elsewhere; affine factors the line kernel in FP32 and the register-pencil
-// kernel in FP64.  BP_AX_VARIANT=pencil
-// or =line in the environment selects that kernel everywhere (for comparisons).
-enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2 };
+// elsewhere; affine factors the tensor-core kernel at Nq = 16 (bp_ax_mma.cu),
+// else the line kernel in FP32 and the register-pencil kernel in FP64.
+// BP_AX_VARIANT=pencil, =line or =mma in the environment selects that kernel
+// wherever it applies (for comparisons).
+enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2, AX_MMA = 3 };
 static int ax_variant() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("BP_AX_VARIANT");
-    v = !e ? AX_AUTO : std::string(e) == "pencil" ? AX_PENCIL : std::string(e) == "line" ? AX_LINE : AX_AUTO;
+    const std::string s = e ? e : "";
+    v = s == "pencil" ? AX_PENCIL : s == "line" ? AX_LINE : s == "mma" ? AX_MMA : AX_AUTO;
   }
   return v;
 }
@@ -200,7 +202,12 @@ static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t*
   // p=10 0.61 vs 1.15 s pencil, p=6 0.68 vs 0.84 s; FP64 BK5 p=6 0.6 vs 0.7 ms).
   // Affine factors: the line kernel in FP32 (p=15: 4.28 vs 4.99 s), the pencil
   // kernel in FP64 (BK5 p=7 0.6 vs 0.8 ms, BK6 p=15 7.4 vs 8.8 ms).
-  if (ax_variant() == AX_LINE || (d.affine && sizeof(F) == 4 && ax_variant() == AX_AUTO))
+  if (d.affine && (ax_variant() == AX_AUTO || ax_variant() == AX_MMA)) {
+    const int rc = launch_ax_mma(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s,
+                                 nblocks);
+    if (rc != 1) return rc;   // 1: not covered (Nq != 16)
+  }
+  if (ax_variant() == AX_LINE || (d.affine && sizeof(F) == 4 && ax_variant() != AX_PENCIL))
     return launch_ax_line(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse, nblocks);
   if (!d.affine && ax_variant() != AX_PENCIL) {
     const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
