@@ -16,10 +16,13 @@
 //   Aq = lambda wJ w q + Dr^T Vr + Ds^T Vs + Dt^T Vt,
 //   (Vr, Vs, Vt) = w G (Dr q, Ds q, Dt q),  w = gllw_i gllw_j gllw_k,
 // G the element's six factors.  One element per block; per field the values go
-// through shared memory in four arrays of NQ^3 (q, then the lambda-term and the
-// divergence sums; the three gradients, then the three fluxes), with padded
-// strides that keep the FP64 fragment loads of all three axes free of bank
-// conflicts.
+// through shared memory in three arrays of NQ^3 with padded strides that keep
+// the FP64 fragment loads of all three axes free of bank conflicts.  A warp's
+// n-tile reads and writes the same 8 columns of a slab, so a contraction may
+// overwrite its own input: the s and t gradients go to two arrays, then the r
+// gradient replaces q, the fluxes replace the gradients, and each divergence
+// contraction replaces its flux; the sum and the mass term are formed at the
+// end, q coming from registers.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -42,7 +45,7 @@ struct MmaShape {
   static constexpr int NTILES = NCOL / 8;      // n-tiles of 8 columns
   static constexpr int PER = NP / THREADS;     // nodes per thread in the pointwise phases
   template <class F>
-  static constexpr size_t smem() { return sizeof(F) * 4 * (size_t)ARR; }
+  static constexpr size_t smem() { return sizeof(F) * 3 * (size_t)ARR; }
   static_assert(NQ % 8 == 0 && NCOL % (8 * WARPS) == 0 && NP % THREADS == 0, "shape");
 };
 
@@ -122,9 +125,9 @@ struct AFrag<NQ, float> {
 };
 
 // One axis of the element: out(x, n) = sum_m A[x][m] in(m, n) for the NCOL
-// columns n = a + NQ b, the columns spread over the warps in tiles of 8.
-// ACC: out += (the divergence sums), else out = (the gradients).
-template <int NQ, bool ACC>
+// columns n = a + NQ b, the columns spread over the warps in tiles of 8.  out
+// may be in: a tile's loads all precede its stores.
+template <int NQ>
 __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, double>& A, const double* in, double* out, int warp,
                                          int lane) {
   using Sh = MmaShape<NQ>;
@@ -142,18 +145,18 @@ __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, double>& A, cons
 #pragma unroll
       for (int mt = 0; mt < AFrag<NQ, double>::MT; ++mt) dmma(c[mt][0], c[mt][1], A.a[mt][kt], b);
     }
+    __syncwarp();
 #pragma unroll
     for (int mt = 0; mt < AFrag<NQ, double>::MT; ++mt)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int n = nt * 8 + 2 * t4 + e;
-        const int o = mma_off<NQ>(d, mt * 8 + g, n % NQ, n / NQ);
-        out[o] = ACC ? out[o] + c[mt][e] : c[mt][e];
+        out[mma_off<NQ>(d, mt * 8 + g, n % NQ, n / NQ)] = c[mt][e];
       }
   }
 }
 
-template <int NQ, bool ACC>
+template <int NQ>
 __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, float>& A, const float* in, float* out, int warp,
                                          int lane) {
   using Sh = MmaShape<NQ>;
@@ -178,19 +181,19 @@ __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, float>& A, const
         tmma(c[mt], A.hi[mt][kt], b0h, b1h);
       }
     }
+    __syncwarp();
 #pragma unroll
     for (int mt = 0; mt < AF::MT; ++mt)
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         const int n = nt * 8 + 2 * t4 + (r & 1);
-        const int o = mma_off<NQ>(d, mt * 16 + g + ((r & 2) ? 8 : 0), n % NQ, n / NQ);
-        out[o] = ACC ? out[o] + c[mt][r] : c[mt][r];
+        out[mma_off<NQ>(d, mt * 16 + g + ((r & 2) ? 8 : 0), n % NQ, n / NQ)] = c[mt][r];
       }
   }
 }
 
 template <int NQ, int NF, bool DOT, class F>
-__global__ void __launch_bounds__(MmaShape<NQ>::THREADS, 1)
+__global__ void __launch_bounds__(MmaShape<NQ>::THREADS, sizeof(F) == 4 ? 2 : 1)
 ax_mma_affine_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
                      const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ gllw,
                      const F* __restrict__ Dg, F lambda, const F* __restrict__ q, F* __restrict__ Aq,
@@ -198,10 +201,9 @@ ax_mma_affine_kernel(int Nelements, const int32_t* __restrict__ elementList, con
   if (skip && *skip) return;
   using Sh = MmaShape<NQ>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  F* sA = reinterpret_cast<F*>(smem_raw);   // q, then the lambda term and the divergence sums
-  F* sU0 = sA + Sh::ARR;                    // gradients, then fluxes (r, s, t)
-  F* sU1 = sU0 + Sh::ARR;
-  F* sU2 = sU1 + Sh::ARR;
+  F* sA = reinterpret_cast<F*>(smem_raw);   // q, then the r gradient, flux and divergence
+  F* sU1 = sA + Sh::ARR;                    // the s gradient, flux and divergence
+  F* sU2 = sU1 + Sh::ARR;                   // the t ones
   __shared__ F sD[NQ * NQ];
   __shared__ F sW[NQ];
 
@@ -232,43 +234,202 @@ ax_mma_affine_kernel(int Nelements, const int32_t* __restrict__ elementList, con
       sA[k * Sh::S2 + j * Sh::S1 + i] = rq[c];
     }
     __syncthreads();
-    // gradients along r, s, t
-    axis_mma<NQ, false>(0, Dgrad, sA, sU0, warp, lane);
-    axis_mma<NQ, false>(1, Dgrad, sA, sU1, warp, lane);
-    axis_mma<NQ, false>(2, Dgrad, sA, sU2, warp, lane);
+    // gradients: s and t from q, then r over q itself
+    axis_mma<NQ>(1, Dgrad, sA, sU1, warp, lane);
+    axis_mma<NQ>(2, Dgrad, sA, sU2, warp, lane);
     __syncthreads();
-    // fluxes w G (ur, us, ut) and the lambda term, node by node
+    axis_mma<NQ>(0, Dgrad, sA, sA, warp, lane);
+    __syncthreads();
+    // fluxes w G (ur, us, ut), node by node
 #pragma unroll
     for (int c = 0; c < Sh::PER; ++c) {
       const int n = t + c * Sh::THREADS;
       const int i = n % NQ, j = (n / NQ) % NQ, k = n / (NQ * NQ);
       const int o = k * Sh::S2 + j * Sh::S1 + i;
       const F w = sW[i] * sW[j] * sW[k];
-      const F ur = sU0[o], us = sU1[o], ut = sU2[o];
-      sU0[o] = w * (G[0] * ur + G[1] * us + G[2] * ut);
+      const F ur = sA[o], us = sU1[o], ut = sU2[o];
+      sA[o] = w * (G[0] * ur + G[1] * us + G[2] * ut);
       sU1[o] = w * (G[1] * ur + G[3] * us + G[4] * ut);
       sU2[o] = w * (G[2] * ur + G[4] * us + G[5] * ut);
-      sA[o] = lambda * eJ * w * rq[c];
     }
     __syncthreads();
-    // divergence: the three transposed contractions, summed into sA in turn
-    axis_mma<NQ, true>(0, Ddiv, sU0, sA, warp, lane);
-    __syncthreads();
-    axis_mma<NQ, true>(1, Ddiv, sU1, sA, warp, lane);
-    __syncthreads();
-    axis_mma<NQ, true>(2, Ddiv, sU2, sA, warp, lane);
+    // divergence: each transposed contraction over its own flux
+    axis_mma<NQ>(0, Ddiv, sA, sA, warp, lane);
+    axis_mma<NQ>(1, Ddiv, sU1, sU1, warp, lane);
+    axis_mma<NQ>(2, Ddiv, sU2, sU2, warp, lane);
     __syncthreads();
 #pragma unroll
     for (int c = 0; c < Sh::PER; ++c) {
       const int n = t + c * Sh::THREADS;
       const int i = n % NQ, j = (n / NQ) % NQ, k = n / (NQ * NQ);
-      const F v = sA[k * Sh::S2 + j * Sh::S1 + i];
+      const int o = k * Sh::S2 + j * Sh::S1 + i;
+      const F w = sW[i] * sW[j] * sW[k];
+      const F v = lambda * eJ * w * rq[c] + sA[o] + sU1[o] + sU2[o];
       Aq[lbase + n] = v;
       if (DOT) pdot += (double)rq[c] * (double)v;
     }
     __syncthreads();   // sA is rewritten by the next field
   }
-  if (DOT) fuse_pap(pdot, fuse, reinterpret_cast<double*>(sU0));
+  if (DOT) fuse_pap(pdot, fuse, reinterpret_cast<double*>(sU1));
+}
+
+// ---------------------------------------------------------------------------
+// Stored-factor FP32 operator on PK = 4 right-hand sides packed per node, at
+// Nq = 8 (the mixed-precision BP5 inner operator of a packed group): each
+// direction is 256 lines (the two other node indices x 4 lanes) times the
+// 8 x 8 matrix, m16n8k8 TF32 MMAs with the data as the A operand (16 lines per
+// tile, both parts of its TF32 split) and D^T (gradient) or D (divergence) as
+// the constant B operand.  A warp's tile reads and writes the same 16 lines,
+// so each divergence contraction runs in place, with no barrier between the
+// three directions.  Factors of the thread's nodes are loaded into registers
+// while the gradients run.
+// ---------------------------------------------------------------------------
+template <int NQ>
+struct Pk4Shape {
+  static_assert(NQ == 8, "packed tensor-core operator: Nq = 8");
+  static constexpr int S1 = 12;                // node stride of j: i- and k-lines load conflict-free
+  static constexpr int S2 = 98;                // node stride of k
+  static constexpr int NODES = NQ * S2;        // padded nodes of one array (float4 each)
+  static constexpr int NP = NQ * NQ * NQ;
+  static constexpr int THREADS = 128;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int MTILES = NQ * NQ * 4 / 16;   // tiles of 16 lines per direction
+  static constexpr int PER = NP / THREADS;     // nodes per thread in the pointwise phases
+  static constexpr size_t SMEM = sizeof(float4) * 4 * (size_t)NODES;
+};
+
+template <int NQ>
+__device__ __forceinline__ int pk_off(int d, int x, int a, int b) {
+  using Sh = Pk4Shape<NQ>;
+  return d == 0 ? b * Sh::S2 + a * Sh::S1 + x : d == 1 ? b * Sh::S2 + x * Sh::S1 + a : x * Sh::S2 + b * Sh::S1 + a;
+}
+
+__device__ __forceinline__ float lane_of(const float4& v, int l) {
+  return l == 0 ? v.x : l == 1 ? v.y : l == 2 ? v.z : v.w;
+}
+
+// one direction d over this warp's tiles: out(line, x) = sum_m in(line, m) B[m][x]
+// (in and out may be the same array: a tile touches only its own lines)
+template <int NQ>
+__device__ __forceinline__ void pk_axis(int d, const uint32_t (&bh)[2], const uint32_t (&bl)[2], const float* in,
+                                        float* out, int warp, int lane) {
+  using Sh = Pk4Shape<NQ>;
+  const int g = lane >> 2, t4 = lane & 3, l = g & 3;
+#pragma unroll 1
+  for (int T = warp; T < Sh::MTILES; T += Sh::WARPS) {
+    const int b = T >> 1, a = (T & 1) * 4 + (g >> 2);   // rows g (a) and g + 8 (a + 2)
+    uint32_t ah[4], al[4];
+    tf32_split(in[4 * pk_off<NQ>(d, t4, a, b) + l], ah[0], al[0]);
+    tf32_split(in[4 * pk_off<NQ>(d, t4, a + 2, b) + l], ah[1], al[1]);
+    tf32_split(in[4 * pk_off<NQ>(d, t4 + 4, a, b) + l], ah[2], al[2]);
+    tf32_split(in[4 * pk_off<NQ>(d, t4 + 4, a + 2, b) + l], ah[3], al[3]);
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    tmma(c, al, bh[0], bh[1]);   // small terms first
+    tmma(c, ah, bl[0], bl[1]);
+    tmma(c, ah, bh[0], bh[1]);
+    __syncwarp();                // every lane's loads of this tile are done before any store
+    out[4 * pk_off<NQ>(d, 2 * t4, a, b) + l] = c[0];
+    out[4 * pk_off<NQ>(d, 2 * t4 + 1, a, b) + l] = c[1];
+    out[4 * pk_off<NQ>(d, 2 * t4, a + 2, b) + l] = c[2];
+    out[4 * pk_off<NQ>(d, 2 * t4 + 1, a + 2, b) + l] = c[3];
+  }
+}
+
+template <int NQ, bool DOT>
+__global__ void __launch_bounds__(Pk4Shape<NQ>::THREADS, 4)
+ax_mma_pk4_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+                  const float* __restrict__ wJ, const float* __restrict__ ggeo, const float* __restrict__ Dg,
+                  float lambda, const float4* __restrict__ q, float4* __restrict__ Aq, const int* __restrict__ skip,
+                  CgFuse fuse) {
+  if (skip && *skip) return;
+  using Sh = Pk4Shape<NQ>;
+  extern __shared__ __align__(16) float4 smem4[];
+  float4* sQ = smem4;
+  float4* sU0 = sQ + Sh::NODES;   // the three directions' arrays follow, NODES apart
+  float4* sU1 = sU0 + Sh::NODES;
+  float4* sU2 = sU1 + Sh::NODES;
+  __shared__ float sD[NQ * NQ];
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int e = elementList[blockIdx.x];
+  const size_t ebase = (size_t)e * Sh::NP;
+  if (t < NQ * NQ) sD[t] = Dg[t];
+  float4 rq[Sh::PER];
+#pragma unroll
+  for (int c = 0; c < Sh::PER; ++c) {
+    const int n = t + c * Sh::THREADS;
+    const int id = __ldg(G2L + ebase + n);
+    rq[c] = id >= 0 ? q[id] : make_float4(0.f, 0.f, 0.f, 0.f);
+    sQ[pk_off<NQ>(0, n % NQ, (n / NQ) % NQ, n / (NQ * NQ))] = rq[c];
+  }
+  __syncthreads();
+  // B operands: gradient B[m][x] = D[x][m], divergence B[m][x] = D[m][x]
+  const int g = lane >> 2, t4 = lane & 3;
+  uint32_t gh[2], gl[2], vh[2], vl[2];
+  tf32_split(sD[g * NQ + t4], gh[0], gl[0]);
+  tf32_split(sD[g * NQ + t4 + 4], gh[1], gl[1]);
+  tf32_split(sD[t4 * NQ + g], vh[0], vl[0]);
+  tf32_split(sD[(t4 + 4) * NQ + g], vh[1], vl[1]);
+  const float* fQ = reinterpret_cast<const float*>(sQ);
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) pk_axis<NQ>(d, gh, gl, fQ, reinterpret_cast<float*>(sU0 + d * Sh::NODES), warp, lane);
+  // the factors of this thread's nodes (in flight while the gradients ran)
+  float G[Sh::PER][6], J[Sh::PER];
+#pragma unroll
+  for (int c = 0; c < Sh::PER; ++c) {
+    const int n = t + c * Sh::THREADS;
+    const float2* g2 = reinterpret_cast<const float2*>(ggeo + 6 * (ebase + n));
+    const float2 x0 = __ldg(g2), x1 = __ldg(g2 + 1), x2 = __ldg(g2 + 2);
+    G[c][0] = x0.x; G[c][1] = x0.y; G[c][2] = x1.x; G[c][3] = x1.y; G[c][4] = x2.x; G[c][5] = x2.y;
+    J[c] = __ldg(wJ + ebase + n);
+  }
+  __syncthreads();
+  // fluxes G (ur, us, ut), node by node (G00 G01 G02 G11 G12 G22)
+#pragma unroll
+  for (int c = 0; c < Sh::PER; ++c) {
+    const int n = t + c * Sh::THREADS;
+    const int o = pk_off<NQ>(0, n % NQ, (n / NQ) % NQ, n / (NQ * NQ));
+    const float4 ur = sU0[o], us = sU1[o], ut = sU2[o];
+    const float* Gc = G[c];
+    sU0[o] = make_float4(Gc[0] * ur.x + Gc[1] * us.x + Gc[2] * ut.x, Gc[0] * ur.y + Gc[1] * us.y + Gc[2] * ut.y,
+                           Gc[0] * ur.z + Gc[1] * us.z + Gc[2] * ut.z, Gc[0] * ur.w + Gc[1] * us.w + Gc[2] * ut.w);
+    sU1[o] = make_float4(Gc[1] * ur.x + Gc[3] * us.x + Gc[4] * ut.x, Gc[1] * ur.y + Gc[3] * us.y + Gc[4] * ut.y,
+                           Gc[1] * ur.z + Gc[3] * us.z + Gc[4] * ut.z, Gc[1] * ur.w + Gc[3] * us.w + Gc[4] * ut.w);
+    sU2[o] = make_float4(Gc[2] * ur.x + Gc[4] * us.x + Gc[5] * ut.x, Gc[2] * ur.y + Gc[4] * us.y + Gc[5] * ut.y,
+                           Gc[2] * ur.z + Gc[4] * us.z + Gc[5] * ut.z, Gc[2] * ur.w + Gc[4] * us.w + Gc[5] * ut.w);
+  }
+  __syncthreads();
+  // divergence, each direction in place
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) {
+    float* u = reinterpret_cast<float*>(sU0 + d * Sh::NODES);
+    pk_axis<NQ>(d, vh, vl, u, u, warp, lane);
+  }
+  __syncthreads();
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < Sh::PER; ++c) {
+    const int n = t + c * Sh::THREADS;
+    const int o = pk_off<NQ>(0, n % NQ, (n / NQ) % NQ, n / (NQ * NQ));
+    const float4 a = sU0[o], b = sU1[o], cc = sU2[o];
+    const float m = lambda * J[c];
+    const float4 r = make_float4(m * rq[c].x + a.x + b.x + cc.x, m * rq[c].y + a.y + b.y + cc.y,
+                                 m * rq[c].z + a.z + b.z + cc.z, m * rq[c].w + a.w + b.w + cc.w);
+    Aq[ebase + n] = r;
+    if (DOT) {
+      v[0] += (double)rq[c].x * r.x;
+      v[1] += (double)rq[c].y * r.y;
+      v[2] += (double)rq[c].z * r.z;
+      v[3] += (double)rq[c].w * r.w;
+    }
+  }
+  if (DOT) {
+    double bs[4];
+    fuse_block_sum_lanes<4>(v, reinterpret_cast<double*>(smem4), bs);
+    if (t == 0)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) fuse.partials[(size_t)l * gridDim.x + blockIdx.x] = bs[l];
+  }
 }
 
 template <int NQ, class F>
@@ -316,6 +477,36 @@ int launch_ax_mma_t(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* ele
 }
 
 }  // namespace
+
+int launch_ax_mma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                         const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
+                         const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                         int* nblocks) {
+  if (pk != 4 || d.affine || d.Nfields != 1 || d.N + 1 != 8 ||
+      ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(Aq)) & 15) || (reinterpret_cast<uintptr_t>(ggeo) & 7))
+    return 1;
+  using Sh = Pk4Shape<8>;
+  const CgFuse Fz = fuse ? *fuse : CgFuse{};
+  if (nblocks) *nblocks = Nelements;
+  if (Nelements == 0) return BP_SUCCESS;
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  float4* a4 = reinterpret_cast<float4*>(Aq);
+#define BP_PK_LAUNCH(DOT)                                                                                      \
+  do {                                                                                                         \
+    static DeviceOnce configured;                                                                              \
+    BP_TRY(once_per_device(configured, []() -> int {                                                           \
+      BP_CUDA_TRY(cudaFuncSetAttribute(ax_mma_pk4_kernel<8, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                       (int)Sh::SMEM));                                                        \
+      return BP_SUCCESS;                                                                                       \
+    }));                                                                                                       \
+    ax_mma_pk4_kernel<8, DOT><<<Nelements, Sh::THREADS, Sh::SMEM, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, \
+                                                                      lambda, q4, a4, skip, Fz);              \
+  } while (0)
+  if (fuse) BP_PK_LAUNCH(true); else BP_PK_LAUNCH(false);
+#undef BP_PK_LAUNCH
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
 
 int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,

@@ -270,8 +270,13 @@ int bp_ax_hex3d_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Neleme
   if ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(Aq)) % (sizeof(float) * nrhs))
     return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: q and Aq must be aligned to nrhs floats");
   const cudaStream_t s = to_stream(stream);
-  int rc = launch_ax_tma_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, D, lambda, q, Aq,
-                                nullptr, nullptr, s, nullptr);
+  int rc = 1;
+  if (ax_variant() == AX_MMA)   // the tensor-core packed form only when asked for (slower at Nq = 8)
+    rc = launch_ax_mma_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, D, lambda, q, Aq,
+                              nullptr, nullptr, s, nullptr);
+  if (rc == 1)
+    rc = launch_ax_tma_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, D, lambda, q, Aq,
+                              nullptr, nullptr, s, nullptr);
   if (rc == 1)
     rc = launch_ax_line_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq,
                                nullptr, nullptr, s, nullptr);

@@ -286,6 +286,16 @@ int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
 int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
                   const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+// Element-operator variant forced by BP_AX_VARIANT (pencil, line, tma, mma),
+// else AX_AUTO: the measured choice per configuration.
+enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2, AX_MMA = 3, AX_TMA = 4 };
+int ax_variant();
+// the packed FP32 stored-factor operator (4 rhs) at Nq = 8 on the tensor cores;
+// 1 when not covered
+int launch_ax_mma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                         const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
+                         const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                         int* nblocks);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

@@ -179,17 +179,13 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
 // kernel where it applies and the line-per-thread kernel (bp_ax_line.cuh)
 // elsewhere; affine factors the tensor-core kernel at Nq = 16 (bp_ax_mma.cu),
 // else the line kernel in FP32 and the register-pencil kernel in FP64.
-// BP_AX_VARIANT=pencil, =line or =mma in the environment selects that kernel
-// wherever it applies (for comparisons).
-enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2, AX_MMA = 3 };
-static int ax_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("BP_AX_VARIANT");
-    const std::string s = e ? e : "";
-    v = s == "pencil" ? AX_PENCIL : s == "line" ? AX_LINE : s == "mma" ? AX_MMA : AX_AUTO;
-  }
-  return v;
+// BP_AX_VARIANT=pencil, =line, =tma or =mma in the environment selects that
+// kernel wherever it applies (for comparisons).
+int ax_variant() {   // read at every launch, so a process (a test) can switch forms
+  const char* e = getenv("BP_AX_VARIANT");
+  if (!e) return AX_AUTO;
+  const std::string s = e;
+  return s == "pencil" ? AX_PENCIL : s == "line" ? AX_LINE : s == "mma" ? AX_MMA : s == "tma" ? AX_TMA : AX_AUTO;
 }
 
 template <int NQ, class F>

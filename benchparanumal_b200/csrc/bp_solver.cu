@@ -1112,8 +1112,16 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   const ElemOperands<float> o = operands32(S);
   const CgFuse fuse{G->parts.ptr};
   int nparts = 0;
-  int rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D,
-                                (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
+  int rc = 1;
+  // The tensor-core packed form (Nq = 8, four lanes) only when asked for: it
+  // measured 1.40 ms per launch against the TMA form's 0.61 ms on the 40^3 p=7
+  // box (latency-bound: 16 warps per SM, five barriers per element).
+  if (ax_variant() == AX_MMA)
+    rc = launch_ax_mma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, (float)S->lambda,
+                              G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
+  if (rc == 1)
+    rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, (float)S->lambda,
+                              G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
   if (rc == 1)   // no TMA form (odd Nq): the line-per-thread kernel
     rc = launch_ax_line_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
                                (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);

@@ -78,3 +78,30 @@ def test_mma_mixed_solve_reaches_tolerance(gpu, oracle):
     assert np.linalg.norm(b_o - Ax.download()) / np.linalg.norm(b_o) <= 1.0001e-8
     _, _, it_o, _, _ = om.cg(b_o, 1.0, 1e-8, 20000, precon=True)
     assert st.iterations <= 1.25 * it_o + 20, (st.iterations, it_o)
+
+
+def test_mma_packed_p7_operator_when_selected(gpu, oracle, monkeypatch):
+    """The packed four-rhs FP32 form at p=7 (BP_AX_VARIANT=mma; the TMA form is
+    the default there, being faster): each lane equals the FP64 oracle's
+    operator to FP32 accuracy and the default form to 1e-6."""
+    om = oracle.Mesh(3, 2, 2, 7, pert=0.1)
+    gm = gpu.Mesh(3, 2, 2, N=7, pert=0.1)
+    v = gm.view
+    ng = gm.E * gm.Np
+    ops = {"wJ": gpu.DeviceBuffer(ng, np.float32), "ggeo": gpu.DeviceBuffer(6 * ng, np.float32),
+           "gllw": gpu.DeviceBuffer(gm.Nq, np.float32), "D": gpu.DeviceBuffer(gm.Nq * gm.Nq, np.float32)}
+    for name, n in (("wJ", ng), ("ggeo", 6 * ng), ("gllw", gm.Nq), ("D", gm.Nq * gm.Nq)):
+        gpu.convert_f64_f32(getattr(v, name), n, ops[name])
+    Q = np.stack([2 * oracle.random(30 + k, gm.Ngather) - 1 for k in range(4)], axis=1).astype(np.float32)
+    dq = gpu.DeviceBuffer.from_host(np.ascontiguousarray(Q).ravel())
+    out = {}
+    for form in ("mma", "tma"):
+        monkeypatch.setenv("BP_AX_VARIANT", form)
+        dA = gpu.DeviceBuffer(gm.NL * 4, np.float32)
+        gpu.ax_hex3d_f32_multi(gm, 4, dq, dA, ops)
+        out[form] = dA.download().reshape(gm.NL, 4)
+    monkeypatch.delenv("BP_AX_VARIANT")
+    for k in range(4):
+        want = om.ax(Q[:, k].astype(np.float64))
+        assert rel(out["mma"][:, k].astype(np.float64), want) <= 2e-6
+        assert rel(out["mma"][:, k], out["tma"][:, k]) <= 1e-6
