@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
@@ -127,7 +128,7 @@ struct AFrag<NQ, float> {
 // One axis of the element: out(x, n) = sum_m A[x][m] in(m, n) for the NCOL
 // columns n = a + NQ b, the columns spread over the warps in tiles of 8.  out
 // may be in: a tile's loads all precede its stores.
-template <int NQ>
+template <int NQ, int TERMS = 1>
 __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, double>& A, const double* in, double* out, int warp,
                                          int lane) {
   using Sh = MmaShape<NQ>;
@@ -156,7 +157,9 @@ __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, double>& A, cons
   }
 }
 
-template <int NQ>
+// TERMS = 3: the split product; 1: plain TF32 (a_hi b_hi only), kept for the
+// precision experiment behind BP_MMA_TF32_TERMS=1
+template <int NQ, int TERMS = 3>
 __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, float>& A, const float* in, float* out, int warp,
                                          int lane) {
   using Sh = MmaShape<NQ>;
@@ -176,8 +179,10 @@ __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, float>& A, const
       tf32_split(in[mma_off<NQ>(d, kt * 8 + t4 + 4, ab, bb)], b1h, b1l);
 #pragma unroll
       for (int mt = 0; mt < AF::MT; ++mt) {   // small terms first
-        tmma(c[mt], A.lo[mt][kt], b0h, b1h);
-        tmma(c[mt], A.hi[mt][kt], b0l, b1l);
+        if (TERMS == 3) {
+          tmma(c[mt], A.lo[mt][kt], b0h, b1h);
+          tmma(c[mt], A.hi[mt][kt], b0l, b1l);
+        }
         tmma(c[mt], A.hi[mt][kt], b0h, b1h);
       }
     }
@@ -192,7 +197,7 @@ __device__ __forceinline__ void axis_mma(int d, const AFrag<NQ, float>& A, const
   }
 }
 
-template <int NQ, int NF, bool DOT, class F>
+template <int NQ, int NF, bool DOT, class F, int TERMS = 3>
 __global__ void __launch_bounds__(MmaShape<NQ>::THREADS, sizeof(F) == 4 ? 2 : 1)
 ax_mma_affine_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
                      const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ gllw,
@@ -235,10 +240,10 @@ ax_mma_affine_kernel(int Nelements, const int32_t* __restrict__ elementList, con
     }
     __syncthreads();
     // gradients: s and t from q, then r over q itself
-    axis_mma<NQ>(1, Dgrad, sA, sU1, warp, lane);
-    axis_mma<NQ>(2, Dgrad, sA, sU2, warp, lane);
+    axis_mma<NQ, TERMS>(1, Dgrad, sA, sU1, warp, lane);
+    axis_mma<NQ, TERMS>(2, Dgrad, sA, sU2, warp, lane);
     __syncthreads();
-    axis_mma<NQ>(0, Dgrad, sA, sA, warp, lane);
+    axis_mma<NQ, TERMS>(0, Dgrad, sA, sA, warp, lane);
     __syncthreads();
     // fluxes w G (ur, us, ut), node by node
 #pragma unroll
@@ -254,9 +259,9 @@ ax_mma_affine_kernel(int Nelements, const int32_t* __restrict__ elementList, con
     }
     __syncthreads();
     // divergence: each transposed contraction over its own flux
-    axis_mma<NQ>(0, Ddiv, sA, sA, warp, lane);
-    axis_mma<NQ>(1, Ddiv, sU1, sU1, warp, lane);
-    axis_mma<NQ>(2, Ddiv, sU2, sU2, warp, lane);
+    axis_mma<NQ, TERMS>(0, Ddiv, sA, sA, warp, lane);
+    axis_mma<NQ, TERMS>(1, Ddiv, sU1, sU1, warp, lane);
+    axis_mma<NQ, TERMS>(2, Ddiv, sU2, sU2, warp, lane);
     __syncthreads();
 #pragma unroll
     for (int c = 0; c < Sh::PER; ++c) {
@@ -440,22 +445,31 @@ int launch_mma_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
   const size_t smem = Sh::template smem<F>();
   const CgFuse Fz = fuse ? *fuse : CgFuse{};
   if (nblocks) *nblocks = Nelements;
-#define BP_MMA_LAUNCH(NF, DOT)                                                                                  \
+  // BP_MMA_TF32_TERMS=1 (FP32 only): plain TF32 products instead of the split
+  // ones, an experiment on how much operator precision the mixed CG needs
+  const char* terms_env = getenv("BP_MMA_TF32_TERMS");
+  const bool plain = sizeof(F) == 4 && terms_env && terms_env[0] == '1';
+#define BP_MMA_LAUNCH(NF, DOT, TERMS)                                                                           \
   do {                                                                                                          \
     static DeviceOnce configured;                                                                               \
     BP_TRY(once_per_device(configured, [smem]() -> int {                                                        \
-      BP_CUDA_TRY(cudaFuncSetAttribute(ax_mma_affine_kernel<NQ, NF, DOT, F>,                                    \
+      BP_CUDA_TRY(cudaFuncSetAttribute(ax_mma_affine_kernel<NQ, NF, DOT, F, TERMS>,                             \
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));               \
       return BP_SUCCESS;                                                                                        \
     }));                                                                                                        \
-    ax_mma_affine_kernel<NQ, NF, DOT, F><<<Nelements, Sh::THREADS, smem, s>>>(Nelements, elementList, G2L, wJ,  \
-                                                                             ggeo, gllw, D, lambda, q, Aq,    \
-                                                                             skip, Fz);                        \
+    ax_mma_affine_kernel<NQ, NF, DOT, F, TERMS><<<Nelements, Sh::THREADS, smem, s>>>(                          \
+        Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, Fz);                               \
   } while (0)
-  if (d.Nfields == 3) {
-    if (fuse) BP_MMA_LAUNCH(3, true); else BP_MMA_LAUNCH(3, false);
+  if (plain) {
+    if (d.Nfields == 3) {
+      if (fuse) BP_MMA_LAUNCH(3, true, 1); else BP_MMA_LAUNCH(3, false, 1);
+    } else {
+      if (fuse) BP_MMA_LAUNCH(1, true, 1); else BP_MMA_LAUNCH(1, false, 1);
+    }
+  } else if (d.Nfields == 3) {
+    if (fuse) BP_MMA_LAUNCH(3, true, 3); else BP_MMA_LAUNCH(3, false, 3);
   } else {
-    if (fuse) BP_MMA_LAUNCH(1, true); else BP_MMA_LAUNCH(1, false);
+    if (fuse) BP_MMA_LAUNCH(1, true, 3); else BP_MMA_LAUNCH(1, false, 3);
   }
 #undef BP_MMA_LAUNCH
   BP_CUDA_TRY(cudaGetLastError());
