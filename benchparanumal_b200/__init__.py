@@ -49,7 +49,7 @@ EXPORTS = [
     "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc", "bp_ogs_check",
-    "bp_test_wait_timeout",
+    "bp_test_wait_timeout", "bp_tune_report", "bp_tune_reset",
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
@@ -163,6 +163,8 @@ def lib():
             "bp_box_vertices": [ctypes.POINTER(BoxDesc), vp, vp, vp],
             "bp_ogs_check": [ctypes.c_int64, vp, i32, vp, vp],
             "bp_test_wait_timeout": [ctypes.c_int],
+            "bp_tune_report": [i32] * 8 + [ctypes.POINTER(i32), ctypes.POINTER(i32), vp, vp, i32],
+            "bp_tune_reset": [],
             "bp_operator_hex3d_noalloc": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, i32, i32, vp,
                                           vp, vp, vp, vp],
             "bp_ax_cub_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
@@ -611,6 +613,23 @@ def basis_cubature(N):
     for k in ("invV", "Dmodal", "MM"):
         out[k] = out[k].reshape(Nq, Nq)
     return out
+
+
+FORMS = {0: "mma", 1: "tma", 2: "line", 3: "pencil"}
+
+
+def tune_report(kind, N, Nfields, affine, precision_bytes, lanes, fused, Nelements):
+    """(chosen form name or None, {form name: ms}) for an element-operator configuration."""
+    f, n = ctypes.c_int32(), ctypes.c_int32()
+    forms = np.zeros(8, np.int32)
+    ms = np.zeros(8, np.float32)
+    _check(lib().bp_tune_report(kind, N, Nfields, int(affine), precision_bytes, lanes, int(fused), Nelements,
+                                ctypes.byref(f), ctypes.byref(n), forms.ctypes.data, ms.ctypes.data, 8))
+    return (FORMS.get(f.value), {FORMS[int(forms[k])]: float(ms[k]) for k in range(n.value)})
+
+
+def tune_reset():
+    _check(lib().bp_tune_reset())
 
 
 def ogs_check(g2l, rowStarts, colIds, Ngather):

@@ -87,6 +87,26 @@ const char* bp_version(void) { return "benchparanumal_b200 0.1 (sm_100a)"; }
 
 int bp_test_wait_timeout(int withhold_slice) { return tma_wait_test(withhold_slice); }
 
+int bp_tune_report(int32_t kind, int32_t N, int32_t Nfields, int32_t affine, int32_t precision_bytes, int32_t lanes,
+                   int32_t fused, int32_t Nelements, int32_t* form, int32_t* nforms, int32_t* forms, float* ms,
+                   int32_t cap) {
+  if (!form || !nforms || (cap > 0 && (!forms || !ms))) return fail(BP_ERROR_ARG, "bp_tune_report: null pointer");
+  const TuneConfig c{kind, N + 1, Nfields, affine ? 1 : 0, precision_bytes, lanes, fused ? 1 : 0,
+                     element_class(Nelements)};
+  int f = -1, n = 0;
+  std::vector<int> fs(cap > 0 ? cap : 0);
+  BP_TRY(tuned_report(c, &f, &n, fs.data(), ms, cap));
+  *form = f;
+  *nforms = n;
+  for (int k = 0; k < n; ++k) forms[k] = fs[k];
+  return BP_SUCCESS;
+}
+
+int bp_tune_reset(void) {
+  tuned_clear();
+  return BP_SUCCESS;
+}
+
 int bp_platform_init(int device_id) {
   int n = 0;
   BP_CUDA_TRY(cudaGetDeviceCount(&n));
@@ -270,17 +290,8 @@ int bp_ax_hex3d_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Neleme
   if ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(Aq)) % (sizeof(float) * nrhs))
     return fail(BP_ERROR_ARG, "bp_ax_hex3d_f32_multi: q and Aq must be aligned to nrhs floats");
   const cudaStream_t s = to_stream(stream);
-  int rc = 1;
-  if (ax_variant() == AX_MMA)   // the tensor-core packed form only when asked for (slower at Nq = 8)
-    rc = launch_ax_mma_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, D, lambda, q, Aq,
-                              nullptr, nullptr, s, nullptr);
-  if (rc == 1)
-    rc = launch_ax_tma_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, D, lambda, q, Aq,
-                              nullptr, nullptr, s, nullptr);
-  if (rc == 1)
-    rc = launch_ax_line_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq,
-                               nullptr, nullptr, s, nullptr);
-  return rc;
+  return launch_ax_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq,
+                          nullptr, nullptr, s, nullptr);
 }
 
 int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream) {

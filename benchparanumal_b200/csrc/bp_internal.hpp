@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -286,10 +287,39 @@ int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
 int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                   const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
                   const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+// ---- kernel-form autotuner (bp_tune.cu) ----
+// Forms of the element operator; kind 0 = one value per node, 1 = packed lanes.
+enum { FORM_MMA = 0, FORM_TMA = 1, FORM_LINE = 2, FORM_PENCIL = 3 };
+struct TuneConfig {
+  int kind, nq, nf, affine, bytes, lanes, fused;
+  int ecls;   // size class: floor(log2(elements))
+};
+inline int element_class(int32_t E) {
+  int c = 0;
+  while (E > 1) {
+    E >>= 1;
+    ++c;
+  }
+  return c;
+}
+// The form to launch for configuration c: the tuned one once measured, else
+// (while s is capturing) forms[0].  run(f) launches form f on s and returns 1
+// when f does not apply.
+int tuned_form(const TuneConfig& c, const std::vector<int>& forms, const std::function<int(int)>& run,
+               cudaStream_t s, int* form);
+// the chosen form (-1: not tuned yet) and the measured times of configuration c
+int tuned_report(const TuneConfig& c, int* form, int* nforms, int* forms, float* ms, int cap);
+void tuned_clear();
+
 // Element-operator variant forced by BP_AX_VARIANT (pencil, line, tma, mma),
-// else AX_AUTO: the measured choice per configuration.
+// else AX_AUTO: the tuned choice per configuration.
 enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2, AX_MMA = 3, AX_TMA = 4 };
 int ax_variant();
+// the packed FP32 operator (2 or 4 rhs per node) in its tuned form (bp_kernels.cu)
+int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                     const int32_t* G2L, const float* wJ, const float* ggeo, const float* gllw, const float* D,
+                     float lambda, const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                     int* nblocks);
 // the packed FP32 stored-factor operator (4 rhs) at Nq = 8 on the tensor cores;
 // 1 when not covered
 int launch_ax_mma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,

@@ -188,30 +188,12 @@ int ax_variant() {   // read at every launch, so a process (a test) can switch f
   return s == "pencil" ? AX_PENCIL : s == "line" ? AX_LINE : s == "mma" ? AX_MMA : s == "tma" ? AX_TMA : AX_AUTO;
 }
 
+// The register-pencil form (FP64 affine default; any configuration)
 template <int NQ, class F>
-static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
-                        const int32_t* G2L, const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda,
-                        const F* q, F* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
+static int launch_pencil(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                         const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda, const F* q, F* Aq,
+                         const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   constexpr int EPB = AxShape<NQ>::EPB;
-  // Measured choices (40^3 or 24^3 boxes): stored factors take the TMA kernel
-  // where it applies (even Nq), else the line kernel (FP32 mixed BP5 to 1e-8:
-  // p=10 0.61 vs 1.15 s pencil, p=6 0.68 vs 0.84 s; FP64 BK5 p=6 0.6 vs 0.7 ms).
-  // Affine factors: the line kernel in FP32 (p=15: 4.28 vs 4.99 s), the pencil
-  // kernel in FP64 (BK5 p=7 0.6 vs 0.8 ms, BK6 p=15 7.4 vs 8.8 ms).
-  if (d.affine && (ax_variant() == AX_AUTO || ax_variant() == AX_MMA)) {
-    const int rc = launch_ax_mma(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s,
-                                 nblocks);
-    if (rc != 1) return rc;   // 1: not covered (Nq != 16)
-  }
-  if (ax_variant() == AX_LINE || (d.affine && sizeof(F) == 4 && ax_variant() != AX_PENCIL))
-    return launch_ax_line(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse, nblocks);
-  if (!d.affine && ax_variant() != AX_PENCIL) {
-    const int rc = launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s, nblocks);
-    if (rc != 1) return rc;   // 1: configuration not covered by the TMA kernel
-    if (ax_variant() == AX_AUTO)
-      return launch_ax_line(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse,
-                            nblocks);
-  }
   const dim3 block(NQ, NQ, EPB);
   const dim3 grid((Nelements + EPB - 1) / EPB);
   if (nblocks) *nblocks = (int)grid.x;
@@ -239,6 +221,108 @@ static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t*
 #undef BP_PENCIL
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
+}
+
+// One form of the element operator; 1 when it does not apply to d
+template <int NQ, class F>
+static int launch_ax_form(int form, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                          const int32_t* G2L, const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda,
+                          const F* q, F* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
+  switch (form) {
+    case FORM_MMA:
+      return launch_ax_mma(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s, nblocks);
+    case FORM_TMA:
+      return d.affine ? 1
+                      : launch_ax_tma(d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse, s,
+                                      nblocks);
+    case FORM_LINE:
+      return launch_ax_line(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, s, fuse, nblocks);
+    default:
+      return launch_pencil<NQ, F>(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s,
+                                  nblocks);
+  }
+}
+
+// The forms that may serve d, the measured static choice first (40^3 or 24^3
+// boxes): stored factors the TMA kernel where it applies (even Nq), else the
+// line kernel (FP32 mixed BP5 p=10: 0.61 vs 1.15 s pencil; FP64 BK5 p=6 0.6
+// vs 0.7 ms); affine factors the tensor-core kernel at Nq = 16 (BK6 p=15 FP64
+// 2.3 vs 7.5 ms, FP32 1.4 vs 4.0 ms), else the line kernel in FP32 and the
+// pencil kernel in FP64 (BK5 p=7 0.6 vs 0.8 ms).  The autotuner measures them
+// all on first use and keeps the fastest.
+template <int NQ, class F>
+static std::vector<int> ax_forms(const bp_ax_desc_t& d) {
+  std::vector<int> f;
+  if (d.affine) {
+    if (NQ == 16) f.push_back(FORM_MMA);
+    if (sizeof(F) == 4) {
+      f.push_back(FORM_LINE);
+      f.push_back(FORM_PENCIL);
+    } else {
+      f.push_back(FORM_PENCIL);
+      f.push_back(FORM_LINE);
+    }
+  } else {
+    f = {FORM_TMA, FORM_LINE, FORM_PENCIL};
+  }
+  return f;
+}
+
+template <int NQ, class F>
+static int launch_ax_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                        const int32_t* G2L, const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda,
+                        const F* q, F* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
+  const std::vector<int> forms = ax_forms<NQ, F>(d);
+  auto run = [&](int f, const int* sk) {
+    return launch_ax_form<NQ, F>(f, d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, sk, fuse, s,
+                                 nblocks);
+  };
+  int form = forms[0];
+  const int v = ax_variant();
+  if (v != AX_AUTO) {
+    form = v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : v == AX_LINE ? FORM_LINE : FORM_PENCIL;
+  } else {
+    const TuneConfig cfg{0, NQ, d.Nfields, d.affine, (int)sizeof(F), 1, fuse != nullptr, element_class(Nelements)};
+    BP_TRY(tuned_form(cfg, forms, [&](int f) { return run(f, nullptr); }, s, &form));
+  }
+  int rc = run(form, skip);
+  for (size_t k = 0; rc == 1 && k < forms.size(); ++k) rc = run(forms[k], skip);   // a forced form that does not apply
+  return rc == 1 ? fail(BP_ERROR_ARG, "element operator: no kernel form covers this configuration") : rc;
+}
+
+// The packed FP32 operator (pk right-hand sides per node, stored or affine
+// factors, one field) in its tuned form: TMA-staged (even Nq >= 8, the static
+// choice), line-per-thread (Nq <= 12), or tensor-core (Nq = 8, four lanes).
+int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                     const int32_t* G2L, const float* wJ, const float* ggeo, const float* gllw, const float* D,
+                     float lambda, const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                     int* nblocks) {
+  auto run = [&](int f, const int* sk) -> int {
+    switch (f) {
+      case FORM_MMA:
+        return launch_ax_mma_packed(pk, d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, sk, fuse, s,
+                                    nblocks);
+      case FORM_TMA:
+        return launch_ax_tma_packed(pk, d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, sk, fuse, s,
+                                    nblocks);
+      default:
+        if (d.N + 1 > 12) return 1;
+        return launch_ax_line_packed(pk, d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, sk, fuse,
+                                     s, nblocks);
+    }
+  };
+  const std::vector<int> forms = {FORM_TMA, FORM_LINE, FORM_MMA};
+  int form = forms[0];
+  const int v = ax_variant();
+  if (v != AX_AUTO) {
+    form = v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : FORM_LINE;
+  } else {
+    const TuneConfig cfg{1, d.N + 1, d.Nfields, d.affine, 4, pk, fuse != nullptr, element_class(Nelements)};
+    BP_TRY(tuned_form(cfg, forms, [&](int f) { return run(f, nullptr); }, s, &form));
+  }
+  int rc = run(form, skip);
+  for (size_t k = 0; rc == 1 && k < forms.size(); ++k) rc = run(forms[k], skip);
+  return rc == 1 ? fail(BP_ERROR_ARG, "packed element operator: no kernel form covers this configuration") : rc;
 }
 
 template <class F>

@@ -684,8 +684,19 @@ static int body32(bp_solver_s* S, void*, void*, cudaStream_t s) {
                                   s);
 }
 
+// One launch of the iteration's element operator outside any capture, on the
+// solver's scratch vectors: the autotuner measures the operator's forms here,
+// so the graphs captured next use the tuned one.
+template <class V>
+static int tune_elem(bp_solver_s* S, const ElemOperands<V>& o, V* p, V* AqL, cudaStream_t s) {
+  const CgFuse fuse{S->fuse_partials.ptr};
+  int nparts = 0;
+  return elem_apply<V>(S, o, p, AqL, nullptr, s, &fuse, &nparts);
+}
+
 static int ensure_graph(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
   if (S->graph && S->g_x == x && S->g_r == r) return BP_SUCCESS;
+  BP_TRY(tune_elem<double>(S, operands64(S), S->p.ptr, S->AqL.ptr, s));
   BP_TRY(capture(&S->graph, s, body64, S, x, r));
   S->g_x = x;
   S->g_r = r;
@@ -806,7 +817,10 @@ static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int max
                        double* hist_alpha, bp_solve_stats_t* stats, cudaStream_t s, bool record_events) {
   if (!(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_solver_solve: a mixed-precision solve needs tol > 0");
   BP_TRY(ensure_hist(S, maxit));
-  if (!S->graph32) BP_TRY(capture(&S->graph32, s, body32, S, nullptr, nullptr));
+  if (!S->graph32) {
+    BP_TRY(tune_elem<float>(S, operands32(S), S->p32.ptr, S->AqL32.ptr, s));
+    BP_TRY(capture(&S->graph32, s, body32, S, nullptr, nullptr));
+  }
   S->launches = 0;
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev0, s));
   BP_TRY(mixed_begin(S, x, r, tol, maxit, s));
@@ -1112,20 +1126,8 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   const ElemOperands<float> o = operands32(S);
   const CgFuse fuse{G->parts.ptr};
   int nparts = 0;
-  int rc = 1;
-  // The tensor-core packed form (Nq = 8, four lanes) only when asked for: it
-  // measured 1.40 ms per launch against the TMA form's 0.61 ms on the 40^3 p=7
-  // box (latency-bound: 16 warps per SM, five barriers per element).
-  if (ax_variant() == AX_MMA)
-    rc = launch_ax_mma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, (float)S->lambda,
-                              G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
-  if (rc == 1)
-    rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, (float)S->lambda,
-                              G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
-  if (rc == 1)   // no TMA form (odd Nq): the line-per-thread kernel
-    rc = launch_ax_line_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
-                               (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
-  BP_TRY(rc);
+  BP_TRY(launch_ax_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
+                          (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts));
   cg_alpha_kernel<PK><<<alpha_grid(nparts), kThreads, 0, s>>>(nparts, G->parts.ptr, G->sc, nullptr, G->gparts.ptr,
                                                                G->gcount.ptr);
   BP_CUDA_TRY(cudaGetLastError());
@@ -1207,6 +1209,21 @@ static int batch_join(bp_batch_s* B, cudaStream_t s) {
 // kBatchChunk iterations of one unit as a graph
 static int unit_capture(bp_batch_s* B, BatchUnit& u, cudaStream_t s) {
   if (u.graph) return BP_SUCCESS;
+  // the element operator once outside the capture: the autotuner picks its form
+  if (u.G) {
+    CgGroup* G = u.G;
+    bp_solver_s* S = G->base;
+    bp_mesh_s* m = S->mesh;
+    const ElemOperands<float> o = operands32(S);
+    const CgFuse fuse{G->parts.ptr};
+    int nparts = 0;
+    BP_TRY(launch_ax_packed(G->pk, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
+                            (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts));
+  } else {
+    bp_solver_s* S = B->sys_solver[u.sys];
+    if (B->mixed) BP_TRY(tune_elem<float>(S, operands32(S), S->p32.ptr, S->AqL32.ptr, s));
+    else BP_TRY(tune_elem<double>(S, operands64(S), S->p.ptr, S->AqL.ptr, s));
+  }
   cudaGraph_t g;
   BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int rc = BP_SUCCESS;

@@ -404,6 +404,32 @@ int bp_batch_solver(bp_batch_t batch, int32_t system, bp_solver_t* solver);
 int bp_driver_main(const char* name, int argc, char** argv);
 
 /* ---------------------------------------------------------------------------
+ * Kernel-form autotuner (extension: the reference picks its OKL variant by a
+ * compile-time rule on the degree, okl/bp5AxHex3D.okl:27-41).  The element
+ * operator has several forms; the first launch of a configuration outside a
+ * stream capture times every applicable form on the caller's operands (one
+ * untimed and three timed launches each) and keeps the fastest for that
+ * configuration and element-count class (floor(log2(Nelements))) on the
+ * device.  Solvers launch their operator once before capturing their graphs.
+ * While a stream captures, an untuned configuration takes the measured static
+ * choice.  BP_AUTOTUNE=0 in the environment keeps the static choice.
+ * ------------------------------------------------------------------------- */
+#define BP_FORM_MMA 0     /* tensor-core MMA (affine Nq = 16; packed Nq = 8) */
+#define BP_FORM_TMA 1     /* TMA-staged register pencils (stored factors, even Nq) */
+#define BP_FORM_LINE 2    /* line-per-thread */
+#define BP_FORM_PENCIL 3  /* register pencil */
+
+/* The form chosen for a configuration (-1 when not tuned yet) and the forms
+   measured with their times in ms (up to cap entries).  kind 0: one value per
+   node (precision_bytes 8 or 4); kind 1: `lanes` packed FP32 right-hand sides.
+   fused: 1 for the CG launches that also form p.Ap. */
+int bp_tune_report(int32_t kind, int32_t N, int32_t Nfields, int32_t affine, int32_t precision_bytes, int32_t lanes,
+                   int32_t fused, int32_t Nelements, int32_t* form, int32_t* nforms, int32_t* forms, float* ms,
+                   int32_t cap);
+/* Forget every tuned choice (the next launches measure again). */
+int bp_tune_reset(void);
+
+/* ---------------------------------------------------------------------------
  * Validation and failure detection.
  * ------------------------------------------------------------------------- */
 

@@ -1,0 +1,67 @@
+"""The element-operator autotuner (bp_tune.cu).
+
+The first launch of a configuration outside a capture measures every form
+that applies and keeps the fastest; BP_AUTOTUNE=0 keeps the measured static
+choice; a solver launches its operator once before capturing its graphs, so
+the graphs use the tuned form; results do not depend on the form (within the
+parity bars).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("N,affine,nforms", [(7, False, 3), (4, False, 2), (4, True, 2), (15, True, 3)])
+def test_first_launch_measures_every_form_and_keeps_the_fastest(gpu, oracle, N, affine, nforms):
+    gpu.tune_reset()
+    nx = 3 if N < 15 else 2
+    gm = gpu.Mesh(nx, nx, 2, N=N, affine=affine, pert=0.0 if affine else 0.1)
+    om = oracle.Mesh(nx, nx, 2, N, affine=affine, pert=0.0 if affine else 0.1)
+    q = 2 * oracle.random(5, om.Ngather) - 1
+    dq, dA = gpu.DeviceBuffer.from_host(q), gpu.DeviceBuffer(om.NL)
+    gpu.ax_hex3d(gm, dq, dA)
+    form, times = gpu.tune_report(0, N, 1, affine, 8, 1, 0, gm.E)
+    # the stored-factor TMA form needs even Nq: at N=4 only the line and pencil forms apply
+    assert len(times) == nforms, times
+    assert form == min(times, key=times.get)
+    assert rel(dA.download(), om.ax(q)) <= 1e-12
+
+
+def test_static_choice_when_autotuning_is_off(gpu, monkeypatch):
+    monkeypatch.setenv("BP_AUTOTUNE", "0")
+    gpu.tune_reset()
+    gm = gpu.Mesh(3, 3, 2, N=7, pert=0.1)
+    dq, dA = gpu.DeviceBuffer.from_host(np.ones(gm.Ngather)), gpu.DeviceBuffer(gm.NL)
+    gpu.ax_hex3d(gm, dq, dA)
+    form, times = gpu.tune_report(0, 7, 1, False, 8, 1, 0, gm.E)
+    assert form == "tma" and times == {}
+    monkeypatch.delenv("BP_AUTOTUNE")
+    gpu.tune_reset()
+
+
+def test_solver_graphs_use_the_tuned_form(gpu, oracle):
+    gpu.tune_reset()
+    gm = gpu.Mesh(4, 4, 4, N=7, pert=0.1)
+    om = oracle.Mesh(4, 4, 4, 7, pert=0.1)
+    S = gpu.BP(gm, precon="JACOBI")
+    x = gpu.DeviceBuffer.from_host(np.zeros(gm.Ngather))
+    st, hr, _ = S.solve(x, S.rhs("RANDOM", 0), tol=0.0, maxit=30)
+    form, times = gpu.tune_report(0, 7, 1, False, 8, 1, 1, gm.E)   # the fused CG launch
+    assert form is not None and len(times) == 3
+    _, b_o = om.rhs_random(0)
+    _, _, _, hr_o, _ = om.cg(b_o, 1.0, 0.0, 30, precon=True)
+    assert np.max(np.abs(hr - hr_o) / hr_o) < 1e-10
+
+
+def test_packed_group_is_tuned(gpu):
+    gpu.tune_reset()
+    B = gpu.Batch([{"nx": 4, "N": 7, "pert": 0.1, "nrhs": 4, "rhs_seed": 0}], precon="JACOBI", precision="MIXED")
+    stats, _ = B.solve(tol=1e-8, maxit=3000)
+    assert all(np.sqrt(s.rdotr / s.rdotr0) <= 1e-8 for s in stats)
+    form, times = gpu.tune_report(1, 7, 1, False, 4, 4, 1, 64)
+    assert form in ("tma", "line", "mma") and set(times) == {"tma", "line", "mma"}
