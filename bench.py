@@ -421,35 +421,54 @@ def main():
     plain["fixed_100_iterations_gdof_it_s"] = world * Nd * ITERS / (st100.elapsed_ms / 1e3) / 1e9
 
     # ---- dominant kernel of the step: the packed FP32 element operator on the four
-    # right-hand sides (what the batched solve launches), timed alone ----
+    # right-hand sides (what each iteration of the batched solve launches), timed
+    # alone; beside it the same operator with the CG direction update fused in
+    # (bp_cg_direction_ax_f32_multi, opt-in in the solver: slower, measured) ----
     v = mesh.view
     ng = mesh.E * mesh.Np
     ops = {"wJ": bp.DeviceBuffer(ng, np.float32), "ggeo": bp.DeviceBuffer(6 * ng, np.float32),
            "gllw": bp.DeviceBuffer(mesh.Nq, np.float32), "D": bp.DeviceBuffer(mesh.Nq * mesh.Nq, np.float32)}
     for name, n in (("wJ", ng), ("ggeo", 6 * ng), ("gllw", mesh.Nq), ("D", mesh.Nq * mesh.Nq)):
         bp.convert_f64_f32(getattr(v, name), n, ops[name])
-    q32 = bp.DeviceBuffer(Nd * NRHS, np.float32)
     b32 = bp.DeviceBuffer(Nd, np.float32)
     bp.convert_f64_f32(b0, Nd, b32)
-    q32.upload(np.repeat(b32.download(), NRHS))   # interleaved: row r, system k at r*NRHS + k
+    packed = np.repeat(b32.download(), NRHS)   # interleaved: row r, system k at r*NRHS + k
+    vec = {k: bp.DeviceBuffer.from_host(packed) for k in ("r", "p0", "p1", "x")}
+    invD32 = bp.DeviceBuffer.from_host(np.full(Nd, 0.5, np.float32))
+    own = bp.DeviceBuffer(mesh.NL, np.int32)
+    bp.ogs_owner_map(mesh, own)
+    parts = bp.DeviceBuffer((mesh.E + 1) * NRHS)
     AqL = bp.DeviceBuffer(mesh.NL * NRHS, np.float32)
-    for _ in range(3):
-        bp.ax_hex3d_f32_multi(mesh, NRHS, q32, AqL, ops)
-    a0, a1 = ev(), ev()
-    bp._check(L.bp_event_record(a0, None))
-    for _ in range(args.ax_launches):
-        bp.ax_hex3d_f32_multi(mesh, NRHS, q32, AqL, ops)
-    bp._check(L.bp_event_record(a1, None))
-    bp._check(L.bp_event_elapsed_ms(a0, a1, bp.ctypes.byref(ms)))
-    ax_s = ms.value / 1e3 / args.ax_launches
+    coef_a, coef_b = [1e-3] * NRHS, [0.5] * NRHS
+
+    def fused():
+        bp.cg_direction_ax_f32_multi(mesh, NRHS, own, ops, coef_a, coef_b, vec["r"], invD32, vec["p0"], vec["p1"],
+                                     vec["x"], AqL, parts)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        a0, a1 = ev(), ev()
+        bp._check(L.bp_event_record(a0, None))
+        for _ in range(args.ax_launches):
+            fn()
+        bp._check(L.bp_event_record(a1, None))
+        bp._check(L.bp_event_elapsed_ms(a0, a1, bp.ctypes.byref(ms)))
+        return ms.value / 1e3 / args.ax_launches
+
+    fused_s = timed(fused)
+    ax_s = timed(lambda: bp.ax_hex3d_f32_multi(mesh, NRHS, vec["p1"], AqL, ops))
     E, Np = mesh.E, mesh.Np
-    # reference model with 4-byte values, the q and Aq terms once per right-hand side
+    # reference model of the operator with 4-byte values, the q and Aq terms once per
+    # right-hand side; the fused step adds the direction update's vectors: r, x
+    # (read and write) and the new p per system, invD once
     ax_bytes = ax_model_bytes(Nd, E, Np, s=4) + (NRHS - 1) * (Nd * 4 + E * Np * 4)
+    fused_bytes = ax_bytes + NRHS * Nd * 4 * 4 + Nd * 4
     peak, peak_kind = read_peaks()
     achieved = ax_bytes / ax_s / 1e9
     smem_mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
     smem_bound_ms = AX_SMEM_WAVEFRONTS / (B200_SMS * smem_mhz * 1e6) * 1e3
-    del AqL, ops, q32, b32
+    del AqL, ops, vec, invD32, own, parts, b32
 
     # free the headline's buffers before the other configurations
     del S, b0, x, r, Ax, xd, mesh, B
@@ -485,6 +504,9 @@ def main():
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes,
                          "launch_ms": ax_s * 1e3,
+                         "fused_direction_step": {"kernel": "bp_cg_direction_ax_f32_multi (4 rhs)",
+                                                  "launch_ms": fused_s * 1e3, "algorithmic_bytes": fused_bytes,
+                                                  "achieved": fused_bytes / fused_s / 1e9},
                          # the roof that binds this kernel: shared-memory wavefronts at one per SM and clock
                          # (clock: the median SM clock sampled during the timed step, else the maximum)
                          "smem": {"wavefronts": AX_SMEM_WAVEFRONTS, "sm_mhz": smem_mhz,

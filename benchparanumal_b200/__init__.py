@@ -53,7 +53,8 @@ EXPORTS = [
     "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
-    "bp_ax_cub_hex3d_f32", "bp_mesh_write_vtu",
+    "bp_ax_cub_hex3d_f32", "bp_mesh_write_vtu", "bp_ogs_owner_map", "bp_cg_direction_ax_hex3d",
+    "bp_cg_direction_ax_f32_multi",
 ]
 
 
@@ -185,6 +186,11 @@ def lib():
             "bp_ax_cub_hex3d_f32": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_float, vp, vp,
                                     vp],
             "bp_mesh_write_vtu": [vp, vp, ctypes.c_char_p],
+            "bp_ogs_owner_map": [i32, vp, i32, vp, vp, vp, vp],
+            "bp_cg_direction_ax_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, dbl, dbl, dbl, vp, vp, vp,
+                                         vp, vp, vp, vp, vp],
+            "bp_cg_direction_ax_f32_multi": [ctypes.POINTER(AxDesc), i32, i32, vp, vp, vp, vp, vp, ctypes.c_float,
+                                             vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -398,6 +404,42 @@ def ax_hex3d_f32_multi(mesh, nrhs, q, Aq, ops, lam=1.0, stream=None):
     _check(lib().bp_ax_hex3d_f32_multi(ctypes.byref(d), nrhs, mesh.E, v.elementList, v.GlobalToLocal,
                                        _ptr(ops["wJ"]), _ptr(ops["ggeo"]), _ptr(ops["gllw"]), _ptr(ops["D"]),
                                        float(lam), _ptr(q), _ptr(Aq), stream))
+
+
+OWNER_BIT = 1 << 30
+
+
+def ogs_owner_map(mesh, out, stream=None):
+    """bp_ogs_owner_map: GlobalToLocal of the mesh with OWNER_BIT on the first
+    local node of every gathered row, into the int32 device buffer `out`."""
+    v = mesh.view
+    _check(lib().bp_ogs_owner_map(mesh.NL, v.GlobalToLocal, mesh.Ngather, v.rowStarts, v.colIds, _ptr(out), stream))
+
+
+def cg_direction_ax(mesh, owner, alpha, beta, r, invD, p_old, p_new, x, Aq, partials, lam=1.0, stream=None):
+    """bp_cg_direction_ax_hex3d (FP64): p_new = invD r + beta p_old (beta = 0:
+    p_new = invD r), x += alpha p_old (alpha = 0: x untouched), Aq = A_e
+    p_new[G2L], p.Ap block partials; invD None means z = r."""
+    v = mesh.view
+    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    _check(lib().bp_cg_direction_ax_hex3d(ctypes.byref(d), mesh.E, v.elementList, _ptr(owner), v.wJ, v.ggeo, v.D,
+                                          float(lam), float(alpha), float(beta), _ptr(r),
+                                          _ptr(invD) if invD is not None else None, _ptr(p_old), _ptr(p_new), _ptr(x),
+                                          _ptr(Aq), _ptr(partials), stream))
+
+
+def cg_direction_ax_f32_multi(mesh, nrhs, owner, ops, alpha, beta, r, invD, p_old, p_new, x, Aq, partials, lam=1.0,
+                              stream=None):
+    """bp_cg_direction_ax_f32_multi: the fused step in FP32 on nrhs interleaved
+    systems; alpha, beta: sequences of nrhs coefficients."""
+    v = mesh.view
+    d = AxDesc(5, mesh.N, int(mesh.affine), 1)
+    a = (ctypes.c_double * nrhs)(*[float(t) for t in alpha])
+    b = (ctypes.c_double * nrhs)(*[float(t) for t in beta])
+    _check(lib().bp_cg_direction_ax_f32_multi(ctypes.byref(d), nrhs, mesh.E, v.elementList, _ptr(owner),
+                                              _ptr(ops["wJ"]), _ptr(ops["ggeo"]), _ptr(ops["D"]), float(lam), a, b,
+                                              _ptr(r), _ptr(invD) if invD is not None else None, _ptr(p_old),
+                                              _ptr(p_new), _ptr(x), _ptr(Aq), _ptr(partials), stream))
 
 
 def ogs_gather(mesh, v, gv, stream=None):

@@ -182,12 +182,21 @@ struct TmaMinBlocks {
 // WITHHOLD >= 0 builds the test-only form: the producer arms the mbarrier of
 // that slice but issues none of its copies, so the wait on it runs out (after
 // the short test limit) with nothing in flight.
-template <int NQ, int NF, bool DOT, int R, class F, class T, int WITHHOLD = -1>
+//
+// DIR builds the form with the CG direction update fused in (CgFuse::dir): q
+// is not read, the pencil is p_k formed from p_{k-1}, r and invD, and the
+// owners of the element's nodes write p_k and the deferred x update.
+template <int NQ, int NF, bool DOT, int R, class F, class T, int WITHHOLD = -1, bool DIR = false>
 __global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF, (TmaMinBlocks<NQ, NF, F, T>::V))
 ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
               const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
               const T* __restrict__ q, T* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
   if (skip && *skip) return;
+  DirStep<PackTraits<T>::R, F> ds;
+  if (DIR) {
+    ds.load(fuse);
+    if (!ds.any) return;   // every lane has finished (grid-uniform)
+  }
   using Sh = TmaShape<NQ, F>;
   using Lay = TmaSmem<NQ, NF, R, F, T>;
   using V2 = typename Vec2<F>::type;
@@ -234,7 +243,53 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
   // the pencil of q and the D rows of this thread, while the copies fly
   const size_t lbase = ((size_t)e * NF + f) * NP + j * NQ + i;
   T r_u[NQ], r_Au[NQ];
-  {
+  if (DIR) {
+    const bool odd = (ds.gen & 1) != 0;   // selects, not indexes: no local-memory copy of the parameters
+    const T* pold = static_cast<const T*>(odd ? fuse.pbuf[1] : fuse.pbuf[0]);
+    T* pnew = static_cast<T*>(odd ? fuse.pbuf[0] : fuse.pbuf[1]);
+    const T* rv = static_cast<const T*>(fuse.r);
+    const F* dv = static_cast<const F*>(fuse.invD);
+    T* xv = static_cast<T*>(fuse.x);
+    int id[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) id[k] = active ? __ldg(G2L + lbase + k * NQ2) : -1;
+    // every load of the pencil is issued before any store: p_old, r and invD
+    // are read-only here (non-coherent loads), x is read at owned nodes only
+    T po[NQ], xo[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      const int g = id[k] & kIdMask;
+      po[k] = id[k] >= 0 ? ldg_val(pold + g) : pack_zero<T>();
+      r_u[k] = id[k] >= 0 ? ldg_val(rv + g) : pack_zero<T>();
+    }
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      const int g = id[k] & kIdMask;
+      const F d = (dv && id[k] >= 0) ? ldg_val(dv + g) : F(1);
+#pragma unroll
+      for (int l = 0; l < PackTraits<T>::R; ++l) {
+        const F z = d * lane(r_u[k], l);
+        lane_set(r_u[k], l, ds.act[l] ? (ds.first[l] ? z : z + ds.beta[l] * lane(po[k], l)) : lane(po[k], l));
+      }
+      r_Au[k] = pack_zero<T>();
+    }
+    if (ds.anyx) {
+#pragma unroll
+      for (int k = 0; k < NQ; ++k)
+        xo[k] = (id[k] >= 0 && (id[k] & kOwnerBit)) ? xv[id[k] & kIdMask] : pack_zero<T>();
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        if (id[k] < 0 || !(id[k] & kOwnerBit)) continue;
+#pragma unroll
+        for (int l = 0; l < PackTraits<T>::R; ++l)
+          if (ds.addx[l]) lane_set(xo[k], l, ds.alpha[l] * lane(po[k], l) + F(1) * lane(xo[k], l));
+        xv[id[k] & kIdMask] = xo[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NQ; ++k)
+      if (id[k] >= 0 && (id[k] & kOwnerBit)) pnew[id[k] & kIdMask] = r_u[k];
+  } else {
     int id[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) id[k] = active ? __ldg(G2L + lbase + k * NQ2) : -1;
@@ -347,7 +402,7 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
   }
 }
 
-template <int NQ, int NF, bool DOT, class F, class T>
+template <int NQ, int NF, bool DOT, class F, class T, bool DIR = false>
 static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ,
                           const F* ggeo, const F* D, F lambda, const T* q, T* Aq, const int* skip,
                           const CgFuse& fuse, cudaStream_t s, int* nblocks) {
@@ -356,7 +411,7 @@ static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const i
   const size_t smem = TmaSmem<NQ, NF, R, F, T>::BYTES;
   static DeviceOnce configured;   // the shared-memory attribute is set once per device
   BP_TRY(once_per_device(configured, [smem]() -> int {
-    BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, NF, DOT, R, F, T>,
+    BP_CUDA_TRY(cudaFuncSetAttribute(ax_tma_kernel<NQ, NF, DOT, R, F, T, -1, DIR>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return BP_SUCCESS;
   }));
@@ -366,8 +421,8 @@ static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const i
   const dim3 block(NQ, NQ, Sh::EPB * NF);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
-  ax_tma_kernel<NQ, NF, DOT, R, F, T><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda,
-                                                                q, Aq, skip, fuse);
+  ax_tma_kernel<NQ, NF, DOT, R, F, T, -1, DIR><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D,
+                                                                         lambda, q, Aq, skip, fuse);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
@@ -376,6 +431,9 @@ template <int NQ, int NF, class F, class T>
 static int launch_tma(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ, const F* ggeo,
                       const F* D, F lambda, const T* q, T* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                       int* nblocks) {
+  if (fuse && fuse->dir)
+    return launch_tma_dot<NQ, NF, true, F, T, true>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip,
+                                                    *fuse, s, nblocks);
   if (fuse)
     return launch_tma_dot<NQ, NF, true, F, T>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, *fuse,
                                               s, nblocks);
@@ -497,6 +555,13 @@ static int launch_ax_tma_pk(const bp_ax_desc_t& d, int32_t Nelements, const int3
     default:
       return 1;
   }
+}
+
+bool tma_covers(const bp_ax_desc_t& d, int lanes) {
+  const int NQ = d.N + 1;
+  if (d.affine || NQ % 2 != 0) return false;
+  if (lanes > 1) return d.Nfields == 1 && (lanes == 2 || lanes == 4) && NQ >= 8 && NQ <= 12;
+  return d.Nfields == 1 ? NQ <= 16 : (d.Nfields == 3 && NQ <= 10);
 }
 
 int launch_ax_tma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,

@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 
+#include "bp_cg_device.cuh"
 #include "bp_internal.hpp"
 
 namespace bp {
@@ -292,6 +293,89 @@ int bp_ax_hex3d_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Neleme
   const cudaStream_t s = to_stream(stream);
   return launch_ax_packed(nrhs, *desc, Nelements, elementList, GlobalToLocal, wJ, ggeo, gllw, D, lambda, q, Aq,
                           nullptr, nullptr, s, nullptr);
+}
+
+int bp_ogs_owner_map(int32_t NL, const int32_t* GlobalToLocal, int32_t Ngather, const int32_t* rowStarts,
+                     const int32_t* colIds, int32_t* ownerMap, bp_stream_t stream) {
+  if (NL < 0 || Ngather < 0) return fail(BP_ERROR_ARG, "bp_ogs_owner_map: negative size");
+  if (Ngather >= kOwnerBit) return fail(BP_ERROR_ARG, "bp_ogs_owner_map: Ngather must be below BP_OWNER_BIT");
+  if ((NL && (!GlobalToLocal || !ownerMap)) || (Ngather && (!rowStarts || !colIds)))
+    return fail(BP_ERROR_ARG, "bp_ogs_owner_map: null array");
+  return launch_owner_map((size_t)NL, GlobalToLocal, Ngather, rowStarts, colIds, ownerMap, to_stream(stream));
+}
+
+// the fused step's common checks; lanes = values per node
+static int check_dir_args(const char* who, const bp_ax_desc_t* desc, int lanes, int32_t Nelements,
+                          const void* elementList, const void* ownerMap, const void* wJ, const void* ggeo,
+                          const void* D, const void* r, const void* p_old, const void* p_new, const void* x,
+                          const void* Aq, const void* partials) {
+  BP_TRY(check_ax_desc(desc));
+  if (Nelements < 0) return fail(BP_ERROR_ARG, std::string(who) + ": negative element count");
+  if (desc->bp < 5 || !tma_covers(*desc, lanes))
+    return fail(BP_ERROR_ARG, std::string(who) + ": the fused step covers stored factors at even Nq (packed: Nq 8..12, "
+                                                 "one field; single: Nq <= 16, or <= 10 with three fields)");
+  // the gathered vectors are only read at unmasked nodes: a mesh without any may pass NULL
+  if (Nelements && (!elementList || !ownerMap || !wJ || !ggeo || !D || !Aq || !partials))
+    return fail(BP_ERROR_ARG, std::string(who) + ": null array");
+  if (p_old && p_old == p_new) return fail(BP_ERROR_ARG, std::string(who) + ": p_new must not alias p_old");
+  return BP_SUCCESS;
+}
+
+int bp_cg_direction_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                             const int32_t* ownerMap, const double* wJ, const double* ggeo, const double* D,
+                             double lambda, double alpha, double beta, const double* r, const double* invD,
+                             const double* p_old, double* p_new, double* x, double* Aq, double* pAp_partials,
+                             bp_stream_t stream) {
+  BP_TRY(check_dir_args("bp_cg_direction_ax_hex3d", desc, 1, Nelements, elementList, ownerMap, wJ, ggeo, D, r,
+                        p_old, p_new, x, Aq, pAp_partials));
+  if (Nelements == 0) return BP_SUCCESS;
+  CgFuse f;
+  f.partials = pAp_partials;
+  f.dir = 1;
+  f.pbuf[0] = const_cast<double*>(p_old);
+  f.pbuf[1] = p_new;
+  f.r = r;
+  f.invD = invD;
+  f.x = x;
+  f.alpha[0] = alpha;
+  f.beta[0] = beta;
+  const int rc = launch_ax_tma(*desc, Nelements, elementList, ownerMap, wJ, ggeo, D, lambda, nullptr, Aq, nullptr,
+                               &f, to_stream(stream), nullptr);
+  return rc == 1 ? fail(BP_ERROR_ARG, "bp_cg_direction_ax_hex3d: factor arrays must be 16-byte aligned") : rc;
+}
+
+int bp_cg_direction_ax_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Nelements,
+                                 const int32_t* elementList, const int32_t* ownerMap, const float* wJ,
+                                 const float* ggeo, const float* D, float lambda, const double* alpha,
+                                 const double* beta, const float* r, const float* invD, const float* p_old,
+                                 float* p_new, float* x, float* Aq, double* pAp_partials, bp_stream_t stream) {
+  if (nrhs != 1 && nrhs != 2 && nrhs != 4)
+    return fail(BP_ERROR_ARG, "bp_cg_direction_ax_f32_multi: nrhs must be 1, 2 or 4");
+  if (!alpha || !beta) return fail(BP_ERROR_ARG, "bp_cg_direction_ax_f32_multi: null coefficients");
+  BP_TRY(check_dir_args("bp_cg_direction_ax_f32_multi", desc, nrhs, Nelements, elementList, ownerMap, wJ, ggeo, D, r,
+                        p_old, p_new, x, Aq, pAp_partials));
+  if (Nelements == 0) return BP_SUCCESS;
+  if ((reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(p_old) | reinterpret_cast<uintptr_t>(p_new) |
+       reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(Aq)) % (sizeof(float) * nrhs))
+    return fail(BP_ERROR_ARG, "bp_cg_direction_ax_f32_multi: vectors must be aligned to nrhs floats");
+  CgFuse f;
+  f.partials = pAp_partials;
+  f.dir = 1;
+  f.pbuf[0] = const_cast<float*>(p_old);
+  f.pbuf[1] = p_new;
+  f.r = r;
+  f.invD = invD;
+  f.x = x;
+  for (int k = 0; k < nrhs; ++k) {
+    f.alpha[k] = alpha[k];
+    f.beta[k] = beta[k];
+  }
+  const cudaStream_t s = to_stream(stream);
+  const int rc = nrhs == 1 ? launch_ax_tma(*desc, Nelements, elementList, ownerMap, wJ, ggeo, D, lambda, nullptr, Aq,
+                                           nullptr, &f, s, nullptr)
+                           : launch_ax_tma_packed(nrhs, *desc, Nelements, elementList, ownerMap, wJ, ggeo, D, lambda,
+                                                  nullptr, Aq, nullptr, &f, s, nullptr);
+  return rc == 1 ? fail(BP_ERROR_ARG, "bp_cg_direction_ax_f32_multi: factor arrays must be 16-byte aligned") : rc;
 }
 
 int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream) {

@@ -25,14 +25,84 @@ struct CgScalars {
   int mixed;          // 1 in a mixed-precision solve
   int skip_x;         // 1: the last iteration's x update has been applied already
   int update;         // mixed: 1 asks the host for a reliable update
+  int gen;            // completed gather-updates (never reset): the current direction p of an operator
+                      // with the fused direction update lives in pbuf[gen & 1] (CgFuse)
 };
 
 // Where an element-operator launch inside CG leaves p.Ap.  Because
 // A = sum_e Q_e^T A_e Q_e, p.Ap = sum_e (Q_e p).(A_e Q_e p): each block adds up
 // q*Aq over its own nodes and stores the sum in partials[blockIdx.x];
 // cg_alpha_kernel then adds the partials in index order and forms alpha.
+//
+// With `dir` set, the operator also does the CG direction update of its step
+// (the work of cg_direction_kernel): it does not read q but, at every node it
+// reads, forms p_k = z + beta p_{k-1} (z = invD r, or r) from p_{k-1} in
+// pbuf[gen & 1], works on p_k, and at the nodes it owns -- GlobalToLocal
+// entries carrying kOwnerBit, one local node per gathered node -- writes p_k
+// to pbuf[(gen + 1) & 1] and applies the deferred x += alpha_{k-1} p_{k-1}.
+// The two buffers keep p_{k-1} intact while other elements still read it; the
+// gather-update that ends the step advances gen.  Per lane l the scalars are
+// sc[l]; gen is the first lane's.
+//
+// Outside a CG solve (sc null) the step is given by value: lane l has
+// coefficients alpha[l], beta[l] (beta[l] = 0 forms p = z, the first step;
+// alpha[l] = 0 leaves x alone), p_{k-1} is pbuf[0] and p_k goes to pbuf[1].
+constexpr int kMaxLanes = 4;
 struct CgFuse {
-  double* partials;        // [number of blocks of the operator launch]
+  double* partials = nullptr;   // [number of blocks of the operator launch]
+  int dir = 0;
+  void* pbuf[2] = {nullptr, nullptr};
+  const void* r = nullptr;
+  const void* invD = nullptr;   // null: no preconditioner (z = r)
+  void* x = nullptr;
+  const CgScalars* sc = nullptr;
+  double alpha[kMaxLanes] = {0, 0, 0, 0}, beta[kMaxLanes] = {0, 0, 0, 0};
+};
+
+// GlobalToLocal entries of an operator with the fused direction update:
+// the gathered index in the low bits, kOwnerBit on the one local node of each
+// gathered node that writes it (the first column of its CSR row); -1 masked.
+constexpr int32_t kOwnerBit = 0x40000000;
+constexpr int32_t kIdMask = kOwnerBit - 1;
+
+// The step's per-lane scalars of the fused direction update (the values
+// cg_direction_kernel and grp_direction_kernel use).
+template <int L, class F>
+struct DirStep {
+  bool act[L], first[L], addx[L];
+  F alpha[L], beta[L];
+  bool any, anyx;
+  int gen;
+  __device__ __forceinline__ void load(const CgFuse& fz) {
+    any = anyx = false;
+    if (!fz.sc) {   // coefficients by value
+      gen = 0;
+      any = true;
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        act[l] = true;
+        first[l] = fz.beta[l] == 0.0;
+        addx[l] = fz.alpha[l] != 0.0;
+        anyx = anyx || addx[l];
+        alpha[l] = (F)fz.alpha[l];
+        beta[l] = (F)fz.beta[l];
+      }
+      return;
+    }
+    const CgScalars* sc = fz.sc;
+    gen = sc[0].gen;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const CgScalars& c = sc[l];
+      act[l] = !c.done;
+      any = any || act[l];
+      first[l] = c.iter == 0;
+      addx[l] = act[l] && c.iter > 0 && !c.skip_x;
+      anyx = anyx || addx[l];
+      alpha[l] = (F)c.alpha;
+      beta[l] = first[l] ? F(0) : (F)(c.precon ? c.rz / c.rz_prev : c.rdotr / c.rdotr_prev);
+    }
+  }
 };
 
 // Sum of v over the block in a fixed order, valid in thread 0.  `scratch`

@@ -159,6 +159,9 @@ struct bp_mesh_s {
   int N, Nq, Np, E, Nfields, affine;
   int32_t Ngather, nnz;
   bp::DeviceArray<int32_t> elementList, G2L, rowStarts, colIds;
+  // GlobalToLocal with the owner bit (kOwnerBit) of each gathered node's first
+  // local node, for operators with the fused CG direction update; built on first use
+  bp::DeviceArray<int32_t> G2Lo;
   bp::DeviceArray<double> wJ, ggeo, D, gllz, gllw, EX, EY, EZ;
   // cubature of the BP1-BP4 operators (bp_mesh_cubature); cubNq = 0 until set up
   int cubNq = 0;
@@ -326,6 +329,15 @@ int launch_ax_mma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const
                          const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
                          const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                          int* nblocks);
+// whether the TMA form covers d with `lanes` values per node (1, or 2 or 4
+// packed FP32 lanes); with factor arrays 16-byte aligned
+bool tma_covers(const bp_ax_desc_t& d, int lanes);
+// the form a CG launch of the element operator (p.Ap fused) of d takes now:
+// forced by BP_AX_VARIANT, tuned, or the static choice while untuned
+int ax_current_form(const bp_ax_desc_t& d, int bytes, int lanes, int32_t Nelements);
+// G2Lo = G2L (NL entries) with kOwnerBit on the first column of every CSR row
+int launch_owner_map(size_t NL, const int32_t* G2L, int32_t Ngather, const int32_t* rowStarts, const int32_t* colIds,
+                     int32_t* G2Lo, cudaStream_t s);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

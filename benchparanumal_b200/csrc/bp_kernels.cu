@@ -325,6 +325,22 @@ int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int
   return rc == 1 ? fail(BP_ERROR_ARG, "packed element operator: no kernel form covers this configuration") : rc;
 }
 
+int ax_current_form(const bp_ax_desc_t& d, int bytes, int lanes, int32_t Nelements) {
+  const int v = ax_variant();
+  if (lanes > 1) {
+    if (v != AX_AUTO) return v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : FORM_LINE;
+  } else if (v != AX_AUTO) {
+    return v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : v == AX_LINE ? FORM_LINE : FORM_PENCIL;
+  }
+  const TuneConfig cfg{lanes > 1 ? 1 : 0, d.N + 1, d.Nfields, d.affine, bytes, lanes, 1, element_class(Nelements)};
+  int form = -1, n = 0, forms[8];
+  float ms[8];
+  if (tuned_report(cfg, &form, &n, forms, ms, 8) == BP_SUCCESS && form >= 0) return form;
+  // the static choice (first of the candidate lists above)
+  if (lanes > 1 || !d.affine) return FORM_TMA;
+  return d.N + 1 == 16 ? FORM_MMA : (bytes == 4 ? FORM_LINE : FORM_PENCIL);
+}
+
 template <class F>
 static int launch_ax_t(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                        const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda, const F* q, F* Aq,

@@ -69,6 +69,37 @@ __device__ __forceinline__ F lane(const Pack<F, R>& a, int l) {
   return a.v[l];
 }
 
+// read-only load through the non-coherent path: the compiler may move it
+// ahead of the kernel's stores (which never alias the array read)
+__device__ __forceinline__ double ldg_val(const double* p) { return __ldg(p); }
+__device__ __forceinline__ float ldg_val(const float* p) { return __ldg(p); }
+__device__ __forceinline__ Pack<float, 2> ldg_val(const Pack<float, 2>* p) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  Pack<float, 2> r;
+  r.v[0] = v.x;
+  r.v[1] = v.y;
+  return r;
+}
+__device__ __forceinline__ Pack<float, 4> ldg_val(const Pack<float, 4>* p) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  Pack<float, 4> r;
+  r.v[0] = v.x;
+  r.v[1] = v.y;
+  r.v[2] = v.z;
+  r.v[3] = v.w;
+  return r;
+}
+
+// lane l of a value set to x
+template <class T>
+__device__ __forceinline__ void lane_set(T& a, int, T x) {
+  a = x;
+}
+template <class F, int R>
+__device__ __forceinline__ void lane_set(Pack<F, R>& a, int l, F x) {
+  a.v[l] = x;
+}
+
 // acc[l] += a_l * b_l in FP64
 template <class T>
 __device__ __forceinline__ void lane_dot(double* acc, const T& a, const T& b) {

@@ -13,6 +13,12 @@
 // and replayed; a finished solve turns the remaining kernels into immediate
 // returns through a device flag.
 //
+// On request (BP_FUSE_DIRECTION=1, where the element operator runs in its TMA
+// form) the direction update is fused into the operator (CgFuse::dir): it
+// forms p = z + beta p at the nodes it reads anyway and writes p and the x
+// update at the nodes it owns, so an iteration is three kernels; p then
+// alternates between two buffers (CgScalars::gen).
+//
 // Mixed precision: the same kernels run on FP32 vectors, FP32 factors and an
 // FP32 operator (dot products accumulate in FP64).  The FP64 iterate is x_hi;
 // the FP32 recursion carries a correction x_lo and residual r_lo.  When the
@@ -266,6 +272,7 @@ cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, co
     }
     if (hist_rnorm) hist_rnorm[sc->iter] = sqrt(tot[0]);
     sc->iter += 1;
+    sc->gen += 1;
     sc->skip_x = 0;
     if (!isfinite(tot[0])) {
       sc->breakdown = 1;
@@ -282,12 +289,14 @@ cg_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, co
 }
 
 // apply the last completed iteration's x update (x and p with element stride
-// `stride`: 1, or the lane count of a packed group)
+// `stride`: 1, or the lane count of a packed group).  With the fused direction
+// update (gsc != null) p is p1 when gsc->gen is odd, else p0.
 template <class V>
 __global__ void __launch_bounds__(kThreads)
-cg_final_kernel(int32_t N, V* __restrict__ x, const V* __restrict__ p, const CgScalars* __restrict__ sc,
-                int stride = 1) {
+cg_final_kernel(int32_t N, V* __restrict__ x, const V* p0, const V* p1, const CgScalars* gsc,
+                const CgScalars* __restrict__ sc, int stride = 1) {
   if (sc->iter == 0 || sc->breakdown || sc->skip_x) return;
+  const V* __restrict__ p = (gsc && (gsc->gen & 1)) ? p1 : p0;
   const V alpha = (V)sc->alpha;
   for (int32_t n = blockIdx.x * kThreads + threadIdx.x; n < N; n += kThreads * gridDim.x)
     x[(size_t)n * stride] = alpha * p[(size_t)n * stride] + V(1) * x[(size_t)n * stride];
@@ -444,6 +453,7 @@ grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, c
   for (int c = 0; c < 2 * PK; ++c) acc[c] = s_acc[c][threadIdx.x];
   double tot[2 * PK];
   if (grid_sum_cg<2 * PK>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    sc[0].gen += 1;
     for (int l = 0; l < PK; ++l) {
       if (!act[l]) continue;
       CgScalars& c = sc[l];
@@ -469,6 +479,14 @@ grp_gather_update_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, c
       }
     }
   }
+}
+
+// the owner bit on the first local node (column) of every gathered row
+__global__ void __launch_bounds__(kThreads)
+owner_bits_kernel(int32_t Nrows, const int32_t* __restrict__ rowStarts, const int32_t* __restrict__ colIds,
+                  int32_t* __restrict__ G2Lo) {
+  for (int32_t row = blockIdx.x * kThreads + threadIdx.x; row < Nrows; row += kThreads * gridDim.x)
+    G2Lo[colIds[rowStarts[row]]] |= kOwnerBit;
 }
 
 __global__ void d2f_kernel(size_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -542,6 +560,10 @@ struct bp_solver_s {
   DeviceArray<double> AqL, p, Ap, invD, xw, rw, partials, hist, fuse_partials, bcopy;
   // FP32 data of the mixed-precision solve
   DeviceArray<float> invD32, AqL32, p32, x32, r32;
+  // second direction buffers of the fused direction update (allocated when used)
+  DeviceArray<double> p_alt;
+  DeviceArray<float> p32_alt;
+  bool dir64 = false, dir32 = false;   // the captured FP64 / FP32 iterations fuse the direction update
   int family = 0;              // operator family of the FP32 data on the mesh (mesh_fp32)
   DeviceArray<unsigned int> counter;
   DeviceArray<CgScalars> sc;
@@ -633,20 +655,92 @@ static int operator_apply(bp_solver_s* S, const double* q, double* Aq, const int
   return launch_gather(m->Ngather, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, Aq, s);
 }
 
-// enqueue one CG iteration on vectors of type V (FP64, or FP32 in a mixed solve)
+// The fused direction update (CgFuse::dir) is used where BP_FUSE_DIRECTION=1.
+// Measured on the 40^3 p=7 box it is slower than the separate direction
+// kernel: the fused four-rhs launch took 1.07 ms against 0.61 ms for the
+// operator alone and 0.28 ms for the direction pass (bench step 2.01 vs
+// 1.82 s; FP64 Jacobi-PCG 22.5 vs 22.9 GDOF*it/s).  The gathered loads of
+// p, r, invD and x, all needed before the element's first slice, lengthen
+// each block's start-up latency, which the 16 resident warps per SM do not
+// hide; the separate pass streams the same vectors at the HBM rate.
+static bool fuse_direction_enabled() {
+  const char* e = getenv("BP_FUSE_DIRECTION");
+  return e && e[0] == '1';
+}
+
+int launch_owner_map(size_t NL, const int32_t* G2L, int32_t Ngather, const int32_t* rowStarts, const int32_t* colIds,
+                     int32_t* G2Lo, cudaStream_t s) {
+  if (NL && G2Lo != G2L)
+    BP_CUDA_TRY(cudaMemcpyAsync(G2Lo, G2L, sizeof(int32_t) * NL, cudaMemcpyDeviceToDevice, s));
+  if (Ngather > 0) {
+    owner_bits_kernel<<<vec_grid(Ngather), kThreads, 0, s>>>(Ngather, rowStarts, colIds, G2Lo);
+    BP_CUDA_TRY(cudaGetLastError());
+  }
+  return BP_SUCCESS;
+}
+
+// GlobalToLocal with owner bits of the mesh, built on first use
+static int mesh_owner_g2l(bp_mesh_s* m, cudaStream_t s) {
+  if (m->G2Lo.ptr || m->G2L.n == 0) return BP_SUCCESS;
+  BP_TRY(m->G2Lo.alloc(m->G2L.n));
+  BP_TRY(launch_owner_map(m->G2L.n, m->G2L.ptr, m->Ngather, m->rowStarts.ptr, m->colIds.ptr, m->G2Lo.ptr, s));
+  BP_CUDA_TRY(cudaStreamSynchronize(s));
+  return BP_SUCCESS;
+}
+
+// Whether the CG iterations of the element operator (d, `lanes` values per
+// node, arithmetic of `bytes`) take the fused direction update: they do where
+// the operator's current form is the TMA form.  Builds the owner bits.
+static int want_dir(bp_mesh_s* m, const bp_ax_desc_t& d, int bytes, int lanes, bool* dir, cudaStream_t s) {
+  *dir = false;
+  if (!fuse_direction_enabled() || d.bp < 5 || m->Ngather >= kOwnerBit || !tma_covers(d, lanes) ||
+      ax_current_form(d, bytes, lanes, m->E) != FORM_TMA)
+    return BP_SUCCESS;
+  BP_TRY(mesh_owner_g2l(m, s));
+  *dir = true;
+  return BP_SUCCESS;
+}
+
 template <class V>
-static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* AqL, const V* invD, const ElemOperands<V>& o,
-                             cudaStream_t s) {
+static int alloc_zero(DeviceArray<V>& a, size_t n, cudaStream_t s) {
+  if (a.n == n && a.ptr) return BP_SUCCESS;
+  BP_TRY(a.alloc(n));
+  if (n) BP_CUDA_TRY(cudaMemsetAsync(a.ptr, 0, sizeof(V) * n, s));
+  return BP_SUCCESS;
+}
+
+// enqueue one CG iteration on vectors of type V (FP64, or FP32 in a mixed solve);
+// dir: the operator does the direction update (p and p_alt alternate)
+template <class V>
+static int enqueue_iteration(bp_solver_s* S, V* x, V* r, V* p, V* p_alt, V* AqL, const V* invD,
+                             const ElemOperands<V>& o, bool dir, cudaStream_t s) {
   bp_mesh_s* m = S->mesh;
   const int32_t N = S->N;
   const int g = vec_grid(N);
   double* hist_alpha = S->hist.ptr;
   double* hist_rnorm = S->hist.ptr ? S->hist.ptr + S->hist_len : nullptr;
-  cg_direction_kernel<V><<<g, kThreads, 0, s>>>(N, x, p, r, invD, S->scal);
-  BP_CUDA_TRY(cudaGetLastError());
-  const CgFuse fuse{S->fuse_partials.ptr};
   int nparts = 0;
-  BP_TRY(elem_apply<V>(S, o, p, AqL, &S->scal->done, s, &fuse, &nparts));
+  if (dir) {
+    CgFuse fuse;
+    fuse.partials = S->fuse_partials.ptr;
+    fuse.dir = 1;
+    fuse.pbuf[0] = p;
+    fuse.pbuf[1] = p_alt;
+    fuse.r = r;
+    fuse.invD = S->precon ? invD : nullptr;
+    fuse.x = x;
+    fuse.sc = S->scal;
+    const int rc = launch_ax_tma(S->ax, m->E, m->elementList.ptr, m->G2Lo.ptr, o.wJ, o.ggeo, o.D, (V)S->lambda,
+                                 nullptr, AqL, &S->scal->done, &fuse, s, &nparts);
+    if (rc == 1) return fail(BP_ERROR_ARG, "CG: the fused direction update does not cover this operator");
+    BP_TRY(rc);
+  } else {
+    cg_direction_kernel<V><<<g, kThreads, 0, s>>>(N, x, p, r, invD, S->scal);
+    BP_CUDA_TRY(cudaGetLastError());
+    CgFuse fuse;
+    fuse.partials = S->fuse_partials.ptr;
+    BP_TRY(elem_apply<V>(S, o, p, AqL, &S->scal->done, s, &fuse, &nparts));
+  }
   cg_alpha_kernel<1><<<alpha_grid(nparts), kThreads, 0, s>>>(nparts, S->fuse_partials.ptr, S->scal, hist_alpha,
                                                               S->partials.ptr, S->counter.ptr);
   BP_CUDA_TRY(cudaGetLastError());
@@ -676,12 +770,13 @@ static int capture(cudaGraphExec_t* out, cudaStream_t s, int (*body)(bp_solver_s
 }
 
 static int body64(bp_solver_s* S, void* x, void* r, cudaStream_t s) {
-  return enqueue_iteration<double>(S, (double*)x, (double*)r, S->p.ptr, S->AqL.ptr, S->invD.ptr, operands64(S), s);
+  return enqueue_iteration<double>(S, (double*)x, (double*)r, S->p.ptr, S->p_alt.ptr, S->AqL.ptr, S->invD.ptr,
+                                   operands64(S), S->dir64, s);
 }
 
 static int body32(bp_solver_s* S, void*, void*, cudaStream_t s) {
-  return enqueue_iteration<float>(S, S->x32.ptr, S->r32.ptr, S->p32.ptr, S->AqL32.ptr, S->invD32.ptr, operands32(S),
-                                  s);
+  return enqueue_iteration<float>(S, S->x32.ptr, S->r32.ptr, S->p32.ptr, S->p32_alt.ptr, S->AqL32.ptr, S->invD32.ptr,
+                                  operands32(S), S->dir32, s);
 }
 
 // One launch of the iteration's element operator outside any capture, on the
@@ -689,14 +784,30 @@ static int body32(bp_solver_s* S, void*, void*, cudaStream_t s) {
 // so the graphs captured next use the tuned one.
 template <class V>
 static int tune_elem(bp_solver_s* S, const ElemOperands<V>& o, V* p, V* AqL, cudaStream_t s) {
-  const CgFuse fuse{S->fuse_partials.ptr};
+  CgFuse fuse;
+  fuse.partials = S->fuse_partials.ptr;
   int nparts = 0;
   return elem_apply<V>(S, o, p, AqL, nullptr, s, &fuse, &nparts);
 }
 
+// before capturing a solver's iterations: tune the operator, then choose
+// whether the iterations fuse the direction update
+static int prepare64(bp_solver_s* S, cudaStream_t s) {
+  BP_TRY(tune_elem<double>(S, operands64(S), S->p.ptr, S->AqL.ptr, s));
+  BP_TRY(want_dir(S->mesh, S->ax, 8, 1, &S->dir64, s));
+  if (S->dir64) BP_TRY(alloc_zero(S->p_alt, S->p.n, s));
+  return BP_SUCCESS;
+}
+static int prepare32(bp_solver_s* S, cudaStream_t s) {
+  BP_TRY(tune_elem<float>(S, operands32(S), S->p32.ptr, S->AqL32.ptr, s));
+  BP_TRY(want_dir(S->mesh, S->ax, 4, 1, &S->dir32, s));
+  if (S->dir32) BP_TRY(alloc_zero(S->p32_alt, S->p32.n, s));
+  return BP_SUCCESS;
+}
+
 static int ensure_graph(bp_solver_s* S, double* x, double* r, cudaStream_t s) {
   if (S->graph && S->g_x == x && S->g_r == r) return BP_SUCCESS;
-  BP_TRY(tune_elem<double>(S, operands64(S), S->p.ptr, S->AqL.ptr, s));
+  BP_TRY(prepare64(S, s));
   BP_TRY(capture(&S->graph, s, body64, S, x, r));
   S->g_x = x;
   S->g_r = r;
@@ -768,14 +879,15 @@ static int solve_fp64(bp_solver_s* S, double* x, double* r, double tol, int maxi
   CgScalars h{};
   for (int c = 0; c < nchunks; ++c) {
     BP_CUDA_TRY(cudaGraphLaunch(S->graph, s));
-    S->launches += 4 * kChunk;
+    S->launches += (S->dir64 ? 3 : 4) * kChunk;
     if (tol > 0.0 && c + 1 < nchunks) {
       BP_TRY(read_scalars(S, h, s));
       if (h.done) break;
     }
   }
   S->launches += 1;
-  cg_final_kernel<double><<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->scal);
+  cg_final_kernel<double><<<vec_grid(N), kThreads, 0, s>>>(N, x, S->p.ptr, S->p_alt.ptr,
+                                                            S->dir64 ? S->scal : nullptr, S->scal);
   BP_CUDA_TRY(cudaGetLastError());
   if (record_events) BP_CUDA_TRY(cudaEventRecord(S->ev1, s));
   BP_TRY(read_scalars(S, h, s));
@@ -806,7 +918,8 @@ static int mixed_begin(bp_solver_s* S, double* x, double* r, double tol, int max
 static int mixed_reliable(bp_solver_s* S, double* x, double* r, double tol, int maxit, cudaStream_t s) {
   const int32_t N = S->N;
   S->launches += 2;
-  cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, S->x32.ptr, S->p32.ptr, S->scal);
+  cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, S->x32.ptr, S->p32.ptr, S->p32_alt.ptr,
+                                                           S->dir32 ? S->scal : nullptr, S->scal);
   BP_CUDA_TRY(cudaGetLastError());
   mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, x, S->x32.ptr);
   BP_CUDA_TRY(cudaGetLastError());
@@ -818,7 +931,7 @@ static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int max
   if (!(tol > 0.0)) return fail(BP_ERROR_ARG, "bp_solver_solve: a mixed-precision solve needs tol > 0");
   BP_TRY(ensure_hist(S, maxit));
   if (!S->graph32) {
-    BP_TRY(tune_elem<float>(S, operands32(S), S->p32.ptr, S->AqL32.ptr, s));
+    BP_TRY(prepare32(S, s));
     BP_TRY(capture(&S->graph32, s, body32, S, nullptr, nullptr));
   }
   S->launches = 0;
@@ -833,7 +946,7 @@ static int solve_mixed(bp_solver_s* S, double* x, double* r, double tol, int max
       ++updates;
     } else {
       BP_CUDA_TRY(cudaGraphLaunch(S->graph32, s));
-      S->launches += 4 * kChunk;
+      S->launches += (S->dir32 ? 3 : 4) * kChunk;
     }
     BP_TRY(read_scalars(S, h, s));
     if (h.breakdown) break;
@@ -1048,6 +1161,8 @@ struct CgGroup {
   int pk = 0;                                   // lanes
   bp_solver_s* base = nullptr;                  // mixed solver on the mesh: FP64 operator, invD, FP32 data
   DeviceArray<float> x32, r32, p32, AqL32;      // packed [N][pk], AqL [NL][pk]
+  DeviceArray<float> p32b;                      // second direction buffer of the fused direction update
+  bool dir = false;                             // the captured iterations fuse the direction update
   DeviceArray<double> parts;                    // operator p.Ap partials [pk][blocks]
   DeviceArray<double> gparts;                   // gather-update grid sums [2 pk][reduction blocks]
   DeviceArray<unsigned int> gcount;             // their arrival counter (zero between launches)
@@ -1119,15 +1234,31 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   bp_mesh_s* m = S->mesh;
   const int32_t N = S->N;
   using T = Pack<float, PK>;
-  const int g = vec_grid_wave(reinterpret_cast<const void*>(&grp_direction_kernel<PK>), N);
-  grp_direction_kernel<PK><<<g, kThreads, 0, s>>>(N, reinterpret_cast<T*>(G->x32.ptr), reinterpret_cast<T*>(G->p32.ptr),
-                                                  reinterpret_cast<const T*>(G->r32.ptr), S->invD32.ptr, G->sc);
-  BP_CUDA_TRY(cudaGetLastError());
   const ElemOperands<float> o = operands32(S);
-  const CgFuse fuse{G->parts.ptr};
+  CgFuse fuse;
+  fuse.partials = G->parts.ptr;
   int nparts = 0;
-  BP_TRY(launch_ax_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
-                          (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts));
+  if (G->dir) {
+    fuse.dir = 1;
+    fuse.pbuf[0] = G->p32.ptr;
+    fuse.pbuf[1] = G->p32b.ptr;
+    fuse.r = G->r32.ptr;
+    fuse.invD = S->precon ? S->invD32.ptr : nullptr;
+    fuse.x = G->x32.ptr;
+    fuse.sc = G->sc;
+    const int rc = launch_ax_tma_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2Lo.ptr, o.wJ, o.ggeo, o.D,
+                                       (float)S->lambda, nullptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts);
+    if (rc == 1) return fail(BP_ERROR_ARG, "CG: the fused direction update does not cover this operator");
+    BP_TRY(rc);
+  } else {
+    const int g = vec_grid_wave(reinterpret_cast<const void*>(&grp_direction_kernel<PK>), N);
+    grp_direction_kernel<PK><<<g, kThreads, 0, s>>>(N, reinterpret_cast<T*>(G->x32.ptr),
+                                                    reinterpret_cast<T*>(G->p32.ptr),
+                                                    reinterpret_cast<const T*>(G->r32.ptr), S->invD32.ptr, G->sc);
+    BP_CUDA_TRY(cudaGetLastError());
+    BP_TRY(launch_ax_packed(PK, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
+                            (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts));
+  }
   cg_alpha_kernel<PK><<<alpha_grid(nparts), kThreads, 0, s>>>(nparts, G->parts.ptr, G->sc, nullptr, G->gparts.ptr,
                                                                G->gcount.ptr);
   BP_CUDA_TRY(cudaGetLastError());
@@ -1162,7 +1293,9 @@ static int grp_reliable(CgGroup* G, int l, double tol, int maxit, cudaStream_t s
   bp_solver_s* S = G->base;
   const int32_t N = S->N;
   S->launches += 2;
-  cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, G->x32.ptr + l, G->p32.ptr + l, G->sc + l, G->pk);
+  cg_final_kernel<float><<<vec_grid(N), kThreads, 0, s>>>(N, G->x32.ptr + l, G->p32.ptr + l,
+                                                           (G->dir ? G->p32b.ptr : G->p32.ptr) + l,
+                                                           G->dir ? G->sc : nullptr, G->sc + l, G->pk);
   BP_CUDA_TRY(cudaGetLastError());
   mixed_fold_kernel<<<vec_grid(N), kThreads, 0, s>>>(N, G->x[l], G->x32.ptr + l, G->pk);
   BP_CUDA_TRY(cudaGetLastError());
@@ -1215,14 +1348,17 @@ static int unit_capture(bp_batch_s* B, BatchUnit& u, cudaStream_t s) {
     bp_solver_s* S = G->base;
     bp_mesh_s* m = S->mesh;
     const ElemOperands<float> o = operands32(S);
-    const CgFuse fuse{G->parts.ptr};
+    CgFuse fuse;
+    fuse.partials = G->parts.ptr;
     int nparts = 0;
     BP_TRY(launch_ax_packed(G->pk, S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D,
                             (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts));
+    BP_TRY(want_dir(m, S->ax, 4, G->pk, &G->dir, s));
+    if (G->dir) BP_TRY(alloc_zero(G->p32b, G->p32.n, s));
   } else {
     bp_solver_s* S = B->sys_solver[u.sys];
-    if (B->mixed) BP_TRY(tune_elem<float>(S, operands32(S), S->p32.ptr, S->AqL32.ptr, s));
-    else BP_TRY(tune_elem<double>(S, operands64(S), S->p.ptr, S->AqL.ptr, s));
+    if (B->mixed) BP_TRY(prepare32(S, s));
+    else BP_TRY(prepare64(S, s));
   }
   cudaGraph_t g;
   BP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1255,6 +1391,7 @@ static int unit_start(bp_batch_s* B, BatchUnit& u, double tol, int maxit, cudaSt
     }
     BP_CUDA_TRY(cudaMemsetAsync(G->x32.ptr, 0, sizeof(float) * G->x32.n, s));
     BP_CUDA_TRY(cudaMemsetAsync(G->p32.ptr, 0, sizeof(float) * G->p32.n, s));
+    if (G->p32b.ptr) BP_CUDA_TRY(cudaMemsetAsync(G->p32b.ptr, 0, sizeof(float) * G->p32b.n, s));
     for (int l = 0; l < G->pk; ++l) BP_TRY(grp_replace(G, l, true, tol, maxit, s));
     return BP_SUCCESS;
   }
@@ -1349,7 +1486,9 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       }
       if (running) {
         BP_CUDA_TRY(cudaGraphLaunch(u.graph, st));
-        (u.G ? u.G->base : B->sys_solver[u.sys])->launches += 4 * kBatchChunk;
+        bp_solver_s* us = u.G ? u.G->base : B->sys_solver[u.sys];
+        const bool ud = u.G ? u.G->dir : (B->mixed ? us->dir32 : us->dir64);
+        us->launches += (ud ? 3 : 4) * kBatchChunk;
         BP_TRY(unit_post(B, u, st));
         ++a;
         continue;
@@ -1358,7 +1497,8 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
       if (!B->mixed && !u.G) {
         bp_solver_s* S = B->sys_solver[u.sys];
         S->launches += 1;
-        cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, st>>>(S->N, B->x[u.sys]->ptr, S->p.ptr, S->scal);
+        cg_final_kernel<double><<<vec_grid(S->N), kThreads, 0, st>>>(S->N, B->x[u.sys]->ptr, S->p.ptr, S->p_alt.ptr,
+                                                                     S->dir64 ? S->scal : nullptr, S->scal);
         BP_CUDA_TRY(cudaGetLastError());
       }
       free_streams.push_back(u.stream);

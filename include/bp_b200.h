@@ -113,6 +113,44 @@ int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* 
 int bp_ax_hex3d_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Nelements, const int32_t* elementList,
                           const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
                           const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream);
+/* GlobalToLocal with owner marks for the fused CG step below: ownerMap[n] =
+   GlobalToLocal[n], with BP_OWNER_BIT added on the first local node (the first
+   column of its CSR row) of every gathered row; masked entries stay -1.
+   Needs Ngather < BP_OWNER_BIT.  ownerMap may equal GlobalToLocal (in place).
+   No counterpart in the reference. */
+#define BP_OWNER_BIT (1 << 30)
+int bp_ogs_owner_map(int32_t NL, const int32_t* GlobalToLocal, int32_t Ngather, const int32_t* rowStarts,
+                     const int32_t* colIds, int32_t* ownerMap, bp_stream_t stream);
+
+/* One CG step's direction update fused into the stored-factor element operator
+   (the TMA-staged form: even Nq, stored factors).  For every system k of nrhs
+   (FP64: 1; FP32: 1, 2 or 4 packed as in bp_ax_hex3d_f32_multi), at every
+   gathered node g:
+     p_new[g] = z[g] + beta[k] p_old[g],  z = invD .* r (r if invD is NULL),
+                or p_new = z where beta[k] == 0 (the first step);
+     x[g]    += alpha[k] p_old[g]          (skipped where alpha[k] == 0);
+   and Aq = A_e p_new[GlobalToLocal] element by element, with the block sums of
+   p_new.Aq per system in pAp_partials[k * nblocks + b] (nblocks <= Nelements).
+   It replaces the pair linAlg axpy (p = r + beta p, libs/core/linearSolverCG.cpp:
+   105-107) + Operator(p, Ap) (:109-110, BP/BP5/src/bp5Operator.cpp:29-85) of the
+   reference's iteration, and takes over the x update of its UpdateCG
+   (:131-156), one step later, so p, r, invD and x are read in the pass over the
+   factors that the operator makes anyway;
+   ownerMap comes from bp_ogs_owner_map.  p_new must not alias p_old; the
+   gathered vectors (r, invD, p_old, p_new, x) are read and written at unmasked
+   nodes only, so a mesh whose nodes are all masked may pass NULL.  Returns
+   BP_ERROR_ARG where the TMA form does not cover desc. */
+int bp_cg_direction_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                             const int32_t* ownerMap, const double* wJ, const double* ggeo, const double* D,
+                             double lambda, double alpha, double beta, const double* r, const double* invD,
+                             const double* p_old, double* p_new, double* x, double* Aq, double* pAp_partials,
+                             bp_stream_t stream);
+int bp_cg_direction_ax_f32_multi(const bp_ax_desc_t* desc, int32_t nrhs, int32_t Nelements,
+                                 const int32_t* elementList, const int32_t* ownerMap, const float* wJ,
+                                 const float* ggeo, const float* D, float lambda, const double* alpha,
+                                 const double* beta, const float* r, const float* invD, const float* p_old,
+                                 float* p_new, float* x, float* Aq, double* pAp_partials, bp_stream_t stream);
+
 /* dst[i] = (float) src[i], i < n, device arrays (to build FP32 operands). */
 int bp_convert_f64_f32(size_t n, const double* src, float* dst, bp_stream_t stream);
 
