@@ -108,9 +108,30 @@ struct DirStep {
 // Sum of v over the block in a fixed order, valid in thread 0.  `scratch`
 // holds at least one double per thread and is free for the caller to reuse
 // (any block shape, partial warps included).
+//
+// A block of whole warps sums each warp by a shuffle tree and thread 0 adds
+// the warp sums in warp order: one barrier pair and nt/32 serial additions
+// (the strided form below ends in 32 dependent shared-memory reads and adds in
+// thread 0, about 1000 cycles per block).
+__device__ __forceinline__ double warp_tree_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __device__ __forceinline__ double fuse_block_sum(double v, double* scratch) {
   const int nt = blockDim.x * blockDim.y * blockDim.z;
   const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  if ((nt & 31) == 0) {
+    v = warp_tree_sum(v);
+    __syncthreads();   // the caller's last reads of scratch are done
+    if ((t & 31) == 0) scratch[t >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (t == 0)
+      for (int w = 0; w < (nt >> 5); ++w) r += scratch[w];
+    return r;
+  }
   __syncthreads();   // the caller's last reads of scratch are done
   scratch[t] = v;
   __syncthreads();
@@ -133,6 +154,24 @@ template <int L>
 __device__ __forceinline__ void fuse_block_sum_lanes(const double (&v)[L], double* scratch, double (&out)[L]) {
   const int nt = blockDim.x * blockDim.y * blockDim.z;
   const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  if ((nt & 31) == 0) {   // whole warps: shuffle trees, then the warp sums in warp order
+    double w[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) w[l] = warp_tree_sum(v[l]);
+    __syncthreads();   // the caller's last reads of scratch are done
+    if ((t & 31) == 0)
+#pragma unroll
+      for (int l = 0; l < L; ++l) scratch[(t >> 5) * L + l] = w[l];
+    __syncthreads();
+    if (t == 0)
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        double r = 0.0;
+        for (int k = 0; k < (nt >> 5); ++k) r += scratch[k * L + l];
+        out[l] = r;
+      }
+    return;
+  }
   __syncthreads();   // the caller's last reads of scratch are done
 #pragma unroll
   for (int l = 0; l < L; ++l) scratch[l * nt + t] = v[l];
