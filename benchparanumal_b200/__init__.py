@@ -657,7 +657,7 @@ def basis_cubature(N):
     return out
 
 
-FORMS = {0: "mma", 1: "tma", 2: "line", 3: "pencil"}
+FORMS = {0: "mma", 1: "tma", 2: "line", 3: "pencil", 4: "rb"}
 
 
 def tune_report(kind, N, Nfields, affine, precision_bytes, lanes, fused, Nelements):

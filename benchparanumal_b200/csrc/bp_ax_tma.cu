@@ -530,6 +530,269 @@ int tma_wait_test(int withhold) {
   return check_device_error();
 }
 
+// ---------------------------------------------------------------------------
+// Register-blocked packed operator (FP32, L right-hand sides packed per node).
+//
+// The packed TMA kernel above gives each thread all L lanes of one k-pencil:
+// every shared-memory value it loads (16 bytes) feeds one multiply-add per
+// lane, so the r- and s-contractions cost 32 16-byte loads per node and slice
+// and the kernel is bound by shared-memory wavefronts (about 126 per warp and
+// slice).  Here a thread owns one lane of four k-pencils, (i, j) for i in
+// {a, Nq-1-a} and j in {b, Nq-1-b}: a value of row j (or column i) of the
+// slice feeds the two pencils that share it, and the four lanes of a node sit
+// in consecutive threads, so a warp's 4-byte loads are broadcast-free and
+// conflict-free in one wavefront each.  The gradient and the weak divergence
+// then cost 16 4-byte loads per pencil pair and direction, about half the
+// shared-memory traffic per node and lane.  The thread keeps rows a and b and
+// columns a and b of D in registers and takes the mirrored rows and columns
+// from the antisymmetry of the GLL differentiation matrix, D[Nq-1-i][Nq-1-m]
+// = -D[i][m] (exact for the true matrix; the computed one, rounded to FP32,
+// satisfies it to an ulp or two, far below this FP32 operator's accuracy);
+// the t-direction uses the slice's row of D from the constant bank, as above.
+// Factors come through the same ring of bulk-copied slices.
+// ---------------------------------------------------------------------------
+template <int NQ, int L>
+struct RbShape {
+  static constexpr int H = NQ / 2;
+  static constexpr int THREADS = L * H * H;
+  static constexpr int NQ2 = NQ * NQ;
+  static constexpr int R = 4;                                    // ring slots
+  static constexpr int SLICE_G = NQ2 * 6;
+  static constexpr int SLICE_BYTES = NQ2 * 7 * (int)sizeof(float);
+  // row stride (floats) of the slice arrays [j][i][lane]: rows b and b+1 (and
+  // Nq-1-b) of a warp's stores fall in opposite halves of the 32 banks
+  static constexpr int BASE = NQ * L;
+  static constexpr int RS = BASE + ((16 - BASE % 32) + 32) % 32;
+  static constexpr int SARR = NQ * RS;                           // floats per slice array
+  static constexpr size_t FACT = sizeof(float) * ((size_t)R * (SLICE_G + NQ2) + NQ2);
+  static constexpr size_t SOFF = (FACT + 15) & ~(size_t)15;
+  static constexpr size_t BAR = (SOFF + sizeof(float) * 3 * SARR + 7) & ~(size_t)7;
+  static constexpr size_t BYTES = BAR + sizeof(uint64_t) * R;
+  static_assert(RS >= BASE && RS % 32 == 16, "slice row stride");
+};
+
+template <int NQ, int L, bool DOT>
+__global__ void __launch_bounds__(RbShape<NQ, L>::THREADS, (L == 4 && NQ == 8) ? 8 : 1)
+ax_rb_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+             const float* __restrict__ wJ, const float* __restrict__ ggeo, const float* __restrict__ Dg,
+             float lambda, const float* __restrict__ q, float* __restrict__ Aq, const int* __restrict__ skip,
+             CgFuse fuse) {
+  if (skip && *skip) return;
+  using Sh = RbShape<NQ, L>;
+  constexpr int H = Sh::H, NQ2 = Sh::NQ2, NP = NQ2 * NQ, R = Sh::R, RS = Sh::RS;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* s_g = reinterpret_cast<float*>(smem_raw);
+  float* s_J = s_g + R * Sh::SLICE_G;
+  float* s_D = s_J + R * NQ2;
+  float* sS = reinterpret_cast<float*>(smem_raw + Sh::SOFF);   // [NQ][RS]: q slice, [j][i][lane]
+  float* sV = sS + Sh::SARR;                                    // r-fluxes
+  float* sW = sV + Sh::SARR;                                    // s-fluxes
+  uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem_raw + Sh::BAR);
+
+  const int t = threadIdx.x;
+  const int l = t % L, a = (t / L) % H, b = t / (L * H);
+  const int i0 = a, i1 = NQ - 1 - a, j0 = b, j1 = NQ - 1 - b;
+  const int e = elementList[blockIdx.x];
+
+  if (t == 0) {
+    for (int r = 0; r < R; ++r) mbar_init(&s_bar[r], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  int armed = R;
+  if (t == 0) {
+    for (int k = 0; k < R; ++k) {
+      mbar_expect_tx(&s_bar[k], Sh::SLICE_BYTES);
+      const size_t eb = (size_t)e * NP + (size_t)k * NQ2;
+      bulk_g2s(s_g + k * Sh::SLICE_G, ggeo + 6 * eb, NQ2 * 6 * sizeof(float), &s_bar[k]);
+      bulk_g2s(s_J + k * NQ2, wJ + eb, NQ2 * sizeof(float), &s_bar[k]);
+    }
+  }
+  for (int n = t; n < NQ2; n += Sh::THREADS) s_D[n] = Dg[n];
+
+  // the four pencils (p = 2 * jj + ii: (i0,j0), (i1,j0), (i0,j1), (i1,j1)), lane l
+  const size_t lbase = (size_t)e * NP;
+  const int nodes[4] = {j0 * NQ + i0, j0 * NQ + i1, j1 * NQ + i0, j1 * NQ + i1};
+  float u[4][NQ], Au[4][NQ];
+  {
+    int id[4][NQ];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) id[p][k] = __ldg(G2L + lbase + k * NQ2 + nodes[p]);
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        u[p][k] = id[p][k] >= 0 ? q[(size_t)id[p][k] * L + l] : 0.0f;
+        Au[p][k] = 0.0f;
+      }
+  }
+  __syncthreads();   // s_D
+  // rows a, b and columns a, b of D; the mirrored ones by antisymmetry
+  float Dra[NQ], Drb[NQ], Dca[NQ], Dcb[NQ];
+#pragma unroll
+  for (int m = 0; m < NQ; ++m) {
+    Dra[m] = s_D[a * NQ + m];
+    Drb[m] = s_D[b * NQ + m];
+    Dca[m] = s_D[m * NQ + a];
+    Dcb[m] = s_D[m * NQ + b];
+  }
+  bool ok = true;
+  constexpr int DSLOT = tma_d_slot(NQ);
+#pragma unroll
+  for (int k = 0; k < NQ; ++k) {
+    const int rs = k % R;
+    if (ok) ok = mbar_wait(&s_bar[rs], (uint32_t)((k / R) & 1), kWaitCycles);
+    sS[j0 * RS + i0 * L + l] = u[0][k];
+    sS[j0 * RS + i1 * L + l] = u[1][k];
+    sS[j1 * RS + i0 * L + l] = u[2][k];
+    sS[j1 * RS + i1 * L + l] = u[3][k];
+    __syncthreads();
+    float ur[4] = {0.f, 0.f, 0.f, 0.f}, us[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int m = 0; m < NQ; ++m) {
+      const float r0 = sS[j0 * RS + m * L + l], r1 = sS[j1 * RS + m * L + l];   // rows j0, j1
+      const float c0 = sS[m * RS + i0 * L + l], c1 = sS[m * RS + i1 * L + l];   // columns i0, i1
+      const float da = Dra[m], da1 = -Dra[NQ - 1 - m];   // D[i0][m], D[i1][m]
+      const float db = Drb[m], db1 = -Drb[NQ - 1 - m];   // D[j0][m], D[j1][m]
+      ur[0] += da * r0;
+      ur[1] += da1 * r0;
+      ur[2] += da * r1;
+      ur[3] += da1 * r1;
+      us[0] += db * c0;
+      us[1] += db * c1;
+      us[2] += db1 * c0;
+      us[3] += db1 * c1;
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      float ut = 0.0f;
+#pragma unroll
+      for (int m = 0; m < NQ; ++m) ut += tma_d<float>(DSLOT + k * NQ + m) * u[p][m];
+      const float2* g2 = reinterpret_cast<const float2*>(s_g + rs * Sh::SLICE_G + 6 * nodes[p]);
+      const float2 ga = g2[0], gb = g2[1], gc = g2[2];
+      const float G00 = ga.x, G01 = ga.y, G02 = gb.x, G11 = gb.y, G12 = gc.x, G22 = gc.y;
+      const float GwJ = s_J[rs * NQ2 + nodes[p]];
+      const int ii = (p & 1) ? i1 : i0, jj = (p & 2) ? j1 : j0;
+      sV[jj * RS + ii * L + l] = G00 * ur[p] + G01 * us[p] + G02 * ut;
+      sW[jj * RS + ii * L + l] = G01 * ur[p] + G11 * us[p] + G12 * ut;
+      const float GDut = G02 * ur[p] + G12 * us[p] + G22 * ut;
+      Au[p][k] += (GwJ * lambda) * u[p][k];
+#pragma unroll
+      for (int m = 0; m < NQ; ++m) Au[p][m] += tma_d<float>(DSLOT + k * NQ + m) * GDut;
+    }
+    __syncthreads();
+    if (k + R < NQ && t == 0 && ok) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&s_bar[rs], Sh::SLICE_BYTES);
+      armed = k + R + 1;
+      const size_t eb = (size_t)e * NP + (size_t)(k + R) * NQ2;
+      bulk_g2s(s_g + rs * Sh::SLICE_G, ggeo + 6 * eb, NQ2 * 6 * sizeof(float), &s_bar[rs]);
+      bulk_g2s(s_J + rs * NQ2, wJ + eb, NQ2 * sizeof(float), &s_bar[rs]);
+    }
+    float dv[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int m = 0; m < NQ; ++m) {
+      const float v0 = sV[j0 * RS + m * L + l], v1 = sV[j1 * RS + m * L + l];   // V(m, j0), V(m, j1)
+      const float w0 = sW[m * RS + i0 * L + l], w1 = sW[m * RS + i1 * L + l];   // W(i0, m), W(i1, m)
+      const float ca = Dca[m], ca1 = -Dca[NQ - 1 - m];   // D[m][i0], D[m][i1]
+      const float cb = Dcb[m], cb1 = -Dcb[NQ - 1 - m];   // D[m][j0], D[m][j1]
+      dv[0] += ca * v0 + cb * w0;
+      dv[1] += ca1 * v0 + cb * w1;
+      dv[2] += ca * v1 + cb1 * w0;
+      dv[3] += ca1 * v1 + cb1 * w1;
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) Au[p][k] += dv[p];
+  }
+  if (!__syncthreads_and(ok)) {   // block-uniform: every thread leaves together
+    if (t == 0) {
+      atomicExch(&g_device_error, 1);
+      for (int r = 0; r < R; ++r) {   // the last armed phase of every slot, bounded
+        const int last = armed - 1 - ((armed - 1 - r) % R + R) % R;
+        if (last >= 0) mbar_wait(&s_bar[r], (uint32_t)((last / R) & 1), kWaitCycles);
+      }
+    }
+    __syncthreads();
+    return;
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) Aq[(lbase + k * NQ2 + nodes[p]) * L + l] = Au[p][k];
+  if (DOT) {
+    double v = 0.0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) v += (double)u[p][k] * (double)Au[p][k];
+    // per lane: shuffle over the threads of this lane in the warp, then the
+    // warps in order (the ring is free for the warp sums)
+#pragma unroll
+    for (int o = 16; o >= L; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    double* ws = reinterpret_cast<double*>(s_g);
+    constexpr int W = (Sh::THREADS + 31) / 32;
+    if ((t & 31) < L) ws[(t >> 5) * L + (t & 31)] = v;
+    __syncthreads();
+    if (t < L) {
+      double sum = 0.0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) sum += ws[w * L + t];
+      fuse.partials[(size_t)t * gridDim.x + blockIdx.x] = sum;
+    }
+  }
+}
+
+template <int NQ, int L, bool DOT>
+static int launch_rb_dot(int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const float* wJ,
+                         const float* ggeo, const float* D, float lambda, const float* q, float* Aq, const int* skip,
+                         const CgFuse& fuse, cudaStream_t s, int* nblocks) {
+  using Sh = RbShape<NQ, L>;
+  static_assert(Sh::THREADS % 32 == 0, "whole warps (the p.Ap sum shuffles over full warps)");
+  const size_t smem = Sh::BYTES;
+  static DeviceOnce configured;
+  BP_TRY(once_per_device(configured, [smem]() -> int {
+    BP_CUDA_TRY(cudaFuncSetAttribute(ax_rb_kernel<NQ, L, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return BP_SUCCESS;
+  }));
+  float* tab = tma_d_table<float>();
+  if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
+  BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), D, sizeof(float) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  if (nblocks) *nblocks = Nelements;
+  ax_rb_kernel<NQ, L, DOT><<<Nelements, Sh::THREADS, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q,
+                                                                 Aq, skip, fuse);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
+
+int launch_ax_rb_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                        const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
+                        const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                        int* nblocks) {
+  const int NQ = d.N + 1;
+  if (d.affine || d.Nfields != 1 || pk != 4 || (fuse && fuse->dir) ||
+      ((reinterpret_cast<uintptr_t>(ggeo) | reinterpret_cast<uintptr_t>(wJ)) & 15) ||
+      (reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(Aq)) % 16)
+    return 1;
+  if (Nelements == 0) {
+    if (nblocks) *nblocks = 0;
+    return BP_SUCCESS;
+  }
+  switch (NQ) {
+#define BP_RB_CASE(nq)                                                                                          \
+  case nq:                                                                                                      \
+    return fuse ? launch_rb_dot<nq, 4, true>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip, *fuse, \
+                                             s, nblocks)                                                         \
+                : launch_rb_dot<nq, 4, false>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, skip,      \
+                                              CgFuse{}, s, nblocks);
+    BP_RB_CASE(8)
+#undef BP_RB_CASE
+    default:
+      return 1;
+  }
+}
+
 // FP32 operator on PK right-hand sides packed per node (q, Aq hold PK floats per
 // node; one field).  Returns 1 when the configuration is not covered.
 template <int PK>

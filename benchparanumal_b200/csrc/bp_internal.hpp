@@ -292,7 +292,7 @@ int launch_ax_mma(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* eleme
                   const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
 // ---- kernel-form autotuner (bp_tune.cu) ----
 // Forms of the element operator; kind 0 = one value per node, 1 = packed lanes.
-enum { FORM_MMA = 0, FORM_TMA = 1, FORM_LINE = 2, FORM_PENCIL = 3 };
+enum { FORM_MMA = 0, FORM_TMA = 1, FORM_LINE = 2, FORM_PENCIL = 3, FORM_RB = 4 };
 struct TuneConfig {
   int kind, nq, nf, affine, bytes, lanes, fused;
   int ecls;   // size class: floor(log2(elements))
@@ -316,13 +316,19 @@ void tuned_clear();
 
 // Element-operator variant forced by BP_AX_VARIANT (pencil, line, tma, mma),
 // else AX_AUTO: the tuned choice per configuration.
-enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2, AX_MMA = 3, AX_TMA = 4 };
+enum { AX_AUTO = 0, AX_PENCIL = 1, AX_LINE = 2, AX_MMA = 3, AX_TMA = 4, AX_RB = 5 };
 int ax_variant();
 // the packed FP32 operator (2 or 4 rhs per node) in its tuned form (bp_kernels.cu)
 int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
                      const int32_t* G2L, const float* wJ, const float* ggeo, const float* gllw, const float* D,
                      float lambda, const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                      int* nblocks);
+// the register-blocked packed FP32 stored-factor operator (4 rhs, Nq = 8; one
+// lane of four pencils per thread, bp_ax_tma.cu); 1 when not covered
+int launch_ax_rb_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,
+                        const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
+                        const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
+                        int* nblocks);
 // the packed FP32 stored-factor operator (4 rhs) at Nq = 8 on the tensor cores;
 // 1 when not covered
 int launch_ax_mma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,

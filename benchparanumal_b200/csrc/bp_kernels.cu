@@ -185,7 +185,8 @@ int ax_variant() {   // read at every launch, so a process (a test) can switch f
   const char* e = getenv("BP_AX_VARIANT");
   if (!e) return AX_AUTO;
   const std::string s = e;
-  return s == "pencil" ? AX_PENCIL : s == "line" ? AX_LINE : s == "mma" ? AX_MMA : s == "tma" ? AX_TMA : AX_AUTO;
+  return s == "pencil" ? AX_PENCIL : s == "line" ? AX_LINE : s == "mma" ? AX_MMA : s == "tma" ? AX_TMA :
+         s == "rb" ? AX_RB : AX_AUTO;
 }
 
 // The register-pencil form (FP64 affine default; any configuration)
@@ -305,17 +306,20 @@ int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int
       case FORM_TMA:
         return launch_ax_tma_packed(pk, d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, sk, fuse, s,
                                     nblocks);
+      case FORM_RB:
+        return launch_ax_rb_packed(pk, d, Nelements, elementList, G2L, wJ, ggeo, D, lambda, q, Aq, sk, fuse, s,
+                                   nblocks);
       default:
         if (d.N + 1 > 12) return 1;
         return launch_ax_line_packed(pk, d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, sk, fuse,
                                      s, nblocks);
     }
   };
-  const std::vector<int> forms = {FORM_TMA, FORM_LINE, FORM_MMA};
+  const std::vector<int> forms = {FORM_TMA, FORM_RB, FORM_LINE, FORM_MMA};
   int form = forms[0];
   const int v = ax_variant();
   if (v != AX_AUTO) {
-    form = v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : FORM_LINE;
+    form = v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : v == AX_RB ? FORM_RB : FORM_LINE;
   } else {
     const TuneConfig cfg{1, d.N + 1, d.Nfields, d.affine, 4, pk, fuse != nullptr, element_class(Nelements)};
     BP_TRY(tuned_form(cfg, forms, [&](int f) { return run(f, nullptr); }, s, &form));
@@ -328,7 +332,7 @@ int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int
 int ax_current_form(const bp_ax_desc_t& d, int bytes, int lanes, int32_t Nelements) {
   const int v = ax_variant();
   if (lanes > 1) {
-    if (v != AX_AUTO) return v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : FORM_LINE;
+    if (v != AX_AUTO) return v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : v == AX_RB ? FORM_RB : FORM_LINE;
   } else if (v != AX_AUTO) {
     return v == AX_MMA ? FORM_MMA : v == AX_TMA ? FORM_TMA : v == AX_LINE ? FORM_LINE : FORM_PENCIL;
   }

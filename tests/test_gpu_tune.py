@@ -64,4 +64,4 @@ def test_packed_group_is_tuned(gpu):
     stats, _ = B.solve(tol=1e-8, maxit=3000)
     assert all(np.sqrt(s.rdotr / s.rdotr0) <= 1e-8 for s in stats)
     form, times = gpu.tune_report(1, 7, 1, False, 4, 4, 1, 64)
-    assert form in ("tma", "line", "mma") and set(times) == {"tma", "line", "mma"}
+    assert form in ("tma", "rb", "line", "mma") and set(times) == {"tma", "rb", "line", "mma"}
