@@ -68,13 +68,13 @@ class BPError(RuntimeError):
 
 class AxDesc(ctypes.Structure):
     _fields_ = [("bp", ctypes.c_int32), ("N", ctypes.c_int32), ("affine", ctypes.c_int32),
-                ("Nfields", ctypes.c_int32)]
+                ("Nfields", ctypes.c_int32), ("dim", ctypes.c_int32)]
 
 
 class BoxDesc(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("N", ctypes.c_int32),
                 ("affine", ctypes.c_int32), ("Nfields", ctypes.c_int32), ("pert", ctypes.c_double),
-                ("pert_seed", ctypes.c_uint64)]
+                ("pert_seed", ctypes.c_uint64), ("dim", ctypes.c_int32)]
 
 
 class MeshView(ctypes.Structure):
@@ -82,7 +82,15 @@ class MeshView(ctypes.Structure):
                 ("Nelements", ctypes.c_int32), ("Nfields", ctypes.c_int32), ("affine", ctypes.c_int32),
                 ("Ngather", ctypes.c_int32), ("nnz", ctypes.c_int32), ("Nlocal", ctypes.c_int64)] + [
         (n, ctypes.c_void_p) for n in ("elementList", "GlobalToLocal", "rowStarts", "colIds", "wJ", "ggeo", "D",
-                                       "gllz", "gllw", "EX", "EY", "EZ")]
+                                       "gllz", "gllw", "EX", "EY", "EZ")] + [("dim", ctypes.c_int32)]
+
+
+def _ax_desc(mesh, bp=None):
+    """The operator descriptor of a mesh: BP5 with one field, BP6 with more."""
+    if bp is None:
+        bp = 6 if mesh.Nfields > 1 else 5
+    nf = 1 if bp == 5 else mesh.Nfields
+    return AxDesc(bp, mesh.N, int(mesh.affine), nf, getattr(mesh, "dim", 3))
 
 
 class CubatureView(ctypes.Structure):
@@ -301,13 +309,14 @@ def _dl(ptr, n, dtype):
 
 
 class Mesh:
-    """Hex3D box mesh on the device (mesh_t + masked ogs), built by bp_mesh_create."""
+    """Box mesh on the device (mesh_t + masked ogs), built by bp_mesh_create:
+    Hex3D, or Quad2D with dim=2 (nz ignored; Nfields 1 or 2)."""
 
-    def __init__(self, nx, ny=None, nz=None, N=4, affine=False, Nfields=1, pert=0.0, pert_seed=1, device=0):
+    def __init__(self, nx, ny=None, nz=None, N=4, affine=False, Nfields=1, pert=0.0, pert_seed=1, device=0, dim=3):
         platform_init(device)
         ny = nx if ny is None else ny
-        nz = nx if nz is None else nz
-        d = BoxDesc(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), int(pert_seed))
+        nz = (nx if nz is None else nz) if dim == 3 else 1
+        d = BoxDesc(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), int(pert_seed), int(dim))
         h = ctypes.c_void_p()
         _check(lib().bp_mesh_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h.value
@@ -315,6 +324,7 @@ class Mesh:
         _check(lib().bp_mesh_view(self._h, ctypes.byref(self.view)))
         v = self.view
         self.nx, self.ny, self.nz = nx, ny, nz
+        self.dim = v.dim
         self.N, self.Nq, self.Np, self.E = v.N, v.Nq, v.Np, v.Nelements
         self.Nfields, self.affine = v.Nfields, bool(v.affine)
         self.Ngather, self.nnz, self.NL = v.Ngather, v.nnz, int(v.Nlocal)
@@ -328,12 +338,13 @@ class Mesh:
         """Copy a device mesh array to the host (names as in bp_mesh_view_t)."""
         v = self.view
         ng = self.E if self.affine else self.E * self.Np
+        nv, ngg = (8, 6) if self.dim == 3 else (4, 3)
         spec = {
             "elementList": (self.E, np.int32), "GlobalToLocal": (self.NL, np.int32),
             "rowStarts": (self.Ngather + 1, np.int32), "colIds": (self.nnz, np.int32),
-            "wJ": (ng, np.float64), "ggeo": (6 * ng, np.float64), "D": (self.Nq * self.Nq, np.float64),
-            "gllz": (self.Nq, np.float64), "gllw": (self.Nq, np.float64), "EX": (8 * self.E, np.float64),
-            "EY": (8 * self.E, np.float64), "EZ": (8 * self.E, np.float64),
+            "wJ": (ng, np.float64), "ggeo": (ngg * ng, np.float64), "D": (self.Nq * self.Nq, np.float64),
+            "gllz": (self.Nq, np.float64), "gllw": (self.Nq, np.float64), "EX": (nv * self.E, np.float64),
+            "EY": (nv * self.E, np.float64), "EZ": ((8 if self.dim == 3 else 0) * self.E, np.float64),
         }
         if name in spec:
             n, dt = spec[name]
@@ -367,7 +378,7 @@ class Mesh:
 def ax_hex3d(mesh, q, Aq, lam=1.0, elementList=None, Nelements=None, stream=None):
     """bp_ax_hex3d on device buffers: Aq (E-vector) = A_e q[GlobalToLocal]."""
     v = mesh.view
-    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    d = _ax_desc(mesh)
     el = v.elementList if elementList is None else elementList
     ne = mesh.E if Nelements is None else Nelements
     _check(lib().bp_ax_hex3d(ctypes.byref(d), ne, el, v.GlobalToLocal, v.wJ, v.ggeo, v.gllw, v.D, float(lam),
@@ -391,7 +402,7 @@ def convert_f64_f32(src, n, dst, stream=None):
 def ax_hex3d_f32(mesh, q, Aq, ops, lam=1.0, stream=None):
     """bp_ax_hex3d_f32 on FP32 device buffers; ops = dict of FP32 buffers wJ, ggeo, gllw, D."""
     v = mesh.view
-    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    d = _ax_desc(mesh)
     _check(lib().bp_ax_hex3d_f32(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, _ptr(ops["wJ"]),
                                  _ptr(ops["ggeo"]), _ptr(ops["gllw"]), _ptr(ops["D"]), float(lam), _ptr(q),
                                  _ptr(Aq), stream))
@@ -400,7 +411,7 @@ def ax_hex3d_f32(mesh, q, Aq, ops, lam=1.0, stream=None):
 def ax_hex3d_f32_multi(mesh, nrhs, q, Aq, ops, lam=1.0, stream=None):
     """bp_ax_hex3d_f32_multi: the FP32 operator on nrhs interleaved right-hand sides."""
     v = mesh.view
-    d = AxDesc(5, mesh.N, int(mesh.affine), 1)
+    d = _ax_desc(mesh, 5)
     _check(lib().bp_ax_hex3d_f32_multi(ctypes.byref(d), nrhs, mesh.E, v.elementList, v.GlobalToLocal,
                                        _ptr(ops["wJ"]), _ptr(ops["ggeo"]), _ptr(ops["gllw"]), _ptr(ops["D"]),
                                        float(lam), _ptr(q), _ptr(Aq), stream))
@@ -421,7 +432,7 @@ def cg_direction_ax(mesh, owner, alpha, beta, r, invD, p_old, p_new, x, Aq, part
     p_new = invD r), x += alpha p_old (alpha = 0: x untouched), Aq = A_e
     p_new[G2L], p.Ap block partials; invD None means z = r."""
     v = mesh.view
-    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    d = _ax_desc(mesh)
     _check(lib().bp_cg_direction_ax_hex3d(ctypes.byref(d), mesh.E, v.elementList, _ptr(owner), v.wJ, v.ggeo, v.D,
                                           float(lam), float(alpha), float(beta), _ptr(r),
                                           _ptr(invD) if invD is not None else None, _ptr(p_old), _ptr(p_new), _ptr(x),
@@ -433,7 +444,7 @@ def cg_direction_ax_f32_multi(mesh, nrhs, owner, ops, alpha, beta, r, invD, p_ol
     """bp_cg_direction_ax_f32_multi: the fused step in FP32 on nrhs interleaved
     systems; alpha, beta: sequences of nrhs coefficients."""
     v = mesh.view
-    d = AxDesc(5, mesh.N, int(mesh.affine), 1)
+    d = _ax_desc(mesh, 5)
     a = (ctypes.c_double * nrhs)(*[float(t) for t in alpha])
     b = (ctypes.c_double * nrhs)(*[float(t) for t in beta])
     _check(lib().bp_cg_direction_ax_f32_multi(ctypes.byref(d), nrhs, mesh.E, v.elementList, _ptr(owner),
@@ -463,7 +474,7 @@ def operator_noalloc(mesh, q, Aq, lam=1.0, stream=None, elements=None, nelements
     mesh's E*Np*Nfields) is the element-local length the indices must stay
     below."""
     v = mesh.view
-    d = AxDesc(6 if mesh.Nfields == 3 else 5, mesh.N, int(mesh.affine), mesh.Nfields)
+    d = _ax_desc(mesh)
     if elements is None:
         elements, nelements = v.elementList, mesh.E
     _check(lib().bp_operator_hex3d_noalloc(ctypes.byref(d), int(nelements), _ptr(elements), v.GlobalToLocal, v.wJ,
@@ -482,11 +493,11 @@ def _ptr(b):
 
 class BP:
     """Benchmark problem on a Mesh: bp 1..6 (odd: one field, even: three
-    fields; default 5 or 6 by the mesh's field count)."""
+    fields, two on a Quad2D mesh; default 5 or 6 by the mesh's field count)."""
 
     def __init__(self, mesh, bp=None, lam=1.0, precon="NONE", precision="FP64"):
         self.mesh = mesh
-        bp = bp or (6 if mesh.Nfields == 3 else 5)
+        bp = bp or (6 if mesh.Nfields > 1 else 5)
         pc = {"NONE": BP_PRECON_NONE, "JACOBI": BP_PRECON_JACOBI}[precon.upper()]
         pr = {"FP64": BP_PRECISION_FP64, "MIXED": BP_PRECISION_MIXED}[precision.upper()]
         d = SolverDesc(bp, float(lam), pc, pr)
@@ -622,13 +633,14 @@ def uneven_problems(count=64, seed=2, nrhs=4, pmin=3, pmax=10, nmin=8, nmax=24, 
     return probs
 
 
-def box_numbering(nx, ny, nz, N, Nfields=1):
-    """Host-only masked numbering of the box: (GlobalToLocal, rowStarts, colIds)."""
-    d = BoxDesc(nx, ny, nz, N, 0, Nfields, 0.0, 1)
+def box_numbering(nx, ny, nz, N, Nfields=1, dim=3):
+    """Host-only masked numbering of the box: (GlobalToLocal, rowStarts, colIds).
+    dim=2: the Quad2D box of nx x ny elements (nz ignored)."""
+    d = BoxDesc(nx, ny, nz if dim == 3 else 1, N, 0, Nfields, 0.0, 1, dim)
     ng, nnz = ctypes.c_int32(), ctypes.c_int32()
     _check(lib().bp_box_numbering(ctypes.byref(d), ctypes.byref(ng), ctypes.byref(nnz), None, None, None))
-    E = nx * ny * nz
-    Np = (N + 1) ** 3
+    E = nx * ny * (nz if dim == 3 else 1)
+    Np = (N + 1) ** dim
     g2l = np.empty(E * Np * Nfields, np.int32)
     rs = np.empty(ng.value + 1, np.int32)
     ci = np.empty(nnz.value, np.int32)
@@ -682,9 +694,15 @@ def ogs_check(g2l, rowStarts, colIds, Ngather):
     _check(lib().bp_ogs_check(g.size, g.ctypes.data, int(Ngather), rs.ctypes.data, ci.ctypes.data))
 
 
-def box_vertices(nx, ny, nz, pert=0.0, pert_seed=1):
-    """Host-only vertex coordinates (EX, EY, EZ), each [E*8]."""
-    d = BoxDesc(nx, ny, nz, 1, 0, 1, float(pert), int(pert_seed))
+def box_vertices(nx, ny, nz, pert=0.0, pert_seed=1, dim=3):
+    """Host-only vertex coordinates (EX, EY, EZ), each [E*8]; dim=2: (EX, EY)
+    of the Quad2D box, each [E*4], and an empty EZ."""
+    d = BoxDesc(nx, ny, nz if dim == 3 else 1, 1, 0, 1, float(pert), int(pert_seed), dim)
+    if dim == 2:
+        E = nx * ny
+        ex, ey = np.empty(4 * E), np.empty(4 * E)
+        _check(lib().bp_box_vertices(ctypes.byref(d), ex.ctypes.data, ey.ctypes.data, None))
+        return ex, ey, np.empty(0)
     E = nx * ny * nz
     ex, ey, ez = (np.empty(8 * E) for _ in range(3))
     _check(lib().bp_box_vertices(ctypes.byref(d), ex.ctypes.data, ey.ctypes.data, ez.ctypes.data))

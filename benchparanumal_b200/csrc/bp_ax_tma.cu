@@ -822,7 +822,7 @@ static int launch_ax_tma_pk(const bp_ax_desc_t& d, int32_t Nelements, const int3
 
 bool tma_covers(const bp_ax_desc_t& d, int lanes) {
   const int NQ = d.N + 1;
-  if (d.affine || NQ % 2 != 0) return false;
+  if (d.dim == 2 || d.affine || NQ % 2 != 0) return false;
   if (lanes > 1) return d.Nfields == 1 && (lanes == 2 || lanes == 4) && NQ >= 8 && NQ <= 12;
   return d.Nfields == 1 ? NQ <= 16 : (d.Nfields == 3 && NQ <= 10);
 }

@@ -245,9 +245,14 @@ int bp_event_elapsed_ms(bp_event_t a, bp_event_t b, float* ms) {
 static int check_ax_desc(const bp_ax_desc_t* d) {
   if (!d) return fail(BP_ERROR_ARG, "bp_ax_hex3d: null descriptor");
   if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_hex3d: degree N must be in 1..15");
-  if (d->Nfields != 1 && d->Nfields != 3) return fail(BP_ERROR_ARG, "bp_ax_hex3d: Nfields must be 1 or 3");
+  if (d->dim != 0 && d->dim != 2 && d->dim != 3) return fail(BP_ERROR_ARG, "bp_ax_hex3d: dim must be 2 or 3");
+  const int nf6 = d->dim == 2 ? 2 : 3;   // BP6 has Nfields = dim
+  if (d->Nfields != 1 && d->Nfields != nf6)
+    return fail(BP_ERROR_ARG, d->dim == 2 ? "bp_ax_hex3d: Quad2D Nfields must be 1 or 2"
+                                          : "bp_ax_hex3d: Nfields must be 1 or 3");
   if (d->bp != 5 && d->bp != 6) return fail(BP_ERROR_ARG, "bp_ax_hex3d: bp must be 5 or 6");
-  if ((d->bp == 6) != (d->Nfields == 3)) return fail(BP_ERROR_ARG, "bp_ax_hex3d: BP6 has 3 fields, BP5 one");
+  if ((d->bp == 6) != (d->Nfields == nf6))
+    return fail(BP_ERROR_ARG, "bp_ax_hex3d: BP6 has dim fields, BP5 one");
   return BP_SUCCESS;
 }
 
@@ -390,6 +395,7 @@ int bp_ax_cub_hex3d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* ele
   if (!d) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: null descriptor");
   if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: degree N must be in 1..15");
   if (d->bp < 1 || d->bp > 4) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: bp must be 1..4");
+  if (d->dim == 2) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: the over-integrated forms are Hex3D only");
   if (d->Nfields != ((d->bp % 2) ? 1 : 3)) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: BP1/BP3 have 1 field, BP2/BP4 3");
   if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d: negative element count");
   if (Nelements == 0) return BP_SUCCESS;
@@ -408,6 +414,7 @@ int bp_ax_cub_hex3d_f32(const bp_ax_desc_t* d, int32_t Nelements, const int32_t*
   if (!d) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: null descriptor");
   if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: degree N must be in 1..15");
   if (d->bp < 1 || d->bp > 4) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: bp must be 1..4");
+  if (d->dim == 2) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: the over-integrated forms are Hex3D only");
   if (d->Nfields != ((d->bp % 2) ? 1 : 3))
     return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: BP1/BP3 have 1 field, BP2/BP4 3");
   if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_cub_hex3d_f32: negative element count");
@@ -493,9 +500,65 @@ int bp_update_cg(int32_t N, const double* Ap, double alpha, double* r, double* r
 // ---------------------------------------------------------------------------
 // mesh
 // ---------------------------------------------------------------------------
+// The Quad2D box: vertices, numbering and factors on the host (a 2D box is
+// small next to a 3D one of the same degree), then uploaded.
+static int mesh_create_quad(const bp_box_desc_t* d, bp_mesh_t* out) {
+  if (d->nx < 1 || d->ny < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
+  if (d->Nfields != 1 && d->Nfields != 2) return fail(BP_ERROR_ARG, "bp_mesh_create: Quad2D Nfields must be 1 or 2");
+  if (!(d->pert >= 0.0 && d->pert < 0.5)) return fail(BP_ERROR_ARG, "bp_mesh_create: perturbation must be in [0, 0.5)");
+  const int Nq = d->N + 1, Np = Nq * Nq;
+  const int64_t E64 = (int64_t)d->nx * d->ny;
+  if (E64 * Np * d->Nfields >= (int64_t)INT32_MAX)
+    return fail(BP_ERROR_ARG, "bp_mesh_create: local node count exceeds int32 (dlong) range");
+  cudaStream_t s = default_stream();
+  HostMesh hm;
+  hm.dim = 2;
+  hm.N = d->N; hm.Nq = Nq; hm.Np = Np;
+  hm.nx = d->nx; hm.ny = d->ny; hm.nz = 1;
+  hm.E = (int)E64; hm.affine = d->affine ? 1 : 0; hm.Nfields = d->Nfields;
+  gll_nodes_weights(hm.N, hm.gllz, hm.gllw);
+  diff_matrix(hm.gllz, hm.D);
+  box_vertices_2d(hm, d->pert, d->pert_seed);
+  box_numbering_2d(hm);
+  std::vector<double> wJ, ggeo;
+  if (!quad_geometry(hm, wJ, ggeo))
+    return fail(BP_ERROR_NUMERIC, "bp_mesh_create: non-positive Jacobian found (perturbation too large?)");
+  bp_mesh_s* m = new bp_mesh_s();
+  m->dim = 2;
+  m->N = hm.N; m->Nq = Nq; m->Np = Np; m->E = hm.E; m->Nfields = hm.Nfields; m->affine = hm.affine;
+  m->Ngather = hm.Ngather; m->nnz = hm.nnz;
+  std::vector<int32_t> elist(hm.E);
+  for (int e = 0; e < hm.E; ++e) elist[e] = e;
+  int rc = BP_SUCCESS;
+  do {
+    if ((rc = m->elementList.upload(elist, s))) break;
+    if ((rc = m->G2L.upload(hm.G2L, s))) break;
+    if ((rc = m->rowStarts.upload(hm.rowStarts, s))) break;
+    if ((rc = m->colIds.upload(hm.colIds, s))) break;
+    if ((rc = m->D.upload(hm.D, s))) break;
+    if ((rc = m->gllz.upload(hm.gllz, s))) break;
+    if ((rc = m->gllw.upload(hm.gllw, s))) break;
+    if ((rc = m->EX.upload(hm.EX, s))) break;
+    if ((rc = m->EY.upload(hm.EY, s))) break;
+    if ((rc = m->wJ.upload(wJ, s))) break;
+    if ((rc = m->ggeo.upload(ggeo, s))) break;
+    cudaError_t ce = cudaStreamSynchronize(s);   // the host vectors are released on return
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_mesh_create", __FILE__, __LINE__); break; }
+  } while (0);
+  if (rc != BP_SUCCESS) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return BP_SUCCESS;
+}
+
 int bp_mesh_create(const bp_box_desc_t* d, bp_mesh_t* out) {
   if (!d || !out) return fail(BP_ERROR_ARG, "bp_mesh_create: null pointer");
   *out = nullptr;
+  if (d->dim != 0 && d->dim != 2 && d->dim != 3) return fail(BP_ERROR_ARG, "bp_mesh_create: dim must be 2 or 3");
+  if (d->dim == 2) return mesh_create_quad(d, out);
   if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
   if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
   if (d->Nfields != 1 && d->Nfields != 3) return fail(BP_ERROR_ARG, "bp_mesh_create: Nfields must be 1 or 3");
@@ -572,11 +635,13 @@ int bp_mesh_view(bp_mesh_t m, bp_mesh_view_t* v) {
   v->rowStarts = m->rowStarts.ptr; v->colIds = m->colIds.ptr;
   v->wJ = m->wJ.ptr; v->ggeo = m->ggeo.ptr; v->D = m->D.ptr; v->gllz = m->gllz.ptr; v->gllw = m->gllw.ptr;
   v->EX = m->EX.ptr; v->EY = m->EY.ptr; v->EZ = m->EZ.ptr;
+  v->dim = m->dim;
   return BP_SUCCESS;
 }
 
 int bp_mesh_cubature(bp_mesh_t m) {
   if (!m) return fail(BP_ERROR_ARG, "bp_mesh_cubature: null mesh");
+  if (m->dim == 2) return fail(BP_ERROR_ARG, "bp_mesh_cubature: the over-integrated BP1-BP4 forms are Hex3D only");
   if (m->cubNq) return BP_SUCCESS;
   cudaStream_t s = default_stream();
   std::vector<double> z(m->Nq);
@@ -657,6 +722,7 @@ int bp_mesh_cubature_view(bp_mesh_t m, bp_cubature_view_t* v) {
 
 int bp_mesh_write_vtu(bp_mesh_t m, const double* xL, const char* filename) {
   if (!m || !xL || !filename) return fail(BP_ERROR_ARG, "bp_mesh_write_vtu: null pointer");
+  if (m->dim == 2) return fail(BP_ERROR_ARG, "bp_mesh_write_vtu: Hex3D meshes only");
   const int Nq = m->Nq, Np = m->Np, E = m->E, Nf = m->Nfields, N = m->N;
   std::vector<double> EX((size_t)8 * E), EY((size_t)8 * E), EZ((size_t)8 * E), z(Nq);
   BP_CUDA_TRY(cudaMemcpy(EX.data(), m->EX.ptr, sizeof(double) * EX.size(), cudaMemcpyDeviceToHost));

@@ -195,16 +195,20 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
   if (!S.compare("THREAD MODEL", "CUDA"))
     throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
                              " is not available: this build runs the CUDA (sm_100a) path only");
-  if (!S.compare("ELEMENT TYPE", "Hex"))
-    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex only");
+  const bool quad = S.compare("ELEMENT TYPE", "Quad");
+  if (!S.compare("ELEMENT TYPE", "Hex") && !quad)
+    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex and Quad only");
+  if (quad && bp <= 4)
+    throw std::runtime_error("ELEMENT TYPE Quad is available for BK5/BK6 and BP5/BP6 (BP1-BP4: Hex only)");
   check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
   bp_box_desc_t d{};
+  d.dim = quad ? 2 : 3;
   d.nx = std::atoi(S.get("BOX NX").c_str());
   d.ny = std::atoi(S.get("BOX NY").c_str());
-  d.nz = std::atoi(S.get("BOX NZ").c_str());
+  d.nz = quad ? 1 : std::atoi(S.get("BOX NZ").c_str());
   d.N = std::atoi(S.get("POLYNOMIAL DEGREE").c_str());
   d.affine = S.compare("AFFINE MESH", "TRUE") ? 1 : 0;
-  d.Nfields = Nfields;
+  d.Nfields = quad && Nfields > 1 ? 2 : Nfields;   // BP6 has Nfields = dim
   d.pert = std::atof(S.get("VERTEX PERTURBATION").c_str());
   d.pert_seed = std::strtoull(S.get("PERTURBATION SEED").c_str(), nullptr, 10);
   check(bp_mesh_create(&d, &P.mesh));
@@ -240,13 +244,15 @@ struct DevVec32 {
 double ax_bytes(int bp, const bp_mesh_view_t& v, long long Ndofs, double sv = 8.0) {
   const double E = v.Nelements, Np = v.Np, Nf = v.Nfields;
   const double cNq = v.N + 2, cNp = cNq * cNq * cNq;
-  const double per_point = bp <= 2 ? 1.0 : 7.0;          // J, or ggeo + wJ
+  const double per_point = bp <= 2 ? 1.0 : (v.dim == 2 ? 4.0 : 7.0);   // J, or ggeo + wJ (mesh.dim==3 ? 7 : 4)
   const double points = v.affine ? 1.0 : (bp <= 4 ? cNp : Np);
   return Ndofs * sv + (points * per_point * sv + 4.0 + Np * Nf * 4.0 + Np * Nf * sv) * E;
 }
 // reference flop model for one Ax application (the same files, Hex branches)
 double ax_flops(int bp, const bp_mesh_view_t& v) {
   const double Nq = v.Nq, E = v.Nelements, Nf = v.Nfields;
+  if (v.dim == 2)   // QUADRILATERALS branches of bp5Run.cpp:144-187
+    return (v.affine ? 8 * Nq * Nq * Nq + 12 * Nq * Nq : 8 * Nq * Nq * Nq + 8 * Nq * Nq) * Nf * E;
   const double cNq = v.N + 2, Nq3 = Nq * Nq * Nq, cNq3 = cNq * cNq * cNq;
   const double interp = 4 * cNq * Nq3 + 4 * cNq * cNq * Nq * Nq + 4 * cNq3 * Nq;
   double f;
@@ -271,6 +277,7 @@ void cg_model(int bp, const bp_mesh_view_t& v, long long Ndofs, int Niter, doubl
 // every system's unknowns x iterations
 int run_bp_batch(const char* name, int bp, Settings& S, int nr) {
   if (bp % 2 == 0) throw std::runtime_error("-nr is available for BP1, BP3 and BP5");
+  if (!S.compare("ELEMENT TYPE", "Hex")) throw std::runtime_error("-nr is available for Hex meshes");
   if (!S.compare("FORCING", "RANDOM")) throw std::runtime_error("-nr needs -f RANDOM");
   if (!S.compare("THREAD MODEL", "CUDA"))
     throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
@@ -380,7 +387,7 @@ int run_bp(const char* name, int bp, Settings& S) {
   const double Nbytes = (4 * Ndofs * 8.0 + NbytesAx + NbytesGather) + (11 * Ndofs * 8.0 + NbytesAx + NbytesGather) * Niter;
   const double NflopsAx = ax_flops(bp, P.view);
   const double Nflops = (5.0 * Ndofs + NflopsAx + NGlobal) + (11.0 * Ndofs + NflopsAx + NGlobal) * Niter;
-  std::string suffix = "Element=Hex";
+  std::string suffix = P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, iterations=%d, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
@@ -431,18 +438,21 @@ int run_bk(const char* name, int bk, Settings& S) {
   d.bp = bk;
   d.N = P.view.N;
   d.affine = P.view.affine;
-  d.Nfields = Nfields;
+  d.Nfields = P.view.Nfields;
+  d.dim = P.view.dim;
   // -fp MIXED times the FP32 operator of the mixed-precision solver (BK5/BK6)
   const bool fp32 = S.compare("PRECISION", "MIXED");
   const size_t ng = P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.view.Np;
   const int nr = std::atoi(S.get("RIGHT-HAND SIDES").c_str());
   if (nr > 1 && (!fp32 || bk != 5)) throw std::runtime_error("-nr is available for BK5 with -fp MIXED");
-  DevVec32 wJ32(fp32 ? ng : 0), ggeo32(fp32 ? 6 * ng : 0), gllw32(fp32 ? P.view.Nq : 0),
+  const size_t nggeo = P.view.dim == 2 ? 3 : 6;
+  if (nr > 1 && P.view.dim == 2) throw std::runtime_error("-nr is available for Hex meshes");
+  DevVec32 wJ32(fp32 ? ng : 0), ggeo32(fp32 ? nggeo * ng : 0), gllw32(fp32 ? P.view.Nq : 0),
       D32(fp32 ? (size_t)P.view.Nq * P.view.Nq : 0), q32(fp32 ? (size_t)Ngather * nr : 0),
       Aq32(fp32 ? (size_t)P.view.Nlocal * nr : 0);
   if (fp32) {
     check(bp_convert_f64_f32(ng, P.view.wJ, wJ32.p, nullptr));
-    check(bp_convert_f64_f32(6 * ng, P.view.ggeo, ggeo32.p, nullptr));
+    check(bp_convert_f64_f32(nggeo * ng, P.view.ggeo, ggeo32.p, nullptr));
     check(bp_convert_f64_f32(P.view.Nq, P.view.gllw, gllw32.p, nullptr));
     check(bp_convert_f64_f32((size_t)P.view.Nq * P.view.Nq, P.view.D, D32.p, nullptr));
     // every right-hand side gets the same input (the timing does not depend on the values)
@@ -500,7 +510,7 @@ int run_bk(const char* name, int bk, Settings& S) {
   double Nbytes = ax_bytes(bk, P.view, Ndofs, fp32 ? 4.0 : 8.0);
   if (nr > 1) Nbytes += (nr - 1) * (Ndofs * 4.0 + (double)P.view.Nlocal * 4.0);
   const double Nflops = ax_flops(bk, P.view) * nr;
-  std::string suffix = "Element=Hex";
+  std::string suffix = P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "

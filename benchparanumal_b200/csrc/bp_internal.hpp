@@ -115,6 +115,7 @@ struct DeviceArray {
 // ---- host-side mesh description produced by the setup code ----
 struct HostMesh {
   int N = 0, Nq = 0, Np = 0, nx = 0, ny = 0, nz = 0, E = 0, affine = 0, Nfields = 1;
+  int dim = 3;                           // 2: Quad2D (Np = Nq^2, 4 vertices, 3 factors)
   std::vector<double> gllz, gllw, D;
   std::vector<double> EX, EY, EZ;        // E*8 (perturbed vertices)
   int32_t Ngather = 0, nnz = 0;
@@ -143,6 +144,13 @@ void cubature_basis(int N, const std::vector<double>& gllz, CubBasis& cb);
 void box_vertices(HostMesh& m, double pert, uint64_t seed);
 // masked gathered numbering, CSR and GlobalToLocal for the box
 void box_numbering(HostMesh& m);
+// the same for the Quad2D box (dim 2): vertices [E*4], numbering, and the
+// geometric factors at the GLL nodes (wJ, ggeo = G00, G01, G11 with the weights
+// folded in; affine: per element, without weights).  quad_geometry returns
+// false on a Jacobian below 1e-8 (the reference's check).
+void box_vertices_2d(HostMesh& m, double pert, uint64_t seed);
+void box_numbering_2d(HostMesh& m);
+bool quad_geometry(const HostMesh& m, std::vector<double>& wJ, std::vector<double>& ggeo);
 
 // trilinear map of the eight hex vertices v (mesh_t vertex order) at (r,s,t)
 __host__ __device__ inline double trilinear(const double* v, double r, double s, double t) {
@@ -157,6 +165,7 @@ __host__ __device__ inline double trilinear(const double* v, double r, double s,
 // ---- the opaque objects of the C ABI ----
 struct bp_mesh_s {
   int N, Nq, Np, E, Nfields, affine;
+  int dim = 3;                                  // 2: Quad2D
   int32_t Ngather, nnz;
   bp::DeviceArray<int32_t> elementList, G2L, rowStarts, colIds;
   // GlobalToLocal with the owner bit (kOwnerBit) of each gathered node's first
@@ -335,6 +344,22 @@ int launch_ax_mma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const
                          const int32_t* G2L, const float* wJ, const float* ggeo, const float* D, float lambda,
                          const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                          int* nblocks);
+// Quad2D forms (bp_ax_quad.cu): the BP5/BP6 element operator (FP64 and FP32;
+// 1 with a fused direction update, which it does not take), the forcing, the
+// lumped mass and the element diagonal
+int launch_ax_quad(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const double* wJ, const double* ggeo, const double* gllw, const double* D, double lambda,
+                   const double* q, double* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+int launch_ax_quad(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                   const float* wJ, const float* ggeo, const float* gllw, const float* D, float lambda,
+                   const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks);
+int launch_rhs_analytic_quad(int N, int affine, int Nfields, int E, const double* EX, const double* EY,
+                             const double* gllz, const double* gllw, const double* wJ, double lambda, double* rL,
+                             cudaStream_t s);
+int launch_mass_local_quad(int N, int affine, int Nfields, int E, const int32_t* G2L, const double* gllw,
+                           const double* wJ, const double* f, double* rL, cudaStream_t s);
+int launch_diag_local_quad(int N, int affine, int Nfields, int E, const double* ggeo, const double* wJ,
+                           const double* gllw, const double* D, double lambda, double* dL, cudaStream_t s);
 // whether the TMA form covers d with `lanes` values per node (1, or 2 or 4
 // packed FP32 lanes); with factor arrays 16-byte aligned
 bool tma_covers(const bp_ax_desc_t& d, int lanes);

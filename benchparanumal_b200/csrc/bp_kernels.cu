@@ -298,6 +298,7 @@ int launch_ax_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int
                      const int32_t* G2L, const float* wJ, const float* ggeo, const float* gllw, const float* D,
                      float lambda, const float* q, float* Aq, const int* skip, const CgFuse* fuse, cudaStream_t s,
                      int* nblocks) {
+  if (d.dim == 2) return fail(BP_ERROR_ARG, "packed element operator: Hex3D only");
   auto run = [&](int f, const int* sk) -> int {
     switch (f) {
       case FORM_MMA:
@@ -350,6 +351,11 @@ static int launch_ax_t(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* 
                        const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda, const F* q, F* Aq,
                        const int* skip, cudaStream_t s, const CgFuse* fuse, int* nblocks) {
   if (nblocks) *nblocks = 0;
+  if (d.dim == 2) {
+    const int rc = launch_ax_quad(d, Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, q, Aq, skip, fuse, s,
+                                  nblocks);
+    return rc == 1 ? fail(BP_ERROR_ARG, "Quad2D operator: no fused direction update") : rc;
+  }
   if (Nelements == 0) return BP_SUCCESS;
   switch (d.N + 1) {
 #define BP_AX_CASE(nq) \

@@ -339,6 +339,161 @@ void box_numbering(HostMesh& m) {
   }
 }
 
+// Quad2D box (meshSetupBoxQuad2D.cpp:30-100): element e = i + j nx, vertices
+// (i,j), (i+1,j), (i+1,j+1), (i,j+1); the seeded perturbation of the Hex3D box
+// in two coordinates (two draws per vertex id, x and y interleaved).
+void box_vertices_2d(HostMesh& m, double pert, uint64_t seed) {
+  const int nx = m.nx, ny = m.ny;
+  const int64_t NnX = nx + 1, NnY = ny + 1;
+  const double dx = 2.0 / nx, dy = 2.0 / ny;
+  m.EX.resize((size_t)m.E * 4);
+  m.EY.resize((size_t)m.E * 4);
+  m.EZ.clear();
+  std::vector<double> u;
+  if (pert != 0.0) {
+    u.resize((size_t)2 * NnX * NnY);
+    uint64_t x = 6364136223846793005ULL * (~seed) + 1ULL;
+    const double scale = 1.0 / (double)std::numeric_limits<uint64_t>::max();
+    for (size_t r = 0; r < u.size(); ++r) {
+      u[r] = (double)x * scale;
+      x = 6364136223846793005ULL * x + 1ULL;
+    }
+  }
+  static const int ci[4] = {0, 1, 1, 0};
+  static const int cj[4] = {0, 0, 1, 1};
+  for (int e = 0; e < m.E; ++e) {
+    const int i = e % nx, j = e / nx;
+    const double x0 = -1.0 + dx * i, y0 = -1.0 + dy * j;
+    for (int c = 0; c < 4; ++c) {
+      double X = ci[c] ? x0 + dx : x0;
+      double Y = cj[c] ? y0 + dy : y0;
+      const int64_t I = i + ci[c], J = j + cj[c];
+      if (pert != 0.0 && I > 0 && I < nx && J > 0 && J < ny) {
+        const int64_t g = I + J * NnX;
+        X += pert * dx * (2 * u[2 * g + 0] - 1);
+        Y += pert * dy * (2 * u[2 * g + 1] - 1);
+      }
+      m.EX[(size_t)e * 4 + c] = X;
+      m.EY[(size_t)e * 4 + c] = Y;
+    }
+  }
+}
+
+// The masked numbering of the Quad2D box in the closed form of box_numbering:
+// row r is the r-th unmasked connectivity class in order of first appearance
+// over the local index e*Np*Nf + f*Np + n (the reference's order at one rank).
+void box_numbering_2d(HostMesh& m) {
+  const int N = m.N, Nq = m.Nq, Np = m.Np, Nf = m.Nfields;
+  const Axis ax{m.nx, N}, ay{m.ny, N};
+  const int E = m.E;
+  std::vector<int64_t> rowBase((size_t)E + 1, 0);
+  for (int e = 0; e < E; ++e) {
+    const int ex = e % m.nx, ey = e / m.nx;
+    rowBase[e + 1] = rowBase[e] + (int64_t)Nf * ax.reps(ex) * ay.reps(ey);
+  }
+  m.Ngather = (int32_t)rowBase[E];
+  auto row_of = [&](int ex, int ey, int i, int j, int f) -> int32_t {
+    const int e = ex + m.nx * ey;
+    const int ci = ax.reps(ex), cj = ay.reps(ey);
+    return (int32_t)(rowBase[e] + (int64_t)f * ci * cj + (int64_t)(j - 1) * ci + (i - 1));
+  };
+  m.rowStarts.assign((size_t)m.Ngather + 1, 0);
+  for (int e = 0; e < E; ++e) {
+    const int ex = e % m.nx, ey = e / m.nx;
+    for (int j = 1; j <= ay.reps(ey); ++j)
+      for (int i = 1; i <= ax.reps(ex); ++i) {
+        const int mult = ax.count(ex * N + i) * ay.count(ey * N + j);
+        for (int f = 0; f < Nf; ++f) m.rowStarts[(size_t)row_of(ex, ey, i, j, f) + 1] = mult;
+      }
+  }
+  for (int32_t r = 0; r < m.Ngather; ++r) m.rowStarts[r + 1] += m.rowStarts[r];
+  m.nnz = m.rowStarts[m.Ngather];
+  m.colIds.assign((size_t)m.nnz, 0);
+  m.G2L.assign((size_t)E * Np * Nf, -1);
+  for (int e = 0; e < E; ++e) {
+    const int ex = e % m.nx, ey = e / m.nx;
+    for (int j = 0; j < Nq; ++j) {
+      const int LJ = ey * N + j;
+      if (ay.boundary(LJ)) continue;
+      const int ry = ay.first(LJ);
+      for (int i = 0; i < Nq; ++i) {
+        const int LI = ex * N + i;
+        if (ax.boundary(LI)) continue;
+        const int rx = ax.first(LI);
+        const int n = i + Nq * j;
+        const int pos = (ey - ry) * ax.count(LI) + (ex - rx);
+        for (int f = 0; f < Nf; ++f) {
+          const int32_t row = row_of(rx, ry, LI - rx * N, LJ - ry * N, f);
+          const int64_t l = ((int64_t)e * Nf + f) * Np + n;
+          m.G2L[(size_t)l] = row;
+          m.colIds[(size_t)m.rowStarts[row] + pos] = (int32_t)l;
+        }
+      }
+    }
+  }
+}
+
+// GeometricFactorsQuad2D (meshGeometricFactorsQuad2D.cpp:31-120) from the
+// bilinear map of the vertices at the GLL nodes (meshPhysicalNodesQuad2D.cpp)
+bool quad_geometry(const HostMesh& m, std::vector<double>& wJ, std::vector<double>& ggeo) {
+  const int Nq = m.Nq, Np = m.Np;
+  bool ok = true;
+  if (m.affine) {
+    wJ.resize(m.E);
+    ggeo.resize((size_t)3 * m.E);
+    for (int e = 0; e < m.E; ++e) {
+      const double* ex = &m.EX[(size_t)e * 4];
+      const double* ey = &m.EY[(size_t)e * 4];
+      const double xr = 0.5 * (ex[1] - ex[0]), xs = 0.5 * (ex[3] - ex[0]);
+      const double yr = 0.5 * (ey[1] - ey[0]), ys = 0.5 * (ey[3] - ey[0]);
+      const double J = xr * ys - xs * yr;
+      if (!(J >= 1e-8)) ok = false;
+      const double rx = ys / J, ry = -xs / J, sx = -yr / J, sy = xr / J;
+      wJ[e] = J;
+      ggeo[3 * (size_t)e + 0] = J * (rx * rx + ry * ry);
+      ggeo[3 * (size_t)e + 1] = J * (rx * sx + ry * sy);
+      ggeo[3 * (size_t)e + 2] = J * (sx * sx + sy * sy);
+    }
+    return ok;
+  }
+  wJ.resize((size_t)m.E * Np);
+  ggeo.resize((size_t)3 * m.E * Np);
+  std::vector<double> x(Np), y(Np);
+#pragma omp parallel for firstprivate(x, y) reduction(&& : ok)
+  for (int e = 0; e < m.E; ++e) {
+    const double* ex = &m.EX[(size_t)e * 4];
+    const double* ey = &m.EY[(size_t)e * 4];
+    for (int j = 0; j < Nq; ++j)
+      for (int i = 0; i < Nq; ++i) {
+        const double r = m.gllz[i], s = m.gllz[j];
+        const double a0 = 0.25 * (1 - r) * (1 - s), a1 = 0.25 * (1 + r) * (1 - s), a2 = 0.25 * (1 + r) * (1 + s),
+                     a3 = 0.25 * (1 - r) * (1 + s);
+        x[i + j * Nq] = a0 * ex[0] + a1 * ex[1] + a2 * ex[2] + a3 * ex[3];
+        y[i + j * Nq] = a0 * ey[0] + a1 * ey[1] + a2 * ey[2] + a3 * ey[3];
+      }
+    for (int j = 0; j < Nq; ++j)
+      for (int i = 0; i < Nq; ++i) {
+        double xr = 0, xs = 0, yr = 0, ys = 0;
+        for (int mm = 0; mm < Nq; ++mm) {
+          xr += m.D[i * Nq + mm] * x[j * Nq + mm];
+          xs += m.D[j * Nq + mm] * x[mm * Nq + i];
+          yr += m.D[i * Nq + mm] * y[j * Nq + mm];
+          ys += m.D[j * Nq + mm] * y[mm * Nq + i];
+        }
+        const double J = xr * ys - xs * yr;
+        if (!(J >= 1e-8)) ok = false;
+        const double rx = ys / J, ry = -xs / J, sx = -yr / J, sy = xr / J;
+        const double JW = J * m.gllw[i] * m.gllw[j];
+        const size_t id = (size_t)e * Np + i + j * Nq;
+        wJ[id] = JW;
+        ggeo[3 * id + 0] = JW * (rx * rx + ry * ry);
+        ggeo[3 * id + 1] = JW * (rx * sx + ry * sy);
+        ggeo[3 * id + 2] = JW * (sx * sx + sy * sy);
+      }
+  }
+  return ok;
+}
+
 }  // namespace bp
 
 // ---------------------------------------------------------------------------
@@ -347,11 +502,15 @@ void box_numbering(HostMesh& m) {
 namespace {
 int host_mesh_from_desc(const bp_box_desc_t* d, bp::HostMesh& m) {
   if (!d) return bp::fail(BP_ERROR_ARG, "null descriptor");
-  if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->N < 1 || d->N > 15 || (d->Nfields != 1 && d->Nfields != 3))
+  if (d->dim != 0 && d->dim != 2 && d->dim != 3) return bp::fail(BP_ERROR_ARG, "box dim must be 2 or 3");
+  m.dim = d->dim == 2 ? 2 : 3;
+  const int nz = m.dim == 2 ? 1 : d->nz;
+  if (d->nx < 1 || d->ny < 1 || nz < 1 || d->N < 1 || d->N > 15 ||
+      (m.dim == 3 && d->Nfields != 1 && d->Nfields != 3) || (m.dim == 2 && d->Nfields != 1 && d->Nfields != 2))
     return bp::fail(BP_ERROR_ARG, "bad box descriptor");
-  m.N = d->N; m.Nq = d->N + 1; m.Np = m.Nq * m.Nq * m.Nq;
-  m.nx = d->nx; m.ny = d->ny; m.nz = d->nz;
-  const int64_t E = (int64_t)d->nx * d->ny * d->nz;
+  m.N = d->N; m.Nq = d->N + 1; m.Np = m.dim == 2 ? m.Nq * m.Nq : m.Nq * m.Nq * m.Nq;
+  m.nx = d->nx; m.ny = d->ny; m.nz = nz;
+  const int64_t E = (int64_t)d->nx * d->ny * nz;
   if (E * m.Np * d->Nfields >= (int64_t)INT32_MAX) return bp::fail(BP_ERROR_ARG, "local node count exceeds int32");
   m.E = (int)E; m.affine = d->affine ? 1 : 0; m.Nfields = d->Nfields;
   return BP_SUCCESS;
@@ -363,7 +522,8 @@ extern "C" int bp_box_numbering(const bp_box_desc_t* d, int32_t* Ngather, int32_
   bp::HostMesh m;
   int rc = host_mesh_from_desc(d, m);
   if (rc) return rc;
-  bp::box_numbering(m);
+  if (m.dim == 2) bp::box_numbering_2d(m);
+  else bp::box_numbering(m);
   if (Ngather) *Ngather = m.Ngather;
   if (nnz) *nnz = m.nnz;
   if (G2L) std::copy(m.G2L.begin(), m.G2L.end(), G2L);
@@ -405,7 +565,8 @@ extern "C" int bp_box_vertices(const bp_box_desc_t* d, double* EX, double* EY, d
   bp::HostMesh m;
   int rc = host_mesh_from_desc(d, m);
   if (rc) return rc;
-  bp::box_vertices(m, d->pert, d->pert_seed);
+  if (m.dim == 2) bp::box_vertices_2d(m, d->pert, d->pert_seed);
+  else bp::box_vertices(m, d->pert, d->pert_seed);
   if (EX) std::copy(m.EX.begin(), m.EX.end(), EX);
   if (EY) std::copy(m.EY.begin(), m.EY.end(), EY);
   if (EZ) std::copy(m.EZ.begin(), m.EZ.end(), EZ);

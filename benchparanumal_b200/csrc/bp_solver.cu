@@ -623,12 +623,13 @@ static int mesh_fp32(bp_solver_s* S, cudaStream_t s) {
   const size_t nD = cub ? (mesh->affine ? mesh->cubDmodal.n : mesh->cubD.n) : mesh->D.n;
   const size_t nT = cub ? (mesh->affine ? mesh->MM.n : mesh->cubInterp.n) : 0;
   BP_TRY(f.wJ.alloc(ng));
-  BP_TRY(f.ggeo.alloc(6 * ng));
+  const int nggeo = mesh->dim == 2 ? 3 : 6;   // factors per node (per element when affine)
+  BP_TRY(f.ggeo.alloc(nggeo * ng));
   BP_TRY(f.D.alloc(nD));
   BP_TRY(f.gllw.alloc(mesh->gllw.n));
   BP_TRY(f.T.alloc(nT));
   BP_TRY(to_float(o.wJ, f.wJ.ptr, ng, s));
-  BP_TRY(to_float(o.ggeo, f.ggeo.ptr, 6 * ng, s));
+  BP_TRY(to_float(o.ggeo, f.ggeo.ptr, nggeo * ng, s));
   BP_TRY(to_float(o.D, f.D.ptr, nD, s));
   BP_TRY(to_float(mesh->gllw.ptr, f.gllw.ptr, mesh->gllw.n, s));
   if (nT) BP_TRY(to_float(o.T, f.T.ptr, nT, s));
@@ -970,8 +971,13 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
   if (!mesh || !d || !out) return fail(BP_ERROR_ARG, "bp_solver_create: null pointer");
   *out = nullptr;
   if (d->bp < 1 || d->bp > 6) return fail(BP_ERROR_ARG, "bp_solver_create: bp must be 1..6");
-  if ((d->bp % 2 == 0) != (mesh->Nfields == 3))
+  if (mesh->dim == 2) {
+    if (d->bp < 5) return fail(BP_ERROR_ARG, "bp_solver_create: Quad2D meshes take BP5 and BP6 (the BP1-BP4 forms are Hex3D only)");
+    if ((d->bp == 6) != (mesh->Nfields == 2))
+      return fail(BP_ERROR_ARG, "bp_solver_create: Quad2D BP6 needs a 2-field mesh, BP5 a 1-field mesh");
+  } else if ((d->bp % 2 == 0) != (mesh->Nfields == 3)) {
     return fail(BP_ERROR_ARG, "bp_solver_create: BP2/BP4/BP6 need a 3-field mesh, BP1/BP3/BP5 a 1-field mesh");
+  }
   if (d->precon != BP_PRECON_NONE && d->precon != BP_PRECON_JACOBI)
     return fail(BP_ERROR_ARG, "bp_solver_create: unknown preconditioner");
   if (d->precision != BP_PRECISION_FP64 && d->precision != BP_PRECISION_MIXED)
@@ -989,6 +995,7 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
   S->ax.N = mesh->N;
   S->ax.affine = mesh->affine;
   S->ax.Nfields = mesh->Nfields;
+  S->ax.dim = mesh->dim;
   const size_t NL = (size_t)mesh->E * mesh->Np * mesh->Nfields;
   int rc = BP_SUCCESS;
   do {
@@ -1063,8 +1070,12 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
   if (mode == BP_RHS_ANALYTIC) {
     // BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
     const double lam = S->bp <= 2 ? 0.0 : S->lambda;
-    BP_TRY(launch_rhs_analytic(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->EZ.ptr, m->gllz.ptr,
-                               m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
+    if (m->dim == 2)
+      BP_TRY(launch_rhs_analytic_quad(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->gllz.ptr,
+                                      m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
+    else
+      BP_TRY(launch_rhs_analytic(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->EZ.ptr, m->gllz.ptr,
+                                 m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
   } else if (mode == BP_RHS_RANDOM) {
     DeviceArray<double> ftmp;
     double* f = f_out;
@@ -1073,8 +1084,12 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
       f = ftmp.ptr;
     }
     BP_TRY(launch_rhs_random(S->N, seed, f, s));
-    BP_TRY(launch_mass_local(m->N, m->affine, m->Nfields, m->E, m->G2L.ptr, m->gllw.ptr, m->wJ.ptr, f, S->AqL.ptr,
-                             s));
+    if (m->dim == 2)
+      BP_TRY(launch_mass_local_quad(m->N, m->affine, m->Nfields, m->E, m->G2L.ptr, m->gllw.ptr, m->wJ.ptr, f,
+                                    S->AqL.ptr, s));
+    else
+      BP_TRY(launch_mass_local(m->N, m->affine, m->Nfields, m->E, m->G2L.ptr, m->gllw.ptr, m->wJ.ptr, f, S->AqL.ptr,
+                               s));
     BP_TRY(launch_gather(m->Ngather, m->rowStarts.ptr, m->colIds.ptr, S->AqL.ptr, b, s));
     BP_CUDA_TRY(cudaStreamSynchronize(s));   // ftmp is released on return
     return BP_SUCCESS;
@@ -1090,7 +1105,10 @@ int bp_solver_diagonal(bp_solver_t S, double* diag) {
   if (!S || !diag) return fail(BP_ERROR_ARG, "bp_solver_diagonal: null pointer");
   bp_mesh_s* m = S->mesh;
   cudaStream_t s = default_stream();
-  if (S->bp >= 5) {
+  if (S->bp >= 5 && m->dim == 2) {
+    BP_TRY(launch_diag_local_quad(m->N, m->affine, m->Nfields, m->E, m->ggeo.ptr, m->wJ.ptr, m->gllw.ptr, m->D.ptr,
+                                  S->lambda, S->AqL.ptr, s));
+  } else if (S->bp >= 5) {
     BP_TRY(launch_diag_local(m->N, m->affine, m->Nfields, m->E, m->ggeo.ptr, m->wJ.ptr, m->gllw.ptr, m->D.ptr,
                              S->lambda, S->AqL.ptr, s));
   } else {

@@ -83,7 +83,10 @@ typedef struct bp_ax_desc {
                         bp_ax_hex3d takes 5/6, bp_ax_cub_hex3d 1..4               */
   int32_t N;         /* polynomial degree 1..15 (p_N)                             */
   int32_t affine;    /* 1: per-element factors (bp5AxAffineHex3D)                 */
-  int32_t Nfields;   /* 1 or 3 (p_Nfields)                                        */
+  int32_t Nfields;   /* 1 or 3 (p_Nfields); Quad2D BP6: 2 (Nfields = dim)          */
+  int32_t dim;       /* 0 or 3: Hex3D; 2: Quad2D (bp 5/6 only: bp5AxQuad2D,
+                        bp5AxAffineQuad2D, bp6AxQuad2D of okl/; ggeo holds
+                        G00, G01, G11 per node, or per element when affine)     */
 } bp_ax_desc_t;
 
 /* Element-local stiffness + lambda*mass operator, Aq[e] = A_e q[GlobalToLocal].
@@ -255,6 +258,9 @@ typedef struct bp_box_desc {
   int32_t Nfields;      /* 1 (BP1/3/5) or 3 (BP2/4/6)                              */
   double pert;          /* interior vertex perturbation, fraction of h (0 = none)  */
   uint64_t pert_seed;   /* LCG seed of the perturbation                            */
+  int32_t dim;          /* 0 or 3: Hex3D box nx x ny x nz (-e Hex); 2: Quad2D box
+                           nx x ny (-e Quad, meshSetupBoxQuad2D.cpp:30-100; nz
+                           ignored; Nfields 1 or 2)                                */
 } bp_box_desc_t;
 
 typedef struct bp_mesh_view {
@@ -272,9 +278,11 @@ typedef struct bp_mesh_view {
   const double* D;                /* [Nq*Nq]                                      */
   const double* gllz;             /* [Nq]                                         */
   const double* gllw;             /* [Nq]                                         */
-  const double* EX;               /* [E*8] vertex coordinates                     */
+  const double* EX;               /* [E*8] vertex coordinates (Quad2D: [E*4])    */
   const double* EY;
-  const double* EZ;
+  const double* EZ;               /* NULL for Quad2D                              */
+  int32_t dim;                    /* 3, or 2 for Quad2D: Np = Nq^2, ggeo [E*Np*3]
+                                     (affine [E*3]), G00, G01, G11               */
 } bp_mesh_view_t;
 
 int bp_mesh_create(const bp_box_desc_t* desc, bp_mesh_t* mesh);

@@ -37,14 +37,21 @@
  * The BP1-BP4 over-integrated forms follow libs/mesh/meshCubatureSetupHex3D.cpp
  * and okl/bp{1,3}Ax{,Affine}Hex3D.okl.
  *
- * PARITY UNPINNED against the reference's own outputs: the reference ships no
- * tests, golden vectors or fixtures for this path, and it cannot be built in
- * this environment (its OCCA submodule is empty; MPI and LAPACK are absent), so
- * no reference run can produce them.  The restatement is pinned instead by
- * known answers of the mathematics it restates (tests/test_oracle.py,
- * tests/test_cub_host.py): quadrature and differentiation exactness, the
- * numbering invariants, affine/curved agreement, symmetry and positivity, and
- * spectral convergence of a manufactured solution.
+ * Quad2D (the reference's other tensor-product element, BP5/BP6 with Nfields
+ * = dim): libs/mesh/meshSetupBoxQuad2D.cpp:30-100, meshBasisQuad2D.cpp:55-170,
+ * meshPhysicalNodesQuad2D.cpp, meshGeometricFactorsQuad2D.cpp:31-120,
+ * okl/bp5AxQuad2D.okl, okl/bp5AxAffineQuad2D.okl, okl/rhsQuad2D.okl.
+ *
+ * Parity pin: the reference ships no tests or golden vectors for this path and
+ * its full build needs OCCA, MPI and LAPACK, none present; its host set-up
+ * code, though, is compiled here against host-only shims (oracle/Makefile,
+ * target ref) and its numbering, CSR, basis, geometric factors and host
+ * gather/scatter are stored as fixtures (tests/golden/); tests/test_ref_golden.py
+ * holds this restatement to them (integers bit-exact).  The element kernels
+ * (OKL) need OCCA; their restatement here is pinned by known answers of the
+ * mathematics (tests/test_oracle.py, tests/test_cub_host.py): quadrature and
+ * differentiation exactness, affine/curved agreement, symmetry and positivity,
+ * and spectral convergence of a manufactured solution.
  */
 #include <algorithm>
 #include <cmath>
@@ -330,6 +337,7 @@ extern "C" int bpo_mass_matrix1d(int N, const double* r, double* MMout) {
 /* ------------------------------------------------------------------------ */
 struct bpo_mesh {
   int N, Nq, Np, Nfp, nx, ny, nz, E, affine, Nfields;
+  int dim = 3, Nfaces = 6, Nverts = 8, Nggeo = 6;   // Quad2D: 2, 4, 4, 3
   std::vector<double> gllz, gllw, D, MM;
   std::vector<double> r, s, t;          // reference node coordinates (Np)
   std::vector<int> faceNodes;            // 6*Nfp
@@ -668,8 +676,8 @@ static void masked_ogs(bpo_mesh& m) {
       for (int f = 0; f < Nf; ++f)
         m.maskedIds[(size_t)e * Np * Nf + f * Np + n] = m.globalIds[(size_t)e * Np + n] * Nf + f;
   for (dlong e = 0; e < m.E; ++e)
-    for (int f = 0; f < 6; ++f)
-      if (m.EToE[f + e * 6] < 0)
+    for (int f = 0; f < m.Nfaces; ++f)
+      if (m.EToE[f + e * m.Nfaces] < 0)
         for (int n = 0; n < Nfp; ++n)
           for (int nf = 0; nf < Nf; ++nf)
             m.maskedIds[(size_t)e * Np * Nf + nf * Np + m.faceNodes[n + f * Nfp]] = 0;
@@ -744,11 +752,296 @@ extern "C" bpo_mesh* bpo_mesh_create(int nx, int ny, int nz, int N, int affine, 
   return m;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Quad2D (2D tensor-product elements)                                        */
+/* ------------------------------------------------------------------------ */
+static const int kEdgeVertices[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};   // meshSetElementType.cpp:56
+
+static inline double bilinear(const double* v, double rn, double sn) {
+  return 0.25 * (1 - rn) * (1 - sn) * v[0] + 0.25 * (1 + rn) * (1 - sn) * v[1] + 0.25 * (1 + rn) * (1 + sn) * v[2] +
+         0.25 * (1 - rn) * (1 + sn) * v[3];
+}
+
+/* NodesQuad2D / FaceNodesQuad2D, meshBasisQuad2D.cpp:31-86 */
+static void reference_nodes_2d(bpo_mesh& m) {
+  const int Nq = m.Nq;
+  m.r.resize(m.Np); m.s.resize(m.Np); m.t.assign(m.Np, 0.0);
+  for (int j = 0; j < Nq; ++j)
+    for (int i = 0; i < Nq; ++i) {
+      m.r[i + j * Nq] = m.gllz[i];
+      m.s[i + j * Nq] = m.gllz[j];
+    }
+  const double tol = 1000. * std::numeric_limits<double>::epsilon() * 0.5;
+  m.faceNodes.assign(4 * m.Nfp, 0);
+  int cnt[4] = {0, 0, 0, 0};
+  for (int n = 0; n < m.Np; ++n) {
+    if (std::fabs(m.s[n] + 1) < tol) m.faceNodes[0 * m.Nfp + cnt[0]++] = n;
+    if (std::fabs(m.r[n] - 1) < tol) m.faceNodes[1 * m.Nfp + cnt[1]++] = n;
+    if (std::fabs(m.s[n] - 1) < tol) m.faceNodes[2 * m.Nfp + cnt[2]++] = n;
+    if (std::fabs(m.r[n] + 1) < tol) m.faceNodes[3 * m.Nfp + cnt[3]++] = n;
+  }
+}
+
+/* SetupBoxQuad2D at one rank, meshSetupBoxQuad2D.cpp:30-100, plus the seeded
+   interior-vertex perturbation of the 3D box: every global vertex draws two
+   uniforms in vertex-id order (x, y interleaved), interior vertices move by
+   pert*h*(2u-1) per coordinate. */
+static void setup_box_2d(bpo_mesh& m, double pert, uint64_t seed) {
+  const int nx = m.nx, ny = m.ny;
+  const hlong NnX = nx + 1, NnY = ny + 1;
+  const double dx = 2.0 / nx, dy = 2.0 / ny;
+  m.EToV.resize(m.E * 4); m.EX.resize(m.E * 4); m.EY.resize(m.E * 4); m.EZ.clear();
+  std::vector<double> u;
+  if (pert != 0.0) {
+    u.resize(2 * NnX * NnY);
+    bpo_random(seed, (int64_t)u.size(), u.data());
+  }
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const dlong e = i + j * nx;
+      const hlong i0 = i, i1 = (i + 1) % NnX, j0 = j, j1 = (j + 1) % NnY;
+      hlong* v = &m.EToV[e * 4];
+      v[0] = i0 + j0 * NnX; v[1] = i1 + j0 * NnX; v[2] = i1 + j1 * NnX; v[3] = i0 + j1 * NnX;
+      const double x0 = -1.0 + dx * i, y0 = -1.0 + dy * j;
+      double* ex = &m.EX[e * 4]; double* ey = &m.EY[e * 4];
+      ex[0] = x0;      ey[0] = y0;
+      ex[1] = x0 + dx; ey[1] = y0;
+      ex[2] = x0 + dx; ey[2] = y0 + dy;
+      ex[3] = x0;      ey[3] = y0 + dy;
+      if (pert != 0.0)
+        for (int c = 0; c < 4; ++c) {
+          const hlong g = v[c];
+          const hlong I = g % NnX, J = g / NnX;
+          if (I == 0 || I == nx || J == 0 || J == ny) continue;
+          ex[c] += pert * dx * (2 * u[2 * g + 0] - 1);
+          ey[c] += pert * dy * (2 * u[2 * g + 1] - 1);
+        }
+    }
+}
+
+/* Connect, meshConnect.cpp:48-140, with the two-vertex faces of Quad2D */
+static void connect_2d(bpo_mesh& m) {
+  struct F { hlong v[2]; dlong e; int f; dlong eN; int fN; };
+  std::vector<F> faces(m.E * 4);
+  for (dlong e = 0; e < m.E; ++e)
+    for (int f = 0; f < 4; ++f) {
+      F& fc = faces[e * 4 + f];
+      for (int n = 0; n < 2; ++n) fc.v[n] = m.EToV[e * 4 + kEdgeVertices[f][n]];
+      std::sort(fc.v, fc.v + 2);
+      fc.e = e; fc.f = f; fc.eN = -1; fc.fN = -1;
+    }
+  std::sort(faces.begin(), faces.end(), [](const F& a, const F& b) {
+    return std::lexicographical_compare(a.v, a.v + 2, b.v, b.v + 2);
+  });
+  for (size_t c = 0; c + 1 < faces.size(); ++c)
+    if (std::equal(faces[c].v, faces[c].v + 2, faces[c + 1].v)) {
+      faces[c].eN = faces[c + 1].e; faces[c].fN = faces[c + 1].f;
+      faces[c + 1].eN = faces[c].e; faces[c + 1].fN = faces[c].f;
+    }
+  m.EToE.assign(m.E * 4, -1);
+  m.EToF.assign(m.E * 4, -1);
+  for (auto& fc : faces) { m.EToE[fc.e * 4 + fc.f] = fc.eN; m.EToF[fc.e * 4 + fc.f] = fc.fN; }
+}
+
+/* FaceNodeMatchingQuad2D, meshBasisQuad2D.cpp:113-170: for (fM, fP, rot) the
+   node of face fP at the place of each node of fM when fP is laid on fM */
+static void face_node_matching_2d(const bpo_mesh& m, std::vector<int>& R) {
+  const int Nfp = m.Nfp;
+  static const double V[2] = {-1.0, 1.0};
+  R.assign(4 * 4 * 2 * Nfp, -1);
+  std::vector<double> x0(Nfp), x1(Nfp);
+  for (int fM = 0; fM < 4; ++fM) {
+    double EX0[4] = {0, 0, 0, 0};
+    for (int v = 0; v < 2; ++v) EX0[kEdgeVertices[fM][v]] = V[v];
+    for (int n = 0; n < Nfp; ++n) {
+      const int fn = m.faceNodes[fM * Nfp + n];
+      x0[n] = bilinear(EX0, m.r[fn], m.s[fn]);
+    }
+    for (int fP = 0; fP < 4; ++fP)
+      for (int rot = 0; rot < 2; ++rot) {
+        double EX1[4] = {0, 0, 0, 0};
+        for (int v = 0; v < 2; ++v) EX1[kEdgeVertices[fP][(v + rot) % 2]] = V[v];
+        for (int n = 0; n < Nfp; ++n) {
+          const int fn = m.faceNodes[fP * Nfp + n];
+          x1[n] = bilinear(EX1, m.r[fn], m.s[fn]);
+        }
+        for (int n = 0; n < Nfp; ++n)
+          for (int k = 0; k < Nfp; ++k)
+            if ((x0[n] - x1[k]) * (x0[n] - x1[k]) < 1.0e-5) {
+              R[fM * 4 * Nfp * 2 + fP * Nfp * 2 + rot * Nfp + n] = k;
+              break;
+            }
+      }
+  }
+}
+
+/* ConnectFaceNodes, meshConnectFaceNodes.cpp:31-98, Quad2D faces */
+static void connect_face_nodes_2d(bpo_mesh& m) {
+  std::vector<int> R;
+  face_node_matching_2d(m, R);
+  const int Nfp = m.Nfp, Np = m.Np;
+  m.vmapM.resize((size_t)m.E * 4 * Nfp);
+  m.vmapP.resize((size_t)m.E * 4 * Nfp);
+  for (dlong eM = 0; eM < m.E; ++eM)
+    for (int fM = 0; fM < 4; ++fM) {
+      const dlong eP = m.EToE[eM * 4 + fM];
+      const int fP = m.EToF[eM * 4 + fM];
+      for (int nM = 0; nM < Nfp; ++nM) {
+        const int idM = m.faceNodes[fM * Nfp + nM];
+        const size_t id = (size_t)eM * 4 * Nfp + fM * Nfp + nM;
+        m.vmapM[id] = idM + eM * Np;
+        if (eP < 0 || fP < 0) { m.vmapP[id] = idM + eM * Np; continue; }
+        const hlong vf0P = m.EToV[eP * 4 + kEdgeVertices[fP][0]];
+        int rot = 0;
+        for (; rot < 2; ++rot)
+          if (m.EToV[eM * 4 + kEdgeVertices[fM][rot]] == vf0P) break;
+        const int nP = R[fM * 4 * Nfp * 2 + fP * Nfp * 2 + rot * Nfp + nM];
+        m.vmapP[id] = m.faceNodes[fP * Nfp + nP] + eP * Np;
+      }
+    }
+}
+
+/* PhysicalNodesQuad2D, meshPhysicalNodesQuad2D.cpp */
+static void physical_nodes_2d(bpo_mesh& m) {
+  const size_t Ntot = (size_t)m.E * m.Np;
+  m.x.resize(Ntot); m.y.resize(Ntot); m.z.clear();
+  for (dlong e = 0; e < m.E; ++e)
+    for (int n = 0; n < m.Np; ++n) {
+      m.x[(size_t)e * m.Np + n] = bilinear(&m.EX[e * 4], m.r[n], m.s[n]);
+      m.y[(size_t)e * m.Np + n] = bilinear(&m.EY[e * 4], m.r[n], m.s[n]);
+    }
+}
+
+/* GeometricFactorsQuad2D, meshGeometricFactorsQuad2D.cpp:31-120: ggeo
+   G00, G01, G11 (3 per node, GLL weights folded in; affine: per element) */
+static int geometric_factors_2d(bpo_mesh& m) {
+  int bad = 0;
+  if (m.affine) {
+    m.wJ.resize(m.E); m.ggeo.resize((size_t)3 * m.E);
+    for (dlong e = 0; e < m.E; ++e) {
+      const double* ex = &m.EX[e * 4]; const double* ey = &m.EY[e * 4];
+      const double xr = 0.5 * (ex[1] - ex[0]), xs = 0.5 * (ex[3] - ex[0]);
+      const double yr = 0.5 * (ey[1] - ey[0]), ys = 0.5 * (ey[3] - ey[0]);
+      const double J = xr * ys - xs * yr;
+      if (J < 1e-8) bad = 1;
+      const double rx = ys / J, ry = -xs / J, sx = -yr / J, sy = xr / J;
+      m.wJ[e] = J;
+      m.ggeo[3 * e + 0] = J * (rx * rx + ry * ry);
+      m.ggeo[3 * e + 1] = J * (rx * sx + ry * sy);
+      m.ggeo[3 * e + 2] = J * (sx * sx + sy * sy);
+    }
+    return bad ? -1 : 0;
+  }
+  const int Nq = m.Nq, Np = m.Np;
+  m.wJ.resize((size_t)m.E * Np); m.ggeo.resize((size_t)3 * m.E * Np);
+  for (dlong e = 0; e < m.E; ++e)
+    for (int j = 0; j < Nq; ++j)
+      for (int i = 0; i < Nq; ++i) {
+        double xr = 0, xs = 0, yr = 0, ys = 0;
+        for (int mm = 0; mm < Nq; ++mm) {
+          const size_t idr = (size_t)e * Np + j * Nq + mm, ids = (size_t)e * Np + mm * Nq + i;
+          xr += m.D[i * Nq + mm] * m.x[idr];
+          xs += m.D[j * Nq + mm] * m.x[ids];
+          yr += m.D[i * Nq + mm] * m.y[idr];
+          ys += m.D[j * Nq + mm] * m.y[ids];
+        }
+        const double J = xr * ys - xs * yr;
+        if (J < 1e-8) bad = 1;
+        const double rx = ys / J, ry = -xs / J, sx = -yr / J, sy = xr / J;
+        const double JW = J * m.gllw[i] * m.gllw[j];
+        const size_t id = (size_t)e * Np + i + j * Nq;
+        m.wJ[id] = JW;
+        m.ggeo[3 * id + 0] = JW * (rx * rx + ry * ry);
+        m.ggeo[3 * id + 1] = JW * (rx * sx + ry * sy);
+        m.ggeo[3 * id + 2] = JW * (sx * sx + sy * sy);
+      }
+  return bad ? -1 : 0;
+}
+
+/* A Quad2D box of nx x ny elements (Nfields 1 or 2: BP5, BP6 with Nfields =
+   dim) with the reference's set-up sequence */
+extern "C" bpo_mesh* bpo_mesh_create2d(int nx, int ny, int N, int affine, int Nfields, double pert,
+                                       uint64_t pert_seed) {
+  if (nx < 1 || ny < 1 || N < 1 || N > 15 || (Nfields != 1 && Nfields != 2)) return nullptr;
+  bpo_mesh* m = new bpo_mesh();
+  m->dim = 2; m->Nfaces = 4; m->Nverts = 4; m->Nggeo = 3;
+  m->N = N; m->Nq = N + 1; m->Np = m->Nq * m->Nq; m->Nfp = m->Nq;
+  m->nx = nx; m->ny = ny; m->nz = 1; m->E = nx * ny; m->affine = affine; m->Nfields = Nfields;
+  m->gllz.resize(m->Nq); m->gllw.resize(m->Nq);
+  if (bpo_jacobi_gll(N, m->gllz.data(), m->gllw.data())) { delete m; return nullptr; }
+  m->D.resize(m->Nq * m->Nq);
+  bpo_dmatrix1d(N, m->gllz.data(), m->Nq, m->gllz.data(), m->D.data());
+  m->MM.resize(m->Nq * m->Nq);
+  bpo_mass_matrix1d(N, m->gllz.data(), m->MM.data());
+  reference_nodes_2d(*m);
+  setup_box_2d(*m, pert, pert_seed);
+  connect_2d(*m);
+  connect_face_nodes_2d(*m);
+  connect_nodes(*m);
+  physical_nodes_2d(*m);
+  if (geometric_factors_2d(*m)) { delete m; return nullptr; }
+  masked_ogs(*m);
+  m->elementList.resize(m->E);
+  std::iota(m->elementList.begin(), m->elementList.end(), 0);
+  return m;
+}
+
+/* bp5AxQuad2D / bp5AxAffineQuad2D (okl/bp5AxQuad2D.okl, okl/bp5AxAffineQuad2D.okl)
+   and the field loop of okl/bp6AxQuad2D.okl, in their arithmetic order */
+static void ax_bp5_e_2d(const bpo_mesh& m, dlong e, const dlong* G2L, double lambda, const double* q, double* AqL,
+                        int f) {
+  const int Nq = m.Nq, Np = m.Np, Nf = m.Nfields;
+  const double* D = m.D.data();
+  thread_local std::vector<double> sq, Gqr, Gqs;
+  sq.resize(Np); Gqr.resize(Np); Gqs.resize(Np);
+  const size_t lbase = (size_t)e * Np * Nf + (size_t)f * Np;
+  for (int n = 0; n < Np; ++n) {
+    const dlong id = G2L[lbase + n];
+    sq[n] = (id != -1) ? q[id] : 0.0;
+  }
+  for (int j = 0; j < Nq; ++j)
+    for (int i = 0; i < Nq; ++i) {
+      double G00, G01, G11;
+      if (m.affine) {
+        G00 = m.ggeo[3 * (size_t)e + 0]; G01 = m.ggeo[3 * (size_t)e + 1]; G11 = m.ggeo[3 * (size_t)e + 2];
+      } else {
+        const size_t gb = (size_t)e * Np + i + j * Nq;
+        G00 = m.ggeo[3 * gb + 0]; G01 = m.ggeo[3 * gb + 1]; G11 = m.ggeo[3 * gb + 2];
+      }
+      double tmp = 0;
+      for (int mm = 0; mm < Nq; ++mm) tmp += D[i * Nq + mm] * sq[j * Nq + mm];
+      double gr = G00 * tmp, gs = G01 * tmp;
+      tmp = 0;
+      for (int mm = 0; mm < Nq; ++mm) tmp += D[j * Nq + mm] * sq[mm * Nq + i];
+      gr += G01 * tmp;
+      gs += G11 * tmp;
+      if (m.affine) {
+        const double w = m.gllw[i] * m.gllw[j];
+        gr *= w;
+        gs *= w;
+      }
+      Gqr[j * Nq + i] = gr;
+      Gqs[j * Nq + i] = gs;
+    }
+  for (int j = 0; j < Nq; ++j)
+    for (int i = 0; i < Nq; ++i) {
+      double ap;
+      if (m.affine) ap = sq[j * Nq + i] * lambda * m.wJ[e] * (m.gllw[i] * m.gllw[j]);
+      else ap = sq[j * Nq + i] * lambda * m.wJ[(size_t)e * Np + i + j * Nq];
+      for (int mm = 0; mm < Nq; ++mm) {
+        ap += D[mm * Nq + i] * Gqr[j * Nq + mm];
+        ap += D[mm * Nq + j] * Gqs[mm * Nq + i];
+      }
+      AqL[lbase + i + j * Nq] = ap;
+    }
+}
+
 extern "C" void bpo_mesh_free(bpo_mesh* m) { delete m; }
 
 extern "C" int64_t bpo_mesh_int(const bpo_mesh* m, const char* name) {
   std::string s(name);
   if (s == "N") return m->N;
+  if (s == "dim") return m->dim;
   if (s == "Nq") return m->Nq;
   if (s == "Np") return m->Np;
   if (s == "E") return m->E;
@@ -921,7 +1214,8 @@ extern "C" void bpo_ax_bp5(const bpo_mesh* m, double lambda, const double* q, do
 #pragma omp parallel for schedule(static)
   for (dlong e = 0; e < m->E; ++e)
     for (int f = 0; f < m->Nfields; ++f) {
-      if (pencil) ax_bp5_e_pencil(*m, e, m->G2L.data(), lambda, q, AqL, f);
+      if (m->dim == 2) ax_bp5_e_2d(*m, e, m->G2L.data(), lambda, q, AqL, f);
+      else if (pencil) ax_bp5_e_pencil(*m, e, m->G2L.data(), lambda, q, AqL, f);
       else ax_bp5_e_3d(*m, e, m->G2L.data(), lambda, q, AqL, f);
     }
 }
@@ -955,6 +1249,24 @@ static const double kPi = 3.14159265358979323846;
 /* rhsHex3D / rhsAffineHex3D (okl/rhsHex3D.okl:29-128), element-local forcing */
 extern "C" void bpo_rhs_analytic(const bpo_mesh* m, double lambda, double* rL) {
   const int Nq = m->Nq, Np = m->Np, Nf = m->Nfields;
+  if (m->dim == 2) {   // rhsQuad2D / rhsAffineQuad2D, okl/rhsQuad2D.okl
+    for (dlong e = 0; e < m->E; ++e)
+      for (int j = 0; j < Nq; ++j)
+        for (int i = 0; i < Nq; ++i) {
+          const int n = i + j * Nq;
+          const size_t id = (size_t)e * Np + n;
+          const double x = m->x[id], y = m->y[id];
+          const double wJ = m->affine ? m->wJ[e] * m->gllw[i] * m->gllw[j] : m->wJ[id];
+          if (Nf == 1) {
+            rL[id] = wJ * ((2 * kPi * kPi + lambda) * std::sin(kPi * x) * std::sin(kPi * y));
+          } else {
+            const size_t base = (size_t)e * Np * Nf + n;
+            rL[base + 0 * Np] = wJ * ((3 * kPi * kPi + lambda) * std::sin(2.0 * kPi * x) * std::sin(kPi * y));
+            rL[base + 1 * Np] = wJ * ((3 * kPi * kPi + lambda) * std::sin(kPi * x) * std::sin(2.0 * kPi * y));
+          }
+        }
+    return;
+  }
 #pragma omp parallel for
   for (dlong e = 0; e < m->E; ++e)
     for (int k = 0; k < Nq; ++k)
@@ -990,7 +1302,8 @@ extern "C" void bpo_rhs_random(const bpo_mesh* m, uint64_t seed, double* f, doub
     for (int fl = 0; fl < Nf; ++fl)
       for (int n = 0; n < Np; ++n) {
         const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
-        const double wJ = m->affine ? m->wJ[e] * m->gllw[i] * m->gllw[j] * m->gllw[k] : m->wJ[(size_t)e * Np + n];
+        const double w = m->dim == 2 ? m->gllw[i] * m->gllw[j] : m->gllw[i] * m->gllw[j] * m->gllw[k];
+        const double wJ = m->affine ? m->wJ[e] * w : m->wJ[(size_t)e * Np + n];
         const size_t l = (size_t)e * Np * Nf + (size_t)fl * Np + n;
         const dlong id = m->G2L[l];
         rL[l] = (id != -1) ? wJ * f[id] : 0.0;
@@ -1005,6 +1318,28 @@ extern "C" void bpo_jacobi_diag_bp5(const bpo_mesh* m, double lambda, double* di
   const int Nq = m->Nq, Np = m->Np, Nf = m->Nfields;
   const double* D = m->D.data();
   std::vector<double> dL((size_t)m->E * Np * Nf);
+  if (m->dim == 2) {
+    for (dlong e = 0; e < m->E; ++e)
+      for (int j = 0; j < Nq; ++j)
+        for (int i = 0; i < Nq; ++i) {
+          auto G = [&](int ii, int jj, int c) -> double {
+            if (m->affine) return m->ggeo[3 * (size_t)e + c] * m->gllw[ii] * m->gllw[jj];
+            return m->ggeo[3 * ((size_t)e * Np + ii + jj * Nq) + c];
+          };
+          const int n = i + j * Nq;
+          double d = 0.0;
+          for (int mm = 0; mm < Nq; ++mm) {
+            d += G(mm, j, 0) * D[mm * Nq + i] * D[mm * Nq + i];
+            d += G(i, mm, 2) * D[mm * Nq + j] * D[mm * Nq + j];
+          }
+          d += 2 * G(i, j, 1) * D[i * Nq + i] * D[j * Nq + j];
+          const double wJ = m->affine ? m->wJ[e] * m->gllw[i] * m->gllw[j] : m->wJ[(size_t)e * Np + n];
+          d += lambda * wJ;
+          for (int f = 0; f < Nf; ++f) dL[(size_t)e * Np * Nf + (size_t)f * Np + n] = d;
+        }
+    bpo_gather(m, dL.data(), diag);
+    return;
+  }
 #pragma omp parallel for
   for (dlong e = 0; e < m->E; ++e)
     for (int k = 0; k < Nq; ++k)

@@ -4,13 +4,15 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
 bench.py's CPU-baseline leg as the checker.  The product package never imports
 this module.
 
-The oracle restates the reference's Hex3D BK/BP hot path on the CPU (see the
-header of bp_oracle.cpp for the reference file:line of every routine).
+The oracle restates the reference's Hex3D (and Quad2D BP5/BP6) BK/BP hot path
+on the CPU (see the header of bp_oracle.cpp for the reference file:line of
+every routine).
 
-Parity unpinned against the reference's own outputs: the reference has no
-golden vectors or tests for this path and cannot be built here, so the oracle is
-pinned by known answers of the mathematics (tests/test_oracle.py,
-tests/test_cub_host.py).
+Parity pin: the reference's own host set-up code, compiled here against
+host-only shims (oracle/Makefile, target ref), produced the fixtures of
+tests/golden/, which tests/test_ref_golden.py holds this restatement to; the
+element kernels (OKL, which need OCCA) are pinned by known answers of the
+mathematics (tests/test_oracle.py, tests/test_cub_host.py).
 """
 import ctypes
 import os
@@ -44,6 +46,8 @@ def lib():
         L.bpo_mass_matrix1d.argtypes = [ctypes.c_int, _c_dp, _c_dp]
         L.bpo_mesh_create.restype = ctypes.c_void_p
         L.bpo_mesh_create.argtypes = [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_uint64]
+        L.bpo_mesh_create2d.restype = ctypes.c_void_p
+        L.bpo_mesh_create2d.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.c_uint64]
         L.bpo_mesh_free.argtypes = [ctypes.c_void_p]
         L.bpo_mesh_int.restype = ctypes.c_int64
         L.bpo_mesh_int.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
@@ -125,17 +129,22 @@ _DTYPES = {
 
 
 class Mesh:
-    """Box Hex3D mesh with masked ogs numbering, built by the oracle.
+    """Box mesh with masked ogs numbering, built by the oracle.
 
     nx, ny, nz: elements per direction; N: degree; affine: store per-element
-    factors; Nfields: 1 (BP5) or 3 (BP6); pert/pert_seed: seeded perturbation
-    of interior vertices by pert*h*(2u-1)."""
+    factors; Nfields: 1 (BP5) or 3 (BP6; 2 in 2D); pert/pert_seed: seeded
+    perturbation of interior vertices by pert*h*(2u-1).  dim=2 builds the
+    Quad2D box of nx x ny elements (nz is ignored; BP5/BP6 only)."""
 
-    def __init__(self, nx, ny, nz, N, affine=False, Nfields=1, pert=0.0, pert_seed=1):
-        self._h = lib().bpo_mesh_create(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), pert_seed)
+    def __init__(self, nx, ny, nz, N, affine=False, Nfields=1, pert=0.0, pert_seed=1, dim=3):
+        if dim == 2:
+            self._h = lib().bpo_mesh_create2d(nx, ny, N, int(bool(affine)), Nfields, float(pert), pert_seed)
+        else:
+            self._h = lib().bpo_mesh_create(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), pert_seed)
         if not self._h:
             raise RuntimeError("oracle mesh setup failed (bad sizes or non-positive Jacobian)")
-        self.nx, self.ny, self.nz, self.N = nx, ny, nz, N
+        self.dim = dim
+        self.nx, self.ny, self.nz, self.N = nx, ny, (nz if dim == 3 else 1), N
         self.affine = bool(affine)
         self.Nfields = Nfields
         for k in ("Nq", "Np", "E", "Ngather", "nnz"):
@@ -172,6 +181,8 @@ class Mesh:
         (the field count comes from the mesh)."""
         q = np.ascontiguousarray(q, dtype=np.float64)
         out = np.empty(self.NL)
+        if self.dim == 2 and bp < 5:
+            raise ValueError("the oracle's Quad2D forms are BP5/BP6")
         if bp >= 5:
             lib().bpo_ax_bp5(self._h, lam, _dp(q), _dp(out))
         else:
@@ -191,6 +202,8 @@ class Mesh:
         return out
 
     def operator(self, q, lam=1.0, bp=5):
+        if self.dim == 2 and bp < 5:
+            raise ValueError("the oracle's Quad2D forms are BP5/BP6")
         q = np.ascontiguousarray(q, dtype=np.float64)
         out = np.empty(self.Ngather)
         lib().bpo_operator(self._h, bp, lam, _dp(q), _dp(out))

@@ -33,6 +33,12 @@ CASES = {
     "hex_2x2x2_p1": (1, 1, "-nx 2 -ny 2 -nz 2 -p 1", False),
     # the BP5 p=4 box of 16^3 affine elements (250,047 unknowns): numbering and CSR at full size
     "hex_16x16x16_p4_affine": (1, 0, "-nx 16 -ny 16 -nz 16 -p 4 -a", True),
+    # Quad2D boxes (-e Quad; BP6 has Nfields = dim = 2 there)
+    "quad_3x2_p4": (1, 4, "-e Quad -nx 3 -ny 2 -p 4", False),
+    "quad_4x3_p7_affine": (1, 7, "-e Quad -nx 4 -ny 3 -p 7 -a", False),
+    "quad_3x3_p5_nf2": (2, 5, "-e Quad -nx 3 -ny 3 -p 5", False),
+    "quad_2x2_p15": (1, 15, "-e Quad -nx 2 -ny 2 -p 15", False),
+    "quad_64x48_p6": (1, 0, "-e Quad -nx 64 -ny 48 -p 6", True),
 }
 INT_RECORDS = {"N", "Nq", "Np", "Nelements", "Nfields", "Ngather", "NgatherGlobal", "cubNq", "GlobalToLocal",
                "rowStartsT", "colIdsT", "rowStartsN", "colIdsN", "gllz", "gllw", "D"}

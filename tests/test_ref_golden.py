@@ -35,10 +35,13 @@ def FP_TOL(N):
 
 
 def case(path):
+    """(fixture, nx, ny, nz, N, affine, Nfields, dim); Quad2D cases (-e Quad) have dim 2 and nz 1."""
     g = np.load(path)
     cli = str(g["cli"]).split()
     opts = {cli[i]: int(cli[i + 1]) for i in range(len(cli) - 1) if cli[i] in ("-nx", "-ny", "-nz", "-p")}
-    return g, opts["-nx"], opts["-ny"], opts["-nz"], opts["-p"], "-a" in cli, int(g["Nfields"][0])
+    dim = 2 if "Quad" in cli else 3
+    nz = opts["-nz"] if dim == 3 else 1
+    return g, opts["-nx"], opts["-ny"], nz, opts["-p"], "-a" in cli, int(g["Nfields"][0]), dim
 
 
 def rel(a, b):
@@ -57,18 +60,22 @@ def ids(paths):
 
 def test_fixtures_present():
     assert len(SMALL) >= 6 and len(FULL) >= 1
+    assert sum("quad" in f for f in SMALL) >= 4 and sum("quad" in f for f in FULL) >= 1
 
 
 @pytest.mark.parametrize("path", SMALL, ids=ids(SMALL))
 def test_oracle_matches_reference_code(oracle, path):
-    g, nx, ny, nz, N, affine, nf = case(path)
-    m = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=nf)
+    g, nx, ny, nz, N, affine, nf, dim = case(path)
+    m = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=nf, dim=dim)
     assert (m.E, m.Np, m.Ngather) == (int(g["Nelements"][0]), int(g["Np"][0]), int(g["Ngather"][0]))
     for ours, theirs in (("G2L", "GlobalToLocal"), ("rowStarts", "rowStartsT"), ("colIds", "colIdsT"),
                          ("globalIds", "globalIds"), ("EToV", "EToV"), ("EX", "EX"), ("EY", "EY"), ("EZ", "EZ")):
         np.testing.assert_array_equal(m.array(ours), g[theirs], err_msg=theirs)
-    names = ["gllz", "gllw", "D", "MM", "x", "y", "z", "wJ", "ggeo", "cubr", "cubw", "cubInterp", "cubD"]
-    names += ["invV"] if affine else ["cubwJ", "cubggeo"]
+    if dim == 2:   # the Quad2D restatement covers the BP5/BP6 data (no over-integration)
+        names = ["gllz", "gllw", "D", "MM", "x", "y", "wJ", "ggeo"]
+    else:
+        names = ["gllz", "gllw", "D", "MM", "x", "y", "z", "wJ", "ggeo", "cubr", "cubw", "cubInterp", "cubD"]
+        names += ["invV"] if affine else ["cubwJ", "cubggeo"]
     for k in names:
         assert rel(m.array(k), g[k]) <= FP_TOL(N), k
     np.testing.assert_array_equal(m.gather(g["gather_in"]), g["gather_out"])
@@ -77,17 +84,19 @@ def test_oracle_matches_reference_code(oracle, path):
 
 @pytest.mark.parametrize("path", SMALL, ids=ids(SMALL))
 def test_library_host_setup_matches_reference_code(bp, path):
-    g, nx, ny, nz, N, affine, nf = case(path)
-    g2l, rs, ci = bp.box_numbering(nx, ny, nz, N, nf)
+    g, nx, ny, nz, N, affine, nf, dim = case(path)
+    g2l, rs, ci = bp.box_numbering(nx, ny, nz, N, nf, dim=dim)
     np.testing.assert_array_equal(g2l, g["GlobalToLocal"])
     np.testing.assert_array_equal(rs, g["rowStartsT"])
     np.testing.assert_array_equal(ci, g["colIdsT"])
-    ex, ey, ez = bp.box_vertices(nx, ny, nz)
+    ex, ey, ez = bp.box_vertices(nx, ny, nz, dim=dim)
     for a, k in ((ex, "EX"), (ey, "EY"), (ez, "EZ")):
         np.testing.assert_array_equal(a, g[k], err_msg=k)
     z, w, D = bp.basis_gll(N)
     assert rel(z, g["gllz"]) <= FP_TOL(N) and rel(w, g["gllw"]) <= FP_TOL(N)
     assert rel(D.ravel(), g["D"]) <= FP_TOL(N)
+    if dim == 2:
+        return
     c = bp.basis_cubature(N)
     assert rel(c["r"], g["cubr"]) <= FP_TOL(N) and rel(c["w"], g["cubw"]) <= FP_TOL(N)
     assert rel(c["I"].ravel(), g["cubInterp"]) <= FP_TOL(N)
@@ -101,11 +110,11 @@ def test_library_host_setup_matches_reference_code(bp, path):
 
 @pytest.mark.parametrize("path", FULL, ids=ids(FULL))
 def test_full_size_numbering_matches_reference_code(bp, oracle, path):
-    """The BP5 p=4 box of 16^3 affine elements (250,047 unknowns): the numbering and CSR of the library's
-    host form and of the oracle hash to the reference's own arrays."""
-    g, nx, ny, nz, N, affine, nf = case(path)
-    g2l, rs, ci = bp.box_numbering(nx, ny, nz, N, nf)
-    m = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=nf)
+    """The BP5 p=4 box of 16^3 affine elements (250,047 unknowns) and a Quad2D box of 64 x 48 p=6 elements:
+    the numbering and CSR of the library's host form and of the oracle hash to the reference's own arrays."""
+    g, nx, ny, nz, N, affine, nf, dim = case(path)
+    g2l, rs, ci = bp.box_numbering(nx, ny, nz, N, nf, dim=dim)
+    m = oracle.Mesh(nx, ny, nz, N, affine=affine, Nfields=nf, dim=dim)
     for arrays in ((g2l, rs, ci), (m.array("G2L"), m.array("rowStarts"), m.array("colIds"))):
         for a, k in zip(arrays, ("GlobalToLocal", "rowStartsT", "colIdsT")):
             assert a.size == int(g["size_" + k]), k
