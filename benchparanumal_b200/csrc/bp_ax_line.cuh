@@ -84,13 +84,17 @@ struct LineMinBlocks {
 // T: the value type of q and Aq, LineReal or Pack<LineReal, PK> (PK right-hand
 // sides of one mesh in lockstep, one pack per node); p.Ap partials per lane at
 // partials[lane * gridDim.x + blockIdx.x].
+//
+// The body works on element block `blk` of `nblk` (partials[lane * nblk +
+// blk]) in the dynamic shared memory smem_raw: the kernel below and the
+// persistent CG step share it.
 template <int NQ, bool AFFINE, class T>
-__global__ void __launch_bounds__(LineShape<NQ, T>::THREADS, (LineMinBlocks<NQ, T>::V))
-ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
-               const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
-               const LineReal* __restrict__ gllw, LineReal lambda, const T* __restrict__ q,
-               T* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
-  if (skip && *skip) return;
+__device__ __forceinline__ void ax_line_body(int blk, int nblk, int Nelements, int Nfields,
+                                             const int32_t* __restrict__ elementList,
+                                             const int32_t* __restrict__ G2L, const LineReal* __restrict__ wJ,
+                                             const LineReal* __restrict__ ggeo, const LineReal* __restrict__ gllw,
+                                             LineReal lambda, const T* __restrict__ q, T* __restrict__ Aq,
+                                             double* __restrict__ partials, unsigned char* smem_raw) {
   using F = LineReal;
   using Sh = LineShape<NQ, T>;
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
@@ -101,7 +105,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
 #define W_(a) c_line[SLOT + NQ * NQ + (a)]
 #define AT(B, z, y, x) B[(z) * PLANE + (y) * RS + (x)]
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __syncthreads();   // a previous call's last uses of this shared memory are done (persistent use)
   T* const sbase = reinterpret_cast<T*>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
   const int tid = tx + NQ * (ty + NQ * es);
@@ -109,7 +113,7 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
   T* const R = U + Sh::FIELD;
   T* const S = R + Sh::FIELD;
 
-  const int eidx = blockIdx.x * EPB + es;
+  const int eidx = blk * EPB + es;
   const bool valid = eidx < Nelements;
   const int element = valid ? elementList[eidx] : 0;
   double pdot[LANES];
@@ -253,11 +257,23 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
     }
     if (tid == 0)
 #pragma unroll
-      for (int l = 0; l < LANES; ++l) partials[(size_t)l * gridDim.x + blockIdx.x] = bs[l];
+      for (int l = 0; l < LANES; ++l) partials[(size_t)l * nblk + blk] = bs[l];
   }
 #undef AT
 #undef W_
 #undef D_
+}
+
+template <int NQ, bool AFFINE, class T>
+__global__ void __launch_bounds__(LineShape<NQ, T>::THREADS, (LineMinBlocks<NQ, T>::V))
+ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+               const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
+               const LineReal* __restrict__ gllw, LineReal lambda, const T* __restrict__ q,
+               T* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ax_line_body<NQ, AFFINE, T>(blockIdx.x, gridDim.x, Nelements, Nfields, elementList, G2L, wJ, ggeo, gllw, lambda, q,
+                              Aq, partials, smem_raw);
 }
 
 // device address of the constant table on the current device

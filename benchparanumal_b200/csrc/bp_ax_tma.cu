@@ -22,6 +22,7 @@
 #include <cstdint>
 
 #include "bp_cg_device.cuh"
+#include "bp_cg_persist.cuh"
 #include "bp_internal.hpp"
 #include "bp_pack.cuh"
 
@@ -186,12 +187,17 @@ struct TmaMinBlocks {
 // DIR builds the form with the CG direction update fused in (CgFuse::dir): q
 // is not read, the pencil is p_k formed from p_{k-1}, r and invD, and the
 // owners of the element's nodes write p_k and the deferred x update.
+//
+// The body works on element block `blk` of `nblk` (the block sums of p.Ap go
+// to partials[lane * nblk + blk]) in the dynamic shared memory smem_raw, so the
+// same code serves the kernel below (blk = blockIdx.x) and the persistent CG
+// step (bp_solver.cu), whose blocks walk over the element blocks.
 template <int NQ, int NF, bool DOT, int R, class F, class T, int WITHHOLD = -1, bool DIR = false>
-__global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF, (TmaMinBlocks<NQ, NF, F, T>::V))
-ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
-              const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
-              const T* __restrict__ q, T* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
-  if (skip && *skip) return;
+__device__ __forceinline__ void ax_tma_body(int blk, int nblk, int Nelements, const int32_t* __restrict__ elementList,
+                                            const int32_t* __restrict__ G2L, const F* __restrict__ wJ,
+                                            const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
+                                            const T* __restrict__ q, T* __restrict__ Aq, const CgFuse& fuse,
+                                            unsigned char* smem_raw) {
   DirStep<PackTraits<T>::R, F> ds;
   if (DIR) {
     ds.load(fuse);
@@ -202,7 +208,6 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
   using V2 = typename Vec2<F>::type;
   constexpr int NQ2 = Sh::NQ2, NP = NQ2 * NQ, EPB = Sh::EPB, S = EPB * NF, LANES = PackTraits<T>::R;
   constexpr int PAD = Lay::PAD;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   F* s_g = reinterpret_cast<F*>(smem_raw);
   F* s_J = s_g + EPB * R * Sh::SLICE_G;
   F* s_D = s_J + EPB * R * NQ2;                     // [NQ][NQ] row-major, rows 8-byte aligned
@@ -214,14 +219,16 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
   const int i = threadIdx.x, j = threadIdx.y, slot = threadIdx.z;
   const int t = i + NQ * (j + NQ * slot);
   const int el = slot / NF, f = slot % NF;
-  const int e0 = blockIdx.x * EPB;
+  const int e0 = blk * EPB;
   const int nact = min(EPB, Nelements - e0);
   const bool active = el < nact;
   const int e = active ? elementList[e0 + el] : 0;
 
+  __syncthreads();   // a previous call's last uses of this shared memory are done (persistent use)
   if (t == 0) {
     for (int r = 0; r < R; ++r) mbar_init(&s_bar[r], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic accesses before the bulk copies
   }
   __syncthreads();
   constexpr long long LIMIT = WITHHOLD >= 0 ? kTestWaitCycles : kWaitCycles;
@@ -398,8 +405,19 @@ ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int3
     }
     if (t == 0)
 #pragma unroll
-      for (int l = 0; l < LANES; ++l) fuse.partials[(size_t)l * gridDim.x + blockIdx.x] = bs[l];
+      for (int l = 0; l < LANES; ++l) fuse.partials[(size_t)l * nblk + blk] = bs[l];
   }
+}
+
+template <int NQ, int NF, bool DOT, int R, class F, class T, int WITHHOLD = -1, bool DIR = false>
+__global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF, (TmaMinBlocks<NQ, NF, F, T>::V))
+ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+              const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
+              const T* __restrict__ q, T* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
+  if (skip && *skip) return;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  ax_tma_body<NQ, NF, DOT, R, F, T, WITHHOLD, DIR>(blockIdx.x, gridDim.x, Nelements, elementList, G2L, wJ, ggeo, Dg,
+                                                   lambda, q, Aq, fuse, smem_raw);
 }
 
 template <int NQ, int NF, bool DOT, class F, class T, bool DIR = false>
@@ -825,6 +843,49 @@ bool tma_covers(const bp_ax_desc_t& d, int lanes) {
   if (d.dim == 2 || d.affine || NQ % 2 != 0) return false;
   if (lanes > 1) return d.Nfields == 1 && (lanes == 2 || lanes == 4) && NQ >= 8 && NQ <= 12;
   return d.Nfields == 1 ? NQ <= 16 : (d.Nfields == 3 && NQ <= 10);
+}
+
+namespace {
+// the TMA body as the operator phase of the persistent CG step
+template <int NQ, class T>
+struct TmaStepOp {
+  static constexpr int THREADS = NQ * NQ * TmaShape<NQ, float>::EPB;
+  static constexpr int MINB = TmaMinBlocks<NQ, 1, float, T>::V;
+  static __device__ __forceinline__ void run(int blk, const GrpStepArgs& a, unsigned char* smem) {
+    CgFuse f;
+    f.partials = a.parts;
+    ax_tma_body<NQ, 1, true, TmaShape<NQ, float>::R, float, T>(blk, a.nblk_op, a.Nelements, a.elementList, a.G2L,
+                                                                a.wJ, a.ggeo, a.D, a.lambda,
+                                                                reinterpret_cast<const T*>(a.p),
+                                                                reinterpret_cast<T*>(a.AqL), f, smem);
+  }
+};
+
+template <int NQ, int PK>
+int launch_step_tma_nq(GrpStepArgs a, int grid_cap, cudaStream_t s) {
+  using T = Pack<float, PK>;
+  using Sh = TmaShape<NQ, float>;
+  float* tab = tma_d_table<float>();
+  if (!tab) return fail(BP_ERROR_CUDA, "persistent CG step: constant table address lookup failed");
+  BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), a.D, sizeof(float) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  a.nblk_op = (a.Nelements + Sh::EPB - 1) / Sh::EPB;
+  return launch_grp_step_kernel<PK, TmaStepOp<NQ, T>>(a, dim3(NQ, NQ, Sh::EPB), TmaSmem<NQ, 1, Sh::R, float, T>::BYTES,
+                                                       grid_cap, s);
+}
+}  // namespace
+
+// One CG step of a packed group as one cooperative kernel with the TMA form of
+// the operator (bp_cg_persist.cuh); pk = 4, stored factors, Nq 8, 10, 12
+int launch_grp_step_tma(int pk, const bp_ax_desc_t& d, const GrpStepArgs& a, int grid_cap, cudaStream_t s) {
+  if (pk != 4 || !tma_covers(d, pk) ||
+      ((reinterpret_cast<uintptr_t>(a.ggeo) | reinterpret_cast<uintptr_t>(a.wJ)) & 15))
+    return 1;
+  switch (d.N + 1) {
+    case 8: return launch_step_tma_nq<8, 4>(a, grid_cap, s);
+    case 10: return launch_step_tma_nq<10, 4>(a, grid_cap, s);
+    case 12: return launch_step_tma_nq<12, 4>(a, grid_cap, s);
+    default: return 1;
+  }
 }
 
 int launch_ax_tma_packed(int pk, const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList,

@@ -8,6 +8,10 @@
 
 namespace bp {
 
+// A mixed-precision lane asks for a reliable update once its FP32 residual
+// has dropped by this factor since the last replacement.
+constexpr double kReliableDrop = 1e-2;
+
 struct CgScalars {
   double rdotr;       // r.r after the last update (plain CG: the reference's rdotr)
   double rdotr_prev;  // r.r one update earlier

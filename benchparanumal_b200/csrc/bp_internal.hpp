@@ -369,6 +369,12 @@ int ax_current_form(const bp_ax_desc_t& d, int bytes, int lanes, int32_t Nelemen
 // G2Lo = G2L (NL entries) with kOwnerBit on the first column of every CSR row
 int launch_owner_map(size_t NL, const int32_t* G2L, int32_t Ngather, const int32_t* rowStarts, const int32_t* colIds,
                      int32_t* G2Lo, cudaStream_t s);
+// One CG step of a packed group (4 lanes) as one cooperative kernel
+// (bp_cg_persist.cuh), with the TMA or the line form of the operator; 1 when
+// the form does not cover d.  grid_cap limits the resident blocks.
+struct GrpStepArgs;
+int launch_grp_step_tma(int pk, const bp_ax_desc_t& d, const GrpStepArgs& a, int grid_cap, cudaStream_t s);
+int launch_grp_step_line(int pk, const bp_ax_desc_t& d, const GrpStepArgs& a, int grid_cap, cudaStream_t s);
 // the device error word set by kernels whose bounded waits gave up
 int* device_error_word();
 int check_device_error();

@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "bp_cg_device.cuh"
+#include "bp_cg_persist.cuh"
 #include "bp_internal.hpp"
 #include "bp_pack.cuh"
 
@@ -47,7 +48,6 @@ constexpr int kChunk = 20;            // iterations per captured graph (divides 
 // update idles until its chunk ends while the group's other lanes go on, so
 // shorter chunks waste fewer iterations (and cost more host round trips).
 constexpr int kBatchChunk = 10;
-constexpr double kReliableDrop = 1e-2;
 
 __device__ __forceinline__ double warp_sum_cg(double v) {
 #pragma unroll
@@ -1181,6 +1181,11 @@ struct CgGroup {
   DeviceArray<float> x32, r32, p32, AqL32;      // packed [N][pk], AqL [NL][pk]
   DeviceArray<float> p32b;                      // second direction buffer of the fused direction update
   bool dir = false;                             // the captured iterations fuse the direction update
+  // one cooperative kernel per CG step (bp_cg_persist.cuh) instead of four
+  bool persist = false;
+  int persist_cap = 0;                          // resident blocks at most
+  DeviceArray<double> step_red;                 // its block sums [3 pk + 1][persist_cap]
+  DeviceArray<unsigned int> step_bar;           // its grid barrier [2]
   DeviceArray<double> parts;                    // operator p.Ap partials [pk][blocks]
   DeviceArray<double> gparts;                   // gather-update grid sums [2 pk][reduction blocks]
   DeviceArray<unsigned int> gcount;             // their arrival counter (zero between launches)
@@ -1289,8 +1294,58 @@ static int grp_iteration(CgGroup* G, cudaStream_t s) {
   return BP_SUCCESS;
 }
 
+// one CG step of the group as one cooperative kernel (bp_cg_persist.cuh)
+static int grp_step(CgGroup* G, cudaStream_t s) {
+  bp_solver_s* S = G->base;
+  bp_mesh_s* m = S->mesh;
+  const ElemOperands<float> o = operands32(S);
+  GrpStepArgs a{};
+  a.N = S->N;
+  a.Nelements = m->E;
+  a.lambda = (float)S->lambda;
+  a.precon = S->precon;
+  a.elementList = m->elementList.ptr;
+  a.G2L = m->G2L.ptr;
+  a.rowStarts = m->rowStarts.ptr;
+  a.colIds = m->colIds.ptr;
+  a.wJ = o.wJ;
+  a.ggeo = o.ggeo;
+  a.gllw = o.gllw;
+  a.D = o.D;
+  a.invD = S->precon ? S->invD32.ptr : nullptr;
+  a.x = G->x32.ptr;
+  a.p = G->p32.ptr;
+  a.r = G->r32.ptr;
+  a.AqL = G->AqL32.ptr;
+  a.sc = G->sc;
+  a.parts = G->parts.ptr;
+  a.red = G->step_red.ptr;
+  a.bar = G->step_bar.ptr;
+  a.err = device_error_word();
+  if (!a.err) return fail(BP_ERROR_CUDA, "persistent CG step: device error word lookup failed");
+  int rc = launch_grp_step_tma(G->pk, S->ax, a, G->persist_cap, s);
+  if (rc == 1) rc = launch_grp_step_line(G->pk, S->ax, a, G->persist_cap, s);
+  return rc == 1 ? fail(BP_ERROR_ARG, "persistent CG step: no form covers this group") : rc;
+}
+
 static int grp_body(CgGroup* G, cudaStream_t s) {
+  if (G->persist) return grp_step(G, s);
   return G->pk == 4 ? grp_iteration<4>(G, s) : grp_iteration<2>(G, s);
+}
+
+// Whether a group's CG steps run as one cooperative kernel: where a form
+// covers it and BP_PERSIST=1.  Measured, it does not pay: the 16^3 p=4 box
+// with four right-hand sides takes 18.4 ms to 1e-8 against 18.3 ms for the
+// graph of four kernels per step (the step is bound by the latency of its
+// phases, the operator's above all, not by launches: 420 kernels instead of
+// 1412 changed nothing), and the 64-problem batch 9.7 s against 5.5 s with it
+// forced on everywhere (a cooperative grid holds the whole GPU, so the units
+// on the other streams of the pool no longer overlap with it).
+static bool want_persist(const CgGroup* G) {
+  const bp_mesh_s* m = G->base->mesh;
+  if (G->pk != 4 || m->dim == 2 || m->Nfields != 1 || m->N + 1 > 12) return false;
+  const char* e = getenv("BP_PERSIST");
+  return e && e[0] == '1';
 }
 
 // FP64 residual of lane l and the restart of its FP32 recursion (init: start of a solve)
@@ -1373,6 +1428,13 @@ static int unit_capture(bp_batch_s* B, BatchUnit& u, cudaStream_t s) {
                             (float)S->lambda, G->p32.ptr, G->AqL32.ptr, nullptr, &fuse, s, &nparts));
     BP_TRY(want_dir(m, S->ax, 4, G->pk, &G->dir, s));
     if (G->dir) BP_TRY(alloc_zero(G->p32b, G->p32.n, s));
+    G->persist = !G->dir && want_persist(G);
+    if (G->persist) {
+      G->persist_cap = 32 * sm_count();
+      BP_TRY(G->step_red.alloc((size_t)(3 * G->pk + 1) * G->persist_cap));
+      BP_TRY(alloc_zero(G->step_bar, 2, s));
+      BP_CUDA_TRY(cudaStreamSynchronize(s));
+    }
   } else {
     bp_solver_s* S = B->sys_solver[u.sys];
     if (B->mixed) BP_TRY(prepare32(S, s));
@@ -1506,7 +1568,7 @@ static int batch_solve(bp_batch_s* B, double tol, int maxit, bp_solve_stats_t* s
         BP_CUDA_TRY(cudaGraphLaunch(u.graph, st));
         bp_solver_s* us = u.G ? u.G->base : B->sys_solver[u.sys];
         const bool ud = u.G ? u.G->dir : (B->mixed ? us->dir32 : us->dir64);
-        us->launches += (ud ? 3 : 4) * kBatchChunk;
+        us->launches += ((u.G && u.G->persist) ? 1 : ud ? 3 : 4) * kBatchChunk;
         BP_TRY(unit_post(B, u, st));
         ++a;
         continue;
