@@ -77,15 +77,19 @@ def test_cub_cg_history_matches_oracle(gpu, oracle, bpn, nx, ny, nz, N, affine, 
     st, hr, ha = S.solve(x, S.rhs("RANDOM", 0), tol=0.0, maxit=maxit)
     assert st.iterations == it_o == maxit
     # How far this problem's history is reproducible at all: the oracle run
-    # again on b perturbed by 1e-15 relative (a rounding-sized change).  The
-    # mass matrices cluster their spectrum and amplify such a change fast
-    # (measured: 1.7e-10 by iteration 11 of BP1 with Jacobi at r/r0 = 4e-5,
-    # the oracle's own affine and curved operators 1e-15 apart give the
-    # same).  The 1e-10 bar holds up to the first iteration where the oracle
+    # again on b perturbed by 1e-15 relative (a rounding-sized change), four
+    # draws, the worst of them.  The mass matrices cluster their spectrum and
+    # amplify such a change fast (measured on BP1 5^3 p=4 with Jacobi: the
+    # four draws differ from the unperturbed run by 3e-12 to 2e-10 at
+    # iteration 12, r/r0 = 1.5e-5, and one draw alone can miss that; the
+    # oracle's own affine and curved operators 1e-15 apart give the same).
+    # The 1e-10 bar holds up to the first iteration where the oracle
     # disagrees with itself by more than 1e-11.
-    noise = 1.0 + 1e-15 * (2 * oracle.random(99, om.Ngather) - 1)
-    _, _, _, hr_p, _ = om.cg(b_o * noise, 1.0, 0.0, maxit, precon=(precon == "JACOBI"), bp=bpn)
-    self_rel = np.abs(hr_p - hr_o) / hr_o
+    self_rel = np.zeros(maxit)
+    for seed in (99, 98, 97, 96):
+        noise = 1.0 + 1e-15 * (2 * oracle.random(seed, om.Ngather) - 1)
+        _, _, _, hr_p, _ = om.cg(b_o * noise, 1.0, 0.0, maxit, precon=(precon == "JACOBI"), bp=bpn)
+        self_rel = np.maximum(self_rel, np.abs(hr_p - hr_o) / hr_o)
     bad = np.flatnonzero(self_rel > HIST_TOL / 10)
     reproducible = np.arange(maxit) < (bad[0] if bad.size else maxit)
     live = _check_history(hr[reproducible], hr_o[reproducible])
