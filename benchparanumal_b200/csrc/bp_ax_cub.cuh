@@ -112,6 +112,21 @@ struct CubShape {
   static constexpr size_t GOFF = (FIELDS + 15) & ~(size_t)15;                        // [EPB][GP*6] ggeo
   static constexpr size_t WOFF = GOFF + (STAGE && STIFF ? sizeof(CubReal) * (size_t)EPB * GP * 6 : 0);   // [EPB][GP] wJ
   static constexpr size_t SMEM = STAGE ? WOFF + sizeof(CubReal) * (size_t)EPB * GP : FIELDS;
+  // The pipelined FP32 form (ax_cub_pipe_kernel): the element groups' indices
+  // and gathered q, double-buffered, and a ring of element ids behind the
+  // staged factors.
+  static constexpr int NP = NQ * NQ * NQ;
+  static constexpr size_t IOFF = (SMEM + 15) & ~(size_t)15;                 // [EPB][NP] GlobalToLocal
+  static constexpr size_t QOFF = IOFF + sizeof(int32_t) * (size_t)EPB * NP;   // [2][EPB][NP] q
+  static constexpr size_t EOFF = QOFF + sizeof(CubReal) * 2 * (size_t)EPB * NP;   // [4][EPB] element ids
+  static constexpr size_t PSMEM = EOFF + sizeof(int32_t) * 4 * (size_t)EPB;
+  // blocks per SM that shared memory allows (228 KB per SM, 1 KB reserved per
+  // block); the pipelined form is used only where it keeps the slot kernel's
+  // residency (Nq = 10 would fall from two blocks to one, Nq = 16 not fit)
+  static constexpr int smem_blocks(size_t bytes) { return (int)((228 * 1024) / (bytes + 1024)); }
+  static constexpr int min_(int a, int b) { return a < b ? a : b; }
+  static constexpr bool PIPE_OK =
+      PSMEM <= 227 * 1024 && min_(smem_blocks(PSMEM), MINB) >= min_(smem_blocks(SMEM), MINB);
 };
 
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
@@ -122,7 +137,240 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
                : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The 1D matrices of a form in the constant bank: T(o, i) maps NQ nodes to G
+// points (MASS_AFFINE applies MM^T), D(a, b) is G x G; AT indexes a G^3 field.
+#define CUB_T(o, i)                                                          \
+  (FORM == CUB_MASS_AFFINE ? c_cub[CubShape<NQ, FORM>::SLOT + (i) * NQ + (o)] \
+                           : c_cub[CubShape<NQ, FORM>::SLOT + (o) * NQ + (i)])
+#define CUB_D(a, b) c_cub[CubShape<NQ, FORM>::SLOT + CubShape<NQ, FORM>::TSIZE + (a) * CubShape<NQ, FORM>::G + (b)]
+#define CUB_AT(B, z, y, x) B[(z) * CubShape<NQ, FORM>::PLANE + (y) * CubShape<NQ, FORM>::RS + (x)]
+
+// Interpolation of one element slot to its G^3 points: along b from the
+// q-line qb of node (a, c) = (tx, ty) (threads tx, ty < NQ), along a over
+// shared memory (rows (j, c) = (tx, ty)), along c into the register column qk
+// of point (i, j) = (tx, ty).  Reads of U after the call are the thread's own
+// column.
+template <int NQ, int FORM>
+__device__ __forceinline__ void cub_interp(const CubReal (&qb)[NQ], CubReal* U,
+                                           CubReal (&qk)[CubShape<NQ, FORM>::G], int tx, int ty) {
+  using F = CubReal;
+  constexpr int G = CubShape<NQ, FORM>::G;
+  if (tx < NQ && ty < NQ) {
+BP_CUB_OUTER
+    for (int jj = 0; jj < G; ++jj) {
+      F t = 0;
+#pragma unroll
+      for (int b = 0; b < NQ; ++b) t += CUB_T(jj, b) * qb[b];
+      CUB_AT(U, ty, jj, tx) = t;
+    }
+  }
+  __syncthreads();
+  if (ty < NQ) {
+    F r[NQ];
+#pragma unroll
+    for (int a = 0; a < NQ; ++a) r[a] = CUB_AT(U, ty, tx, a);
+BP_CUB_OUTER
+    for (int ii = 0; ii < G; ++ii) {
+      F t = 0;
+#pragma unroll
+      for (int a = 0; a < NQ; ++a) t += CUB_T(ii, a) * r[a];
+      CUB_AT(U, ty, tx, ii) = t;
+    }
+  }
+  __syncthreads();
+  F r[NQ];
+#pragma unroll
+  for (int c = 0; c < NQ; ++c) r[c] = CUB_AT(U, c, ty, tx);
+#pragma unroll
+  for (int k = 0; k < G; ++k) {
+    F t = 0;
+#pragma unroll
+    for (int c = 0; c < NQ; ++c) t += CUB_T(k, c) * r[c];
+    qk[k] = t;
+  }
+}
+
+// Factors at the points of column (tx, ty), three sources.  ready() runs before
+// the barrier ahead of the flux loop, released() after the barrier behind it
+// (no thread reads factors after that).
+template <class F>
+struct CubStagedFactors {   // staged in shared memory by cp.async at the element's start
+  const F* sG;
+  const F* sW;
+  __device__ __forceinline__ void ready() const { cp_async_wait_all(); }
+  __device__ __forceinline__ void released() const {}
+  __device__ __forceinline__ void get(int pt, F (&g)[6], F& w) const {
+    using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
+    const V2* gv = reinterpret_cast<const V2*>(sG + 6 * pt);
+    const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
+    g[0] = a0.x; g[1] = a0.y; g[2] = a1.x; g[3] = a1.y; g[4] = a2.x; g[5] = a2.y;
+    w = sW[pt];
+  }
+};
+template <class F>
+struct CubGlobalFactors {   // read from global memory at the flux loop
+  const F* ggeo;              // the element's block
+  const F* wJ;
+  __device__ __forceinline__ void ready() const {}
+  __device__ __forceinline__ void released() const {}
+  __device__ __forceinline__ void get(int pt, F (&g)[6], F& w) const {
+    using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
+    const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * pt);
+    const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
+    g[0] = a0.x; g[1] = a0.y; g[2] = a1.x; g[3] = a1.y; g[4] = a2.x; g[5] = a2.y;
+    w = wJ[pt];
+  }
+};
+template <class F>
+struct CubAffineFactors {   // one set per element, in registers
+  F ga[6];
+  F wa;
+  __device__ __forceinline__ void ready() const {}
+  __device__ __forceinline__ void released() const {}
+  __device__ __forceinline__ void get(int, F (&g)[6], F& w) const {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) g[c] = ga[c];
+    w = wa;
+  }
+};
+
+// Stiffness plus lambda mass at the points of column (i, j) = (tx, ty):
+// acc = Dr^T(G00 dr + G01 ds + G02 dt) + Ds^T(...) + Dt^T(...) + lambda w qk.
+// The r- and s-parts run over shared memory (U, R, S), the t-part in
+// registers; U's own column receives qk first.
+template <int NQ, int FORM, class Fac>
+__device__ __forceinline__ void cub_stiff(const CubReal (&qk)[CubShape<NQ, FORM>::G],
+                                          CubReal (&acc)[CubShape<NQ, FORM>::G], CubReal* U, CubReal* R,
+                                          CubReal* S, int tx, int ty, CubReal lambda, const Fac& fac) {
+  using F = CubReal;
+  constexpr int G = CubShape<NQ, FORM>::G;
+  // own column: every earlier read of it was this thread's
+#pragma unroll
+  for (int k = 0; k < G; ++k) CUB_AT(U, k, ty, tx) = qk[k];
+  __syncthreads();
+  // r-derivative on the row (y, z) = (tx, ty); s-derivative on the column (x, z) = (tx, ty)
+  {
+    F r[G];
+#pragma unroll
+    for (int n = 0; n < G; ++n) r[n] = CUB_AT(U, ty, tx, n);
+BP_CUB_OUTER
+    for (int i = 0; i < G; ++i) {
+      F t = 0;
+#pragma unroll
+      for (int n = 0; n < G; ++n) t += CUB_D(i, n) * r[n];
+      CUB_AT(R, ty, tx, i) = t;
+    }
+#pragma unroll
+    for (int n = 0; n < G; ++n) r[n] = CUB_AT(U, ty, n, tx);
+BP_CUB_OUTER
+    for (int j = 0; j < G; ++j) {
+      F t = 0;
+#pragma unroll
+      for (int n = 0; n < G; ++n) t += CUB_D(j, n) * r[n];
+      CUB_AT(S, ty, j, tx) = t;
+    }
+  }
+  // t-derivative on the column (x, y) = (tx, ty) in registers
+  F gt[G];
+#pragma unroll
+  for (int k = 0; k < G; ++k) {
+    F t = 0;
+#pragma unroll
+    for (int n = 0; n < G; ++n) t += CUB_D(k, n) * qk[n];
+    gt[k] = t;
+  }
+  fac.ready();   // this thread's copies; the barrier below makes all visible
+  __syncthreads();
+  // fluxes at the points of column (tx, ty)
+#pragma unroll
+  for (int k = 0; k < G; ++k) {
+    F g[6], w;
+    fac.get(k * G * G + ty * G + tx, g, w);
+    const F dr = CUB_AT(R, k, ty, tx), ds = CUB_AT(S, k, ty, tx), dt = gt[k];
+    CUB_AT(R, k, ty, tx) = g[0] * dr + g[1] * ds + g[2] * dt;
+    CUB_AT(S, k, ty, tx) = g[1] * dr + g[3] * ds + g[4] * dt;
+    gt[k] = g[2] * dr + g[4] * ds + g[5] * dt;
+    acc[k] = lambda * w * qk[k];
+  }
+  // t-part of the weak divergence, in registers
+#pragma unroll
+  for (int n = 0; n < G; ++n) {
+    F t = acc[n];
+#pragma unroll
+    for (int k = 0; k < G; ++k) t += CUB_D(k, n) * gt[k];
+    acc[n] = t;
+  }
+  __syncthreads();
+  fac.released();
+  // r-part on rows, s-part on columns, in place
+  {
+    F r[G];
+#pragma unroll
+    for (int n = 0; n < G; ++n) r[n] = CUB_AT(R, ty, tx, n);
+BP_CUB_OUTER
+    for (int i = 0; i < G; ++i) {
+      F t = 0;
+#pragma unroll
+      for (int n = 0; n < G; ++n) t += CUB_D(n, i) * r[n];
+      CUB_AT(R, ty, tx, i) = t;
+    }
+#pragma unroll
+    for (int n = 0; n < G; ++n) r[n] = CUB_AT(S, ty, n, tx);
+BP_CUB_OUTER
+    for (int j = 0; j < G; ++j) {
+      F t = 0;
+#pragma unroll
+      for (int n = 0; n < G; ++n) t += CUB_D(n, j) * r[n];
+      CUB_AT(S, ty, j, tx) = t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < G; ++k) acc[k] += CUB_AT(R, k, ty, tx) + CUB_AT(S, k, ty, tx);
+}
+
+// Projection to the nodes along c (from the register column acc of point
+// (i, j) = (tx, ty)) and along a (rows (j, c) = (tx, ty)); the caller
+// finishes along b from U: node (a, c) = (tx, ty) reads U(c, :, a).
+template <int NQ, int FORM>
+__device__ __forceinline__ void cub_project_ca(const CubReal (&acc)[CubShape<NQ, FORM>::G], CubReal* U, int tx,
+                                               int ty) {
+  using F = CubReal;
+  constexpr int G = CubShape<NQ, FORM>::G;
+  // own column of U
+BP_CUB_OUTER
+  for (int c = 0; c < NQ; ++c) {
+    F t = 0;
+#pragma unroll
+    for (int k = 0; k < G; ++k) t += CUB_T(k, c) * acc[k];
+    CUB_AT(U, c, ty, tx) = t;
+  }
+  __syncthreads();
+  if (ty < NQ) {
+    F r[G];
+#pragma unroll
+    for (int ii = 0; ii < G; ++ii) r[ii] = CUB_AT(U, ty, tx, ii);
+BP_CUB_OUTER
+    for (int a = 0; a < NQ; ++a) {
+      F t = 0;
+#pragma unroll
+      for (int ii = 0; ii < G; ++ii) t += CUB_T(ii, a) * r[ii];
+      CUB_AT(U, ty, tx, a) = t;
+    }
+  }
+  __syncthreads();
+}
 
 template <int NQ, int FORM>
 __global__ void __launch_bounds__(CubShape<NQ, FORM>::THREADS, CubShape<NQ, FORM>::MINB)
@@ -133,22 +381,15 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
   if (skip && *skip) return;
   using F = CubReal;
   using Sh = CubShape<NQ, FORM>;
-  using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
-  constexpr int G = Sh::G, GP = Sh::GP, RS = Sh::RS, PLANE = Sh::PLANE, EPB = Sh::EPB;
+  constexpr int G = Sh::G, GP = Sh::GP, EPB = Sh::EPB;
   constexpr int NQ2 = NQ * NQ, NP = NQ * NQ * NQ;
-  constexpr int SLOT = Sh::SLOT, DOFF = Sh::SLOT + Sh::TSIZE;
-  // T(o, i): 1D transform from NQ nodes to G points; MASS_AFFINE applies MM^T
-#define T_(o, i) (FORM == CUB_MASS_AFFINE ? c_cub[SLOT + (i) * NQ + (o)] : c_cub[SLOT + (o) * NQ + (i)])
-#define D_(a, b) c_cub[DOFF + (a) * G + (b)]
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   F* const sbase = reinterpret_cast<F*>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
-  const int tid = tx + G * (ty + G * es);
   F* const U = sbase + (size_t)es * Sh::NBUF * Sh::FIELD;   // the field
   F* const R = U + Sh::FIELD;                                // r-derivative / r-flux
   F* const S = R + Sh::FIELD;                                // s-derivative / s-flux
-#define AT(B, z, y, x) B[(z) * PLANE + (y) * RS + (x)]
 
   const int eidx = blockIdx.x * EPB + es;
   const bool valid = eidx < Nelements;
@@ -168,69 +409,26 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
     for (int c = tl; c < GP; c += G * G) cp_async4(sW + c, srcw + c);
   }
 
-  F wa = 0, ga[6] = {0, 0, 0, 0, 0, 0};
-  if (!Sh::CURVED) {
-    wa = wJ[element];
-    if (Sh::STIFF)
-#pragma unroll
-      for (int c = 0; c < 6; ++c) ga[c] = ggeo[6 * (size_t)element + c];
-  }
-
   for (int f = 0; f < Nfields; ++f) {
     const size_t lbase = ((size_t)element * Nfields + f) * NP;
     if (f > 0) __syncthreads();   // the previous field's last reads of U are done
-    // load q[c][b][a] along b and interpolate along b in registers
-    if (tx < NQ && ty < NQ) {
-      F qb[NQ];   // q along b of node (a, c) = (tx, ty)
+    // q[c][b][a] along b of node (a, c) = (tx, ty)
+    F qb[NQ];
 #pragma unroll
-      for (int b = 0; b < NQ; ++b) {
-        F v = 0;
-        if (valid) {
-          const int32_t id = G2L[lbase + ty * NQ2 + b * NQ + tx];
-          v = (id >= 0) ? q[id] : F(0);
-        }
-        qb[b] = v;
+    for (int b = 0; b < NQ; ++b) {
+      F v = 0;
+      if (valid && tx < NQ && ty < NQ) {
+        const int32_t id = G2L[lbase + ty * NQ2 + b * NQ + tx];
+        v = (id >= 0) ? q[id] : F(0);
       }
-BP_CUB_OUTER
-      for (int jj = 0; jj < G; ++jj) {
-        F t = 0;
-#pragma unroll
-        for (int b = 0; b < NQ; ++b) t += T_(jj, b) * qb[b];
-        AT(U, ty, jj, tx) = t;
-      }
+      qb[b] = v;
     }
-    __syncthreads();
-    // along a: thread (jj, c) = (tx, ty)
-    if (ty < NQ) {
-      F r[NQ];
-#pragma unroll
-      for (int a = 0; a < NQ; ++a) r[a] = AT(U, ty, tx, a);
-BP_CUB_OUTER
-      for (int ii = 0; ii < G; ++ii) {
-        F t = 0;
-#pragma unroll
-        for (int a = 0; a < NQ; ++a) t += T_(ii, a) * r[a];
-        AT(U, ty, tx, ii) = t;
-      }
-    }
-    __syncthreads();
-    // along c: thread (ii, jj) = (tx, ty); the grid column stays in registers
     F qk[G];
-    {
-      F r[NQ];
-#pragma unroll
-      for (int c = 0; c < NQ; ++c) r[c] = AT(U, c, ty, tx);
-#pragma unroll
-      for (int k = 0; k < G; ++k) {
-        F t = 0;
-#pragma unroll
-        for (int c = 0; c < NQ; ++c) t += T_(k, c) * r[c];
-        qk[k] = t;
-      }
-    }
+    cub_interp<NQ, FORM>(qb, U, qk, tx, ty);
     if (FORM == CUB_MASS_AFFINE) {
       // G == NQ: the result column of node (tx, ty) is wJ_e * qk
       if (valid) {
+        const F wa = wJ[element];
 #pragma unroll
         for (int k = 0; k < NQ; ++k) {
           const F out = wa * qk[k];
@@ -256,138 +454,29 @@ BP_CUB_OUTER
 #pragma unroll
         for (int k = 0; k < G; ++k) acc[k] = wJ[gb + k * G * G] * qk[k];
       }
+    } else if (Sh::STAGE) {
+      cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda, CubStagedFactors<F>{sG, sW});
+    } else if (Sh::CURVED) {
+      cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda,
+                          CubGlobalFactors<F>{ggeo + 6 * (size_t)element * GP, wJ + (size_t)element * GP});
     } else {
-      // own column: every earlier read of it was this thread's
+      CubAffineFactors<F> fa;
 #pragma unroll
-      for (int k = 0; k < G; ++k) AT(U, k, ty, tx) = qk[k];
-      __syncthreads();
-      // r-derivative on the row (y, z) = (tx, ty); s-derivative on the column (x, z) = (tx, ty)
-      {
-        F r[G];
-#pragma unroll
-        for (int n = 0; n < G; ++n) r[n] = AT(U, ty, tx, n);
-BP_CUB_OUTER
-        for (int i = 0; i < G; ++i) {
-          F t = 0;
-#pragma unroll
-          for (int n = 0; n < G; ++n) t += D_(i, n) * r[n];
-          AT(R, ty, tx, i) = t;
-        }
-#pragma unroll
-        for (int n = 0; n < G; ++n) r[n] = AT(U, ty, n, tx);
-BP_CUB_OUTER
-        for (int j = 0; j < G; ++j) {
-          F t = 0;
-#pragma unroll
-          for (int n = 0; n < G; ++n) t += D_(j, n) * r[n];
-          AT(S, ty, j, tx) = t;
-        }
-      }
-      // t-derivative on the column (x, y) = (tx, ty) in registers
-      F gt[G];
-#pragma unroll
-      for (int k = 0; k < G; ++k) {
-        F t = 0;
-#pragma unroll
-        for (int n = 0; n < G; ++n) t += D_(k, n) * qk[n];
-        gt[k] = t;
-      }
-      if (Sh::STAGE) cp_async_wait_all();   // this thread's copies; the barrier below makes all visible
-      __syncthreads();
-      // fluxes at the points of column (tx, ty)
-#pragma unroll
-      for (int k = 0; k < G; ++k) {
-        F g0, g1, g2, g3, g4, g5, w;
-        if (Sh::STAGE) {
-          const int pt = k * G * G + ty * G + tx;
-          const V2* gv = reinterpret_cast<const V2*>(sG + 6 * pt);
-          const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
-          g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
-          w = sW[pt];
-        } else if (Sh::CURVED) {
-          const size_t gb = (size_t)element * GP + k * G * G + ty * G + tx;
-          const V2* gv = reinterpret_cast<const V2*>(ggeo + 6 * gb);
-          const V2 a0 = gv[0], a1 = gv[1], a2 = gv[2];
-          g0 = a0.x; g1 = a0.y; g2 = a1.x; g3 = a1.y; g4 = a2.x; g5 = a2.y;
-          w = wJ[gb];
-        } else {
-          g0 = ga[0]; g1 = ga[1]; g2 = ga[2]; g3 = ga[3]; g4 = ga[4]; g5 = ga[5];
-          w = wa;
-        }
-        const F dr = AT(R, k, ty, tx), ds = AT(S, k, ty, tx), dt = gt[k];
-        AT(R, k, ty, tx) = g0 * dr + g1 * ds + g2 * dt;
-        AT(S, k, ty, tx) = g1 * dr + g3 * ds + g4 * dt;
-        gt[k] = g2 * dr + g4 * ds + g5 * dt;
-        acc[k] = lambda * w * qk[k];
-      }
-      // t-part of the weak divergence, in registers
-#pragma unroll
-      for (int n = 0; n < G; ++n) {
-        F t = acc[n];
-#pragma unroll
-        for (int k = 0; k < G; ++k) t += D_(k, n) * gt[k];
-        acc[n] = t;
-      }
-      __syncthreads();
-      // r-part on rows, s-part on columns, in place
-      {
-        F r[G];
-#pragma unroll
-        for (int n = 0; n < G; ++n) r[n] = AT(R, ty, tx, n);
-BP_CUB_OUTER
-        for (int i = 0; i < G; ++i) {
-          F t = 0;
-#pragma unroll
-          for (int n = 0; n < G; ++n) t += D_(n, i) * r[n];
-          AT(R, ty, tx, i) = t;
-        }
-#pragma unroll
-        for (int n = 0; n < G; ++n) r[n] = AT(S, ty, n, tx);
-BP_CUB_OUTER
-        for (int j = 0; j < G; ++j) {
-          F t = 0;
-#pragma unroll
-          for (int n = 0; n < G; ++n) t += D_(n, j) * r[n];
-          AT(S, ty, j, tx) = t;
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < G; ++k) acc[k] += AT(R, k, ty, tx) + AT(S, k, ty, tx);
+      for (int c = 0; c < 6; ++c) fa.ga[c] = ggeo[6 * (size_t)element + c];
+      fa.wa = wJ[element];
+      cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda, fa);
     }
-    // projection along c in registers: column (ii, jj) = (tx, ty); own column of U
-BP_CUB_OUTER
-    for (int c = 0; c < NQ; ++c) {
-      F t = 0;
-#pragma unroll
-      for (int k = 0; k < G; ++k) t += T_(k, c) * acc[k];
-      AT(U, c, ty, tx) = t;
-    }
-    __syncthreads();
-    // along a: row (jj, c) = (tx, ty)
-    if (ty < NQ) {
-      F r[G];
-#pragma unroll
-      for (int ii = 0; ii < G; ++ii) r[ii] = AT(U, ty, tx, ii);
-BP_CUB_OUTER
-      for (int a = 0; a < NQ; ++a) {
-        F t = 0;
-#pragma unroll
-        for (int ii = 0; ii < G; ++ii) t += T_(ii, a) * r[ii];
-        AT(U, ty, tx, a) = t;
-      }
-    }
-    __syncthreads();
+    cub_project_ca<NQ, FORM>(acc, U, tx, ty);
     // along b: node (a, c) = (tx, ty), the line q was loaded along
     if (tx < NQ && ty < NQ && valid) {
       F r[G];
 #pragma unroll
-      for (int jj = 0; jj < G; ++jj) r[jj] = AT(U, ty, jj, tx);
+      for (int jj = 0; jj < G; ++jj) r[jj] = CUB_AT(U, ty, jj, tx);
 #pragma unroll
       for (int b = 0; b < NQ; ++b) {
         F t = 0;
 #pragma unroll
-        for (int jj = 0; jj < G; ++jj) t += T_(jj, b) * r[jj];
+        for (int jj = 0; jj < G; ++jj) t += CUB_T(jj, b) * r[jj];
         const size_t l = lbase + ty * NQ2 + b * NQ + tx;
         Aq[l] = t;
         if (partials) {   // q again (a cache hit) rather than a line held in registers throughout
@@ -400,11 +489,179 @@ BP_CUB_OUTER
   if (partials) {
     static_assert(Sh::FIELDS >= sizeof(double) * Sh::THREADS, "scratch too small");
     const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(sbase));
+    if (tx == 0 && ty == 0 && es == 0) partials[blockIdx.x] = bs;
+  }
+}
+
+// FP32 curved stiffness (BP3, one field, even Nq) with the memory traffic of
+// the next element groups in flight while a group computes.  A resident grid
+// of blocks loops over groups of EPB elements; with iteration i of a block on
+// group h_i = blockIdx.x + i gridDim.x, the pipeline holds
+//   element ids of h_{i+3}  -> sEl[(i+3) & 3]   (4-byte copies)
+//   GlobalToLocal of h_{i+2} -> sIdx            (16-byte copies)
+//   q of h_{i+1}             -> sQ[(i+1) & 1]   (4-byte gathers through sIdx)
+// issued as one commit group at the start of iteration i, and the factors of
+// h_{i+1} -> sG, sW issued as the next group once iteration i's flux loop is
+// done with h_i's.  A thread gathers the nodes of the same 16-byte index chunks
+// it copies, so sIdx needs no barrier; q, the ids and the factors are read by
+// other threads after a wait and a barrier.  The q.Aq partial reads q from sQ.
+template <int NQ>
+__global__ void __launch_bounds__(CubShape<NQ, CUB_STIFF>::THREADS, CubShape<NQ, CUB_STIFF>::MINB)
+ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+                   const CubReal* __restrict__ wJ, const CubReal* __restrict__ ggeo, CubReal lambda,
+                   const CubReal* __restrict__ q, CubReal* __restrict__ Aq, const int* __restrict__ skip,
+                   double* __restrict__ partials) {
+  constexpr int FORM = CUB_STIFF;
+  using F = CubReal;
+  using Sh = CubShape<NQ, FORM>;
+  static_assert(sizeof(F) == 4 && Sh::STAGE && NQ % 2 == 0, "FP32, staged factors, whole 16-byte index chunks");
+  constexpr int G = Sh::G, GP = Sh::GP, EPB = Sh::EPB, NP = Sh::NP, NQ2 = NQ * NQ;
+  constexpr int CH = NP / 4;   // 16-byte chunks of an element's GlobalToLocal
+  if (skip && *skip) return;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  F* const sbase = reinterpret_cast<F*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
+  const int tid = tx + G * (ty + G * es);
+  F* const U = sbase + (size_t)es * Sh::NBUF * Sh::FIELD;
+  F* const R = U + Sh::FIELD;
+  F* const S = R + Sh::FIELD;
+  F* const sG0 = reinterpret_cast<F*>(smem_raw + Sh::GOFF);
+  F* const sW0 = reinterpret_cast<F*>(smem_raw + Sh::WOFF);
+  int32_t* const sIdx = reinterpret_cast<int32_t*>(smem_raw + Sh::IOFF);
+  F* const sQ = reinterpret_cast<F*>(smem_raw + Sh::QOFF);
+  int32_t* const sEl = reinterpret_cast<int32_t*>(smem_raw + Sh::EOFF);
+
+  const int ngroups = (Nelements + EPB - 1) / EPB;
+  auto group = [&](int i) { return blockIdx.x + i * gridDim.x; };
+  // element ids of iteration i's group (-1 past the end) into sEl[i & 3]
+  auto issue_ids = [&](int i, bool async) {
+    if (tid < EPB) {
+      const int e = group(i) * EPB + tid;
+      int32_t* dst = sEl + (i & 3) * EPB + tid;
+      if (group(i) < ngroups && e < Nelements) {
+        if (async) cp_async4(dst, elementList + e);
+        else *dst = elementList[e];
+      } else {
+        *dst = -1;
+      }
+    }
+  };
+  // GlobalToLocal of iteration i's group into sIdx (ids in sEl[i & 3] visible)
+  auto issue_idx = [&](int i) {
+    for (int w = tid; w < EPB * CH; w += Sh::THREADS) {
+      const int s = w / CH, c = w - s * CH;
+      const int32_t e = sEl[(i & 3) * EPB + s];
+      if (e >= 0) cp_async16(sIdx + s * NP + 4 * c, G2L + (size_t)e * NP + 4 * c);
+    }
+  };
+  // q of iteration i's group into sQ[i & 1] through this thread's chunks of sIdx
+  auto issue_q = [&](int i) {
+    F* dstq = sQ + (size_t)(i & 1) * EPB * NP;
+    for (int w = tid; w < EPB * CH; w += Sh::THREADS) {
+      const int s = w / CH, c = w - s * CH;
+      const bool live = sEl[(i & 3) * EPB + s] >= 0;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const int pos = s * NP + 4 * c + n;
+        const int32_t id = live ? sIdx[pos] : -1;
+        if (id >= 0) cp_async4(dstq + pos, q + id);
+        else dstq[pos] = F(0);
+      }
+    }
+  };
+  // factors of iteration i's group into sG, sW
+  auto issue_factors = [&](int i) {
+    const int32_t e = sEl[(i & 3) * EPB + es];
+    if (e >= 0) {
+      const int tl = tx + G * ty;
+      const F* src = ggeo + 6 * (size_t)e * GP;   // 8-byte aligned: 24 bytes per point
+      F* sG = sG0 + (size_t)es * GP * 6;
+      for (int c = tl; c < GP * 3; c += G * G) cp_async8(sG + 2 * c, src + 2 * c);
+      const F* srcw = wJ + (size_t)e * GP;
+      F* sW = sW0 + (size_t)es * GP;
+      for (int c = tl; c < GP; c += G * G) cp_async4(sW + c, srcw + c);
+    }
+  };
+  struct PipeFactors {
+    CubStagedFactors<F> st;
+    const decltype(issue_factors)* next;
+    int i;
+    __device__ __forceinline__ void ready() const { cp_async_wait_group<1>(); }
+    __device__ __forceinline__ void released() const {
+      (*next)(i + 1);
+      cp_async_commit();
+    }
+    __device__ __forceinline__ void get(int pt, F (&g)[6], F& w) const { st.get(pt, g, w); }
+  };
+
+  // prologue: ids of iterations 0 and 1, indices of 0; then q of 0, indices
+  // of 1 and ids of 2 as one group, the factors of 0 as the next
+  issue_ids(0, false);
+  issue_ids(1, false);
+  __syncthreads();
+  issue_idx(0);
+  cp_async_commit();
+  cp_async_wait_group<0>();   // this thread's index chunks
+  issue_q(0);
+  issue_idx(1);
+  issue_ids(2, true);
+  cp_async_commit();
+  issue_factors(0);
+  cp_async_commit();
+
+  double pdot = 0.0;
+  for (int i = 0; group(i) < ngroups; ++i) {
+    cp_async_wait_group<1>();   // all but the factors of this group
+    __syncthreads();
+    const F* qg = sQ + (size_t)(i & 1) * EPB * NP + (size_t)es * NP;
+    const int32_t element = sEl[(i & 3) * EPB + es];
+    F qb[NQ];
+#pragma unroll
+    for (int b = 0; b < NQ; ++b) qb[b] = (tx < NQ && ty < NQ) ? qg[ty * NQ2 + b * NQ + tx] : F(0);
+    // the next groups' ids, indices and q
+    issue_q(i + 1);
+    issue_idx(i + 2);
+    issue_ids(i + 3, true);
+    cp_async_commit();
+
+    F qk[G], acc[G];
+    cub_interp<NQ, FORM>(qb, U, qk, tx, ty);
+    const PipeFactors fac{CubStagedFactors<F>{sG0 + (size_t)es * GP * 6, sW0 + (size_t)es * GP}, &issue_factors, i};
+    cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda, fac);
+    cub_project_ca<NQ, FORM>(acc, U, tx, ty);
+    if (tx < NQ && ty < NQ && element >= 0) {
+      F r[G];
+#pragma unroll
+      for (int jj = 0; jj < G; ++jj) r[jj] = CUB_AT(U, ty, jj, tx);
+      const size_t lbase = (size_t)element * NP;
+#pragma unroll
+      for (int b = 0; b < NQ; ++b) {
+        F t = 0;
+#pragma unroll
+        for (int jj = 0; jj < G; ++jj) t += CUB_T(jj, b) * r[jj];
+        Aq[lbase + ty * NQ2 + b * NQ + tx] = t;
+        if (partials) pdot += (double)qg[ty * NQ2 + b * NQ + tx] * (double)t;
+      }
+    }
+  }
+  cp_async_wait_all();   // nothing is left in flight (groups past the end issue no copies)
+  if (partials) {
+    static_assert(Sh::FIELDS >= sizeof(double) * Sh::THREADS, "scratch too small");
+    const double bs = fuse_block_sum(pdot, reinterpret_cast<double*>(sbase));
     if (tid == 0) partials[blockIdx.x] = bs;
   }
-#undef AT
-#undef D_
-#undef T_
+}
+#undef CUB_AT
+#undef CUB_D
+#undef CUB_T
+
+// The pipelined FP32 stiffness kernel is the default where it applies;
+// BP_CUB_PIPE=0, read at every launch, keeps the one-element-per-slot kernel
+// (for comparisons and tests).
+static bool cub_pipe_enabled() {
+  const char* e = getenv("BP_CUB_PIPE");
+  return !(e && e[0] == '0');
 }
 
 // device address of the constant table on the current device
@@ -427,10 +684,35 @@ static int launch_cub_form(int32_t Nelements, int Nfields, const int32_t* elemen
   if (Sh::STIFF)
     BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT + Sh::TSIZE, o.D, sizeof(CubReal) * Sh::DSIZE,
                                 cudaMemcpyDeviceToDevice, s));
+  const dim3 block(Sh::G, Sh::G, Sh::EPB);
+  if constexpr (FORM == CUB_STIFF && Sh::STAGE && NQ % 2 == 0 && Sh::PIPE_OK) {
+    if (Nfields == 1 && !(reinterpret_cast<uintptr_t>(G2L) & 15) && cub_pipe_enabled()) {
+      static DeviceOnce configured;
+      static int resident[kMaxDevices] = {};
+      BP_TRY(once_per_device(configured, []() -> int {
+        BP_CUDA_TRY(cudaFuncSetAttribute(ax_cub_pipe_kernel<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Sh::PSMEM));
+        int dev = 0, nb = 0;
+        BP_TRY(current_device(&dev));
+        BP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ax_cub_pipe_kernel<NQ>, Sh::THREADS,
+                                                                  Sh::PSMEM));
+        resident[dev] = nb > 0 ? nb * sm_count() : 1;
+        return BP_SUCCESS;
+      }));
+      int dev = 0;
+      BP_TRY(current_device(&dev));
+      const int ngroups = (Nelements + Sh::EPB - 1) / Sh::EPB;
+      const dim3 grid(ngroups < resident[dev] ? ngroups : resident[dev]);
+      if (nblocks) *nblocks = (int)grid.x;
+      ax_cub_pipe_kernel<NQ><<<grid, block, Sh::PSMEM, s>>>(Nelements, elementList, G2L, o.wJ, o.ggeo, lambda, q, Aq,
+                                                            skip, partials);
+      BP_CUDA_TRY(cudaGetLastError());
+      return BP_SUCCESS;
+    }
+  }
   if (Sh::SMEM > 48 * 1024)
     BP_CUDA_TRY(cudaFuncSetAttribute(ax_cub_kernel<NQ, FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)Sh::SMEM));
-  const dim3 block(Sh::G, Sh::G, Sh::EPB);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
   ax_cub_kernel<NQ, FORM><<<grid, block, Sh::SMEM, s>>>(Nelements, Nfields, elementList, G2L, o.wJ, o.ggeo, lambda,

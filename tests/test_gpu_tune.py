@@ -1,7 +1,8 @@
 """The element-operator autotuner (bp_tune.cu).
 
 The first launch of a configuration outside a capture measures every form
-that applies and keeps the fastest; BP_AUTOTUNE=0 keeps the measured static
+that applies, in interleaved rounds, and keeps the fastest (the static choice
+unless beaten by more than 2%); BP_AUTOTUNE=0 keeps the measured static
 choice; a solver launches its operator once before capturing its graphs, so
 the graphs use the tuned form; results do not depend on the form (within the
 parity bars).
@@ -28,7 +29,11 @@ def test_first_launch_measures_every_form_and_keeps_the_fastest(gpu, oracle, N, 
     form, times = gpu.tune_report(0, N, 1, affine, 8, 1, 0, gm.E)
     # the stored-factor TMA form needs even Nq: at N=4 only the line and pencil forms apply
     assert len(times) == nforms, times
-    assert form == min(times, key=times.get)
+    # the fastest form, unless the static choice (the first form measured) is
+    # within 2% of it
+    fastest = min(times, key=times.get)
+    first = next(iter(times))
+    assert form == fastest or (form == first and times[first] <= times[fastest] / 0.98)
     assert rel(dA.download(), om.ax(q)) <= 1e-12
 
 
