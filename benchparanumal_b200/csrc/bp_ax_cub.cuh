@@ -63,7 +63,8 @@ enum CubForm { CUB_MASS_AFFINE = 0, CUB_MASS = 1, CUB_STIFF_AFFINE = 2, CUB_STIF
 // slot, both write the mesh's cubInterp), the affine stiffness forms of
 // BP3/BP4 (T = invV [NQ x NQ], then the modal cubD [NQ x NQ]) and the affine
 // mass forms of BP1/BP2 (T = MM [NQ x NQ]).  Each launch first copies its
-// operands into its slot on the launch stream, so two launches of the same
+// operands into its slot on the launch stream (once per slot and source in a
+// stream capture: const_slot_copy), so two launches of the same
 // degree and group on different streams must pass the same matrices (every
 // caller that passes its mesh's own matrices does); operators of different
 // groups never share a slot.
@@ -95,6 +96,13 @@ struct CubShape {
   static constexpr int PLANE = G * RS;
   static constexpr int FIELD = G * PLANE;           // one G^3 field in shared memory
   static constexpr int NBUF = STIFF ? 3 : 1;        // u, and the r/s buffers of the stiffness
+  // words between consecutive element slots' buffers beyond NBUF fields: the
+  // warps that straddle two slots then spread their shared-memory accesses
+  // over more banks (padding chosen per Nq by counting the wavefronts of every
+  // access pattern of the FP32 kernels: 12-25% fewer at Nq = 2, 4, 5, 6, 8)
+  static constexpr int SPAD = sizeof(CubReal) != 4 ? 0
+                              : NQ == 2 ? 10 : NQ == 4 ? 2 : NQ == 5 ? 8 : NQ == 6 ? 12 : NQ == 8 ? 6 : NQ == 9 ? 8 : 0;
+  static constexpr int SLOTW = NBUF * FIELD + SPAD;   // words per element slot
   static constexpr int EPB0 = 256 / G2 < 1 ? 1 : 256 / G2;
   static constexpr int EPB = EPB0 > 8 ? 8 : EPB0;   // element slots per block
   static constexpr int THREADS = G2 * EPB;
@@ -108,7 +116,7 @@ struct CubShape {
   // and the interpolation (the FP64 factors would halve the resident blocks)
   static constexpr bool STAGE = CURVED && sizeof(CubReal) == 4;
   static constexpr int GP = G * G * G;
-  static constexpr size_t FIELDS = sizeof(CubReal) * (size_t)NBUF * FIELD * EPB;
+  static constexpr size_t FIELDS = sizeof(CubReal) * (size_t)SLOTW * EPB;
   static constexpr size_t GOFF = (FIELDS + 15) & ~(size_t)15;                        // [EPB][GP*6] ggeo
   static constexpr size_t WOFF = GOFF + (STAGE && STIFF ? sizeof(CubReal) * (size_t)EPB * GP * 6 : 0);   // [EPB][GP] wJ
   static constexpr size_t SMEM = STAGE ? WOFF + sizeof(CubReal) * (size_t)EPB * GP : FIELDS;
@@ -281,14 +289,21 @@ BP_CUB_OUTER
       CUB_AT(S, ty, j, tx) = t;
     }
   }
-  // t-derivative on the column (x, y) = (tx, ty) in registers
+  // t-derivative on the column (x, y) = (tx, ty) in registers, from U's own
+  // column (which keeps qk until the projection) rather than from registers
+  // held through the r/s phase
   F gt[G];
+  {
+    F u[G];
 #pragma unroll
-  for (int k = 0; k < G; ++k) {
-    F t = 0;
+    for (int n = 0; n < G; ++n) u[n] = CUB_AT(U, n, ty, tx);
 #pragma unroll
-    for (int n = 0; n < G; ++n) t += CUB_D(k, n) * qk[n];
-    gt[k] = t;
+    for (int k = 0; k < G; ++k) {
+      F t = 0;
+#pragma unroll
+      for (int n = 0; n < G; ++n) t += CUB_D(k, n) * u[n];
+      gt[k] = t;
+    }
   }
   fac.ready();   // this thread's copies; the barrier below makes all visible
   __syncthreads();
@@ -301,7 +316,7 @@ BP_CUB_OUTER
     CUB_AT(R, k, ty, tx) = g[0] * dr + g[1] * ds + g[2] * dt;
     CUB_AT(S, k, ty, tx) = g[1] * dr + g[3] * ds + g[4] * dt;
     gt[k] = g[2] * dr + g[4] * ds + g[5] * dt;
-    acc[k] = lambda * w * qk[k];
+    acc[k] = lambda * w * CUB_AT(U, k, ty, tx);
   }
   // t-part of the weak divergence, in registers
 #pragma unroll
@@ -378,6 +393,8 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
               const CubReal* __restrict__ wJ, const CubReal* __restrict__ ggeo, CubReal lambda,
               const CubReal* __restrict__ q, CubReal* __restrict__ Aq, const int* __restrict__ skip,
               double* __restrict__ partials) {
+  pdl_wait();
+  pdl_release();
   if (skip && *skip) return;
   using F = CubReal;
   using Sh = CubShape<NQ, FORM>;
@@ -387,7 +404,7 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
   extern __shared__ __align__(16) unsigned char smem_raw[];
   F* const sbase = reinterpret_cast<F*>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
-  F* const U = sbase + (size_t)es * Sh::NBUF * Sh::FIELD;   // the field
+  F* const U = sbase + (size_t)es * Sh::SLOTW;   // the field
   F* const R = U + Sh::FIELD;                                // r-derivative / r-flux
   F* const S = R + Sh::FIELD;                                // s-derivative / s-flux
 
@@ -493,18 +510,20 @@ ax_cub_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLis
   }
 }
 
-// FP32 curved stiffness (BP3, one field, even Nq) with the memory traffic of
-// the next element groups in flight while a group computes.  A resident grid
-// of blocks loops over groups of EPB elements; with iteration i of a block on
+// Curved stiffness (BP3, one field, even Nq) with the memory traffic of the
+// next element groups in flight while a group computes.  A resident grid of
+// blocks loops over groups of EPB elements; with iteration i of a block on
 // group h_i = blockIdx.x + i gridDim.x, the pipeline holds
 //   element ids of h_{i+3}  -> sEl[(i+3) & 3]   (4-byte copies)
 //   GlobalToLocal of h_{i+2} -> sIdx            (16-byte copies)
-//   q of h_{i+1}             -> sQ[(i+1) & 1]   (4-byte gathers through sIdx)
-// issued as one commit group at the start of iteration i, and the factors of
-// h_{i+1} -> sG, sW issued as the next group once iteration i's flux loop is
-// done with h_i's.  A thread gathers the nodes of the same 16-byte index chunks
-// it copies, so sIdx needs no barrier; q, the ids and the factors are read by
-// other threads after a wait and a barrier.  The q.Aq partial reads q from sQ.
+//   q of h_{i+1}             -> sQ[(i+1) & 1]   (gathers through sIdx)
+// issued as one commit group at the start of iteration i; in FP32 the factors
+// of h_{i+1} -> sG, sW follow as the next group once iteration i's flux loop
+// is done with h_i's (FP64 reads its factors at the flux loop: staging them
+// would halve the resident blocks).  A thread gathers the nodes of the same
+// 16-byte index chunks it copies, so sIdx needs no barrier; q, the ids and the
+// factors are read by other threads after a wait and a barrier.  The q.Aq
+// partial reads q from sQ instead of gathering it again.
 template <int NQ>
 __global__ void __launch_bounds__(CubShape<NQ, CUB_STIFF>::THREADS, CubShape<NQ, CUB_STIFF>::MINB)
 ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
@@ -514,16 +533,19 @@ ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const
   constexpr int FORM = CUB_STIFF;
   using F = CubReal;
   using Sh = CubShape<NQ, FORM>;
-  static_assert(sizeof(F) == 4 && Sh::STAGE && NQ % 2 == 0, "FP32, staged factors, whole 16-byte index chunks");
+  static_assert(NQ % 2 == 0, "whole 16-byte index chunks");
+  constexpr bool STG = Sh::STAGE;   // FP32 stages the factors; FP64 reads them at the flux loop
   constexpr int G = Sh::G, GP = Sh::GP, EPB = Sh::EPB, NP = Sh::NP, NQ2 = NQ * NQ;
   constexpr int CH = NP / 4;   // 16-byte chunks of an element's GlobalToLocal
+  pdl_wait();
+  pdl_release();
   if (skip && *skip) return;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   F* const sbase = reinterpret_cast<F*>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, es = threadIdx.z;
   const int tid = tx + G * (ty + G * es);
-  F* const U = sbase + (size_t)es * Sh::NBUF * Sh::FIELD;
+  F* const U = sbase + (size_t)es * Sh::SLOTW;
   F* const R = U + Sh::FIELD;
   F* const S = R + Sh::FIELD;
   F* const sG0 = reinterpret_cast<F*>(smem_raw + Sh::GOFF);
@@ -565,8 +587,9 @@ ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const
       for (int n = 0; n < 4; ++n) {
         const int pos = s * NP + 4 * c + n;
         const int32_t id = live ? sIdx[pos] : -1;
-        if (id >= 0) cp_async4(dstq + pos, q + id);
-        else dstq[pos] = F(0);
+        if (id < 0) dstq[pos] = F(0);
+        else if constexpr (sizeof(F) == 8) cp_async8(dstq + pos, q + id);
+        else cp_async4(dstq + pos, q + id);
       }
     }
   };
@@ -607,12 +630,15 @@ ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const
   issue_idx(1);
   issue_ids(2, true);
   cp_async_commit();
-  issue_factors(0);
-  cp_async_commit();
+  if (STG) {
+    issue_factors(0);
+    cp_async_commit();
+  }
 
   double pdot = 0.0;
   for (int i = 0; group(i) < ngroups; ++i) {
-    cp_async_wait_group<1>();   // all but the factors of this group
+    if (STG) cp_async_wait_group<1>();   // all but the factors of this group
+    else cp_async_wait_group<0>();
     __syncthreads();
     const F* qg = sQ + (size_t)(i & 1) * EPB * NP + (size_t)es * NP;
     const int32_t element = sEl[(i & 3) * EPB + es];
@@ -627,8 +653,14 @@ ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const
 
     F qk[G], acc[G];
     cub_interp<NQ, FORM>(qb, U, qk, tx, ty);
-    const PipeFactors fac{CubStagedFactors<F>{sG0 + (size_t)es * GP * 6, sW0 + (size_t)es * GP}, &issue_factors, i};
-    cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda, fac);
+    if constexpr (STG) {
+      const PipeFactors fac{CubStagedFactors<F>{sG0 + (size_t)es * GP * 6, sW0 + (size_t)es * GP}, &issue_factors,
+                            i};
+      cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda, fac);
+    } else {
+      const size_t e = element >= 0 ? (size_t)element : 0;
+      cub_stiff<NQ, FORM>(qk, acc, U, R, S, tx, ty, lambda, CubGlobalFactors<F>{ggeo + 6 * e * GP, wJ + e * GP});
+    }
     cub_project_ca<NQ, FORM>(acc, U, tx, ty);
     if (tx < NQ && ty < NQ && element >= 0) {
       F r[G];
@@ -656,7 +688,7 @@ ax_cub_pipe_kernel(int Nelements, const int32_t* __restrict__ elementList, const
 #undef CUB_D
 #undef CUB_T
 
-// The pipelined FP32 stiffness kernel is the default where it applies;
+// The pipelined stiffness kernel is the default where it applies;
 // BP_CUB_PIPE=0, read at every launch, keeps the one-element-per-slot kernel
 // (for comparisons and tests).
 static bool cub_pipe_enabled() {
@@ -680,12 +712,11 @@ static int launch_cub_form(int32_t Nelements, int Nfields, const int32_t* elemen
   CubReal* tab = cub_table_address();
   if (!tab) return fail(BP_ERROR_CUDA, "over-integrated operator: constant table address lookup failed");
   // this launch's 1D operands into its slot of the constant bank, in stream order
-  BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT, o.T, sizeof(CubReal) * Sh::TSIZE, cudaMemcpyDeviceToDevice, s));
+  BP_TRY(const_slot_copy(tab + Sh::SLOT, o.T, sizeof(CubReal) * Sh::TSIZE, s));
   if (Sh::STIFF)
-    BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT + Sh::TSIZE, o.D, sizeof(CubReal) * Sh::DSIZE,
-                                cudaMemcpyDeviceToDevice, s));
+    BP_TRY(const_slot_copy(tab + Sh::SLOT + Sh::TSIZE, o.D, sizeof(CubReal) * Sh::DSIZE, s));
   const dim3 block(Sh::G, Sh::G, Sh::EPB);
-  if constexpr (FORM == CUB_STIFF && Sh::STAGE && NQ % 2 == 0 && Sh::PIPE_OK) {
+  if constexpr (FORM == CUB_STIFF && NQ % 2 == 0 && Sh::PIPE_OK) {
     if (Nfields == 1 && !(reinterpret_cast<uintptr_t>(G2L) & 15) && cub_pipe_enabled()) {
       static DeviceOnce configured;
       static int resident[kMaxDevices] = {};
@@ -704,9 +735,8 @@ static int launch_cub_form(int32_t Nelements, int Nfields, const int32_t* elemen
       const int ngroups = (Nelements + Sh::EPB - 1) / Sh::EPB;
       const dim3 grid(ngroups < resident[dev] ? ngroups : resident[dev]);
       if (nblocks) *nblocks = (int)grid.x;
-      ax_cub_pipe_kernel<NQ><<<grid, block, Sh::PSMEM, s>>>(Nelements, elementList, G2L, o.wJ, o.ggeo, lambda, q, Aq,
-                                                            skip, partials);
-      BP_CUDA_TRY(cudaGetLastError());
+      BP_CUDA_TRY(launch_pdl(ax_cub_pipe_kernel<NQ>, grid, block, Sh::PSMEM, s, Nelements, elementList, G2L, o.wJ,
+                             o.ggeo, lambda, q, Aq, skip, partials));
       return BP_SUCCESS;
     }
   }
@@ -715,9 +745,8 @@ static int launch_cub_form(int32_t Nelements, int Nfields, const int32_t* elemen
                                      (int)Sh::SMEM));
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
-  ax_cub_kernel<NQ, FORM><<<grid, block, Sh::SMEM, s>>>(Nelements, Nfields, elementList, G2L, o.wJ, o.ggeo, lambda,
-                                                         q, Aq, skip, partials);
-  BP_CUDA_TRY(cudaGetLastError());
+  BP_CUDA_TRY(launch_pdl(ax_cub_kernel<NQ, FORM>, grid, block, Sh::SMEM, s, Nelements, Nfields, elementList, G2L, o.wJ,
+                         o.ggeo, lambda, q, Aq, skip, partials));
   return BP_SUCCESS;
 }
 

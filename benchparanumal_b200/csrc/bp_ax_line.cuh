@@ -270,6 +270,8 @@ ax_line_kernel(int Nelements, int Nfields, const int32_t* __restrict__ elementLi
                const LineReal* __restrict__ wJ, const LineReal* __restrict__ ggeo,
                const LineReal* __restrict__ gllw, LineReal lambda, const T* __restrict__ q,
                T* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
+  pdl_wait();
+  pdl_release();
   if (skip && *skip) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ax_line_body<NQ, AFFINE, T>(blockIdx.x, gridDim.x, Nelements, Nfields, elementList, G2L, wJ, ggeo, gllw, lambda, q,
@@ -293,9 +295,9 @@ static int launch_line_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_
     return fail(BP_ERROR_ARG, "element operator: ggeo must be aligned to two elements");
   LineReal* tab = line_table_address();
   if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
-  BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT, D, sizeof(LineReal) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  BP_TRY(const_slot_copy(tab + Sh::SLOT, D, sizeof(LineReal) * NQ * NQ, s));
   if (d.affine)
-    BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT + NQ * NQ, gllw, sizeof(LineReal) * NQ, cudaMemcpyDeviceToDevice, s));
+    BP_TRY(const_slot_copy(tab + Sh::SLOT + NQ * NQ, gllw, sizeof(LineReal) * NQ, s));
   const dim3 block(NQ, NQ, Sh::EPB);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
@@ -303,14 +305,14 @@ static int launch_line_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_
     if (SMEM > 48 * 1024)
       BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)SMEM));
-    ax_line_kernel<NQ, true, T><<<grid, block, SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
-                                                          lambda, q, Aq, skip, partials);
+    BP_CUDA_TRY(launch_pdl(ax_line_kernel<NQ, true, T>, grid, block, SMEM, s, Nelements, d.Nfields, elementList, G2L,
+                           wJ, ggeo, gllw, lambda, q, Aq, skip, partials));
   } else {
     if (SMEM > 48 * 1024)
       BP_CUDA_TRY(cudaFuncSetAttribute(ax_line_kernel<NQ, false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)SMEM));
-    ax_line_kernel<NQ, false, T><<<grid, block, SMEM, s>>>(Nelements, d.Nfields, elementList, G2L, wJ, ggeo, gllw,
-                                                           lambda, q, Aq, skip, partials);
+    BP_CUDA_TRY(launch_pdl(ax_line_kernel<NQ, false, T>, grid, block, SMEM, s, Nelements, d.Nfields, elementList,
+                           G2L, wJ, ggeo, gllw, lambda, q, Aq, skip, partials));
   }
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;

@@ -25,9 +25,9 @@ int launch_step_line_nq(const bp_ax_desc_t& d, GrpStepArgs a, int grid_cap, cuda
   using Sh = LineShape<NQ, T>;
   LineReal* tab = line_table_address();
   if (!tab) return fail(BP_ERROR_CUDA, "persistent CG step: constant table address lookup failed");
-  BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT, a.D, sizeof(float) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  BP_TRY(const_slot_copy(tab + Sh::SLOT, a.D, sizeof(float) * NQ * NQ, s));
   if (d.affine)
-    BP_CUDA_TRY(cudaMemcpyAsync(tab + Sh::SLOT + NQ * NQ, a.gllw, sizeof(float) * NQ, cudaMemcpyDeviceToDevice, s));
+    BP_TRY(const_slot_copy(tab + Sh::SLOT + NQ * NQ, a.gllw, sizeof(float) * NQ, s));
   a.nblk_op = (a.Nelements + Sh::EPB - 1) / Sh::EPB;
   const dim3 block(NQ, NQ, Sh::EPB);
   if (d.affine) return launch_grp_step_kernel<PK, LineStepOp<NQ, true, T>>(a, block, Sh::smem(), grid_cap, s);

@@ -414,6 +414,8 @@ __global__ void __launch_bounds__(NQ * NQ * TmaShape<NQ, F>::EPB * NF, (TmaMinBl
 ax_tma_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
               const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ Dg, F lambda,
               const T* __restrict__ q, T* __restrict__ Aq, const int* __restrict__ skip, CgFuse fuse) {
+  pdl_wait();
+  pdl_release();
   if (skip && *skip) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   ax_tma_body<NQ, NF, DOT, R, F, T, WITHHOLD, DIR>(blockIdx.x, gridDim.x, Nelements, elementList, G2L, wJ, ggeo, Dg,
@@ -435,13 +437,12 @@ static int launch_tma_dot(int32_t Nelements, const int32_t* elementList, const i
   }));
   F* tab = tma_d_table<F>();
   if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
-  BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), D, sizeof(F) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  BP_TRY(const_slot_copy(tab + tma_d_slot(NQ), D, sizeof(F) * NQ * NQ, s));
   const dim3 block(NQ, NQ, Sh::EPB * NF);
   const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
   if (nblocks) *nblocks = (int)grid.x;
-  ax_tma_kernel<NQ, NF, DOT, R, F, T, -1, DIR><<<grid, block, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D,
-                                                                         lambda, q, Aq, skip, fuse);
-  BP_CUDA_TRY(cudaGetLastError());
+  BP_CUDA_TRY(launch_pdl(ax_tma_kernel<NQ, NF, DOT, R, F, T, -1, DIR>, grid, block, smem, s, Nelements, elementList,
+                         G2L, wJ, ggeo, D, lambda, q, Aq, skip, fuse));
   return BP_SUCCESS;
 }
 
@@ -595,6 +596,8 @@ ax_rb_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32
              const float* __restrict__ wJ, const float* __restrict__ ggeo, const float* __restrict__ Dg,
              float lambda, const float* __restrict__ q, float* __restrict__ Aq, const int* __restrict__ skip,
              CgFuse fuse) {
+  pdl_wait();
+  pdl_release();
   if (skip && *skip) return;
   using Sh = RbShape<NQ, L>;
   constexpr int H = Sh::H, NQ2 = Sh::NQ2, NP = NQ2 * NQ, R = Sh::R, RS = Sh::RS;
@@ -776,11 +779,10 @@ static int launch_rb_dot(int32_t Nelements, const int32_t* elementList, const in
   }));
   float* tab = tma_d_table<float>();
   if (!tab) return fail(BP_ERROR_CUDA, "element operator: constant table address lookup failed");
-  BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), D, sizeof(float) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  BP_TRY(const_slot_copy(tab + tma_d_slot(NQ), D, sizeof(float) * NQ * NQ, s));
   if (nblocks) *nblocks = Nelements;
-  ax_rb_kernel<NQ, L, DOT><<<Nelements, Sh::THREADS, smem, s>>>(Nelements, elementList, G2L, wJ, ggeo, D, lambda, q,
-                                                                 Aq, skip, fuse);
-  BP_CUDA_TRY(cudaGetLastError());
+  BP_CUDA_TRY(launch_pdl(ax_rb_kernel<NQ, L, DOT>, Nelements, Sh::THREADS, smem, s, Nelements, elementList, G2L, wJ,
+                         ggeo, D, lambda, q, Aq, skip, fuse));
   return BP_SUCCESS;
 }
 
@@ -867,7 +869,7 @@ int launch_step_tma_nq(GrpStepArgs a, int grid_cap, cudaStream_t s) {
   using Sh = TmaShape<NQ, float>;
   float* tab = tma_d_table<float>();
   if (!tab) return fail(BP_ERROR_CUDA, "persistent CG step: constant table address lookup failed");
-  BP_CUDA_TRY(cudaMemcpyAsync(tab + tma_d_slot(NQ), a.D, sizeof(float) * NQ * NQ, cudaMemcpyDeviceToDevice, s));
+  BP_TRY(const_slot_copy(tab + tma_d_slot(NQ), a.D, sizeof(float) * NQ * NQ, s));
   a.nblk_op = (a.Nelements + Sh::EPB - 1) / Sh::EPB;
   return launch_grp_step_kernel<PK, TmaStepOp<NQ, T>>(a, dim3(NQ, NQ, Sh::EPB), TmaSmem<NQ, 1, Sh::R, float, T>::BYTES,
                                                        grid_cap, s);

@@ -3,7 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <utility>
 #include <vector>
@@ -63,6 +65,42 @@ cudaStream_t default_stream() {
   if (!s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess)
     g_stream[dev].store(s, std::memory_order_release);
   return s;
+}
+
+// The last copy captured into each constant-bank slot: (capture, stream,
+// source, bytes).  Keyed by the slot's device address (unique across devices
+// under unified addressing).
+struct SlotCopy {
+  unsigned long long capture = 0;
+  cudaStream_t stream = nullptr;
+  const void* src = nullptr;
+  size_t bytes = 0;
+};
+static std::mutex g_slot_lock;
+static std::map<void*, SlotCopy> g_slot_last;
+
+int const_slot_copy(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  unsigned long long id = 0;
+  BP_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, &id));
+  if (st == cudaStreamCaptureStatusActive) {
+    std::lock_guard<std::mutex> lock(g_slot_lock);
+    SlotCopy& last = g_slot_last[dst];
+    if (last.capture == id && last.stream == s && last.src == src && last.bytes == bytes) return BP_SUCCESS;
+    BP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    last = SlotCopy{id, s, src, bytes};
+    return BP_SUCCESS;
+  }
+  BP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+  return BP_SUCCESS;
+}
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("BP_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 int sm_count() {

@@ -78,6 +78,42 @@ inline cudaStream_t to_stream(bp_stream_t s) {
 }
 int sm_count();   // multiprocessors of the current device
 
+// Copies `bytes` of device memory `src` into the constant-bank slot `dst` on
+// stream s.  Inside a stream capture, a copy of the same source into the same
+// slot already captured on the same stream in the same capture is still in
+// effect (stream order), so it is not captured again: a CUDA graph of many CG
+// iterations holds one copy per slot rather than one per operator launch (and
+// its kernels stay adjacent for programmatic dependent launch).  Outside
+// captures every call copies.
+int const_slot_copy(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
+// Programmatic dependent launch for the kernels of a CG iteration: launched
+// with launch_pdl, a kernel may be scheduled while its predecessor on the
+// stream finishes.  Every such kernel calls pdl_wait() before it reads
+// anything (it returns once the predecessor has completed and its memory is
+// visible; at once for a kernel launched without the attribute) and
+// pdl_release() to let its own successor be scheduled.  BP_PDL=0, read once,
+// launches without the attribute.
+bool pdl_enabled();
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+#endif
+
 // ---- device buffer owned by the library ----
 template <class T>
 struct DeviceArray {

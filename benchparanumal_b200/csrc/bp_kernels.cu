@@ -50,6 +50,8 @@ ax_pencil_kernel(int Nelements, const int32_t* __restrict__ elementList, const i
                  const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ gllw,
                  const F* __restrict__ Dg, F lambda, const F* __restrict__ q, F* __restrict__ Aq,
                  const int* __restrict__ skip, CgFuse fuse) {
+  pdl_wait();
+  pdl_release();
   if (skip && *skip) return;
   using V2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
   constexpr int EPB = AxShape<NQ>::EPB;
@@ -200,9 +202,9 @@ static int launch_pencil(const bp_ax_desc_t& d, int32_t Nelements, const int32_t
   if (nblocks) *nblocks = (int)grid.x;
   const bool vec = ((reinterpret_cast<uintptr_t>(ggeo) & (2 * sizeof(F) - 1)) == 0);
   const CgFuse Fz = fuse ? *fuse : CgFuse{};
-#define BP_PENCIL(NF, AFF, VEC, DOT)                                                                          \
-  ax_pencil_kernel<NQ, NF, AFF, VEC, DOT, F><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, \
-                                                                    lambda, q, Aq, skip, Fz)
+#define BP_PENCIL(NF, AFF, VEC, DOT)                                                                             \
+  BP_CUDA_TRY(launch_pdl(ax_pencil_kernel<NQ, NF, AFF, VEC, DOT, F>, grid, block, 0, s, Nelements, elementList, G2L, \
+                         wJ, ggeo, gllw, D, lambda, q, Aq, skip, Fz))
   if (fuse) {
     if (!d.affine && !vec) return fail(BP_ERROR_ARG, "CG operator needs aligned geometric factors");
     if (d.Nfields == 1) {

@@ -5,7 +5,8 @@
 // multi-rhs variants), each best somewhere in (degree, fields, factor storage,
 // precision, lanes).  The first time a configuration is launched outside a
 // stream capture, every applicable form is run on the caller's own operands --
-// one untimed launch, then three timed with CUDA events on the launch stream --
+// one untimed launch, then timed in interleaved rounds with CUDA events on the
+// launch stream --
 // and the fastest is kept for that configuration (and element-count class, a
 // power of two) on that device; later
 // launches, the captured CUDA graphs of the solvers included, use it.  While a
