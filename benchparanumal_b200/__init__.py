@@ -43,14 +43,14 @@ EXPORTS = [
     "bp_malloc", "bp_free", "bp_host_malloc", "bp_host_free", "bp_memcpy_htod", "bp_memcpy_dtoh",
     "bp_memcpy_dtod", "bp_memset", "bp_stream_create", "bp_stream_destroy", "bp_finish",
     "bp_event_create", "bp_event_destroy", "bp_event_record", "bp_event_elapsed_ms",
-    "bp_ax_hex3d", "bp_ogs_gather", "bp_ogs_scatter", "bp_linalg_set", "bp_linalg_axpy",
+    "bp_ax_hex3d", "bp_ax_tri2d", "bp_ogs_gather", "bp_ogs_scatter", "bp_linalg_set", "bp_linalg_axpy",
     "bp_linalg_inner_prod", "bp_linalg_norm2", "bp_update_cg",
     "bp_mesh_create", "bp_mesh_view", "bp_mesh_destroy",
     "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc", "bp_ogs_check",
     "bp_test_wait_timeout", "bp_tune_report", "bp_tune_reset",
-    "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature",
+    "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature", "bp_basis_tri2d",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
     "bp_ax_cub_hex3d_f32", "bp_mesh_write_vtu", "bp_ogs_owner_map", "bp_cg_direction_ax_hex3d",
@@ -74,7 +74,7 @@ class AxDesc(ctypes.Structure):
 class BoxDesc(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("N", ctypes.c_int32),
                 ("affine", ctypes.c_int32), ("Nfields", ctypes.c_int32), ("pert", ctypes.c_double),
-                ("pert_seed", ctypes.c_uint64), ("dim", ctypes.c_int32)]
+                ("pert_seed", ctypes.c_uint64), ("dim", ctypes.c_int32), ("simplex", ctypes.c_int32)]
 
 
 class MeshView(ctypes.Structure):
@@ -82,7 +82,10 @@ class MeshView(ctypes.Structure):
                 ("Nelements", ctypes.c_int32), ("Nfields", ctypes.c_int32), ("affine", ctypes.c_int32),
                 ("Ngather", ctypes.c_int32), ("nnz", ctypes.c_int32), ("Nlocal", ctypes.c_int64)] + [
         (n, ctypes.c_void_p) for n in ("elementList", "GlobalToLocal", "rowStarts", "colIds", "wJ", "ggeo", "D",
-                                       "gllz", "gllw", "EX", "EY", "EZ")] + [("dim", ctypes.c_int32)]
+                                       "gllz", "gllw", "EX", "EY", "EZ")] + [("dim", ctypes.c_int32),
+                                                                              ("simplex", ctypes.c_int32),
+                                                                              ("S", ctypes.c_void_p),
+                                                                              ("MM", ctypes.c_void_p)]
 
 
 def _ax_desc(mesh, bp=None):
@@ -148,6 +151,7 @@ def lib():
             "bp_event_record": [vp, vp],
             "bp_event_elapsed_ms": [vp, vp, ctypes.POINTER(ctypes.c_float)],
             "bp_ax_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
+            "bp_ax_tri2d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
             "bp_ogs_gather": [i32, vp, vp, vp, vp, vp],
             "bp_ogs_scatter": [i32, vp, vp, vp, vp, vp],
             "bp_linalg_set": [i32, dbl, vp, vp],
@@ -178,6 +182,7 @@ def lib():
                                           vp, vp, vp, vp],
             "bp_ax_cub_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
             "bp_mesh_cubature": [vp],
+            "bp_basis_tri2d": [i32, vp, vp, vp, vp, vp],
             "bp_mesh_cubature_view": [vp, ctypes.POINTER(CubatureView)],
             "bp_basis_cubature": [i32, vp, vp, vp, vp, vp, vp, vp],
             "bp_batch_create": [ctypes.POINTER(BatchProblem), i32, ctypes.POINTER(SolverDesc), ctypes.POINTER(vp)],
@@ -310,13 +315,16 @@ def _dl(ptr, n, dtype):
 
 class Mesh:
     """Box mesh on the device (mesh_t + masked ogs), built by bp_mesh_create:
-    Hex3D, or Quad2D with dim=2 (nz ignored; Nfields 1 or 2)."""
+    Hex3D, or Quad2D with dim=2 (nz ignored; Nfields 1 or 2), or Tri2D with
+    dim=2 and simplex=True (affine, one field, 2*nx*ny triangles)."""
 
-    def __init__(self, nx, ny=None, nz=None, N=4, affine=False, Nfields=1, pert=0.0, pert_seed=1, device=0, dim=3):
+    def __init__(self, nx, ny=None, nz=None, N=4, affine=False, Nfields=1, pert=0.0, pert_seed=1, device=0, dim=3,
+                 simplex=False):
         platform_init(device)
         ny = nx if ny is None else ny
         nz = (nx if nz is None else nz) if dim == 3 else 1
-        d = BoxDesc(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), int(pert_seed), int(dim))
+        d = BoxDesc(nx, ny, nz, N, int(bool(affine)), Nfields, float(pert), int(pert_seed), int(dim),
+                    int(bool(simplex)))
         h = ctypes.c_void_p()
         _check(lib().bp_mesh_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h.value
@@ -325,6 +333,7 @@ class Mesh:
         v = self.view
         self.nx, self.ny, self.nz = nx, ny, nz
         self.dim = v.dim
+        self.simplex = bool(v.simplex)
         self.N, self.Nq, self.Np, self.E = v.N, v.Nq, v.Np, v.Nelements
         self.Nfields, self.affine = v.Nfields, bool(v.affine)
         self.Ngather, self.nnz, self.NL = v.Ngather, v.nnz, int(v.Nlocal)
@@ -338,7 +347,12 @@ class Mesh:
         """Copy a device mesh array to the host (names as in bp_mesh_view_t)."""
         v = self.view
         ng = self.E if self.affine else self.E * self.Np
-        nv, ngg = (8, 6) if self.dim == 3 else (4, 3)
+        nv, ngg = (8, 6) if self.dim == 3 else ((3, 3) if self.simplex else (4, 3))
+        if self.simplex:   # Tri2D: D holds Dr and Ds, S the three stiffness matrices, MM the mass matrix
+            NP2 = self.Np * self.Np
+            tri = {"D": 2 * NP2, "S": 3 * NP2, "MM": NP2}
+            if name in tri:
+                return _dl(getattr(v, name), tri[name], np.float64)
         spec = {
             "elementList": (self.E, np.int32), "GlobalToLocal": (self.NL, np.int32),
             "rowStarts": (self.Ngather + 1, np.int32), "colIds": (self.nnz, np.int32),
@@ -397,6 +411,14 @@ def ax_cub_hex3d(mesh, bp, q, Aq, lam=1.0, stream=None):
 def convert_f64_f32(src, n, dst, stream=None):
     """dst (FP32 device) = src (FP64 device address or buffer), n elements."""
     _check(lib().bp_convert_f64_f32(n, src if isinstance(src, int) else _ptr(src), _ptr(dst), stream))
+
+
+def ax_tri2d(mesh, q, Aq, lam=1.0, stream=None):
+    """bp_ax_tri2d on a Tri2D mesh's own arrays: Aq (E-vector) = A_e q[G2L]."""
+    v = mesh.view
+    d = AxDesc(5, mesh.N, 1, 1, 2)
+    _check(lib().bp_ax_tri2d(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, v.wJ, v.ggeo, v.S, v.MM,
+                             float(lam), q.ptr, Aq.ptr, stream))
 
 
 def ax_hex3d_f32(mesh, q, Aq, ops, lam=1.0, stream=None):
@@ -633,19 +655,32 @@ def uneven_problems(count=64, seed=2, nrhs=4, pmin=3, pmax=10, nmin=8, nmax=24, 
     return probs
 
 
-def box_numbering(nx, ny, nz, N, Nfields=1, dim=3):
+def box_numbering(nx, ny, nz, N, Nfields=1, dim=3, simplex=False):
     """Host-only masked numbering of the box: (GlobalToLocal, rowStarts, colIds).
-    dim=2: the Quad2D box of nx x ny elements (nz ignored)."""
-    d = BoxDesc(nx, ny, nz if dim == 3 else 1, N, 0, Nfields, 0.0, 1, dim)
+    dim=2: the Quad2D box of nx x ny elements (nz ignored); with simplex=True
+    the Tri2D box of 2 nx ny triangles."""
+    d = BoxDesc(nx, ny, nz if dim == 3 else 1, N, int(bool(simplex)), Nfields, 0.0, 1, dim, int(bool(simplex)))
     ng, nnz = ctypes.c_int32(), ctypes.c_int32()
     _check(lib().bp_box_numbering(ctypes.byref(d), ctypes.byref(ng), ctypes.byref(nnz), None, None, None))
-    E = nx * ny * (nz if dim == 3 else 1)
-    Np = (N + 1) ** dim
+    E = nx * ny * (nz if dim == 3 else 1) * (2 if simplex else 1)
+    Np = (N + 1) * (N + 2) // 2 if simplex else (N + 1) ** dim
     g2l = np.empty(E * Np * Nfields, np.int32)
     rs = np.empty(ng.value + 1, np.int32)
     ci = np.empty(nnz.value, np.int32)
     _check(lib().bp_box_numbering(ctypes.byref(d), None, None, g2l.ctypes.data, rs.ctypes.data, ci.ctypes.data))
     return g2l, rs, ci
+
+
+def basis_tri2d(N):
+    """Host-only Tri2D reference element: r, s [Np], Dr, Ds, MM, Srr, Srs, Sss as
+    row-major Np x Np arrays (X[n, k] weighs node k in output n)."""
+    Np = (N + 1) * (N + 2) // 2
+    r, s = np.empty(Np), np.empty(Np)
+    D, MM, S = np.empty(2 * Np * Np), np.empty(Np * Np), np.empty(3 * Np * Np)
+    _check(lib().bp_basis_tri2d(N, r.ctypes.data, s.ctypes.data, D.ctypes.data, MM.ctypes.data, S.ctypes.data))
+    D = D.reshape(2, Np, Np).transpose(0, 2, 1)
+    S = S.reshape(3, Np, Np).transpose(0, 2, 1)
+    return r, s, D[0], D[1], MM.reshape(Np, Np), S[0], S[1], S[2]
 
 
 def basis_gll(N):

@@ -306,6 +306,21 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                    to_stream(stream));
 }
 
+int bp_ax_tri2d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* elementList, const int32_t* GlobalToLocal,
+                const double* wJ, const double* ggeo, const double* S, const double* MM, double lambda,
+                const double* q, double* Aq, bp_stream_t stream) {
+  if (!d) return fail(BP_ERROR_ARG, "bp_ax_tri2d: null descriptor");
+  if (d->bp != 5 || d->Nfields != 1 || d->dim != 2 || !d->affine)
+    return fail(BP_ERROR_ARG, "bp_ax_tri2d: the Tri2D operator is BP5, one field, dim 2, affine");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_tri2d: degree N must be in 1..15");
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_tri2d: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  if (!elementList || !GlobalToLocal || !wJ || !ggeo || !S || !MM || !q || !Aq)
+    return fail(BP_ERROR_ARG, "bp_ax_tri2d: null array");
+  return launch_ax_tri(d->N, Nelements, elementList, GlobalToLocal, wJ, ggeo, S, MM, lambda, q, Aq, nullptr,
+                       to_stream(stream));
+}
+
 int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
                     const int32_t* GlobalToLocal, const float* wJ, const float* ggeo, const float* gllw,
                     const float* D, float lambda, const float* q, float* Aq, bp_stream_t stream) {
@@ -592,10 +607,76 @@ static int mesh_create_quad(const bp_box_desc_t* d, bp_mesh_t* out) {
   return BP_SUCCESS;
 }
 
+// the node-fastest device layout of row-major Np x Np blocks: out[k*Np + n] = in[n*Np + k]
+static std::vector<double> node_fastest(const std::vector<double>& rm, int Np) {
+  std::vector<double> t(rm.size());
+  const size_t NP2 = (size_t)Np * Np;
+  for (size_t b = 0; b < rm.size() / NP2; ++b)
+    for (int n = 0; n < Np; ++n)
+      for (int k = 0; k < Np; ++k) t[b * NP2 + (size_t)k * Np + n] = rm[b * NP2 + (size_t)n * Np + k];
+  return t;
+}
+
+static int mesh_create_tri(const bp_box_desc_t* d, bp_mesh_t* out) {
+  if (d->nx < 1 || d->ny < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
+  if (d->Nfields != 1) return fail(BP_ERROR_ARG, "bp_mesh_create: Tri2D meshes take one field (BP5)");
+  if (!d->affine) return fail(BP_ERROR_ARG, "bp_mesh_create: Tri2D meshes are affine here (-a)");
+  if (d->pert != 0.0) return fail(BP_ERROR_ARG, "bp_mesh_create: the Tri2D box has no vertex perturbation");
+  TriBasis tb;
+  if (!tri_basis(d->N, tb)) return fail(BP_ERROR_NUMERIC, "bp_mesh_create: singular Tri2D Vandermonde matrix");
+  const int Np = tb.Np;
+  const int64_t E64 = 2 * (int64_t)d->nx * d->ny;
+  if (E64 * Np >= (int64_t)INT32_MAX)
+    return fail(BP_ERROR_ARG, "bp_mesh_create: local node count exceeds int32 (dlong) range");
+  cudaStream_t s = default_stream();
+  HostMesh hm;
+  hm.dim = 2;
+  hm.N = d->N; hm.Nq = d->N + 1; hm.Np = Np;
+  hm.nx = d->nx; hm.ny = d->ny; hm.nz = 1;
+  hm.E = (int)E64; hm.affine = 1; hm.Nfields = 1;
+  std::vector<double> wJ, ggeo;
+  if (!box_tri(hm, tb, wJ, ggeo))
+    return fail(BP_ERROR_NUMERIC, "bp_mesh_create: non-positive Jacobian found");
+  std::vector<double> D(tb.Dr);
+  D.insert(D.end(), tb.Ds.begin(), tb.Ds.end());
+  bp_mesh_s* m = new bp_mesh_s();
+  m->dim = 2;
+  m->simplex = 1;
+  m->N = hm.N; m->Nq = hm.Nq; m->Np = Np; m->E = hm.E; m->Nfields = 1; m->affine = 1;
+  m->Ngather = hm.Ngather; m->nnz = hm.nnz;
+  std::vector<int32_t> elist(hm.E);
+  for (int e = 0; e < hm.E; ++e) elist[e] = e;
+  int rc = BP_SUCCESS;
+  do {
+    if ((rc = m->elementList.upload(elist, s))) break;
+    if ((rc = m->G2L.upload(hm.G2L, s))) break;
+    if ((rc = m->rowStarts.upload(hm.rowStarts, s))) break;
+    if ((rc = m->colIds.upload(hm.colIds, s))) break;
+    if ((rc = m->D.upload(node_fastest(D, Np), s))) break;
+    if ((rc = m->S.upload(node_fastest(tb.S, Np), s))) break;
+    if ((rc = m->MM.upload(tb.MM, s))) break;   // symmetric
+    if ((rc = m->EX.upload(hm.EX, s))) break;
+    if ((rc = m->EY.upload(hm.EY, s))) break;
+    if ((rc = m->wJ.upload(wJ, s))) break;
+    if ((rc = m->ggeo.upload(ggeo, s))) break;
+    cudaError_t ce = cudaStreamSynchronize(s);   // the host vectors are released on return
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_mesh_create", __FILE__, __LINE__); break; }
+  } while (0);
+  if (rc != BP_SUCCESS) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return BP_SUCCESS;
+}
+
 int bp_mesh_create(const bp_box_desc_t* d, bp_mesh_t* out) {
   if (!d || !out) return fail(BP_ERROR_ARG, "bp_mesh_create: null pointer");
   *out = nullptr;
   if (d->dim != 0 && d->dim != 2 && d->dim != 3) return fail(BP_ERROR_ARG, "bp_mesh_create: dim must be 2 or 3");
+  if (d->simplex && d->dim != 2) return fail(BP_ERROR_ARG, "bp_mesh_create: simplex meshes are Tri2D (dim 2)");
+  if (d->dim == 2 && d->simplex) return mesh_create_tri(d, out);
   if (d->dim == 2) return mesh_create_quad(d, out);
   if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
   if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
@@ -674,6 +755,9 @@ int bp_mesh_view(bp_mesh_t m, bp_mesh_view_t* v) {
   v->wJ = m->wJ.ptr; v->ggeo = m->ggeo.ptr; v->D = m->D.ptr; v->gllz = m->gllz.ptr; v->gllw = m->gllw.ptr;
   v->EX = m->EX.ptr; v->EY = m->EY.ptr; v->EZ = m->EZ.ptr;
   v->dim = m->dim;
+  v->simplex = m->simplex;
+  v->S = m->simplex ? m->S.ptr : nullptr;
+  v->MM = m->simplex ? m->MM.ptr : nullptr;
   return BP_SUCCESS;
 }
 

@@ -195,17 +195,22 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
   if (!S.compare("THREAD MODEL", "CUDA"))
     throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
                              " is not available: this build runs the CUDA (sm_100a) path only");
+  const bool tri = S.compare("ELEMENT TYPE", "Tri");
   const bool quad = S.compare("ELEMENT TYPE", "Quad");
-  if (!S.compare("ELEMENT TYPE", "Hex") && !quad)
-    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex and Quad only");
+  if (!S.compare("ELEMENT TYPE", "Hex") && !quad && !tri)
+    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex, Quad and Tri only");
   if (quad && bp <= 4)
     throw std::runtime_error("ELEMENT TYPE Quad is available for BK5/BK6 and BP5/BP6 (BP1-BP4: Hex only)");
+  if (tri && (bp != 5 || !S.compare("AFFINE MESH", "TRUE") || S.compare("PRECISION", "MIXED") ||
+              !S.compare("FORCING", "RANDOM")))
+    throw std::runtime_error("ELEMENT TYPE Tri is available for BK5 and BP5 with -a, FP64 and -f RANDOM");
   check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
   bp_box_desc_t d{};
-  d.dim = quad ? 2 : 3;
+  d.dim = quad || tri ? 2 : 3;
+  d.simplex = tri ? 1 : 0;
   d.nx = std::atoi(S.get("BOX NX").c_str());
   d.ny = std::atoi(S.get("BOX NY").c_str());
-  d.nz = quad ? 1 : std::atoi(S.get("BOX NZ").c_str());
+  d.nz = quad || tri ? 1 : std::atoi(S.get("BOX NZ").c_str());
   d.N = std::atoi(S.get("POLYNOMIAL DEGREE").c_str());
   d.affine = S.compare("AFFINE MESH", "TRUE") ? 1 : 0;
   d.Nfields = quad && Nfields > 1 ? 2 : Nfields;   // BP6 has Nfields = dim
@@ -251,6 +256,8 @@ double ax_bytes(int bp, const bp_mesh_view_t& v, long long Ndofs, double sv = 8.
 // reference flop model for one Ax application (the same files, Hex branches)
 double ax_flops(int bp, const bp_mesh_view_t& v) {
   const double Nq = v.Nq, E = v.Nelements, Nf = v.Nfields;
+  if (v.simplex)   // affine TRIANGLES branch of bp5Run.cpp:145-150
+    return (8.0 * v.Np * v.Np + 8.0 * v.Np) * Nf * E;
   if (v.dim == 2)   // QUADRILATERALS branches of bp5Run.cpp:144-187
     return (v.affine ? 8 * Nq * Nq * Nq + 12 * Nq * Nq : 8 * Nq * Nq * Nq + 8 * Nq * Nq) * Nf * E;
   const double cNq = v.N + 2, Nq3 = Nq * Nq * Nq, cNq3 = cNq * cNq * cNq;
@@ -387,7 +394,7 @@ int run_bp(const char* name, int bp, Settings& S) {
   const double Nbytes = (4 * Ndofs * 8.0 + NbytesAx + NbytesGather) + (11 * Ndofs * 8.0 + NbytesAx + NbytesGather) * Niter;
   const double NflopsAx = ax_flops(bp, P.view);
   const double Nflops = (5.0 * Ndofs + NflopsAx + NGlobal) + (11.0 * Ndofs + NflopsAx + NGlobal) * Niter;
-  std::string suffix = P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
+  std::string suffix = P.view.simplex ? "Element=Tri" : P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, iterations=%d, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
@@ -491,6 +498,9 @@ int run_bk(const char* name, int bk, Settings& S) {
     else if (fp32)
       check(bp_ax_hex3d_f32_multi(&d, nr, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, wJ32.p,
                                   ggeo32.p, gllw32.p, D32.p, 1.0f, q32.p, Aq32.p, nullptr));
+    else if (P.view.simplex)
+      check(bp_ax_tri2d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
+                        P.view.S, P.view.MM, 1.0, q.p, Aq.p, nullptr));
     else if (bk >= 5)
       check(bp_ax_hex3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
                         P.view.gllw, P.view.D, 1.0, q.p, Aq.p, nullptr));
@@ -510,7 +520,7 @@ int run_bk(const char* name, int bk, Settings& S) {
   double Nbytes = ax_bytes(bk, P.view, Ndofs, fp32 ? 4.0 : 8.0);
   if (nr > 1) Nbytes += (nr - 1) * (Ndofs * 4.0 + (double)P.view.Nlocal * 4.0);
   const double Nflops = ax_flops(bk, P.view) * nr;
-  std::string suffix = P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
+  std::string suffix = P.view.simplex ? "Element=Tri" : P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "

@@ -187,6 +187,17 @@ void box_numbering(HostMesh& m);
 void box_vertices_2d(HostMesh& m, double pert, uint64_t seed);
 void box_numbering_2d(HostMesh& m);
 bool quad_geometry(const HostMesh& m, std::vector<double>& wJ, std::vector<double>& ggeo);
+// Tri2D (dim 2, simplex): reference-element nodes and matrices (row-major),
+// and the box with its affine factors and masked numbering (HostMesh EX/EY
+// hold 3 vertices per element)
+struct TriBasis {
+  int N = 0, Np = 0;
+  std::vector<double> r, s;           // nodes [Np]
+  std::vector<double> Dr, Ds, MM;     // [Np*Np]
+  std::vector<double> S;              // Srr, Srs, Sss [3*Np*Np]
+};
+bool tri_basis(int N, TriBasis& b);
+bool box_tri(HostMesh& m, const TriBasis& b, std::vector<double>& wJ, std::vector<double>& ggeo);
 
 // trilinear map of the eight hex vertices v (mesh_t vertex order) at (r,s,t)
 __host__ __device__ inline double trilinear(const double* v, double r, double s, double t) {
@@ -201,7 +212,8 @@ __host__ __device__ inline double trilinear(const double* v, double r, double s,
 // ---- the opaque objects of the C ABI ----
 struct bp_mesh_s {
   int N, Nq, Np, E, Nfields, affine;
-  int dim = 3;                                  // 2: Quad2D
+  int dim = 3;                                  // 2: Quad2D, or Tri2D when simplex
+  int simplex = 0;                              // 1: Tri2D (affine triangles)
   int32_t Ngather, nnz;
   bp::DeviceArray<int32_t> elementList, G2L, rowStarts, colIds;
   // GlobalToLocal with the owner bit (kOwnerBit) of each gathered node's first
@@ -214,6 +226,9 @@ struct bp_mesh_s {
   bp::DeviceArray<double> cubDV;                // derivative columns for the diagonal: cubD*cubInterp
                                                 // (curved) or cubDmodal*invV (affine)
   bp::DeviceArray<double> cubwJ_c, cubggeo_c;   // curved mesh only
+  // Tri2D: Srr, Srs, Sss [3*Np*Np] node-fastest (X[k*Np + n] weighs node k in
+  // output n); MM above holds the triangle mass matrix and D [2*Np*Np] Dr, Ds
+  bp::DeviceArray<double> S;
   // factors at the quadrature points: curved [E*cubNp], [6*E*cubNp]; affine the
   // per-element wJ and ggeo
   const double* cubwJ() const { return affine ? wJ.ptr : cubwJ_c.ptr; }
@@ -228,6 +243,17 @@ struct bp_mesh_s {
 };
 
 struct bp_solver_s;
+
+// ---- Tri2D (bp_ax_tri.cu) ----
+namespace bp {
+int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
+                  const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,
+                  const int* skip, cudaStream_t s, double* partials = nullptr, int* nblocks = nullptr);
+int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const double* wJ, const double* MM,
+                          const double* f, double* bL, cudaStream_t s);
+int launch_diag_local_tri(int N, int32_t Nelements, const double* wJ, const double* ggeo, const double* S,
+                          const double* MM, double lambda, double* dL, cudaStream_t s);
+}  // namespace bp
 
 // ---- kernel launchers (bp_kernels.cu) ----
 namespace bp {

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <unordered_map>
 
 #include "bp_internal.hpp"
 
@@ -433,6 +434,277 @@ void box_numbering_2d(HostMesh& m) {
   }
 }
 
+// ---- Tri2D ----------------------------------------------------------------
+
+// Orthonormal Jacobi polynomial P_n^(a,b)(x) by its three-term recurrence, and
+// its derivative sqrt(n (n+a+b+1)) P_{n-1}^(a+1,b+1)(x).
+static double jacobi_on(double x, double a, double b, int n) {
+  const double g0 = std::pow(2.0, a + b + 1) / (a + b + 1) * std::tgamma(a + 1) * std::tgamma(b + 1) /
+                    std::tgamma(a + b + 1);
+  double pm = 1.0 / std::sqrt(g0);
+  if (n == 0) return pm;
+  const double g1 = (a + 1) * (b + 1) / (a + b + 3) * g0;
+  double p = ((a + b + 2) * x / 2 + (a - b) / 2) / std::sqrt(g1);
+  double aold = 2 / (2 + a + b) * std::sqrt((a + 1) * (b + 1) / (a + b + 3));
+  for (int i = 1; i < n; ++i) {
+    const double h1 = 2 * i + a + b;
+    const double anew =
+        2 / (h1 + 2) * std::sqrt((i + 1) * (i + 1 + a + b) * (i + 1 + a) * (i + 1 + b) / (h1 + 1) / (h1 + 3));
+    const double bnew = -(a * a - b * b) / h1 / (h1 + 2);
+    const double pn = (-aold * pm + (x - bnew) * p) / anew;
+    pm = p;
+    p = pn;
+    aold = anew;
+  }
+  return p;
+}
+static double jacobi_on_deriv(double x, double a, double b, int n) {
+  return n == 0 ? 0.0 : std::sqrt(n * (n + a + b + 1)) * jacobi_on(x, a + 1, b + 1, n - 1);
+}
+
+// Warp & blend nodes of the triangle (Warburton 2006): equispaced (r, s) rows
+// in the reference's order (meshBasisTri2D.cpp:200-217), each edge warped
+// toward the GLL distribution by the equispaced-to-GLL displacement,
+// interpolated and divided by 1 - r^2, blended into the interior with the
+// optimised alpha of each degree (:509-585).
+static void tri_nodes(int N, std::vector<double>& r, std::vector<double>& s) {
+  static const double alpha_opt[15] = {0.0000, 0.0000, 1.4152, 0.1001, 0.2751, 0.9800, 1.0999, 1.2832,
+                                       1.3648, 1.4773, 1.4959, 1.5743, 1.5770, 1.6223, 1.6258};
+  const double alpha = N < 16 ? alpha_opt[N - 1] : 5.0 / 3.0;
+  r.clear();
+  s.clear();
+  for (int n = 0; n <= N; ++n)
+    for (int m = 0; m + n <= N; ++m) {
+      r.push_back(-1.0 + 2.0 * m / N);
+      s.push_back(-1.0 + 2.0 * n / N);
+    }
+  std::vector<double> gll, w, req(N + 1);
+  gll_nodes_weights(N, gll, w);
+  for (int i = 0; i <= N; ++i) req[i] = -1.0 + 2.0 * i / N;
+  auto warp = [&](double x) {
+    std::vector<double> I;
+    interp_matrix(req, std::vector<double>{x}, I);
+    double v = 0.0;
+    for (int i = 0; i <= N; ++i) v += I[i] * (gll[i] - req[i]);
+    const double inside = std::fabs(x) < 1.0 - 1.0e-10 ? 1.0 : 0.0;
+    const double sf = 1.0 - (inside * x) * (inside * x);
+    return v / sf + v * (inside - 1.0);
+  };
+  const double pi = 3.14159265358979323846, r3 = std::sqrt(3.0);
+  for (size_t k = 0; k < r.size(); ++k) {
+    const double L1 = 0.5 * (1 + s[k]), L2 = -0.5 * (r[k] + s[k]), L3 = 0.5 * (1 + r[k]);
+    double x = -L2 + L3, y = (-L2 - L3 + 2 * L1) / r3;
+    const double w1 = 4 * L2 * L3 * warp(L3 - L2) * (1 + alpha * alpha * L1 * L1);
+    const double w2 = 4 * L3 * L1 * warp(L1 - L3) * (1 + alpha * alpha * L2 * L2);
+    const double w3 = 4 * L1 * L2 * warp(L2 - L1) * (1 + alpha * alpha * L3 * L3);
+    x += w1 + std::cos(2 * pi / 3) * w2 + std::cos(4 * pi / 3) * w3;
+    y += std::sin(2 * pi / 3) * w2 + std::sin(4 * pi / 3) * w3;
+    const double l1 = (r3 * y + 1) / 3, l2 = (-3 * x - r3 * y + 2) / 6, l3 = (3 * x - r3 * y + 2) / 6;
+    r[k] = -l2 + l3 - l1;
+    s[k] = -l2 - l3 + l1;
+  }
+}
+
+// Reference-element matrices of the triangle: the Vandermonde V (and Vr, Vs)
+// of the orthonormal basis sqrt(2) P_i(a) P_j^(2i+1,0)(b) (1-b)^i of P_N at
+// the nodes, Dr = Vr V^-1, Ds = Vs V^-1, MM = (V V^T)^-1
+// (meshReferenceNodesTri2D.cpp:41-52) and the stiffness matrices
+// Srr = Dr^T MM Dr, Srs = Dr^T MM Ds + Ds^T MM Dr, Sss = Ds^T MM Ds
+// (meshBasisTri2D.cpp:406-430).  The matrices do not depend on the basis of
+// P_N that builds V.  All row-major: X[n*Np + m] maps node m to node n.
+bool tri_basis(int N, TriBasis& b) {
+  const int Np = (N + 1) * (N + 2) / 2;
+  b.N = N;
+  b.Np = Np;
+  tri_nodes(N, b.r, b.s);
+  std::vector<double> V((size_t)Np * Np), Vr(V.size()), Vs(V.size());
+  for (int k = 0; k < Np; ++k) {
+    const double r = b.r[k], s = b.s[k];
+    const double a = s != 1.0 ? 2 * (1 + r) / (1 - s) - 1 : -1.0, bb = s;
+    int col = 0;
+    for (int i = 0; i <= N; ++i)
+      for (int j = 0; i + j <= N; ++j, ++col) {
+        const double fa = jacobi_on(a, 0, 0, i), dfa = jacobi_on_deriv(a, 0, 0, i);
+        const double gb = jacobi_on(bb, 2 * i + 1, 0, j), dgb = jacobi_on_deriv(bb, 2 * i + 1, 0, j);
+        const double h = 0.5 * (1 - bb);
+        const double hm1 = i > 0 ? std::pow(h, i - 1) : 1.0;
+        V[(size_t)k * Np + col] = std::sqrt(2.0) * fa * gb * std::pow(1 - bb, i);
+        const double dr = dfa * gb * hm1;
+        double ds = dfa * gb * 0.5 * (1 + a) * hm1;
+        double t = dgb * std::pow(h, i);
+        if (i > 0) t -= 0.5 * i * gb * hm1;
+        ds += fa * t;
+        Vr[(size_t)k * Np + col] = std::pow(2.0, i + 0.5) * dr;
+        Vs[(size_t)k * Np + col] = std::pow(2.0, i + 0.5) * ds;
+      }
+  }
+  std::vector<double> Vi = V;
+  if (!invert(Np, Vi)) return false;
+  auto mul = [Np](const std::vector<double>& A, const std::vector<double>& B, bool ta) {
+    std::vector<double> C((size_t)Np * Np, 0.0);
+    for (int i = 0; i < Np; ++i)
+      for (int k = 0; k < Np; ++k) {
+        const double aik = ta ? A[(size_t)k * Np + i] : A[(size_t)i * Np + k];
+        if (aik == 0.0) continue;
+        for (int j = 0; j < Np; ++j) C[(size_t)i * Np + j] += aik * B[(size_t)k * Np + j];
+      }
+    return C;
+  };
+  b.Dr = mul(Vr, Vi, false);
+  b.Ds = mul(Vs, Vi, false);
+  std::vector<double> VVt((size_t)Np * Np, 0.0);
+  for (int i = 0; i < Np; ++i)
+    for (int j = 0; j < Np; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < Np; ++k) acc += V[(size_t)i * Np + k] * V[(size_t)j * Np + k];
+      VVt[(size_t)i * Np + j] = acc;
+    }
+  if (!invert(Np, VVt)) return false;
+  b.MM = VVt;
+  const std::vector<double> MDr = mul(b.MM, b.Dr, false), MDs = mul(b.MM, b.Ds, false);
+  const std::vector<double> Srr = mul(b.Dr, MDr, true), Sss = mul(b.Ds, MDs, true);
+  const std::vector<double> Srs1 = mul(b.Dr, MDs, true), Srs2 = mul(b.Ds, MDr, true);
+  b.S.assign((size_t)3 * Np * Np, 0.0);
+  for (size_t k = 0; k < (size_t)Np * Np; ++k) {
+    b.S[k] = Srr[k];
+    b.S[(size_t)Np * Np + k] = Srs1[k] + Srs2[k];
+    b.S[(size_t)2 * Np * Np + k] = Sss[k];
+  }
+  return true;
+}
+
+// Tri2D box (meshSetupBoxTri2D.cpp:78-107): cell (i, j) holds triangles
+// 2(i + j nx) with vertices (i,j), (i+1,j), (i+1,j+1) and 2(i + j nx) + 1 with
+// (i,j), (i+1,j+1), (i,j+1); affine geometric factors per element
+// (wJ = J; ggeo = J (rx^2+ry^2), J (rx sx + ry sy), J (sx^2+sy^2)); the masked
+// numbering: a node's copies are found by topology (vertex, edge position,
+// interior), its global id is its lowest copy (meshConnectNodes.cpp:32-82),
+// the copies on boundary faces (faces 0, 1, 2: s = -1, r + s = 0, r = -1) are
+// masked copy by copy, so a boundary vertex stays live through the elements
+// that touch the boundary only there (meshMaskedGatherScatterSetup.cpp:31-56),
+// rows follow each node's first unmasked copy and each row's columns ascend.
+// Returns false on a non-positive Jacobian.
+bool box_tri(HostMesh& m, const TriBasis& b, std::vector<double>& wJ, std::vector<double>& ggeo) {
+  const int nx = m.nx, ny = m.ny, N = b.N, Np = b.Np, E = m.E;
+  const int64_t NnX = nx + 1;
+  const double dx = 2.0 / nx, dy = 2.0 / ny;
+  std::vector<int64_t> EToV((size_t)E * 3);
+  m.EX.resize((size_t)E * 3);
+  m.EY.resize((size_t)E * 3);
+  m.EZ.clear();
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const int e = 2 * (i + j * nx);
+      const double x0 = -1.0 + dx * i, y0 = -1.0 + dy * j;
+      const int64_t v00 = i + j * NnX, v10 = v00 + 1, v11 = v10 + NnX, v01 = v00 + NnX;
+      const int64_t va[6] = {v00, v10, v11, v00, v11, v01};
+      const double xa[6] = {x0, x0 + dx, x0 + dx, x0, x0 + dx, x0};
+      const double ya[6] = {y0, y0, y0 + dy, y0, y0 + dy, y0 + dy};
+      for (int c = 0; c < 6; ++c) {
+        EToV[(size_t)e * 3 + c] = va[c];
+        m.EX[(size_t)e * 3 + c] = xa[c];
+        m.EY[(size_t)e * 3 + c] = ya[c];
+      }
+    }
+  wJ.resize(E);
+  ggeo.resize((size_t)3 * E);
+  for (int e = 0; e < E; ++e) {
+    const double* X = &m.EX[(size_t)e * 3];
+    const double* Y = &m.EY[(size_t)e * 3];
+    const double xr = 0.5 * (X[1] - X[0]), xs = 0.5 * (X[2] - X[0]);
+    const double yr = 0.5 * (Y[1] - Y[0]), ys = 0.5 * (Y[2] - Y[0]);
+    const double J = xr * ys - xs * yr;
+    if (!(J > 0.0)) return false;
+    const double rx = ys / J, ry = -xs / J, sx = -yr / J, sy = xr / J;
+    wJ[e] = J;
+    ggeo[(size_t)3 * e + 0] = J * (rx * rx + ry * ry);
+    ggeo[(size_t)3 * e + 1] = J * (rx * sx + ry * sy);
+    ggeo[(size_t)3 * e + 2] = J * (sx * sx + sy * sy);
+  }
+  // node roles in the reference element: vertex v (0..2), or edge f (0..2)
+  // at position k from the edge's first vertex, or interior
+  const double tol = 1.0e-5;
+  std::vector<int> vert(Np, -1), edge(Np, -1), epos(Np, 0);
+  static const int fv[3][2] = {{0, 1}, {1, 2}, {0, 2}};   // faces s=-1, r+s=0, r=-1, oriented by local index
+  std::vector<std::vector<int>> fn(3);
+  for (int n = 0; n < Np; ++n) {
+    const bool on[3] = {std::fabs(b.s[n] + 1) < tol, std::fabs(b.r[n] + b.s[n]) < tol, std::fabs(b.r[n] + 1) < tol};
+    for (int f = 0; f < 3; ++f)
+      if (on[f]) fn[f].push_back(n);
+    if (on[0] && on[2]) vert[n] = 0;
+    else if (on[0] && on[1]) vert[n] = 1;
+    else if (on[1] && on[2]) vert[n] = 2;
+  }
+  for (int f = 0; f < 3; ++f)
+    for (size_t k = 0; k < fn[f].size(); ++k)
+      if (vert[fn[f][k]] < 0) {
+        edge[fn[f][k]] = f;
+        epos[fn[f][k]] = (int)k;   // 1..N-1 from the face's first vertex (local index order)
+      }
+  // key of each copy: vertex id, or (edge's vertex pair, position from its lower vertex), or the copy itself
+  const int64_t NV = (int64_t)(nx + 1) * (ny + 1);
+  const int64_t NL = (int64_t)E * Np;
+  std::vector<int64_t> key((size_t)NL);
+  std::unordered_map<int64_t, int64_t> edge_key;   // undirected vertex pair -> base key
+  int64_t next = NV;
+  for (int e = 0; e < E; ++e)
+    for (int n = 0; n < Np; ++n) {
+      const int64_t l = (int64_t)e * Np + n;
+      if (vert[n] >= 0) {
+        key[(size_t)l] = EToV[(size_t)e * 3 + vert[n]];
+      } else if (edge[n] >= 0) {
+        int64_t a = EToV[(size_t)e * 3 + fv[edge[n]][0]], c = EToV[(size_t)e * 3 + fv[edge[n]][1]];
+        int k = epos[n];
+        if (a > c) {
+          std::swap(a, c);
+          k = N - k;
+        }
+        const int64_t pair = a * NV + c;
+        auto it = edge_key.find(pair);
+        if (it == edge_key.end()) it = edge_key.emplace(pair, (next += N) - N).first;
+        key[(size_t)l] = it->second + k;
+      } else {
+        key[(size_t)l] = -1 - l;   // interior: its own class
+      }
+    }
+  // copies on boundary faces are masked
+  std::vector<char> masked((size_t)NL, 0);
+  for (int e = 0; e < E; ++e) {
+    const double* X = &m.EX[(size_t)e * 3];
+    const double* Y = &m.EY[(size_t)e * 3];
+    for (int f = 0; f < 3; ++f) {
+      const int a = fv[f][0], c = fv[f][1];
+      auto at = [](double v, double w) { return std::fabs(v - w) < 1.0e-12; };
+      const bool bnd = (at(X[a], -1.0) && at(X[c], -1.0)) || (at(X[a], 1.0) && at(X[c], 1.0)) ||
+                       (at(Y[a], -1.0) && at(Y[c], -1.0)) || (at(Y[a], 1.0) && at(Y[c], 1.0));
+      if (bnd)
+        for (int n : fn[f]) masked[(size_t)e * Np + n] = 1;
+    }
+  }
+  std::unordered_map<int64_t, int32_t> row;
+  m.G2L.assign((size_t)NL, -1);
+  std::vector<int32_t> count;
+  for (int64_t l = 0; l < NL; ++l) {
+    if (masked[(size_t)l]) continue;
+    auto it = row.find(key[(size_t)l]);
+    if (it == row.end()) {
+      it = row.emplace(key[(size_t)l], (int32_t)count.size()).first;
+      count.push_back(0);
+    }
+    m.G2L[(size_t)l] = it->second;
+    ++count[it->second];
+  }
+  m.Ngather = (int32_t)count.size();
+  m.rowStarts.assign((size_t)m.Ngather + 1, 0);
+  for (int32_t r = 0; r < m.Ngather; ++r) m.rowStarts[r + 1] = m.rowStarts[r] + count[r];
+  m.nnz = m.rowStarts[m.Ngather];
+  m.colIds.assign((size_t)m.nnz, 0);
+  std::vector<int32_t> fill(m.rowStarts.begin(), m.rowStarts.end() - 1);
+  for (int64_t l = 0; l < NL; ++l)
+    if (m.G2L[(size_t)l] >= 0) m.colIds[(size_t)fill[m.G2L[(size_t)l]]++] = (int32_t)l;
+  return true;
+}
+
 // GeometricFactorsQuad2D (meshGeometricFactorsQuad2D.cpp:31-120) from the
 // bilinear map of the vertices at the GLL nodes (meshPhysicalNodesQuad2D.cpp)
 bool quad_geometry(const HostMesh& m, std::vector<double>& wJ, std::vector<double>& ggeo) {
@@ -504,6 +776,16 @@ int host_mesh_from_desc(const bp_box_desc_t* d, bp::HostMesh& m) {
   if (!d) return bp::fail(BP_ERROR_ARG, "null descriptor");
   if (d->dim != 0 && d->dim != 2 && d->dim != 3) return bp::fail(BP_ERROR_ARG, "box dim must be 2 or 3");
   m.dim = d->dim == 2 ? 2 : 3;
+  if (d->simplex) {
+    if (m.dim != 2 || d->nx < 1 || d->ny < 1 || d->N < 1 || d->N > 15 || d->Nfields != 1)
+      return bp::fail(BP_ERROR_ARG, "bad Tri2D box descriptor");
+    m.N = d->N; m.Nq = d->N + 1; m.Np = (d->N + 1) * (d->N + 2) / 2;
+    m.nx = d->nx; m.ny = d->ny; m.nz = 1;
+    const int64_t E = 2 * (int64_t)d->nx * d->ny;
+    if (E * m.Np >= (int64_t)INT32_MAX) return bp::fail(BP_ERROR_ARG, "local node count exceeds int32");
+    m.E = (int)E; m.affine = 1; m.Nfields = 1;
+    return BP_SUCCESS;
+  }
   const int nz = m.dim == 2 ? 1 : d->nz;
   if (d->nx < 1 || d->ny < 1 || nz < 1 || d->N < 1 || d->N > 15 ||
       (m.dim == 3 && d->Nfields != 1 && d->Nfields != 3) || (m.dim == 2 && d->Nfields != 1 && d->Nfields != 2))
@@ -522,8 +804,16 @@ extern "C" int bp_box_numbering(const bp_box_desc_t* d, int32_t* Ngather, int32_
   bp::HostMesh m;
   int rc = host_mesh_from_desc(d, m);
   if (rc) return rc;
-  if (m.dim == 2) bp::box_numbering_2d(m);
-  else bp::box_numbering(m);
+  if (d->simplex) {
+    bp::TriBasis tb;
+    std::vector<double> wJ, ggeo;
+    if (!bp::tri_basis(m.N, tb) || !bp::box_tri(m, tb, wJ, ggeo))
+      return bp::fail(BP_ERROR_NUMERIC, "bp_box_numbering: Tri2D set-up failed");
+  } else if (m.dim == 2) {
+    bp::box_numbering_2d(m);
+  } else {
+    bp::box_numbering(m);
+  }
   if (Ngather) *Ngather = m.Ngather;
   if (nnz) *nnz = m.nnz;
   if (G2L) std::copy(m.G2L.begin(), m.G2L.end(), G2L);
@@ -540,6 +830,31 @@ extern "C" int bp_basis_gll(int32_t N, double* z, double* w, double* D) {
   if (z) std::copy(zz.begin(), zz.end(), z);
   if (w) std::copy(ww.begin(), ww.end(), w);
   if (D) std::copy(DD.begin(), DD.end(), D);
+  return BP_SUCCESS;
+}
+
+extern "C" int bp_basis_tri2d(int32_t N, double* r, double* s, double* D, double* MM, double* S) {
+  if (N < 1 || N > 15) return bp::fail(BP_ERROR_ARG, "bp_basis_tri2d: degree must be in 1..15");
+  bp::TriBasis tb;
+  if (!bp::tri_basis(N, tb)) return bp::fail(BP_ERROR_NUMERIC, "bp_basis_tri2d: singular Vandermonde matrix");
+  const int Np = tb.Np;
+  const size_t NP2 = (size_t)Np * Np;
+  auto put = [&](const std::vector<double>& rm, double* out, size_t off) {   // node-fastest
+    for (int n = 0; n < Np; ++n)
+      for (int k = 0; k < Np; ++k) out[off + (size_t)k * Np + n] = rm[(size_t)n * Np + k];
+  };
+  if (r) std::copy(tb.r.begin(), tb.r.end(), r);
+  if (s) std::copy(tb.s.begin(), tb.s.end(), s);
+  if (D) {
+    put(tb.Dr, D, 0);
+    put(tb.Ds, D, NP2);
+  }
+  if (MM) std::copy(tb.MM.begin(), tb.MM.end(), MM);
+  if (S)
+    for (int b = 0; b < 3; ++b) {
+      const std::vector<double> blk(tb.S.begin() + b * NP2, tb.S.begin() + (b + 1) * NP2);
+      put(blk, S, b * NP2);
+    }
   return BP_SUCCESS;
 }
 

@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstring>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "bp_cg_device.cuh"
@@ -641,6 +642,7 @@ struct ElemOperands {
 
 static ElemOperands<double> operands64(const bp_solver_s* S) {
   const bp_mesh_s* m = S->mesh;
+  if (m->simplex) return {m->wJ.ptr, m->ggeo.ptr, nullptr, m->S.ptr, m->MM.ptr};   // Tri2D: S and MM
   if (S->bp >= 5) return {m->wJ.ptr, m->ggeo.ptr, m->gllw.ptr, m->D.ptr, nullptr};
   const double* D = m->affine ? m->cubDmodal.ptr : m->cubD.ptr;
   const double* T = !m->affine ? m->cubInterp.ptr : (S->bp >= 3 ? m->invV.ptr : m->MM.ptr);
@@ -683,6 +685,13 @@ template <class V>
 static int elem_apply(bp_solver_s* S, const ElemOperands<V>& o, const V* q, V* AqL, const int* skip, cudaStream_t s,
                       const CgFuse* fuse = nullptr, int* nblocks = nullptr) {
   bp_mesh_s* m = S->mesh;
+  if (m->simplex) {   // Tri2D, FP64 only (the solver rejects mixed precision on it)
+    if constexpr (std::is_same<V, double>::value)
+      return launch_ax_tri(m->N, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, o.T, S->lambda, q, AqL,
+                           skip, s, fuse ? fuse->partials : nullptr, nblocks);
+    else
+      return fail(BP_ERROR_ARG, "Tri2D operator: FP64 only");
+  }
   if (S->bp >= 5)
     return launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D, (V)S->lambda, q,
                           AqL, skip, s, fuse, nblocks);
@@ -1009,7 +1018,11 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
   if (!mesh || !d || !out) return fail(BP_ERROR_ARG, "bp_solver_create: null pointer");
   *out = nullptr;
   if (d->bp < 1 || d->bp > 6) return fail(BP_ERROR_ARG, "bp_solver_create: bp must be 1..6");
-  if (mesh->dim == 2) {
+  if (mesh->simplex) {
+    if (d->bp != 5) return fail(BP_ERROR_ARG, "bp_solver_create: Tri2D meshes take BP5");
+    if (d->precision != BP_PRECISION_FP64)
+      return fail(BP_ERROR_ARG, "bp_solver_create: Tri2D solves are FP64 (no mixed-precision operator)");
+  } else if (mesh->dim == 2) {
     if (d->bp < 5) return fail(BP_ERROR_ARG, "bp_solver_create: Quad2D meshes take BP5 and BP6 (the BP1-BP4 forms are Hex3D only)");
     if ((d->bp == 6) != (mesh->Nfields == 2))
       return fail(BP_ERROR_ARG, "bp_solver_create: Quad2D BP6 needs a 2-field mesh, BP5 a 1-field mesh");
@@ -1108,6 +1121,7 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
   if (mode == BP_RHS_ANALYTIC) {
     // BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
     const double lam = S->bp <= 2 ? 0.0 : S->lambda;
+    if (m->simplex) return fail(BP_ERROR_ARG, "bp_solver_rhs: Tri2D meshes take the seeded forcing (BP_RHS_RANDOM)");
     if (m->dim == 2)
       BP_TRY(launch_rhs_analytic_quad(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->gllz.ptr,
                                       m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
@@ -1122,7 +1136,9 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
       f = ftmp.ptr;
     }
     BP_TRY(launch_rhs_random(S->N, seed, f, s));
-    if (m->dim == 2)
+    if (m->simplex)
+      BP_TRY(launch_mass_local_tri(m->N, m->E, m->G2L.ptr, m->wJ.ptr, m->MM.ptr, f, S->AqL.ptr, s));
+    else if (m->dim == 2)
       BP_TRY(launch_mass_local_quad(m->N, m->affine, m->Nfields, m->E, m->G2L.ptr, m->gllw.ptr, m->wJ.ptr, f,
                                     S->AqL.ptr, s));
     else
@@ -1143,7 +1159,9 @@ int bp_solver_diagonal(bp_solver_t S, double* diag) {
   if (!S || !diag) return fail(BP_ERROR_ARG, "bp_solver_diagonal: null pointer");
   bp_mesh_s* m = S->mesh;
   cudaStream_t s = default_stream();
-  if (S->bp >= 5 && m->dim == 2) {
+  if (m->simplex) {
+    BP_TRY(launch_diag_local_tri(m->N, m->E, m->wJ.ptr, m->ggeo.ptr, m->S.ptr, m->MM.ptr, S->lambda, S->AqL.ptr, s));
+  } else if (S->bp >= 5 && m->dim == 2) {
     BP_TRY(launch_diag_local_quad(m->N, m->affine, m->Nfields, m->E, m->ggeo.ptr, m->wJ.ptr, m->gllw.ptr, m->D.ptr,
                                   S->lambda, S->AqL.ptr, s));
   } else if (S->bp >= 5) {

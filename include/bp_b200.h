@@ -103,6 +103,16 @@ int bp_ax_hex3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                 const double* gllw, const double* D, double lambda, const double* q,
                 double* Aq, bp_stream_t stream);
 
+/* Tri2D affine stiffness + lambda*mass operator, Aq[e] = A_e q[GlobalToLocal]
+   with A_e = G00 Srr + G01 Srs + G11 Sss + lambda J MM.  Replaces
+   bp5AxAffineTri2D (okl/bp5AxAffineTri2D.okl:27-89); argument order follows its
+   signature minus the unused vgeo, gllw and D.  desc: bp 5, N 1..15, affine 1,
+   Nfields 1, dim 2.  wJ [E] (J), ggeo [E*3] (G00, G01, G11), S [3*Np*Np] and
+   MM [Np*Np] as in bp_mesh_view_t (node-fastest); Aq [E*Np]. */
+int bp_ax_tri2d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                const int32_t* GlobalToLocal, const double* wJ, const double* ggeo, const double* S,
+                const double* MM, double lambda, const double* q, double* Aq, bp_stream_t stream);
+
 /* The same operator in FP32 (the inner operator of the mixed-precision CG):
    all arrays FP32, dot products of the CG stay FP64.  No counterpart in the
    reference (dfloat is FP64 there, include/types.h:31-39). */
@@ -261,6 +271,9 @@ typedef struct bp_box_desc {
   int32_t dim;          /* 0 or 3: Hex3D box nx x ny x nz (-e Hex); 2: Quad2D box
                            nx x ny (-e Quad, meshSetupBoxQuad2D.cpp:30-100; nz
                            ignored; Nfields 1 or 2)                                */
+  int32_t simplex;      /* 1 with dim 2: Tri2D box (-e Tri, meshSetupBoxTri2D.cpp:
+                           30-107): two triangles per cell, affine, one field, no
+                           perturbation; 0 otherwise                              */
 } bp_box_desc_t;
 
 typedef struct bp_mesh_view {
@@ -283,6 +296,13 @@ typedef struct bp_mesh_view {
   const double* EZ;               /* NULL for Quad2D                              */
   int32_t dim;                    /* 3, or 2 for Quad2D: Np = Nq^2, ggeo [E*Np*3]
                                      (affine [E*3]), G00, G01, G11               */
+  int32_t simplex;                /* 1: Tri2D: Np = (N+1)(N+2)/2, affine: wJ [E],
+                                     ggeo [E*3] G00, G01, G11; EX, EY [E*3];
+                                     D [2*Np*Np] Dr, Ds; gllz, gllw NULL        */
+  const double* S;                /* Tri2D: Srr, Srs, Sss [3*Np*Np]; X[k*Np + n] is
+                                     the weight of node k in output n (the layout
+                                     of the reference's o_S, o_D); else NULL    */
+  const double* MM;               /* Tri2D: mass matrix [Np*Np] (symmetric)       */
 } bp_mesh_view_t;
 
 int bp_mesh_create(const bp_box_desc_t* desc, bp_mesh_t* mesh);
@@ -317,6 +337,12 @@ typedef struct bp_cubature_view {
    (7*8*E*cubNp bytes of device memory). */
 int bp_mesh_cubature(bp_mesh_t mesh);
 int bp_mesh_cubature_view(bp_mesh_t mesh, bp_cubature_view_t* view);
+
+/* Host-only Tri2D reference element of degree N (meshReferenceNodesTri2D.cpp:
+   31-52, meshBasisTri2D.cpp): warp & blend nodes r, s [Np]; D [2*Np*Np] (Dr, Ds),
+   MM [Np*Np], S [3*Np*Np] (Srr, Srs, Sss), node-fastest as in bp_mesh_view_t.
+   Np = (N+1)(N+2)/2; any pointer may be NULL. */
+int bp_basis_tri2d(int32_t N, double* r, double* s, double* D, double* MM, double* S);
 
 /* Host-only 1D cubature data for degree N (meshCubatureSetupHex3D.cpp:31-51,
    meshBasis1D.cpp JacobiGQ / InterpolationMatrix1D / Dmatrix1D / MassMatrix1D):

@@ -122,6 +122,7 @@ int main(int argc, char** argv) {
     put("gllw", mesh.gllw);
     put("D", mesh.D);
     put("MM", mesh.MM);
+    if (mesh.S.length()) put("S", mesh.S);   // Tri2D: Srr, Srs, Sss
     put("x", mesh.x);
     put("y", mesh.y);
     put("z", mesh.z);
