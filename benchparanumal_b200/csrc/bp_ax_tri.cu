@@ -136,7 +136,43 @@ __global__ void tri_diag_local_kernel(int Nelements, int Np, const double* __res
   }
 }
 
+// rhsAffineTri2D (okl/rhsTri2D.okl): b_e = MM (J_e f) with
+// f = (2 pi^2 + lambda) sin(pi x) sin(pi y) at every node of the element
+__global__ void __launch_bounds__(kTriThreads + 32)
+tri_rhs_analytic_kernel(int Nelements, int Np, int epb, const double* __restrict__ wJ,
+                        const double* __restrict__ MM, const double* __restrict__ x, const double* __restrict__ y,
+                        double lambda, double* __restrict__ bL) {
+  extern __shared__ __align__(16) double s_f[];
+  const double pi = 3.14159265358979323846;
+  const int t = threadIdx.x;
+  const int es = t / Np, n = t - es * Np;
+  const int e = blockIdx.x * epb + es;
+  const bool active = es < epb && e < Nelements;
+  if (active) {
+    const size_t id = (size_t)e * Np + n;
+    s_f[es * Np + n] = wJ[e] * ((2 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]));
+  }
+  __syncthreads();
+  if (!active) return;
+  double acc = 0.0;
+  for (int m = 0; m < Np; ++m) acc += __ldg(MM + (size_t)m * Np + n) * s_f[es * Np + m];
+  bL[(size_t)e * Np + n] = acc;
+}
+
 }  // namespace
+
+int launch_rhs_analytic_tri(int N, int32_t Nelements, const double* wJ, const double* MM, const double* x,
+                            const double* y, double lambda, double* bL, cudaStream_t s) {
+  if (Nelements == 0) return BP_SUCCESS;
+  const int Np = (N + 1) * (N + 2) / 2;
+  int epb = 0, threads = 0;
+  tri_shape(Np, &epb, &threads);
+  const int grid = (Nelements + epb - 1) / epb;
+  tri_rhs_analytic_kernel<<<grid, threads, sizeof(double) * epb * Np, s>>>(Nelements, Np, epb, wJ, MM, x, y, lambda,
+                                                                          bL);
+  BP_CUDA_TRY(cudaGetLastError());
+  return BP_SUCCESS;
+}
 
 int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
                   const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,

@@ -640,6 +640,8 @@ static int mesh_create_tri(const bp_box_desc_t* d, bp_mesh_t* out) {
     return fail(BP_ERROR_NUMERIC, "bp_mesh_create: non-positive Jacobian found");
   std::vector<double> D(tb.Dr);
   D.insert(D.end(), tb.Ds.begin(), tb.Ds.end());
+  std::vector<double> xn, yn;
+  tri_nodes_xy(hm, tb, xn, yn);
   bp_mesh_s* m = new bp_mesh_s();
   m->dim = 2;
   m->simplex = 1;
@@ -656,6 +658,8 @@ static int mesh_create_tri(const bp_box_desc_t* d, bp_mesh_t* out) {
     if ((rc = m->D.upload(node_fastest(D, Np), s))) break;
     if ((rc = m->S.upload(node_fastest(tb.S, Np), s))) break;
     if ((rc = m->MM.upload(tb.MM, s))) break;   // symmetric
+    if ((rc = m->x.upload(xn, s))) break;
+    if ((rc = m->y.upload(yn, s))) break;
     if ((rc = m->EX.upload(hm.EX, s))) break;
     if ((rc = m->EY.upload(hm.EY, s))) break;
     if ((rc = m->wJ.upload(wJ, s))) break;

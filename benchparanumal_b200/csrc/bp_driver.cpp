@@ -201,9 +201,8 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
     throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex, Quad and Tri only");
   if (quad && bp <= 4)
     throw std::runtime_error("ELEMENT TYPE Quad is available for BK5/BK6 and BP5/BP6 (BP1-BP4: Hex only)");
-  if (tri && (bp != 5 || !S.compare("AFFINE MESH", "TRUE") || S.compare("PRECISION", "MIXED") ||
-              !S.compare("FORCING", "RANDOM")))
-    throw std::runtime_error("ELEMENT TYPE Tri is available for BK5 and BP5 with -a, FP64 and -f RANDOM");
+  if (tri && (bp != 5 || !S.compare("AFFINE MESH", "TRUE") || S.compare("PRECISION", "MIXED")))
+    throw std::runtime_error("ELEMENT TYPE Tri is available for BK5 and BP5 with -a, in FP64");
   check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
   bp_box_desc_t d{};
   d.dim = quad || tri ? 2 : 3;

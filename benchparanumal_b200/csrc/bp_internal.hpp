@@ -198,6 +198,8 @@ struct TriBasis {
 };
 bool tri_basis(int N, TriBasis& b);
 bool box_tri(HostMesh& m, const TriBasis& b, std::vector<double>& wJ, std::vector<double>& ggeo);
+// physical node coordinates of the Tri2D box [E*Np] each (meshPhysicalNodesTri2D.cpp)
+void tri_nodes_xy(const HostMesh& m, const TriBasis& b, std::vector<double>& x, std::vector<double>& y);
 
 // trilinear map of the eight hex vertices v (mesh_t vertex order) at (r,s,t)
 __host__ __device__ inline double trilinear(const double* v, double r, double s, double t) {
@@ -229,6 +231,7 @@ struct bp_mesh_s {
   // Tri2D: Srr, Srs, Sss [3*Np*Np] node-fastest (X[k*Np + n] weighs node k in
   // output n); MM above holds the triangle mass matrix and D [2*Np*Np] Dr, Ds
   bp::DeviceArray<double> S;
+  bp::DeviceArray<double> x, y;                 // Tri2D: physical node coordinates [E*Np]
   // factors at the quadrature points: curved [E*cubNp], [6*E*cubNp]; affine the
   // per-element wJ and ggeo
   const double* cubwJ() const { return affine ? wJ.ptr : cubwJ_c.ptr; }
@@ -253,6 +256,8 @@ int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const do
                           const double* f, double* bL, cudaStream_t s);
 int launch_diag_local_tri(int N, int32_t Nelements, const double* wJ, const double* ggeo, const double* S,
                           const double* MM, double lambda, double* dL, cudaStream_t s);
+int launch_rhs_analytic_tri(int N, int32_t Nelements, const double* wJ, const double* MM, const double* x,
+                            const double* y, double lambda, double* bL, cudaStream_t s);
 }  // namespace bp
 
 // ---- kernel launchers (bp_kernels.cu) ----

@@ -705,6 +705,23 @@ bool box_tri(HostMesh& m, const TriBasis& b, std::vector<double>& wJ, std::vecto
   return true;
 }
 
+// the affine map of each triangle's vertices at the reference nodes
+// (meshPhysicalNodesTri2D.cpp): x = -(r+s)/2 x1 + (1+r)/2 x2 + (1+s)/2 x3
+void tri_nodes_xy(const HostMesh& m, const TriBasis& b, std::vector<double>& x, std::vector<double>& y) {
+  const int Np = b.Np;
+  x.resize((size_t)m.E * Np);
+  y.resize((size_t)m.E * Np);
+  for (int e = 0; e < m.E; ++e) {
+    const double* X = &m.EX[(size_t)e * 3];
+    const double* Y = &m.EY[(size_t)e * 3];
+    for (int n = 0; n < Np; ++n) {
+      const double r = b.r[n], s = b.s[n];
+      x[(size_t)e * Np + n] = -0.5 * (r + s) * X[0] + 0.5 * (1 + r) * X[1] + 0.5 * (1 + s) * X[2];
+      y[(size_t)e * Np + n] = -0.5 * (r + s) * Y[0] + 0.5 * (1 + r) * Y[1] + 0.5 * (1 + s) * Y[2];
+    }
+  }
+}
+
 // GeometricFactorsQuad2D (meshGeometricFactorsQuad2D.cpp:31-120) from the
 // bilinear map of the vertices at the GLL nodes (meshPhysicalNodesQuad2D.cpp)
 bool quad_geometry(const HostMesh& m, std::vector<double>& wJ, std::vector<double>& ggeo) {

@@ -1121,8 +1121,9 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
   if (mode == BP_RHS_ANALYTIC) {
     // BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
     const double lam = S->bp <= 2 ? 0.0 : S->lambda;
-    if (m->simplex) return fail(BP_ERROR_ARG, "bp_solver_rhs: Tri2D meshes take the seeded forcing (BP_RHS_RANDOM)");
-    if (m->dim == 2)
+    if (m->simplex)
+      BP_TRY(launch_rhs_analytic_tri(m->N, m->E, m->wJ.ptr, m->MM.ptr, m->x.ptr, m->y.ptr, lam, S->AqL.ptr, s));
+    else if (m->dim == 2)
       BP_TRY(launch_rhs_analytic_quad(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->gllz.ptr,
                                       m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
     else

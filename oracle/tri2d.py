@@ -27,7 +27,8 @@ What it restates (reference files, paths relative to the reference root):
                local columns ascending (ogsSetup.cpp)
   operator     AqL_e = G00 Srr q_e + G01 Srs q_e + G11 Sss q_e + lambda J MM q_e
                (okl/bp5AxAffineTri2D.okl:27-89)
-  forcing      b = Gather(J MM f_e) of a seeded nodal f = 2u - 1
+  forcing      b = Gather(J MM f_e) of a seeded nodal f = 2u - 1, or the
+               analytic forcing of okl/rhsTri2D.okl (rhsAffineTri2D)
   CG           the reference's cg::Solve with optional Jacobi (as the Hex3D oracle)
 
 Parity pin: tests/golden/ref_tri_*.npz, written by the reference's own set-up
@@ -264,6 +265,13 @@ class Mesh:
         fL = self.scatter(f).reshape(self.E, self.Np)
         bL = (self.wJ[:, None] * (fL @ self.MM.T)).ravel()
         return f, self.gather(bL)
+
+    def rhs_analytic(self, lam=1.0):
+        """rhsAffineTri2D (okl/rhsTri2D.okl): Gather(MM (J f)) with
+        f = (2 pi^2 + lambda) sin(pi x) sin(pi y) at every node."""
+        f = (2 * np.pi ** 2 + lam) * np.sin(np.pi * self.x) * np.sin(np.pi * self.y)
+        bL = (self.wJ[:, None] * f) @ self.MM.T
+        return self.gather(bL.ravel())
 
     def jacobi_diag(self, lam=1.0):
         d = (self.ggeo[:, 0:1] * np.diag(self.Srr)[None, :] + self.ggeo[:, 1:2] * np.diag(self.Srs)[None, :]

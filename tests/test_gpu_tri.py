@@ -82,6 +82,7 @@ def test_forcing_and_diagonal_match_oracle(gpu, tri, nx, ny, N):
     om = tri.Mesh(nx, ny, N)
     gm = _mesh(gpu, nx, ny, N)
     S = gpu.BP(gm, precon="JACOBI")
+    assert _rel(S.rhs("ANALYTIC").download(), om.rhs_analytic(1.0)) < 1e-13
     f = gpu.DeviceBuffer(om.Ngather)
     b = S.rhs("RANDOM", 3, f=f)
     f_o, b_o = om.rhs_random(3)
@@ -125,7 +126,7 @@ def test_driver_result_line(gpu, capfd):
     out = capfd.readouterr().out
     line = [l for l in out.splitlines() if l.startswith("BP5: N=")][0]
     assert "iterations=50," in line and line.rstrip().endswith("Element=Tri, Affine")
-    assert gpu.driver_main("BK5", ["-e", "Tri", "-nx", "8", "-ny", "6", "-p", "7", "-a", "-f", "RANDOM"]) == 0
+    assert gpu.driver_main("BK5", ["-e", "Tri", "-nx", "8", "-ny", "6", "-p", "7", "-a"]) == 0   # analytic forcing
     out = capfd.readouterr().out
     assert any(l.startswith("BK5: N= 7,") and "Element=Tri, Affine" in l for l in out.splitlines())
 
@@ -136,9 +137,7 @@ def test_rejections(gpu):
         gpu.BP(gm, precision="MIXED")     # no FP32 triangle operator
     with pytest.raises(gpu.BPError):
         gpu.BP(gm, bp=6)
-    S = gpu.BP(gm)
-    with pytest.raises(gpu.BPError):
-        S.rhs("ANALYTIC")                 # seeded forcing only
     with pytest.raises(gpu.BPError):
         gpu.Mesh(3, 3, N=4, affine=False, dim=2, simplex=True)
-    assert gpu.driver_main("BP5", ["-e", "Tri", "-nx", "4", "-ny", "4"]) != 0   # needs -a and -f RANDOM
+    assert gpu.driver_main("BP5", ["-e", "Tri", "-nx", "4", "-ny", "4"]) != 0   # needs -a
+    assert gpu.driver_main("BP5", ["-e", "Tri", "-nx", "4", "-ny", "4", "-a", "-fp", "MIXED", "-tol", "1e-8"]) != 0
