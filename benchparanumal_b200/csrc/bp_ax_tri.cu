@@ -39,23 +39,24 @@ static void tri_shape(int Np, int* epb, int* threads) {
 // 43.4 ms (132 registers in the CG form with the p.Ap sum).
 constexpr int kTriElems = 4;
 
-template <bool DOT>
+template <class F, bool DOT>
 __global__ void __launch_bounds__(kTriThreads + 32)
 ax_tri_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ elementList,
-              const int32_t* __restrict__ G2L, const double* __restrict__ wJ, const double* __restrict__ ggeo,
-              const double* __restrict__ S, const double* __restrict__ MM, double lambda,
-              const double* __restrict__ q, double* __restrict__ Aq, const int* __restrict__ skip,
-              double* __restrict__ partials) {
+              const int32_t* __restrict__ G2L, const F* __restrict__ wJ, const F* __restrict__ ggeo,
+              const F* __restrict__ S, const F* __restrict__ MM, F lambda, const F* __restrict__ q,
+              F* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
   pdl_wait();
   pdl_release();
   if (skip && *skip) return;
-  extern __shared__ __align__(16) double s_q[];   // [groups*kTriElems][Np]; the block sum reuses it
+  // [groups*kTriElems][Np] values; the block sum reuses it (sized for doubles)
+  extern __shared__ __align__(16) double s_raw[];
+  F* const s_q = reinterpret_cast<F*>(s_raw);
   const int t = threadIdx.x;
   const int slots = groups * kTriElems;
   const int e0 = blockIdx.x * slots;
   for (int i = t; i < slots * Np; i += blockDim.x) {
     const int j = i / Np, m = i - j * Np;
-    double v = 0.0;
+    F v = 0;
     if (e0 + j < Nelements) {
       const int32_t id = G2L[(size_t)elementList[e0 + j] * Np + m];
       if (id >= 0) v = q[id];
@@ -66,17 +67,17 @@ ax_tri_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ ele
   const int g = t / Np, n = t - g * Np;
   double pdot = 0.0;
   if (g < groups) {
-    const double* sq = s_q + (size_t)g * kTriElems * Np;
+    const F* sq = s_q + (size_t)g * kTriElems * Np;
     const size_t NP2 = (size_t)Np * Np;
-    double qrr[kTriElems], qrs[kTriElems], qss[kTriElems], qM[kTriElems];
+    F qrr[kTriElems], qrs[kTriElems], qss[kTriElems], qM[kTriElems];
 #pragma unroll
-    for (int j = 0; j < kTriElems; ++j) qrr[j] = qrs[j] = qss[j] = qM[j] = 0.0;
+    for (int j = 0; j < kTriElems; ++j) qrr[j] = qrs[j] = qss[j] = qM[j] = 0;
     for (int k = 0; k < Np; ++k) {
       const size_t o = (size_t)k * Np + n;
-      const double a = __ldg(S + o), b = __ldg(S + NP2 + o), c = __ldg(S + 2 * NP2 + o), d = __ldg(MM + o);
+      const F a = __ldg(S + o), b = __ldg(S + NP2 + o), c = __ldg(S + 2 * NP2 + o), d = __ldg(MM + o);
 #pragma unroll
       for (int j = 0; j < kTriElems; ++j) {
-        const double qk = sq[j * Np + k];
+        const F qk = sq[j * Np + k];
         qrr[j] += a * qk;
         qrs[j] += b * qk;
         qss[j] += c * qk;
@@ -88,15 +89,15 @@ ax_tri_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ ele
       const int eidx = e0 + g * kTriElems + j;
       if (eidx < Nelements) {
         const int element = elementList[eidx];
-        const double* gg = ggeo + 3 * (size_t)element;
-        const double out = gg[0] * qrr[j] + gg[1] * qrs[j] + gg[2] * qss[j] + wJ[element] * lambda * qM[j];
+        const F* gg = ggeo + 3 * (size_t)element;
+        const F out = gg[0] * qrr[j] + gg[1] * qrs[j] + gg[2] * qss[j] + wJ[element] * lambda * qM[j];
         Aq[(size_t)element * Np + n] = out;
-        if (DOT) pdot += sq[j * Np + n] * out;
+        if (DOT) pdot += (double)sq[j * Np + n] * (double)out;
       }
     }
   }
   if (DOT) {
-    const double bs = fuse_block_sum(pdot, s_q);
+    const double bs = fuse_block_sum(pdot, s_raw);
     if (t == 0) partials[blockIdx.x] = bs;
   }
 }
@@ -174,9 +175,10 @@ int launch_rhs_analytic_tri(int N, int32_t Nelements, const double* wJ, const do
   return BP_SUCCESS;
 }
 
-int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
-                  const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,
-                  const int* skip, cudaStream_t s, double* partials, int* nblocks) {
+template <class F>
+static int launch_ax_tri_t(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ,
+                           const F* ggeo, const F* S, const F* MM, F lambda, const F* q, F* Aq, const int* skip,
+                           cudaStream_t s, double* partials, int* nblocks) {
   if (nblocks) *nblocks = 0;
   if (N < 1 || N > 15) return fail(BP_ERROR_ARG, "Tri2D operator: degree N must be in 1..15");
   if (Nelements == 0) return BP_SUCCESS;
@@ -188,12 +190,26 @@ int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const in
   if (nblocks) *nblocks = grid;
   const size_t smem = sizeof(double) * (size_t)(slots * Np > threads ? slots * Np : threads);
   if (partials)
-    BP_CUDA_TRY(launch_pdl(ax_tri_kernel<true>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList, G2L,
-                           wJ, ggeo, S, MM, lambda, q, Aq, skip, partials));
+    BP_CUDA_TRY(launch_pdl(ax_tri_kernel<F, true>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
+                           G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, partials));
   else
-    BP_CUDA_TRY(launch_pdl(ax_tri_kernel<false>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
+    BP_CUDA_TRY(launch_pdl(ax_tri_kernel<F, false>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
                            G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, (double*)nullptr));
   return BP_SUCCESS;
+}
+
+int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
+                  const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,
+                  const int* skip, cudaStream_t s, double* partials, int* nblocks) {
+  return launch_ax_tri_t<double>(N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s, partials,
+                                 nblocks);
+}
+
+int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const float* wJ,
+                  const float* ggeo, const float* S, const float* MM, float lambda, const float* q, float* Aq,
+                  const int* skip, cudaStream_t s, double* partials, int* nblocks) {
+  return launch_ax_tri_t<float>(N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s, partials,
+                                nblocks);
 }
 
 int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const double* wJ, const double* MM,

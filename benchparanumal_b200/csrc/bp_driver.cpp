@@ -201,8 +201,8 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
     throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex, Quad and Tri only");
   if (quad && bp <= 4)
     throw std::runtime_error("ELEMENT TYPE Quad is available for BK5/BK6 and BP5/BP6 (BP1-BP4: Hex only)");
-  if (tri && (bp != 5 || !S.compare("AFFINE MESH", "TRUE") || S.compare("PRECISION", "MIXED")))
-    throw std::runtime_error("ELEMENT TYPE Tri is available for BK5 and BP5 with -a, in FP64");
+  if (tri && (bp != 5 || !S.compare("AFFINE MESH", "TRUE")))
+    throw std::runtime_error("ELEMENT TYPE Tri is available for BK5 and BP5 with -a");
   check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
   bp_box_desc_t d{};
   d.dim = quad || tri ? 2 : 3;
@@ -448,6 +448,7 @@ int run_bk(const char* name, int bk, Settings& S) {
   d.dim = P.view.dim;
   // -fp MIXED times the FP32 operator of the mixed-precision solver (BK5/BK6)
   const bool fp32 = S.compare("PRECISION", "MIXED");
+  if (fp32 && P.view.simplex) throw std::runtime_error("BK5 -e Tri times the FP64 operator only");
   const size_t ng = P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.view.Np;
   const int nr = std::atoi(S.get("RIGHT-HAND SIDES").c_str());
   if (nr > 1 && (!fp32 || bk != 5)) throw std::runtime_error("-nr is available for BK5 with -fp MIXED");

@@ -252,6 +252,9 @@ namespace bp {
 int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
                   const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,
                   const int* skip, cudaStream_t s, double* partials = nullptr, int* nblocks = nullptr);
+int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const float* wJ,
+                  const float* ggeo, const float* S, const float* MM, float lambda, const float* q, float* Aq,
+                  const int* skip, cudaStream_t s, double* partials = nullptr, int* nblocks = nullptr);
 int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const double* wJ, const double* MM,
                           const double* f, double* bL, cudaStream_t s);
 int launch_diag_local_tri(int N, int32_t Nelements, const double* wJ, const double* ggeo, const double* S,

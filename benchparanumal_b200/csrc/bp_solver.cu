@@ -663,8 +663,8 @@ static int mesh_fp32(bp_solver_s* S, cudaStream_t s) {
   const ElemOperands<double> o = operands64(S);
   const bool cub = S->bp <= 4;
   const size_t ng = cub ? (mesh->affine ? (size_t)mesh->E : mesh->cubwJ_c.n) : mesh->wJ.n;
-  const size_t nD = cub ? (mesh->affine ? mesh->cubDmodal.n : mesh->cubD.n) : mesh->D.n;
-  const size_t nT = cub ? (mesh->affine ? mesh->MM.n : mesh->cubInterp.n) : 0;
+  const size_t nD = mesh->simplex ? mesh->S.n : cub ? (mesh->affine ? mesh->cubDmodal.n : mesh->cubD.n) : mesh->D.n;
+  const size_t nT = mesh->simplex ? mesh->MM.n : cub ? (mesh->affine ? mesh->MM.n : mesh->cubInterp.n) : 0;
   BP_TRY(f.wJ.alloc(ng));
   const int nggeo = mesh->dim == 2 ? 3 : 6;   // factors per node (per element when affine)
   BP_TRY(f.ggeo.alloc(nggeo * ng));
@@ -685,13 +685,9 @@ template <class V>
 static int elem_apply(bp_solver_s* S, const ElemOperands<V>& o, const V* q, V* AqL, const int* skip, cudaStream_t s,
                       const CgFuse* fuse = nullptr, int* nblocks = nullptr) {
   bp_mesh_s* m = S->mesh;
-  if (m->simplex) {   // Tri2D, FP64 only (the solver rejects mixed precision on it)
-    if constexpr (std::is_same<V, double>::value)
-      return launch_ax_tri(m->N, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, o.T, S->lambda, q, AqL,
-                           skip, s, fuse ? fuse->partials : nullptr, nblocks);
-    else
-      return fail(BP_ERROR_ARG, "Tri2D operator: FP64 only");
-  }
+  if (m->simplex)   // Tri2D: D carries the stiffness matrices S, T the mass matrix
+    return launch_ax_tri(m->N, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, o.T, (V)S->lambda, q, AqL,
+                         skip, s, fuse ? fuse->partials : nullptr, nblocks);
   if (S->bp >= 5)
     return launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D, (V)S->lambda, q,
                           AqL, skip, s, fuse, nblocks);
@@ -1020,8 +1016,6 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
   if (d->bp < 1 || d->bp > 6) return fail(BP_ERROR_ARG, "bp_solver_create: bp must be 1..6");
   if (mesh->simplex) {
     if (d->bp != 5) return fail(BP_ERROR_ARG, "bp_solver_create: Tri2D meshes take BP5");
-    if (d->precision != BP_PRECISION_FP64)
-      return fail(BP_ERROR_ARG, "bp_solver_create: Tri2D solves are FP64 (no mixed-precision operator)");
   } else if (mesh->dim == 2) {
     if (d->bp < 5) return fail(BP_ERROR_ARG, "bp_solver_create: Quad2D meshes take BP5 and BP6 (the BP1-BP4 forms are Hex3D only)");
     if ((d->bp == 6) != (mesh->Nfields == 2))

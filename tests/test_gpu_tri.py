@@ -1,6 +1,6 @@
 """Tri2D (affine triangles, BP5) through the C ABI: the device mesh against the
 reference's own set-up (tests/golden/ref_tri_*.npz), bp_ax_tri2d, the gather,
-the seeded forcing, the Jacobi diagonal and FP64 CG against the oracle's
+the forcings, the Jacobi diagonal, FP64 and mixed-precision CG against the oracle's
 restatement of okl/bp5AxAffineTri2D.okl (oracle/tri2d.py, itself held to the
 same fixtures by tests/test_tri2d.py).
 
@@ -120,6 +120,23 @@ def test_cg_history_matches_oracle(gpu, tri, nx, ny, N, precon):
     assert _rel(x.download(), x_t) < 1e-6
 
 
+@pytest.mark.parametrize("nx,ny,N", [(12, 10, 6), (8, 8, 3)])
+def test_mixed_solve_reaches_tolerance(gpu, tri, nx, ny, N):
+    # FP32 triangle operator inside the reliable-update CG: the FP64 residual of
+    # the returned x, and the FP64 oracle's solution
+    om = tri.Mesh(nx, ny, N)
+    gm = _mesh(gpu, nx, ny, N)
+    S = gpu.BP(gm, precon="JACOBI", precision="MIXED")
+    _, b_o = om.rhs_random(1)
+    x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
+    st, _, _ = S.solve(x, gpu.DeviceBuffer.from_host(b_o), tol=1e-8, maxit=5000)
+    assert st.updates >= 1
+    xh = x.download()
+    assert np.linalg.norm(b_o - om.operator(xh)) <= 1.0001e-8 * np.linalg.norm(b_o)
+    x64, _, _ = om.cg(b_o, 1.0, 1e-12, 5000, precon=True)
+    assert _rel(xh, x64) < 1e-6
+
+
 def test_driver_result_line(gpu, capfd):
     assert gpu.driver_main("BP5", ["-e", "Tri", "-nx", "8", "-ny", "6", "-p", "5", "-a", "-f", "RANDOM", "-pc",
                                    "JACOBI", "-wi", "5", "-it", "50"]) == 0
@@ -134,10 +151,8 @@ def test_driver_result_line(gpu, capfd):
 def test_rejections(gpu):
     gm = _mesh(gpu, 3, 3, 4)
     with pytest.raises(gpu.BPError):
-        gpu.BP(gm, precision="MIXED")     # no FP32 triangle operator
-    with pytest.raises(gpu.BPError):
         gpu.BP(gm, bp=6)
     with pytest.raises(gpu.BPError):
         gpu.Mesh(3, 3, N=4, affine=False, dim=2, simplex=True)
     assert gpu.driver_main("BP5", ["-e", "Tri", "-nx", "4", "-ny", "4"]) != 0   # needs -a
-    assert gpu.driver_main("BP5", ["-e", "Tri", "-nx", "4", "-ny", "4", "-a", "-fp", "MIXED", "-tol", "1e-8"]) != 0
+    assert gpu.driver_main("BK5", ["-e", "Tri", "-nx", "4", "-ny", "4", "-a", "-fp", "MIXED"]) != 0
