@@ -43,14 +43,14 @@ EXPORTS = [
     "bp_malloc", "bp_free", "bp_host_malloc", "bp_host_free", "bp_memcpy_htod", "bp_memcpy_dtoh",
     "bp_memcpy_dtod", "bp_memset", "bp_stream_create", "bp_stream_destroy", "bp_finish",
     "bp_event_create", "bp_event_destroy", "bp_event_record", "bp_event_elapsed_ms",
-    "bp_ax_hex3d", "bp_ax_tri2d", "bp_ogs_gather", "bp_ogs_scatter", "bp_linalg_set", "bp_linalg_axpy",
+    "bp_ax_hex3d", "bp_ax_tri2d", "bp_ax_tet3d", "bp_ogs_gather", "bp_ogs_scatter", "bp_linalg_set", "bp_linalg_axpy",
     "bp_linalg_inner_prod", "bp_linalg_norm2", "bp_update_cg",
     "bp_mesh_create", "bp_mesh_view", "bp_mesh_destroy",
     "bp_solver_create", "bp_solver_destroy", "bp_solver_size", "bp_solver_operator", "bp_solver_rhs",
     "bp_solver_diagonal", "bp_solver_solve", "bp_solver_solve_host", "bp_driver_main",
     "bp_box_numbering", "bp_basis_gll", "bp_box_vertices", "bp_operator_hex3d_noalloc", "bp_ogs_check",
     "bp_test_wait_timeout", "bp_tune_report", "bp_tune_reset",
-    "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature", "bp_basis_tri2d",
+    "bp_ax_cub_hex3d", "bp_mesh_cubature", "bp_mesh_cubature_view", "bp_basis_cubature", "bp_basis_tri2d", "bp_basis_tet3d",
     "bp_batch_create", "bp_batch_destroy", "bp_batch_systems", "bp_batch_system_info", "bp_batch_solve",
     "bp_batch_vectors", "bp_batch_solver", "bp_ax_hex3d_f32", "bp_convert_f64_f32", "bp_ax_hex3d_f32_multi",
     "bp_ax_cub_hex3d_f32", "bp_mesh_write_vtu", "bp_ogs_owner_map", "bp_cg_direction_ax_hex3d",
@@ -152,6 +152,7 @@ def lib():
             "bp_event_elapsed_ms": [vp, vp, ctypes.POINTER(ctypes.c_float)],
             "bp_ax_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
             "bp_ax_tri2d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
+            "bp_ax_tet3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
             "bp_ogs_gather": [i32, vp, vp, vp, vp, vp],
             "bp_ogs_scatter": [i32, vp, vp, vp, vp, vp],
             "bp_linalg_set": [i32, dbl, vp, vp],
@@ -183,6 +184,7 @@ def lib():
             "bp_ax_cub_hex3d": [ctypes.POINTER(AxDesc), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp, vp, vp],
             "bp_mesh_cubature": [vp],
             "bp_basis_tri2d": [i32, vp, vp, vp, vp, vp],
+            "bp_basis_tet3d": [i32, vp, vp, vp, vp, vp, vp],
             "bp_mesh_cubature_view": [vp, ctypes.POINTER(CubatureView)],
             "bp_basis_cubature": [i32, vp, vp, vp, vp, vp, vp, vp],
             "bp_batch_create": [ctypes.POINTER(BatchProblem), i32, ctypes.POINTER(SolverDesc), ctypes.POINTER(vp)],
@@ -316,7 +318,8 @@ def _dl(ptr, n, dtype):
 class Mesh:
     """Box mesh on the device (mesh_t + masked ogs), built by bp_mesh_create:
     Hex3D, or Quad2D with dim=2 (nz ignored; Nfields 1 or 2), or Tri2D with
-    dim=2 and simplex=True (affine, one field, 2*nx*ny triangles)."""
+    dim=2 and simplex=True (affine, one field, 2*nx*ny triangles), or Tet3D with
+    dim=3 and simplex=True (6*nx*ny*nz tetrahedra)."""
 
     def __init__(self, nx, ny=None, nz=None, N=4, affine=False, Nfields=1, pert=0.0, pert_seed=1, device=0, dim=3,
                  simplex=False):
@@ -347,10 +350,13 @@ class Mesh:
         """Copy a device mesh array to the host (names as in bp_mesh_view_t)."""
         v = self.view
         ng = self.E if self.affine else self.E * self.Np
-        nv, ngg = (8, 6) if self.dim == 3 else ((3, 3) if self.simplex else (4, 3))
-        if self.simplex:   # Tri2D: D holds Dr and Ds, S the three stiffness matrices, MM the mass matrix
+        if self.simplex:
+            nv, ngg = (3, 3) if self.dim == 2 else (4, 6)
+        else:
+            nv, ngg = (8, 6) if self.dim == 3 else (4, 3)
+        if self.simplex:   # D holds Dr, Ds (, Dt), S the stiffness matrices, MM the mass matrix
             NP2 = self.Np * self.Np
-            tri = {"D": 2 * NP2, "S": 3 * NP2, "MM": NP2}
+            tri = {"D": self.dim * NP2, "S": (3 if self.dim == 2 else 6) * NP2, "MM": NP2}
             if name in tri:
                 return _dl(getattr(v, name), tri[name], np.float64)
         spec = {
@@ -358,7 +364,7 @@ class Mesh:
             "rowStarts": (self.Ngather + 1, np.int32), "colIds": (self.nnz, np.int32),
             "wJ": (ng, np.float64), "ggeo": (ngg * ng, np.float64), "D": (self.Nq * self.Nq, np.float64),
             "gllz": (self.Nq, np.float64), "gllw": (self.Nq, np.float64), "EX": (nv * self.E, np.float64),
-            "EY": (nv * self.E, np.float64), "EZ": ((8 if self.dim == 3 else 0) * self.E, np.float64),
+            "EY": (nv * self.E, np.float64), "EZ": ((nv if self.dim == 3 else 0) * self.E, np.float64),
         }
         if name in spec:
             n, dt = spec[name]
@@ -411,6 +417,14 @@ def ax_cub_hex3d(mesh, bp, q, Aq, lam=1.0, stream=None):
 def convert_f64_f32(src, n, dst, stream=None):
     """dst (FP32 device) = src (FP64 device address or buffer), n elements."""
     _check(lib().bp_convert_f64_f32(n, src if isinstance(src, int) else _ptr(src), _ptr(dst), stream))
+
+
+def ax_tet3d(mesh, q, Aq, lam=1.0, stream=None):
+    """bp_ax_tet3d on a Tet3D mesh's own arrays: Aq (E-vector) = A_e q[G2L]."""
+    v = mesh.view
+    d = AxDesc(5, mesh.N, 1, 1, 3)
+    _check(lib().bp_ax_tet3d(ctypes.byref(d), mesh.E, v.elementList, v.GlobalToLocal, v.wJ, v.ggeo, v.S, v.MM,
+                             float(lam), q.ptr, Aq.ptr, stream))
 
 
 def ax_tri2d(mesh, q, Aq, lam=1.0, stream=None):
@@ -662,8 +676,11 @@ def box_numbering(nx, ny, nz, N, Nfields=1, dim=3, simplex=False):
     d = BoxDesc(nx, ny, nz if dim == 3 else 1, N, int(bool(simplex)), Nfields, 0.0, 1, dim, int(bool(simplex)))
     ng, nnz = ctypes.c_int32(), ctypes.c_int32()
     _check(lib().bp_box_numbering(ctypes.byref(d), ctypes.byref(ng), ctypes.byref(nnz), None, None, None))
-    E = nx * ny * (nz if dim == 3 else 1) * (2 if simplex else 1)
-    Np = (N + 1) * (N + 2) // 2 if simplex else (N + 1) ** dim
+    E = nx * ny * (nz if dim == 3 else 1) * ((2 if dim == 2 else 6) if simplex else 1)
+    if simplex:
+        Np = (N + 1) * (N + 2) // 2 if dim == 2 else (N + 1) * (N + 2) * (N + 3) // 6
+    else:
+        Np = (N + 1) ** dim
     g2l = np.empty(E * Np * Nfields, np.int32)
     rs = np.empty(ng.value + 1, np.int32)
     ci = np.empty(nnz.value, np.int32)
@@ -681,6 +698,19 @@ def basis_tri2d(N):
     D = D.reshape(2, Np, Np).transpose(0, 2, 1)
     S = S.reshape(3, Np, Np).transpose(0, 2, 1)
     return r, s, D[0], D[1], MM.reshape(Np, Np), S[0], S[1], S[2]
+
+
+def basis_tet3d(N):
+    """Host-only Tet3D reference element: r, s, t [Np], Dr, Ds, Dt, MM and S [6]
+    (rr, rs, rt, ss, st, tt) as row-major Np x Np arrays."""
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    r, s, t = np.empty(Np), np.empty(Np), np.empty(Np)
+    D, MM, S = np.empty(3 * Np * Np), np.empty(Np * Np), np.empty(6 * Np * Np)
+    _check(lib().bp_basis_tet3d(N, r.ctypes.data, s.ctypes.data, t.ctypes.data, D.ctypes.data, MM.ctypes.data,
+                                S.ctypes.data))
+    D = D.reshape(3, Np, Np).transpose(0, 2, 1)
+    S = S.reshape(6, Np, Np).transpose(0, 2, 1)
+    return r, s, t, D[0], D[1], D[2], MM.reshape(Np, Np), S
 
 
 def basis_gll(N):

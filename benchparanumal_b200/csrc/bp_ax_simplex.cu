@@ -1,10 +1,11 @@
-// Tri2D (affine triangles) BP5 element operator, forcing mass and Jacobi
+// Simplex (affine Tri2D and Tet3D) BP5 element operator, forcings and Jacobi
 // diagonal.
 //
-// The reference's affine triangle operator (okl/bp5AxAffineTri2D.okl:27-89)
-// applies four dense Np x Np reference matrices per element:
-//   Aq_e = G00 Srr q_e + G01 Srs q_e + G11 Sss q_e + lambda J MM q_e
-// with the per-element factors (G00, G01, G11, J).  Np = (N+1)(N+2)/2 is not a
+// The reference's affine simplex operators (okl/bp5AxAffineTri2D.okl:27-89,
+// okl/bp5AxAffineTet3D.okl) apply dense Np x Np reference matrices per element:
+//   Aq_e = sum_ab G_ab S_ab q_e + lambda J MM q_e
+// over ab = rr, rs, ss (triangles: NSM = 3) or rr, rs, rt, ss, st, tt
+// (tetrahedra: NSM = 6), with per-element factors G_ab and J.  Np is not a
 // tensor product, so there is no sum factorisation: a batched product of the
 // four stacked matrices with the elements' gathered values (in shared memory),
 // the matrices read with node-fastest layout (X[k*Np + n] is the weight of
@@ -25,6 +26,9 @@ namespace {
 
 constexpr int kTriThreads = 256;
 
+// nodes of the degree-N triangle (dim 2) or tetrahedron (dim 3)
+int simplex_np(int dim, int N) { return dim == 2 ? (N + 1) * (N + 2) / 2 : (N + 1) * (N + 2) * (N + 3) / 6; }
+
 // node groups per block (element slots for the forcing) and threads per block (whole warps)
 static void tri_shape(int Np, int* epb, int* threads) {
   *epb = Np >= kTriThreads ? 1 : kTriThreads / Np;
@@ -39,9 +43,9 @@ static void tri_shape(int Np, int* epb, int* threads) {
 // 43.4 ms (132 registers in the CG form with the p.Ap sum).
 constexpr int kTriElems = 4;
 
-template <class F, bool DOT>
+template <class F, int NSM, bool DOT>
 __global__ void __launch_bounds__(kTriThreads + 32)
-ax_tri_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ elementList,
+ax_simplex_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ elementList,
               const int32_t* __restrict__ G2L, const F* __restrict__ wJ, const F* __restrict__ ggeo,
               const F* __restrict__ S, const F* __restrict__ MM, F lambda, const F* __restrict__ q,
               F* __restrict__ Aq, const int* __restrict__ skip, double* __restrict__ partials) {
@@ -69,19 +73,22 @@ ax_tri_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ ele
   if (g < groups) {
     const F* sq = s_q + (size_t)g * kTriElems * Np;
     const size_t NP2 = (size_t)Np * Np;
-    F qrr[kTriElems], qrs[kTriElems], qss[kTriElems], qM[kTriElems];
+    F acc[NSM + 1][kTriElems];   // the S_ab sums, then the mass sum
 #pragma unroll
-    for (int j = 0; j < kTriElems; ++j) qrr[j] = qrs[j] = qss[j] = qM[j] = 0;
+    for (int a = 0; a <= NSM; ++a)
+#pragma unroll
+      for (int j = 0; j < kTriElems; ++j) acc[a][j] = 0;
     for (int k = 0; k < Np; ++k) {
       const size_t o = (size_t)k * Np + n;
-      const F a = __ldg(S + o), b = __ldg(S + NP2 + o), c = __ldg(S + 2 * NP2 + o), d = __ldg(MM + o);
+      F w[NSM + 1];
+#pragma unroll
+      for (int a = 0; a < NSM; ++a) w[a] = __ldg(S + a * NP2 + o);
+      w[NSM] = __ldg(MM + o);
 #pragma unroll
       for (int j = 0; j < kTriElems; ++j) {
         const F qk = sq[j * Np + k];
-        qrr[j] += a * qk;
-        qrs[j] += b * qk;
-        qss[j] += c * qk;
-        qM[j] += d * qk;
+#pragma unroll
+        for (int a = 0; a <= NSM; ++a) acc[a][j] += w[a] * qk;
       }
     }
 #pragma unroll
@@ -89,8 +96,11 @@ ax_tri_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ ele
       const int eidx = e0 + g * kTriElems + j;
       if (eidx < Nelements) {
         const int element = elementList[eidx];
-        const F* gg = ggeo + 3 * (size_t)element;
-        const F out = gg[0] * qrr[j] + gg[1] * qrs[j] + gg[2] * qss[j] + wJ[element] * lambda * qM[j];
+        const F* gg = ggeo + NSM * (size_t)element;
+        F out = gg[0] * acc[0][j];
+#pragma unroll
+        for (int a = 1; a < NSM; ++a) out += gg[a] * acc[a][j];
+        out += wJ[element] * lambda * acc[NSM][j];
         Aq[(size_t)element * Np + n] = out;
         if (DOT) pdot += (double)sq[j * Np + n] * (double)out;
       }
@@ -123,26 +133,29 @@ tri_mass_local_kernel(int Nelements, int Np, int epb, const int32_t* __restrict_
   bL[(size_t)e * Np + n] = wJ[e] * acc;
 }
 
-// diagonal of A_e: G00 Srr(n,n) + G01 Srs(n,n) + G11 Sss(n,n) + lambda J MM(n,n)
-__global__ void tri_diag_local_kernel(int Nelements, int Np, const double* __restrict__ wJ,
-                                      const double* __restrict__ ggeo, const double* __restrict__ S,
-                                      const double* __restrict__ MM, double lambda, double* __restrict__ dL) {
+// diagonal of A_e: sum_ab G_ab S_ab(n,n) + lambda J MM(n,n)
+__global__ void simplex_diag_local_kernel(int Nelements, int Np, int nsm, const double* __restrict__ wJ,
+                                          const double* __restrict__ ggeo, const double* __restrict__ S,
+                                          const double* __restrict__ MM, double lambda, double* __restrict__ dL) {
   const size_t NP2 = (size_t)Np * Np;
   const size_t total = (size_t)Nelements * Np;
   for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < total; l += (size_t)blockDim.x * gridDim.x) {
     const size_t e = l / Np, n = l - e * Np;
     const size_t dn = n * Np + n;
-    const double* g = ggeo + 3 * e;
-    dL[l] = g[0] * S[dn] + g[1] * S[NP2 + dn] + g[2] * S[2 * NP2 + dn] + lambda * wJ[e] * MM[dn];
+    const double* g = ggeo + nsm * e;
+    double d = g[0] * S[dn];
+    for (int a = 1; a < nsm; ++a) d += g[a] * S[a * NP2 + dn];
+    dL[l] = d + lambda * wJ[e] * MM[dn];
   }
 }
 
-// rhsAffineTri2D (okl/rhsTri2D.okl): b_e = MM (J_e f) with
-// f = (2 pi^2 + lambda) sin(pi x) sin(pi y) at every node of the element
+// rhsAffineTri2D / rhsAffineTet3D (okl/rhsTri2D.okl, okl/rhsTet3D.okl):
+// b_e = MM (J_e f) with f = (2 pi^2 + lambda) sin(pi x) sin(pi y) on triangles,
+// (3 pi^2 + lambda) sin(pi x) sin(pi y) sin(pi z) on tetrahedra (z given)
 __global__ void __launch_bounds__(kTriThreads + 32)
-tri_rhs_analytic_kernel(int Nelements, int Np, int epb, const double* __restrict__ wJ,
-                        const double* __restrict__ MM, const double* __restrict__ x, const double* __restrict__ y,
-                        double lambda, double* __restrict__ bL) {
+simplex_rhs_analytic_kernel(int Nelements, int Np, int epb, const double* __restrict__ wJ,
+                            const double* __restrict__ MM, const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, double lambda, double* __restrict__ bL) {
   extern __shared__ __align__(16) double s_f[];
   const double pi = 3.14159265358979323846;
   const int t = threadIdx.x;
@@ -151,7 +164,9 @@ tri_rhs_analytic_kernel(int Nelements, int Np, int epb, const double* __restrict
   const bool active = es < epb && e < Nelements;
   if (active) {
     const size_t id = (size_t)e * Np + n;
-    s_f[es * Np + n] = wJ[e] * ((2 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]));
+    const double f = z ? (3 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]) * sin(pi * z[id])
+                       : (2 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]);
+    s_f[es * Np + n] = wJ[e] * f;
   }
   __syncthreads();
   if (!active) return;
@@ -162,27 +177,28 @@ tri_rhs_analytic_kernel(int Nelements, int Np, int epb, const double* __restrict
 
 }  // namespace
 
-int launch_rhs_analytic_tri(int N, int32_t Nelements, const double* wJ, const double* MM, const double* x,
-                            const double* y, double lambda, double* bL, cudaStream_t s) {
+int launch_rhs_analytic_simplex(int dim, int N, int32_t Nelements, const double* wJ, const double* MM,
+                                const double* x, const double* y, const double* z, double lambda, double* bL,
+                                cudaStream_t s) {
   if (Nelements == 0) return BP_SUCCESS;
-  const int Np = (N + 1) * (N + 2) / 2;
+  const int Np = simplex_np(dim, N);
   int epb = 0, threads = 0;
   tri_shape(Np, &epb, &threads);
   const int grid = (Nelements + epb - 1) / epb;
-  tri_rhs_analytic_kernel<<<grid, threads, sizeof(double) * epb * Np, s>>>(Nelements, Np, epb, wJ, MM, x, y, lambda,
-                                                                          bL);
+  simplex_rhs_analytic_kernel<<<grid, threads, sizeof(double) * epb * Np, s>>>(Nelements, Np, epb, wJ, MM, x, y,
+                                                                              dim == 3 ? z : nullptr, lambda, bL);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }
 
-template <class F>
-static int launch_ax_tri_t(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ,
-                           const F* ggeo, const F* S, const F* MM, F lambda, const F* q, F* Aq, const int* skip,
-                           cudaStream_t s, double* partials, int* nblocks) {
+template <class F, int NSM>
+static int launch_ax_simplex_t(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const F* wJ,
+                               const F* ggeo, const F* S, const F* MM, F lambda, const F* q, F* Aq, const int* skip,
+                               cudaStream_t s, double* partials, int* nblocks) {
   if (nblocks) *nblocks = 0;
-  if (N < 1 || N > 15) return fail(BP_ERROR_ARG, "Tri2D operator: degree N must be in 1..15");
+  if (N < 1 || N > 15) return fail(BP_ERROR_ARG, "simplex operator: degree N must be in 1..15");
   if (Nelements == 0) return BP_SUCCESS;
-  const int Np = (N + 1) * (N + 2) / 2;
+  const int Np = simplex_np(NSM == 3 ? 2 : 3, N);
   int groups = 0, threads = 0;
   tri_shape(Np, &groups, &threads);
   const int slots = groups * kTriElems;
@@ -190,32 +206,43 @@ static int launch_ax_tri_t(int N, int32_t Nelements, const int32_t* elementList,
   if (nblocks) *nblocks = grid;
   const size_t smem = sizeof(double) * (size_t)(slots * Np > threads ? slots * Np : threads);
   if (partials)
-    BP_CUDA_TRY(launch_pdl(ax_tri_kernel<F, true>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
+    BP_CUDA_TRY(launch_pdl(ax_simplex_kernel<F, NSM, true>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
                            G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, partials));
   else
-    BP_CUDA_TRY(launch_pdl(ax_tri_kernel<F, false>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
+    BP_CUDA_TRY(launch_pdl(ax_simplex_kernel<F, NSM, false>, grid, threads, smem, s, (int)Nelements, Np, groups, elementList,
                            G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, (double*)nullptr));
   return BP_SUCCESS;
 }
 
-int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
-                  const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,
-                  const int* skip, cudaStream_t s, double* partials, int* nblocks) {
-  return launch_ax_tri_t<double>(N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s, partials,
-                                 nblocks);
+template <class F>
+static int launch_ax_simplex_any(int dim, int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                                 const F* wJ, const F* ggeo, const F* S, const F* MM, F lambda, const F* q, F* Aq,
+                                 const int* skip, cudaStream_t s, double* partials, int* nblocks) {
+  if (dim == 2)
+    return launch_ax_simplex_t<F, 3>(N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s,
+                                     partials, nblocks);
+  return launch_ax_simplex_t<F, 6>(N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s, partials,
+                                   nblocks);
 }
 
-int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const float* wJ,
-                  const float* ggeo, const float* S, const float* MM, float lambda, const float* q, float* Aq,
-                  const int* skip, cudaStream_t s, double* partials, int* nblocks) {
-  return launch_ax_tri_t<float>(N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s, partials,
-                                nblocks);
+int launch_ax_simplex(int dim, int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                      const double* wJ, const double* ggeo, const double* S, const double* MM, double lambda,
+                      const double* q, double* Aq, const int* skip, cudaStream_t s, double* partials, int* nblocks) {
+  return launch_ax_simplex_any<double>(dim, N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s,
+                                       partials, nblocks);
 }
 
-int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const double* wJ, const double* MM,
-                          const double* f, double* bL, cudaStream_t s) {
+int launch_ax_simplex(int dim, int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                      const float* wJ, const float* ggeo, const float* S, const float* MM, float lambda,
+                      const float* q, float* Aq, const int* skip, cudaStream_t s, double* partials, int* nblocks) {
+  return launch_ax_simplex_any<float>(dim, N, Nelements, elementList, G2L, wJ, ggeo, S, MM, lambda, q, Aq, skip, s,
+                                      partials, nblocks);
+}
+
+int launch_mass_local_simplex(int dim, int N, int32_t Nelements, const int32_t* G2L, const double* wJ,
+                              const double* MM, const double* f, double* bL, cudaStream_t s) {
   if (Nelements == 0) return BP_SUCCESS;
-  const int Np = (N + 1) * (N + 2) / 2;
+  const int Np = simplex_np(dim, N);
   int epb = 0, threads = 0;
   tri_shape(Np, &epb, &threads);
   const int grid = (Nelements + epb - 1) / epb;
@@ -224,13 +251,13 @@ int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const do
   return BP_SUCCESS;
 }
 
-int launch_diag_local_tri(int N, int32_t Nelements, const double* wJ, const double* ggeo, const double* S,
-                          const double* MM, double lambda, double* dL, cudaStream_t s) {
+int launch_diag_local_simplex(int dim, int N, int32_t Nelements, const double* wJ, const double* ggeo,
+                              const double* S, const double* MM, double lambda, double* dL, cudaStream_t s) {
   if (Nelements == 0) return BP_SUCCESS;
-  const int Np = (N + 1) * (N + 2) / 2;
+  const int Np = simplex_np(dim, N);
   const size_t total = (size_t)Nelements * Np;
   const int grid = (int)((total + 255) / 256 < 65535 ? (total + 255) / 256 : 65535);
-  tri_diag_local_kernel<<<grid, 256, 0, s>>>(Nelements, Np, wJ, ggeo, S, MM, lambda, dL);
+  simplex_diag_local_kernel<<<grid, 256, 0, s>>>(Nelements, Np, dim == 2 ? 3 : 6, wJ, ggeo, S, MM, lambda, dL);
   BP_CUDA_TRY(cudaGetLastError());
   return BP_SUCCESS;
 }

@@ -317,8 +317,23 @@ int bp_ax_tri2d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* element
   if (Nelements == 0) return BP_SUCCESS;
   if (!elementList || !GlobalToLocal || !wJ || !ggeo || !S || !MM || !q || !Aq)
     return fail(BP_ERROR_ARG, "bp_ax_tri2d: null array");
-  return launch_ax_tri(d->N, Nelements, elementList, GlobalToLocal, wJ, ggeo, S, MM, lambda, q, Aq, nullptr,
-                       to_stream(stream));
+  return launch_ax_simplex(2, d->N, Nelements, elementList, GlobalToLocal, wJ, ggeo, S, MM, lambda, q, Aq, nullptr,
+                           to_stream(stream));
+}
+
+int bp_ax_tet3d(const bp_ax_desc_t* d, int32_t Nelements, const int32_t* elementList, const int32_t* GlobalToLocal,
+                const double* wJ, const double* ggeo, const double* S, const double* MM, double lambda,
+                const double* q, double* Aq, bp_stream_t stream) {
+  if (!d) return fail(BP_ERROR_ARG, "bp_ax_tet3d: null descriptor");
+  if (d->bp != 5 || d->Nfields != 1 || (d->dim != 3 && d->dim != 0) || !d->affine)
+    return fail(BP_ERROR_ARG, "bp_ax_tet3d: the Tet3D operator is BP5, one field, dim 3, affine");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_ax_tet3d: degree N must be in 1..15");
+  if (Nelements < 0) return fail(BP_ERROR_ARG, "bp_ax_tet3d: negative element count");
+  if (Nelements == 0) return BP_SUCCESS;
+  if (!elementList || !GlobalToLocal || !wJ || !ggeo || !S || !MM || !q || !Aq)
+    return fail(BP_ERROR_ARG, "bp_ax_tet3d: null array");
+  return launch_ax_simplex(3, d->N, Nelements, elementList, GlobalToLocal, wJ, ggeo, S, MM, lambda, q, Aq, nullptr,
+                           to_stream(stream));
 }
 
 int bp_ax_hex3d_f32(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
@@ -675,12 +690,71 @@ static int mesh_create_tri(const bp_box_desc_t* d, bp_mesh_t* out) {
   return BP_SUCCESS;
 }
 
+static int mesh_create_tet(const bp_box_desc_t* d, bp_mesh_t* out) {
+  if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
+  if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
+  if (d->Nfields != 1) return fail(BP_ERROR_ARG, "bp_mesh_create: Tet3D meshes take one field (BP5)");
+  if (!d->affine) return fail(BP_ERROR_ARG, "bp_mesh_create: Tet3D meshes are affine here (-a)");
+  if (d->pert != 0.0) return fail(BP_ERROR_ARG, "bp_mesh_create: the Tet3D box has no vertex perturbation");
+  TetBasis tb;
+  if (!tet_basis(d->N, tb)) return fail(BP_ERROR_NUMERIC, "bp_mesh_create: singular Tet3D Vandermonde matrix");
+  const int Np = tb.Np;
+  const int64_t E64 = 6 * (int64_t)d->nx * d->ny * d->nz;
+  if (E64 * Np >= (int64_t)INT32_MAX)
+    return fail(BP_ERROR_ARG, "bp_mesh_create: local node count exceeds int32 (dlong) range");
+  cudaStream_t s = default_stream();
+  HostMesh hm;
+  hm.dim = 3;
+  hm.N = d->N; hm.Nq = d->N + 1; hm.Np = Np;
+  hm.nx = d->nx; hm.ny = d->ny; hm.nz = d->nz;
+  hm.E = (int)E64; hm.affine = 1; hm.Nfields = 1;
+  std::vector<double> wJ, ggeo, xn, yn, zn;
+  if (!box_tet(hm, tb, wJ, ggeo, xn, yn, zn))
+    return fail(BP_ERROR_NUMERIC, "bp_mesh_create: non-positive Jacobian found");
+  std::vector<double> D(tb.Dr);
+  D.insert(D.end(), tb.Ds.begin(), tb.Ds.end());
+  D.insert(D.end(), tb.Dt.begin(), tb.Dt.end());
+  bp_mesh_s* m = new bp_mesh_s();
+  m->dim = 3;
+  m->simplex = 1;
+  m->N = hm.N; m->Nq = hm.Nq; m->Np = Np; m->E = hm.E; m->Nfields = 1; m->affine = 1;
+  m->Ngather = hm.Ngather; m->nnz = hm.nnz;
+  std::vector<int32_t> elist(hm.E);
+  for (int e = 0; e < hm.E; ++e) elist[e] = e;
+  int rc = BP_SUCCESS;
+  do {
+    if ((rc = m->elementList.upload(elist, s))) break;
+    if ((rc = m->G2L.upload(hm.G2L, s))) break;
+    if ((rc = m->rowStarts.upload(hm.rowStarts, s))) break;
+    if ((rc = m->colIds.upload(hm.colIds, s))) break;
+    if ((rc = m->D.upload(node_fastest(D, Np), s))) break;
+    if ((rc = m->S.upload(node_fastest(tb.S, Np), s))) break;
+    if ((rc = m->MM.upload(tb.MM, s))) break;   // symmetric
+    if ((rc = m->x.upload(xn, s))) break;
+    if ((rc = m->y.upload(yn, s))) break;
+    if ((rc = m->z.upload(zn, s))) break;
+    if ((rc = m->EX.upload(hm.EX, s))) break;
+    if ((rc = m->EY.upload(hm.EY, s))) break;
+    if ((rc = m->EZ.upload(hm.EZ, s))) break;
+    if ((rc = m->wJ.upload(wJ, s))) break;
+    if ((rc = m->ggeo.upload(ggeo, s))) break;
+    cudaError_t ce = cudaStreamSynchronize(s);   // the host vectors are released on return
+    if (ce != cudaSuccess) { rc = cuda_fail(ce, "bp_mesh_create", __FILE__, __LINE__); break; }
+  } while (0);
+  if (rc != BP_SUCCESS) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return BP_SUCCESS;
+}
+
 int bp_mesh_create(const bp_box_desc_t* d, bp_mesh_t* out) {
   if (!d || !out) return fail(BP_ERROR_ARG, "bp_mesh_create: null pointer");
   *out = nullptr;
   if (d->dim != 0 && d->dim != 2 && d->dim != 3) return fail(BP_ERROR_ARG, "bp_mesh_create: dim must be 2 or 3");
-  if (d->simplex && d->dim != 2) return fail(BP_ERROR_ARG, "bp_mesh_create: simplex meshes are Tri2D (dim 2)");
   if (d->dim == 2 && d->simplex) return mesh_create_tri(d, out);
+  if (d->simplex) return mesh_create_tet(d, out);
   if (d->dim == 2) return mesh_create_quad(d, out);
   if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(BP_ERROR_ARG, "bp_mesh_create: element counts must be >= 1");
   if (d->N < 1 || d->N > 15) return fail(BP_ERROR_ARG, "bp_mesh_create: degree must be in 1..15");
@@ -767,7 +841,8 @@ int bp_mesh_view(bp_mesh_t m, bp_mesh_view_t* v) {
 
 int bp_mesh_cubature(bp_mesh_t m) {
   if (!m) return fail(BP_ERROR_ARG, "bp_mesh_cubature: null mesh");
-  if (m->dim == 2) return fail(BP_ERROR_ARG, "bp_mesh_cubature: the over-integrated BP1-BP4 forms are Hex3D only");
+  if (m->dim == 2 || m->simplex)
+    return fail(BP_ERROR_ARG, "bp_mesh_cubature: the over-integrated BP1-BP4 forms are Hex3D only");
   if (m->cubNq) return BP_SUCCESS;
   cudaStream_t s = default_stream();
   std::vector<double> z(m->Nq);
@@ -848,7 +923,7 @@ int bp_mesh_cubature_view(bp_mesh_t m, bp_cubature_view_t* v) {
 
 int bp_mesh_write_vtu(bp_mesh_t m, const double* xL, const char* filename) {
   if (!m || !xL || !filename) return fail(BP_ERROR_ARG, "bp_mesh_write_vtu: null pointer");
-  if (m->dim == 2) return fail(BP_ERROR_ARG, "bp_mesh_write_vtu: Hex3D meshes only");
+  if (m->dim == 2 || m->simplex) return fail(BP_ERROR_ARG, "bp_mesh_write_vtu: Hex3D meshes only");
   const int Nq = m->Nq, Np = m->Np, E = m->E, Nf = m->Nfields, N = m->N;
   std::vector<double> EX((size_t)8 * E), EY((size_t)8 * E), EZ((size_t)8 * E), z(Nq);
   BP_CUDA_TRY(cudaMemcpy(EX.data(), m->EX.ptr, sizeof(double) * EX.size(), cudaMemcpyDeviceToHost));

@@ -196,17 +196,16 @@ void setup(const Settings& S, Problem& P, int Nfields, int bp) {
     throw std::runtime_error("THREAD MODEL " + S.get("THREAD MODEL") +
                              " is not available: this build runs the CUDA (sm_100a) path only");
   const bool tri = S.compare("ELEMENT TYPE", "Tri");
+  const bool tet = S.compare("ELEMENT TYPE", "Tet");
   const bool quad = S.compare("ELEMENT TYPE", "Quad");
-  if (!S.compare("ELEMENT TYPE", "Hex") && !quad && !tri)
-    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is not available: Hex, Quad and Tri only");
   if (quad && bp <= 4)
     throw std::runtime_error("ELEMENT TYPE Quad is available for BK5/BK6 and BP5/BP6 (BP1-BP4: Hex only)");
-  if (tri && (bp != 5 || !S.compare("AFFINE MESH", "TRUE")))
-    throw std::runtime_error("ELEMENT TYPE Tri is available for BK5 and BP5 with -a");
+  if ((tri || tet) && (bp != 5 || !S.compare("AFFINE MESH", "TRUE")))
+    throw std::runtime_error("ELEMENT TYPE " + S.get("ELEMENT TYPE") + " is available for BK5 and BP5 with -a");
   check(bp_platform_init(std::atoi(S.get("DEVICE NUMBER").c_str())));
   bp_box_desc_t d{};
   d.dim = quad || tri ? 2 : 3;
-  d.simplex = tri ? 1 : 0;
+  d.simplex = tri || tet ? 1 : 0;
   d.nx = std::atoi(S.get("BOX NX").c_str());
   d.ny = std::atoi(S.get("BOX NY").c_str());
   d.nz = quad || tri ? 1 : std::atoi(S.get("BOX NZ").c_str());
@@ -255,8 +254,8 @@ double ax_bytes(int bp, const bp_mesh_view_t& v, long long Ndofs, double sv = 8.
 // reference flop model for one Ax application (the same files, Hex branches)
 double ax_flops(int bp, const bp_mesh_view_t& v) {
   const double Nq = v.Nq, E = v.Nelements, Nf = v.Nfields;
-  if (v.simplex)   // affine TRIANGLES branch of bp5Run.cpp:145-150
-    return (8.0 * v.Np * v.Np + 8.0 * v.Np) * Nf * E;
+  if (v.simplex)   // affine TRIANGLES and TETRAHEDRA branches of bp5Run.cpp:145-155
+    return (v.dim == 2 ? 8.0 * v.Np * v.Np + 8.0 * v.Np : 14.0 * v.Np * v.Np + 14.0 * v.Np) * Nf * E;
   if (v.dim == 2)   // QUADRILATERALS branches of bp5Run.cpp:144-187
     return (v.affine ? 8 * Nq * Nq * Nq + 12 * Nq * Nq : 8 * Nq * Nq * Nq + 8 * Nq * Nq) * Nf * E;
   const double cNq = v.N + 2, Nq3 = Nq * Nq * Nq, cNq3 = cNq * cNq * cNq;
@@ -393,7 +392,8 @@ int run_bp(const char* name, int bp, Settings& S) {
   const double Nbytes = (4 * Ndofs * 8.0 + NbytesAx + NbytesGather) + (11 * Ndofs * 8.0 + NbytesAx + NbytesGather) * Niter;
   const double NflopsAx = ax_flops(bp, P.view);
   const double Nflops = (5.0 * Ndofs + NflopsAx + NGlobal) + (11.0 * Ndofs + NflopsAx + NGlobal) * Niter;
-  std::string suffix = P.view.simplex ? "Element=Tri" : P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
+  std::string suffix = P.view.simplex ? (P.view.dim == 2 ? "Element=Tri" : "Element=Tet")
+                                       : P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, iterations=%d, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "
@@ -448,7 +448,7 @@ int run_bk(const char* name, int bk, Settings& S) {
   d.dim = P.view.dim;
   // -fp MIXED times the FP32 operator of the mixed-precision solver (BK5/BK6)
   const bool fp32 = S.compare("PRECISION", "MIXED");
-  if (fp32 && P.view.simplex) throw std::runtime_error("BK5 -e Tri times the FP64 operator only");
+  if (fp32 && P.view.simplex) throw std::runtime_error("BK5 -e Tri/Tet times the FP64 operator only");
   const size_t ng = P.view.affine ? (size_t)P.view.Nelements : (size_t)P.view.Nelements * P.view.Np;
   const int nr = std::atoi(S.get("RIGHT-HAND SIDES").c_str());
   if (nr > 1 && (!fp32 || bk != 5)) throw std::runtime_error("-nr is available for BK5 with -fp MIXED");
@@ -498,6 +498,9 @@ int run_bk(const char* name, int bk, Settings& S) {
     else if (fp32)
       check(bp_ax_hex3d_f32_multi(&d, nr, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, wJ32.p,
                                   ggeo32.p, gllw32.p, D32.p, 1.0f, q32.p, Aq32.p, nullptr));
+    else if (P.view.simplex && P.view.dim == 3)
+      check(bp_ax_tet3d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
+                        P.view.S, P.view.MM, 1.0, q.p, Aq.p, nullptr));
     else if (P.view.simplex)
       check(bp_ax_tri2d(&d, P.view.Nelements, P.view.elementList, P.view.GlobalToLocal, P.view.wJ, P.view.ggeo,
                         P.view.S, P.view.MM, 1.0, q.p, Aq.p, nullptr));
@@ -520,7 +523,8 @@ int run_bk(const char* name, int bk, Settings& S) {
   double Nbytes = ax_bytes(bk, P.view, Ndofs, fp32 ? 4.0 : 8.0);
   if (nr > 1) Nbytes += (nr - 1) * (Ndofs * 4.0 + (double)P.view.Nlocal * 4.0);
   const double Nflops = ax_flops(bk, P.view) * nr;
-  std::string suffix = P.view.simplex ? "Element=Tri" : P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
+  std::string suffix = P.view.simplex ? (P.view.dim == 2 ? "Element=Tri" : "Element=Tet")
+                                       : P.view.dim == 2 ? "Element=Quad" : "Element=Hex";
   if (P.view.affine) suffix += ", Affine";
   std::printf(
       "%s: N=%2d, DOFs=%lld, elapsed=%4.4f, time per DOF=%1.2e, avg BW (GB/s)=%6.1f, avg GFLOPs=%6.1f, "

@@ -200,6 +200,20 @@ bool tri_basis(int N, TriBasis& b);
 bool box_tri(HostMesh& m, const TriBasis& b, std::vector<double>& wJ, std::vector<double>& ggeo);
 // physical node coordinates of the Tri2D box [E*Np] each (meshPhysicalNodesTri2D.cpp)
 void tri_nodes_xy(const HostMesh& m, const TriBasis& b, std::vector<double>& x, std::vector<double>& y);
+// Tet3D (dim 3, simplex): reference element (r, s, t; Dr, Ds, Dt, MM; S = Srr,
+// Srs, Srt, Sss, Sst, Stt, row-major) and the box of six tetrahedra per cell
+// with its affine factors (wJ [E], ggeo [6E]), numbering (HostMesh EX/EY/EZ hold
+// 4 vertices per element) and physical node coordinates
+struct TetBasis {
+  int N = 0, Np = 0;
+  std::vector<double> r, s, t;
+  std::vector<int> bary;              // [Np*4] lattice weights of the nodes on the vertices
+  std::vector<double> Dr, Ds, Dt, MM;
+  std::vector<double> S;              // [6*Np*Np]
+};
+bool tet_basis(int N, TetBasis& b);
+bool box_tet(HostMesh& m, const TetBasis& b, std::vector<double>& wJ, std::vector<double>& ggeo,
+             std::vector<double>& x, std::vector<double>& y, std::vector<double>& z);
 
 // trilinear map of the eight hex vertices v (mesh_t vertex order) at (r,s,t)
 __host__ __device__ inline double trilinear(const double* v, double r, double s, double t) {
@@ -215,7 +229,7 @@ __host__ __device__ inline double trilinear(const double* v, double r, double s,
 struct bp_mesh_s {
   int N, Nq, Np, E, Nfields, affine;
   int dim = 3;                                  // 2: Quad2D, or Tri2D when simplex
-  int simplex = 0;                              // 1: Tri2D (affine triangles)
+  int simplex = 0;                              // 1: Tri2D (dim 2) or Tet3D (dim 3), affine
   int32_t Ngather, nnz;
   bp::DeviceArray<int32_t> elementList, G2L, rowStarts, colIds;
   // GlobalToLocal with the owner bit (kOwnerBit) of each gathered node's first
@@ -228,10 +242,11 @@ struct bp_mesh_s {
   bp::DeviceArray<double> cubDV;                // derivative columns for the diagonal: cubD*cubInterp
                                                 // (curved) or cubDmodal*invV (affine)
   bp::DeviceArray<double> cubwJ_c, cubggeo_c;   // curved mesh only
-  // Tri2D: Srr, Srs, Sss [3*Np*Np] node-fastest (X[k*Np + n] weighs node k in
-  // output n); MM above holds the triangle mass matrix and D [2*Np*Np] Dr, Ds
+  // simplex: the stiffness matrices S_ab [3 or 6 Np*Np] node-fastest (X[k*Np + n]
+  // weighs node k in output n); MM above holds the element mass matrix and D
+  // the derivative matrices
   bp::DeviceArray<double> S;
-  bp::DeviceArray<double> x, y;                 // Tri2D: physical node coordinates [E*Np]
+  bp::DeviceArray<double> x, y, z;              // simplex: physical node coordinates [E*Np]
   // factors at the quadrature points: curved [E*cubNp], [6*E*cubNp]; affine the
   // per-element wJ and ggeo
   const double* cubwJ() const { return affine ? wJ.ptr : cubwJ_c.ptr; }
@@ -247,20 +262,23 @@ struct bp_mesh_s {
 
 struct bp_solver_s;
 
-// ---- Tri2D (bp_ax_tri.cu) ----
+// ---- simplex elements: Tri2D (dim 2), Tet3D (dim 3) (bp_ax_simplex.cu) ----
 namespace bp {
-int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const double* wJ,
-                  const double* ggeo, const double* S, const double* MM, double lambda, const double* q, double* Aq,
-                  const int* skip, cudaStream_t s, double* partials = nullptr, int* nblocks = nullptr);
-int launch_ax_tri(int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L, const float* wJ,
-                  const float* ggeo, const float* S, const float* MM, float lambda, const float* q, float* Aq,
-                  const int* skip, cudaStream_t s, double* partials = nullptr, int* nblocks = nullptr);
-int launch_mass_local_tri(int N, int32_t Nelements, const int32_t* G2L, const double* wJ, const double* MM,
-                          const double* f, double* bL, cudaStream_t s);
-int launch_diag_local_tri(int N, int32_t Nelements, const double* wJ, const double* ggeo, const double* S,
-                          const double* MM, double lambda, double* dL, cudaStream_t s);
-int launch_rhs_analytic_tri(int N, int32_t Nelements, const double* wJ, const double* MM, const double* x,
-                            const double* y, double lambda, double* bL, cudaStream_t s);
+int launch_ax_simplex(int dim, int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                      const double* wJ, const double* ggeo, const double* S, const double* MM, double lambda,
+                      const double* q, double* Aq, const int* skip, cudaStream_t s, double* partials = nullptr,
+                      int* nblocks = nullptr);
+int launch_ax_simplex(int dim, int N, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
+                      const float* wJ, const float* ggeo, const float* S, const float* MM, float lambda,
+                      const float* q, float* Aq, const int* skip, cudaStream_t s, double* partials = nullptr,
+                      int* nblocks = nullptr);
+int launch_mass_local_simplex(int dim, int N, int32_t Nelements, const int32_t* G2L, const double* wJ,
+                              const double* MM, const double* f, double* bL, cudaStream_t s);
+int launch_diag_local_simplex(int dim, int N, int32_t Nelements, const double* wJ, const double* ggeo,
+                              const double* S, const double* MM, double lambda, double* dL, cudaStream_t s);
+int launch_rhs_analytic_simplex(int dim, int N, int32_t Nelements, const double* wJ, const double* MM,
+                                const double* x, const double* y, const double* z, double lambda, double* bL,
+                                cudaStream_t s);
 }  // namespace bp
 
 // ---- kernel launchers (bp_kernels.cu) ----

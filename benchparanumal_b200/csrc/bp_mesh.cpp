@@ -16,8 +16,10 @@
 // Here those orders follow from the lattice coordinates, so every element is
 // handled independently (OpenMP over elements) with no sort.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <limits>
+#include <map>
 #include <numeric>
 #include <unordered_map>
 
@@ -722,6 +724,322 @@ void tri_nodes_xy(const HostMesh& m, const TriBasis& b, std::vector<double>& x, 
   }
 }
 
+// ---- Tet3D ----------------------------------------------------------------
+
+// the 2D warp of one face of the tetrahedron, in its two tangential directions
+// (WarpShiftFace3D, meshBasisTet3D.cpp:604-645)
+static void face_warp(int N, double alpha, double L1, double L2, double L3, const std::vector<double>& gll,
+                      const std::vector<double>& req, double& w1, double& w2) {
+  auto warp = [&](double x) {
+    std::vector<double> I;
+    interp_matrix(req, std::vector<double>{x}, I);
+    double v = 0.0;
+    for (int i = 0; i <= N; ++i) v += I[i] * (gll[i] - req[i]);
+    const double inside = std::fabs(x) < 1.0 - 1.0e-10 ? 1.0 : 0.0;
+    const double sf = 1.0 - (inside * x) * (inside * x);
+    return v / sf + v * (inside - 1.0);
+  };
+  const double pi = 3.14159265358979323846;
+  const double a = 4 * L2 * L3 * warp(L3 - L2) * (1 + alpha * alpha * L1 * L1);
+  const double b = 4 * L3 * L1 * warp(L1 - L3) * (1 + alpha * alpha * L2 * L2);
+  const double c = 4 * L1 * L2 * warp(L2 - L1) * (1 + alpha * alpha * L3 * L3);
+  w1 = a + std::cos(2 * pi / 3) * b + std::cos(4 * pi / 3) * c;
+  w2 = std::sin(2 * pi / 3) * b + std::sin(4 * pi / 3) * c;
+}
+
+// Warp & blend nodes of the tetrahedron (Warburton 2006; meshBasisTet3D.cpp:
+// 227-248, 647-763): equispaced (r, s, t) layers in the reference's order, the
+// face warps along each face's unit tangents blended by Lb Lc Ld (with the
+// alpha of each degree), a face's own warp on its edges, mapped back from the
+// equilateral tetrahedron.  Also the nodes' lattice weights on the vertices.
+static void tet_nodes(int N, TetBasis& b) {
+  static const double alpha_opt[15] = {0.0000, 0.0000, 0.00000, 0.1002, 1.1332, 1.5608, 1.3413, 1.2577,
+                                       1.1603, 1.10153, 0.6080, 0.4523, 0.8856, 0.8717, 0.9655};
+  const double alpha = N < 16 ? alpha_opt[N - 1] : 1.0;
+  const double r3 = std::sqrt(3.0), r6 = std::sqrt(6.0);
+  const double v[4][3] = {{-1.0, -1 / r3, -1 / r6}, {1.0, -1 / r3, -1 / r6}, {0.0, 2 / r3, -1 / r6}, {0.0, 0.0, 3 / r6}};
+  double t1[4][3], t2[4][3];
+  for (int i = 0; i < 3; ++i) {
+    t1[0][i] = v[1][i] - v[0][i];
+    t1[1][i] = v[1][i] - v[0][i];
+    t1[2][i] = v[2][i] - v[1][i];
+    t1[3][i] = v[2][i] - v[0][i];
+    t2[0][i] = v[2][i] - 0.5 * (v[0][i] + v[1][i]);
+    t2[1][i] = v[3][i] - 0.5 * (v[0][i] + v[1][i]);
+    t2[2][i] = v[3][i] - 0.5 * (v[1][i] + v[2][i]);
+    t2[3][i] = v[3][i] - 0.5 * (v[0][i] + v[2][i]);
+  }
+  for (int f = 0; f < 4; ++f) {
+    const double n1 = std::sqrt(t1[f][0] * t1[f][0] + t1[f][1] * t1[f][1] + t1[f][2] * t1[f][2]);
+    const double n2 = std::sqrt(t2[f][0] * t2[f][0] + t2[f][1] * t2[f][1] + t2[f][2] * t2[f][2]);
+    for (int i = 0; i < 3; ++i) {
+      t1[f][i] /= n1;
+      t2[f][i] /= n2;
+    }
+  }
+  std::vector<double> gll, w, req(N + 1);
+  gll_nodes_weights(N, gll, w);
+  for (int i = 0; i <= N; ++i) req[i] = -1.0 + 2.0 * i / N;
+  b.r.clear(); b.s.clear(); b.t.clear(); b.bary.clear();
+  for (int k = 0; k <= N; ++k)
+    for (int n = 0; n + k <= N; ++n)
+      for (int m = 0; m + n + k <= N; ++m) {
+        const double r = -1.0 + 2.0 * m / N, s = -1.0 + 2.0 * n / N, t = -1.0 + 2.0 * k / N;
+        const double L[4] = {0.5 * (1 + t), 0.5 * (1 + s), -0.5 * (1 + r + s + t), 0.5 * (1 + r)};   // L1..L4
+        double X[3];
+        for (int i = 0; i < 3; ++i) X[i] = L[2] * v[0][i] + L[3] * v[1][i] + L[1] * v[2][i] + L[0] * v[3][i];
+        double sh[3] = {0, 0, 0};
+        static const int perm[4][4] = {{0, 1, 2, 3}, {1, 0, 2, 3}, {2, 0, 3, 1}, {3, 0, 2, 1}};   // La, Lb, Lc, Ld
+        for (int f = 0; f < 4; ++f) {
+          const double La = L[perm[f][0]], Lb = L[perm[f][1]], Lc = L[perm[f][2]], Ld = L[perm[f][3]];
+          double w1, w2;
+          face_warp(N, alpha, Lb, Lc, Ld, gll, req, w1, w2);
+          double blend = Lb * Lc * Ld;
+          const double denom = (Lb + 0.5 * La) * (Lc + 0.5 * La) * (Ld + 0.5 * La);
+          if (denom > 1.0e-10) blend = (1 + (alpha * La) * (alpha * La)) * blend / denom;
+          for (int i = 0; i < 3; ++i) sh[i] += (blend * w1) * t1[f][i] + (blend * w2) * t2[f][i];
+          if (La < 1.0e-10 && (Lb < 1.0e-10 || Lc < 1.0e-10 || Ld < 1.0e-10))
+            for (int i = 0; i < 3; ++i) sh[i] = w1 * t1[f][i] + w2 * t2[f][i];
+        }
+        for (int i = 0; i < 3; ++i) X[i] += sh[i];
+        // back to (r, s, t): X - c = r a1 + s a2 + t a3, a_j = (v_{j+1} - v_0)/2
+        double A[9], B[3];
+        for (int i = 0; i < 3; ++i) {
+          A[i * 3 + 0] = 0.5 * (v[1][i] - v[0][i]);
+          A[i * 3 + 1] = 0.5 * (v[2][i] - v[0][i]);
+          A[i * 3 + 2] = 0.5 * (v[3][i] - v[0][i]);
+          B[i] = X[i] - 0.5 * (v[1][i] + v[2][i] + v[3][i] - v[0][i]);
+        }
+        std::vector<double> Ai(A, A + 9);
+        invert(3, Ai);
+        b.r.push_back(Ai[0] * B[0] + Ai[1] * B[1] + Ai[2] * B[2]);
+        b.s.push_back(Ai[3] * B[0] + Ai[4] * B[1] + Ai[5] * B[2]);
+        b.t.push_back(Ai[6] * B[0] + Ai[7] * B[1] + Ai[8] * B[2]);
+        const int bw[4] = {N - m - n - k, m, n, k};   // on vertices (-1,-1,-1), r = 1, s = 1, t = 1
+        b.bary.insert(b.bary.end(), bw, bw + 4);
+      }
+}
+
+// Reference-element matrices of the tetrahedron: the Vandermonde (and its r,
+// s, t derivatives) of the orthonormal basis of P_N in collapsed coordinates,
+// Dr, Ds, Dt = Vr,s,t V^-1, MM = (V V^T)^-1, and the six stiffness matrices
+// S_ab = Da^T MM Db (+ Db^T MM Da for a != b) (meshBasisTet3D.cpp:494-527).
+bool tet_basis(int N, TetBasis& b) {
+  const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
+  b.N = N;
+  b.Np = Np;
+  tet_nodes(N, b);
+  std::vector<double> V((size_t)Np * Np), Vr(V.size()), Vs(V.size()), Vt(V.size());
+  for (int p = 0; p < Np; ++p) {
+    const double r = b.r[p], s = b.s[p], t = b.t[p];
+    const double a = std::fabs(s + t) > 1e-14 ? 2 * (1 + r) / (-s - t) - 1 : -1.0;
+    const double bb = std::fabs(t - 1) > 1e-14 ? 2 * (1 + s) / (1 - t) - 1 : -1.0;
+    const double c = t;
+    int col = 0;
+    for (int i = 0; i <= N; ++i)
+      for (int j = 0; i + j <= N; ++j)
+        for (int k = 0; i + j + k <= N; ++k, ++col) {
+          const double fa = jacobi_on(a, 0, 0, i), dfa = jacobi_on_deriv(a, 0, 0, i);
+          const double gb = jacobi_on(bb, 2 * i + 1, 0, j), dgb = jacobi_on_deriv(bb, 2 * i + 1, 0, j);
+          const double hc = jacobi_on(c, 2 * (i + j) + 2, 0, k), dhc = jacobi_on_deriv(c, 2 * (i + j) + 2, 0, k);
+          const double hb = 0.5 * (1 - bb), hcc = 0.5 * (1 - c);
+          V[(size_t)p * Np + col] = 2 * std::sqrt(2.0) * fa * gb * std::pow(1 - bb, i) * hc * std::pow(1 - c, i + j);
+          double dr = dfa * gb * hc;
+          if (i > 0) dr *= std::pow(hb, i - 1);
+          if (i + j > 0) dr *= std::pow(hcc, i + j - 1);
+          double ds = 0.5 * (1 + a) * dr;
+          double tmp = dgb * std::pow(hb, i);
+          if (i > 0) tmp -= 0.5 * i * gb * std::pow(hb, i - 1);
+          if (i + j > 0) tmp *= std::pow(hcc, i + j - 1);
+          tmp = fa * tmp * hc;
+          ds += tmp;
+          double dt = 0.5 * (1 + a) * dr + 0.5 * (1 + bb) * tmp;
+          tmp = dhc * std::pow(hcc, i + j);
+          if (i + j > 0) tmp -= 0.5 * (i + j) * hc * std::pow(hcc, i + j - 1);
+          tmp = fa * gb * tmp * std::pow(hb, i);
+          dt += tmp;
+          const double sc = std::pow(2.0, 2 * i + j + 1.5);
+          Vr[(size_t)p * Np + col] = dr * sc;
+          Vs[(size_t)p * Np + col] = ds * sc;
+          Vt[(size_t)p * Np + col] = dt * sc;
+        }
+  }
+  std::vector<double> Vi = V;
+  if (!invert(Np, Vi)) return false;
+  auto mul = [Np](const std::vector<double>& A, const std::vector<double>& B, bool ta) {
+    std::vector<double> C((size_t)Np * Np, 0.0);
+    for (int i = 0; i < Np; ++i)
+      for (int k = 0; k < Np; ++k) {
+        const double aik = ta ? A[(size_t)k * Np + i] : A[(size_t)i * Np + k];
+        if (aik == 0.0) continue;
+        for (int j = 0; j < Np; ++j) C[(size_t)i * Np + j] += aik * B[(size_t)k * Np + j];
+      }
+    return C;
+  };
+  b.Dr = mul(Vr, Vi, false);
+  b.Ds = mul(Vs, Vi, false);
+  b.Dt = mul(Vt, Vi, false);
+  std::vector<double> VVt((size_t)Np * Np, 0.0);
+  for (int i = 0; i < Np; ++i)
+    for (int j = 0; j < Np; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < Np; ++k) acc += V[(size_t)i * Np + k] * V[(size_t)j * Np + k];
+      VVt[(size_t)i * Np + j] = acc;
+    }
+  if (!invert(Np, VVt)) return false;
+  b.MM = VVt;
+  const std::vector<double>* D[3] = {&b.Dr, &b.Ds, &b.Dt};
+  std::vector<double> MD[3];
+  for (int a = 0; a < 3; ++a) MD[a] = mul(b.MM, *D[a], false);
+  static const int pairs[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  const size_t NP2 = (size_t)Np * Np;
+  b.S.assign(6 * NP2, 0.0);
+  for (int q = 0; q < 6; ++q) {
+    const int a = pairs[q][0], c = pairs[q][1];
+    std::vector<double> X = mul(*D[a], MD[c], true);
+    if (a != c) {
+      const std::vector<double> Y = mul(*D[c], MD[a], true);
+      for (size_t k = 0; k < NP2; ++k) X[k] += Y[k];
+    }
+    std::copy(X.begin(), X.end(), b.S.begin() + q * NP2);
+  }
+  return true;
+}
+
+// Tet3D box (meshSetupBoxTet3D.cpp): cell (i, j, k) holds tetrahedra
+// 6(i + j nx + k nx ny) + 0..5 on the cell corners (0,3,2,7), (0,1,3,7),
+// (0,2,6,7), (0,6,4,7), (0,5,1,7), (0,4,5,7) (corner bits: x, y, z); affine
+// factors per element (wJ = J; ggeo = J grad a . grad b for ab = rr, rs, rt,
+// ss, st, tt; meshGeometricFactorsTet3D.cpp:31-110); the masked numbering as
+// for Tri2D, a node identified by its lattice weights on the global vertices;
+// boundary faces 0..3 (t = -1, s = -1, r + s + t = -1, r = -1).  Returns false
+// on a non-positive Jacobian.
+bool box_tet(HostMesh& m, const TetBasis& b, std::vector<double>& wJ, std::vector<double>& ggeo,
+             std::vector<double>& x, std::vector<double>& y, std::vector<double>& z) {
+  static const int tets[6][4] = {{0, 3, 2, 7}, {0, 1, 3, 7}, {0, 2, 6, 7}, {0, 6, 4, 7}, {0, 5, 1, 7}, {0, 4, 5, 7}};
+  const int nx = m.nx, ny = m.ny, nz = m.nz, N = b.N, Np = b.Np, E = m.E;
+  const int64_t NnX = nx + 1, NnY = ny + 1;
+  const double dx = 2.0 / nx, dy = 2.0 / ny, dz = 2.0 / nz;
+  std::vector<int64_t> EToV((size_t)E * 4);
+  m.EX.resize((size_t)E * 4);
+  m.EY.resize((size_t)E * 4);
+  m.EZ.resize((size_t)E * 4);
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double x0 = -1.0 + dx * i, y0 = -1.0 + dy * j, z0 = -1.0 + dz * k;
+        for (int q = 0; q < 6; ++q) {
+          const int e = 6 * (i + j * nx + k * nx * ny) + q;
+          for (int c = 0; c < 4; ++c) {
+            const int cn = tets[q][c], ci = cn & 1, cj = (cn >> 1) & 1, ck = (cn >> 2) & 1;
+            EToV[(size_t)e * 4 + c] = (i + ci) + (j + cj) * NnX + (k + ck) * NnX * NnY;
+            m.EX[(size_t)e * 4 + c] = ci ? x0 + dx : x0;
+            m.EY[(size_t)e * 4 + c] = cj ? y0 + dy : y0;
+            m.EZ[(size_t)e * 4 + c] = ck ? z0 + dz : z0;
+          }
+        }
+      }
+  wJ.resize(E);
+  ggeo.resize((size_t)6 * E);
+  x.resize((size_t)E * Np);
+  y.resize((size_t)E * Np);
+  z.resize((size_t)E * Np);
+  for (int e = 0; e < E; ++e) {
+    const double* X = &m.EX[(size_t)e * 4];
+    const double* Y = &m.EY[(size_t)e * 4];
+    const double* Z = &m.EZ[(size_t)e * 4];
+    const double xr = 0.5 * (X[1] - X[0]), xs = 0.5 * (X[2] - X[0]), xt = 0.5 * (X[3] - X[0]);
+    const double yr = 0.5 * (Y[1] - Y[0]), ys = 0.5 * (Y[2] - Y[0]), yt = 0.5 * (Y[3] - Y[0]);
+    const double zr = 0.5 * (Z[1] - Z[0]), zs = 0.5 * (Z[2] - Z[0]), zt = 0.5 * (Z[3] - Z[0]);
+    const double J = xr * (ys * zt - zs * yt) - yr * (xs * zt - zs * xt) + zr * (xs * yt - ys * xt);
+    if (!(J > 0.0)) return false;
+    const double rx = (ys * zt - zs * yt) / J, ry = -(xs * zt - zs * xt) / J, rz = (xs * yt - ys * xt) / J;
+    const double sx = -(yr * zt - zr * yt) / J, sy = (xr * zt - zr * xt) / J, sz = -(xr * yt - yr * xt) / J;
+    const double tx = (yr * zs - zr * ys) / J, ty = -(xr * zs - zr * xs) / J, tz = (xr * ys - yr * xs) / J;
+    wJ[e] = J;
+    double* g = &ggeo[(size_t)6 * e];
+    g[0] = J * (rx * rx + ry * ry + rz * rz);
+    g[1] = J * (rx * sx + ry * sy + rz * sz);
+    g[2] = J * (rx * tx + ry * ty + rz * tz);
+    g[3] = J * (sx * sx + sy * sy + sz * sz);
+    g[4] = J * (sx * tx + sy * ty + sz * tz);
+    g[5] = J * (tx * tx + ty * ty + tz * tz);
+    for (int n = 0; n < Np; ++n) {
+      const double r = b.r[n], s = b.s[n], t = b.t[n];
+      const double w[4] = {-0.5 * (1 + r + s + t), 0.5 * (1 + r), 0.5 * (1 + s), 0.5 * (1 + t)};
+      double px = 0, py = 0, pz = 0;
+      for (int c = 0; c < 4; ++c) {
+        px += w[c] * X[c];
+        py += w[c] * Y[c];
+        pz += w[c] * Z[c];
+      }
+      x[(size_t)e * Np + n] = px;
+      y[(size_t)e * Np + n] = py;
+      z[(size_t)e * Np + n] = pz;
+    }
+  }
+  // a node's identity: its nonzero lattice weights on global vertex ids
+  const int64_t NL = (int64_t)E * Np;
+  std::map<std::array<int64_t, 4>, int64_t> cls;
+  std::vector<int64_t> key((size_t)NL);
+  for (int e = 0; e < E; ++e)
+    for (int n = 0; n < Np; ++n) {
+      std::array<int64_t, 4> k4;
+      int cnt = 0;
+      for (int c = 0; c < 4; ++c)
+        if (b.bary[(size_t)n * 4 + c] > 0) k4[cnt++] = EToV[(size_t)e * 4 + c] * (N + 1) + b.bary[(size_t)n * 4 + c];
+      std::sort(k4.begin(), k4.begin() + cnt);
+      for (int c = cnt; c < 4; ++c) k4[c] = -1;
+      auto it = cls.emplace(k4, (int64_t)cls.size()).first;
+      key[(size_t)e * Np + n] = it->second;
+    }
+  // copies on boundary faces are masked
+  const double tol = 1.0e-5;
+  std::vector<std::vector<int>> fn(4);
+  for (int n = 0; n < Np; ++n) {
+    const double r = b.r[n], s = b.s[n], t = b.t[n];
+    if (std::fabs(t + 1) < tol) fn[0].push_back(n);
+    if (std::fabs(s + 1) < tol) fn[1].push_back(n);
+    if (std::fabs(r + s + t + 1) < tol) fn[2].push_back(n);
+    if (std::fabs(r + 1) < tol) fn[3].push_back(n);
+  }
+  static const int fv[4][3] = {{0, 1, 2}, {0, 1, 3}, {1, 2, 3}, {0, 2, 3}};
+  std::vector<char> masked((size_t)NL, 0);
+  auto at = [](double v, double w) { return std::fabs(v - w) < 1.0e-12; };
+  for (int e = 0; e < E; ++e) {
+    const double* C[3] = {&m.EX[(size_t)e * 4], &m.EY[(size_t)e * 4], &m.EZ[(size_t)e * 4]};
+    for (int f = 0; f < 4; ++f) {
+      bool bnd = false;
+      for (int d = 0; d < 3 && !bnd; ++d)
+        for (double side : {-1.0, 1.0})
+          if (at(C[d][fv[f][0]], side) && at(C[d][fv[f][1]], side) && at(C[d][fv[f][2]], side)) bnd = true;
+      if (bnd)
+        for (int n : fn[f]) masked[(size_t)e * Np + n] = 1;
+    }
+  }
+  std::vector<int32_t> row(cls.size(), -1), count;
+  m.G2L.assign((size_t)NL, -1);
+  for (int64_t l = 0; l < NL; ++l) {
+    if (masked[(size_t)l]) continue;
+    int32_t& rw = row[(size_t)key[(size_t)l]];
+    if (rw < 0) {
+      rw = (int32_t)count.size();
+      count.push_back(0);
+    }
+    m.G2L[(size_t)l] = rw;
+    ++count[rw];
+  }
+  m.Ngather = (int32_t)count.size();
+  m.rowStarts.assign((size_t)m.Ngather + 1, 0);
+  for (int32_t r = 0; r < m.Ngather; ++r) m.rowStarts[r + 1] = m.rowStarts[r] + count[r];
+  m.nnz = m.rowStarts[m.Ngather];
+  m.colIds.assign((size_t)m.nnz, 0);
+  std::vector<int32_t> fill(m.rowStarts.begin(), m.rowStarts.end() - 1);
+  for (int64_t l = 0; l < NL; ++l)
+    if (m.G2L[(size_t)l] >= 0) m.colIds[(size_t)fill[m.G2L[(size_t)l]]++] = (int32_t)l;
+  return true;
+}
+
 // GeometricFactorsQuad2D (meshGeometricFactorsQuad2D.cpp:31-120) from the
 // bilinear map of the vertices at the GLL nodes (meshPhysicalNodesQuad2D.cpp)
 bool quad_geometry(const HostMesh& m, std::vector<double>& wJ, std::vector<double>& ggeo) {
@@ -794,11 +1112,13 @@ int host_mesh_from_desc(const bp_box_desc_t* d, bp::HostMesh& m) {
   if (d->dim != 0 && d->dim != 2 && d->dim != 3) return bp::fail(BP_ERROR_ARG, "box dim must be 2 or 3");
   m.dim = d->dim == 2 ? 2 : 3;
   if (d->simplex) {
-    if (m.dim != 2 || d->nx < 1 || d->ny < 1 || d->N < 1 || d->N > 15 || d->Nfields != 1)
-      return bp::fail(BP_ERROR_ARG, "bad Tri2D box descriptor");
-    m.N = d->N; m.Nq = d->N + 1; m.Np = (d->N + 1) * (d->N + 2) / 2;
-    m.nx = d->nx; m.ny = d->ny; m.nz = 1;
-    const int64_t E = 2 * (int64_t)d->nx * d->ny;
+    const int nzs = m.dim == 2 ? 1 : d->nz;
+    if (d->nx < 1 || d->ny < 1 || nzs < 1 || d->N < 1 || d->N > 15 || d->Nfields != 1)
+      return bp::fail(BP_ERROR_ARG, "bad simplex box descriptor");
+    m.N = d->N; m.Nq = d->N + 1;
+    m.Np = m.dim == 2 ? (d->N + 1) * (d->N + 2) / 2 : (d->N + 1) * (d->N + 2) * (d->N + 3) / 6;
+    m.nx = d->nx; m.ny = d->ny; m.nz = nzs;
+    const int64_t E = (m.dim == 2 ? 2 : 6) * (int64_t)d->nx * d->ny * nzs;
     if (E * m.Np >= (int64_t)INT32_MAX) return bp::fail(BP_ERROR_ARG, "local node count exceeds int32");
     m.E = (int)E; m.affine = 1; m.Nfields = 1;
     return BP_SUCCESS;
@@ -821,7 +1141,12 @@ extern "C" int bp_box_numbering(const bp_box_desc_t* d, int32_t* Ngather, int32_
   bp::HostMesh m;
   int rc = host_mesh_from_desc(d, m);
   if (rc) return rc;
-  if (d->simplex) {
+  if (d->simplex && m.dim == 3) {
+    bp::TetBasis tb;
+    std::vector<double> wJ, ggeo, x, y, z;
+    if (!bp::tet_basis(m.N, tb) || !bp::box_tet(m, tb, wJ, ggeo, x, y, z))
+      return bp::fail(BP_ERROR_NUMERIC, "bp_box_numbering: Tet3D set-up failed");
+  } else if (d->simplex) {
     bp::TriBasis tb;
     std::vector<double> wJ, ggeo;
     if (!bp::tri_basis(m.N, tb) || !bp::box_tri(m, tb, wJ, ggeo))
@@ -872,6 +1197,30 @@ extern "C" int bp_basis_tri2d(int32_t N, double* r, double* s, double* D, double
       const std::vector<double> blk(tb.S.begin() + b * NP2, tb.S.begin() + (b + 1) * NP2);
       put(blk, S, b * NP2);
     }
+  return BP_SUCCESS;
+}
+
+extern "C" int bp_basis_tet3d(int32_t N, double* r, double* s, double* t, double* D, double* MM, double* S) {
+  if (N < 1 || N > 15) return bp::fail(BP_ERROR_ARG, "bp_basis_tet3d: degree must be in 1..15");
+  bp::TetBasis tb;
+  if (!bp::tet_basis(N, tb)) return bp::fail(BP_ERROR_NUMERIC, "bp_basis_tet3d: singular Vandermonde matrix");
+  const int Np = tb.Np;
+  const size_t NP2 = (size_t)Np * Np;
+  auto put = [&](const double* rm, double* out) {   // node-fastest
+    for (int n = 0; n < Np; ++n)
+      for (int k = 0; k < Np; ++k) out[(size_t)k * Np + n] = rm[(size_t)n * Np + k];
+  };
+  if (r) std::copy(tb.r.begin(), tb.r.end(), r);
+  if (s) std::copy(tb.s.begin(), tb.s.end(), s);
+  if (t) std::copy(tb.t.begin(), tb.t.end(), t);
+  if (D) {
+    put(tb.Dr.data(), D);
+    put(tb.Ds.data(), D + NP2);
+    put(tb.Dt.data(), D + 2 * NP2);
+  }
+  if (MM) std::copy(tb.MM.begin(), tb.MM.end(), MM);
+  if (S)
+    for (int q = 0; q < 6; ++q) put(tb.S.data() + q * NP2, S + q * NP2);
   return BP_SUCCESS;
 }
 

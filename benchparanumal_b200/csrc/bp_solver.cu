@@ -685,8 +685,8 @@ template <class V>
 static int elem_apply(bp_solver_s* S, const ElemOperands<V>& o, const V* q, V* AqL, const int* skip, cudaStream_t s,
                       const CgFuse* fuse = nullptr, int* nblocks = nullptr) {
   bp_mesh_s* m = S->mesh;
-  if (m->simplex)   // Tri2D: D carries the stiffness matrices S, T the mass matrix
-    return launch_ax_tri(m->N, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, o.T, (V)S->lambda, q, AqL,
+  if (m->simplex)   // Tri2D, Tet3D: D carries the stiffness matrices S, T the mass matrix
+    return launch_ax_simplex(m->dim, m->N, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.D, o.T, (V)S->lambda, q, AqL,
                          skip, s, fuse ? fuse->partials : nullptr, nblocks);
   if (S->bp >= 5)
     return launch_ax_skip(S->ax, m->E, m->elementList.ptr, m->G2L.ptr, o.wJ, o.ggeo, o.gllw, o.D, (V)S->lambda, q,
@@ -1015,7 +1015,7 @@ int bp_solver_create(bp_mesh_t mesh, const bp_solver_desc_t* d, bp_solver_t* out
   *out = nullptr;
   if (d->bp < 1 || d->bp > 6) return fail(BP_ERROR_ARG, "bp_solver_create: bp must be 1..6");
   if (mesh->simplex) {
-    if (d->bp != 5) return fail(BP_ERROR_ARG, "bp_solver_create: Tri2D meshes take BP5");
+    if (d->bp != 5) return fail(BP_ERROR_ARG, "bp_solver_create: Tri2D and Tet3D meshes take BP5");
   } else if (mesh->dim == 2) {
     if (d->bp < 5) return fail(BP_ERROR_ARG, "bp_solver_create: Quad2D meshes take BP5 and BP6 (the BP1-BP4 forms are Hex3D only)");
     if ((d->bp == 6) != (mesh->Nfields == 2))
@@ -1116,7 +1116,8 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
     // BP1/BP2 force with lambda = 0 (BP/BP1/src/bp1Run.cpp:54-62)
     const double lam = S->bp <= 2 ? 0.0 : S->lambda;
     if (m->simplex)
-      BP_TRY(launch_rhs_analytic_tri(m->N, m->E, m->wJ.ptr, m->MM.ptr, m->x.ptr, m->y.ptr, lam, S->AqL.ptr, s));
+      BP_TRY(launch_rhs_analytic_simplex(m->dim, m->N, m->E, m->wJ.ptr, m->MM.ptr, m->x.ptr, m->y.ptr, m->z.ptr, lam,
+                                         S->AqL.ptr, s));
     else if (m->dim == 2)
       BP_TRY(launch_rhs_analytic_quad(m->N, m->affine, m->Nfields, m->E, m->EX.ptr, m->EY.ptr, m->gllz.ptr,
                                       m->gllw.ptr, m->wJ.ptr, lam, S->AqL.ptr, s));
@@ -1132,7 +1133,7 @@ int bp_solver_rhs(bp_solver_t S, int32_t mode, uint64_t seed, double* b, double*
     }
     BP_TRY(launch_rhs_random(S->N, seed, f, s));
     if (m->simplex)
-      BP_TRY(launch_mass_local_tri(m->N, m->E, m->G2L.ptr, m->wJ.ptr, m->MM.ptr, f, S->AqL.ptr, s));
+      BP_TRY(launch_mass_local_simplex(m->dim, m->N, m->E, m->G2L.ptr, m->wJ.ptr, m->MM.ptr, f, S->AqL.ptr, s));
     else if (m->dim == 2)
       BP_TRY(launch_mass_local_quad(m->N, m->affine, m->Nfields, m->E, m->G2L.ptr, m->gllw.ptr, m->wJ.ptr, f,
                                     S->AqL.ptr, s));
@@ -1155,7 +1156,8 @@ int bp_solver_diagonal(bp_solver_t S, double* diag) {
   bp_mesh_s* m = S->mesh;
   cudaStream_t s = default_stream();
   if (m->simplex) {
-    BP_TRY(launch_diag_local_tri(m->N, m->E, m->wJ.ptr, m->ggeo.ptr, m->S.ptr, m->MM.ptr, S->lambda, S->AqL.ptr, s));
+    BP_TRY(launch_diag_local_simplex(m->dim, m->N, m->E, m->wJ.ptr, m->ggeo.ptr, m->S.ptr, m->MM.ptr, S->lambda,
+                                     S->AqL.ptr, s));
   } else if (S->bp >= 5 && m->dim == 2) {
     BP_TRY(launch_diag_local_quad(m->N, m->affine, m->Nfields, m->E, m->ggeo.ptr, m->wJ.ptr, m->gllw.ptr, m->D.ptr,
                                   S->lambda, S->AqL.ptr, s));

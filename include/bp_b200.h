@@ -113,6 +113,14 @@ int bp_ax_tri2d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elem
                 const int32_t* GlobalToLocal, const double* wJ, const double* ggeo, const double* S,
                 const double* MM, double lambda, const double* q, double* Aq, bp_stream_t stream);
 
+/* Tet3D affine stiffness + lambda*mass operator, A_e = sum_ab G_ab S_ab +
+   lambda J MM over ab = rr, rs, rt, ss, st, tt.  Replaces bp5AxAffineTet3D
+   (okl/bp5AxAffineTet3D.okl); desc: bp 5, N 1..15, affine 1, Nfields 1, dim 3.
+   wJ [E], ggeo [E*6], S [6*Np*Np] and MM [Np*Np] as in bp_mesh_view_t. */
+int bp_ax_tet3d(const bp_ax_desc_t* desc, int32_t Nelements, const int32_t* elementList,
+                const int32_t* GlobalToLocal, const double* wJ, const double* ggeo, const double* S,
+                const double* MM, double lambda, const double* q, double* Aq, bp_stream_t stream);
+
 /* The same operator in FP32 (the inner operator of the mixed-precision CG):
    all arrays FP32, dot products of the CG stay FP64.  No counterpart in the
    reference (dfloat is FP64 there, include/types.h:31-39). */
@@ -272,8 +280,10 @@ typedef struct bp_box_desc {
                            nx x ny (-e Quad, meshSetupBoxQuad2D.cpp:30-100; nz
                            ignored; Nfields 1 or 2)                                */
   int32_t simplex;      /* 1 with dim 2: Tri2D box (-e Tri, meshSetupBoxTri2D.cpp:
-                           30-107): two triangles per cell, affine, one field, no
-                           perturbation; 0 otherwise                              */
+                           30-107), two triangles per cell; 1 with dim 3: Tet3D
+                           box (-e Tet, meshSetupBoxTet3D.cpp), six tetrahedra
+                           per cell; affine, one field, no perturbation; 0
+                           otherwise                                               */
 } bp_box_desc_t;
 
 typedef struct bp_mesh_view {
@@ -296,13 +306,18 @@ typedef struct bp_mesh_view {
   const double* EZ;               /* NULL for Quad2D                              */
   int32_t dim;                    /* 3, or 2 for Quad2D: Np = Nq^2, ggeo [E*Np*3]
                                      (affine [E*3]), G00, G01, G11               */
-  int32_t simplex;                /* 1: Tri2D: Np = (N+1)(N+2)/2, affine: wJ [E],
-                                     ggeo [E*3] G00, G01, G11; EX, EY [E*3];
-                                     D [2*Np*Np] Dr, Ds; gllz, gllw NULL        */
-  const double* S;                /* Tri2D: Srr, Srs, Sss [3*Np*Np]; X[k*Np + n] is
-                                     the weight of node k in output n (the layout
-                                     of the reference's o_S, o_D); else NULL    */
-  const double* MM;               /* Tri2D: mass matrix [Np*Np] (symmetric)       */
+  int32_t simplex;                /* 1: Tri2D (dim 2): Np = (N+1)(N+2)/2, affine:
+                                     wJ [E], ggeo [E*3] G00, G01, G11; EX, EY
+                                     [E*3]; D [2*Np*Np] Dr, Ds.  Tet3D (dim 3):
+                                     Np = (N+1)(N+2)(N+3)/6, ggeo [E*6] G00, G01,
+                                     G02, G11, G12, G22; EX, EY, EZ [E*4]; D
+                                     [3*Np*Np].  gllz, gllw NULL               */
+  const double* S;                /* simplex: Srr, Srs, Sss [3*Np*Np] (Tri2D) or
+                                     Srr, Srs, Srt, Sss, Sst, Stt [6*Np*Np]
+                                     (Tet3D); X[k*Np + n] is the weight of node k
+                                     in output n (the layout of the reference's
+                                     o_S, o_D); else NULL                       */
+  const double* MM;               /* simplex: mass matrix [Np*Np] (symmetric)     */
 } bp_mesh_view_t;
 
 int bp_mesh_create(const bp_box_desc_t* desc, bp_mesh_t* mesh);
@@ -343,6 +358,11 @@ int bp_mesh_cubature_view(bp_mesh_t mesh, bp_cubature_view_t* view);
    MM [Np*Np], S [3*Np*Np] (Srr, Srs, Sss), node-fastest as in bp_mesh_view_t.
    Np = (N+1)(N+2)/2; any pointer may be NULL. */
 int bp_basis_tri2d(int32_t N, double* r, double* s, double* D, double* MM, double* S);
+/* Host-only Tet3D reference element of degree N (meshReferenceNodesTet3D.cpp,
+   meshBasisTet3D.cpp): warp & blend nodes r, s, t [Np]; D [3*Np*Np] (Dr, Ds,
+   Dt), MM [Np*Np], S [6*Np*Np] (Srr, Srs, Srt, Sss, Sst, Stt), node-fastest.
+   Np = (N+1)(N+2)(N+3)/6; any pointer may be NULL. */
+int bp_basis_tet3d(int32_t N, double* r, double* s, double* t, double* D, double* MM, double* S);
 
 /* Host-only 1D cubature data for degree N (meshCubatureSetupHex3D.cpp:31-51,
    meshBasis1D.cpp JacobiGQ / InterpolationMatrix1D / Dmatrix1D / MassMatrix1D):

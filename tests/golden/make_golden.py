@@ -46,6 +46,12 @@ CASES = {
     "tri_2x2_p15": (1, 15, "-e Tri -nx 2 -ny 2 -p 15 -a", False),
     "tri_5x4_p3": (1, 3, "-e Tri -nx 5 -ny 4 -p 3 -a", False),
     "tri_96x80_p5": (1, 0, "-e Tri -nx 96 -ny 80 -p 5 -a", True),
+    # Tet3D boxes (-e Tet, affine: six tetrahedra per cell)
+    "tet_2x2x1_p3": (1, 3, "-e Tet -nx 2 -ny 2 -nz 1 -p 3 -a", False),
+    "tet_3x2x2_p4": (1, 4, "-e Tet -nx 3 -ny 2 -nz 2 -p 4 -a", False),
+    "tet_2x1x2_p1": (1, 1, "-e Tet -nx 2 -ny 1 -nz 2 -p 1 -a", False),
+    "tet_2x2x2_p7": (1, 7, "-e Tet -nx 2 -ny 2 -nz 2 -p 7 -a", False),
+    "tet_12x10x8_p3": (1, 0, "-e Tet -nx 12 -ny 10 -nz 8 -p 3 -a", True),
 }
 INT_RECORDS = {"N", "Nq", "Np", "Nelements", "Nfields", "Ngather", "NgatherGlobal", "cubNq", "GlobalToLocal",
                "rowStartsT", "colIdsT", "rowStartsN", "colIdsN", "gllz", "gllw", "D"}
@@ -80,7 +86,7 @@ def main():
         tmp = os.path.join(ROOT, "oracle", "_ref", name + ".bin")
         subprocess.run([DUMP, tmp, str(nf), str(seed)] + cli.split(), check=True)
         d = read_dump(tmp)
-        if name.startswith("tri"):   # the Tri2D BP5 path uses no cubature data
+        if name.startswith(("tri", "tet")):   # the simplex BP5 paths use no cubature data
             d = {k: v for k, v in d.items() if not k.startswith("cub")}
         if ints_only:
             # full-size integer records as SHA-256 digests of their little-endian

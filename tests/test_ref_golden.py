@@ -25,8 +25,10 @@ import numpy as np
 import pytest
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-# Hex3D and Quad2D fixtures (the Tri2D ones, ref_tri_*, are read by tests/test_tri2d.py)
-FILES = sorted(f for f in glob.glob(os.path.join(GOLDEN, "ref_*.npz")) if not os.path.basename(f).startswith("ref_tri_"))
+# Hex3D and Quad2D fixtures (the simplex ones, ref_tri_* and ref_tet_*, are read by
+# tests/test_tri2d.py and tests/test_tet3d.py)
+FILES = sorted(f for f in glob.glob(os.path.join(GOLDEN, "ref_*.npz"))
+               if not os.path.basename(f).startswith(("ref_tri_", "ref_tet_")))
 FULL = [f for f in FILES if "sha256_GlobalToLocal" in np.load(f).files]
 SMALL = [f for f in FILES if f not in FULL]
 
