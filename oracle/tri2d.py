@@ -37,8 +37,14 @@ geometric factors, the numbering, the CSR and the host gather/scatter that
 tests/test_tri2d.py compares this restatement to.
 """
 import numpy as np
+from threadpoolctl import threadpool_limits
 
 from oracle import oracle as _o
+
+# One BLAS thread for the dense inverses and products here: a threaded BLAS
+# pool next to torch's OpenMP runtime in the same test process has deadlocked
+# in np.linalg.inv.
+threadpool_limits(limits=1, user_api="blas")
 
 ALPHA_OPT = [0.0000, 0.0000, 1.4152, 0.1001, 0.2751, 0.9800, 1.0999, 1.2832, 1.3648, 1.4773, 1.4959, 1.5743,
              1.5770, 1.6223, 1.6258]
