@@ -177,12 +177,14 @@ struct TmaMinBlocks {
   static constexpr int R = PackTraits<T>::R;
   static constexpr int WANT = 2 * NQ * R + 2 * NQ + 40;
   static constexpr int REGS = WANT > 128 ? WANT : 128;
-  // One system: FP64 at Nq = 8 is capped to 128 registers too (140 uncapped, 7
-  // blocks of two warps per SM; capped, 8 blocks with no spills: BK5 40^3
-  // 0.501 -> 0.475 ms, FP64 CG 100 iterations 90.7 -> 87.2 ms; a 96-register
-  // cap spilled and lost, 0.520 ms).  Other single-system shapes stay uncapped.
+  // One system: FP64 at Nq = 8, 10, 12 is capped to 128 registers too (Nq = 8:
+  // 140 uncapped, 7 blocks of two warps per SM; capped, 8 blocks with no
+  // spills: BK5 40^3 0.501 -> 0.475 ms, FP64 CG 100 iterations 90.7 -> 87.2
+  // ms, while a 96-register cap spilled and lost, 0.520 ms; Nq = 10 on 24^3
+  // 0.276 -> 0.263 ms, Nq = 12 on 20^3 0.481 -> 0.315 ms).  FP32 single-system
+  // shapes need fewer registers and stay uncapped.
   static constexpr int V = R > 1 ? (65536 / (ALLOC * REGS) > 0 ? 65536 / (ALLOC * REGS) : 1)
-                                 : (sizeof(F) == 8 && NQ == 8 ? 65536 / (ALLOC * 128) : 1);
+                                 : (sizeof(F) == 8 && (NQ == 8 || NQ == 10 || NQ == 12) ? 65536 / (ALLOC * 128) : 1);
 };
 
 // WITHHOLD >= 0 builds the test-only form: the producer arms the mbarrier of
