@@ -68,6 +68,11 @@ B200_SMS = 148
 # pipe: one wavefront per SM and clock.
 AX_DRAM_BYTES = 1396588800 + 498959616
 AX_SMEM_WAVEFRONTS = 141570589
+# kernel instantiations of the packed four-system FP32 operator, by autotuner form
+AX_KERNELS = {"tma": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,float,Pack<float,4>>",
+              "rb": "ax_rb_kernel<NQ=8,L=4,DOT=0>",
+              "line": "ax_line_kernel<NQ=8,AFFINE=0,Pack<float,4>>",
+              "mma": "ax_mma_pk4_kernel<NQ=8,DOT=0>"}
 
 
 def ax_model_bytes(Ndofs, E, Np, Nf=1, s=8):
@@ -458,6 +463,8 @@ def main():
 
     fused_s = timed(fused)
     ax_s = timed(lambda: bp.ax_hex3d_f32_multi(mesh, NRHS, vec["p1"], AqL, ops))
+    # the form the autotuner chose for this launch (packed FP32 group, not fused)
+    ax_form = bp.tune_report(1, P, 1, False, 4, NRHS, 0, mesh.E)[0]
     E, Np = mesh.E, mesh.Np
     # reference model of the operator with 4-byte values, the q and Aq terms once per
     # right-hand side; the fused step adds the direction update's vectors: r, x
@@ -500,9 +507,11 @@ def main():
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": value / plain["gdof_it_s"],
             "roofline": {"bound": "hbm",
-                         "kernel": "ax_tma_kernel<NQ=8,NF=1,DOT=0,R=4,float,Pack<float,4>> (bp_ax_hex3d_f32_multi, 4 rhs)",
+                         "kernel": AX_KERNELS.get(ax_form, str(ax_form)) + " (bp_ax_hex3d_f32_multi, 4 rhs)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": AX_DRAM_BYTES, "algorithmic_bytes": ax_bytes,
+                         "frac": achieved / peak, "algorithmic_bytes": ax_bytes,
+                         # DRAM bytes and wavefronts were captured with ncu on the TMA form
+                         "traffic": AX_DRAM_BYTES if ax_form == "tma" else None,
                          "launch_ms": ax_s * 1e3,
                          "fused_direction_step": {"kernel": "bp_cg_direction_ax_f32_multi (4 rhs)",
                                                   "launch_ms": fused_s * 1e3, "algorithmic_bytes": fused_bytes,
@@ -510,7 +519,8 @@ def main():
                          # the roof that binds this kernel: shared-memory wavefronts at one per SM and clock
                          # (clock: the median SM clock sampled during the timed step, else the maximum)
                          "smem": {"wavefronts": AX_SMEM_WAVEFRONTS, "sm_mhz": smem_mhz,
-                                  "bound_ms": smem_bound_ms, "frac": smem_bound_ms / (ax_s * 1e3)}},
+                                  "bound_ms": smem_bound_ms, "frac": smem_bound_ms / (ax_s * 1e3)}
+                         if ax_form == "tma" else None},
             "cpu_baseline": cpu,
             "cpu": cpu_info(),
             "configs": extras,
