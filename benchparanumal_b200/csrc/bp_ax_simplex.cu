@@ -16,6 +16,7 @@
 // reference's order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "bp_cg_device.cuh"
@@ -29,10 +30,12 @@ constexpr int kTriThreads = 256;
 // nodes of the degree-N triangle (dim 2) or tetrahedron (dim 3)
 int simplex_np(int dim, int N) { return dim == 2 ? (N + 1) * (N + 2) / 2 : (N + 1) * (N + 2) * (N + 3) / 6; }
 
-// node groups per block (element slots for the forcing) and threads per block (whole warps)
+// node groups per block (element slots for the forcing) and threads per block
+// (whole warps, at most kTriThreads + 32: tetrahedra of degree 11..15 have
+// 364..816 nodes, and their threads walk the nodes of the element in strides)
 static void tri_shape(int Np, int* epb, int* threads) {
   *epb = Np >= kTriThreads ? 1 : kTriThreads / Np;
-  *threads = (*epb * Np + 31) / 32 * 32;
+  *threads = std::min((*epb * Np + 31) / 32 * 32, kTriThreads + 32);
 }
 
 // Thread (n, g) of a block computes node n of the kTriElems elements of group
@@ -43,8 +46,14 @@ static void tri_shape(int Np, int* epb, int* threads) {
 // 43.4 ms (132 registers in the CG form with the p.Ap sum).
 constexpr int kTriElems = 4;
 
+// Triangles are held to three blocks per SM (72 registers instead of 82,
+// a few words of spills): ncu showed two blocks (16 warps) waiting on the
+// matrix loads (long scoreboard); three gave BK5 p=5 5.29 -> 6.18 and p=7
+// 7.46 -> 8.14 TFLOP/s and 100 CG iterations at p=5 32.1 -> 29.4 ms (400x400,
+// the same box).  Tetrahedra need their 110 registers (seven sums of four
+// elements).
 template <class F, int NSM, bool DOT>
-__global__ void __launch_bounds__(kTriThreads + 32)
+__global__ void __launch_bounds__(kTriThreads + 32, NSM == 3 ? 3 : 1)
 ax_simplex_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__ elementList,
               const int32_t* __restrict__ G2L, const F* __restrict__ wJ, const F* __restrict__ ggeo,
               const F* __restrict__ S, const F* __restrict__ MM, F lambda, const F* __restrict__ q,
@@ -68,9 +77,11 @@ ax_simplex_kernel(int Nelements, int Np, int groups, const int32_t* __restrict__
     s_q[i] = v;
   }
   __syncthreads();
-  const int g = t / Np, n = t - g * Np;
+  // one node per thread; with more nodes than threads (one group), the
+  // threads take the element's nodes in strides of the block
+  const int g = t / Np;
   double pdot = 0.0;
-  if (g < groups) {
+  for (int n = t - g * Np; g < groups && n < Np; n += blockDim.x) {
     const F* sq = s_q + (size_t)g * kTriElems * Np;
     const size_t NP2 = (size_t)Np * Np;
     F acc[NSM + 1][kTriElems];   // the S_ab sums, then the mass sum
@@ -118,19 +129,21 @@ tri_mass_local_kernel(int Nelements, int Np, int epb, const int32_t* __restrict_
                       const double* __restrict__ wJ, const double* __restrict__ MM, const double* __restrict__ f,
                       double* __restrict__ bL) {
   extern __shared__ __align__(16) double s_f[];
-  const int t = threadIdx.x;
-  const int es = t / Np, n = t - es * Np;
-  const int e = blockIdx.x * epb + es;
-  const bool active = es < epb && e < Nelements;
-  if (active) {
-    const int32_t id = G2L[(size_t)e * Np + n];
-    s_f[es * Np + n] = id >= 0 ? f[id] : 0.0;
+  for (int i = threadIdx.x; i < epb * Np; i += blockDim.x) {
+    const int es = i / Np, n = i - es * Np, e = blockIdx.x * epb + es;
+    if (e < Nelements) {
+      const int32_t id = G2L[(size_t)e * Np + n];
+      s_f[i] = id >= 0 ? f[id] : 0.0;
+    }
   }
   __syncthreads();
-  if (!active) return;
-  double acc = 0.0;
-  for (int k = 0; k < Np; ++k) acc += __ldg(MM + (size_t)k * Np + n) * s_f[es * Np + k];
-  bL[(size_t)e * Np + n] = wJ[e] * acc;
+  for (int i = threadIdx.x; i < epb * Np; i += blockDim.x) {
+    const int es = i / Np, n = i - es * Np, e = blockIdx.x * epb + es;
+    if (e >= Nelements) continue;
+    double acc = 0.0;
+    for (int k = 0; k < Np; ++k) acc += __ldg(MM + (size_t)k * Np + n) * s_f[es * Np + k];
+    bL[(size_t)e * Np + n] = wJ[e] * acc;
+  }
 }
 
 // diagonal of A_e: sum_ab G_ab S_ab(n,n) + lambda J MM(n,n)
@@ -158,21 +171,23 @@ simplex_rhs_analytic_kernel(int Nelements, int Np, int epb, const double* __rest
                             const double* __restrict__ z, double lambda, double* __restrict__ bL) {
   extern __shared__ __align__(16) double s_f[];
   const double pi = 3.14159265358979323846;
-  const int t = threadIdx.x;
-  const int es = t / Np, n = t - es * Np;
-  const int e = blockIdx.x * epb + es;
-  const bool active = es < epb && e < Nelements;
-  if (active) {
-    const size_t id = (size_t)e * Np + n;
-    const double f = z ? (3 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]) * sin(pi * z[id])
-                       : (2 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]);
-    s_f[es * Np + n] = wJ[e] * f;
+  for (int i = threadIdx.x; i < epb * Np; i += blockDim.x) {
+    const int es = i / Np, e = blockIdx.x * epb + es;
+    if (e < Nelements) {
+      const size_t id = (size_t)e * Np + (i - es * Np);
+      const double f = z ? (3 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]) * sin(pi * z[id])
+                         : (2 * pi * pi + lambda) * sin(pi * x[id]) * sin(pi * y[id]);
+      s_f[i] = wJ[e] * f;
+    }
   }
   __syncthreads();
-  if (!active) return;
-  double acc = 0.0;
-  for (int m = 0; m < Np; ++m) acc += __ldg(MM + (size_t)m * Np + n) * s_f[es * Np + m];
-  bL[(size_t)e * Np + n] = acc;
+  for (int i = threadIdx.x; i < epb * Np; i += blockDim.x) {
+    const int es = i / Np, n = i - es * Np, e = blockIdx.x * epb + es;
+    if (e >= Nelements) continue;
+    double acc = 0.0;
+    for (int m = 0; m < Np; ++m) acc += __ldg(MM + (size_t)m * Np + n) * s_f[es * Np + m];
+    bL[(size_t)e * Np + n] = acc;
+  }
 }
 
 }  // namespace
