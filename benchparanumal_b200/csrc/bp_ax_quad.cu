@@ -99,18 +99,135 @@ ax_quad_kernel(int Nelements, const int32_t* __restrict__ elementList, const int
   if (DOT) fuse_pap(pdot, fuse, s_red);
 }
 
+// Column form (affine factors, NQ <= kQuadColMax): one thread per column i of
+// an element, holding the column's q values and s-fluxes in registers and row
+// and column i of D; shared memory carries only what crosses columns (the rows
+// of q and of the r-flux), and the other reads of D use a slice index that is
+// the same for every lane (broadcasts).  The sums run in the node form's
+// order.  Measured on 800x800 boxes (the same box, two alternating runs): BK5
+// affine p=3 3.59 -> 4.96, p=5 4.34 -> 5.10, p=7 4.77 -> 5.87, p=9 4.61 ->
+// 5.04 TFLOP/s, 100 CG iterations at p=7 123.0 -> 107.1 ms; with stored
+// factors it lost (p=7 3.03 -> 2.48 TB/s: 88-102 registers leave two blocks
+// per SM to wait on the per-node factor loads), so those keep the node form.
+constexpr int kQuadColMax = 10;
+
+template <int NQ>
+struct QuadColShape {
+  static constexpr int EPB = (NQ <= 8 ? 256 : 160) / NQ;   // element slots per block
+  static constexpr int RS = NQ + 1;
+  static constexpr int THREADS = NQ * EPB;
+};
+
+template <int NQ, int NF, bool AFFINE, bool DOT, class F>
+__global__ void __launch_bounds__(QuadColShape<NQ>::THREADS)
+ax_quad_col_kernel(int Nelements, const int32_t* __restrict__ elementList, const int32_t* __restrict__ G2L,
+                   const F* __restrict__ wJ, const F* __restrict__ ggeo, const F* __restrict__ gllw,
+                   const F* __restrict__ Dg, F lambda, const F* __restrict__ q, F* __restrict__ Aq,
+                   const int* __restrict__ skip, CgFuse fuse) {
+  if (skip && *skip) return;
+  using Sh = QuadColShape<NQ>;
+  constexpr int EPB = Sh::EPB, RS = Sh::RS, NP = NQ * NQ;
+  __shared__ F s_D[NQ][NQ];
+  __shared__ F s_w[NQ];
+  __shared__ F s_q[EPB][NQ][RS];   // rows of q (one field at a time)
+  __shared__ F s_r[EPB][NQ][RS];   // rows of the r-flux
+  __shared__ double s_red[Sh::THREADS];
+
+  const int i = threadIdx.x, es = threadIdx.y;
+  const int t = i + NQ * es;
+  const int eidx = blockIdx.x * EPB + es;
+  const bool active = eidx < Nelements;
+  const int e = active ? elementList[eidx] : 0;
+  for (int n = t; n < NP; n += Sh::THREADS) s_D[n / NQ][n % NQ] = Dg[n];
+  if (AFFINE && t < NQ) s_w[t] = gllw[t];
+  __syncthreads();
+  F Di[NQ], Dci[NQ];   // row i and column i of D
+#pragma unroll
+  for (int m = 0; m < NQ; ++m) {
+    Di[m] = s_D[i][m];
+    Dci[m] = s_D[m][i];
+  }
+  F A00 = 0, A01 = 0, A11 = 0, AJ = 0;   // affine factors (the weights w_i w_j applied per node)
+  if (AFFINE && active) {
+    A00 = ggeo[3 * (size_t)e + 0];
+    A01 = ggeo[3 * (size_t)e + 1];
+    A11 = ggeo[3 * (size_t)e + 2];
+    AJ = wJ[e];
+  }
+  double pdot = 0.0;
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    const size_t lb = ((size_t)e * NF + f) * NP + i;
+    F qc[NQ];
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      const int32_t id = active ? G2L[lb + j * NQ] : -1;
+      qc[j] = (id != -1) ? q[id] : F(0);
+      s_q[es][j][i] = qc[j];
+    }
+    __syncthreads();
+    F fs[NQ];
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      F ur = 0, us = 0;
+#pragma unroll
+      for (int m = 0; m < NQ; ++m) {
+        ur += Di[m] * s_q[es][j][m];
+        us += s_D[j][m] * qc[m];
+      }
+      F G00, G01, G11;
+      if (AFFINE) {
+        const F w = s_w[i] * s_w[j];
+        G00 = A00 * w;
+        G01 = A01 * w;
+        G11 = A11 * w;
+      } else {
+        const size_t gb = (size_t)e * NP + j * NQ + i;
+        G00 = active ? ggeo[3 * gb + 0] : F(0);
+        G01 = active ? ggeo[3 * gb + 1] : F(0);
+        G11 = active ? ggeo[3 * gb + 2] : F(0);
+      }
+      s_r[es][j][i] = G00 * ur + G01 * us;
+      fs[j] = G01 * ur + G11 * us;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      const F GwJ = AFFINE ? AJ * (s_w[i] * s_w[j]) : (active ? wJ[(size_t)e * NP + j * NQ + i] : F(0));
+      F ap = qc[j] * lambda * GwJ;
+#pragma unroll
+      for (int m = 0; m < NQ; ++m) {
+        ap += Dci[m] * s_r[es][j][m];
+        ap += s_D[m][j] * fs[m];
+      }
+      if (active) Aq[lb + j * NQ] = ap;
+      if (DOT) pdot += (double)qc[j] * (double)ap;
+    }
+    if (NF > 1) __syncthreads();   // the next field reuses s_q and s_r
+  }
+  if (DOT) fuse_pap(pdot, fuse, s_red);
+}
+
 template <int NQ, class F>
 static int launch_quad_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                           const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda, const F* q, F* Aq,
                           const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
-  using Sh = QuadShape<NQ>;
-  const dim3 block(NQ, NQ, Sh::EPB);
-  const dim3 grid((Nelements + Sh::EPB - 1) / Sh::EPB);
+  constexpr bool COL = NQ <= kQuadColMax;
+  const bool col = COL && d.affine;
+  const int epb = col ? QuadColShape<NQ>::EPB : QuadShape<NQ>::EPB;
+  const dim3 block = col ? dim3(NQ, epb) : dim3(NQ, NQ, epb);
+  const dim3 grid((Nelements + epb - 1) / epb);
   if (nblocks) *nblocks = (int)grid.x;
   const CgFuse Fz = fuse ? *fuse : CgFuse{};
-#define BP_QUAD(NF, AFF, DOT) \
-  ax_quad_kernel<NQ, NF, AFF, DOT, F><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, lambda, \
-                                                            q, Aq, skip, Fz)
+#define BP_QUAD(NF, AFF, DOT)                                                                                        \
+  do {                                                                                                               \
+    if constexpr (COL && AFF)                                                                                        \
+      ax_quad_col_kernel<NQ, NF, AFF, DOT, F><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D, \
+                                                                    lambda, q, Aq, skip, Fz);                        \
+    else                                                                                                             \
+      ax_quad_kernel<NQ, NF, AFF, DOT, F><<<grid, block, 0, s>>>(Nelements, elementList, G2L, wJ, ggeo, gllw, D,     \
+                                                                lambda, q, Aq, skip, Fz);                            \
+  } while (0)
   const bool dot = fuse != nullptr;
   if (d.Nfields == 1) {
     if (d.affine) { if (dot) BP_QUAD(1, true, true); else BP_QUAD(1, true, false); }
