@@ -98,10 +98,12 @@ def test_quad_cg_history_matches_oracle(gpu, oracle, nx, ny, N, affine, pert, nf
     assert np.all(np.abs(hr - hr_o) <= HIST_TOL * hr_o[0])
 
 
-@pytest.mark.parametrize("nf", [1, 2])
-def test_quad_mixed_solve_reaches_tolerance(gpu, oracle, nf):
-    om = oracle.Mesh(12, 10, 0, 6, Nfields=nf, pert=0.1, dim=2)
-    gm = gpu.Mesh(12, 10, N=6, Nfields=nf, pert=0.1, dim=2)
+# affine: the FP32 column form of the operator (one thread per column of nodes)
+@pytest.mark.parametrize("nf,affine", [(1, False), (2, False), (1, True), (2, True)])
+def test_quad_mixed_solve_reaches_tolerance(gpu, oracle, nf, affine):
+    pert = 0.0 if affine else 0.1
+    om = oracle.Mesh(12, 10, 0, 6, Nfields=nf, pert=pert, affine=affine, dim=2)
+    gm = gpu.Mesh(12, 10, N=6, Nfields=nf, pert=pert, affine=affine, dim=2)
     S = gpu.BP(gm, precon="JACOBI", precision="MIXED")
     _, b_o = om.rhs_random(1)
     x = gpu.DeviceBuffer.from_host(np.zeros(om.Ngather))
