@@ -108,7 +108,10 @@ ax_quad_kernel(int Nelements, const int32_t* __restrict__ elementList, const int
 // affine p=3 3.59 -> 4.96, p=5 4.34 -> 5.10, p=7 4.77 -> 5.87, p=9 4.61 ->
 // 5.04 TFLOP/s, 100 CG iterations at p=7 123.0 -> 107.1 ms; with stored
 // factors it lost (p=7 3.03 -> 2.48 TB/s: 88-102 registers leave two blocks
-// per SM to wait on the per-node factor loads), so those keep the node form.
+// per SM to wait on the per-node factor loads), so those keep the node form;
+// staging each slot's stored factors in shared memory first (coalesced loads,
+// 12 slots per block for the space, 142 registers) was slower still: p=7 1.55
+// TB/s.
 constexpr int kQuadColMax = 10;
 
 template <int NQ>
@@ -208,13 +211,22 @@ ax_quad_col_kernel(int Nelements, const int32_t* __restrict__ elementList, const
   if (DOT) fuse_pap(pdot, fuse, s_red);
 }
 
+// element slots per block of the form that runs (the column form exists for NQ <= kQuadColMax)
+template <int NQ>
+int quad_epb(bool col) {
+  if constexpr (NQ <= kQuadColMax)
+    return col ? QuadColShape<NQ>::EPB : QuadShape<NQ>::EPB;
+  else
+    return QuadShape<NQ>::EPB;
+}
+
 template <int NQ, class F>
 static int launch_quad_nq(const bp_ax_desc_t& d, int32_t Nelements, const int32_t* elementList, const int32_t* G2L,
                           const F* wJ, const F* ggeo, const F* gllw, const F* D, F lambda, const F* q, F* Aq,
                           const int* skip, const CgFuse* fuse, cudaStream_t s, int* nblocks) {
   constexpr bool COL = NQ <= kQuadColMax;
   const bool col = COL && d.affine;
-  const int epb = col ? QuadColShape<NQ>::EPB : QuadShape<NQ>::EPB;
+  const int epb = quad_epb<NQ>(col);
   const dim3 block = col ? dim3(NQ, epb) : dim3(NQ, NQ, epb);
   const dim3 grid((Nelements + epb - 1) / epb);
   if (nblocks) *nblocks = (int)grid.x;
